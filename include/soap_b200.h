@@ -1,0 +1,227 @@
+/*
+ * soap_b200.h -- C ABI of libsoapb200.so, a B200 (sm_100a) implementation of
+ * soap_turbo's SOAP descriptor path: get_soap, its Cartesian derivatives and
+ * the soap_contract force vector-Jacobian product.
+ *
+ * Two layers:
+ *
+ *  1. Drop-in entry points with the reference's argument lists and host
+ *     arrays (soapb_get_soap, soapb_soap_contract, ...).  They keep module
+ *     state the way the reference's Fortran module does (basis cache, the
+ *     contract state), on the current CUDA device.  A Fortran iso_c_binding
+ *     module binds exactly these (soap_turbo_b200/fortran/).
+ *
+ *  2. A context API on device pointers and a caller-chosen CUDA stream, for
+ *     callers that keep their neighbour lists on the GPU.  No call of this
+ *     layer synchronises the stream.
+ *
+ * Layouts are the reference's Fortran column-major layouts:
+ *   soap(n_soap, n_sites)             soap[i*n_soap + s]
+ *   soap_cart_der(3, n_soap, n_pairs) cart[(k*n_soap + s)*3 + c]
+ *   G(n_sites, n_soap)                G[s*n_sites + i]
+ *   pair(3, n_pairs)                  pair[k*3 + c]
+ *   mask(n_pairs, n_species)          mask[s*n_pairs + k]  (one byte, 0/1)
+ *   species(max_mult, n_sites)        species[i*max_mult + m] (1-based)
+ *   W, S (n_max, n_max)               W[col*n_max + row]
+ *
+ * Every function returns SOAPB_OK (0) or one of the status codes below;
+ * soapb_last_error() gives the message of the last failure on this thread.
+ */
+#ifndef SOAP_B200_H
+#define SOAP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+enum {
+  SOAPB_OK = 0,
+  SOAPB_ERR_ARGUMENT = 1,        /* bad size, null pointer, unsupported value            */
+  SOAPB_ERR_ALPHA_TOO_LARGE = 2, /* alpha_max above the basis' limit: poly3 > 10,
+                                    poly3gauss > 11 (src/soap_turbo_radial.f90:144-153,
+                                    210-219)                                            */
+  SOAPB_ERR_CONTRACT_STATE = 3,  /* soap_contract without a preceding get_soap with
+                                    contract (src/soap_turbo.f90:1744-1747)             */
+  SOAPB_ERR_COMPRESS_MODE = 4,   /* compress_mode not understood
+                                    (src/soap_turbo_compress.f90:305-306)               */
+  SOAPB_ERR_BASIS = 5,           /* basis other than poly3 / poly3gauss                  */
+  SOAPB_ERR_CUDA = 6,            /* CUDA runtime failure                                 */
+  SOAPB_ERR_NO_DEVICE = 7,       /* no usable sm_100 device                              */
+  SOAPB_ERR_INPUT = 8,           /* non-finite or negative distance, bad CSR, bad mask   */
+  SOAPB_ERR_BASIS_MATRIX = 9     /* overlap matrix not positive definite                 */
+};
+
+enum { SOAPB_BASIS_POLY3 = 0, SOAPB_BASIS_POLY3GAUSS = 1 };
+enum { SOAPB_SCALING_POLYNOMIAL = 0, SOAPB_SCALING_NONE = 1 };
+/* Arithmetic of the descriptor + VJP path. */
+enum {
+  SOAPB_PREC_MIXED = 0, /* FP32 pair/contraction arithmetic; FP64 radial integrals,
+                           W-transform and angular prefactors (the default)         */
+  SOAPB_PREC_FP64 = 1   /* plain FP64, staged like the reference (materialises
+                           soap_cart_der, then contracts)                            */
+};
+/* Layout of the upstream gradient G given to the contract calls. */
+enum {
+  SOAPB_G_SITE_FASTEST = 0, /* the reference's G(n_sites, n_soap)  */
+  SOAPB_G_SOAP_FASTEST = 1  /* G(n_soap, n_sites), soap's own layout */
+};
+
+const char *soapb_last_error(void);
+const char *soapb_version(void);
+
+/* ============================================================ drop-in layer */
+
+/* get_soap (src/soap_turbo.f90:139-169).  Same arguments in the same order,
+ * as plain pointers plus the extents Fortran would carry in the descriptors:
+ * max_species_multiplicity = size(species,1), n_soap = size(soap,1).
+ * basis: "poly3" | "poly3gauss"; scaling_mode: "polynomial" | other.
+ * soap is overwritten (the reference accumulates into it when compressing,
+ * so its callers pass it zeroed; the results then agree).
+ * do_derivatives && !contract: soap_cart_der (3, n_soap, n_atom_pairs) is
+ * written, computed in FP64 as the reference does; otherwise it may be NULL.
+ * do_derivatives && contract: the state for soapb_soap_contract is kept.
+ * do_timing prints per-phase GPU times, as the reference's do_timing does. */
+int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species,
+                   const int32_t *species, int32_t max_species_multiplicity,
+                   const int32_t *species_multiplicity, int32_t n_atom_pairs,
+                   const uint8_t *mask, const double *rjs, const double *thetas,
+                   const double *phis, const int32_t *alpha_max, int32_t l_max,
+                   const double *rcut_hard, const double *rcut_soft, const double *nf,
+                   const double *global_scaling, const double *atom_sigma_r,
+                   const double *atom_sigma_r_scaling, const double *atom_sigma_t,
+                   const double *atom_sigma_t_scaling, const double *amplitude_scaling,
+                   int32_t radial_enhancement, const double *central_weight,
+                   const char *basis, const char *scaling_mode, int32_t do_timing,
+                   int32_t do_derivatives, int32_t compress_soap,
+                   int32_t compress_P_nonzero, const int32_t *compress_P_i,
+                   const int32_t *compress_P_j, const double *compress_P_el,
+                   double *soap, int32_t n_soap, double *soap_cart_der, int32_t contract);
+
+/* soap_contract (src/soap_turbo.f90:1723-1730): pair(1:3,k) =
+ * sgn * sum_s G(i,s) * d soap(s,i) / d r_k, for the batch of the last
+ * soapb_get_soap called with do_derivatives and contract.  G is
+ * G(n_sites, n_soap) (site fastest), soap the normalised descriptor that call
+ * returned.  The extents must match that call. */
+int soapb_soap_contract(const double *soap, const double *G, double sgn, double *pair,
+                        int32_t n_sites, int32_t n_soap, int32_t n_atom_pairs);
+
+/* Module flag legacy_filter_seed (src/soap_turbo_radial.f90:67); default 1. */
+int soapb_set_legacy_filter_seed(int32_t legacy);
+int soapb_get_legacy_filter_seed(int32_t *legacy);
+
+/* Arithmetic of the drop-in layer (SOAPB_PREC_*); default mixed. */
+int soapb_set_precision(int32_t precision);
+
+/* Replace the drop-in layer's basis matrices with caller-supplied ones (the
+ * same W and S the caller feeds another implementation); n_max x n_max,
+ * block diagonal.  Kept until the basis definition changes. */
+int soapb_set_basis_matrices(int32_t n_max, const double *W, const double *S);
+
+/* get_compress_indices (src/soap_turbo_compress.f90:44).  what_to_do =
+ * "get_dim" fills dim and P_nonzero only; "set_indices" also fills P_i, P_j
+ * (1-based) and P_el, each of capacity P_nonzero.  Supported mode: "trivial"
+ * ("Trivial"); other modes return SOAPB_ERR_COMPRESS_MODE. */
+int soapb_get_compress_indices(const char *compress_mode, int32_t n_species,
+                               const int32_t *alpha_max, int32_t l_max, int32_t *dim,
+                               int32_t *P_nonzero, int32_t *P_i, int32_t *P_j, double *P_el,
+                               const char *what_to_do);
+
+/* Overlap S and W = S^{-1/2} of one species' basis, alpha x alpha, computed
+ * in extended precision (get_orthonormalization_matrix_poly3[gauss],
+ * src/soap_turbo_radial.f90:1023-1219). */
+int soapb_orthonormalization_matrix(int32_t basis, int32_t alpha_max, double atom_sigma_r,
+                                    double rcut_hard, double *S, double *W);
+
+/* ============================================================ context layer */
+
+typedef struct soapb_context soapb_context;
+
+/* One descriptor definition: the per-species and scalar hyperparameters of
+ * get_soap plus the compression map.  Arrays are host pointers of length
+ * n_species (P_* of length P_nonzero) and are copied. */
+typedef struct {
+  int32_t n_species;
+  int32_t l_max;
+  int32_t basis;              /* SOAPB_BASIS_*   */
+  int32_t scaling_mode;       /* SOAPB_SCALING_* */
+  int32_t radial_enhancement; /* 0, 1 or 2       */
+  int32_t legacy_filter_seed; /* 1 = reference default */
+  const int32_t *alpha_max;
+  const double *rcut_hard, *rcut_soft, *nf, *global_scaling;
+  const double *atom_sigma_r, *atom_sigma_r_scaling;
+  const double *atom_sigma_t, *atom_sigma_t_scaling;
+  const double *amplitude_scaling, *central_weight;
+  int32_t compress;           /* 0: uncompressed */
+  int32_t P_nonzero;
+  const int32_t *P_i, *P_j;   /* 1-based */
+  const double *P_el;
+} soapb_hyper;
+
+/* One batch of sites: the CSR neighbour list, all DEVICE pointers. */
+typedef struct {
+  int32_t n_sites;
+  int32_t n_atom_pairs;
+  int32_t max_species_multiplicity;
+  const int32_t *n_neigh;              /* n_sites */
+  const int32_t *species;              /* (max_mult, n_sites), 1-based */
+  const int32_t *species_multiplicity; /* n_sites */
+  const uint8_t *mask;                 /* (n_pairs, n_species) */
+  const double *rjs, *thetas, *phis;   /* n_pairs */
+} soapb_batch;
+
+/* Creates a context on `device` (-1: the current device) and builds W, S. */
+int soapb_create(const soapb_hyper *hyper, int32_t device, soapb_context **out);
+int soapb_destroy(soapb_context *ctx);
+/* Caller-supplied basis matrices (host, n_max x n_max, block diagonal). */
+int soapb_set_basis(soapb_context *ctx, const double *W, const double *S);
+int soapb_get_basis(const soapb_context *ctx, double *W, double *S);
+/* n_soap of the definition (compressed length when compressing). */
+int soapb_n_soap(const soapb_context *ctx, int32_t *n_soap);
+/* Work on this cudaStream_t from now on (0 = legacy default stream). */
+int soapb_set_stream(soapb_context *ctx, void *stream);
+/* Work tuning: threads per site CTA (64, 128 or 256; 0 = automatic). */
+int soapb_set_threads_per_site(soapb_context *ctx, int32_t threads);
+
+/* Descriptor of one batch: d_soap (n_soap, n_sites), normalised.  With
+ * keep_for_contract, the expansion coefficients c_nlm and norms stay in the
+ * context for soapb_contract on the same batch. */
+int soapb_descriptor(soapb_context *ctx, const soapb_batch *batch, double *d_soap,
+                     int32_t keep_for_contract);
+
+/* Force VJP on the batch of the last soapb_descriptor(keep_for_contract = 1):
+ * d_pair (3, n_pairs) = sgn * G . d soap / d r, never forming soap_cart_der.
+ * The pair expansions are recomputed per pair from the CSR inputs. */
+int soapb_contract(soapb_context *ctx, const soapb_batch *batch, const double *d_soap,
+                   const double *d_G, int32_t g_layout, double sgn, double *d_pair);
+
+/* Descriptor and force VJP in one kernel, for an upstream gradient known up
+ * front (e.g. a linear model): same outputs as the two calls above. */
+int soapb_descriptor_and_vjp(soapb_context *ctx, const soapb_batch *batch, const double *d_G,
+                             int32_t g_layout, double sgn, double *d_soap, double *d_pair);
+
+/* Plain FP64 form, staged like the reference: radial, angular, c_nlm, power
+ * spectrum, then (when d_cart is not NULL) soap_cart_der (3, n_soap, n_pairs)
+ * with the self column minus the sum of the others. */
+int soapb_descriptor_fp64(soapb_context *ctx, const soapb_batch *batch, double *d_soap,
+                          double *d_cart);
+
+/* pair = sgn * G . soap_cart_der over a materialised soap_cart_der. */
+int soapb_contract_cart_der(soapb_context *ctx, const soapb_batch *batch, const double *d_cart,
+                            const double *d_G, int32_t g_layout, double sgn, double *d_pair);
+
+/* Status of the device-side input checks of the last calls on this context
+ * (waits for the stream): SOAPB_OK or SOAPB_ERR_INPUT, with the first bad
+ * pair index in *bad_pair (or -1). */
+int soapb_check_inputs(soapb_context *ctx, int64_t *bad_pair);
+
+/* Number of kernel launches issued by this context since creation. */
+int soapb_launch_count(const soapb_context *ctx, int64_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SOAP_B200_H */

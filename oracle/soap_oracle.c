@@ -1,0 +1,1066 @@
+/*
+ * soap_oracle.c -- TEST INFRASTRUCTURE, NOT PART OF THE PRODUCT.
+ *
+ * A plain FP64 CPU restatement of soap_turbo's descriptor path (get_soap with
+ * its derivatives and the soap_contract adjoint).  Only the test suite, the
+ * smoke check and the CPU-baseline leg of bench.py load this file's library;
+ * the product path (libsoapb200.so) never links or calls it.
+ *
+ * Every routine follows the reference's arithmetic in the reference's order,
+ * so that FP64 results agree with a gfortran build of the reference to a few
+ * ulps.  Citations are file:line inside the reference project.
+ *
+ * Parity pinning: the reference ships no tests or fixtures and no Fortran
+ * compiler exists on either machine of this project, so the reference itself
+ * cannot be run.  The oracle is pinned by (a) the reference's own poly3tab
+ * W/S tables (src/soap_turbo_radial.f90:1247-1528) against the W built here,
+ * (b) the reference's documented identities (soap_contract equals
+ * soap_cart_der contracted with G, src/soap_turbo.f90:1721; the self column is
+ * minus the sum of the others, :888-892; the unified filter seed makes the
+ * radial derivative a finite-difference-exact derivative,
+ * src/soap_turbo_radial.f90:53-54; unit norm, :805-809), and (c) the scalar
+ * reference functions plm_double / ilexp_double
+ * (src/soap_turbo_functions.f90:44-77, 279-330) against the array routines.
+ *
+ * Layouts are Fortran column-major, as the reference's arguments:
+ *   soap(n_soap, n_sites)              -> soap[i*n_soap + s]
+ *   soap_cart_der(3, n_soap, n_pairs)  -> cart[(k*n_soap + s)*3 + c]
+ *   G(n_sites, n_soap)                 -> G[s*n_sites + i]
+ *   pair(3, n_pairs)                   -> pair[k*3 + c]
+ *   mask(n_pairs, n_species)           -> mask[s*n_pairs + k]   (uint8)
+ *   species(max_mult, n_sites)         -> species[i*max_mult + m]  (1-based)
+ *   W, S (n_max, n_max)                -> W[col*n_max + row]
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <stdint.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define OR_PI 3.141592653589793238462643383279502884
+
+/* ------------------------------------------------------------------------ */
+/* Arguments of get_soap (src/soap_turbo.f90:139-169), flattened.            */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int n_sites, n_species, n_pairs, max_mult, l_max, radial_enhancement;
+  int basis;            /* 0 = poly3, 1 = poly3gauss */
+  int scaling_poly;     /* 1 when scaling_mode == "polynomial" */
+  int legacy_filter_seed;
+  const int *n_neigh, *species, *species_multiplicity;
+  const uint8_t *mask;
+  const double *rjs, *thetas, *phis;
+  const int *alpha_max;
+  const double *rcut_hard, *rcut_soft, *nf, *global_scaling;
+  const double *atom_sigma_r, *atom_sigma_r_scaling;
+  const double *atom_sigma_t, *atom_sigma_t_scaling;
+  const double *amplitude_scaling, *central_weight;
+  int compress, P_nonzero;
+  const int *P_i, *P_j;     /* 1-based, as the reference */
+  const double *P_el;
+  const double *W, *S;      /* n_max x n_max block diagonal, column-major */
+} or_args;
+
+static int kidx(int l, int m) { return l * (l + 1) / 2 + m; } /* 0-based k */
+
+/* ------------------------------------------------------------------------ */
+/* Math primitives                                                           */
+/* ------------------------------------------------------------------------ */
+
+/* get_preflm, src/soap_turbo_functions.f90:215-241 */
+void or_preflm(int lmax, double *preflm) {
+  int k = 0;
+  for (int l = 0; l <= lmax; l++) {
+    double ppi = sqrt((double)(2 * l + 1) / 4.0 / acos(-1.0));
+    double fact2 = 1.0;
+    for (int i = 1; i <= l; i++) fact2 *= (double)i;
+    double fact1 = fact2;
+    for (int m = 0; m <= l; m++) {
+      if (m > 0) {
+        fact1 = fact1 / (double)(l + 1 - m);
+        fact2 = fact2 * (double)(l + m);
+      }
+      preflm[k++] = ppi * sqrt(fact1 / fact2);
+    }
+  }
+}
+
+/* get_plm_array, src/soap_turbo_angular.f90:108-160, with the l-recursion
+ * coefficients of build_plm_tables (:55-74) evaluated inline. */
+void or_plm_array(int lmax, double x, double *p) {
+  double x2 = x * x, sq = sqrt(1.0 - x2);
+  p[0] = 1.0;
+  if (lmax < 1) return;
+  p[1] = x;
+  p[2] = -sq;
+  if (lmax < 2) return;
+  p[3] = 1.5 * x2 - 0.5;
+  p[4] = -3.0 * x * sq;
+  p[5] = 3.0 - 3.0 * x2;
+  for (int l = 3; l <= lmax; l++) {
+    int k = 0;
+    for (int m = 0; m <= l - 2; m++) {
+      k = kidx(l, m);
+      double a = (double)(2 * l - 1) / (double)(l - m);
+      double b = (double)(l - 1 + m) / (double)(l - m);
+      p[k] = a * x * p[k - l] - b * p[k - 2 * l + 1];
+    }
+    k++;
+    p[k] = x * (double)(2 * l - 1) * p[k - l];
+    k++;
+    p[k] = -(double)(2 * l - 1) * sq * p[k - l - 1];
+  }
+}
+
+/* get_plm_array_der, src/soap_turbo_angular.f90:181-248 (tables :80-99).
+ * p must hold P_l^m up to lmax+1. */
+void or_plm_array_der(int lmax, const double *p, double *div_sin, double *der_mul_sin) {
+  for (int l = 0; l <= lmax; l++) {
+    for (int m = 0; m <= l; m++) {
+      int k = kidx(l, m);
+      double part1, part2;
+      if (m == 0) {
+        part1 = (l == 0) ? 0.0 : -0.5 * p[kidx(l, 1)];
+      } else {
+        part1 = 0.5 * (double)(l + m) * (double)(l - m + 1) * p[k - 1];
+      }
+      part2 = (m == l) ? 0.0 : -0.5 * p[k + 1];
+      der_mul_sin[k] = part1 + part2;
+    }
+  }
+  for (int l = 0; l <= lmax; l++) div_sin[kidx(l, 0)] = 0.0;
+  for (int l = 0; l <= lmax; l++) {
+    for (int m = 1; m <= l; m++) {
+      int k = kidx(l, m);
+      double part1 = 0.5 * (double)(l - m + 1) * (double)(l - m + 2) * p[kidx(l + 1, m - 1)];
+      double part2 = 0.5 * p[kidx(l + 1, m + 1)];
+      div_sin[k] = part1 + part2;
+    }
+  }
+}
+
+/* plm_double, src/soap_turbo_functions.f90:44-77 (scalar cross-check) */
+double or_plm_double(int l, int m, double x) {
+  double pmm = 1.0, pl2m = 0.0;
+  if (m > 0) {
+    double sq = sqrt(1.0 - x * x), dfact = -1.0;
+    for (int i = 1; i <= m; i++) { dfact += 2.0; pmm = -pmm * dfact * sq; }
+  }
+  if (l == m) return pmm;
+  double pmp1m = x * (2.0 * (double)m + 1.0) * pmm;
+  if (l == m + 1) return pmp1m;
+  for (int l2 = m + 2; l2 <= l; l2++) {
+    pl2m = (x * (double)(2 * l2 - 1) * pmp1m - (double)(l2 + m - 1) * pmm) / (double)(l2 - m);
+    pmm = pmp1m;
+    pmp1m = pl2m;
+  }
+  return pl2m;
+}
+
+/* get_ilexp, src/soap_turbo_angular.f90:361-422 (semifactorials :344-356).
+ * i_l(x^2) exp(-x^2) for l = 0..lmax; out needs lmax+1 entries. */
+void or_ilexp_array(int lmax, double x, double *out) {
+  const double xcut = 1.0e-7;
+  double x2 = x * x, x4 = x2 * x2;
+  double inv_x2 = (x2 > 0.0) ? 1.0 / x2 : 0.0;
+  double x2pow = x2 * x2;
+  double flm2, flm1;
+  if (x > 0.0) {
+    flm2 = fabs((1.0 - exp(-2.0 * x2)) / 2.0 / x2);
+    flm1 = fabs((x2 - 1.0 + exp(-2.0 * x2) * (x2 + 1.0)) / 2.0 / x4);
+  } else {
+    flm2 = 1.0;
+    flm1 = 0.0;
+  }
+  double fact = 1.0;
+  for (int l = 0; l <= lmax; l++) {
+    if (l > 0) fact *= (2.0 * (double)l + 1.0);
+    if (l == 0) {
+      out[0] = (x < xcut) ? 1.0 - x2 : flm2;
+    } else if (l == 1) {
+      out[1] = (x2 / 1000.0 < xcut) ? (x2 - x4) / fact : flm1;
+    } else {
+      double ratio = x2pow / fact, fl;
+      if (ratio * (double)l < xcut) fl = ratio;
+      else fl = fabs(flm2 - (2.0 * (double)l - 1.0) * inv_x2 * flm1);
+      x2pow *= x2;
+      flm2 = flm1;
+      flm1 = fl;
+      out[l] = fl;
+    }
+  }
+}
+
+/* ilexp_double, src/soap_turbo_functions.f90:279-330 (scalar cross-check) */
+double or_ilexp_double(int l, double x) {
+  const double xcut = 1.0e-7;
+  double x2 = x * x, x4 = pow(x, 4.0), fact = 1.0;
+  if (l == 0 && x < xcut) return 1.0 - x2;
+  for (int i = 1; i <= l; i++) fact *= (2.0 * (double)i + 1.0);
+  if (l == 1 && x2 / 1000.0 < xcut) return (x2 - x4) / fact;
+  if (l > 1 && pow(x2, (double)l) / fact * (double)l < xcut) return pow(x2, (double)l) / fact;
+  double flm2 = fabs((1.0 - exp(-2.0 * x2)) / 2.0 / x2);
+  double flm1 = fabs((x2 - 1.0 + exp(-2.0 * x2) * (x2 + 1.0)) / 2.0 / x4);
+  if (l == 0) return flm2;
+  if (l == 1) return flm1;
+  double fl = 0.0;
+  for (int i = 2; i <= l; i++) {
+    fl = fabs(flm2 - (2.0 * (double)i - 1.0) / x2 * flm1);
+    flm2 = flm1;
+    flm1 = fl;
+  }
+  return fl;
+}
+
+/* get_ilexp_der, src/soap_turbo_angular.f90:436-463.  il needs lmax+2
+ * entries (the l = 0 term reads il[1]). */
+static void or_ilexp_der(const double *il, int lmax, double rj, double sig, double scaling, double *der) {
+  double c1 = 2.0 * rj / (sig * sig), c2 = 1.0 - scaling * rj / sig;
+  for (int l = 0; l <= lmax; l++) der[l] = 0.0;
+  if (rj < 1.0e-5) return;
+  der[0] = c1 * (il[1] - il[0]);
+  for (int l = 1; l <= lmax; l++)
+    der[l] = (-c1 - (double)(2 * l + 2) / rj) * il[l] + c1 * il[l - 1];
+  for (int l = 0; l <= lmax; l++) der[l] *= c2;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Orthonormalisation matrices                                               */
+/* ------------------------------------------------------------------------ */
+
+/* Overlap of the primitive poly3 functions, src/soap_turbo_radial.f90:1041-1047 */
+void or_overlap_poly3(int a, double *S) {
+  for (int i = 1; i <= a; i++) {
+    S[(i - 1) * a + (i - 1)] = 1.0;
+    for (int j = i + 1; j <= a; j++) {
+      double v = sqrt((double)(5 + 2 * i) * (double)(5 + 2 * j)) / (double)(5 + i + j);
+      S[(j - 1) * a + (i - 1)] = v;
+      S[(i - 1) * a + (j - 1)] = v;
+    }
+  }
+}
+
+/* Overlap of poly3 + origin Gaussian, src/soap_turbo_radial.f90:1133-1172
+ * (N_a at :82-96 with rcut = 1). */
+void or_overlap_poly3gauss(int a, double sigma_in, double rcut_in, double *S) {
+  for (int i = 1; i <= a - 1; i++) {
+    S[(i - 1) * a + (i - 1)] = 1.0;
+    for (int j = i + 1; j <= a - 1; j++) {
+      double v = sqrt((double)(5 + 2 * i) * (double)(5 + 2 * j)) / (double)(5 + i + j);
+      S[(j - 1) * a + (i - 1)] = v;
+      S[(i - 1) * a + (j - 1)] = v;
+    }
+  }
+  double sig = sigma_in / rcut_in, rc = 1.0, s2 = sig * sig;
+  double sq2 = sqrt(2.0), pi = acos(-1.0);
+  double I_n = 0.0, N_n = 1.0;
+  double N_np1 = sqrt(rc / (double)(2 * (-2) + 5));
+  double I_np1 = sqrt(pi / 2.0) * sig * erf(rc / sq2 / sig) / N_np1;
+  double C2 = s2 / rc;
+  for (int n = -1; n <= a - 1; n++) {
+    C2 = C2 * rc;
+    double N_np2 = sqrt(rc / (double)(2 * n + 5));
+    double I_np2 = s2 * (double)(n + 1) * N_n / N_np2 * I_n + N_np1 * rc / N_np2 * I_np1 - C2 / N_np2;
+    if (n > 0) {
+      double v = I_np2 * sq2 / sqrt(sig) / pow(pi, 0.25);
+      S[(n - 1) * a + (a - 1)] = v;
+      S[(a - 1) * a + (n - 1)] = v;
+    }
+    N_n = N_np1;
+    N_np1 = N_np2;
+    I_n = I_np1;
+    I_np1 = I_np2;
+  }
+  S[(a - 1) * a + (a - 1)] = 1.0;
+}
+
+/* W = S^{-1/2}.  The reference forms it as SVD -> U sqrt(sigma) V^T ->
+ * Cholesky inverse (src/soap_turbo_radial.f90:1052-1087); for a symmetric
+ * positive definite S that is the inverse principal square root, computed
+ * here from a cyclic Jacobi eigendecomposition in long double.  Returns 0,
+ * or 1 if S is not positive definite. */
+int or_inverse_sqrt(int a, const double *S, double *W) {
+  long double A[16 * 16], V[16 * 16];
+  if (a > 16 || a < 1) return 2;
+  for (int i = 0; i < a * a; i++) A[i] = S[i];
+  for (int i = 0; i < a; i++)
+    for (int j = 0; j < a; j++) V[j * a + i] = (i == j) ? 1.0L : 0.0L;
+  for (int sweep = 0; sweep < 100; sweep++) {
+    long double off = 0.0L;
+    for (int p = 0; p < a; p++)
+      for (int q = p + 1; q < a; q++) off += A[q * a + p] * A[q * a + p];
+    if (off < 1.0e-70L) break;
+    for (int p = 0; p < a; p++) {
+      for (int q = p + 1; q < a; q++) {
+        long double apq = A[q * a + p];
+        if (apq == 0.0L) continue;
+        long double app = A[p * a + p], aqq = A[q * a + q];
+        long double theta = (aqq - app) / (2.0L * apq);
+        long double t = (theta >= 0 ? 1.0L : -1.0L) / (fabsl(theta) + sqrtl(theta * theta + 1.0L));
+        long double c = 1.0L / sqrtl(t * t + 1.0L), s = t * c;
+        for (int k = 0; k < a; k++) {
+          long double akp = A[p * a + k], akq = A[q * a + k];
+          A[p * a + k] = c * akp - s * akq;
+          A[q * a + k] = s * akp + c * akq;
+        }
+        for (int k = 0; k < a; k++) {
+          long double apk = A[k * a + p], aqk = A[k * a + q];
+          A[k * a + p] = c * apk - s * aqk;
+          A[k * a + q] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < a; k++) {
+          long double vkp = V[p * a + k], vkq = V[q * a + k];
+          V[p * a + k] = c * vkp - s * vkq;
+          V[q * a + k] = s * vkp + c * vkq;
+        }
+      }
+    }
+  }
+  long double d[16];
+  for (int i = 0; i < a; i++) {
+    if (!(A[i * a + i] > 0.0L)) return 1;
+    d[i] = 1.0L / sqrtl(A[i * a + i]);
+  }
+  for (int i = 0; i < a; i++)
+    for (int j = 0; j < a; j++) {
+      long double s = 0.0L;
+      for (int k = 0; k < a; k++) s += V[k * a + i] * d[k] * V[k * a + j];
+      W[j * a + i] = (double)s;
+    }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Radial expansion: radial_expansion_kernel + process_block,                */
+/* src/soap_turbo_radial.f90:281-1004, one pair at a time.                   */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int alpha, n_poly, n_hi, with_gauss, unified, has_filter, do_der;
+  double rcut_soft, atom_sigma, c, dr, sqrt_rcut, inv_sqrt_rcut, inv_rcut;
+  double q, drnf, sigma_sq0, N_gauss, inv_Nm2, amp_scaling, cw;
+  int do_central, scaling_poly, radial_enhancement;
+  double Nv[32], ra[32], rb[32], rc[32], R1[32], R2[32]; /* index n+4 */
+  const double *W; int ldw;                                /* alpha x alpha block */
+} or_radial_setup;
+
+#define NI(n) ((n) + 4)
+
+static void or_radial_init(or_radial_setup *s, int alpha, double rcut_soft_in, double rcut_hard_in,
+                           double sigma_in, double sigma_scaling, double amp_scaling, double nf,
+                           const double *W, int ldw, int scaling_poly, int radial_enhancement,
+                           int do_der, int do_central, double central_weight, int with_gauss,
+                           int legacy_seed) {
+  memset(s, 0, sizeof(*s));
+  s->alpha = alpha;
+  s->inv_rcut = 1.0 / rcut_hard_in;                                 /* :459-464 */
+  s->rcut_soft = rcut_soft_in * s->inv_rcut;
+  s->atom_sigma = sigma_in * s->inv_rcut;
+  s->dr = 1.0 - s->rcut_soft;
+  s->sqrt_rcut = sqrt(rcut_hard_in);
+  s->inv_sqrt_rcut = 1.0 / s->sqrt_rcut;
+  s->sigma_sq0 = s->atom_sigma * s->atom_sigma;                     /* :467-468 */
+  s->N_gauss = sqrt(2.0 / s->atom_sigma) / pow(OR_PI, 0.25);
+  s->has_filter = s->dr > 0.0;                                      /* :475-481 */
+  if (s->has_filter) { s->drnf = s->dr / nf; s->q = s->drnf * s->drnf; }
+  s->n_poly = with_gauss ? alpha - 1 : alpha;                       /* :483-491 */
+  s->n_hi = s->n_poly + (do_der ? 2 : 0);
+  s->with_gauss = with_gauss;
+  s->unified = !legacy_seed;
+  s->do_der = do_der;
+  s->c = sigma_scaling;
+  s->amp_scaling = amp_scaling;
+  s->cw = central_weight;
+  s->do_central = do_central;
+  s->scaling_poly = scaling_poly;
+  s->radial_enhancement = radial_enhancement;
+  s->W = W;
+  s->ldw = ldw;
+  s->Nv[NI(-3)] = 1.0;                                              /* :503-513 */
+  for (int n = -2; n <= alpha + 4; n++) s->Nv[NI(n)] = sqrt(1.0 / (double)(2 * n + 5));
+  for (int n = -1; n <= s->n_hi; n++) {
+    s->ra[NI(n)] = (double)(n + 1) * s->Nv[NI(n - 2)] / s->Nv[NI(n)];
+    s->rb[NI(n)] = s->Nv[NI(n - 1)] / s->Nv[NI(n)];
+    s->rc[NI(n)] = 1.0 / s->Nv[NI(n)];
+  }
+  s->ra[NI(-1)] = 0.0;
+  s->inv_Nm2 = 1.0 / s->Nv[NI(-2)];
+  for (int n = 1; n <= s->n_poly; n++) {                            /* :515-519 */
+    s->R1[NI(n)] = s->Nv[NI(n + 1)] / s->Nv[NI(n)];
+    s->R2[NI(n)] = s->Nv[NI(n + 2)] / s->Nv[NI(n)];
+  }
+}
+
+/* One pair of process_block (src/soap_turbo_radial.f90:550-1002).  rj_in is
+ * the unscaled distance.  Writes alpha values to out (and der if do_der). */
+static void or_radial_pair(const or_radial_setup *s, double rj_in, int is_central, double *out, double *der) {
+  const double pi = acos(-1.0), sq2 = sqrt(2.0), isq2 = 1.0 / sq2;
+  const double sqpi2 = sqrt(pi / 2.0), sq2pi = sqrt(2.0 / pi), sq8pi = sqrt(8.0 / pi);
+  const int a = s->alpha, n_hi = s->n_hi, n_poly = s->n_poly;
+  const double c = s->c, rs = s->rcut_soft, dr = s->dr;
+  double T1[40], T2[40], pol[40], DT[40], dtot[40];
+  double rj = rj_in * s->inv_rcut;
+  for (int i = 0; i < 40; i++) { T1[i] = T2[i] = pol[i] = DT[i] = dtot[i] = 0.0; }
+
+  double sig = s->atom_sigma + c * rj, s2 = sig * sig;               /* :560-570 */
+  double isig = 1.0 / sig, is2 = isig * isig, is3 = is2 * isig;
+
+  double amp, ampd;                                                  /* :589-635 */
+  if (!s->scaling_poly) {
+    amp = 1.0; ampd = 0.0;
+  } else if (s->amp_scaling == 0.0) {
+    amp = isig; ampd = -c * is2;
+  } else if (s->amp_scaling == 1.0) {
+    double h = 1.0 + 2.0 * (rj * rj * rj) - 3.0 * rj * rj;
+    double hp = 6.0 * rj * rj - 6.0 * rj;
+    double g = isig * h;
+    amp = (h <= 1.0e-10) ? 0.0 : g;
+    ampd = (h <= 1.0e-10) ? 0.0 : hp * isig - c * isig * g;
+  } else {
+    double h = 1.0 + 2.0 * (rj * rj * rj) - 3.0 * rj * rj;
+    if (h <= 1.0e-10) { amp = 0.0; ampd = 0.0; }
+    else {
+      double hp = 6.0 * rj * rj - 6.0 * rj, aa = s->amp_scaling;
+      amp = isig * pow(h, aa);
+      ampd = aa * pow(h, aa - 1.0) * hp * isig - c * isig * amp;
+    }
+  }
+  if (s->do_central && s->cw != 1.0 && is_central) { amp *= s->cw; ampd *= s->cw; } /* :638-646 */
+  if (s->radial_enhancement == 1) {                                  /* :651-670 */
+    double g = rj + sq2pi * sig, f = 1.0 + sq2pi * c;
+    ampd = amp * f + ampd * g;
+    amp = amp * g;
+  } else if (s->radial_enhancement == 2) {
+    double g = rj * rj + s2 + sq8pi * sig * rj;
+    double f = 2.0 * rj + 2.0 * sig * c + sq8pi * sig + sq8pi * rj * c;
+    ampd = amp * f + ampd * g;
+    amp = amp * g;
+  }
+
+  /* inner overlap on [0, rcut_soft], :676-698 */
+  double es = exp(-0.5 * (rs - rj) * (rs - rj) * is2);
+  double e0 = exp(-0.5 * rj * rj * is2);
+  double C1 = s2 * es, C2 = s2 * e0;
+  T1[NI(-3)] = 0.0;
+  T1[NI(-2)] = sqpi2 * sig * (erf((rs - rj) * isq2 * isig) + erf(rj * isq2 * isig)) * s->inv_Nm2;
+  for (int n = -1; n <= n_hi; n++) {
+    if (n >= 0) C1 = C1 * dr;
+    T1[NI(n)] = s2 * s->ra[NI(n)] * T1[NI(n - 2)] - s->rb[NI(n)] * (rj - 1.0) * T1[NI(n - 1)]
+                + (C1 - C2) * s->rc[NI(n)];
+  }
+  if (s->do_der && n_poly >= 1 && !s->unified) {                     /* :701-714 */
+    double f = rj - 1.0, g = c * f * isig;
+    double ca = f * is2 * (g - 1.0), cb = is2 * (2.0 * g - 1.0), cc = c * is3;
+    for (int n = 1; n <= n_poly; n++)
+      DT[NI(n)] = ca * T1[NI(n)] + s->R1[NI(n)] * cb * T1[NI(n + 1)] + s->R2[NI(n)] * cc * T1[NI(n + 2)];
+  }
+
+  double pref = 0.0;
+  if (s->has_filter) {                                               /* :721-795 */
+    double q = s->q, drnf = s->drnf;
+    double den = s2 + q, iD = 1.0 / den, sqiD = sqrt(iD);
+    double sgf = sig * drnf * sqiD;
+    double rjf = (s2 * rs + q * rj) * iD;
+    double sf2 = sgf * sgf;
+    int keep = (rs - rj) < 4.0 * sig;
+    double isgf = 1.0 / sgf, isf2 = isgf * isgf;
+    pref = keep ? exp(-0.5 * (rs - rj) * (rs - rj) * iD) : 0.0;
+    double C2f = sf2 * exp(-0.5 * (rs - rjf) * (rs - rjf) * isf2);
+    T2[NI(-3)] = 0.0;
+    T2[NI(-2)] = sqpi2 * sgf * (erf((1.0 - rjf) * isq2 * isgf) - erf((rs - rjf) * isq2 * isgf)) * s->inv_Nm2;
+    for (int n = -1; n <= n_hi; n++) {
+      if (n >= 0) C2f = C2f * dr;
+      T2[NI(n)] = sf2 * s->ra[NI(n)] * T2[NI(n - 2)] - s->rb[NI(n)] * (rjf - 1.0) * T2[NI(n - 1)]
+                  - C2f * s->rc[NI(n)];
+      if (n == -1 && s->unified)
+        T2[NI(-1)] = T2[NI(-1)] + sf2 * exp(-0.5 * (1.0 - rjf) * (1.0 - rjf) * isf2) * s->rc[NI(-1)];
+    }
+    if (s->do_der && n_poly >= 1 && !s->unified) {
+      double f = rs - rj;
+      double dpref = pref * (f * iD + f * f * iD * iD * sig * c);
+      double drjf = (2.0 * sig * rs * c + q) * iD - (s2 * rs + q * rj) * 2.0 * sig * c * iD * iD;
+      double dsgf = c * drnf * sqiD * (1.0 - s2 * iD);
+      double ff = rjf - 1.0, g = dsgf * ff * isgf;
+      double ca = pref * ff * isf2 * (g - drjf);
+      double cb = pref * isf2 * (2.0 * g - drjf);
+      double cc = pref * dsgf * isgf * isf2;
+      for (int n = 1; n <= n_poly; n++)
+        DT[NI(n)] = DT[NI(n)] + ca * T2[NI(n)] + s->R1[NI(n)] * cb * T2[NI(n + 1)]
+                    + s->R2[NI(n)] * cc * T2[NI(n + 2)] + dpref * T2[NI(n)];
+    }
+  } else {
+    for (int n = 1; n <= n_hi; n++) T2[NI(n)] = 0.0;
+  }
+  for (int n = 1; n <= n_hi; n++) pol[NI(n)] = T1[NI(n)] + pref * T2[NI(n)];   /* :808-812 */
+
+  if (s->do_der && n_poly >= 1 && s->unified) {                      /* :825-836 */
+    double f = 1.0 - rj;
+    double g0 = f * is2 + c * f * f * is3;
+    double g1 = -(is2 + 2.0 * c * f * is3);
+    double g2 = c * is3;
+    for (int n = 1; n <= n_poly; n++)
+      DT[NI(n)] = g0 * pol[NI(n)] + s->R1[NI(n)] * g1 * pol[NI(n + 1)] + s->R2[NI(n)] * g2 * pol[NI(n + 2)];
+  }
+
+  if (s->with_gauss) {                                               /* :875-908 */
+    double ss2 = s->sigma_sq0 + s2, iss = 1.0 / ss2, siss = sqrt(iss);
+    int gm = rj < 4.0 * (s->atom_sigma + sig);
+    double ge = gm ? s->N_gauss * e0 : 0.0;
+    double M0 = gm ? exp(-0.5 * rj * rj * iss) * sqpi2 * sig * s->atom_sigma * siss
+                     * (1.0 + erf(s->atom_sigma * isig * rj * isq2 * siss)) * s->N_gauss
+                   : 0.0;
+    pol[NI(a)] = M0;
+    if (s->do_der) {
+      double sc0 = s->sigma_sq0 * s2 * iss, pp = s2 * rj * iss;
+      double M1 = sc0 * ge - pp * M0;
+      double M2 = sc0 * ge * (-rj) - pp * M1 + sc0 * M0;
+      DT[NI(a)] = M1 * is2 + c * M2 * is3;
+    }
+  }
+
+  if (s->do_der) {                                                   /* :911-942 */
+    for (int n = 1; n <= a; n++) dtot[NI(n)] = amp * DT[NI(n)] + ampd * pol[NI(n)];
+    for (int n = 1; n <= a; n++) {
+      double acc = s->W[0 * s->ldw + (n - 1)] * dtot[NI(1)];
+      for (int m = 2; m <= a; m++) acc = acc + s->W[(m - 1) * s->ldw + (n - 1)] * dtot[NI(m)];
+      der[n - 1] = acc * s->inv_sqrt_rcut;
+    }
+  }
+  for (int n = 1; n <= a; n++) {                                     /* :962-976 */
+    double acc = s->W[0 * s->ldw + (n - 1)] * pol[NI(1)];
+    for (int m = 2; m <= a; m++) acc = acc + s->W[(m - 1) * s->ldw + (n - 1)] * pol[NI(m)];
+    out[n - 1] = amp * acc * s->sqrt_rcut;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Per-call state shared by get_soap and soap_contract                       */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int n_sites, n_pairs, n_max, k_max, l_max, n_soap, n_soap_unc, compress, P_nonzero;
+  int *k_first;
+  double *rad, *rad_der;                          /* (n_max, n_pairs) */
+  double *ang, *ang_r, *ang_a, *ang_p;            /* complex (k_max, n_pairs): re,im interleaved */
+  double *cnk;                                    /* complex (k_max, n_max, n_sites) */
+  double *sqrt_dot_p;                             /* n_sites */
+  unsigned char *skip;                            /* n_soap_unc */
+  const int *P_i, *P_j; const double *P_el;
+  const double *rjs, *thetas, *phis; const int *n_neigh;
+} or_ctx;
+
+void or_ctx_free(or_ctx *c) {
+  if (!c) return;
+  free(c->k_first); free(c->rad); free(c->rad_der);
+  free(c->ang); free(c->ang_r); free(c->ang_a); free(c->ang_p);
+  free(c->cnk); free(c->sqrt_dot_p); free(c->skip);
+  free(c);
+}
+
+/* The species blocks of the radial basis, src/soap_turbo.f90:256-264 */
+static void species_blocks(const or_args *a, int *i_beg, int *n_max) {
+  int acc = 0;
+  for (int s = 0; s < a->n_species; s++) { i_beg[s] = acc; acc += a->alpha_max[s]; }
+  *n_max = acc;
+}
+
+/* get_soap, src/soap_turbo.f90:139-1037.
+ *   soap:          (n_soap, n_sites), overwritten and normalised
+ *   soap_cart_der: (3, n_soap, n_pairs) or NULL; overwritten (the reference
+ *                  accumulates into the self columns, so its callers zero it)
+ *   ctx_out:       when non-NULL, receives the state soap_contract needs
+ *                  (the reference's contract = .true.; :1008-1035)
+ * Returns n_soap, or a negative code. */
+int or_get_soap(const or_args *a, int do_derivatives, double *soap, double *soap_cart_der, or_ctx **ctx_out) {
+  const double pi = acos(-1.0);
+  int i_beg[64], n_max;
+  if (a->n_species > 64) return -1;
+  species_blocks(a, i_beg, &n_max);
+  const int l_max = a->l_max, k_max = (l_max + 1) * (l_max + 2) / 2;
+  const int n_pairs = a->n_pairs, n_sites = a->n_sites;
+  const int n_soap_unc = n_max * (n_max + 1) / 2 * (l_max + 1);      /* :396 */
+  const int need_der = do_derivatives;
+
+  or_ctx *c = (or_ctx *)calloc(1, sizeof(or_ctx));
+  c->n_sites = n_sites; c->n_pairs = n_pairs; c->n_max = n_max; c->k_max = k_max; c->l_max = l_max;
+  c->n_soap_unc = n_soap_unc;
+  c->k_first = (int *)malloc(sizeof(int) * (n_sites + 1));
+  c->rad = (double *)calloc((size_t)n_max * n_pairs + 1, sizeof(double));
+  c->rad_der = (double *)calloc((size_t)n_max * n_pairs + 1, sizeof(double));
+  c->ang = (double *)calloc((size_t)2 * k_max * n_pairs + 1, sizeof(double));
+  if (need_der) {
+    c->ang_r = (double *)calloc((size_t)2 * k_max * n_pairs + 1, sizeof(double));
+    c->ang_a = (double *)calloc((size_t)2 * k_max * n_pairs + 1, sizeof(double));
+    c->ang_p = (double *)calloc((size_t)2 * k_max * n_pairs + 1, sizeof(double));
+  }
+  c->cnk = (double *)calloc((size_t)2 * k_max * n_max * n_sites + 1, sizeof(double));
+  c->sqrt_dot_p = (double *)calloc((size_t)n_sites + 1, sizeof(double));
+  c->skip = (unsigned char *)calloc((size_t)n_soap_unc + 1, 1);
+  c->rjs = a->rjs; c->thetas = a->thetas; c->phis = a->phis; c->n_neigh = a->n_neigh;
+  int k2 = 0;
+  for (int i = 0; i < n_sites; i++) { c->k_first[i] = k2; k2 += a->n_neigh[i]; }
+  c->k_first[n_sites] = k2;
+
+  /* ---- radial, per species (:491-544 -> src/soap_turbo_radial.f90:281-384) */
+  for (int sp = 0; sp < a->n_species; sp++) {
+    int alpha = a->alpha_max[sp];
+    int with_gauss = a->basis == 1;
+    int do_central = with_gauss ? 0 : (a->central_weight[sp] != 0.0);  /* :238-245; :232-238 */
+    or_radial_setup st;
+    or_radial_init(&st, alpha, a->rcut_soft[sp], a->rcut_hard[sp], a->atom_sigma_r[sp],
+                   a->atom_sigma_r_scaling[sp], a->amplitude_scaling[sp], a->nf[sp],
+                   a->W + (size_t)i_beg[sp] * n_max + i_beg[sp], n_max, a->scaling_poly,
+                   a->radial_enhancement, need_der, do_central, a->central_weight[sp], with_gauss,
+                   a->legacy_filter_seed);
+    const double gsc = a->global_scaling[sp];
+    #pragma omp parallel for schedule(dynamic, 16)
+    for (int i = 0; i < n_sites; i++) {
+      for (int j = 0; j < a->n_neigh[i]; j++) {
+        int k = c->k_first[i] + j;
+        double *out = c->rad + (size_t)k * n_max + i_beg[sp];
+        double *der = c->rad_der + (size_t)k * n_max + i_beg[sp];
+        for (int n = 0; n < alpha; n++) { out[n] = 0.0; der[n] = 0.0; }   /* :328-340 */
+        if (j == 0 && !do_central) continue;                               /* :342-355 */
+        if (a->rjs[k] >= a->rcut_hard[sp]) continue;
+        if (!a->mask[(size_t)sp * n_pairs + k]) continue;
+        double o[32], d[32];
+        or_radial_pair(&st, a->rjs[k], j == 0, o, d);
+        for (int n = 0; n < alpha; n++) {
+          out[n] = o[n] * gsc;                                             /* :510-511, :532-533 */
+          if (need_der) der[n] = d[n] * gsc;
+        }
+      }
+    }
+  }
+
+  /* ---- angular, src/soap_turbo_angular.f90:485-617 */
+  double rcut_max = 0.0;
+  for (int sp = 0; sp < a->n_species; sp++) if (a->rcut_hard[sp] > rcut_max) rcut_max = a->rcut_hard[sp];
+  double *preflm = (double *)malloc(sizeof(double) * k_max);
+  or_preflm(l_max, preflm);
+  {
+    const double rcut2 = rcut_max * rcut_max;
+    #pragma omp parallel for schedule(dynamic, 64)
+    for (int k = 0; k < n_pairs; k++) {
+      double plm[128], div_sin[128], der_mul_sin[128], il[32], ild[32];
+      double pm_re[32], pm_im[32];
+      double rj = a->rjs[k];
+      int i_sp = -1;
+      if (rj < rcut_max)
+        for (int s = 0; s < a->n_species; s++) if (a->mask[(size_t)s * n_pairs + k]) { i_sp = s; break; }
+      double *A = c->ang + (size_t)2 * k_max * k;
+      if (i_sp < 0) {
+        for (int kk = 0; kk < 2 * k_max; kk++) A[kk] = 0.0;
+        if (need_der)
+          for (int kk = 0; kk < 2 * k_max; kk++) {
+            c->ang_r[(size_t)2 * k_max * k + kk] = 0.0;
+            c->ang_a[(size_t)2 * k_max * k + kk] = 0.0;
+            c->ang_p[(size_t)2 * k_max * k + kk] = 0.0;
+          }
+        continue;
+      }
+      double phi = a->phis[k], x = cos(a->thetas[k]);
+      double sig = a->atom_sigma_t[i_sp] + a->atom_sigma_t_scaling[i_sp] * rj;
+      double amplitude = rcut2 / (sig * sig);
+      /* get_eimphi_conjg, :267-329 */
+      or_ilexp_array(l_max + 1, rj / sig, il);
+      double cosm2 = cos(phi), cosphi2 = 2.0 * cosm2, sinm2 = -sin(phi), cosm1 = 1.0, sinm1 = 0.0;
+      pm_re[0] = 1.0; pm_im[0] = 0.0;
+      for (int l = 1; l <= l_max; l++) {
+        double cos0 = cosphi2 * cosm1 - cosm2, sin0 = cosphi2 * sinm1 - sinm2;
+        cosm2 = cosm1; sinm2 = sinm1; cosm1 = cos0; sinm1 = sin0;
+        pm_re[l] = cos0; pm_im[l] = -sin0;
+      }
+      if (need_der) {
+        or_ilexp_der(il, l_max, rj, sig, a->atom_sigma_t_scaling[i_sp], ild);
+        or_plm_array(l_max + 1, x, plm);
+        or_plm_array_der(l_max, plm, div_sin, der_mul_sin);
+        double sig_fac = 2.0 * a->atom_sigma_t_scaling[i_sp] / sig;
+        double *Ar = c->ang_r + (size_t)2 * k_max * k, *Aa = c->ang_a + (size_t)2 * k_max * k;
+        double *Ap = c->ang_p + (size_t)2 * k_max * k;
+        for (int l = 0; l <= l_max; l++)
+          for (int m = 0; m <= l; m++) {
+            int kk = kidx(l, m);
+            double e_re = il[l] * pm_re[m], e_im = il[l] * pm_im[m];        /* eimphi */
+            double er_re = ild[l] * pm_re[m], er_im = ild[l] * pm_im[m];    /* eimphi_rad_der */
+            double u = amplitude * preflm[kk];
+            double v = u * plm[kk];
+            double ec_re = v * e_re, ec_im = v * e_im;
+            A[2 * kk] = ec_re; A[2 * kk + 1] = ec_im;
+            Ar[2 * kk] = v * er_re - sig_fac * ec_re;
+            Ar[2 * kk + 1] = v * er_im - sig_fac * ec_im;
+            double w = u * div_sin[kk];
+            double ez_re = w * e_re, ez_im = w * e_im;
+            Aa[2 * kk] = -ez_im; Aa[2 * kk + 1] = ez_re;
+            double w2 = u * der_mul_sin[kk];
+            Ap[2 * kk] = w2 * e_re; Ap[2 * kk + 1] = w2 * e_im;
+          }
+      } else {
+        or_plm_array(l_max, x, plm);
+        for (int l = 0; l <= l_max; l++)
+          for (int m = 0; m <= l; m++) {
+            int kk = kidx(l, m);
+            double e_re = il[l] * pm_re[m], e_im = il[l] * pm_im[m];
+            double v = amplitude * preflm[kk] * plm[kk];
+            A[2 * kk] = v * e_re; A[2 * kk + 1] = v * e_im;
+          }
+      }
+    }
+  }
+
+  /* ---- cnk, src/soap_turbo.f90:619-664 */
+  #pragma omp parallel for schedule(dynamic, 16)
+  for (int i = 0; i < n_sites; i++) {
+    double *ci = c->cnk + (size_t)2 * k_max * n_max * i;
+    for (int j = 0; j < a->n_neigh[i]; j++) {
+      int k = c->k_first[i] + j;
+      const double *A = c->ang + (size_t)2 * k_max * k;
+      for (int n = 0; n < n_max; n++) {
+        double fr = 4.0 * pi * c->rad[(size_t)k * n_max + n];
+        double *cn = ci + (size_t)2 * k_max * n;
+        for (int kk = 0; kk < k_max; kk++) {
+          cn[2 * kk] = cn[2 * kk] + fr * A[2 * kk];
+          cn[2 * kk + 1] = cn[2 * kk + 1] + fr * A[2 * kk + 1];
+        }
+      }
+    }
+    for (int mm = 0; mm < a->species_multiplicity[i]; mm++) {
+      int sj = a->species[(size_t)i * a->max_mult + mm] - 1;
+      if (sj < 0) continue;
+      if (a->basis == 1 && a->central_weight[sj] != 0.0) {
+        double amplitude;
+        if (a->radial_enhancement == 1) amplitude = sqrt(2.0 / pi) * a->atom_sigma_r[sj] / a->rcut_hard[sj];
+        else if (a->radial_enhancement == 2)
+          amplitude = pow(a->atom_sigma_r[sj], 2) / pow(a->rcut_hard[sj], 2);
+        else amplitude = 1.0;
+        double fac = amplitude * a->central_weight[sj] * sqrt(4.0 * pi) * pow(pi, 0.25)
+                     * sqrt(a->atom_sigma_r[sj] / 2.0) * pow(a->rcut_hard[sj], 3)
+                     / pow(a->atom_sigma_t[sj], 2) / a->atom_sigma_r[sj];
+        int b = i_beg[sj], al = a->alpha_max[sj];
+        for (int n = 0; n < al; n++) {
+          double ws = 0.0;
+          for (int m = 0; m < al; m++)
+            ws += a->W[(size_t)(b + m) * n_max + (b + n)] * a->S[(size_t)(b + al - 1) * n_max + (b + m)];
+          ci[(size_t)2 * k_max * (b + n)] += fac * ws;
+        }
+      }
+    }
+  }
+
+  /* ---- compression skip mask, :411-431 */
+  int n_soap;
+  if (a->compress) {
+    int mx = 0;
+    for (int t = 0; t < a->P_nonzero; t++) if (a->P_i[t] > mx) mx = a->P_i[t];
+    n_soap = mx;
+    for (int t = 0; t < n_soap_unc; t++) c->skip[t] = 1;
+    for (int t = 0; t < a->P_nonzero; t++) c->skip[a->P_j[t] - 1] = 0;
+  } else {
+    n_soap = n_soap_unc;
+  }
+  c->n_soap = n_soap; c->compress = a->compress; c->P_nonzero = a->P_nonzero;
+  c->P_i = a->P_i; c->P_j = a->P_j; c->P_el = a->P_el;
+
+  /* ---- power spectrum + compression + norm, :687-813 */
+  #pragma omp parallel
+  {
+    double *this_soap = (double *)calloc((size_t)n_soap_unc + 1, sizeof(double));
+    #pragma omp for schedule(dynamic, 16)
+    for (int i = 0; i < n_sites; i++) {
+      const double *ci = c->cnk + (size_t)2 * k_max * n_max * i;
+      int counter = 0;
+      for (int n = 0; n < n_max; n++)
+        for (int np = n; np < n_max; np++)
+          for (int l = 0; l <= l_max; l++) {
+            int cidx = counter++;
+            if (c->skip[cidx]) { this_soap[cidx] = 0.0; continue; }
+            double acc = 0.0;
+            for (int m = 0; m <= l; m++) {
+              int kk = kidx(l, m);
+              double mult = 1.0;
+              if (n != np) mult *= sqrt(2.0);
+              if (m > 0) mult *= 2.0;
+              double unr = ci[(size_t)2 * (k_max * n + kk)], uni = ci[(size_t)2 * (k_max * n + kk) + 1];
+              double upr = ci[(size_t)2 * (k_max * np + kk)], upi = ci[(size_t)2 * (k_max * np + kk) + 1];
+              acc = acc + mult * (unr * upr + uni * upi);
+            }
+            this_soap[cidx] = acc;
+          }
+      double *si = soap + (size_t)n_soap * i;
+      if (a->compress) {
+        for (int s = 0; s < n_soap; s++) si[s] = 0.0;
+        for (int t = 0; t < a->P_nonzero; t++)
+          si[a->P_i[t] - 1] = si[a->P_i[t] - 1] + a->P_el[t] * this_soap[a->P_j[t] - 1];
+      } else {
+        for (int s = 0; s < n_soap; s++) si[s] = this_soap[s];
+      }
+      double dot = 0.0;
+      for (int s = 0; s < n_soap; s++) dot += si[s] * si[s];
+      c->sqrt_dot_p[i] = sqrt(dot);
+      if (c->sqrt_dot_p[i] < 1.0e-5) c->sqrt_dot_p[i] = 1.0;
+    }
+    free(this_soap);
+  }
+
+  /* ---- spherical derivatives + Cartesian rotation, :816-902, :1927-2075 */
+  if (need_der && soap_cart_der) {
+    const double fourpi = 4.0 * pi, sq2 = sqrt(2.0);
+    #pragma omp parallel
+    {
+      double *trad = (double *)calloc((size_t)n_soap_unc + 1, sizeof(double));
+      double *tazi = (double *)calloc((size_t)n_soap_unc + 1, sizeof(double));
+      double *tpol = (double *)calloc((size_t)n_soap_unc + 1, sizeof(double));
+      double *drad = (double *)calloc((size_t)n_soap + 1, sizeof(double));
+      double *dazi = (double *)calloc((size_t)n_soap + 1, sizeof(double));
+      double *dpol = (double *)calloc((size_t)n_soap + 1, sizeof(double));
+      double *P = (double *)malloc(sizeof(double) * n_max * (l_max + 1));
+      double *Q = (double *)malloc(sizeof(double) * n_max * (l_max + 1));
+      double *Qa = (double *)malloc(sizeof(double) * n_max * (l_max + 1));
+      double *Qo = (double *)malloc(sizeof(double) * n_max * (l_max + 1));
+      #pragma omp for schedule(dynamic, 16)
+      for (int i = 0; i < n_sites; i++) {
+        const double *ci = c->cnk + (size_t)2 * k_max * n_max * i;
+        const double *si = soap + (size_t)n_soap * i;
+        int k3 = c->k_first[i];
+        double inv_p = 1.0 / c->sqrt_dot_p[i];
+        double inv_p3 = 1.0 / pow(c->sqrt_dot_p[i], 3);
+        double *self = soap_cart_der + (size_t)k3 * n_soap * 3;
+        if (a->n_neigh[i] > 0)
+          for (int t = 0; t < 3 * n_soap; t++) self[t] = 0.0;
+        for (int j = 1; j < a->n_neigh[i]; j++) {
+          int k2 = c->k_first[i] + j;
+          const double *A = c->ang + (size_t)2 * k_max * k2, *Ar = c->ang_r + (size_t)2 * k_max * k2;
+          const double *Aa = c->ang_a + (size_t)2 * k_max * k2, *Ap = c->ang_p + (size_t)2 * k_max * k2;
+          for (int n = 0; n < n_max; n++)
+            for (int l = 0; l <= l_max; l++) {
+              double ap = 0, aq = 0, aa = 0, ao = 0;
+              for (int m = 0; m <= l; m++) {
+                int kk = kidx(l, m);
+                double w = (m == 0) ? 1.0 : 2.0;
+                double cr = ci[(size_t)2 * (k_max * n + kk)], cim = ci[(size_t)2 * (k_max * n + kk) + 1];
+                ap = ap + w * (A[2 * kk] * cr + A[2 * kk + 1] * cim);
+                aq = aq + w * (Ar[2 * kk] * cr + Ar[2 * kk + 1] * cim);
+                aa = aa + w * (Aa[2 * kk] * cr + Aa[2 * kk + 1] * cim);
+                ao = ao + w * (Ap[2 * kk] * cr + Ap[2 * kk + 1] * cim);
+              }
+              P[n * (l_max + 1) + l] = ap; Q[n * (l_max + 1) + l] = aq;
+              Qa[n * (l_max + 1) + l] = aa; Qo[n * (l_max + 1) + l] = ao;
+            }
+          int counter = 0;
+          for (int n = 0; n < n_max; n++) {
+            double rn = c->rad[(size_t)k2 * n_max + n], rdn = c->rad_der[(size_t)k2 * n_max + n];
+            for (int np = n; np < n_max; np++) {
+              double rnp = c->rad[(size_t)k2 * n_max + np], rdnp = c->rad_der[(size_t)k2 * n_max + np];
+              double base = (n == np) ? 1.0 : sq2, pre = fourpi * base;
+              for (int l = 0; l <= l_max; l++) {
+                int cidx = counter++;
+                if (c->skip[cidx]) continue;
+                int L1 = l_max + 1;
+                trad[cidx] = pre * (rdn * P[np * L1 + l] + rn * Q[np * L1 + l] + rdnp * P[n * L1 + l] + rnp * Q[n * L1 + l]);
+                tazi[cidx] = pre * (rn * Qa[np * L1 + l] + rnp * Qa[n * L1 + l]);
+                tpol[cidx] = pre * (rn * Qo[np * L1 + l] + rnp * Qo[n * L1 + l]);
+              }
+            }
+          }
+          if (a->compress) {
+            for (int s = 0; s < n_soap; s++) drad[s] = dazi[s] = dpol[s] = 0.0;
+            for (int t = 0; t < a->P_nonzero; t++) {
+              int pi_ = a->P_i[t] - 1, pj = a->P_j[t] - 1;
+              drad[pi_] = drad[pi_] + a->P_el[t] * trad[pj];
+              dazi[pi_] = dazi[pi_] + a->P_el[t] * tazi[pj];
+              dpol[pi_] = dpol[pi_] + a->P_el[t] * tpol[pj];
+            }
+          } else {
+            for (int s = 0; s < n_soap; s++) { drad[s] = trad[s]; dazi[s] = tazi[s]; dpol[s] = tpol[s]; }
+          }
+          double dot_r = 0, dot_a = 0, dot_o = 0;
+          for (int s = 0; s < n_soap; s++) {
+            dot_r = dot_r + si[s] * drad[s];
+            dot_a = dot_a + si[s] * dazi[s];
+            dot_o = dot_o + si[s] * dpol[s];
+          }
+          double sin_t = sin(a->thetas[k2]), cos_t = cos(a->thetas[k2]);
+          double sin_f = sin(a->phis[k2]), cos_f = cos(a->phis[k2]);
+          double inv_r = 1.0 / a->rjs[k2];
+          double cx = sin_t * cos_f, cy = sin_t * sin_f, cz = cos_t;
+          double px = -cos_t * cos_f * inv_r, py = -cos_t * sin_f * inv_r, pz = sin_t * inv_r;
+          double ax = -sin_f * inv_r, ay = cos_f * inv_r;
+          double *out = soap_cart_der + (size_t)k2 * n_soap * 3;
+          for (int s = 0; s < n_soap; s++) {
+            double sv = si[s];
+            double vr = drad[s] * inv_p - sv * inv_p3 * dot_r;
+            double va = dazi[s] * inv_p - sv * inv_p3 * dot_a;
+            double vo = dpol[s] * inv_p - sv * inv_p3 * dot_o;
+            out[3 * s + 0] = cx * vr + px * vo + ax * va;
+            out[3 * s + 1] = cy * vr + py * vo + ay * va;
+            out[3 * s + 2] = cz * vr + pz * vo;
+          }
+          for (int t = 0; t < 3 * n_soap; t++) self[t] = self[t] - out[t];
+        }
+      }
+      free(trad); free(tazi); free(tpol); free(drad); free(dazi); free(dpol);
+      free(P); free(Q); free(Qa); free(Qo);
+    }
+  }
+
+  /* ---- normalise, :904-909 */
+  #pragma omp parallel for schedule(static)
+  for (int i = 0; i < n_sites; i++)
+    for (int s = 0; s < n_soap; s++) soap[(size_t)n_soap * i + s] = soap[(size_t)n_soap * i + s] / c->sqrt_dot_p[i];
+
+  free(preflm);
+  if (ctx_out) *ctx_out = c; else or_ctx_free(c);
+  return n_soap;
+}
+
+/* soap_contract, src/soap_turbo.f90:1723-1884.  ctx comes from or_get_soap
+ * called with do_derivatives = 1. */
+int or_soap_contract(const or_ctx *c, const double *soap, const double *G, double sgn, double *pair) {
+  if (!c || !c->ang_r) return -1;
+  const double fourpi = 4.0 * acos(-1.0), sq2 = sqrt(2.0);
+  const int n_max = c->n_max, k_max = c->k_max, l_max = c->l_max, n_soap = c->n_soap;
+  const int n_sites = c->n_sites;
+  #pragma omp parallel
+  {
+    double *Gp = (double *)malloc(sizeof(double) * (n_soap + 1));
+    double *Gu = (double *)malloc(sizeof(double) * (c->n_soap_unc + 1));
+    double *Y = (double *)malloc(sizeof(double) * n_max * n_max * (l_max + 1));
+    double *H = (double *)malloc(sizeof(double) * 2 * k_max * n_max);
+    #pragma omp for schedule(dynamic, 16)
+    for (int i = 0; i < n_sites; i++) {
+      const double *si = soap + (size_t)n_soap * i;
+      const double *ci = c->cnk + (size_t)2 * k_max * n_max * i;
+      double qg = 0.0;
+      for (int k = 0; k < n_soap; k++) qg = qg + si[k] * G[(size_t)k * n_sites + i];
+      double inv = 1.0 / c->sqrt_dot_p[i];
+      for (int k = 0; k < n_soap; k++) Gp[k] = (G[(size_t)k * n_sites + i] - si[k] * qg) * inv;
+      if (c->compress) {
+        for (int t = 0; t < c->n_soap_unc; t++) Gu[t] = 0.0;
+        for (int t = 0; t < c->P_nonzero; t++)
+          Gu[c->P_j[t] - 1] = Gu[c->P_j[t] - 1] + c->P_el[t] * Gp[c->P_i[t] - 1];
+      } else {
+        for (int k = 0; k < n_soap; k++) Gu[k] = Gp[k];
+      }
+      int counter = 0;
+      for (int n = 0; n < n_max; n++)
+        for (int np = n; np < n_max; np++) {
+          double base = (n == np) ? 1.0 : sq2;
+          for (int l = 0; l <= l_max; l++) {
+            int cidx = counter++;
+            double x = 0.0;
+            if (!c->skip[cidx]) x = Gu[cidx] * base;
+            if (n == np) Y[(l * n_max + n) * n_max + n] = 2.0 * x;
+            else { Y[(l * n_max + np) * n_max + n] = x; Y[(l * n_max + n) * n_max + np] = x; }
+          }
+        }
+      for (int n = 0; n < n_max; n++)
+        for (int l = 0; l <= l_max; l++)
+          for (int m = 0; m <= l; m++) {
+            int kk = kidx(l, m);
+            double hr = 0.0, hi = 0.0;
+            for (int np = 0; np < n_max; np++) {
+              double y = Y[(l * n_max + np) * n_max + n];
+              hr = hr + y * ci[(size_t)2 * (k_max * np + kk)];
+              hi = hi + y * ci[(size_t)2 * (k_max * np + kk) + 1];
+            }
+            double w = (m == 0) ? 1.0 : 2.0;
+            H[2 * (kk * n_max + n)] = w * hr;
+            H[2 * (kk * n_max + n) + 1] = w * hi;
+          }
+      int k3 = c->k_first[i];
+      double sx = 0, sy = 0, sz = 0;
+      for (int j = 1; j < c->n_neigh[i]; j++) {
+        int k2 = c->k_first[i] + j;
+        const double *A = c->ang + (size_t)2 * k_max * k2, *Ar = c->ang_r + (size_t)2 * k_max * k2;
+        const double *Aa = c->ang_a + (size_t)2 * k_max * k2, *Ap = c->ang_p + (size_t)2 * k_max * k2;
+        double f_rad = 0, f_azi = 0, f_pol = 0;
+        for (int n = 0; n < n_max; n++) {
+          double sd = 0, sr = 0, sa = 0, so = 0;
+          for (int kk = 0; kk < k_max; kk++) {
+            double hr = H[2 * (kk * n_max + n)], hi = H[2 * (kk * n_max + n) + 1];
+            sd = sd + A[2 * kk] * hr + A[2 * kk + 1] * hi;
+            sr = sr + Ar[2 * kk] * hr + Ar[2 * kk + 1] * hi;
+            sa = sa + Aa[2 * kk] * hr + Aa[2 * kk + 1] * hi;
+            so = so + Ap[2 * kk] * hr + Ap[2 * kk + 1] * hi;
+          }
+          f_rad = f_rad + c->rad_der[(size_t)k2 * n_max + n] * sd + c->rad[(size_t)k2 * n_max + n] * sr;
+          f_azi = f_azi + c->rad[(size_t)k2 * n_max + n] * sa;
+          f_pol = f_pol + c->rad[(size_t)k2 * n_max + n] * so;
+        }
+        f_rad *= fourpi; f_azi *= fourpi; f_pol *= fourpi;
+        double sin_t = sin(c->thetas[k2]), cos_t = cos(c->thetas[k2]);
+        double sin_f = sin(c->phis[k2]), cos_f = cos(c->phis[k2]);
+        double inv_r = 1.0 / c->rjs[k2];
+        double px = sgn * (sin_t * cos_f * f_rad - cos_t * cos_f * inv_r * f_pol - sin_f * inv_r * f_azi);
+        double py = sgn * (sin_t * sin_f * f_rad - cos_t * sin_f * inv_r * f_pol + cos_f * inv_r * f_azi);
+        double pz = sgn * (cos_t * f_rad + sin_t * inv_r * f_pol);
+        pair[3 * k2] = px; pair[3 * k2 + 1] = py; pair[3 * k2 + 2] = pz;
+        sx = sx - px; sy = sy - py; sz = sz - pz;
+      }
+      if (c->n_neigh[i] > 0) { pair[3 * k3] = sx; pair[3 * k3 + 1] = sy; pair[3 * k3 + 2] = sz; }
+    }
+    free(Gp); free(Gu); free(Y); free(H);
+  }
+  return 0;
+}
+
+/* The radial expansion of one species at a list of distances (the columns a
+ * masked, in-cutoff pair would get; src/soap_turbo_radial.f90:394-1004,
+ * global_scaling not applied).  W is the species' alpha x alpha block. */
+int or_radial_eval(int basis, int alpha, double rcut_soft, double rcut_hard, double sigma,
+                   double sigma_scaling, double amp_scaling, double nf, const double *W,
+                   int scaling_poly, int radial_enhancement, double central_weight, int is_central,
+                   int legacy_seed, int n, const double *r, double *out, double *der) {
+  or_radial_setup st;
+  int with_gauss = basis == 1;
+  int do_central = with_gauss ? 0 : (central_weight != 0.0);
+  or_radial_init(&st, alpha, rcut_soft, rcut_hard, sigma, sigma_scaling, amp_scaling, nf, W, alpha,
+                 scaling_poly, radial_enhancement, 1, do_central, central_weight, with_gauss, legacy_seed);
+  for (int t = 0; t < n; t++) {
+    double o[32], d[32];
+    or_radial_pair(&st, r[t], is_central, o, d);
+    for (int q = 0; q < alpha; q++) { out[(size_t)t * alpha + q] = o[q]; der[(size_t)t * alpha + q] = d[q]; }
+  }
+  return 0;
+}
+
+/* Accessors for intermediate arrays (tests compare them stage by stage). */
+const double *or_ctx_cnk(const or_ctx *c) { return c->cnk; }
+const double *or_ctx_rad(const or_ctx *c) { return c->rad; }
+const double *or_ctx_rad_der(const or_ctx *c) { return c->rad_der; }
+const double *or_ctx_ang(const or_ctx *c, int which) {
+  return which == 0 ? c->ang : which == 1 ? c->ang_r : which == 2 ? c->ang_a : c->ang_p;
+}
+const double *or_ctx_norm(const or_ctx *c) { return c->sqrt_dot_p; }
+int or_ctx_n_max(const or_ctx *c) { return c->n_max; }
+
+/* get_compress_indices, trivial branch, src/soap_turbo_compress.f90:86-119.
+ * With P_i == NULL only the dimension is returned ("get_dim"). */
+int or_compress_trivial(int n_species, const int *alpha_max, int l_max, int *P_i, int *P_j, double *P_el) {
+  int pivot[64], n_max = 0;
+  if (n_species > 64) return -1;
+  pivot[0] = 1;
+  for (int i = 0; i < n_species - 1; i++) pivot[i + 1] = pivot[i] + alpha_max[i];
+  for (int i = 0; i < n_species; i++) n_max += alpha_max[i];
+  int counter = 0, k = 1;
+  for (int n = 1; n <= n_max; n++)
+    for (int m = n; m <= n_max; m++)
+      for (int l = 0; l <= l_max; l++) {
+        int hit = 0;
+        for (int s = 0; s < n_species; s++) if (n == pivot[s] || m == pivot[s]) hit = 1;
+        if (hit) {
+          counter++;
+          if (P_i) { P_i[counter - 1] = counter; P_j[counter - 1] = k; P_el[counter - 1] = 1.0; }
+        }
+        k++;
+      }
+  return counter;
+}
+
+int or_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}

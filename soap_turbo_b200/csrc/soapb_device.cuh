@@ -1,0 +1,354 @@
+// soapb_device.cuh -- per-pair device math shared by the mixed-precision and
+// the plain-FP64 kernels.
+//
+// radial_entry: the poly3 / poly3gauss radial expansion of one (pair, species)
+// entry (src/soap_turbo_radial.f90:550-1002), in FP64.  The basis matrix W has
+// norm ~1e6 and the primitive overlaps cancel against it, so this part cannot
+// run in FP32 (a 3e-2 relative error at alpha = 8); it is a few hundred FP64
+// operations per entry.  Instead of the reference's block buffers it streams
+// over alpha: the two overlap recursions advance together, each polynomial
+// value is folded into the W-transform accumulators as it appears, and the
+// derivative DT(m) is formed two steps later from a three-value window.  The
+// summation order of every W-transform is the reference's (m ascending, the
+// origin Gaussian last).
+//
+// angular_scalars: the per-pair FP64 inputs of the angular expansion
+// (src/soap_turbo_angular.f90:267-463, 578-589): i_l(x^2)e^{-x^2} and its
+// radial derivative, e^{-i m phi} by the reference's Chebyshev recursion, the
+// amplitude rcut_max^2/sigma_t^2 and cos/sin theta.
+#pragma once
+
+#include "soapb_internal.h"
+
+namespace soapb {
+
+// Recursion table index for alpha index n (n >= -4).
+#define SOAPB_TI(n) ((n) + 4)
+
+template <int AMAX>
+__device__ __forceinline__ void radial_entry(const DevParams &P, const RadSp &S,
+                                             const double *__restrict__ W, double r_in,
+                                             bool is_central, bool do_der, double (&val)[AMAX],
+                                             double (&der)[AMAX]) {
+  const double sqpi2 = 1.2533141373155002512, isq2 = 0.70710678118654752440;
+  const double sq2pi = 0.79788456080286535588, sq8pi = 1.5957691216057307118;
+  const int a = S.alpha;
+  const int n_poly = S.n_poly;
+  const int n_hi = n_poly + (do_der ? 2 : 0);
+  const bool unified = !P.legacy_seed;
+  const double c = S.c, rs = S.rs, dr = S.dr;
+  const double rj = r_in * S.inv_rcut;
+
+  const double sig = S.atom_sigma + c * rj, s2 = sig * sig;             // :560-570
+  const double isig = 1.0 / sig, is2 = isig * isig, is3 = is2 * isig;
+
+  double amp, ampd;                                                      // :589-635
+  if (!P.scaling_poly) {
+    amp = 1.0;
+    ampd = 0.0;
+  } else if (S.amp_scaling == 0.0) {
+    amp = isig;
+    ampd = -c * is2;
+  } else {
+    const double h = 1.0 + 2.0 * (rj * rj * rj) - 3.0 * rj * rj;
+    const double hp = 6.0 * rj * rj - 6.0 * rj;
+    if (h <= 1.0e-10) {
+      amp = 0.0;
+      ampd = 0.0;
+    } else if (S.amp_scaling == 1.0) {
+      const double g = isig * h;
+      amp = g;
+      ampd = hp * isig - c * isig * g;
+    } else {
+      const double aa = S.amp_scaling;
+      amp = isig * pow(h, aa);
+      ampd = aa * pow(h, aa - 1.0) * hp * isig - c * isig * amp;
+    }
+  }
+  if (S.do_central && S.cw != 1.0 && is_central) {                      // :638-646
+    amp *= S.cw;
+    ampd *= S.cw;
+  }
+  if (P.radial_enh == 1) {                                               // :651-670
+    const double g = rj + sq2pi * sig, f = 1.0 + sq2pi * c;
+    ampd = amp * f + ampd * g;
+    amp = amp * g;
+  } else if (P.radial_enh == 2) {
+    const double g = rj * rj + s2 + sq8pi * sig * rj;
+    const double f = 2.0 * rj + 2.0 * sig * c + sq8pi * sig + sq8pi * rj * c;
+    ampd = amp * f + ampd * g;
+    amp = amp * g;
+  }
+
+  // Overlap with the atom Gaussian on [0, rcut_soft], seeded by erf (:676-686)
+  const double es = exp(-0.5 * (rs - rj) * (rs - rj) * is2);
+  const double e0 = exp(-0.5 * rj * rj * is2);
+  double C1 = s2 * es;
+  const double C2 = s2 * e0;
+  double t1m2 = 0.0;
+  double t1m1 = sqpi2 * sig * (erf((rs - rj) * isq2 * isig) + erf(rj * isq2 * isig));  // inv_Nm2 = 1
+
+  // Gaussian filter on [rcut_soft, rcut_hard] (:721-769)
+  const bool filt = S.has_filter != 0;
+  double pref = 0.0, sf2 = 0.0, rjf = 0.0, isf2 = 0.0, C2f = 0.0, t2m2 = 0.0, t2m1 = 0.0;
+  double iD = 0.0, sqiD = 0.0, sgf = 0.0, isgf = 0.0;
+  if (filt) {
+    const double q = S.q, drnf = S.drnf;
+    iD = 1.0 / (s2 + q);
+    sqiD = sqrt(iD);
+    sgf = sig * drnf * sqiD;
+    rjf = (s2 * rs + q * rj) * iD;
+    sf2 = sgf * sgf;
+    const bool keep = (rs - rj) < 4.0 * sig;
+    isgf = 1.0 / sgf;
+    isf2 = isgf * isgf;
+    pref = keep ? exp(-0.5 * (rs - rj) * (rs - rj) * iD) : 0.0;
+    C2f = sf2 * exp(-0.5 * (rs - rjf) * (rs - rjf) * isf2);
+    t2m1 = sqpi2 * sgf * (erf((1.0 - rjf) * isq2 * isgf) - erf((rs - rjf) * isq2 * isgf));
+  }
+
+  // Derivative coefficients (legacy :701-713, :774-788; unified :825-831)
+  double g0 = 0, g1 = 0, g2 = 0;           // unified
+  double ca = 0, cb = 0, cc = 0;           // legacy, inner piece
+  double ca2 = 0, cb2 = 0, cc2 = 0, dpref = 0;  // legacy, filter piece
+  if (do_der) {
+    if (unified) {
+      const double f = 1.0 - rj;
+      g0 = f * is2 + c * f * f * is3;
+      g1 = -(is2 + 2.0 * c * f * is3);
+      g2 = c * is3;
+    } else {
+      const double f = rj - 1.0, g = c * f * isig;
+      ca = f * is2 * (g - 1.0);
+      cb = is2 * (2.0 * g - 1.0);
+      cc = c * is3;
+      if (filt) {
+        const double q = S.q;
+        const double fs = rs - rj;
+        dpref = pref * (fs * iD + fs * fs * iD * iD * sig * c);
+        const double drjf = (2.0 * sig * rs * c + q) * iD - (s2 * rs + q * rj) * 2.0 * sig * c * iD * iD;
+        const double dsgf = c * S.drnf * sqiD * (1.0 - s2 * iD);
+        const double ff = rjf - 1.0, gg = dsgf * ff * isgf;
+        ca2 = pref * ff * isf2 * (gg - drjf);
+        cb2 = pref * isf2 * (2.0 * gg - drjf);
+        cc2 = pref * dsgf * isgf * isf2;
+      }
+    }
+  }
+
+#pragma unroll
+  for (int i = 0; i < AMAX; ++i) {
+    val[i] = 0.0;
+    der[i] = 0.0;
+  }
+  double p0 = 0, p1 = 0, p2 = 0;  // pol window (n-2, n-1, n)
+  double q0 = 0, q1 = 0, q2 = 0;  // T1 window
+  double z0 = 0, z1 = 0, z2 = 0;  // T2 window
+
+#pragma unroll 1
+  for (int n = -1; n <= n_hi; ++n) {                                     // :688-698, :751-770
+    if (n >= 0) {
+      C1 = C1 * dr;
+      C2f = C2f * dr;
+    }
+    const double t1 = s2 * P.ra[SOAPB_TI(n)] * t1m2 - P.rb[SOAPB_TI(n)] * (rj - 1.0) * t1m1 +
+                      (C1 - C2) * P.rc[SOAPB_TI(n)];
+    double t2 = 0.0;
+    if (filt) {
+      t2 = sf2 * P.ra[SOAPB_TI(n)] * t2m2 - P.rb[SOAPB_TI(n)] * (rjf - 1.0) * t2m1 -
+           C2f * P.rc[SOAPB_TI(n)];
+      if (n == -1 && unified)
+        t2 = t2 + sf2 * exp(-0.5 * (1.0 - rjf) * (1.0 - rjf) * isf2) * P.rc[SOAPB_TI(-1)];
+    }
+    t1m2 = t1m1;
+    t1m1 = t1;
+    t2m2 = t2m1;
+    t2m1 = t2;
+    if (n < 1) continue;
+    const double pol = t1 + pref * t2;                                   // :808-812
+    p0 = p1; p1 = p2; p2 = pol;
+    q0 = q1; q1 = q2; q2 = t1;
+    z0 = z1; z1 = z2; z2 = t2;
+    if (n <= n_poly) {                                                   // :962-976
+      const double *Wc = W + (n - 1) * a;
+#pragma unroll
+      for (int i = 0; i < AMAX; ++i)
+        if (i < a) val[i] = val[i] + Wc[i] * pol;
+    }
+    if (do_der && n >= 3) {                                              // :911-942
+      const int m = n - 2;
+      double DT;
+      if (unified) {
+        DT = g0 * p0 + P.R1[SOAPB_TI(m)] * g1 * p1 + P.R2[SOAPB_TI(m)] * g2 * p2;
+      } else {
+        DT = ca * q0 + P.R1[SOAPB_TI(m)] * cb * q1 + P.R2[SOAPB_TI(m)] * cc * q2;
+        if (filt)
+          DT = DT + ca2 * z0 + P.R1[SOAPB_TI(m)] * cb2 * z1 + P.R2[SOAPB_TI(m)] * cc2 * z2 + dpref * z0;
+      }
+      const double dtot = amp * DT + ampd * p0;
+      const double *Wc = W + (m - 1) * a;
+#pragma unroll
+      for (int i = 0; i < AMAX; ++i)
+        if (i < a) der[i] = der[i] + Wc[i] * dtot;
+    }
+  }
+
+  if (P.basis == 1) {                                                    // :875-908
+    const double ss2 = S.sigma_sq0 + s2, iss = 1.0 / ss2, siss = sqrt(iss);
+    const bool gm = rj < 4.0 * (S.atom_sigma + sig);
+    const double ge = gm ? S.N_gauss * e0 : 0.0;
+    const double M0 = gm ? exp(-0.5 * rj * rj * iss) * sqpi2 * sig * S.atom_sigma * siss *
+                               (1.0 + erf(S.atom_sigma * isig * rj * isq2 * siss)) * S.N_gauss
+                         : 0.0;
+    const double *Wc = W + (a - 1) * a;
+#pragma unroll
+    for (int i = 0; i < AMAX; ++i)
+      if (i < a) val[i] = val[i] + Wc[i] * M0;
+    if (do_der) {
+      const double sc0 = S.sigma_sq0 * s2 * iss, pp = s2 * rj * iss;
+      const double M1 = sc0 * ge - pp * M0;
+      const double M2 = sc0 * ge * (-rj) - pp * M1 + sc0 * M0;
+      const double dtot = amp * (M1 * is2 + c * M2 * is3) + ampd * M0;
+#pragma unroll
+      for (int i = 0; i < AMAX; ++i)
+        if (i < a) der[i] = der[i] + Wc[i] * dtot;
+    }
+  }
+
+#pragma unroll
+  for (int i = 0; i < AMAX; ++i) {
+    val[i] = amp * val[i] * S.sqrt_rcut;
+    der[i] = der[i] * S.inv_sqrt_rcut;
+  }
+}
+
+// ---------------------------------------------------------------- angular
+template <int LC>
+struct AngScalars {
+  double il[LC + 2];   // i_l(x^2) exp(-x^2), l = 0..LC+1
+  double ild[LC + 1];  // its radial derivative
+  double er[LC + 1], ei[LC + 1];  // e^{-i m phi} = cos(m phi) - i sin(m phi)
+  double amp;          // rcut_max^2 / sigma_t^2
+  double sig_fac;      // 2 sigma_t_scaling / sigma_t
+  double x, sq;        // cos(theta), sqrt(1 - x^2)
+};
+
+// get_ilexp (src/soap_turbo_angular.f90:361-422) for l = 0..lmax
+template <int LC>
+__device__ __forceinline__ void ilexp_array(int lmax, double x, double (&out)[LC + 2]) {
+  const double xcut = 1.0e-7;
+  const double x2 = x * x, x4 = x2 * x2;
+  const double inv_x2 = (x2 > 0.0) ? 1.0 / x2 : 0.0;
+  double x2pow = x2 * x2;
+  double flm2, flm1;
+  if (x > 0.0) {
+    const double e2 = exp(-2.0 * x2);
+    flm2 = fabs((1.0 - e2) / 2.0 / x2);
+    flm1 = fabs((x2 - 1.0 + e2 * (x2 + 1.0)) / 2.0 / x4);
+  } else {
+    flm2 = 1.0;
+    flm1 = 0.0;
+  }
+  double fact = 1.0;
+#pragma unroll
+  for (int l = 0; l < LC + 2; ++l) {
+    if (l > lmax) {
+      out[l] = 0.0;
+      continue;
+    }
+    if (l > 0) fact = fact * (2.0 * (double)l + 1.0);
+    if (l == 0) {
+      out[0] = (x < xcut) ? 1.0 - x2 : flm2;
+    } else if (l == 1) {
+      out[1] = (x2 / 1000.0 < xcut) ? (x2 - x4) / fact : flm1;
+    } else {
+      const double ratio = x2pow / fact;
+      double fl;
+      if (ratio * (double)l < xcut)
+        fl = ratio;
+      else
+        fl = fabs(flm2 - (2.0 * (double)l - 1.0) * inv_x2 * flm1);
+      x2pow = x2pow * x2;
+      flm2 = flm1;
+      flm1 = fl;
+      out[l] = fl;
+    }
+  }
+}
+
+template <int LC>
+__device__ __forceinline__ void angular_scalars(const DevParams &P, int i_sp, double rj,
+                                                double theta, double phi, bool do_der,
+                                                AngScalars<LC> &A) {
+  const int L = P.l_max;
+  const double sig = P.sig_t[i_sp] + P.sig_t_c[i_sp] * rj;               // :579-580
+  A.amp = P.rcut2 / (sig * sig);
+  A.x = cos(theta);
+  A.sq = sqrt(1.0 - A.x * A.x);
+  ilexp_array<LC>(L + 1, rj / sig, A.il);
+  // e^{-i m phi}, Chebyshev recursion of get_eimphi_conjg (:284-298)
+  double cosm2 = cos(phi), sinm2 = -sin(phi);
+  const double cosphi2 = 2.0 * cosm2;
+  double cosm1 = 1.0, sinm1 = 0.0;
+  A.er[0] = 1.0;
+  A.ei[0] = 0.0;
+#pragma unroll
+  for (int l = 1; l <= LC; ++l) {
+    const double cos0 = cosphi2 * cosm1 - cosm2, sin0 = cosphi2 * sinm1 - sinm2;
+    cosm2 = cosm1;
+    sinm2 = sinm1;
+    cosm1 = cos0;
+    sinm1 = sin0;
+    A.er[l] = cos0;
+    A.ei[l] = -sin0;
+  }
+  A.sig_fac = 0.0;
+  if (do_der) {                                                          // :436-463
+    const double sc = P.sig_t_c[i_sp];
+    const double c1 = 2.0 * rj / (sig * sig), c2 = 1.0 - sc * rj / sig;
+#pragma unroll
+    for (int l = 0; l <= LC; ++l) A.ild[l] = 0.0;
+    if (rj >= 1.0e-5) {
+      A.ild[0] = c1 * (A.il[1] - A.il[0]) * c2;
+#pragma unroll
+      for (int l = 1; l <= LC; ++l)
+        if (l <= L) A.ild[l] = ((-c1 - (double)(2 * l + 2) / rj) * A.il[l] + c1 * A.il[l - 1]) * c2;
+    }
+    A.sig_fac = 2.0 * sc / sig;                                          // :589
+  }
+}
+
+// Associated Legendre P_l^m(x) for l = 0..lmax (get_plm_array,
+// src/soap_turbo_angular.f90:108-160), k = l(l+1)/2 + m.  T is float or double.
+template <int LC, typename T>
+__device__ __forceinline__ void plm_array(int lmax, T x, T sq, T (&p)[(LC + 1) * (LC + 2) / 2]) {
+  const T x2 = x * x;
+#pragma unroll
+  for (int k = 0; k < (LC + 1) * (LC + 2) / 2; ++k) p[k] = T(0);
+  p[0] = T(1);
+  if (LC >= 1) {
+    p[1] = x;
+    p[2] = -sq;
+  }
+  if (LC >= 2) {
+    p[3] = T(1.5) * x2 - T(0.5);
+    p[4] = T(-3) * x * sq;
+    p[5] = T(3) - T(3) * x2;
+  }
+#pragma unroll
+  for (int l = 3; l <= LC; ++l) {
+    if (l > lmax) break;
+#pragma unroll
+    for (int m = 0; m <= l - 2; ++m) {
+      const int k = l * (l + 1) / 2 + m;
+      const T aa = T(2 * l - 1) / T(l - m);
+      const T bb = T(l - 1 + m) / T(l - m);
+      p[k] = aa * x * p[k - l] - bb * p[k - 2 * l + 1];
+    }
+    const int k1 = l * (l + 1) / 2 + l - 1;
+    p[k1] = x * T(2 * l - 1) * p[k1 - l];
+    p[k1 + 1] = -T(2 * l - 1) * sq * p[k1 - l];
+  }
+}
+
+}  // namespace soapb

@@ -1,0 +1,386 @@
+// soapb_fp64.cu -- the plain FP64 form of the descriptor path, staged like the
+// reference (src/soap_turbo.f90:491-909): radial and angular expansions of
+// every pair to global memory, c_nlm per site, power spectrum, then the
+// spherical derivatives, normalisation derivative and Cartesian rotation into
+// a materialised soap_cart_der (3, n_soap, n_pairs), and a contraction of
+// that array with G.  It serves callers that read soap_cart_der itself
+// (get_soap with do_derivatives and contract = .false.) and is the FP64
+// baseline the mixed-precision adjoint path is measured against.  Kernels are
+// coalesced and do no redundant zeroing, but keep the reference's structure.
+#include "soapb_device.cuh"
+
+namespace soapb {
+
+constexpr double kFourPi64 = 12.566370614359172954;
+
+// ---- radial, one thread per pair, every species block (:491-544)
+template <int AMAX>
+__global__ void k64_radial(const DevParams P, const DevBatch B, int do_der, double *rad,
+                           double *rad_der) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= B.n_pairs) return;
+  // site-local index: binary search of the CSR offsets
+  int lo = 0, hi = B.n_sites;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (B.off[mid] <= k) lo = mid; else hi = mid;
+  }
+  const bool is_self = (B.off[lo] == k);
+  const double r = B.rjs[k];
+  const unsigned bits = B.bits[k];
+  double *ro = rad + (size_t)k * P.n_max, *rdo = rad_der + (size_t)k * P.n_max;
+  for (int s = 0; s < P.n_species; ++s) {
+    const RadSp &S = P.rad[s];
+    const bool ok = ((bits >> s) & 1u) && r < S.rcut_hard && (!is_self || S.do_central);
+    double val[AMAX], der[AMAX];
+    if (ok) radial_entry<AMAX>(P, S, P.Wblk + (size_t)s * P.wstride, r, is_self, do_der != 0, val, der);
+    for (int n = 0; n < S.alpha; ++n) {
+      ro[S.nbeg + n] = ok ? val[n] * S.gscale : 0.0;
+      if (do_der) rdo[S.nbeg + n] = ok ? der[n] * S.gscale : 0.0;
+    }
+  }
+}
+
+// ---- angular, one thread per pair (src/soap_turbo_angular.f90:549-607)
+template <int LC>
+__global__ void k64_angular(const DevParams P, const DevBatch B, int do_der, double2 *ang) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= B.n_pairs) return;
+  const int K = P.k_max;
+  const size_t plane = (size_t)B.n_pairs * K;
+  double2 *A = ang + (size_t)k * K;
+  const double r = B.rjs[k];
+  const unsigned bits = B.bits[k];
+  if (!(r < P.rcut_max) || bits == 0u) {
+    for (int kk = 0; kk < K; ++kk) {
+      A[kk] = make_double2(0.0, 0.0);
+      if (do_der) {
+        A[plane + kk] = make_double2(0.0, 0.0);
+        A[2 * plane + kk] = make_double2(0.0, 0.0);
+        A[3 * plane + kk] = make_double2(0.0, 0.0);
+      }
+    }
+    return;
+  }
+  AngScalars<LC> S;
+  angular_scalars<LC>(P, __ffs(bits) - 1, r, B.thetas[k], B.phis[k], do_der != 0, S);
+  double plm[(LC + 2) * (LC + 3) / 2];
+  plm_array<LC + 1, double>(P.l_max + 1, S.x, S.sq, plm);
+  for (int l = 0; l <= P.l_max; ++l) {
+    for (int m = 0; m <= l; ++m) {
+      const int kk = l * (l + 1) / 2 + m;
+      const double e_re = S.il[l] * S.er[m], e_im = S.il[l] * S.ei[m];
+      const double u = S.amp * P.preflm64[kk];
+      const double v = u * plm[kk];
+      A[kk] = make_double2(v * e_re, v * e_im);
+      if (do_der) {
+        const double er_re = S.ild[l] * S.er[m], er_im = S.ild[l] * S.ei[m];
+        A[plane + kk] = make_double2(v * er_re - S.sig_fac * v * e_re, v * er_im - S.sig_fac * v * e_im);
+        double dms, dvs;
+        if (m == 0) {
+          dms = (l == 0) ? 0.0 : -0.5 * plm[l * (l + 1) / 2 + 1];
+          dvs = 0.0;
+        } else {
+          dms = 0.5 * (double)(l + m) * (double)(l - m + 1) * plm[kk - 1];
+          dvs = 0.5 * (double)(l - m + 1) * (double)(l - m + 2) * plm[(l + 1) * (l + 2) / 2 + m - 1] +
+                0.5 * plm[(l + 1) * (l + 2) / 2 + m + 1];
+        }
+        if (m != l) dms = dms + -0.5 * plm[kk + 1];
+        const double w = u * dvs;
+        A[2 * plane + kk] = make_double2(-(w * e_im), w * e_re);
+        const double w2 = u * dms;
+        A[3 * plane + kk] = make_double2(w2 * e_re, w2 * e_im);
+      }
+    }
+  }
+}
+
+// ---- c_nlm, one CTA per site, threads over (n, k) (src/soap_turbo.f90:626-664)
+__global__ void k64_cnk(const DevParams P, const DevBatch B, const double *rad, const double2 *ang,
+                        double2 *cnk) {
+  const int site = blockIdx.x;
+  const int K = P.k_max, N = P.n_max;
+  const int p0 = B.off[site], p1 = min(B.off[site + 1], B.n_pairs);
+  double2 *c = cnk + (size_t)site * N * K;
+  for (int it = threadIdx.x; it < N * K; it += blockDim.x) {
+    const int n = it / K, kk = it - n * K;
+    double cr = 0.0, ci = 0.0;
+    for (int k = p0; k < p1; ++k) {
+      const double fr = kFourPi64 * rad[(size_t)k * N + n];
+      const double2 a = ang[(size_t)k * K + kk];
+      cr = cr + fr * a.x;
+      ci = ci + fr * a.y;
+    }
+    if (P.basis == 1 && kk == 0) {
+      for (int mm = 0; mm < B.species_mult[site]; ++mm) {
+        const int s = B.species[(size_t)site * B.max_mult + mm] - 1;
+        if (s >= 0 && s < P.n_species && n >= P.rad[s].nbeg && n < P.rad[s].nbeg + P.rad[s].alpha)
+          cr += P.central[n];
+      }
+    }
+    c[it] = make_double2(cr, ci);
+  }
+}
+
+// ---- power spectrum + compression + norm, one CTA per site (:750-813)
+__global__ void k64_soap(const DevParams P, const DevBatch B, const double2 *cnk, double *soap_un,
+                         double *norm) {
+  extern __shared__ double sp[];  // n_kept
+  __shared__ double red[32];
+  const int site = blockIdx.x;
+  const int K = P.k_max;
+  const double2 *c = cnk + (size_t)site * P.n_max * K;
+  for (int q = threadIdx.x; q < P.n_kept; q += blockDim.x) {
+    const int code = P.kept_nnl[q];
+    const int n = code & 0xff, np = (code >> 8) & 0xff, l = code >> 16;
+    double acc = 0.0;
+    const double base = (n == np) ? 1.0 : sqrt(2.0);
+    for (int m = 0; m <= l; ++m) {
+      const int kk = l * (l + 1) / 2 + m;
+      const double2 a = c[(size_t)n * K + kk], b = c[(size_t)np * K + kk];
+      const double mult = base * ((m > 0) ? 2.0 : 1.0);
+      acc = acc + mult * (a.x * b.x + a.y * b.y);
+    }
+    sp[q] = acc;
+  }
+  __syncthreads();
+  double part = 0.0;
+  double *out = soap_un + (size_t)site * P.n_soap;
+  for (int o = threadIdx.x; o < P.n_soap; o += blockDim.x) {
+    double v = 0.0;
+    for (int t = P.pi_off[o]; t < P.pi_off[o + 1]; ++t) v = v + P.pi_el64[t] * sp[P.pi_q[t]];
+    out[o] = v;
+    part += v * v;
+  }
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    double nr = sqrt(t);
+    if (nr < 1.0e-5) nr = 1.0;
+    norm[site] = nr;
+  }
+}
+
+// ---- spherical derivatives + rotation into soap_cart_der, one CTA per pair
+// (src/soap_turbo.f90:837-895, 1999-2066)
+__global__ void k64_cart(const DevParams P, const DevBatch B, const double *rad,
+                         const double *rad_der, const double2 *ang, const double2 *cnk,
+                         const double *soap_un, const double *norm, double *cart) {
+  extern __shared__ double sm[];
+  const int k = blockIdx.x;
+  int lo = 0, hi = B.n_sites;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (B.off[mid] <= k) lo = mid; else hi = mid;
+  }
+  const int site = lo;
+  if (B.off[site] == k) return;  // self column: built by k64_self
+  const int N = P.n_max, K = P.k_max, L1 = P.l_max + 1, ns = P.n_soap;
+  const size_t plane = (size_t)B.n_pairs * K;
+  double *sPQ = sm;                     // 4 * N * L1
+  double *sd = sPQ + 4 * N * L1;        // n_kept * 3
+  double *sdc = sd + 3 * P.n_kept;      // n_soap * 3
+  __shared__ double red[3][32];
+  const double2 *c = cnk + (size_t)site * N * K;
+  const double2 *A = ang + (size_t)k * K;
+  for (int it = threadIdx.x; it < N * L1; it += blockDim.x) {
+    const int n = it / L1, l = it - n * L1;
+    double ap = 0, aq = 0, aa = 0, ao = 0;
+    for (int m = 0; m <= l; ++m) {
+      const int kk = l * (l + 1) / 2 + m;
+      const double w = (m == 0) ? 1.0 : 2.0;
+      const double2 cc = c[(size_t)n * K + kk];
+      const double2 a0 = A[kk], a1 = A[plane + kk], a2 = A[2 * plane + kk], a3 = A[3 * plane + kk];
+      ap = ap + w * (a0.x * cc.x + a0.y * cc.y);
+      aq = aq + w * (a1.x * cc.x + a1.y * cc.y);
+      aa = aa + w * (a2.x * cc.x + a2.y * cc.y);
+      ao = ao + w * (a3.x * cc.x + a3.y * cc.y);
+    }
+    sPQ[it] = ap;
+    sPQ[N * L1 + it] = aq;
+    sPQ[2 * N * L1 + it] = aa;
+    sPQ[3 * N * L1 + it] = ao;
+  }
+  __syncthreads();
+  const double *R = rad + (size_t)k * N, *Rd = rad_der + (size_t)k * N;
+  for (int q = threadIdx.x; q < P.n_kept; q += blockDim.x) {
+    const int code = P.kept_nnl[q];
+    const int n = code & 0xff, np = (code >> 8) & 0xff, l = code >> 16;
+    const double pre = kFourPi64 * ((n == np) ? 1.0 : sqrt(2.0));
+    const double rn = R[n], rdn = Rd[n], rnp = R[np], rdnp = Rd[np];
+    const double *Pp = sPQ, *Q = sPQ + N * L1, *Qa = sPQ + 2 * N * L1, *Qo = sPQ + 3 * N * L1;
+    sd[3 * q + 0] = pre * (rdn * Pp[np * L1 + l] + rn * Q[np * L1 + l] + rdnp * Pp[n * L1 + l] + rnp * Q[n * L1 + l]);
+    sd[3 * q + 1] = pre * (rn * Qa[np * L1 + l] + rnp * Qa[n * L1 + l]);
+    sd[3 * q + 2] = pre * (rn * Qo[np * L1 + l] + rnp * Qo[n * L1 + l]);
+  }
+  __syncthreads();
+  const double *sv = soap_un + (size_t)site * ns;
+  double dr = 0, da = 0, dp = 0;
+  for (int o = threadIdx.x; o < ns; o += blockDim.x) {
+    double vr = 0, va = 0, vp = 0;
+    for (int t = P.pi_off[o]; t < P.pi_off[o + 1]; ++t) {
+      const double el = P.pi_el64[t];
+      const int q = P.pi_q[t];
+      vr = vr + el * sd[3 * q];
+      va = va + el * sd[3 * q + 1];
+      vp = vp + el * sd[3 * q + 2];
+    }
+    sdc[3 * o] = vr;
+    sdc[3 * o + 1] = va;
+    sdc[3 * o + 2] = vp;
+    dr += sv[o] * vr;
+    da += sv[o] * va;
+    dp += sv[o] * vp;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    dr += __shfl_xor_sync(0xffffffffu, dr, o);
+    da += __shfl_xor_sync(0xffffffffu, da, o);
+    dp += __shfl_xor_sync(0xffffffffu, dp, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = dr;
+    red[1][threadIdx.x >> 5] = da;
+    red[2][threadIdx.x >> 5] = dp;
+  }
+  __syncthreads();
+  double dot_r = 0, dot_a = 0, dot_o = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    dot_r += red[0][w];
+    dot_a += red[1][w];
+    dot_o += red[2][w];
+  }
+  const double nr = norm[site];
+  const double inv_p = 1.0 / nr, inv_p3 = 1.0 / (nr * nr * nr);
+  double st, ct, sf, cf;
+  sincos(B.thetas[k], &st, &ct);
+  sincos(B.phis[k], &sf, &cf);
+  const double ir = 1.0 / B.rjs[k];
+  const double cx = st * cf, cy = st * sf, cz = ct;
+  const double px = -ct * cf * ir, py = -ct * sf * ir, pz = st * ir;
+  const double ax = -sf * ir, ay = cf * ir;
+  double *out = cart + (size_t)k * ns * 3;
+  for (int o = threadIdx.x; o < ns; o += blockDim.x) {
+    const double s = sv[o];
+    const double vr = sdc[3 * o] * inv_p - s * inv_p3 * dot_r;
+    const double va = sdc[3 * o + 1] * inv_p - s * inv_p3 * dot_a;
+    const double vo = sdc[3 * o + 2] * inv_p - s * inv_p3 * dot_o;
+    out[3 * o + 0] = cx * vr + px * vo + ax * va;
+    out[3 * o + 1] = cy * vr + py * vo + ay * va;
+    out[3 * o + 2] = cz * vr + pz * vo;
+  }
+}
+
+// ---- self column = minus the sum of the site's other columns (:888-892)
+__global__ void k64_self(const DevParams P, const DevBatch B, double *cart) {
+  const int site = blockIdx.x;
+  const int p0 = B.off[site], p1 = min(B.off[site + 1], B.n_pairs);
+  if (p1 <= p0) return;
+  const int w = 3 * P.n_soap;
+  for (int t = threadIdx.x; t < w; t += blockDim.x) {
+    double acc = 0.0;
+    for (int k = p0 + 1; k < p1; ++k) acc = acc - cart[(size_t)k * w + t];
+    cart[(size_t)p0 * w + t] = acc;
+  }
+}
+
+__global__ void k64_normalise(const DevParams P, const DevBatch B, const double *soap_un,
+                              const double *norm, double *soap) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t n = (size_t)B.n_sites * P.n_soap;
+  if (t >= n) return;
+  soap[t] = soap_un[t] / norm[t / P.n_soap];
+}
+
+// ---- pair = sgn * sum_s G(i,s) soap_cart_der(:, s, k), one warp per pair
+__global__ void k64_contract_cart(const DevParams P, const DevBatch B, const double *cart,
+                                  const double *G, int g_layout, double sgn, double *pair) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= B.n_pairs) return;
+  const int k = warp;
+  int lo = 0, hi = B.n_sites;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (B.off[mid] <= k) lo = mid; else hi = mid;
+  }
+  const int site = lo, ns = P.n_soap;
+  const double *ck = cart + (size_t)k * ns * 3;
+  double x = 0, y = 0, z = 0;
+  for (int o = lane; o < ns; o += 32) {
+    const double g = g_layout == 0 ? G[(size_t)o * B.n_sites + site] : G[(size_t)site * ns + o];
+    x += g * ck[3 * o];
+    y += g * ck[3 * o + 1];
+    z += g * ck[3 * o + 2];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    x += __shfl_xor_sync(0xffffffffu, x, o);
+    y += __shfl_xor_sync(0xffffffffu, y, o);
+    z += __shfl_xor_sync(0xffffffffu, z, o);
+  }
+  if (lane == 0) {
+    pair[3 * (size_t)k] = sgn * x;
+    pair[3 * (size_t)k + 1] = sgn * y;
+    pair[3 * (size_t)k + 2] = sgn * z;
+  }
+}
+
+static int max_alpha64(const DevParams &P) {
+  int a = 0;
+  for (int s = 0; s < P.n_species; ++s) a = a > P.rad[s].alpha ? a : P.rad[s].alpha;
+  return a;
+}
+
+cudaError_t launch_fp64_descriptor(const DevParams &P, const DevBatch &B, cudaStream_t s,
+                                   const Fp64Work &w, int do_der, double *soap, double *cart,
+                                   int *launches) {
+  const int np = B.n_pairs, nsites = B.n_sites;
+  int nl = 0;
+  if (np > 0) {
+    const int blocks = (np + 127) / 128;
+    if (max_alpha64(P) <= 8) k64_radial<8><<<blocks, 128, 0, s>>>(P, B, do_der, w.rad, w.rad_der);
+    else k64_radial<16><<<blocks, 128, 0, s>>>(P, B, do_der, w.rad, w.rad_der);
+    if (P.l_max <= 8) k64_angular<8><<<blocks, 128, 0, s>>>(P, B, do_der, (double2 *)w.ang);
+    else k64_angular<12><<<blocks, 128, 0, s>>>(P, B, do_der, (double2 *)w.ang);
+    nl += 2;
+  }
+  if (nsites > 0) {
+    k64_cnk<<<nsites, 256, 0, s>>>(P, B, w.rad, (const double2 *)w.ang, (double2 *)w.cnk);
+    const size_t sm = (size_t)P.n_kept * sizeof(double);
+    cudaFuncSetAttribute(k64_soap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k64_soap<<<nsites, 256, sm, s>>>(P, B, (const double2 *)w.cnk, w.soap_unnorm, w.norm);
+    nl += 2;
+  }
+  if (do_der && cart && np > 0) {
+    const size_t sm = ((size_t)4 * P.n_max * (P.l_max + 1) + 3 * (size_t)P.n_kept + 3 * (size_t)P.n_soap) *
+                      sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(k64_cart, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k64_cart<<<np, 128, sm, s>>>(P, B, w.rad, w.rad_der, (const double2 *)w.ang,
+                                 (const double2 *)w.cnk, w.soap_unnorm, w.norm, cart);
+    k64_self<<<nsites, 256, 0, s>>>(P, B, cart);
+    nl += 2;
+  }
+  if (nsites > 0) {
+    const size_t n = (size_t)nsites * P.n_soap;
+    k64_normalise<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, B, w.soap_unnorm, w.norm, soap);
+    nl += 1;
+  }
+  if (launches) *launches += nl;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fp64_contract(const DevParams &P, const DevBatch &B, cudaStream_t s,
+                                 const double *cart, const double *G, int g_layout, double sgn,
+                                 double *pair, int *launches) {
+  if (B.n_pairs <= 0) return cudaSuccess;
+  const size_t threads = (size_t)B.n_pairs * 32;
+  k64_contract_cart<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(P, B, cart, G, g_layout, sgn,
+                                                                      pair);
+  if (launches) *launches += 1;
+  return cudaGetLastError();
+}
+
+}  // namespace soapb

@@ -1,0 +1,1131 @@
+// soapb_host.cpp -- host side of libsoapb200.so: argument checks, the basis
+// matrices, the compression and adjoint index tables, device memory, and the
+// two API layers declared in include/soap_b200.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/soap_b200.h"
+#include "soapb_internal.h"
+
+using namespace soapb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  return fail(SOAPB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CU(call)                                                   \
+  do {                                                             \
+    cudaError_t _e = (call);                                       \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call);            \
+  } while (0)
+
+// ---------------------------------------------------------------- basis
+// Overlap of the primitive poly3 functions (src/soap_turbo_radial.f90:1041-1047)
+void overlap_poly3(int a, double *S) {
+  for (int i = 1; i <= a; ++i) {
+    S[(i - 1) * a + (i - 1)] = 1.0;
+    for (int j = i + 1; j <= a; ++j) {
+      const double v = std::sqrt((double)(5 + 2 * i) * (double)(5 + 2 * j)) / (double)(5 + i + j);
+      S[(j - 1) * a + (i - 1)] = v;
+      S[(i - 1) * a + (j - 1)] = v;
+    }
+  }
+}
+
+// poly3 functions plus the origin Gaussian; the Gaussian-polynomial overlaps
+// come from the recursion of src/soap_turbo_radial.f90:1145-1172.
+void overlap_poly3gauss(int a, double sigma_in, double rcut_in, double *S) {
+  overlap_poly3(a - 1, S);  // fills an (a-1)x(a-1) block with stride a-1; re-stride below
+  std::vector<double> tmp(S, S + (size_t)(a - 1) * (a - 1));
+  for (int j = 0; j < a; ++j)
+    for (int i = 0; i < a; ++i) S[j * a + i] = (i < a - 1 && j < a - 1) ? tmp[j * (a - 1) + i] : 0.0;
+  const double pi = std::acos(-1.0), sq2 = std::sqrt(2.0);
+  const double sig = sigma_in / rcut_in, rc = 1.0, s2 = sig * sig;
+  double I_n = 0.0, N_n = 1.0;
+  double N_np1 = std::sqrt(rc / 1.0);
+  double I_np1 = std::sqrt(pi / 2.0) * sig * std::erf(rc / sq2 / sig) / N_np1;
+  double C2 = s2 / rc;
+  for (int n = -1; n <= a - 1; ++n) {
+    C2 = C2 * rc;
+    const double N_np2 = std::sqrt(rc / (double)(2 * n + 5));
+    const double I_np2 = s2 * (double)(n + 1) * N_n / N_np2 * I_n + N_np1 * rc / N_np2 * I_np1 - C2 / N_np2;
+    if (n > 0) {
+      const double v = I_np2 * sq2 / std::sqrt(sig) / std::pow(pi, 0.25);
+      S[(n - 1) * a + (a - 1)] = v;
+      S[(a - 1) * a + (n - 1)] = v;
+    }
+    N_n = N_np1;
+    N_np1 = N_np2;
+    I_n = I_np1;
+    I_np1 = I_np2;
+  }
+  S[(a - 1) * a + (a - 1)] = 1.0;
+}
+
+// W = S^{-1/2}, the inverse principal square root of the SPD overlap matrix.
+// The reference builds it with dgesvd + dpotrf/dpotri in FP64
+// (src/soap_turbo_radial.f90:1052-1087); S is ill-conditioned (cond ~1e13 at
+// alpha = 8), so this does a cyclic Jacobi eigendecomposition in long double
+// and forms V diag(lambda^{-1/2}) V^T there.
+int inverse_sqrt(int a, const double *S, double *W) {
+  std::vector<long double> A((size_t)a * a), V((size_t)a * a, 0.0L);
+  for (int i = 0; i < a * a; ++i) A[i] = S[i];
+  for (int i = 0; i < a; ++i) V[i * a + i] = 1.0L;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    long double off = 0.0L;
+    for (int p = 0; p < a; ++p)
+      for (int q = p + 1; q < a; ++q) off += A[q * a + p] * A[q * a + p];
+    if (off < 1.0e-70L) break;
+    for (int p = 0; p < a; ++p)
+      for (int q = p + 1; q < a; ++q) {
+        const long double apq = A[q * a + p];
+        if (apq == 0.0L) continue;
+        const long double theta = (A[q * a + q] - A[p * a + p]) / (2.0L * apq);
+        const long double t = (theta >= 0 ? 1.0L : -1.0L) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0L));
+        const long double c = 1.0L / std::sqrt(t * t + 1.0L), s = t * c;
+        for (int k = 0; k < a; ++k) {
+          const long double akp = A[p * a + k], akq = A[q * a + k];
+          A[p * a + k] = c * akp - s * akq;
+          A[q * a + k] = s * akp + c * akq;
+        }
+        for (int k = 0; k < a; ++k) {
+          const long double apk = A[k * a + p], aqk = A[k * a + q];
+          A[k * a + p] = c * apk - s * aqk;
+          A[k * a + q] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < a; ++k) {
+          const long double vkp = V[p * a + k], vkq = V[q * a + k];
+          V[p * a + k] = c * vkp - s * vkq;
+          V[q * a + k] = s * vkp + c * vkq;
+        }
+      }
+  }
+  std::vector<long double> d(a);
+  for (int i = 0; i < a; ++i) {
+    if (!(A[i * a + i] > 0.0L)) return 1;
+    d[i] = 1.0L / std::sqrt(A[i * a + i]);
+  }
+  for (int i = 0; i < a; ++i)
+    for (int j = 0; j < a; ++j) {
+      long double acc = 0.0L;
+      for (int k = 0; k < a; ++k) acc += V[k * a + i] * d[k] * V[k * a + j];
+      W[j * a + i] = (double)acc;
+    }
+  return 0;
+}
+
+// get_preflm (src/soap_turbo_functions.f90:215-241)
+void preflm(int lmax, double *out) {
+  int k = 0;
+  for (int l = 0; l <= lmax; ++l) {
+    const double ppi = std::sqrt((double)(2 * l + 1) / 4.0 / std::acos(-1.0));
+    double fact2 = 1.0;
+    for (int i = 1; i <= l; ++i) fact2 *= (double)i;
+    double fact1 = fact2;
+    for (int m = 0; m <= l; ++m) {
+      if (m > 0) {
+        fact1 = fact1 / (double)(l + 1 - m);
+        fact2 = fact2 * (double)(l + m);
+      }
+      out[k++] = ppi * std::sqrt(fact1 / fact2);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- device memory
+struct DBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return SOAPB_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    if (bytes == 0) return SOAPB_OK;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+    cap = bytes;
+    return SOAPB_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <typename T>
+  T *as() const { return (T *)p; }
+};
+
+}  // namespace
+
+// ====================================================================== context
+struct soapb_context {
+  int device = 0;
+  // definition
+  int n_species = 0, l_max = 0, basis = 0, scaling = 0, radial_enh = 0, legacy = 1;
+  std::vector<int> alpha;
+  std::vector<double> rcut_hard, rcut_soft, nf, gscale, sig_r, sig_r_c, sig_t, sig_t_c, amp_sc, cw;
+  int compress = 0;
+  std::vector<int> P_i, P_j;
+  std::vector<double> P_el;
+  int n_max = 0, n_soap = 0, n_kept = 0;
+  std::vector<double> W, S;  // n_max x n_max
+  DevParams P{};
+  // device tables
+  DBuf tables;
+  // arena
+  DBuf off, bits, err, keep_c, keep_norm;
+  DBuf f64_rad, f64_rad_der, f64_ang, f64_cnk, f64_soap_un, f64_norm;
+  cudaStream_t stream = 0;
+  int threads = 0;
+  int64_t launches = 0;
+  int keep_valid = 0, keep_sites = 0, keep_pairs = 0;
+
+  ~soapb_context() {
+    for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &f64_rad, &f64_rad_der,
+                    &f64_ang, &f64_cnk, &f64_soap_un, &f64_norm})
+      b->release();
+  }
+};
+
+namespace {
+
+int basis_limit_check(int basis, int alpha) {
+  if (alpha < 1) return fail(SOAPB_ERR_ARGUMENT, "alpha_max must be >= 1");
+  if (basis == SOAPB_BASIS_POLY3 && alpha > 10)
+    return fail(SOAPB_ERR_ALPHA_TOO_LARGE,
+                "ERROR: Due to numerical instabilities in the basis construction for the poly3 "
+                "basis, alpha_max > 10 is refused (recommended: <= 7)");
+  if (basis == SOAPB_BASIS_POLY3GAUSS && alpha > 11)
+    return fail(SOAPB_ERR_ALPHA_TOO_LARGE,
+                "ERROR: Due to numerical instabilities in the basis construction for the "
+                "poly3gauss basis, alpha_max > 11 is refused (recommended: <= 8)");
+  if (alpha > SOAPB_MAX_ALPHA) return fail(SOAPB_ERR_ARGUMENT, "alpha_max above %d", SOAPB_MAX_ALPHA);
+  return SOAPB_OK;
+}
+
+int species_basis(int basis, int alpha, double sig, double rcut, double *S, double *W) {
+  if (basis == SOAPB_BASIS_POLY3) overlap_poly3(alpha, S);
+  else overlap_poly3gauss(alpha, sig, rcut, S);
+  if (inverse_sqrt(alpha, S, W)) return fail(SOAPB_ERR_BASIS_MATRIX, "overlap matrix not positive definite");
+  return SOAPB_OK;
+}
+
+int u_index(int n, int np, int l, int N, int L) {  // uncompressed component, 0-based, n <= np
+  return (n * N - n * (n - 1) / 2 + (np - n)) * (L + 1) + l;
+}
+
+// Builds DevParams and the device tables from the context's definition.
+int build_tables(soapb_context *c) {
+  DevParams &P = c->P;
+  std::memset(&P, 0, sizeof(P));
+  const int N = c->n_max, L = c->l_max, K = (L + 1) * (L + 2) / 2;
+  P.n_species = c->n_species;
+  P.l_max = L;
+  P.k_max = K;
+  P.n_max = N;
+  P.basis = c->basis;
+  P.scaling_poly = c->scaling == SOAPB_SCALING_POLYNOMIAL;
+  P.radial_enh = c->radial_enh;
+  P.legacy_seed = c->legacy;
+  double rcut_max = 0.0;
+  for (int s = 0; s < c->n_species; ++s) rcut_max = std::max(rcut_max, c->rcut_hard[s]);
+  P.rcut_max = rcut_max;
+  P.rcut2 = rcut_max * rcut_max;
+  const double pi = std::acos(-1.0);
+  int nbeg = 0, amax = 0;
+  for (int s = 0; s < c->n_species; ++s) {
+    RadSp &R = P.rad[s];
+    R.inv_rcut = 1.0 / c->rcut_hard[s];
+    R.rs = c->rcut_soft[s] * R.inv_rcut;
+    R.atom_sigma = c->sig_r[s] * R.inv_rcut;
+    R.dr = 1.0 - R.rs;
+    R.sqrt_rcut = std::sqrt(c->rcut_hard[s]);
+    R.inv_sqrt_rcut = 1.0 / R.sqrt_rcut;
+    R.sigma_sq0 = R.atom_sigma * R.atom_sigma;
+    R.N_gauss = std::sqrt(2.0 / R.atom_sigma) / std::pow(pi, 0.25);
+    R.has_filter = R.dr > 0.0;
+    if (R.has_filter) {
+      R.drnf = R.dr / c->nf[s];
+      R.q = R.drnf * R.drnf;
+    }
+    R.c = c->sig_r_c[s];
+    R.amp_scaling = c->amp_sc[s];
+    R.cw = c->cw[s];
+    R.gscale = c->gscale[s];
+    R.rcut_hard = c->rcut_hard[s];
+    R.alpha = c->alpha[s];
+    R.n_poly = c->basis == SOAPB_BASIS_POLY3GAUSS ? c->alpha[s] - 1 : c->alpha[s];
+    R.nbeg = nbeg;
+    R.do_central = c->basis == SOAPB_BASIS_POLY3GAUSS ? 0 : (c->cw[s] != 0.0);
+    nbeg += c->alpha[s];
+    amax = std::max(amax, c->alpha[s]);
+    P.sig_t[s] = c->sig_t[s];
+    P.sig_t_c[s] = c->sig_t_c[s];
+  }
+  // alpha recursion tables (src/soap_turbo_radial.f90:503-526), index n+4
+  double Nv[SOAPB_NTAB + 8];
+  auto NV = [&](int n) -> double & { return Nv[n + 4]; };
+  NV(-3) = 1.0;
+  for (int n = -2; n <= SOAPB_NTAB; ++n) NV(n) = std::sqrt(1.0 / (double)(2 * n + 5));
+  for (int n = -1; n < SOAPB_NTAB - 4; ++n) {
+    P.ra[n + 4] = (double)(n + 1) * NV(n - 2) / NV(n);
+    P.rb[n + 4] = NV(n - 1) / NV(n);
+    P.rc[n + 4] = 1.0 / NV(n);
+  }
+  P.ra[3] = 0.0;
+  for (int n = 1; n < SOAPB_NTAB - 4; ++n) {
+    P.R1[n + 4] = NV(n + 1) / NV(n);
+    P.R2[n + 4] = NV(n + 2) / NV(n);
+  }
+  std::vector<double> pf(K);
+  preflm(L, pf.data());
+  for (int k = 0; k < K; ++k) {
+    P.preflm[k] = (float)pf[k];
+    P.preflm64[k] = pf[k];
+  }
+
+  // compression: kept components and the two CSR maps
+  const int n_unc = N * (N + 1) / 2 * (L + 1);
+  std::vector<int> Pi, Pj;
+  std::vector<double> Pel;
+  if (c->compress) {
+    Pi = c->P_i;
+    Pj = c->P_j;
+    Pel = c->P_el;
+    int mx = 0;
+    for (size_t t = 0; t < Pi.size(); ++t) {
+      if (Pi[t] < 1 || Pj[t] < 1 || Pj[t] > n_unc)
+        return fail(SOAPB_ERR_ARGUMENT, "compression index out of range at entry %zu", t);
+      mx = std::max(mx, Pi[t]);
+    }
+    c->n_soap = mx;
+  } else {
+    Pi.resize(n_unc);
+    Pj.resize(n_unc);
+    Pel.assign(n_unc, 1.0);
+    for (int u = 0; u < n_unc; ++u) Pi[u] = Pj[u] = u + 1;
+    c->n_soap = n_unc;
+  }
+  std::vector<int> qof(n_unc, -1);
+  for (size_t t = 0; t < Pj.size(); ++t) qof[Pj[t] - 1] = 0;
+  std::vector<int> kept_nnl;
+  {
+    int q = 0;
+    for (int n = 0; n < N; ++n)
+      for (int np = n; np < N; ++np)
+        for (int l = 0; l <= L; ++l) {
+          const int u = u_index(n, np, l, N, L);
+          if (qof[u] < 0) continue;
+          qof[u] = q++;
+          kept_nnl.push_back(n | (np << 8) | (l << 16));
+        }
+    c->n_kept = q;
+  }
+  const int ns = c->n_soap, nk = c->n_kept, nz = (int)Pi.size();
+  std::vector<int> pi_off(ns + 1, 0), pi_q(nz);
+  std::vector<float> pi_el(nz);
+  std::vector<double> pi_el64(nz);
+  for (int t = 0; t < nz; ++t) pi_off[Pi[t]]++;
+  for (int o = 0; o < ns; ++o) pi_off[o + 1] += pi_off[o];
+  {
+    std::vector<int> fill(pi_off.begin(), pi_off.end() - 1);
+    for (int t = 0; t < nz; ++t) {
+      const int o = Pi[t] - 1, pos = fill[o]++;
+      pi_q[pos] = qof[Pj[t] - 1];
+      pi_el[pos] = (float)Pel[t];
+      pi_el64[pos] = Pel[t];
+    }
+  }
+  std::vector<int> pj_off(nk + 1, 0), pj_o(nz);
+  std::vector<float> pj_el(nz);
+  std::vector<double> pj_el64(nz);
+  for (int t = 0; t < nz; ++t) pj_off[qof[Pj[t] - 1] + 1]++;
+  for (int q = 0; q < nk; ++q) pj_off[q + 1] += pj_off[q];
+  {
+    std::vector<int> fill(pj_off.begin(), pj_off.end() - 1);
+    for (int t = 0; t < nz; ++t) {
+      const int q = qof[Pj[t] - 1], pos = fill[q]++;
+      pj_o[pos] = Pi[t] - 1;
+      pj_el[pos] = (float)Pel[t];
+      pj_el64[pos] = Pel[t];
+    }
+  }
+  // Y(n, np, l) lists for H (src/soap_turbo.f90:1800-1835)
+  std::vector<int> hl_off((L + 1) * N + 1, 0), hl_np, hl_q;
+  std::vector<float> hl_fac;
+  std::vector<double> hl_fac64;
+  for (int l = 0; l <= L; ++l)
+    for (int n = 0; n < N; ++n) {
+      for (int np = 0; np < N; ++np) {
+        const int u = u_index(std::min(n, np), std::max(n, np), l, N, L);
+        if (qof[u] < 0) continue;
+        hl_np.push_back(np);
+        hl_q.push_back(qof[u]);
+        const double fac = (n == np) ? 2.0 : std::sqrt(2.0);
+        hl_fac.push_back((float)fac);
+        hl_fac64.push_back(fac);
+      }
+      hl_off[l * N + n + 1] = (int)hl_np.size();
+    }
+  // poly3gauss central-atom term (src/soap_turbo.f90:646-662)
+  std::vector<double> central(N, 0.0);
+  if (c->basis == SOAPB_BASIS_POLY3GAUSS) {
+    for (int s = 0; s < c->n_species; ++s) {
+      if (c->cw[s] == 0.0) continue;
+      double amplitude = 1.0;
+      if (c->radial_enh == 1) amplitude = std::sqrt(2.0 / pi) * c->sig_r[s] / c->rcut_hard[s];
+      else if (c->radial_enh == 2) amplitude = std::pow(c->sig_r[s], 2) / std::pow(c->rcut_hard[s], 2);
+      const double fac = amplitude * c->cw[s] * std::sqrt(4.0 * pi) * std::pow(pi, 0.25) *
+                         std::sqrt(c->sig_r[s] / 2.0) * std::pow(c->rcut_hard[s], 3) /
+                         std::pow(c->sig_t[s], 2) / c->sig_r[s];
+      const int b = P.rad[s].nbeg, a = c->alpha[s];
+      for (int n = 0; n < a; ++n) {
+        double ws = 0.0;
+        for (int m = 0; m < a; ++m) ws += c->W[(size_t)(b + m) * N + (b + n)] * c->S[(size_t)(b + a - 1) * N + (b + m)];
+        central[b + n] = fac * ws;
+      }
+    }
+  }
+  // W blocks, alpha_s x alpha_s each, stride amax^2
+  const int wstride = amax * amax;
+  std::vector<double> Wblk((size_t)c->n_species * wstride, 0.0);
+  for (int s = 0; s < c->n_species; ++s) {
+    const int b = P.rad[s].nbeg, a = c->alpha[s];
+    for (int j = 0; j < a; ++j)
+      for (int i = 0; i < a; ++i) Wblk[(size_t)s * wstride + j * a + i] = c->W[(size_t)(b + j) * N + (b + i)];
+  }
+  // one device allocation for every table
+  struct Piece { const void *src; size_t bytes; size_t off; };
+  std::vector<Piece> pcs;
+  size_t total = 0;
+  auto add = [&](const void *src, size_t bytes) {
+    total = (total + 255) / 256 * 256;
+    pcs.push_back({src, bytes, total});
+    total += bytes;
+    return pcs.size() - 1;
+  };
+  const size_t iW = add(Wblk.data(), Wblk.size() * 8), iC = add(central.data(), central.size() * 8);
+  const size_t iK = add(kept_nnl.data(), kept_nnl.size() * 4);
+  const size_t iPo = add(pi_off.data(), pi_off.size() * 4), iPq = add(pi_q.data(), pi_q.size() * 4);
+  const size_t iPe = add(pi_el.data(), pi_el.size() * 4), iPe64 = add(pi_el64.data(), pi_el64.size() * 8);
+  const size_t iJo = add(pj_off.data(), pj_off.size() * 4), iJq = add(pj_o.data(), pj_o.size() * 4);
+  const size_t iJe = add(pj_el.data(), pj_el.size() * 4), iJe64 = add(pj_el64.data(), pj_el64.size() * 8);
+  const size_t iHo = add(hl_off.data(), hl_off.size() * 4), iHn = add(hl_np.data(), hl_np.size() * 4);
+  const size_t iHq = add(hl_q.data(), hl_q.size() * 4), iHf = add(hl_fac.data(), hl_fac.size() * 4);
+  const size_t iHf64 = add(hl_fac64.data(), hl_fac64.size() * 8);
+  int rc = c->tables.ensure(total + 256);
+  if (rc) return rc;
+  std::vector<unsigned char> host(total + 256, 0);
+  for (auto &p : pcs)
+    if (p.bytes) std::memcpy(host.data() + p.off, p.src, p.bytes);
+  CU(cudaMemcpy(c->tables.p, host.data(), total, cudaMemcpyHostToDevice));
+  auto at = [&](size_t i) { return (void *)((char *)c->tables.p + pcs[i].off); };
+  P.Wblk = (const double *)at(iW);
+  P.wstride = wstride;
+  P.central = (const double *)at(iC);
+  P.kept_nnl = (const int *)at(iK);
+  P.pi_off = (const int *)at(iPo);
+  P.pi_q = (const int *)at(iPq);
+  P.pi_el = (const float *)at(iPe);
+  P.pi_el64 = (const double *)at(iPe64);
+  P.pj_off = (const int *)at(iJo);
+  P.pj_o = (const int *)at(iJq);
+  P.pj_el = (const float *)at(iJe);
+  P.pj_el64 = (const double *)at(iJe64);
+  P.hl_off = (const int *)at(iHo);
+  P.hl_np = (const int *)at(iHn);
+  P.hl_q = (const int *)at(iHq);
+  P.hl_fac = (const float *)at(iHf);
+  P.hl_fac64 = (const double *)at(iHf64);
+  P.n_soap = c->n_soap;
+  P.n_kept = c->n_kept;
+  return SOAPB_OK;
+}
+
+int init_context(soapb_context *c, const soapb_hyper *h) {
+  if (!h) return fail(SOAPB_ERR_ARGUMENT, "null hyperparameters");
+  if (h->n_species < 1 || h->n_species > SOAPB_MAX_SPECIES)
+    return fail(SOAPB_ERR_ARGUMENT, "n_species must be in 1..%d", SOAPB_MAX_SPECIES);
+  if (h->l_max < 0 || h->l_max > SOAPB_MAX_LMAX)
+    return fail(SOAPB_ERR_ARGUMENT, "l_max must be in 0..%d", SOAPB_MAX_LMAX);
+  if (h->basis != SOAPB_BASIS_POLY3 && h->basis != SOAPB_BASIS_POLY3GAUSS)
+    return fail(SOAPB_ERR_BASIS, "basis must be poly3 or poly3gauss");
+  if (h->radial_enhancement < 0 || h->radial_enhancement > 2)
+    return fail(SOAPB_ERR_ARGUMENT, "radial_enhancement must be 0, 1 or 2");
+  const double *arrs[] = {h->rcut_hard, h->rcut_soft, h->nf, h->global_scaling, h->atom_sigma_r,
+                          h->atom_sigma_r_scaling, h->atom_sigma_t, h->atom_sigma_t_scaling,
+                          h->amplitude_scaling, h->central_weight};
+  if (!h->alpha_max) return fail(SOAPB_ERR_ARGUMENT, "null alpha_max");
+  for (const double *a : arrs)
+    if (!a) return fail(SOAPB_ERR_ARGUMENT, "null per-species hyperparameter array");
+  const int ns = h->n_species;
+  c->n_species = ns;
+  c->l_max = h->l_max;
+  c->basis = h->basis;
+  c->scaling = h->scaling_mode;
+  c->radial_enh = h->radial_enhancement;
+  c->legacy = h->legacy_filter_seed ? 1 : 0;
+  c->alpha.assign(h->alpha_max, h->alpha_max + ns);
+  auto cp = [&](std::vector<double> &v, const double *a) { v.assign(a, a + ns); };
+  cp(c->rcut_hard, h->rcut_hard);
+  cp(c->rcut_soft, h->rcut_soft);
+  cp(c->nf, h->nf);
+  cp(c->gscale, h->global_scaling);
+  cp(c->sig_r, h->atom_sigma_r);
+  cp(c->sig_r_c, h->atom_sigma_r_scaling);
+  cp(c->sig_t, h->atom_sigma_t);
+  cp(c->sig_t_c, h->atom_sigma_t_scaling);
+  cp(c->amp_sc, h->amplitude_scaling);
+  cp(c->cw, h->central_weight);
+  int n_max = 0;
+  for (int s = 0; s < ns; ++s) {
+    int rc = basis_limit_check(h->basis, c->alpha[s]);
+    if (rc) return rc;
+    if (!(c->rcut_hard[s] > 0.0) || !(c->sig_r[s] > 0.0) || !(c->sig_t[s] > 0.0) || !(c->nf[s] > 0.0))
+      return fail(SOAPB_ERR_ARGUMENT, "rcut_hard, atom_sigma_r, atom_sigma_t and nf must be > 0");
+    if (c->rcut_soft[s] > c->rcut_hard[s])
+      return fail(SOAPB_ERR_ARGUMENT, "rcut_soft must not exceed rcut_hard");
+    n_max += c->alpha[s];
+  }
+  if (n_max > 255) return fail(SOAPB_ERR_ARGUMENT, "sum of alpha_max above 255");
+  c->n_max = n_max;
+  c->compress = h->compress ? 1 : 0;
+  if (c->compress) {
+    if (h->P_nonzero < 1 || !h->P_i || !h->P_j || !h->P_el)
+      return fail(SOAPB_ERR_ARGUMENT, "compression map missing");
+    c->P_i.assign(h->P_i, h->P_i + h->P_nonzero);
+    c->P_j.assign(h->P_j, h->P_j + h->P_nonzero);
+    c->P_el.assign(h->P_el, h->P_el + h->P_nonzero);
+  }
+  // basis matrices, block diagonal over species (src/soap_turbo.f90:356-387)
+  c->W.assign((size_t)n_max * n_max, 0.0);
+  c->S.assign((size_t)n_max * n_max, 0.0);
+  int b = 0;
+  for (int s = 0; s < ns; ++s) {
+    const int a = c->alpha[s];
+    std::vector<double> Ss((size_t)a * a), Ws((size_t)a * a);
+    int rc = species_basis(h->basis, a, c->sig_r[s], c->rcut_hard[s], Ss.data(), Ws.data());
+    if (rc) return rc;
+    for (int j = 0; j < a; ++j)
+      for (int i = 0; i < a; ++i) {
+        c->W[(size_t)(b + j) * n_max + b + i] = Ws[j * a + i];
+        c->S[(size_t)(b + j) * n_max + b + i] = Ss[j * a + i];
+      }
+    b += a;
+  }
+  return build_tables(c);
+}
+
+int ensure_batch(soapb_context *c, const soapb_batch *b, DevBatch &B) {
+  if (!b) return fail(SOAPB_ERR_ARGUMENT, "null batch");
+  if (b->n_sites < 0 || b->n_atom_pairs < 0) return fail(SOAPB_ERR_ARGUMENT, "negative batch size");
+  if (b->n_sites > 0 && (!b->n_neigh || !b->species_multiplicity || !b->species))
+    return fail(SOAPB_ERR_ARGUMENT, "null site arrays");
+  if (b->n_atom_pairs > 0 && (!b->mask || !b->rjs || !b->thetas || !b->phis))
+    return fail(SOAPB_ERR_ARGUMENT, "null pair arrays");
+  int rc;
+  if ((rc = c->off.ensure(sizeof(int) * ((size_t)b->n_sites + 1)))) return rc;
+  if ((rc = c->bits.ensure((size_t)b->n_atom_pairs + 16))) return rc;
+  if ((rc = c->err.ensure(16))) return rc;
+  B.n_sites = b->n_sites;
+  B.n_pairs = b->n_atom_pairs;
+  B.max_mult = b->max_species_multiplicity;
+  B.n_neigh = b->n_neigh;
+  B.species = b->species;
+  B.species_mult = b->species_multiplicity;
+  B.mask = b->mask;
+  B.rjs = b->rjs;
+  B.thetas = b->thetas;
+  B.phis = b->phis;
+  B.off = c->off.as<int>();
+  B.bits = c->bits.as<uint8_t>();
+  B.err = c->err.as<unsigned long long>();
+  return SOAPB_OK;
+}
+
+int run_prep(soapb_context *c, const DevBatch &B) {
+  CU(cudaMemsetAsync(B.err, 0xff, sizeof(unsigned long long), c->stream));
+  DevParams P = c->P;
+  P.n_pairs = B.n_pairs;
+  P.n_sites = B.n_sites;
+  CU(launch_prep(P, B, c->stream));
+  c->launches += 1;
+  return SOAPB_OK;
+}
+
+int pick_threads(const soapb_context *c) {
+  if (c->threads == 64 || c->threads == 128) return c->threads;
+  return 128;
+}
+
+int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int keep) {
+  DevBatch B{};
+  int rc = ensure_batch(c, b, B);
+  if (rc) return rc;
+  if (b->n_sites > 0 && !d_soap) return fail(SOAPB_ERR_ARGUMENT, "null soap output");
+  if ((rc = run_prep(c, B))) return rc;
+  DevParams P = c->P;
+  P.n_pairs = B.n_pairs;
+  P.n_sites = B.n_sites;
+  if (keep) {
+    if ((rc = c->keep_c.ensure(sizeof(float) * 2 * (size_t)c->n_max * P.k_max * ((size_t)b->n_sites + 1)))) return rc;
+    if ((rc = c->keep_norm.ensure(sizeof(double) * ((size_t)b->n_sites + 1)))) return rc;
+  }
+  LaunchCfg cfg{pick_threads(c), c->stream};
+  CU(launch_descriptor(P, B, cfg, d_soap, keep ? c->keep_c.as<float>() : nullptr,
+                       keep ? c->keep_norm.as<double>() : nullptr, keep));
+  c->launches += (b->n_sites > 0);
+  c->keep_valid = keep;
+  c->keep_sites = b->n_sites;
+  c->keep_pairs = b->n_atom_pairs;
+  return SOAPB_OK;
+}
+
+int ctx_contract(soapb_context *c, const soapb_batch *b, const double *d_soap, const double *d_G,
+                 int g_layout, double sgn, double *d_pair) {
+  if (!c->keep_valid || c->keep_sites != b->n_sites || c->keep_pairs != b->n_atom_pairs)
+    return fail(SOAPB_ERR_CONTRACT_STATE,
+                "ERROR: soap_contract needs get_soap called with contract = .true. first");
+  if (g_layout != 0 && g_layout != 1) return fail(SOAPB_ERR_ARGUMENT, "bad g_layout");
+  if (b->n_sites > 0 && (!d_soap || !d_G || !d_pair)) return fail(SOAPB_ERR_ARGUMENT, "null pointer");
+  DevBatch B{};
+  int rc = ensure_batch(c, b, B);
+  if (rc) return rc;
+  DevParams P = c->P;
+  P.n_pairs = B.n_pairs;
+  P.n_sites = B.n_sites;
+  LaunchCfg cfg{pick_threads(c), c->stream};
+  CU(launch_contract(P, B, cfg, d_soap, d_G, g_layout, sgn, c->keep_c.as<float>(),
+                     c->keep_norm.as<double>(), d_pair));
+  c->launches += (b->n_sites > 0);
+  return SOAPB_OK;
+}
+
+int ctx_fp64(soapb_context *c, const soapb_batch *b, double *d_soap, double *d_cart) {
+  DevBatch B{};
+  int rc = ensure_batch(c, b, B);
+  if (rc) return rc;
+  if ((rc = run_prep(c, B))) return rc;
+  DevParams P = c->P;
+  P.n_pairs = B.n_pairs;
+  P.n_sites = B.n_sites;
+  const size_t np = (size_t)b->n_atom_pairs + 1, ns = (size_t)b->n_sites + 1;
+  const int do_der = d_cart != nullptr;
+  if ((rc = c->f64_rad.ensure(8 * np * c->n_max))) return rc;
+  if ((rc = c->f64_rad_der.ensure(8 * np * c->n_max))) return rc;
+  if ((rc = c->f64_ang.ensure(16 * np * P.k_max * (do_der ? 4 : 1)))) return rc;
+  if ((rc = c->f64_cnk.ensure(16 * ns * c->n_max * P.k_max))) return rc;
+  if ((rc = c->f64_soap_un.ensure(8 * ns * c->n_soap))) return rc;
+  if ((rc = c->f64_norm.ensure(8 * ns))) return rc;
+  Fp64Work w{c->f64_rad.as<double>(), c->f64_rad_der.as<double>(), c->f64_ang.as<double>(),
+             c->f64_cnk.as<double>(), c->f64_soap_un.as<double>(), c->f64_norm.as<double>()};
+  int nl = 0;
+  CU(launch_fp64_descriptor(P, B, c->stream, w, do_der, d_soap, d_cart, &nl));
+  c->launches += nl;
+  return SOAPB_OK;
+}
+
+int ctx_contract_cart(soapb_context *c, const soapb_batch *b, const double *d_cart, const double *d_G,
+                      int g_layout, double sgn, double *d_pair) {
+  DevBatch B{};
+  int rc = ensure_batch(c, b, B);
+  if (rc) return rc;
+  DevParams P = c->P;
+  P.n_pairs = B.n_pairs;
+  P.n_sites = B.n_sites;
+  int nl = 0;
+  CU(launch_fp64_contract(P, B, c->stream, d_cart, d_G, g_layout, sgn, d_pair, &nl));
+  c->launches += nl;
+  return SOAPB_OK;
+}
+
+int check_device() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return fail(SOAPB_ERR_NO_DEVICE, "no CUDA device available (%s)", cudaGetErrorString(e));
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, dev);
+  if (prop.major != 10)
+    return fail(SOAPB_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a", dev,
+                prop.major, prop.minor);
+  return SOAPB_OK;
+}
+
+}  // namespace
+
+// ================================================================ context layer
+extern "C" {
+
+const char *soapb_last_error(void) { return g_last_error.c_str(); }
+const char *soapb_version(void) { return "soap_b200 0.1 (sm_100a)"; }
+
+int soapb_create(const soapb_hyper *hyper, int32_t device, soapb_context **out) {
+  if (!out) return fail(SOAPB_ERR_ARGUMENT, "null output handle");
+  *out = nullptr;
+  int rc = check_device();
+  if (rc) return rc;
+  if (device >= 0) CU(cudaSetDevice(device));
+  auto *c = new soapb_context();
+  cudaGetDevice(&c->device);
+  rc = init_context(c, hyper);
+  if (rc) {
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return SOAPB_OK;
+}
+
+int soapb_destroy(soapb_context *ctx) {
+  delete ctx;
+  return SOAPB_OK;
+}
+
+int soapb_set_basis(soapb_context *c, const double *W, const double *S) {
+  if (!c || !W || !S) return fail(SOAPB_ERR_ARGUMENT, "null argument");
+  c->W.assign(W, W + (size_t)c->n_max * c->n_max);
+  c->S.assign(S, S + (size_t)c->n_max * c->n_max);
+  return build_tables(c);
+}
+
+int soapb_get_basis(const soapb_context *c, double *W, double *S) {
+  if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
+  if (W) std::memcpy(W, c->W.data(), c->W.size() * 8);
+  if (S) std::memcpy(S, c->S.data(), c->S.size() * 8);
+  return SOAPB_OK;
+}
+
+int soapb_n_soap(const soapb_context *c, int32_t *n_soap) {
+  if (!c || !n_soap) return fail(SOAPB_ERR_ARGUMENT, "null argument");
+  *n_soap = c->n_soap;
+  return SOAPB_OK;
+}
+
+int soapb_set_stream(soapb_context *c, void *stream) {
+  if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
+  c->stream = (cudaStream_t)stream;
+  return SOAPB_OK;
+}
+
+int soapb_set_threads_per_site(soapb_context *c, int32_t threads) {
+  if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
+  if (threads != 0 && threads != 64 && threads != 128)
+    return fail(SOAPB_ERR_ARGUMENT, "threads per site must be 0, 64 or 128");
+  c->threads = threads;
+  return SOAPB_OK;
+}
+
+int soapb_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int32_t keep) {
+  if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
+  return ctx_descriptor(c, b, d_soap, keep);
+}
+
+int soapb_contract(soapb_context *c, const soapb_batch *b, const double *d_soap, const double *d_G,
+                   int32_t g_layout, double sgn, double *d_pair) {
+  if (!c || !b) return fail(SOAPB_ERR_ARGUMENT, "null argument");
+  return ctx_contract(c, b, d_soap, d_G, g_layout, sgn, d_pair);
+}
+
+int soapb_descriptor_and_vjp(soapb_context *c, const soapb_batch *b, const double *d_G,
+                             int32_t g_layout, double sgn, double *d_soap, double *d_pair) {
+  if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
+  int rc = ctx_descriptor(c, b, d_soap, 1);
+  if (rc) return rc;
+  return ctx_contract(c, b, d_soap, d_G, g_layout, sgn, d_pair);
+}
+
+int soapb_descriptor_fp64(soapb_context *c, const soapb_batch *b, double *d_soap, double *d_cart) {
+  if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
+  return ctx_fp64(c, b, d_soap, d_cart);
+}
+
+int soapb_contract_cart_der(soapb_context *c, const soapb_batch *b, const double *d_cart,
+                            const double *d_G, int32_t g_layout, double sgn, double *d_pair) {
+  if (!c || !b) return fail(SOAPB_ERR_ARGUMENT, "null argument");
+  return ctx_contract_cart(c, b, d_cart, d_G, g_layout, sgn, d_pair);
+}
+
+int soapb_check_inputs(soapb_context *c, int64_t *bad_pair) {
+  if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
+  if (bad_pair) *bad_pair = -1;
+  if (!c->err.p) return SOAPB_OK;
+  unsigned long long v = 0;
+  CU(cudaMemcpyAsync(&v, c->err.p, sizeof v, cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  if (v == ~0ull) return SOAPB_OK;
+  if (v == (1ull << 62)) return fail(SOAPB_ERR_INPUT, "n_neigh is negative or does not sum to n_atom_pairs");
+  if (bad_pair) *bad_pair = (int64_t)v;
+  return fail(SOAPB_ERR_INPUT, "non-finite or negative pair input at pair %llu", v);
+}
+
+int soapb_launch_count(const soapb_context *c, int64_t *count) {
+  if (!c || !count) return fail(SOAPB_ERR_ARGUMENT, "null argument");
+  *count = c->launches;
+  return SOAPB_OK;
+}
+
+int soapb_orthonormalization_matrix(int32_t basis, int32_t alpha_max, double atom_sigma_r,
+                                    double rcut_hard, double *S, double *W) {
+  if (!S || !W) return fail(SOAPB_ERR_ARGUMENT, "null output");
+  if (basis != SOAPB_BASIS_POLY3 && basis != SOAPB_BASIS_POLY3GAUSS)
+    return fail(SOAPB_ERR_BASIS, "basis must be poly3 or poly3gauss");
+  int rc = basis_limit_check(basis, alpha_max);
+  if (rc) return rc;
+  return species_basis(basis, alpha_max, atom_sigma_r, rcut_hard, S, W);
+}
+
+int soapb_get_compress_indices(const char *compress_mode, int32_t n_species, const int32_t *alpha_max,
+                               int32_t l_max, int32_t *dim, int32_t *P_nonzero, int32_t *P_i,
+                               int32_t *P_j, double *P_el, const char *what_to_do) {
+  if (!compress_mode || !alpha_max || !dim || !P_nonzero || !what_to_do)
+    return fail(SOAPB_ERR_ARGUMENT, "null argument");
+  bool set;
+  if (!std::strcmp(what_to_do, "get_dim")) set = false;
+  else if (!std::strcmp(what_to_do, "set_indices")) set = true;
+  else return fail(SOAPB_ERR_ARGUMENT, "ERROR: incorrect what_to_do in get_compress_indices() subroutine!");
+  if (std::strcmp(compress_mode, "trivial") && std::strcmp(compress_mode, "Trivial"))
+    return fail(SOAPB_ERR_COMPRESS_MODE, "ERROR: I don't understand compress_mode = %s", compress_mode);
+  if (n_species < 1) return fail(SOAPB_ERR_ARGUMENT, "n_species must be >= 1");
+  // trivial recipe (src/soap_turbo_compress.f90:86-119)
+  std::vector<int> pivot(n_species);
+  pivot[0] = 1;
+  int n_max = alpha_max[0];
+  for (int i = 0; i < n_species - 1; ++i) {
+    pivot[i + 1] = pivot[i] + alpha_max[i];
+    n_max += alpha_max[i + 1];
+  }
+  if (set && (!P_i || !P_j || !P_el)) return fail(SOAPB_ERR_ARGUMENT, "null index arrays");
+  int counter = 0, k = 1;
+  for (int n = 1; n <= n_max; ++n)
+    for (int m = n; m <= n_max; ++m)
+      for (int l = 0; l <= l_max; ++l) {
+        bool hit = false;
+        for (int s = 0; s < n_species; ++s) hit = hit || n == pivot[s] || m == pivot[s];
+        if (hit) {
+          ++counter;
+          if (set) {
+            if (counter > *P_nonzero) return fail(SOAPB_ERR_ARGUMENT, "index arrays too short");
+            P_i[counter - 1] = counter;
+            P_j[counter - 1] = k;
+            P_el[counter - 1] = 1.0;
+          }
+        }
+        ++k;
+      }
+  *dim = counter;
+  *P_nonzero = counter;
+  return SOAPB_OK;
+}
+
+}  // extern "C"
+
+// ================================================================== drop-in layer
+namespace {
+
+struct DropIn {
+  std::mutex mu;
+  soapb_context *ctx = nullptr;
+  int legacy = 1;
+  int precision = SOAPB_PREC_MIXED;
+  std::vector<double> user_W, user_S;  // caller-supplied basis, if any
+  bool warned_poly3 = false, warned_gauss = false;
+  // device copies of the last batch
+  DBuf n_neigh, species, species_mult, mask, rjs, thetas, phis, soap, G, pair, cart;
+  soapb_batch batch{};
+  int ct_ready = 0, ct_fp64 = 0, ct_n_sites = 0, ct_n_pairs = 0, ct_n_soap = 0;
+  cudaStream_t stream = nullptr;
+};
+
+DropIn &dropin() {
+  static DropIn d;
+  return d;
+}
+
+bool same_definition(const soapb_context *c, const soapb_hyper &h, int legacy) {
+  if (!c) return false;
+  if (c->n_species != h.n_species || c->l_max != h.l_max || c->basis != h.basis ||
+      c->scaling != h.scaling_mode || c->radial_enh != h.radial_enhancement || c->legacy != legacy ||
+      c->compress != (h.compress ? 1 : 0))
+    return false;
+  const int ns = h.n_species;
+  if (std::memcmp(c->alpha.data(), h.alpha_max, 4 * ns)) return false;
+  const std::vector<double> *v[] = {&c->rcut_hard, &c->rcut_soft, &c->nf, &c->gscale, &c->sig_r,
+                                    &c->sig_r_c, &c->sig_t, &c->sig_t_c, &c->amp_sc, &c->cw};
+  const double *a[] = {h.rcut_hard, h.rcut_soft, h.nf, h.global_scaling, h.atom_sigma_r,
+                       h.atom_sigma_r_scaling, h.atom_sigma_t, h.atom_sigma_t_scaling,
+                       h.amplitude_scaling, h.central_weight};
+  for (int i = 0; i < 10; ++i)
+    if (std::memcmp(v[i]->data(), a[i], 8 * ns)) return false;
+  if (c->compress) {
+    if ((int)c->P_i.size() != h.P_nonzero) return false;
+    if (std::memcmp(c->P_i.data(), h.P_i, 4 * h.P_nonzero) ||
+        std::memcmp(c->P_j.data(), h.P_j, 4 * h.P_nonzero) ||
+        std::memcmp(c->P_el.data(), h.P_el, 8 * h.P_nonzero))
+      return false;
+  }
+  return true;
+}
+
+template <typename T>
+int upload(DBuf &b, const T *src, size_t n, cudaStream_t s) {
+  int rc = b.ensure(sizeof(T) * (n + 1));
+  if (rc) return rc;
+  if (n) CU(cudaMemcpyAsync(b.p, src, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+  return SOAPB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int soapb_set_legacy_filter_seed(int32_t legacy) {
+  DropIn &d = dropin();
+  std::lock_guard<std::mutex> g(d.mu);
+  d.legacy = legacy ? 1 : 0;
+  return SOAPB_OK;
+}
+
+int soapb_get_legacy_filter_seed(int32_t *legacy) {
+  if (!legacy) return fail(SOAPB_ERR_ARGUMENT, "null argument");
+  DropIn &d = dropin();
+  std::lock_guard<std::mutex> g(d.mu);
+  *legacy = d.legacy;
+  return SOAPB_OK;
+}
+
+int soapb_set_precision(int32_t precision) {
+  if (precision != SOAPB_PREC_MIXED && precision != SOAPB_PREC_FP64)
+    return fail(SOAPB_ERR_ARGUMENT, "precision must be SOAPB_PREC_MIXED or SOAPB_PREC_FP64");
+  DropIn &d = dropin();
+  std::lock_guard<std::mutex> g(d.mu);
+  d.precision = precision;
+  return SOAPB_OK;
+}
+
+int soapb_set_basis_matrices(int32_t n_max, const double *W, const double *S) {
+  DropIn &d = dropin();
+  std::lock_guard<std::mutex> g(d.mu);
+  if (n_max <= 0 || !W || !S) {
+    d.user_W.clear();
+    d.user_S.clear();
+  } else {
+    d.user_W.assign(W, W + (size_t)n_max * n_max);
+    d.user_S.assign(S, S + (size_t)n_max * n_max);
+  }
+  if (d.ctx && !d.user_W.empty() && (int)d.user_W.size() == d.ctx->n_max * d.ctx->n_max) {
+    int rc = soapb_set_basis(d.ctx, d.user_W.data(), d.user_S.data());
+    if (rc) return rc;
+  }
+  return SOAPB_OK;
+}
+
+int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, const int32_t *species,
+                   int32_t max_species_multiplicity, const int32_t *species_multiplicity,
+                   int32_t n_atom_pairs, const uint8_t *mask, const double *rjs, const double *thetas,
+                   const double *phis, const int32_t *alpha_max, int32_t l_max, const double *rcut_hard,
+                   const double *rcut_soft, const double *nf, const double *global_scaling,
+                   const double *atom_sigma_r, const double *atom_sigma_r_scaling,
+                   const double *atom_sigma_t, const double *atom_sigma_t_scaling,
+                   const double *amplitude_scaling, int32_t radial_enhancement,
+                   const double *central_weight, const char *basis, const char *scaling_mode,
+                   int32_t do_timing, int32_t do_derivatives, int32_t compress_soap,
+                   int32_t compress_P_nonzero, const int32_t *compress_P_i,
+                   const int32_t *compress_P_j, const double *compress_P_el, double *soap,
+                   int32_t n_soap, double *soap_cart_der, int32_t contract) {
+  DropIn &d = dropin();
+  std::lock_guard<std::mutex> g(d.mu);
+  d.ct_ready = 0;
+  if (!basis || !scaling_mode) return fail(SOAPB_ERR_ARGUMENT, "null basis or scaling_mode");
+  int b;
+  if (!std::strcmp(basis, "poly3")) b = SOAPB_BASIS_POLY3;
+  else if (!std::strcmp(basis, "poly3gauss")) b = SOAPB_BASIS_POLY3GAUSS;
+  else return fail(SOAPB_ERR_BASIS, "basis \"%s\" is not supported (poly3, poly3gauss)", basis);
+  if (n_sites < 0 || n_atom_pairs < 0) return fail(SOAPB_ERR_ARGUMENT, "negative sizes");
+  if (n_sites > 0 && !n_neigh) return fail(SOAPB_ERR_ARGUMENT, "null n_neigh");
+  // CSR check on the host: the kernels trust the offsets
+  long long total = 0;
+  for (int i = 0; i < n_sites; ++i) {
+    if (n_neigh[i] < 0) return fail(SOAPB_ERR_INPUT, "n_neigh(%d) is negative", i + 1);
+    total += n_neigh[i];
+  }
+  if (total != n_atom_pairs)
+    return fail(SOAPB_ERR_INPUT, "sum(n_neigh) = %lld but n_atom_pairs = %d", total, n_atom_pairs);
+  for (int i = 0; i < n_sites; ++i)
+    if (species_multiplicity[i] > max_species_multiplicity || species_multiplicity[i] < 0)
+      return fail(SOAPB_ERR_INPUT, "species_multiplicity(%d) out of range", i + 1);
+  for (int s = 0; s < n_species && s < SOAPB_MAX_SPECIES; ++s) {
+    if (b == SOAPB_BASIS_POLY3 && alpha_max[s] > 7 && alpha_max[s] <= 10 && !d.warned_poly3) {
+      d.warned_poly3 = true;
+      std::fprintf(stderr,
+                   "WARNING: Due to numerical instabilities in the basis construction for the poly3 "
+                   "basis, it is strongly recommended not to exceed alpha_max = 7.\n");
+    }
+    if (b == SOAPB_BASIS_POLY3GAUSS && alpha_max[s] > 8 && alpha_max[s] <= 11 && !d.warned_gauss) {
+      d.warned_gauss = true;
+      std::fprintf(stderr,
+                   "WARNING: Due to numerical instabilities in the basis construction for the "
+                   "poly3gauss basis, it is strongly recommended not to exceed alpha_max = 8.\n");
+    }
+  }
+  soapb_hyper h{};
+  h.n_species = n_species;
+  h.l_max = l_max;
+  h.basis = b;
+  h.scaling_mode = std::strcmp(scaling_mode, "polynomial") ? SOAPB_SCALING_NONE : SOAPB_SCALING_POLYNOMIAL;
+  h.radial_enhancement = radial_enhancement;
+  h.legacy_filter_seed = d.legacy;
+  h.alpha_max = alpha_max;
+  h.rcut_hard = rcut_hard;
+  h.rcut_soft = rcut_soft;
+  h.nf = nf;
+  h.global_scaling = global_scaling;
+  h.atom_sigma_r = atom_sigma_r;
+  h.atom_sigma_r_scaling = atom_sigma_r_scaling;
+  h.atom_sigma_t = atom_sigma_t;
+  h.atom_sigma_t_scaling = atom_sigma_t_scaling;
+  h.amplitude_scaling = amplitude_scaling;
+  h.central_weight = central_weight;
+  h.compress = compress_soap;
+  h.P_nonzero = compress_P_nonzero;
+  h.P_i = compress_P_i;
+  h.P_j = compress_P_j;
+  h.P_el = compress_P_el;
+  int rc;
+  if (!same_definition(d.ctx, h, d.legacy)) {
+    // the reference recomputes its basis when the definition changes (:289-388)
+    soapb_context *nc = nullptr;
+    rc = soapb_create(&h, -1, &nc);
+    if (rc) return rc;
+    if (d.ctx) soapb_destroy(d.ctx);
+    d.ctx = nc;
+    if (!d.stream) CU(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking));
+    d.ctx->stream = d.stream;
+    if (!d.user_W.empty() && (int)d.user_W.size() == nc->n_max * nc->n_max)
+      if ((rc = soapb_set_basis(nc, d.user_W.data(), d.user_S.data()))) return rc;
+  }
+  soapb_context *c = d.ctx;
+  if (n_soap != c->n_soap)
+    return fail(SOAPB_ERR_ARGUMENT, "size(soap,1) = %d but the descriptor has n_soap = %d", n_soap, c->n_soap);
+  if (n_sites > 0 && !soap) return fail(SOAPB_ERR_ARGUMENT, "null soap");
+  const bool want_cart = do_derivatives && !contract;
+  if (want_cart && n_atom_pairs > 0 && !soap_cart_der)
+    return fail(SOAPB_ERR_ARGUMENT, "soap_cart_der is needed when do_derivatives and not contract");
+  const bool fp64 = d.precision == SOAPB_PREC_FP64 || want_cart;
+  cudaStream_t s = d.stream;
+  cudaEvent_t ev[4];
+  if (do_timing)
+    for (auto &e : ev) cudaEventCreate(&e);
+  if (do_timing) cudaEventRecord(ev[0], s);
+  if ((rc = upload(d.n_neigh, n_neigh, n_sites, s))) return rc;
+  if ((rc = upload(d.species, species, (size_t)n_sites * max_species_multiplicity, s))) return rc;
+  if ((rc = upload(d.species_mult, species_multiplicity, n_sites, s))) return rc;
+  if ((rc = upload(d.mask, mask, (size_t)n_atom_pairs * n_species, s))) return rc;
+  if ((rc = upload(d.rjs, rjs, n_atom_pairs, s))) return rc;
+  if ((rc = upload(d.thetas, thetas, n_atom_pairs, s))) return rc;
+  if ((rc = upload(d.phis, phis, n_atom_pairs, s))) return rc;
+  if ((rc = d.soap.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
+  soapb_batch &bt = d.batch;
+  bt.n_sites = n_sites;
+  bt.n_atom_pairs = n_atom_pairs;
+  bt.max_species_multiplicity = max_species_multiplicity;
+  bt.n_neigh = d.n_neigh.as<int32_t>();
+  bt.species = d.species.as<int32_t>();
+  bt.species_multiplicity = d.species_mult.as<int32_t>();
+  bt.mask = d.mask.as<uint8_t>();
+  bt.rjs = d.rjs.as<double>();
+  bt.thetas = d.thetas.as<double>();
+  bt.phis = d.phis.as<double>();
+  if (do_timing) cudaEventRecord(ev[1], s);
+  const bool keep_cart = fp64 && do_derivatives;  // FP64 contract works on soap_cart_der
+  if (fp64) {
+    if (keep_cart && (rc = d.cart.ensure(8 * ((size_t)n_atom_pairs * n_soap * 3 + 1)))) return rc;
+    rc = soapb_descriptor_fp64(c, &bt, d.soap.as<double>(), keep_cart ? d.cart.as<double>() : nullptr);
+  } else {
+    rc = soapb_descriptor(c, &bt, d.soap.as<double>(), do_derivatives && contract);
+  }
+  if (rc) return rc;
+  if (do_timing) cudaEventRecord(ev[2], s);
+  if (n_sites > 0)
+    CU(cudaMemcpyAsync(soap, d.soap.p, 8 * (size_t)n_sites * n_soap, cudaMemcpyDeviceToHost, s));
+  if (want_cart && n_atom_pairs > 0)
+    CU(cudaMemcpyAsync(soap_cart_der, d.cart.p, 8 * (size_t)n_atom_pairs * n_soap * 3,
+                       cudaMemcpyDeviceToHost, s));
+  if (do_timing) cudaEventRecord(ev[3], s);
+  CU(cudaStreamSynchronize(s));
+  int64_t bad = -1;
+  if ((rc = soapb_check_inputs(c, &bad))) return rc;
+  if (do_timing) {
+    float t01, t12, t23;
+    cudaEventElapsedTime(&t01, ev[0], ev[1]);
+    cudaEventElapsedTime(&t12, ev[1], ev[2]);
+    cudaEventElapsedTime(&t23, ev[2], ev[3]);
+    std::printf("                                       |\n");
+    std::printf("SOAP timings (GPU, %s):              |\n", fp64 ? "FP64" : "mixed");
+    std::printf("  *) Host to device copies: %8.3f ms |\n", t01);
+    std::printf("  *) Descriptor kernels:    %8.3f ms |\n", t12);
+    std::printf("  *) Device to host copies: %8.3f ms |\n", t23);
+    for (auto &e : ev) cudaEventDestroy(e);
+  }
+  if (do_derivatives && contract) {
+    d.ct_ready = 1;
+    d.ct_fp64 = fp64;
+    d.ct_n_sites = n_sites;
+    d.ct_n_pairs = n_atom_pairs;
+    d.ct_n_soap = n_soap;
+  }
+  return SOAPB_OK;
+}
+
+int soapb_soap_contract(const double *soap, const double *G, double sgn, double *pair, int32_t n_sites,
+                        int32_t n_soap, int32_t n_atom_pairs) {
+  DropIn &d = dropin();
+  std::lock_guard<std::mutex> g(d.mu);
+  if (!d.ct_ready || !d.ctx)
+    return fail(SOAPB_ERR_CONTRACT_STATE, "ERROR: soap_contract needs get_soap called with contract = .true. first");
+  if (n_sites != d.ct_n_sites || n_soap != d.ct_n_soap || n_atom_pairs != d.ct_n_pairs)
+    return fail(SOAPB_ERR_ARGUMENT, "extents differ from the last get_soap call");
+  if (n_sites > 0 && (!soap || !G || !pair)) return fail(SOAPB_ERR_ARGUMENT, "null pointer");
+  cudaStream_t s = d.stream;
+  int rc;
+  if ((rc = upload(d.soap, soap, (size_t)n_sites * n_soap, s))) return rc;
+  if ((rc = upload(d.G, G, (size_t)n_sites * n_soap, s))) return rc;
+  if ((rc = d.pair.ensure(8 * (3 * (size_t)n_atom_pairs + 1)))) return rc;
+  if (d.ct_fp64)
+    rc = soapb_contract_cart_der(d.ctx, &d.batch, d.cart.as<double>(), d.G.as<double>(),
+                                 SOAPB_G_SITE_FASTEST, sgn, d.pair.as<double>());
+  else
+    rc = soapb_contract(d.ctx, &d.batch, d.soap.as<double>(), d.G.as<double>(), SOAPB_G_SITE_FASTEST,
+                        sgn, d.pair.as<double>());
+  if (rc) return rc;
+  if (n_atom_pairs > 0)
+    CU(cudaMemcpyAsync(pair, d.pair.p, 24 * (size_t)n_atom_pairs, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  return SOAPB_OK;
+}
+
+}  // extern "C"

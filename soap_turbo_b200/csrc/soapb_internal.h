@@ -1,0 +1,106 @@
+// soapb_internal.h -- definitions shared by the host API and the kernels.
+//
+// DevParams is the whole descriptor definition as the kernels see it.  It is
+// passed by value as a kernel argument (a few KB), so a launch needs no
+// constant-memory symbol and two contexts never share state.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define SOAPB_MAX_SPECIES 8
+#define SOAPB_MAX_ALPHA 16
+#define SOAPB_MAX_LMAX 12
+#define SOAPB_KMAX_CAP ((SOAPB_MAX_LMAX + 1) * (SOAPB_MAX_LMAX + 2) / 2)
+#define SOAPB_NTAB 28 /* recursion tables, index n+4 for n = -4 .. 23 */
+
+// Radial constants of one species, in the scaled units of the reference's
+// radial kernel (rcut_hard = 1; src/soap_turbo_radial.f90:455-526).
+struct RadSp {
+  double inv_rcut, rs, atom_sigma, dr, sqrt_rcut, inv_sqrt_rcut;
+  double q, drnf, sigma_sq0, N_gauss;
+  double c;            // atom_sigma_r_scaling (scaled by nothing: dimensionless)
+  double amp_scaling;  // amplitude_scaling
+  double cw;           // central_weight
+  double gscale;       // global_scaling
+  double rcut_hard;    // unscaled
+  int alpha, n_poly, nbeg, has_filter, do_central, pad;
+};
+
+struct DevParams {
+  int n_species, l_max, k_max, n_max;
+  int basis;          // 0 poly3, 1 poly3gauss
+  int scaling_poly;   // scaling_mode == "polynomial"
+  int radial_enh;     // radial_enhancement
+  int legacy_seed;    // legacy_filter_seed
+  int n_soap, n_kept, n_pairs, n_sites;
+  double rcut_max, rcut2;
+  RadSp rad[SOAPB_MAX_SPECIES];
+  double sig_t[SOAPB_MAX_SPECIES], sig_t_c[SOAPB_MAX_SPECIES];
+  double ra[SOAPB_NTAB], rb[SOAPB_NTAB], rc[SOAPB_NTAB], R1[SOAPB_NTAB], R2[SOAPB_NTAB];
+  float preflm[SOAPB_KMAX_CAP];
+  double preflm64[SOAPB_KMAX_CAP];
+  // device tables (owned by the context)
+  const double *Wblk;     // per species alpha x alpha, column-major, at s*AMAX2
+  int wstride;            // doubles between species blocks
+  const double *central;  // n_max: poly3gauss central-atom term per radial index
+  const int *kept_nnl;    // n_kept: n | np << 8 | l << 16 of the kept components
+  const int *pi_off;      // n_soap + 1: CSR over outputs of the compression map
+  const int *pi_q;        //   kept position feeding each entry
+  const float *pi_el;
+  const double *pi_el64;
+  const int *pj_off;      // n_kept + 1: CSR over kept components (transpose)
+  const int *pj_o;        //   output index of each entry
+  const float *pj_el;
+  const double *pj_el64;
+  const int *hl_off;      // (l_max+1)*n_max + 1: per (l, n) list of (np, q, fac)
+  const int *hl_np;
+  const int *hl_q;
+  const float *hl_fac;
+  const double *hl_fac64;
+};
+
+// Batch tables the prep kernel derives from the caller's CSR arrays.
+struct DevBatch {
+  int n_sites, n_pairs, max_mult;
+  const int *n_neigh, *species, *species_mult;
+  const uint8_t *mask;
+  const double *rjs, *thetas, *phis;
+  int *off;              // n_sites + 1 (prep output)
+  uint8_t *bits;         // n_pairs: mask bits (prep output)
+  unsigned long long *err;  // first bad pair index + 1 (0 = none)
+};
+
+// Kernel launchers (soapb_mixed.cu, soapb_fp64.cu)
+namespace soapb {
+struct LaunchCfg {
+  int threads;           // threads per site CTA
+  cudaStream_t stream;
+};
+cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s);
+cudaError_t launch_descriptor(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
+                              double *soap, float *keep_c, double *keep_norm, int keep);
+cudaError_t launch_contract(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
+                            const double *soap, const double *G, int g_layout, double sgn,
+                            const float *keep_c, const double *keep_norm, double *pair);
+cudaError_t launch_fused(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
+                         const double *G, int g_layout, double sgn, double *soap, double *pair);
+size_t descriptor_smem(const DevParams &P, int threads);
+size_t contract_smem(const DevParams &P, int threads);
+size_t fused_smem(const DevParams &P, int threads);
+
+// Plain FP64 staged path
+struct Fp64Work {
+  double *rad, *rad_der;   // (n_pairs, n_max)
+  double *ang;             // 4 x (n_pairs, k_max) complex
+  double *cnk;             // (n_sites, n_max, k_max) complex
+  double *soap_unnorm;     // (n_sites, n_soap)
+  double *norm;            // n_sites
+};
+cudaError_t launch_fp64_descriptor(const DevParams &P, const DevBatch &B, cudaStream_t s,
+                                   const Fp64Work &w, int do_der, double *soap, double *cart,
+                                   int *launches);
+cudaError_t launch_fp64_contract(const DevParams &P, const DevBatch &B, cudaStream_t s,
+                                 const double *cart, const double *G, int g_layout, double sgn,
+                                 double *pair, int *launches);
+}  // namespace soapb
