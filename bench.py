@@ -1,0 +1,438 @@
+"""Benchmark: SOAP environments/s of the descriptor + force VJP step on B200.
+
+One step is the reference's force path on one structure of the 3-species
+configuration (4096 atoms, Z = {1, 6, 8} at 0.4/0.4/0.2, rho = 0.10 /A^3,
+d_min = 0.9 A, poly3gauss alpha = {8,8,8}, l_max = 8, rcut 5.0/4.5, trivial
+compression, central species C): get_soap with contract, then soap_contract
+with an upstream gradient G ~ N(0,1).  Inputs are seeded synthetic structures
+of those shapes (no dataset is involved).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs one process per GPU (torchrun): every rank processes its own
+structure (sites are independent; no collective on the data path), so the
+scaling is weak and the value is all ranks' sites over the slowest rank's time.
+``--impl reference`` times the reference algorithm on the host cores instead:
+the FP64 CPU restatement of soap_turbo's get_soap + soap_contract (the
+reference is Fortran and no Fortran compiler exists on these machines).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SOAP envs/s (desc+force VJP) 1×B200: mixed/adjoint vs FP64 plain at stated err"
+WORKLOAD = ("3-species Z={1,6,8} 0.4/0.4/0.2, 4096 atoms, rho=0.10/A^3, d_min=0.9 A, poly3gauss "
+            "alpha={8,8,8}, l_max=8, rcut_hard=5.0, rcut_soft=4.5, compress=trivial, central Z=6")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=2024)
+    return ap.parse_args()
+
+
+def workload(rank, seed):
+    from soap_turbo_b200 import synthetic as syn
+    return syn.config(2, seed=seed + 7919 * rank)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------- reference arm
+def cpu_reference_step_rate(w, seconds=10.0, max_steps=None, compare=None):
+    """The oracle (FP64 C restatement of get_soap + soap_contract, OpenMP over
+    all host threads) timed on the workload; returns (envs/s, threads, steps,
+    errors of `compare` against it)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    hp, nl = w.hyper, w.nl
+    W, S = compare["W"], compare["S"]
+    G = compare["G"]
+    times = []
+    t_end = time.perf_counter() + seconds
+    ref = pair = None
+    while True:
+        t0 = time.perf_counter()
+        ref = O.get_soap(hp, nl, W, S, do_derivatives=True)
+        pair = ref.contract(G, 1.0)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() > t_end or (max_steps and len(times) >= max_steps):
+            break
+    errs = {}
+    if compare.get("soap") is not None:
+        s = compare["soap"]
+        errs["soap_max_rel"] = float((np.abs(s - ref.soap).max(1) / np.abs(ref.soap).max(1)).max())
+        errs["soap_median_rel"] = float(np.median(np.abs(s - ref.soap).max(1) / np.abs(ref.soap).max(1)))
+        p = compare["pair"]
+        errs["vjp_max_rel"] = float(np.abs(p - pair).max() / np.abs(pair).max())
+    t = statistics.median(times)
+    return nl.n_sites / t, O.num_threads(), len(times), t, errs
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    w = workload(0, args.seed)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    W, S = O.basis_matrices(w.hyper)
+    G = np.random.default_rng(args.seed).standard_normal((621, w.nl.n_sites))
+    rate, cores, n, t, _ = cpu_reference_step_rate(
+        w, seconds=1e9, max_steps=max(args.warmup, 0) + max(args.steps, 1),
+        compare={"W": W, "S": S, "G": G})
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "envs/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "sites": w.nl.n_sites,
+                                         "pairs": w.nl.n_pairs},
+        "cpu_baseline": {"value": rate, "unit": "envs/s", "cores": cores, "kind": "port",
+                         "sample": f"{n} full steps of the workload ({w.nl.n_sites} sites), median"},
+        "e2e": {"value": rate, "unit": "envs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while it runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_flops(w):
+    """The reference algorithm's operation count for one step (cnk, W
+    transforms, power spectrum, H and the per-pair VJP contractions), with
+    transcendentals and recursions counted as zero; see the roofline notes."""
+    hp, nl = w.hyper, w.nl
+    K = (hp.l_max + 1) * (hp.l_max + 2) // 2
+    N = hp.n_max
+    alpha = np.asarray(hp.alpha_max)
+    mask = nl.mask.astype(bool)
+    r = nl.rjs
+    first = np.zeros(nl.n_pairs, bool)
+    first[np.concatenate([[0], np.cumsum(nl.n_neigh)[:-1]])] = True
+    cnt = np.zeros(len(alpha))
+    for s in range(len(alpha)):
+        cnt[s] = np.sum(mask[s] & (r < 5.0) & ~first)
+    F_cnk = float(np.sum(cnt * 4 * alpha * K))
+    F_W = float(np.sum(cnt * 4 * alpha ** 2))
+    F_vjp = float(np.sum(cnt * 16 * alpha * K))
+    n_keep = 69
+    F_ps = nl.n_sites * 4.0 * K * n_keep
+    F_H = nl.n_sites * 4.0 * N * N * K
+    return {"descriptor": F_cnk + F_W / 2 + F_ps, "contract": F_W / 2 + F_H + F_vjp,
+            "total": F_cnk + F_W + F_ps + F_H + F_vjp}
+
+
+def algorithmic_bytes(w):
+    """Bytes each kernel must move: per pair r, theta, phi (FP64) and the mask
+    byte per species; per site the CSR offset, the soap row (FP64) and, for the
+    contract, G (FP64), the kept c_nlm (FP32) and the pair forces out."""
+    nl, hp = w.nl, w.hyper
+    K = (hp.l_max + 1) * (hp.l_max + 2) // 2
+    per_pair_in = 24 + hp.n_species
+    n_soap = 621
+    desc = nl.n_pairs * per_pair_in + nl.n_sites * (8 + 8 * n_soap + 8 * hp.n_max * K + 8)
+    con = (nl.n_pairs * (per_pair_in + 24) +
+           nl.n_sites * (8 + 16 * n_soap + 8 * hp.n_max * K + 8))
+    return {"descriptor": float(desc), "contract": float(con)}
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return json.load(open(p)).get("hbm_gbs")
+    return 6650.0
+
+
+def fp32_peak_tflops(torch):
+    """FP32 CUDA-core peak measured here: cuBLAS SGEMM with TF32 disabled."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192
+    a = torch.randn(n, n, device="cuda")
+    b = torch.randn(n, n, device="cuda")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    return best
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    from soap_turbo_b200 import descriptor as D
+    from soap_turbo_b200 import shard
+    from soap_turbo_b200.context import Context
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    w = workload(rank, args.seed)
+    nl = w.nl
+    ctx = Context(w.hyper)
+    b = ctx.batch(nl)
+    rng = np.random.default_rng(args.seed + rank)
+    G_host = rng.standard_normal((ctx.n_soap, nl.n_sites))  # Fortran G(n_sites, n_soap)
+    G = torch.as_tensor(G_host).to(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+    stream = torch.cuda.current_stream()
+
+    def step():
+        s = ctx.descriptor(b, keep=True)
+        p = ctx.contract(b, s, G)
+        return s, p
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    launches0 = ctx.launch_count
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clk:
+        for i in range(K):
+            flush.fill_(float(i))
+            e0, e1, e2 = ev[i]
+            e0.record(stream)
+            s = ctx.descriptor(b, keep=True)
+            e1.record(stream)
+            p = ctx.contract(b, s, G)
+            e2.record(stream)
+        torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    launches = ctx.launch_count - launches0
+    t_desc = [e0.elapsed_time(e1) for e0, e1, _ in ev]
+    t_con = [e1.elapsed_time(e2) for _, e1, e2 in ev]
+    ms_step = (sum(t_desc) + sum(t_con)) / K
+    ms_step_max = shard.max_over_ranks(ms_step, device=dev)
+    value = ws * nl.n_sites / (ms_step_max * 1e-3)
+
+    # ---- plain FP64 GPU form (materialised soap_cart_der, then contracted)
+    for _ in range(2):
+        s64, cart = ctx.descriptor_fp64(b, cart=True)
+        ctx.contract_cart_der(b, cart, G)
+    torch.cuda.synchronize()
+    t64 = []
+    for _ in range(10):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s64, cart = ctx.descriptor_fp64(b, cart=True)
+        p64 = ctx.contract_cart_der(b, cart, G)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t64.append(e0.elapsed_time(e1))
+    del cart
+    ms64 = statistics.median(t64)
+
+    # ---- end to end through the drop-in host API (pinned host buffers)
+    def pinned(a, dtype, order="F"):
+        a = np.asarray(a, dtype=dtype)
+        t = torch.empty(a.size, dtype={np.float64: torch.float64, np.int32: torch.int32,
+                                       np.uint8: torch.uint8}[np.dtype(dtype).type],
+                        pin_memory=True)
+        out = t.numpy().reshape(a.shape, order=order)
+        out[...] = a
+        return out, t
+    hp = w.hyper
+    _, _, P_i, P_j, P_el = D.get_compress_indices("trivial", hp.alpha_max, hp.l_max)
+    keep = []
+    h_mask, t = pinned(nl.mask.T, np.uint8); keep.append(t)
+    h_rjs, t = pinned(nl.rjs, np.float64); keep.append(t)
+    h_th, t = pinned(nl.thetas, np.float64); keep.append(t)
+    h_ph, t = pinned(nl.phis, np.float64); keep.append(t)
+    h_nn, t = pinned(nl.n_neigh, np.int32); keep.append(t)
+    h_sp, t = pinned(nl.species.T, np.int32); keep.append(t)
+    h_sm, t = pinned(nl.species_multiplicity, np.int32); keep.append(t)
+    h_G, t = pinned(G_host.T, np.float64); keep.append(t)
+    h_soap, t = pinned(np.zeros((ctx.n_soap, nl.n_sites)), np.float64); keep.append(t)
+    h_pair, t = pinned(np.zeros((3, nl.n_pairs)), np.float64); keep.append(t)
+
+    def e2e_step():
+        D.get_soap(nl.n_sites, h_nn, hp.n_species, h_sp, h_sm, nl.n_pairs, h_mask, h_rjs, h_th, h_ph,
+                   hp.alpha_max, hp.l_max, hp.rcut_hard, hp.rcut_soft, hp.nf, hp.global_scaling,
+                   hp.atom_sigma_r, hp.atom_sigma_r_scaling, hp.atom_sigma_t,
+                   hp.atom_sigma_t_scaling, hp.amplitude_scaling, hp.radial_enhancement,
+                   hp.central_weight, hp.basis, hp.scaling_mode, False, True, True, len(P_i), P_i,
+                   P_j, P_el, h_soap, None, contract=True)
+        D.soap_contract(h_soap, h_G, 1.0, h_pair)
+    for _ in range(3):
+        e2e_step()
+    n_e2e = max(20, min(200, K // 5))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        e2e_step()
+    t_e2e = (time.perf_counter() - t0) / n_e2e
+    t_e2e = shard.max_over_ranks(t_e2e, device=dev)
+    h2d = (h_nn.nbytes + h_sp.nbytes + h_sm.nbytes + h_mask.nbytes + h_rjs.nbytes + h_th.nbytes +
+           h_ph.nbytes + h_soap.nbytes + h_G.nbytes)
+    d2h = h_soap.nbytes + h_pair.nbytes
+
+    # ---- roofline of the dominant kernel (the adjoint contract)
+    flops = algorithmic_flops(w)
+    t_con_avg = sum(t_con) / K * 1e-3
+    t_desc_avg = sum(t_desc) / K * 1e-3
+    dominant = "contract" if t_con_avg >= t_desc_avg else "descriptor"
+    t_dom = max(t_con_avg, t_desc_avg)
+    peak = fp32_peak_tflops(torch)
+    achieved = flops[dominant] / t_dom / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get("k_" + dominant)
+
+    result = None
+    if rank == 0:
+        soap_np = s.cpu().numpy()
+        pair_np = p.cpu().numpy()
+        W, S = ctx.basis()
+        cpu_rate, cores, n_cpu, t_cpu, errs = (None, None, 0, None, {})
+        if ws == 1:
+            cpu_rate, cores, n_cpu, t_cpu, errs = cpu_reference_step_rate(
+                w, seconds=10.0, compare={"W": W, "S": S, "G": G_host, "soap": soap_np,
+                                          "pair": pair_np})
+        result = {
+            "metric": METRIC, "value": value, "unit": "envs/s", "n_gpus": ws, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms_step_max, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded random periodic structures of the configuration's shape)",
+            "config": {"workload": WORKLOAD, "sites_per_gpu": nl.n_sites, "pairs_per_gpu": nl.n_pairs,
+                       "step": "get_soap(do_derivatives, contract) + soap_contract(G), G~N(0,1)",
+                       "precision": "FP32 pair/contraction arithmetic; FP64 radial integrals, "
+                                    "W transform, i_l and e^{-im phi}; FP64 accumulation of c_nlm "
+                                    "over groups of 4 pairs",
+                       "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": f"site shards, {ws} GPU(s), no data-path collective"},
+            "kernels_ms": {"descriptor": t_desc_avg * 1e3, "contract": t_con_avg * 1e3},
+            "fp64_plain": {"value": nl.n_sites * ws / (ms64 * 1e-3), "unit": "envs/s",
+                           "ms_per_step": ms64,
+                           "what": "FP64 staged like the reference: radial, angular, c_nlm, power "
+                                   "spectrum, materialised soap_cart_der, contraction with G",
+                           "speedup_of_value": value / (nl.n_sites * ws / (ms64 * 1e-3))},
+            "error_vs_fp64_oracle": errs,
+            "e2e": {"value": ws * nl.n_sites / t_e2e, "unit": "envs/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h),
+                    "path": "soapb_get_soap(contract=1) + soapb_soap_contract on pinned host arrays"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "fp32", "kernel": "k_" + dominant, "achieved": achieved,
+                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": traffic,
+                         "flops_per_launch": flops[dominant],
+                         "peak_source": "FP32 CUDA-core rate measured in this run (cuBLAS SGEMM "
+                                        "8192^3, TF32 off); MEASURED_PEAKS.json has HBM and bf16 "
+                                        "tensor peaks only",
+                         "hbm": {"algorithmic_bytes_per_launch": algorithmic_bytes(w)[dominant],
+                                 "algorithmic_GBps": algorithmic_bytes(w)[dominant] / t_dom / 1e9,
+                                 "peak_GBps": hbm_peak()}},
+            "clocks": clk.summary(),
+        }
+        if ws == 1:
+            result["cpu_baseline"] = {"value": cpu_rate, "unit": "envs/s", "cores": cores,
+                                      "kind": "port",
+                                      "sample": f"{n_cpu} full steps ({nl.n_sites} sites) of the "
+                                                f"FP64 C restatement, median {t_cpu * 1e3:.1f} ms"}
+        print(json.dumps(result), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -185,66 +185,138 @@ __device__ __forceinline__ int build_entries(const DevParams &P, const DevBatch 
 
 __device__ __forceinline__ int first_species(unsigned bits) { return __ffs(bits) - 1; }
 
-// Shared-memory layout of the kernels (bytes).  Host and device agree on it.
+// ------------------------------------------------------------ layouts
+// Shared-memory layout of the kernels (bytes); host and device agree on it.
+// Region X holds the per-round entry staging; outside the chunk loop the same
+// bytes hold other per-site arrays (c for the power spectrum; c, Gp, Gu while
+// H is built).
 struct Layout {
-  size_t W, C, H, R, E, U, P, S, red, ent, wcnt, misc, F, total;
+  size_t W, rad, kt, red, ent, wcnt, misc;
+  size_t C64, H;        // descriptor: FP64 c accumulators; contract: H
+  size_t X;             // aliased region
+  size_t R, Rd, E, U, A, F;  // staging inside X
+  size_t C, P, S;       // per-site arrays inside X (after / before the rounds)
+  size_t total;
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// entries per round = NT / 2 (one radial and one angular thread per entry)
+__host__ __device__ inline int ang_stride(int LC) {
+  return (LC + 2) * (LC + 3) / 2 + 4 * (LC + 1) + 2;  // P (to L+1), il, ild, er, ei, amp, sfac
+}
+
 __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AMAX, int LC, int mode) {
-  // mode 0: descriptor, 1: contract
   Layout L{};
   const size_t KS = (size_t)(P.k_max | 1);
-  const size_t nsp = (size_t)P.n_species;
+  const size_t nsp = (size_t)P.n_species, CH = (size_t)NT / 2;
+  const size_t nC = 2 * (size_t)P.n_max * KS;
   size_t o = 0;
-  L.W = o;   o += nsp * AMAX * AMAX * sizeof(double);
-  L.red = o; o += 40 * sizeof(double);
-  L.C = o;   o += 2 * (size_t)P.n_max * KS * sizeof(float);
-  if (mode == 1) { L.H = o; o += 2 * (size_t)P.n_max * KS * sizeof(float); }
-  if (mode == 0) {
-    L.R = o; o += (size_t)NT * AMAX * sizeof(float);
-    o = align_up(o, 8);
-    L.E = o; o += (size_t)NT * (LC + 1) * sizeof(float2);
-    L.U = o; o += (size_t)NT * KS * sizeof(float);
-  }
-  L.P = o;   o += (size_t)P.n_kept * sizeof(float);
-  L.S = o;   o += (size_t)P.n_soap * sizeof(float);
+  L.W = o;    o += nsp * AMAX * AMAX * sizeof(double);
+  L.rad = o;  o += nsp * sizeof(RadSp);
   o = align_up(o, 16);
-  L.ent = o; o += (size_t)NT * nsp * sizeof(int);
+  L.kt = o;   o += KS * 48;  // per k: int4 idx, float4 coef, l|m<<8, preflm
+  L.red = o;  o += 40 * sizeof(double);
+  L.ent = o;  o += (size_t)NT * nsp * sizeof(int);
   L.wcnt = o; o += (size_t)SOAPB_MAX_SPECIES * (NT / 32) * sizeof(int);
   L.misc = o; o += 64 * sizeof(int);
-  if (mode == 1) { L.F = o; o += (size_t)NT * nsp * 3 * sizeof(float); }
+  o = align_up(o, 16);
+  if (mode == 0) { L.C64 = o; o += nC * sizeof(double); }
+  else { L.H = o; o += nC * sizeof(float); }
+  o = align_up(o, 16);
+  L.X = o;
+  // staging
+  size_t x = o;
+  L.R = x;  x += CH * AMAX * sizeof(float);
+  if (mode == 1) { L.Rd = x; x += CH * AMAX * sizeof(float); }
+  x = align_up(x, 8);
+  if (mode == 0) {
+    L.E = x; x += CH * (LC + 1) * sizeof(float2);
+    L.U = x; x += CH * KS * sizeof(float);
+  } else {
+    L.A = x; x += CH * (size_t)ang_stride(LC) * sizeof(float);
+    L.F = x; x += (size_t)NT * nsp * 3 * sizeof(float);
+  }
+  const size_t end_stage = x;
+  // per-site arrays, aliased over the staging
+  x = o;
+  L.C = x; x += nC * sizeof(float);
+  L.P = x; x += (size_t)P.n_kept * sizeof(float);
+  L.S = x; x += (size_t)P.n_soap * sizeof(float);
+  const size_t end_site = x;
+  o = end_stage > end_site ? end_stage : end_site;
   L.total = align_up(o, 16);
   return L;
 }
 
-// Loads the species' W blocks (FP64) into shared memory, AMAX*AMAX apart.
+// Per-site prologue shared by both kernels: W blocks, species constants and
+// the per-k tables into shared memory.
 template <int NT, int AMAX>
-__device__ __forceinline__ void load_W(const DevParams &P, double *sW) {
+__device__ __forceinline__ void load_tables(const DevParams &P, double *sW, RadSp *sRad,
+                                            unsigned char *kt) {
   const int n = P.n_species * AMAX * AMAX;
   for (int t = threadIdx.x; t < n; t += NT) {
     const int s = t / (AMAX * AMAX), r = t % (AMAX * AMAX);
     const int a = P.rad[s].alpha;
     sW[t] = (r < a * a) ? P.Wblk[(size_t)s * P.wstride + r] : 0.0;
   }
+  for (int s = threadIdx.x; s < P.n_species; s += NT) sRad[s] = P.rad[s];
+  const int KS = P.k_max | 1;
+  int4 *kidx = (int4 *)kt;
+  float4 *kcoef = (float4 *)(kt + (size_t)KS * 16);
+  int *klm = (int *)(kt + (size_t)KS * 32);
+  float *kpref = (float *)(kt + (size_t)KS * 40);
+  for (int kk = threadIdx.x; kk < P.k_max; kk += NT) {
+    int l = 0;
+    while ((l + 1) * (l + 2) / 2 <= kk) ++l;
+    const int m = kk - l * (l + 1) / 2;
+    klm[kk] = l | (m << 8);
+    kpref[kk] = P.preflm[kk];
+    // sin(t) dP/dx and -m P / sin(t) from P_l^{m-1}, P_l^{m+1}, P_{l+1}^{m-1},
+    // P_{l+1}^{m+1} (src/soap_turbo_angular.f90:194-246)
+    int4 ix = make_int4(kk, kk, kk, kk);
+    float4 cf = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (m == 0) {
+      if (l > 0) {
+        ix.x = ix.y = l * (l + 1) / 2 + 1;
+        cf.x = cf.y = -0.5f;
+      }
+    } else {
+      ix.x = kk - 1;
+      cf.x = 0.5f * (float)((l + m) * (l - m + 1));
+      if (m != l) {
+        ix.y = kk + 1;
+        cf.y = -0.5f;
+      }
+      ix.z = (l + 1) * (l + 2) / 2 + m - 1;
+      cf.z = 0.5f * (float)((l - m + 1) * (l - m + 2));
+      ix.w = (l + 1) * (l + 2) / 2 + m + 1;
+      cf.w = 0.5f;
+    }
+    kidx[kk] = ix;
+    kcoef[kk] = cf;
+  }
 }
 
 // ------------------------------------------------------------ descriptor
 template <int NT, int AMAX, int LC>
-__global__ void __launch_bounds__(NT) k_descriptor(const DevParams P, const DevBatch B,
-                                                   double *__restrict__ soap_out,
-                                                   float *__restrict__ keep_c,
-                                                   double *__restrict__ keep_norm, int keep) {
+__global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const DevBatch B,
+                                                      double *__restrict__ soap_out,
+                                                      float *__restrict__ keep_c,
+                                                      double *__restrict__ keep_norm, int keep) {
   extern __shared__ __align__(16) unsigned char smem[];
+  constexpr int CH = NT / 2;
   constexpr int NPLM = (LC + 1) * (LC + 2) / 2;
+  constexpr int NH = AMAX / 2;  // radial indices per c_nlm item
   const Layout Ly = make_layout(P, NT, AMAX, LC, 0);
   double *sW = (double *)(smem + Ly.W);
+  RadSp *sRad = (RadSp *)(smem + Ly.rad);
   double *sRed = (double *)(smem + Ly.red);
-  float *sC = (float *)(smem + Ly.C);
+  double *sC64 = (double *)(smem + Ly.C64);
   float *sR = (float *)(smem + Ly.R);
   float2 *sE = (float2 *)(smem + Ly.E);
   float *sU = (float *)(smem + Ly.U);
+  float *sC = (float *)(smem + Ly.C);
   float *sP = (float *)(smem + Ly.P);
   float *sS = (float *)(smem + Ly.S);
   int *sEnt = (int *)(smem + Ly.ent);
@@ -257,8 +329,8 @@ __global__ void __launch_bounds__(NT) k_descriptor(const DevParams P, const DevB
   const int KS = P.k_max | 1;
   const int n_max = P.n_max, k_max = P.k_max, L = P.l_max;
 
-  load_W<NT, AMAX>(P, sW);
-  for (int t = tid; t < 2 * n_max * KS; t += NT) sC[t] = 0.f;
+  load_tables<NT, AMAX>(P, sW, sRad, smem + Ly.kt);
+  for (int t = tid; t < 2 * n_max * KS; t += NT) sC64[t] = 0.0;
 
   const int p_begin = B.off[site];
   const int p_end = min(B.off[site + 1], B.n_pairs);
@@ -269,70 +341,95 @@ __global__ void __launch_bounds__(NT) k_descriptor(const DevParams P, const DevB
     unsigned my_bits;
     const int n_ent = build_entries<NT>(P, B, p_begin, chunk, p_end, false, sEnt, sW_cnt, sBase,
                                         sCnt, sNent, slot, my_bits);
-    for (int ebase = 0; ebase < n_ent; ebase += NT) {
-      // ---- A. per-entry expansions
-      const int e = ebase + tid;
-      if (e < n_ent) {
-        const int pl = sEnt[e] & 0xffffff, s = sEnt[e] >> 24;
-        const int k = chunk + pl;
-        const double r = B.rjs[k];
-        double val[AMAX], der[AMAX];
-        radial_entry<AMAX>(P, P.rad[s], sW + s * AMAX * AMAX, r, k == p_begin, false, val, der);
-        const float g4 = (float)(kFourPi * P.rad[s].gscale);
-        float *Re = sR + (size_t)(e - ebase) * AMAX;
+    for (int ebase = 0; ebase < n_ent; ebase += CH) {
+      const int n_round = min(CH, n_ent - ebase);
+      // ---- A. expansions: threads [0, CH) radial (FP64), [CH, NT) angular
+      if (tid < CH) {
+        const int el = tid;
+        if (el < n_round) {
+          const int code = sEnt[ebase + el];
+          const int pl = code & 0xffffff, s = code >> 24;
+          const int k = chunk + pl;
+          double val[AMAX], der[AMAX];
+          radial_entry<AMAX>(P, sRad[s], sW + s * AMAX * AMAX, B.rjs[k], k == p_begin, false,
+                             val, der);
+          const double g4 = kFourPi * sRad[s].gscale;
+          float *Re = sR + (size_t)el * AMAX;
 #pragma unroll
-        for (int n = 0; n < AMAX; ++n) Re[n] = g4 * (float)val[n];
-        AngScalars<LC> A;
-        angular_scalars<LC>(P, first_species(B.bits[k]), r, B.thetas[k], B.phis[k], false, A);
-        float plm[NPLM];
-        plm_array<LC, float>(L, (float)A.x, (float)A.sq, plm);
-        float2 *Ee = sE + (size_t)(e - ebase) * (LC + 1);
+          for (int n = 0; n < AMAX; ++n) Re[n] = (float)(g4 * val[n]);
+        }
+      } else {
+        const int el = tid - CH;
+        if (el < n_round) {
+          const int pl = sEnt[ebase + el] & 0xffffff;
+          const int k = chunk + pl;
+          AngScalars<LC> A;
+          angular_scalars<LC>(P, first_species(B.bits[k]), B.rjs[k], B.thetas[k], B.phis[k],
+                              false, A);
+          float plm[NPLM];
+          plm_array<LC, float>(L, (float)A.x, (float)A.sq, plm);
+          float2 *Ee = sE + (size_t)el * (LC + 1);
 #pragma unroll
-        for (int m = 0; m <= LC; ++m) Ee[m] = make_float2((float)A.er[m], (float)A.ei[m]);
-        float *Ue = sU + (size_t)(e - ebase) * KS;
-        const float ampf = (float)A.amp;
+          for (int m = 0; m <= LC; ++m) Ee[m] = make_float2((float)A.er[m], (float)A.ei[m]);
+          float *Ue = sU + (size_t)el * KS;
+          const float ampf = (float)A.amp;
 #pragma unroll
-        for (int l = 0; l <= LC; ++l) {
-          if (l > L) break;
-          const float il = (float)A.il[l];
+          for (int l = 0; l <= LC; ++l) {
+            if (l > L) break;
+            const float il = (float)A.il[l];
 #pragma unroll
-          for (int m = 0; m <= l; ++m) {
-            const int kk = l * (l + 1) / 2 + m;
-            Ue[kk] = ampf * P.preflm[kk] * plm[kk] * il;
+            for (int m = 0; m <= l; ++m) {
+              const int kk = l * (l + 1) / 2 + m;
+              Ue[kk] = ampf * P.preflm[kk] * plm[kk] * il;
+            }
           }
         }
       }
       __syncthreads();
-      // ---- B. c_nlm, fixed-order sum over each species' entries
-      const int e_hi = min(ebase + NT, n_ent);
-      for (int it = tid; it < P.n_species * k_max; it += NT) {
-        const int s = it / k_max, kk = it - s * k_max;
+      // ---- B. c_nlm: item = (species, k, half of the species' radial block);
+      // FP32 partial sums over groups of 4 entries, flushed into FP64
+      const int e_hi = ebase + n_round;
+      for (int it = tid; it < P.n_species * k_max * 2; it += NT) {
+        const int s = it / (2 * k_max), rem = it - s * 2 * k_max;
+        const int kk = rem >> 1, half = rem & 1;
+        const int lo = max(sBase[s], ebase), hi = min(sBase[s] + sCnt[s], e_hi);
+        if (lo >= hi) continue;
+        const int nb = sRad[s].nbeg, a = sRad[s].alpha, n0 = half * NH;
+        if (n0 >= a) continue;
         int l = 0;
         while ((l + 1) * (l + 2) / 2 <= kk) ++l;
         const int m = kk - l * (l + 1) / 2;
-        const int lo = max(sBase[s], ebase), hi = min(sBase[s] + sCnt[s], e_hi);
-        if (lo >= hi) continue;
-        float accr[AMAX], acci[AMAX];
+        double dr[NH], di[NH];
+        float pr[NH], pi[NH];
 #pragma unroll
-        for (int n = 0; n < AMAX; ++n) accr[n] = acci[n] = 0.f;
+        for (int n = 0; n < NH; ++n) dr[n] = di[n] = 0.0, pr[n] = pi[n] = 0.f;
+        int cnt = 0;
         for (int e2 = lo; e2 < hi; ++e2) {
           const int el = e2 - ebase;
           const float u = sU[(size_t)el * KS + kk];
           const float2 E = sE[(size_t)el * (LC + 1) + m];
           const float ar = u * E.x, ai = u * E.y;
-          const float *Re = sR + (size_t)el * AMAX;
+          const float *Re = sR + (size_t)el * AMAX + n0;
 #pragma unroll
-          for (int n = 0; n < AMAX; ++n) {
-            accr[n] = fmaf(Re[n], ar, accr[n]);
-            acci[n] = fmaf(Re[n], ai, acci[n]);
+          for (int n = 0; n < NH; ++n) {
+            pr[n] = fmaf(Re[n], ar, pr[n]);
+            pi[n] = fmaf(Re[n], ai, pi[n]);
+          }
+          if (++cnt == 4) {
+            cnt = 0;
+#pragma unroll
+            for (int n = 0; n < NH; ++n) {
+              dr[n] += (double)pr[n];
+              di[n] += (double)pi[n];
+              pr[n] = pi[n] = 0.f;
+            }
           }
         }
-        const int nb = P.rad[s].nbeg, a = P.rad[s].alpha;
 #pragma unroll
-        for (int n = 0; n < AMAX; ++n) {
-          if (n < a) {
-            sC[(size_t)(nb + n) * KS + kk] += accr[n];
-            sC[(size_t)(n_max + nb + n) * KS + kk] += acci[n];
+        for (int n = 0; n < NH; ++n) {
+          if (n0 + n < a) {
+            sC64[(size_t)(nb + n0 + n) * KS + kk] += dr[n] + (double)pr[n];
+            sC64[(size_t)(n_max + nb + n0 + n) * KS + kk] += di[n] + (double)pi[n];
           }
         }
       }
@@ -346,10 +443,12 @@ __global__ void __launch_bounds__(NT) k_descriptor(const DevParams P, const DevB
     for (int mm = 0; mm < mult; ++mm) {
       const int s = B.species[(size_t)site * B.max_mult + mm] - 1;
       if (s < 0 || s >= P.n_species) continue;
-      const int nb = P.rad[s].nbeg, a = P.rad[s].alpha;
-      for (int n = 0; n < a; ++n) sC[(size_t)(nb + n) * KS] += (float)P.central[nb + n];
+      const int nb = sRad[s].nbeg, a = sRad[s].alpha;
+      for (int n = 0; n < a; ++n) sC64[(size_t)(nb + n) * KS] += P.central[nb + n];
     }
   }
+  __syncthreads();
+  for (int t = tid; t < 2 * n_max * KS; t += NT) sC[t] = (float)sC64[t];
   __syncthreads();
 
   // ---- C. power spectrum of the kept components (src/soap_turbo.f90:750-795)
@@ -359,7 +458,7 @@ __global__ void __launch_bounds__(NT) k_descriptor(const DevParams P, const DevB
     const int kb = l * (l + 1) / 2;
     const float *cn_r = sC + (size_t)n * KS + kb, *cn_i = sC + (size_t)(n_max + n) * KS + kb;
     const float *cp_r = sC + (size_t)np * KS + kb, *cp_i = sC + (size_t)(n_max + np) * KS + kb;
-    float acc0 = cn_r[0] * cp_r[0] + cn_i[0] * cp_i[0];
+    const float acc0 = cn_r[0] * cp_r[0] + cn_i[0] * cp_i[0];
     float acc = 0.f;
     for (int m = 1; m <= l; ++m) acc += cn_r[m] * cp_r[m] + cn_i[m] * cp_i[m];
     const float base = (n == np) ? 1.f : 1.41421356237309504880f;
@@ -392,34 +491,47 @@ __global__ void __launch_bounds__(NT) k_descriptor(const DevParams P, const DevB
 
 // ------------------------------------------------------------ contract
 template <int NT, int AMAX, int LC>
-__global__ void __launch_bounds__(NT) k_contract(const DevParams P, const DevBatch B,
-                                                 const double *__restrict__ soap_in,
-                                                 const double *__restrict__ G, int g_layout,
-                                                 double sgn, const float *__restrict__ keep_c,
-                                                 const double *__restrict__ keep_norm,
-                                                 double *__restrict__ pair_out) {
+__global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const DevBatch B,
+                                                    const double *__restrict__ soap_in,
+                                                    const double *__restrict__ G, int g_layout,
+                                                    double sgn, const float *__restrict__ keep_c,
+                                                    const double *__restrict__ keep_norm,
+                                                    double *__restrict__ pair_out) {
   extern __shared__ __align__(16) unsigned char smem[];
-  constexpr int NPLM = (LC + 2) * (LC + 3) / 2;
+  constexpr int CH = NT / 2;
+  constexpr int NPLM1 = (LC + 2) * (LC + 3) / 2;
+  constexpr int AS = (LC + 2) * (LC + 3) / 2 + 4 * (LC + 1) + 2;
+  constexpr int O_IL = NPLM1, O_ILD = NPLM1 + (LC + 1), O_ER = NPLM1 + 2 * (LC + 1),
+                O_EI = NPLM1 + 3 * (LC + 1), O_AMP = NPLM1 + 4 * (LC + 1), O_SF = O_AMP + 1;
   const Layout Ly = make_layout(P, NT, AMAX, LC, 1);
   double *sW = (double *)(smem + Ly.W);
+  RadSp *sRad = (RadSp *)(smem + Ly.rad);
   double *sRed = (double *)(smem + Ly.red);
-  float *sC = (float *)(smem + Ly.C);
   float *sH = (float *)(smem + Ly.H);
+  float *sC = (float *)(smem + Ly.C);
   float *sGu = (float *)(smem + Ly.P);
   float *sGp = (float *)(smem + Ly.S);
+  float *sR = (float *)(smem + Ly.R);
+  float *sRd = (float *)(smem + Ly.Rd);
+  float *sA = (float *)(smem + Ly.A);
+  float *sF = (float *)(smem + Ly.F);
   int *sEnt = (int *)(smem + Ly.ent);
   int *sW_cnt = (int *)(smem + Ly.wcnt);
   int *sMisc = (int *)(smem + Ly.misc);
-  float *sF = (float *)(smem + Ly.F);
   int *sBase = sMisc, *sCnt = sMisc + SOAPB_MAX_SPECIES, *sNent = sMisc + 2 * SOAPB_MAX_SPECIES;
+  unsigned char *kt = smem + Ly.kt;
 
   const int tid = threadIdx.x;
   const int site = blockIdx.x;
   const int KS = P.k_max | 1;
   const int n_max = P.n_max, k_max = P.k_max, L = P.l_max, n_soap = P.n_soap;
   const int n_sites = B.n_sites;
+  const int4 *kidx = (const int4 *)kt;
+  const float4 *kcoef = (const float4 *)(kt + (size_t)KS * 16);
+  const int *klm = (const int *)(kt + (size_t)KS * 32);
+  const float *kpref = (const float *)(kt + (size_t)KS * 40);
 
-  load_W<NT, AMAX>(P, sW);
+  load_tables<NT, AMAX>(P, sW, sRad, smem + Ly.kt);
   {
     const float *kc = keep_c + (size_t)site * 2 * n_max * k_max;
     for (int t = tid; t < 2 * n_max * k_max; t += NT) {
@@ -429,14 +541,15 @@ __global__ void __launch_bounds__(NT) k_contract(const DevParams P, const DevBat
   }
   // ---- back through the normalisation (src/soap_turbo.f90:1783-1790)
   const double *q = soap_in + (size_t)site * n_soap;
-  auto g_at = [&](int o) -> double {
-    return g_layout == 0 ? G[(size_t)o * n_sites + site] : G[(size_t)site * n_soap + o];
-  };
   double qg = 0.0;
-  for (int o = tid; o < n_soap; o += NT) qg += q[o] * g_at(o);
+  for (int o = tid; o < n_soap; o += NT)
+    qg += q[o] * (g_layout == 0 ? G[(size_t)o * n_sites + site] : G[(size_t)site * n_soap + o]);
   qg = block_sum<NT>(qg, sRed);
   const double inv = 1.0 / keep_norm[site];
-  for (int o = tid; o < n_soap; o += NT) sGp[o] = (float)((g_at(o) - q[o] * qg) * inv);
+  for (int o = tid; o < n_soap; o += NT) {
+    const double g = g_layout == 0 ? G[(size_t)o * n_sites + site] : G[(size_t)site * n_soap + o];
+    sGp[o] = (float)((g - q[o] * qg) * inv);
+  }
   __syncthreads();
   // ---- back through the compression (:1791-1798), on the kept components
   for (int t = tid; t < P.n_kept; t += NT) {
@@ -448,9 +561,7 @@ __global__ void __launch_bounds__(NT) k_contract(const DevParams P, const DevBat
   // ---- H(k,n) = w(m) sum_np Y(n,np,l) c(k,np) over the non-zero Y (:1800-1835)
   for (int it = tid; it < n_max * k_max; it += NT) {
     const int n = it / k_max, kk = it - n * k_max;
-    int l = 0;
-    while ((l + 1) * (l + 2) / 2 <= kk) ++l;
-    const int m = kk - l * (l + 1) / 2;
+    const int lm = klm[kk], l = lm & 0xff, m = lm >> 8;
     float hr = 0.f, hi = 0.f;
     const int li = l * n_max + n;
     for (int t = P.hl_off[li]; t < P.hl_off[li + 1]; ++t) {
@@ -468,82 +579,120 @@ __global__ void __launch_bounds__(NT) k_contract(const DevParams P, const DevBat
   const int p_begin = B.off[site];
   const int p_end = min(B.off[site + 1], B.n_pairs);
   double self_x = 0.0, self_y = 0.0, self_z = 0.0;
+  const int hw = tid >> 4, hl = tid & 15;
 
   for (int chunk = p_begin; chunk < p_end; chunk += NT) {
     int slot[SOAPB_MAX_SPECIES];
     unsigned my_bits;
     const int n_ent = build_entries<NT>(P, B, p_begin, chunk, p_end, true, sEnt, sW_cnt, sBase,
                                         sCnt, sNent, slot, my_bits);
-    // ---- per entry: expansions and their derivatives, contracted against H
-    for (int e = tid; e < n_ent; e += NT) {
-      const int pl = sEnt[e] & 0xffffff, s = sEnt[e] >> 24;
-      const int k = chunk + pl;
-      const double r = B.rjs[k];
-      double val[AMAX], der[AMAX];
-      radial_entry<AMAX>(P, P.rad[s], sW + s * AMAX * AMAX, r, false, true, val, der);
-      const double g4 = kFourPi * P.rad[s].gscale;
-      float R[AMAX], Rd[AMAX];
-#pragma unroll
-      for (int n = 0; n < AMAX; ++n) {
-        R[n] = (float)(g4 * val[n]);
-        Rd[n] = (float)(g4 * der[n]);
-      }
-      AngScalars<LC> A;
-      angular_scalars<LC>(P, first_species(B.bits[k]), r, B.thetas[k], B.phis[k], true, A);
-      float plm[NPLM];
-      plm_array<LC + 1, float>(L + 1, (float)A.x, (float)A.sq, plm);
-      const float ampf = (float)A.amp, sfac = (float)A.sig_fac;
-      const int nb = P.rad[s].nbeg, a = P.rad[s].alpha;
-      const float *Hr = sH + (size_t)nb * KS, *Hi = sH + (size_t)(n_max + nb) * KS;
-      float f_rad = 0.f, f_azi = 0.f, f_pol = 0.f;
-#pragma unroll
-      for (int l = 0; l <= LC; ++l) {
-        if (l > L) break;
-        const float il = (float)A.il[l], ild = (float)A.ild[l];
-#pragma unroll
-        for (int m = 0; m <= l; ++m) {
-          const int kk = l * (l + 1) / 2 + m;
-          const float ap = ampf * P.preflm[kk];
-          // sin(t) dP/dx and -m P/sin(t), pole-safe forms (src/soap_turbo_angular.f90:194-246)
-          float dms, dvs;
-          if (m == 0) {
-            dms = (l == 0) ? 0.f : -0.5f * plm[l * (l + 1) / 2 + 1];
-            dvs = 0.f;
-          } else {
-            dms = 0.5f * (float)((l + m) * (l - m + 1)) * plm[kk - 1];
-            dvs = 0.5f * (float)((l - m + 1) * (l - m + 2)) * plm[(l + 1) * (l + 2) / 2 + m - 1] +
-                  0.5f * plm[(l + 1) * (l + 2) / 2 + m + 1];
-          }
-          if (m != l) dms += -0.5f * plm[kk + 1];
-          const float u = ap * plm[kk] * il;
-          const float ur = ap * plm[kk] * ild - sfac * u;
-          const float ua = ap * dvs * il;
-          const float up = ap * dms * il;
-          float Ur = 0.f, Ui = 0.f, Vr = 0.f, Vi = 0.f;
+    for (int ebase = 0; ebase < n_ent; ebase += CH) {
+      const int n_round = min(CH, n_ent - ebase);
+      // ---- A. expansions and derivatives: [0, CH) radial, [CH, NT) angular
+      if (tid < CH) {
+        const int el = tid;
+        if (el < n_round) {
+          const int code = sEnt[ebase + el];
+          const int pl = code & 0xffffff, s = code >> 24;
+          const int k = chunk + pl;
+          double val[AMAX], der[AMAX];
+          radial_entry<AMAX>(P, sRad[s], sW + s * AMAX * AMAX, B.rjs[k], false, true, val, der);
+          const double g4 = kFourPi * sRad[s].gscale;
+          float *Re = sR + (size_t)el * AMAX, *Rde = sRd + (size_t)el * AMAX;
 #pragma unroll
           for (int n = 0; n < AMAX; ++n) {
-            if (n < a) {
-              const float hr = Hr[(size_t)n * KS + kk], hi = Hi[(size_t)n * KS + kk];
-              Ur = fmaf(Rd[n], hr, Ur);
-              Ui = fmaf(Rd[n], hi, Ui);
-              Vr = fmaf(R[n], hr, Vr);
-              Vi = fmaf(R[n], hi, Vi);
-            }
+            Re[n] = (float)(g4 * val[n]);
+            Rde[n] = (float)(g4 * der[n]);
           }
-          const float er = (float)A.er[m], ei = (float)A.ei[m];
-          const float reU = er * Ur + ei * Ui;
-          const float reV = er * Vr + ei * Vi;
-          const float imV = ei * Vr - er * Vi;
-          f_rad = fmaf(u, reU, fmaf(ur, reV, f_rad));
-          f_azi = fmaf(-ua, imV, f_azi);
-          f_pol = fmaf(up, reV, f_pol);
+        }
+      } else {
+        const int el = tid - CH;
+        if (el < n_round) {
+          const int pl = sEnt[ebase + el] & 0xffffff;
+          const int k = chunk + pl;
+          AngScalars<LC> A;
+          angular_scalars<LC>(P, first_species(B.bits[k]), B.rjs[k], B.thetas[k], B.phis[k], true,
+                              A);
+          float *Ae = sA + (size_t)el * AS;
+#pragma unroll
+          for (int l = 0; l <= LC; ++l) {
+            Ae[O_IL + l] = (float)A.il[l];
+            Ae[O_ILD + l] = (float)A.ild[l];
+            Ae[O_ER + l] = (float)A.er[l];
+            Ae[O_EI + l] = (float)A.ei[l];
+          }
+          Ae[O_AMP] = (float)A.amp;
+          Ae[O_SF] = (float)A.sig_fac;
+          const float xf = (float)A.x, sqf = (float)A.sq;
+          float plm[NPLM1];
+          plm_array<LC + 1, float>(L + 1, xf, sqf, plm);
+#pragma unroll
+          for (int t = 0; t < NPLM1; ++t) Ae[t] = plm[t];
         }
       }
-      sF[3 * e + 0] = f_rad;
-      sF[3 * e + 1] = f_azi;
-      sF[3 * e + 2] = f_pol;
+      __syncthreads();
+      // ---- B. contraction against H: a half-warp per entry, lanes over k.
+      // The loop bound is uniform per warp (both halves iterate together) so
+      // the full-mask shuffles below always see all 32 lanes.
+      for (int eb = 2 * (tid >> 5); eb < n_round; eb += NT / 16) {
+        const int el = eb + (hw & 1);
+        const bool act = el < n_round;
+        float f_rad = 0.f, f_azi = 0.f, f_pol = 0.f;
+        if (act) {
+          const int s = sEnt[ebase + el] >> 24;
+          const int nb = sRad[s].nbeg, a = sRad[s].alpha;
+          const float *Ae = sA + (size_t)el * AS;
+          const float *Re = sR + (size_t)el * AMAX, *Rde = sRd + (size_t)el * AMAX;
+          const float *Hr = sH + (size_t)nb * KS, *Hi = sH + (size_t)(n_max + nb) * KS;
+          const float amp = Ae[O_AMP], sfac = Ae[O_SF];
+          for (int kk = hl; kk < k_max; kk += 16) {
+            const int lm = klm[kk], l = lm & 0xff, m = lm >> 8;
+            const int4 ix = kidx[kk];
+            const float4 cf = kcoef[kk];
+            const float Pk = Ae[kk];
+            const float dms = cf.x * Ae[ix.x] + cf.y * Ae[ix.y];
+            const float dvs = cf.z * Ae[ix.z] + cf.w * Ae[ix.w];
+            const float il = Ae[O_IL + l], ild = Ae[O_ILD + l];
+            const float er = Ae[O_ER + m], ei = Ae[O_EI + m];
+            const float ap = amp * kpref[kk];
+            const float u = ap * Pk * il;
+            const float ur = ap * Pk * ild - sfac * u;
+            const float ua = ap * dvs * il;
+            const float up = ap * dms * il;
+            float Ur = 0.f, Ui = 0.f, Vr = 0.f, Vi = 0.f;
+#pragma unroll
+            for (int n = 0; n < AMAX; ++n) {
+              if (n < a) {
+                const float hr = Hr[(size_t)n * KS + kk], hi = Hi[(size_t)n * KS + kk];
+                Ur = fmaf(Rde[n], hr, Ur);
+                Ui = fmaf(Rde[n], hi, Ui);
+                Vr = fmaf(Re[n], hr, Vr);
+                Vi = fmaf(Re[n], hi, Vi);
+              }
+            }
+            const float reU = er * Ur + ei * Ui;
+            const float reV = er * Vr + ei * Vi;
+            const float imV = ei * Vr - er * Vi;
+            f_rad = fmaf(u, reU, fmaf(ur, reV, f_rad));
+            f_azi = fmaf(-ua, imV, f_azi);
+            f_pol = fmaf(up, reV, f_pol);
+          }
+        }
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) {
+          f_rad += __shfl_xor_sync(0xffffffffu, f_rad, o);
+          f_azi += __shfl_xor_sync(0xffffffffu, f_azi, o);
+          f_pol += __shfl_xor_sync(0xffffffffu, f_pol, o);
+        }
+        if (act && hl == 0) {
+          float *Fe = sF + (size_t)(ebase + el) * 3;
+          Fe[0] = f_rad;
+          Fe[1] = f_azi;
+          Fe[2] = f_pol;
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
     // ---- per pair: sum its entries, rotate to Cartesian (:1864-1875)
     const int k = chunk + tid;
     double px = 0.0, py = 0.0, pz = 0.0;
@@ -620,15 +769,11 @@ cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-#define SOAPB_DISPATCH(FN, ...)                                                    \
-  do {                                                                             \
-    const int am = max_alpha(P);                                                   \
-    const int nt = cfg.threads;                                                    \
-    if (am <= 8 && P.l_max <= 8) {                                                 \
-      if (nt == 64) return FN<64, 8, 8>(__VA_ARGS__);                              \
-      return FN<128, 8, 8>(__VA_ARGS__);                                           \
-    }                                                                              \
-    return FN<128, 16, 12>(__VA_ARGS__);                                           \
+#define SOAPB_DISPATCH(FN, ...)                          \
+  do {                                                   \
+    if (max_alpha(P) <= 8 && P.l_max <= 8)               \
+      return FN<128, 8, 8>(__VA_ARGS__);                 \
+    return FN<128, 16, 12>(__VA_ARGS__);                 \
   } while (0)
 
 cudaError_t launch_descriptor(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
@@ -642,13 +787,13 @@ cudaError_t launch_contract(const DevParams &P, const DevBatch &B, const LaunchC
   SOAPB_DISPATCH(run_contract, P, B, cfg.stream, soap, G, g_layout, sgn, keep_c, keep_norm, pair);
 }
 
-size_t descriptor_smem(const DevParams &P, int threads) {
+size_t descriptor_smem(const DevParams &P, int) {
   const bool small = max_alpha(P) <= 8 && P.l_max <= 8;
-  return make_layout(P, small ? threads : 128, small ? 8 : 16, small ? 8 : 12, 0).total;
+  return make_layout(P, 128, small ? 8 : 16, small ? 8 : 12, 0).total;
 }
-size_t contract_smem(const DevParams &P, int threads) {
+size_t contract_smem(const DevParams &P, int) {
   const bool small = max_alpha(P) <= 8 && P.l_max <= 8;
-  return make_layout(P, small ? threads : 128, small ? 8 : 16, small ? 8 : 12, 1).total;
+  return make_layout(P, 128, small ? 8 : 16, small ? 8 : 12, 1).total;
 }
 
 }  // namespace soapb

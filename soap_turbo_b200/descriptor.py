@@ -54,7 +54,7 @@ def get_soap(n_sites, n_neigh, n_species, species, species_multiplicity, n_atom_
     species = _f(species, _i32)
     if species.ndim == 1:
         species = species.reshape(1, -1, order="F")
-    mask_u8 = _f(np.asarray(mask).astype(np.uint8), np.uint8)
+    mask_u8 = _f(mask, np.uint8)  # no copy when already uint8 and Fortran-ordered
     n_neigh = np.ascontiguousarray(n_neigh, dtype=_i32)
     species_multiplicity = np.ascontiguousarray(species_multiplicity, dtype=_i32)
     rjs = np.ascontiguousarray(rjs, dtype=_f64)

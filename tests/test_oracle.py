@@ -1,0 +1,268 @@
+"""The FP64 CPU oracle, pinned against the reference's own known answers.
+
+The reference ships no tests or fixtures; what it does ship is the poly3tab
+W/S tables (src/soap_turbo_radial.f90:1247-1528, extracted to
+tests/golden/poly3tab.json by tests/golden/make_golden.py), its scalar
+reference functions (plm_double, ilexp_double), and documented identities
+(soap_contract == soap_cart_der . G, the self column, unit norm, the
+finite-difference consistency of the unified filter seed).  These tests pin
+the oracle to all of them, plus independent special-function values from
+scipy.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+import scipy.special as sp
+
+import oracle as O
+from conftest import ROOT
+from soap_turbo_b200 import synthetic as syn
+
+GOLDEN = json.load(open(os.path.join(ROOT, "tests", "golden", "poly3tab.json")))["tables"]
+
+
+def table(a, name):
+    return np.array(GOLDEN[str(a)][name]).reshape(a, a, order="F")
+
+
+@pytest.mark.parametrize("a", range(1, 12))
+def test_poly3_overlap_matches_reference_table(a):
+    # S is closed-form: the oracle must reproduce the reference's table exactly
+    np.testing.assert_array_equal(O.overlap("poly3", a), table(a, "S"))
+
+
+@pytest.mark.parametrize("a", range(1, 9))
+def test_poly3_W_matches_reference_table(a):
+    # The reference's own W table was produced by FP64 LAPACK; at alpha = 8
+    # the FP64 construction itself is only good to ~1e-5 (cond(S) ~ 1e13).
+    W = O.inverse_sqrt(table(a, "S"))
+    ref = table(a, "W")
+    assert np.abs(W - ref).max() / np.abs(ref).max() < 2.0e-5
+
+
+@pytest.mark.parametrize("a", range(9, 12))
+def test_poly3_W_large_alpha_is_ill_conditioned_like_the_reference_says(a):
+    # README.md:66-76: unstable above 7 and catastrophically so by 12; the
+    # tables and an extended-precision W still agree to a few percent.
+    W = O.inverse_sqrt(table(a, "S"))
+    ref = table(a, "W")
+    assert np.abs(W - ref).max() / np.abs(ref).max() < 5.0e-2
+
+
+@pytest.mark.parametrize("a", [2, 5, 8, 11])
+def test_poly3gauss_overlap_is_spd_and_W_inverts_it(a):
+    S = O.overlap("poly3gauss", a, 0.5, 5.0)
+    assert np.allclose(S, S.T, atol=0)
+    assert np.all(np.diag(S) == 1.0)
+    W = O.inverse_sqrt(S)
+    assert np.allclose(W, W.T, rtol=0, atol=1e-9 * np.abs(W).max())
+    assert np.all(np.linalg.eigvalsh(S) > 0)
+
+
+def _wsw_error(W, S):
+    Wl = W.astype(np.longdouble)
+    Sl = S.astype(np.longdouble)
+    return float(np.abs(Wl @ Sl @ Wl - np.eye(W.shape[0], dtype=np.longdouble)).max())
+
+
+@pytest.mark.parametrize("basis,a", [("poly3", 4), ("poly3", 8), ("poly3gauss", 4), ("poly3gauss", 8)])
+def test_W_is_inverse_sqrt(basis, a):
+    S = O.overlap(basis, a, 0.5, 5.0)
+    W = O.inverse_sqrt(S)
+    assert _wsw_error(W, S) < 5.0e-6
+
+
+def test_poly3gauss_overlap_against_quadrature():
+    # S(alpha, gauss) = int_0^1 g_alpha(r) phi(r) r^2 dr with the primitive
+    # g_alpha(r) = (1-r)^(alpha+2) / N_alpha, N_alpha = sqrt(1/(2 alpha + 5))
+    # (src/soap_turbo_radial.f90:82-96) and phi the normalised origin Gaussian
+    # sqrt(2/sigma)/pi^(1/4) exp(-r^2/(2 sigma^2)) (:468), in units of rcut.
+    a, sig_in, rc = 6, 0.5, 5.0
+    sig = sig_in / rc
+    S = O.overlap("poly3gauss", a, sig_in, rc)
+    x, w = np.polynomial.legendre.leggauss(200)
+    r = 0.5 * (x + 1.0)
+    w = 0.5 * w
+    phi = math.sqrt(2.0 / sig) / math.pi ** 0.25 * np.exp(-r * r / (2 * sig * sig))
+    for al in range(1, a):
+        g = (1.0 - r) ** (al + 2) / math.sqrt(1.0 / (2 * al + 5))
+        # the poly3 overlaps S_ij = sqrt((5+2i)(5+2j))/(5+i+j) are integrals
+        # with the plain measure dr, and so are the Gaussian ones
+        val = np.sum(w * g * phi)
+        assert abs(val - S[al - 1, a - 1]) < 1e-10 * max(1.0, abs(val)), al
+
+
+def test_preflm_closed_form():
+    pf = O.preflm(8)
+    k = 0
+    for l in range(9):
+        for m in range(l + 1):
+            ref = math.sqrt((2 * l + 1) / (4 * math.pi) * math.factorial(l - m) / math.factorial(l + m))
+            assert abs(pf[k] - ref) < 1e-15 * ref
+            k += 1
+
+
+@pytest.mark.parametrize("x", [-1.0, -0.73, -0.2, 0.0, 0.31, 0.999, 1.0])
+def test_plm_array_matches_scalar_reference_and_scipy(x):
+    lmax = 9
+    arr = O.plm_array(lmax, x)
+    k = 0
+    for l in range(lmax + 1):
+        for m in range(l + 1):
+            scal = O.plm_double(l, m, x)
+            ref = sp.lpmv(m, l, x)  # includes the Condon-Shortley phase
+            tol = 1e-12 * max(1.0, abs(ref))
+            assert abs(arr[k] - scal) < tol
+            assert abs(arr[k] - ref) < 1e-10 * max(1.0, abs(ref))
+            k += 1
+
+
+@pytest.mark.parametrize("x", [0.0, 1e-9, 1e-3, 0.05, 0.4, 1.0, 2.7, 6.0, 10.0])
+def test_ilexp_array_matches_scalar_reference(x):
+    arr = O.ilexp_array(8, x)
+    for l in range(9):
+        # the two reference formulations divide vs multiply by 1/x^2; the upward
+        # recursion amplifies that ulp by prod (2l-1)/x^2 at small x (1.5e-13 at
+        # x = 0.4, l = 4), so compare with an absolute floor
+        assert abs(arr[l] - O.ilexp_double(l, x)) <= 1e-12 * abs(arr[l]) + 1e-12
+
+
+@pytest.mark.parametrize("x", [2.2, 3.0, 5.0, 8.0])
+def test_ilexp_against_scipy(x):
+    # i_l(x^2) exp(-x^2) with i_l the modified spherical Bessel function
+    arr = O.ilexp_array(8, x)
+    for l in range(9):
+        ref = sp.spherical_in(l, x * x) * math.exp(-x * x)
+        assert abs(arr[l] - ref) < 1e-9 * ref + 1e-15
+
+
+def test_ilexp_reference_recursion_loses_accuracy_at_small_x():
+    # The reference's upward recursion (src/soap_turbo_angular.f90:407-419)
+    # amplifies rounding by prod (2l-1)/x^2: at x = 1 (r = sigma_t) and l = 8 it
+    # is off the true value by ~2.5e-3 even in FP64.  Parity is with the
+    # reference's algorithm, so the oracle and the GPU kernels both keep it.
+    x = 1.0
+    arr = O.ilexp_array(8, x)
+    ref = sp.spherical_in(8, x * x) * math.exp(-x * x)
+    assert 1e-4 < abs(arr[8] - ref) / ref < 1e-2
+
+
+def test_trivial_compression_indices():
+    for am, L in [([8, 8, 8], 8), ([8], 8), ([4, 6], 3), ([3, 3, 3, 3], 5)]:
+        P_i, P_j, P_el = O.compress_trivial(am, L)
+        Q_i, Q_j, Q_el = syn.trivial_compress_indices(am, L)
+        np.testing.assert_array_equal(P_i, Q_i)
+        np.testing.assert_array_equal(P_j, Q_j)
+        np.testing.assert_array_equal(P_el, Q_el)
+    assert O.compress_trivial([8, 8, 8], 8)[0].shape[0] == 621
+
+
+@pytest.fixture(scope="module")
+def cfg1():
+    w = syn.config(1, seed=7)
+    W, S = O.basis_matrices(w.hyper)
+    return w, W, S
+
+
+def test_oracle_identities(cfg1):
+    w, W, S = cfg1
+    nl = w.nl
+    r = O.get_soap(w.hyper, nl, W, S, do_derivatives=True, cart_der=True)
+    # unit norm (src/soap_turbo.f90:904-909)
+    np.testing.assert_allclose(np.linalg.norm(r.soap, axis=1), 1.0, atol=1e-14)
+    # self column = -sum of the others (:888-892)
+    off = np.concatenate([[0], np.cumsum(nl.n_neigh)])
+    for i in range(nl.n_sites):
+        c = r.soap_cart_der
+        assert np.abs(c[off[i]] + c[off[i] + 1:off[i + 1]].sum(0)).max() < 1e-13
+    # soap_contract == soap_cart_der . G (:1721)
+    rng = np.random.default_rng(1)
+    G = rng.standard_normal((r.soap.shape[1], nl.n_sites))
+    pair = r.contract(G, -1.0)
+    site = np.repeat(np.arange(nl.n_sites), nl.n_neigh)
+    ref = -np.einsum("ksc,sk->kc", r.soap_cart_der, G[:, site])
+    assert np.abs(pair - ref).max() < 1e-12 * np.abs(ref).max()
+
+
+def _rotate_nl(nl, R):
+    d = nl.disp @ R.T
+    r = np.sqrt((d * d).sum(1))
+    th = np.zeros_like(r)
+    ph = np.zeros_like(r)
+    nz = r > 0
+    th[nz] = np.arccos(np.clip(d[nz, 2] / r[nz], -1, 1))
+    ph[nz] = np.arctan2(d[nz, 1], d[nz, 0])
+    import copy
+    out = copy.copy(nl)
+    out.rjs, out.thetas, out.phis, out.disp = r, th, ph, d
+    return out
+
+
+def test_oracle_rotation_invariance(cfg1):
+    w, W, S = cfg1
+    R = np.linalg.qr(np.random.default_rng(3).standard_normal((3, 3)))[0]
+    a = O.get_soap(w.hyper, w.nl, W, S, do_derivatives=False).soap
+    b = O.get_soap(w.hyper, _rotate_nl(w.nl, R), W, S, do_derivatives=False).soap
+    assert np.abs(a - b).max() < 1e-10
+
+
+def test_radial_derivative_unified_seed_is_fd_exact(cfg1):
+    # W (norm ~1e6) turns FP64 rounding into ~4e-10 of noise in the values, so
+    # the difference quotient uses a wide step with Richardson extrapolation.
+    w, W, _ = cfg1
+    hp = w.hyper
+    r = np.linspace(0.3, 4.99, 57)
+
+    def D(h):
+        vp, _ = O.radial_eval(hp, 0, W, r + h, legacy_seed=False)
+        vm, _ = O.radial_eval(hp, 0, W, r - h, legacy_seed=False)
+        return (vp - vm) / (2 * h)
+    h = 2e-3
+    fd = (4.0 * D(h / 2) - D(h)) / 3.0
+    _, d = O.radial_eval(hp, 0, W, r, legacy_seed=False)
+    assert np.abs(fd - d).max() < 2e-6 * np.abs(d).max()
+
+
+def test_radial_legacy_seed_differs_near_the_cutoff_only(cfg1):
+    # src/soap_turbo_radial.f90:44-67: the seeds differ only in the filter
+    # integral, which is switched off (pref = 0) more than 4 sigma inside
+    # rcut_soft, and matters at the 1e-5 level near rcut_hard.
+    w, W, _ = cfg1
+    hp = w.hyper
+    inner = np.linspace(0.5, 2.4, 20)
+    vl, dl = O.radial_eval(hp, 0, W, inner, legacy_seed=True)
+    vu, du = O.radial_eval(hp, 0, W, inner, legacy_seed=False)
+    np.testing.assert_array_equal(vl, vu)
+    outer = np.linspace(4.6, 4.99, 20)
+    vl, _ = O.radial_eval(hp, 0, W, outer, legacy_seed=True)
+    vu, _ = O.radial_eval(hp, 0, W, outer, legacy_seed=False)
+    rel = np.abs(vl - vu).max() / np.abs(vu).max()
+    assert 1e-9 < rel < 1e-3
+
+
+def test_oracle_vjp_against_finite_differences(cfg1):
+    w, W, S = cfg1
+    hp = w.hyper
+    st = w.structures[0]
+    nl = w.nl
+    rng = np.random.default_rng(5)
+    r0 = O.get_soap(hp, nl, W, S, do_derivatives=True, legacy_filter_seed=False)
+    G = rng.standard_normal((r0.soap.shape[1], nl.n_sites))
+    F = np.zeros((st.positions.shape[0], 3))
+    np.add.at(F, nl.neigh_atom, r0.contract(G, 1.0))
+
+    def L(pos):
+        nl2 = syn.neighbour_list(syn.Structure(pos, st.box, st.species), 5.0, 1)
+        return float(np.sum(G.T * O.get_soap(hp, nl2, W, S, do_derivatives=False,
+                                             legacy_filter_seed=False).soap))
+    h = 1e-4
+    for a in (0, 9):
+        for c in range(3):
+            p, m = st.positions.copy(), st.positions.copy()
+            p[a, c] += h
+            m[a, c] -= h
+            fd = (L(p) - L(m)) / (2 * h)
+            assert abs(fd - F[a, c]) < 1e-6 * np.abs(F).max()
