@@ -43,6 +43,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--quick", action="store_true",
+                    help="time the two kernels only (no FP64 path, e2e, CPU baseline or peak "
+                         "measurement); for profiling runs")
     return ap.parse_args()
 
 
@@ -294,6 +297,17 @@ def run_ours(args):
     ms_step = (sum(t_desc) + sum(t_con)) / K
     ms_step_max = shard.max_over_ranks(ms_step, device=dev)
     value = ws * nl.n_sites / (ms_step_max * 1e-3)
+
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "envs/s", "n_gpus": ws,
+                              "steps": K, "warmup": args.warmup, "ms_per_step": ms_step_max,
+                              "kernels_ms": {"descriptor": sum(t_desc) / K, "contract": sum(t_con) / K},
+                              "quick": True, "gpu_launches": int(launches)}), flush=True)
+        if ws > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return
 
     # ---- plain FP64 GPU form (materialised soap_cart_der, then contracted)
     for _ in range(2):

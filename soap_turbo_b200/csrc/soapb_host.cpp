@@ -3,6 +3,7 @@
 // two API layers declared in include/soap_b200.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -435,6 +436,89 @@ int build_tables(soapb_context *c) {
   const size_t iHo = add(hl_off.data(), hl_off.size() * 4), iHn = add(hl_np.data(), hl_np.size() * 4);
   const size_t iHq = add(hl_q.data(), hl_q.size() * 4), iHf = add(hl_fac.data(), hl_fac.size() * 4);
   const size_t iHf64 = add(hl_fac64.data(), hl_fac64.size() * 8);
+  // ---- per-CTA constants of the mixed kernels (one blob, copied to shared memory)
+  const int amax_t = (amax <= 8 && L <= 8) ? 8 : 16;
+  const int KS = K | 1;
+  std::vector<unsigned char> blob;
+  auto put = [&](const void *src, size_t bytes) {
+    const size_t o = blob.size();
+    blob.resize((o + bytes + 15) / 16 * 16, 0);
+    if (bytes) std::memcpy(blob.data() + o, src, bytes);
+    return (int)o;
+  };
+  {
+    std::vector<double> Wt((size_t)c->n_species * amax_t * amax_t, 0.0);
+    for (int s = 0; s < c->n_species; ++s) {
+      const int b = P.rad[s].nbeg, a = c->alpha[s];
+      for (int j = 0; j < a; ++j)
+        for (int i = 0; i < a; ++i) Wt[(size_t)s * amax_t * amax_t + j * a + i] = c->W[(size_t)(b + j) * N + (b + i)];
+    }
+    P.off_W = put(Wt.data(), Wt.size() * 8);
+    std::vector<unsigned char> rs((size_t)c->n_species * SOAPB_RADSP_BYTES, 0);
+    for (int s = 0; s < c->n_species; ++s) std::memcpy(rs.data() + (size_t)s * SOAPB_RADSP_BYTES, &P.rad[s], sizeof(RadSp));
+    P.off_rad = put(rs.data(), rs.size());
+    std::vector<int4> kidx(KS, make_int4(0, 0, 0, 0));
+    std::vector<float4> kcoef(KS, make_float4(0.f, 0.f, 0.f, 0.f));
+    std::vector<int> klm(KS, 0);
+    std::vector<float> kpref(KS, 0.f);
+    for (int l = 0; l <= L; ++l)
+      for (int m = 0; m <= l; ++m) {
+        const int kk = l * (l + 1) / 2 + m;
+        klm[kk] = l | (m << 8);
+        kpref[kk] = (float)pf[kk];
+        // sin(t) dP/dx and -m P/sin(t) from P_l^{m-1}, P_l^{m+1}, P_{l+1}^{m-1}, P_{l+1}^{m+1}
+        // (src/soap_turbo_angular.f90:194-246)
+        int4 ix = make_int4(kk, kk, kk, kk);
+        float4 cf = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (m == 0) {
+          if (l > 0) {
+            ix.x = ix.y = l * (l + 1) / 2 + 1;
+            cf.x = cf.y = -0.5f;
+          }
+        } else {
+          ix.x = kk - 1;
+          cf.x = 0.5f * (float)((l + m) * (l - m + 1));
+          if (m != l) {
+            ix.y = kk + 1;
+            cf.y = -0.5f;
+          }
+          ix.z = (l + 1) * (l + 2) / 2 + m - 1;
+          cf.z = 0.5f * (float)((l - m + 1) * (l - m + 2));
+          ix.w = (l + 1) * (l + 2) / 2 + m + 1;
+          cf.w = 0.5f;
+        }
+        kidx[kk] = ix;
+        kcoef[kk] = cf;
+      }
+    P.off_kidx = put(kidx.data(), kidx.size() * 16);
+    P.off_kcoef = put(kcoef.data(), kcoef.size() * 16);
+    P.off_klm = put(klm.data(), klm.size() * 4);
+    P.off_kpref = put(kpref.data(), kpref.size() * 4);
+    std::vector<int> nmap(N);
+    for (int s = 0; s < c->n_species; ++s)
+      for (int n = 0; n < c->alpha[s]; ++n) nmap[P.rad[s].nbeg + n] = s | (n << 8);
+    P.off_nmap = put(nmap.data(), nmap.size() * 4);
+    std::vector<int> citem;
+    for (int s = 0; s < c->n_species; ++s)
+      for (int kk = 0; kk < K; ++kk)
+        for (int half = 0; half < 2; ++half)
+          if (half * (amax_t / 2) < c->alpha[s]) citem.push_back(s | (kk << 4) | (half << 12));
+    P.n_citem = (int)citem.size();
+    P.off_citem = put(citem.data(), citem.size() * 4);
+    // H items (n, l), heaviest first so a strided assignment balances
+    std::vector<std::pair<long, int>> hw;
+    for (int l = 0; l <= L; ++l)
+      for (int n = 0; n < N; ++n)
+        hw.push_back({-(long)(hl_off[l * N + n + 1] - hl_off[l * N + n]) * (l + 1), n | (l << 8)});
+    std::stable_sort(hw.begin(), hw.end());
+    std::vector<int> hitem;
+    for (auto &p : hw) hitem.push_back(p.second);
+    P.n_hitem = (int)hitem.size();
+    P.off_hitem = put(hitem.data(), hitem.size() * 4);
+  }
+  P.amax_t = amax_t;
+  P.blob_bytes = (int)blob.size();
+  const size_t iBlob = add(blob.data(), blob.size());
   int rc = c->tables.ensure(total + 256);
   if (rc) return rc;
   std::vector<unsigned char> host(total + 256, 0);
@@ -459,6 +543,7 @@ int build_tables(soapb_context *c) {
   P.hl_q = (const int *)at(iHq);
   P.hl_fac = (const float *)at(iHf);
   P.hl_fac64 = (const double *)at(iHf64);
+  P.blob = (const unsigned char *)at(iBlob);
   P.n_soap = c->n_soap;
   P.n_kept = c->n_kept;
   return SOAPB_OK;
@@ -590,7 +675,7 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
   P.n_pairs = B.n_pairs;
   P.n_sites = B.n_sites;
   if (keep) {
-    if ((rc = c->keep_c.ensure(sizeof(float) * 2 * (size_t)c->n_max * P.k_max * ((size_t)b->n_sites + 1)))) return rc;
+    if ((rc = c->keep_c.ensure(sizeof(float) * 2 * (size_t)c->n_max * (P.k_max | 1) * ((size_t)b->n_sites + 1)))) return rc;
     if ((rc = c->keep_norm.ensure(sizeof(double) * ((size_t)b->n_sites + 1)))) return rc;
   }
   LaunchCfg cfg{pick_threads(c), c->stream};

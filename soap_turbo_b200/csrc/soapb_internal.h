@@ -58,7 +58,25 @@ struct DevParams {
   const int *hl_q;
   const float *hl_fac;
   const double *hl_fac64;
+  // Per-CTA constants of the mixed kernels, one contiguous blob copied into
+  // shared memory with 16-byte loads.  Offsets in bytes from its start.
+  const unsigned char *blob;
+  int blob_bytes;         // multiple of 16
+  int amax_t;             // the kernel instantiation's radial block (8 or 16)
+  int off_W;              // n_species blocks of amax_t^2 doubles (alpha x alpha used)
+  int off_rad;            // n_species RadSp
+  int off_kidx;           // KS int4: P_l^m indices of the derivative forms
+  int off_kcoef;          // KS float4: their coefficients
+  int off_klm;            // KS int: l | m << 8
+  int off_kpref;          // KS float: preflm
+  int off_nmap;           // n_max int: species | local index << 8
+  int off_citem;          // n_citem int: c_nlm items species | k << 4 | half << 12
+  int off_hitem;          // n_hitem int: H items n | l << 8
+  int n_citem, n_hitem;
 };
+
+// Size of RadSp padded to 16 bytes, as laid out in the constants blob.
+#define SOAPB_RADSP_BYTES ((int)((sizeof(RadSp) + 15) / 16 * 16))
 
 // Batch tables the prep kernel derives from the caller's CSR arrays.
 struct DevBatch {

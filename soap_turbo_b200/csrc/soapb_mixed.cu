@@ -187,58 +187,57 @@ __device__ __forceinline__ int first_species(unsigned bits) { return __ffs(bits)
 
 // ------------------------------------------------------------ layouts
 // Shared-memory layout of the kernels (bytes); host and device agree on it.
-// Region X holds the per-round entry staging; outside the chunk loop the same
-// bytes hold other per-site arrays (c for the power spectrum; c, Gp, Gu while
-// H is built).
+// The constants blob (W blocks, species constants, per-k tables, item maps)
+// comes first.  Region X holds the per-round entry staging; outside the chunk
+// loop the same bytes hold per-site arrays (c, Gp, Gu, the kept components).
 struct Layout {
-  size_t W, rad, kt, red, ent, wcnt, misc;
-  size_t C64, H;        // descriptor: FP64 c accumulators; contract: H
-  size_t X;             // aliased region
-  size_t R, Rd, E, U, A, F;  // staging inside X
-  size_t C, P, S;       // per-site arrays inside X (after / before the rounds)
+  size_t red, ent, wcnt, misc;
+  size_t C64, H, Rot, F;   // descriptor: FP64 c accumulators; contract: H, rotations, results
+  size_t X;                // aliased region
+  size_t R, Rd, E, U, A;   // staging inside X
+  size_t C, P, S;          // per-site arrays inside X
   size_t total;
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-// entries per round = NT / 2 (one radial and one angular thread per entry)
-__host__ __device__ inline int ang_stride(int LC) {
-  return (LC + 2) * (LC + 3) / 2 + 4 * (LC + 1) + 2;  // P (to L+1), il, ild, er, ei, amp, sfac
-}
+// P_l^m to l_max+1, i_l, di_l/dr, cos(m phi), -sin(m phi), amplitude, sigma factor
+__host__ __device__ inline int ang_stride(int LC) { return (LC + 2) * (LC + 3) / 2 + 4 * (LC + 1) + 2; }
+// row stride of H (floats): the species blocks padded to AMAX, plus 4 so that
+// 128-bit loads of consecutive k rows fall in distinct banks
+__host__ __device__ inline int h_stride(int n_species, int AMAX) { return n_species * AMAX + 4; }
 
 __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AMAX, int LC, int mode) {
   Layout L{};
   const size_t KS = (size_t)(P.k_max | 1);
   const size_t nsp = (size_t)P.n_species, CH = (size_t)NT / 2;
   const size_t nC = 2 * (size_t)P.n_max * KS;
-  size_t o = 0;
-  L.W = o;    o += nsp * AMAX * AMAX * sizeof(double);
-  L.rad = o;  o += nsp * sizeof(RadSp);
-  o = align_up(o, 16);
-  L.kt = o;   o += KS * 48;  // per k: int4 idx, float4 coef, l|m<<8, preflm
+  size_t o = (size_t)P.blob_bytes;
   L.red = o;  o += 40 * sizeof(double);
   L.ent = o;  o += (size_t)NT * nsp * sizeof(int);
   L.wcnt = o; o += (size_t)SOAPB_MAX_SPECIES * (NT / 32) * sizeof(int);
   L.misc = o; o += 64 * sizeof(int);
   o = align_up(o, 16);
-  if (mode == 0) { L.C64 = o; o += nC * sizeof(double); }
-  else { L.H = o; o += nC * sizeof(float); }
+  if (mode == 0) {
+    L.C64 = o; o += nC * sizeof(double);
+  } else {
+    L.H = o;   o += 2 * KS * (size_t)h_stride(P.n_species, AMAX) * sizeof(float);
+    L.Rot = o; o += (size_t)NT * 4 * sizeof(float);
+    L.F = o;   o += (size_t)NT * nsp * 3 * sizeof(float);
+  }
   o = align_up(o, 16);
   L.X = o;
-  // staging
   size_t x = o;
-  L.R = x;  x += CH * AMAX * sizeof(float);
+  L.R = x; x += CH * AMAX * sizeof(float);
   if (mode == 1) { L.Rd = x; x += CH * AMAX * sizeof(float); }
-  x = align_up(x, 8);
+  x = align_up(x, 16);
   if (mode == 0) {
     L.E = x; x += CH * (LC + 1) * sizeof(float2);
     L.U = x; x += CH * KS * sizeof(float);
   } else {
     L.A = x; x += CH * (size_t)ang_stride(LC) * sizeof(float);
-    L.F = x; x += (size_t)NT * nsp * 3 * sizeof(float);
   }
   const size_t end_stage = x;
-  // per-site arrays, aliased over the staging
   x = o;
   L.C = x; x += nC * sizeof(float);
   L.P = x; x += (size_t)P.n_kept * sizeof(float);
@@ -249,53 +248,15 @@ __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AM
   return L;
 }
 
-// Per-site prologue shared by both kernels: W blocks, species constants and
-// the per-k tables into shared memory.
-template <int NT, int AMAX>
-__device__ __forceinline__ void load_tables(const DevParams &P, double *sW, RadSp *sRad,
-                                            unsigned char *kt) {
-  const int n = P.n_species * AMAX * AMAX;
-  for (int t = threadIdx.x; t < n; t += NT) {
-    const int s = t / (AMAX * AMAX), r = t % (AMAX * AMAX);
-    const int a = P.rad[s].alpha;
-    sW[t] = (r < a * a) ? P.Wblk[(size_t)s * P.wstride + r] : 0.0;
-  }
-  for (int s = threadIdx.x; s < P.n_species; s += NT) sRad[s] = P.rad[s];
-  const int KS = P.k_max | 1;
-  int4 *kidx = (int4 *)kt;
-  float4 *kcoef = (float4 *)(kt + (size_t)KS * 16);
-  int *klm = (int *)(kt + (size_t)KS * 32);
-  float *kpref = (float *)(kt + (size_t)KS * 40);
-  for (int kk = threadIdx.x; kk < P.k_max; kk += NT) {
-    int l = 0;
-    while ((l + 1) * (l + 2) / 2 <= kk) ++l;
-    const int m = kk - l * (l + 1) / 2;
-    klm[kk] = l | (m << 8);
-    kpref[kk] = P.preflm[kk];
-    // sin(t) dP/dx and -m P / sin(t) from P_l^{m-1}, P_l^{m+1}, P_{l+1}^{m-1},
-    // P_{l+1}^{m+1} (src/soap_turbo_angular.f90:194-246)
-    int4 ix = make_int4(kk, kk, kk, kk);
-    float4 cf = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (m == 0) {
-      if (l > 0) {
-        ix.x = ix.y = l * (l + 1) / 2 + 1;
-        cf.x = cf.y = -0.5f;
-      }
-    } else {
-      ix.x = kk - 1;
-      cf.x = 0.5f * (float)((l + m) * (l - m + 1));
-      if (m != l) {
-        ix.y = kk + 1;
-        cf.y = -0.5f;
-      }
-      ix.z = (l + 1) * (l + 2) / 2 + m - 1;
-      cf.z = 0.5f * (float)((l - m + 1) * (l - m + 2));
-      ix.w = (l + 1) * (l + 2) / 2 + m + 1;
-      cf.w = 0.5f;
-    }
-    kidx[kk] = ix;
-    kcoef[kk] = cf;
-  }
+template <int NT>
+__device__ __forceinline__ void copy_blob(const DevParams &P, unsigned char *smem) {
+  const uint4 *src = (const uint4 *)P.blob;
+  uint4 *dst = (uint4 *)smem;
+  for (int t = threadIdx.x; t < P.blob_bytes / 16; t += NT) dst[t] = src[t];
+}
+
+__device__ __forceinline__ const RadSp &rad_of(const unsigned char *smem, const DevParams &P, int s) {
+  return *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
 }
 
 // ------------------------------------------------------------ descriptor
@@ -309,8 +270,9 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
   constexpr int NPLM = (LC + 1) * (LC + 2) / 2;
   constexpr int NH = AMAX / 2;  // radial indices per c_nlm item
   const Layout Ly = make_layout(P, NT, AMAX, LC, 0);
-  double *sW = (double *)(smem + Ly.W);
-  RadSp *sRad = (RadSp *)(smem + Ly.rad);
+  const double *sW = (const double *)(smem + P.off_W);
+  const int *klm = (const int *)(smem + P.off_klm);
+  const int *citem = (const int *)(smem + P.off_citem);
   double *sRed = (double *)(smem + Ly.red);
   double *sC64 = (double *)(smem + Ly.C64);
   float *sR = (float *)(smem + Ly.R);
@@ -327,9 +289,9 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
   const int tid = threadIdx.x;
   const int site = blockIdx.x;
   const int KS = P.k_max | 1;
-  const int n_max = P.n_max, k_max = P.k_max, L = P.l_max;
+  const int n_max = P.n_max, L = P.l_max;
 
-  load_tables<NT, AMAX>(P, sW, sRad, smem + Ly.kt);
+  copy_blob<NT>(P, smem);
   for (int t = tid; t < 2 * n_max * KS; t += NT) sC64[t] = 0.0;
 
   const int p_begin = B.off[site];
@@ -350,10 +312,10 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
           const int code = sEnt[ebase + el];
           const int pl = code & 0xffffff, s = code >> 24;
           const int k = chunk + pl;
+          const RadSp &RS = rad_of(smem, P, s);
           double val[AMAX], der[AMAX];
-          radial_entry<AMAX>(P, sRad[s], sW + s * AMAX * AMAX, B.rjs[k], k == p_begin, false,
-                             val, der);
-          const double g4 = kFourPi * sRad[s].gscale;
+          radial_entry<AMAX>(P, RS, sW + s * AMAX * AMAX, B.rjs[k], k == p_begin, false, val, der);
+          const double g4 = kFourPi * RS.gscale;
           float *Re = sR + (size_t)el * AMAX;
 #pragma unroll
           for (int n = 0; n < AMAX; ++n) Re[n] = (float)(g4 * val[n]);
@@ -366,21 +328,23 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
           AngScalars<LC> A;
           angular_scalars<LC>(P, first_species(B.bits[k]), B.rjs[k], B.thetas[k], B.phis[k],
                               false, A);
-          float plm[NPLM];
-          plm_array<LC, float>(L, (float)A.x, (float)A.sq, plm);
           float2 *Ee = sE + (size_t)el * (LC + 1);
 #pragma unroll
           for (int m = 0; m <= LC; ++m) Ee[m] = make_float2((float)A.er[m], (float)A.ei[m]);
+          float ilf[LC + 1];
+#pragma unroll
+          for (int l = 0; l <= LC; ++l) ilf[l] = (float)A.il[l];
+          const float ampf = (float)A.amp, xf = (float)A.x, sqf = (float)A.sq;
+          float plm[NPLM];
+          plm_array<LC, float>(L, xf, sqf, plm);
           float *Ue = sU + (size_t)el * KS;
-          const float ampf = (float)A.amp;
 #pragma unroll
           for (int l = 0; l <= LC; ++l) {
             if (l > L) break;
-            const float il = (float)A.il[l];
 #pragma unroll
             for (int m = 0; m <= l; ++m) {
               const int kk = l * (l + 1) / 2 + m;
-              Ue[kk] = ampf * P.preflm[kk] * plm[kk] * il;
+              Ue[kk] = ampf * P.preflm[kk] * plm[kk] * ilf[l];
             }
           }
         }
@@ -389,20 +353,21 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
       // ---- B. c_nlm: item = (species, k, half of the species' radial block);
       // FP32 partial sums over groups of 4 entries, flushed into FP64
       const int e_hi = ebase + n_round;
-      for (int it = tid; it < P.n_species * k_max * 2; it += NT) {
-        const int s = it / (2 * k_max), rem = it - s * 2 * k_max;
-        const int kk = rem >> 1, half = rem & 1;
+      for (int it = tid; it < P.n_citem; it += NT) {
+        const int code = citem[it];
+        const int s = code & 15, kk = (code >> 4) & 0xff, half = code >> 12;
         const int lo = max(sBase[s], ebase), hi = min(sBase[s] + sCnt[s], e_hi);
         if (lo >= hi) continue;
-        const int nb = sRad[s].nbeg, a = sRad[s].alpha, n0 = half * NH;
-        if (n0 >= a) continue;
-        int l = 0;
-        while ((l + 1) * (l + 2) / 2 <= kk) ++l;
-        const int m = kk - l * (l + 1) / 2;
+        const RadSp &RS = rad_of(smem, P, s);
+        const int nb = RS.nbeg, a = RS.alpha, n0 = half * NH;
+        const int m = klm[kk] >> 8;
         double dr[NH], di[NH];
         float pr[NH], pi[NH];
 #pragma unroll
-        for (int n = 0; n < NH; ++n) dr[n] = di[n] = 0.0, pr[n] = pi[n] = 0.f;
+        for (int n = 0; n < NH; ++n) {
+          dr[n] = di[n] = 0.0;
+          pr[n] = pi[n] = 0.f;
+        }
         int cnt = 0;
         for (int e2 = lo; e2 < hi; ++e2) {
           const int el = e2 - ebase;
@@ -443,8 +408,8 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
     for (int mm = 0; mm < mult; ++mm) {
       const int s = B.species[(size_t)site * B.max_mult + mm] - 1;
       if (s < 0 || s >= P.n_species) continue;
-      const int nb = sRad[s].nbeg, a = sRad[s].alpha;
-      for (int n = 0; n < a; ++n) sC64[(size_t)(nb + n) * KS] += P.central[nb + n];
+      const RadSp &RS = rad_of(smem, P, s);
+      for (int n = 0; n < RS.alpha; ++n) sC64[(size_t)(RS.nbeg + n) * KS] += P.central[RS.nbeg + n];
     }
   }
   __syncthreads();
@@ -480,11 +445,8 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
   double *out = soap_out + (size_t)site * P.n_soap;
   for (int o = tid; o < P.n_soap; o += NT) out[o] = (double)sS[o] * inv;
   if (keep) {
-    float *kc = keep_c + (size_t)site * 2 * n_max * k_max;
-    for (int t = tid; t < 2 * n_max * k_max; t += NT) {
-      const int row = t / k_max, kk = t - row * k_max;
-      kc[t] = sC[(size_t)row * KS + kk];
-    }
+    float *kc = keep_c + (size_t)site * 2 * n_max * KS;
+    for (int t = tid; t < 2 * n_max * KS; t += NT) kc[t] = sC[t];
     if (tid == 0) keep_norm[site] = norm;
   }
 }
@@ -499,45 +461,49 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
                                                     double *__restrict__ pair_out) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int CH = NT / 2;
+  constexpr int KC = (LC + 1) * (LC + 2) / 2;
+  constexpr int KJ = (KC + 15) / 16;
   constexpr int NPLM1 = (LC + 2) * (LC + 3) / 2;
   constexpr int AS = (LC + 2) * (LC + 3) / 2 + 4 * (LC + 1) + 2;
   constexpr int O_IL = NPLM1, O_ILD = NPLM1 + (LC + 1), O_ER = NPLM1 + 2 * (LC + 1),
                 O_EI = NPLM1 + 3 * (LC + 1), O_AMP = NPLM1 + 4 * (LC + 1), O_SF = O_AMP + 1;
+  static_assert(AMAX % 4 == 0, "vector loads of H need AMAX % 4 == 0");
   const Layout Ly = make_layout(P, NT, AMAX, LC, 1);
-  double *sW = (double *)(smem + Ly.W);
-  RadSp *sRad = (RadSp *)(smem + Ly.rad);
+  const double *sW = (const double *)(smem + P.off_W);
+  const int4 *kidx = (const int4 *)(smem + P.off_kidx);
+  const float4 *kcoef = (const float4 *)(smem + P.off_kcoef);
+  const int *klm = (const int *)(smem + P.off_klm);
+  const float *kpref = (const float *)(smem + P.off_kpref);
+  const int *nmap = (const int *)(smem + P.off_nmap);
+  const int *hitem = (const int *)(smem + P.off_hitem);
   double *sRed = (double *)(smem + Ly.red);
   float *sH = (float *)(smem + Ly.H);
+  float *sRot = (float *)(smem + Ly.Rot);
+  float *sF = (float *)(smem + Ly.F);
   float *sC = (float *)(smem + Ly.C);
   float *sGu = (float *)(smem + Ly.P);
   float *sGp = (float *)(smem + Ly.S);
   float *sR = (float *)(smem + Ly.R);
   float *sRd = (float *)(smem + Ly.Rd);
   float *sA = (float *)(smem + Ly.A);
-  float *sF = (float *)(smem + Ly.F);
   int *sEnt = (int *)(smem + Ly.ent);
   int *sW_cnt = (int *)(smem + Ly.wcnt);
   int *sMisc = (int *)(smem + Ly.misc);
   int *sBase = sMisc, *sCnt = sMisc + SOAPB_MAX_SPECIES, *sNent = sMisc + 2 * SOAPB_MAX_SPECIES;
-  unsigned char *kt = smem + Ly.kt;
 
   const int tid = threadIdx.x;
   const int site = blockIdx.x;
   const int KS = P.k_max | 1;
+  const int HS = h_stride(P.n_species, AMAX);
+  const size_t HPL = (size_t)KS * HS;  // H plane (re, then im)
   const int n_max = P.n_max, k_max = P.k_max, L = P.l_max, n_soap = P.n_soap;
   const int n_sites = B.n_sites;
-  const int4 *kidx = (const int4 *)kt;
-  const float4 *kcoef = (const float4 *)(kt + (size_t)KS * 16);
-  const int *klm = (const int *)(kt + (size_t)KS * 32);
-  const float *kpref = (const float *)(kt + (size_t)KS * 40);
 
-  load_tables<NT, AMAX>(P, sW, sRad, smem + Ly.kt);
+  copy_blob<NT>(P, smem);
   {
-    const float *kc = keep_c + (size_t)site * 2 * n_max * k_max;
-    for (int t = tid; t < 2 * n_max * k_max; t += NT) {
-      const int row = t / k_max, kk = t - row * k_max;
-      sC[(size_t)row * KS + kk] = kc[t];
-    }
+    const float *kc = keep_c + (size_t)site * 2 * n_max * KS;
+    for (int t = tid; t < 2 * n_max * KS; t += NT) sC[t] = kc[t];
+    for (int t = tid; t < 2 * (int)HPL; t += NT) sH[t] = 0.f;
   }
   // ---- back through the normalisation (src/soap_turbo.f90:1783-1790)
   const double *q = soap_in + (size_t)site * n_soap;
@@ -558,28 +524,46 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
     sGu[t] = v;
   }
   __syncthreads();
-  // ---- H(k,n) = w(m) sum_np Y(n,np,l) c(k,np) over the non-zero Y (:1800-1835)
-  for (int it = tid; it < n_max * k_max; it += NT) {
-    const int n = it / k_max, kk = it - n * k_max;
-    const int lm = klm[kk], l = lm & 0xff, m = lm >> 8;
-    float hr = 0.f, hi = 0.f;
+  // ---- H(k,n) = w(m) sum_np Y(n,np,l) c(k,np) over the non-zero Y (:1800-1835);
+  // one item per (n, l) walks its Y list once for all m
+  for (int it = tid; it < P.n_hitem; it += NT) {
+    const int code = hitem[it];
+    const int n = code & 0xff, l = code >> 8;
+    const int kb = l * (l + 1) / 2;
+    float hr[LC + 1], hi[LC + 1];
+#pragma unroll
+    for (int m = 0; m <= LC; ++m) hr[m] = hi[m] = 0.f;
     const int li = l * n_max + n;
     for (int t = P.hl_off[li]; t < P.hl_off[li + 1]; ++t) {
       const float y = P.hl_fac[t] * sGu[P.hl_q[t]];
-      const int np = P.hl_np[t];
-      hr = fmaf(y, sC[(size_t)np * KS + kk], hr);
-      hi = fmaf(y, sC[(size_t)(n_max + np) * KS + kk], hi);
+      const float *cr = sC + (size_t)P.hl_np[t] * KS + kb;
+      const float *ci = cr + (size_t)n_max * KS;
+#pragma unroll
+      for (int m = 0; m <= LC; ++m) {
+        if (m <= l) {
+          hr[m] = fmaf(y, cr[m], hr[m]);
+          hi[m] = fmaf(y, ci[m], hi[m]);
+        }
+      }
     }
-    const float w = (m == 0) ? 1.f : 2.f;
-    sH[(size_t)n * KS + kk] = w * hr;
-    sH[(size_t)(n_max + n) * KS + kk] = w * hi;
+    const int nm = nmap[n];
+    const int col = (nm & 0xff) * AMAX + (nm >> 8);
+#pragma unroll
+    for (int m = 0; m <= LC; ++m) {
+      if (m <= l) {
+        const float w = (m == 0) ? 1.f : 2.f;
+        sH[(size_t)(kb + m) * HS + col] = w * hr[m];
+        sH[HPL + (size_t)(kb + m) * HS + col] = w * hi[m];
+      }
+    }
   }
   __syncthreads();
+
+  const int hw = tid >> 4, hl = tid & 15;
 
   const int p_begin = B.off[site];
   const int p_end = min(B.off[site + 1], B.n_pairs);
   double self_x = 0.0, self_y = 0.0, self_z = 0.0;
-  const int hw = tid >> 4, hl = tid & 15;
 
   for (int chunk = p_begin; chunk < p_end; chunk += NT) {
     int slot[SOAPB_MAX_SPECIES];
@@ -595,9 +579,10 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
           const int code = sEnt[ebase + el];
           const int pl = code & 0xffffff, s = code >> 24;
           const int k = chunk + pl;
+          const RadSp &RS = rad_of(smem, P, s);
           double val[AMAX], der[AMAX];
-          radial_entry<AMAX>(P, sRad[s], sW + s * AMAX * AMAX, B.rjs[k], false, true, val, der);
-          const double g4 = kFourPi * sRad[s].gscale;
+          radial_entry<AMAX>(P, RS, sW + s * AMAX * AMAX, B.rjs[k], false, true, val, der);
+          const double g4 = kFourPi * RS.gscale;
           float *Re = sR + (size_t)el * AMAX, *Rde = sRd + (size_t)el * AMAX;
 #pragma unroll
           for (int n = 0; n < AMAX; ++n) {
@@ -623,6 +608,12 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
           }
           Ae[O_AMP] = (float)A.amp;
           Ae[O_SF] = (float)A.sig_fac;
+          // the rotation to Cartesian needs the same angles (:1867-1871)
+          float *rot = sRot + 4 * pl;
+          rot[0] = (float)A.x;
+          rot[1] = (float)A.sq;
+          rot[2] = (float)A.er[1];
+          rot[3] = (float)(-A.ei[1]);
           const float xf = (float)A.x, sqf = (float)A.sq;
           float plm[NPLM1];
           plm_array<LC + 1, float>(L + 1, xf, sqf, plm);
@@ -632,6 +623,21 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
       }
       __syncthreads();
       // ---- B. contraction against H: a half-warp per entry, lanes over k.
+      // Lane hl of a half-warp handles k = hl + 16 j; its k tables are loaded
+      // here rather than held through phase A, whose FP64 work needs the registers.
+      int4 kix[KJ];
+      float4 kcf[KJ];
+      int klmr[KJ];
+      float kpr[KJ];
+#pragma unroll
+      for (int j = 0; j < KJ; ++j) {
+        const int kk = hl + 16 * j;
+        const bool v = kk < k_max;
+        kix[j] = v ? kidx[kk] : make_int4(0, 0, 0, 0);
+        kcf[j] = v ? kcoef[kk] : make_float4(0.f, 0.f, 0.f, 0.f);
+        klmr[j] = v ? klm[kk] : -1;
+        kpr[j] = v ? kpref[kk] : 0.f;
+      }
       // The loop bound is uniform per warp (both halves iterate together) so
       // the full-mask shuffles below always see all 32 lanes.
       for (int eb = 2 * (tid >> 5); eb < n_round; eb += NT / 16) {
@@ -640,35 +646,46 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
         float f_rad = 0.f, f_azi = 0.f, f_pol = 0.f;
         if (act) {
           const int s = sEnt[ebase + el] >> 24;
-          const int nb = sRad[s].nbeg, a = sRad[s].alpha;
           const float *Ae = sA + (size_t)el * AS;
-          const float *Re = sR + (size_t)el * AMAX, *Rde = sRd + (size_t)el * AMAX;
-          const float *Hr = sH + (size_t)nb * KS, *Hi = sH + (size_t)(n_max + nb) * KS;
+          float R[AMAX], Rd[AMAX];
+#pragma unroll
+          for (int n4 = 0; n4 < AMAX / 4; ++n4) {
+            const float4 a = ((const float4 *)(sR + (size_t)el * AMAX))[n4];
+            const float4 d = ((const float4 *)(sRd + (size_t)el * AMAX))[n4];
+            R[4 * n4] = a.x; R[4 * n4 + 1] = a.y; R[4 * n4 + 2] = a.z; R[4 * n4 + 3] = a.w;
+            Rd[4 * n4] = d.x; Rd[4 * n4 + 1] = d.y; Rd[4 * n4 + 2] = d.z; Rd[4 * n4 + 3] = d.w;
+          }
           const float amp = Ae[O_AMP], sfac = Ae[O_SF];
-          for (int kk = hl; kk < k_max; kk += 16) {
-            const int lm = klm[kk], l = lm & 0xff, m = lm >> 8;
-            const int4 ix = kidx[kk];
-            const float4 cf = kcoef[kk];
+          const float *Hs = sH + (size_t)s * AMAX;
+#pragma unroll
+          for (int j = 0; j < KJ; ++j) {
+            if (klmr[j] < 0) continue;
+            const int kk = hl + 16 * j;
+            const int l = klmr[j] & 0xff, m = klmr[j] >> 8;
             const float Pk = Ae[kk];
-            const float dms = cf.x * Ae[ix.x] + cf.y * Ae[ix.y];
-            const float dvs = cf.z * Ae[ix.z] + cf.w * Ae[ix.w];
+            const float dms = kcf[j].x * Ae[kix[j].x] + kcf[j].y * Ae[kix[j].y];
+            const float dvs = kcf[j].z * Ae[kix[j].z] + kcf[j].w * Ae[kix[j].w];
             const float il = Ae[O_IL + l], ild = Ae[O_ILD + l];
             const float er = Ae[O_ER + m], ei = Ae[O_EI + m];
-            const float ap = amp * kpref[kk];
+            const float ap = amp * kpr[j];
             const float u = ap * Pk * il;
             const float ur = ap * Pk * ild - sfac * u;
             const float ua = ap * dvs * il;
             const float up = ap * dms * il;
+            const float4 *hr4 = (const float4 *)(Hs + (size_t)kk * HS);
+            const float4 *hi4 = (const float4 *)(Hs + HPL + (size_t)kk * HS);
             float Ur = 0.f, Ui = 0.f, Vr = 0.f, Vi = 0.f;
 #pragma unroll
-            for (int n = 0; n < AMAX; ++n) {
-              if (n < a) {
-                const float hr = Hr[(size_t)n * KS + kk], hi = Hi[(size_t)n * KS + kk];
-                Ur = fmaf(Rde[n], hr, Ur);
-                Ui = fmaf(Rde[n], hi, Ui);
-                Vr = fmaf(Re[n], hr, Vr);
-                Vi = fmaf(Re[n], hi, Vi);
-              }
+            for (int n4 = 0; n4 < AMAX / 4; ++n4) {
+              const float4 hr = hr4[n4], hi = hi4[n4];
+              Ur = fmaf(Rd[4 * n4], hr.x, Ur); Ur = fmaf(Rd[4 * n4 + 1], hr.y, Ur);
+              Ur = fmaf(Rd[4 * n4 + 2], hr.z, Ur); Ur = fmaf(Rd[4 * n4 + 3], hr.w, Ur);
+              Ui = fmaf(Rd[4 * n4], hi.x, Ui); Ui = fmaf(Rd[4 * n4 + 1], hi.y, Ui);
+              Ui = fmaf(Rd[4 * n4 + 2], hi.z, Ui); Ui = fmaf(Rd[4 * n4 + 3], hi.w, Ui);
+              Vr = fmaf(R[4 * n4], hr.x, Vr); Vr = fmaf(R[4 * n4 + 1], hr.y, Vr);
+              Vr = fmaf(R[4 * n4 + 2], hr.z, Vr); Vr = fmaf(R[4 * n4 + 3], hr.w, Vr);
+              Vi = fmaf(R[4 * n4], hi.x, Vi); Vi = fmaf(R[4 * n4 + 1], hi.y, Vi);
+              Vi = fmaf(R[4 * n4 + 2], hi.z, Vi); Vi = fmaf(R[4 * n4 + 3], hi.w, Vi);
             }
             const float reU = er * Ur + ei * Ui;
             const float reV = er * Vr + ei * Vi;
@@ -697,22 +714,23 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
     const int k = chunk + tid;
     double px = 0.0, py = 0.0, pz = 0.0;
     if (k < p_end && k > p_begin) {
-      double fr = 0.0, fa = 0.0, fp = 0.0;
+      if (my_bits != 0u) {
+        double fr = 0.0, fa = 0.0, fp = 0.0;
 #pragma unroll
-      for (int s = 0; s < SOAPB_MAX_SPECIES; ++s) {
-        if (s < P.n_species && slot[s] >= 0) {
-          fr += sF[3 * slot[s] + 0];
-          fa += sF[3 * slot[s] + 1];
-          fp += sF[3 * slot[s] + 2];
+        for (int s = 0; s < SOAPB_MAX_SPECIES; ++s) {
+          if (s < P.n_species && slot[s] >= 0) {
+            fr += sF[3 * slot[s] + 0];
+            fa += sF[3 * slot[s] + 1];
+            fp += sF[3 * slot[s] + 2];
+          }
         }
+        const float *rot = sRot + 4 * tid;
+        const double ct = rot[0], st = rot[1], cf = rot[2], sf = rot[3];
+        const double ir = 1.0 / B.rjs[k];
+        px = sgn * (st * cf * fr - ct * cf * ir * fp - sf * ir * fa);
+        py = sgn * (st * sf * fr - ct * sf * ir * fp + cf * ir * fa);
+        pz = sgn * (ct * fr + st * ir * fp);
       }
-      double st, ct, sf, cf;
-      sincos(B.thetas[k], &st, &ct);
-      sincos(B.phis[k], &sf, &cf);
-      const double ir = 1.0 / B.rjs[k];
-      px = sgn * (st * cf * fr - ct * cf * ir * fp - sf * ir * fa);
-      py = sgn * (st * sf * fr - ct * sf * ir * fp + cf * ir * fa);
-      pz = sgn * (ct * fr + st * ir * fp);
       double *po = pair_out + (size_t)3 * k;
       po[0] = px;
       po[1] = py;
@@ -757,22 +775,17 @@ static cudaError_t run_contract(const DevParams &P, const DevBatch &B, cudaStrea
   return cudaGetLastError();
 }
 
-static int max_alpha(const DevParams &P) {
-  int a = 0;
-  for (int s = 0; s < P.n_species; ++s) a = a > P.rad[s].alpha ? a : P.rad[s].alpha;
-  return a;
-}
-
 cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s) {
   const int blocks = 1 + (B.n_pairs + 255) / 256;
   k_prep<<<blocks, 256, 0, s>>>(B, P.n_species);
   return cudaGetLastError();
 }
 
+// The instantiation is fixed by the definition: the host lays the constants
+// blob out for amax_t (8 when every alpha <= 8 and l_max <= 8, else 16).
 #define SOAPB_DISPATCH(FN, ...)                          \
   do {                                                   \
-    if (max_alpha(P) <= 8 && P.l_max <= 8)               \
-      return FN<128, 8, 8>(__VA_ARGS__);                 \
+    if (P.amax_t == 8) return FN<128, 8, 8>(__VA_ARGS__); \
     return FN<128, 16, 12>(__VA_ARGS__);                 \
   } while (0)
 
@@ -788,12 +801,10 @@ cudaError_t launch_contract(const DevParams &P, const DevBatch &B, const LaunchC
 }
 
 size_t descriptor_smem(const DevParams &P, int) {
-  const bool small = max_alpha(P) <= 8 && P.l_max <= 8;
-  return make_layout(P, 128, small ? 8 : 16, small ? 8 : 12, 0).total;
+  return make_layout(P, 128, P.amax_t, P.amax_t == 8 ? 8 : 12, 0).total;
 }
 size_t contract_smem(const DevParams &P, int) {
-  const bool small = max_alpha(P) <= 8 && P.l_max <= 8;
-  return make_layout(P, 128, small ? 8 : 16, small ? 8 : 12, 1).total;
+  return make_layout(P, 128, P.amax_t, P.amax_t == 8 ? 8 : 12, 1).total;
 }
 
 }  // namespace soapb
