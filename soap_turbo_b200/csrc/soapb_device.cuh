@@ -351,4 +351,129 @@ __device__ __forceinline__ void plm_array(int lmax, T x, T sq, T (&p)[(LC + 1) *
   }
 }
 
+// ---------------------------------------------------------------- streamed angular stage
+// The same quantities as angular_scalars, written in FP32 to `out` as each one
+// appears so that only the last two terms of each recursion are live in FP64:
+//   out[o_il + l], out[o_ild + l] (DER), out[o_er + m], out[o_ei + m], out[o_amp],
+//   out[o_sf]; cos(theta) and sqrt(1 - cos^2) are returned in x, sq.
+template <int LC, bool DER>
+__device__ __forceinline__ void angular_stage(const DevParams &P, int i_sp, double rj, double theta,
+                                              double phi, float *out, int o_il, int o_ild, int o_er,
+                                              int o_ei, int o_amp, int o_sf, double &x, double &sq) {
+  const int L = P.l_max;
+  const double sig = P.sig_t[i_sp] + P.sig_t_c[i_sp] * rj;               // :579-580
+  out[o_amp] = (float)(P.rcut2 / (sig * sig));
+  x = cos(theta);
+  sq = sqrt(1.0 - x * x);
+  // i_l(x^2) exp(-x^2) (src/soap_turbo_angular.f90:361-422) and its radial
+  // derivative (:436-463), streamed over l
+  const double xx = rj / sig;
+  const double xcut = 1.0e-7;
+  const double x2 = xx * xx, x4 = x2 * x2;
+  const double inv_x2 = (x2 > 0.0) ? 1.0 / x2 : 0.0;
+  double x2pow = x2 * x2;
+  double flm2, flm1;
+  if (xx > 0.0) {
+    const double e2 = exp(-2.0 * x2);
+    flm2 = fabs((1.0 - e2) / 2.0 / x2);
+    flm1 = fabs((x2 - 1.0 + e2 * (x2 + 1.0)) / 2.0 / x4);
+  } else {
+    flm2 = 1.0;
+    flm1 = 0.0;
+  }
+  const double sc = P.sig_t_c[i_sp];
+  const double c1 = 2.0 * rj / (sig * sig), c2 = 1.0 - sc * rj / sig;
+  const bool dz = !(rj >= 1.0e-5);
+  double fact = 1.0, il_prev = 0.0, il0 = 0.0;
+#pragma unroll
+  for (int l = 0; l <= LC + 1; ++l) {
+    if (l > L + 1) break;
+    if (l > 0) fact = fact * (2.0 * (double)l + 1.0);
+    double il;
+    if (l == 0) {
+      il = (xx < xcut) ? 1.0 - x2 : flm2;
+    } else if (l == 1) {
+      il = (x2 / 1000.0 < xcut) ? (x2 - x4) / fact : flm1;
+    } else {
+      const double ratio = x2pow / fact;
+      double fl;
+      if (ratio * (double)l < xcut)
+        fl = ratio;
+      else
+        fl = fabs(flm2 - (2.0 * (double)l - 1.0) * inv_x2 * flm1);
+      x2pow = x2pow * x2;
+      flm2 = flm1;
+      flm1 = fl;
+      il = fl;
+    }
+    if (l <= LC) out[o_il + l] = (float)il;
+    if (DER) {
+      if (l == 0) il0 = il;
+      if (l == 1 && L >= 0) out[o_ild + 0] = dz ? 0.f : (float)(c1 * (il - il0) * c2);
+      if (l >= 1 && l <= L && l <= LC)
+        out[o_ild + l] = dz ? 0.f : (float)(((-c1 - (double)(2 * l + 2) / rj) * il + c1 * il_prev) * c2);
+    }
+    il_prev = il;
+  }
+  if (DER) out[o_sf] = (float)(2.0 * sc / sig);                         // :589
+  // e^{-i m phi}, Chebyshev recursion of get_eimphi_conjg (:284-298)
+  double cosm2 = cos(phi), sinm2 = -sin(phi);
+  const double cosphi2 = 2.0 * cosm2;
+  double cosm1 = 1.0, sinm1 = 0.0;
+  out[o_er] = 1.f;
+  out[o_ei] = 0.f;
+#pragma unroll
+  for (int l = 1; l <= LC; ++l) {
+    const double cos0 = cosphi2 * cosm1 - cosm2, sin0 = cosphi2 * sinm1 - sinm2;
+    cosm2 = cosm1;
+    sinm2 = sinm1;
+    cosm1 = cos0;
+    sinm1 = sin0;
+    out[o_er + l] = (float)cos0;
+    out[o_ei + l] = (float)(-sin0);
+  }
+}
+
+// P_l^m(x) for l = 0..lmax row by row (get_plm_array,
+// src/soap_turbo_angular.f90:108-160), keeping two rows in registers and
+// handing each value to emit(k, value) with k = l(l+1)/2 + m.
+template <int LC, typename Emit>
+__device__ __forceinline__ void plm_rows(int lmax, float x, float sq, Emit emit) {
+  float rm2[LC + 1], rm1[LC + 1], cur[LC + 1];
+#pragma unroll
+  for (int m = 0; m <= LC; ++m) rm2[m] = rm1[m] = cur[m] = 0.f;
+  const float x2 = x * x;
+#pragma unroll
+  for (int l = 0; l <= LC; ++l) {
+    if (l > lmax) break;
+    if (l == 0) {
+      cur[0] = 1.f;
+    } else if (l == 1) {
+      cur[0] = x;
+      cur[1] = -sq;
+    } else if (l == 2) {
+      cur[0] = 1.5f * x2 - 0.5f;
+      cur[1] = -3.f * x * sq;
+      cur[2] = 3.f - 3.f * x2;
+    } else {
+#pragma unroll
+      for (int m = 0; m <= LC; ++m) {
+        if (m <= l - 2) {
+          const float aa = (float)(2 * l - 1) / (float)(l - m);
+          const float bb = (float)(l - 1 + m) / (float)(l - m);
+          cur[m] = aa * x * rm1[m] - bb * rm2[m];
+        }
+      }
+      cur[l - 1] = x * (float)(2 * l - 1) * rm1[l - 1];
+      cur[l] = -(float)(2 * l - 1) * sq * rm1[l - 1];
+    }
+#pragma unroll
+    for (int m = 0; m <= LC; ++m) {
+      if (m <= l) emit(l * (l + 1) / 2 + m, cur[m]);
+      rm2[m] = rm1[m];
+      rm1[m] = cur[m];
+    }
+  }
+}
+
 }  // namespace soapb

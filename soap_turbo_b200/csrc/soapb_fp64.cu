@@ -29,14 +29,27 @@ __global__ void k64_radial(const DevParams P, const DevBatch B, int do_der, doub
   const double r = B.rjs[k];
   const unsigned bits = B.bits[k];
   double *ro = rad + (size_t)k * P.n_max, *rdo = rad_der + (size_t)k * P.n_max;
+  unsigned todo = 0u;
   for (int s = 0; s < P.n_species; ++s) {
     const RadSp &S = P.rad[s];
     const bool ok = ((bits >> s) & 1u) && r < S.rcut_hard && (!is_self || S.do_central);
+    if (ok) todo |= 1u << s;
+    else
+      for (int n = 0; n < S.alpha; ++n) {
+        ro[S.nbeg + n] = 0.0;
+        if (do_der) rdo[S.nbeg + n] = 0.0;
+      }
+  }
+  // one expansion call per valid species; lanes of different species share it
+  while (todo) {
+    const int s = __ffs(todo) - 1;
+    todo &= todo - 1u;
+    const RadSp &S = P.rad[s];
     double val[AMAX], der[AMAX];
-    if (ok) radial_entry<AMAX>(P, S, P.Wblk + (size_t)s * P.wstride, r, is_self, do_der != 0, val, der);
+    radial_entry<AMAX>(P, S, P.Wblk + (size_t)s * P.wstride, r, is_self, do_der != 0, val, der);
     for (int n = 0; n < S.alpha; ++n) {
-      ro[S.nbeg + n] = ok ? val[n] * S.gscale : 0.0;
-      if (do_der) rdo[S.nbeg + n] = ok ? der[n] * S.gscale : 0.0;
+      ro[S.nbeg + n] = val[n] * S.gscale;
+      if (do_der) rdo[S.nbeg + n] = der[n] * S.gscale;
     }
   }
 }

@@ -196,15 +196,16 @@ struct soapb_context {
   // device tables
   DBuf tables;
   // arena
-  DBuf off, bits, err, keep_c, keep_norm;
+  DBuf off, bits, err, keep_c, keep_norm, rad, ticket;
   DBuf f64_rad, f64_rad_der, f64_ang, f64_cnk, f64_soap_un, f64_norm;
   cudaStream_t stream = 0;
   int threads = 0;
+  int max_ctas = 0;
   int64_t launches = 0;
   int keep_valid = 0, keep_sites = 0, keep_pairs = 0;
 
   ~soapb_context() {
-    for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &f64_rad, &f64_rad_der,
+    for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &rad, &ticket, &f64_rad, &f64_rad_der,
                     &f64_ang, &f64_cnk, &f64_soap_un, &f64_norm})
       b->release();
   }
@@ -390,6 +391,7 @@ int build_tables(soapb_context *c) {
       }
       hl_off[l * N + n + 1] = (int)hl_np.size();
     }
+  std::vector<int> hl_packed;
   // poly3gauss central-atom term (src/soap_turbo.f90:646-662)
   std::vector<double> central(N, 0.0);
   if (c->basis == SOAPB_BASIS_POLY3GAUSS) {
@@ -515,10 +517,29 @@ int build_tables(soapb_context *c) {
     for (auto &p : hw) hitem.push_back(p.second);
     P.n_hitem = (int)hitem.size();
     P.off_hitem = put(hitem.data(), hitem.size() * 4);
+    P.off_kept = put(kept_nnl.data(), kept_nnl.size() * 4);
+    P.off_central = put(central.data(), central.size() * 8);
+    P.off_hloff = put(hl_off.data(), hl_off.size() * 4);
+    // Y lists packed as np | q << 8 | (n == np) << 31
+    if (nk >= 65536) return fail(SOAPB_ERR_ARGUMENT, "more than 65535 kept components");
+    hl_packed.resize(hl_np.size());
+    for (int l = 0; l <= L; ++l)
+      for (int n = 0; n < N; ++n)
+        for (int t = hl_off[l * N + n]; t < hl_off[l * N + n + 1]; ++t)
+          hl_packed[t] = (int)((unsigned)hl_np[t] | ((unsigned)hl_q[t] << 8) | ((n == hl_np[t]) ? 0x80000000u : 0u));
+    P.hl_in_blob = hl_packed.size() * 4 <= 16384;
+    P.off_hl = P.hl_in_blob ? put(hl_packed.data(), hl_packed.size() * 4) : 0;
+    // one-to-one compression: output q is kept component q with weight 1
+    bool ident = (ns == nk) && (nz == nk);
+    for (int o = 0; ident && o < ns; ++o)
+      ident = (pi_off[o + 1] - pi_off[o] == 1) && pi_q[pi_off[o]] == o && Pel[0] == Pel[0] &&
+              pi_el64[pi_off[o]] == 1.0;
+    P.cmap_identity = ident ? 1 : 0;
   }
   P.amax_t = amax_t;
   P.blob_bytes = (int)blob.size();
   const size_t iBlob = add(blob.data(), blob.size());
+  const size_t iHp = add(hl_packed.data(), hl_packed.size() * 4);
   int rc = c->tables.ensure(total + 256);
   if (rc) return rc;
   std::vector<unsigned char> host(total + 256, 0);
@@ -544,6 +565,7 @@ int build_tables(soapb_context *c) {
   P.hl_fac = (const float *)at(iHf);
   P.hl_fac64 = (const double *)at(iHf64);
   P.blob = (const unsigned char *)at(iBlob);
+  P.hl_packed = (const int *)at(iHp);
   P.n_soap = c->n_soap;
   P.n_kept = c->n_kept;
   return SOAPB_OK;
@@ -634,6 +656,9 @@ int ensure_batch(soapb_context *c, const soapb_batch *b, DevBatch &B) {
   if ((rc = c->off.ensure(sizeof(int) * ((size_t)b->n_sites + 1)))) return rc;
   if ((rc = c->bits.ensure((size_t)b->n_atom_pairs + 16))) return rc;
   if ((rc = c->err.ensure(16))) return rc;
+  if ((rc = c->ticket.ensure(16))) return rc;
+  if ((rc = c->rad.ensure(sizeof(float) * 2 * (size_t)c->P.amax_t * c->n_species * ((size_t)b->n_atom_pairs + 1))))
+    return rc;
   B.n_sites = b->n_sites;
   B.n_pairs = b->n_atom_pairs;
   B.max_mult = b->max_species_multiplicity;
@@ -647,6 +672,8 @@ int ensure_batch(soapb_context *c, const soapb_batch *b, DevBatch &B) {
   B.off = c->off.as<int>();
   B.bits = c->bits.as<uint8_t>();
   B.err = c->err.as<unsigned long long>();
+  B.rad = c->rad.as<float>();
+  B.ticket = c->ticket.as<int>();
   return SOAPB_OK;
 }
 
@@ -678,7 +705,10 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
     if ((rc = c->keep_c.ensure(sizeof(float) * 2 * (size_t)c->n_max * (P.k_max | 1) * ((size_t)b->n_sites + 1)))) return rc;
     if ((rc = c->keep_norm.ensure(sizeof(double) * ((size_t)b->n_sites + 1)))) return rc;
   }
-  LaunchCfg cfg{pick_threads(c), c->stream};
+  LaunchCfg cfg{pick_threads(c), c->stream, c->max_ctas};
+  CU(launch_radial(P, B, c->stream, keep));
+  c->launches += (b->n_atom_pairs > 0);
+  CU(cudaMemsetAsync(B.ticket, 0, 2 * sizeof(int), c->stream));
   CU(launch_descriptor(P, B, cfg, d_soap, keep ? c->keep_c.as<float>() : nullptr,
                        keep ? c->keep_norm.as<double>() : nullptr, keep));
   c->launches += (b->n_sites > 0);
@@ -701,7 +731,8 @@ int ctx_contract(soapb_context *c, const soapb_batch *b, const double *d_soap, c
   DevParams P = c->P;
   P.n_pairs = B.n_pairs;
   P.n_sites = B.n_sites;
-  LaunchCfg cfg{pick_threads(c), c->stream};
+  LaunchCfg cfg{pick_threads(c), c->stream, c->max_ctas};
+  CU(cudaMemsetAsync(B.ticket + 1, 0, sizeof(int), c->stream));
   CU(launch_contract(P, B, cfg, d_soap, d_G, g_layout, sgn, c->keep_c.as<float>(),
                      c->keep_norm.as<double>(), d_pair));
   c->launches += (b->n_sites > 0);

@@ -72,7 +72,14 @@ struct DevParams {
   int off_nmap;           // n_max int: species | local index << 8
   int off_citem;          // n_citem int: c_nlm items species | k << 4 | half << 12
   int off_hitem;          // n_hitem int: H items n | l << 8
+  int off_kept;           // n_kept int: kept_nnl
+  int off_central;        // n_max double: poly3gauss central-atom term
+  int off_hloff;          // (l_max+1)*n_max + 1 int: per (l, n) list offsets
+  int off_hl;             // packed Y-list entries np | q << 8 | (n == np) << 31, when hl_in_blob
   int n_citem, n_hitem;
+  int hl_in_blob;         // the packed Y lists fit in the blob (else read from hl_packed)
+  const int *hl_packed;   // global copy of the packed Y lists
+  int cmap_identity;      // the compression map sends kept component q to output q, weight 1
 };
 
 // Size of RadSp padded to 16 bytes, as laid out in the constants blob.
@@ -87,6 +94,8 @@ struct DevBatch {
   int *off;              // n_sites + 1 (prep output)
   uint8_t *bits;         // n_pairs: mask bits (prep output)
   unsigned long long *err;  // first bad pair index + 1 (0 = none)
+  float *rad;            // (n_pairs, n_species, 2, amax_t): 4 pi R_n and its r-derivative
+  int *ticket;           // work counters of the persistent site kernels
 };
 
 // Kernel launchers (soapb_mixed.cu, soapb_fp64.cu)
@@ -94,8 +103,10 @@ namespace soapb {
 struct LaunchCfg {
   int threads;           // threads per site CTA
   cudaStream_t stream;
+  int max_ctas;          // persistent grid cap (0 = from the occupancy)
 };
 cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s);
+cudaError_t launch_radial(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der);
 cudaError_t launch_descriptor(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
                               double *soap, float *keep_c, double *keep_norm, int keep);
 cudaError_t launch_contract(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,

@@ -108,9 +108,44 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
   return red[32];
 }
 
-struct Chunk {
-  int n_ent;
-};
+// Three sums at once, same fixed order as block_sum.
+template <int NT>
+__device__ __forceinline__ void block_sum3(double &a, double &b, double &c, double *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) {
+    red[warp] = a;
+    red[8 + warp] = b;
+    red[16 + warp] = c;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    double x = (lane < NT / 32) ? red[lane] : 0.0;
+    double y = (lane < NT / 32) ? red[8 + lane] : 0.0;
+    double z = (lane < NT / 32) ? red[16 + lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      x += __shfl_xor_sync(0xffffffffu, x, o);
+      y += __shfl_xor_sync(0xffffffffu, y, o);
+      z += __shfl_xor_sync(0xffffffffu, z, o);
+    }
+    if (lane == 0) {
+      red[32] = x;
+      red[33] = y;
+      red[34] = z;
+    }
+  }
+  __syncthreads();
+  a = red[32];
+  b = red[33];
+  c = red[34];
+}
 
 // Builds the entry list of one chunk of NT pairs.  Returns, per thread, the
 // radial-valid species bits of its own pair and (in slot[]) the entry slot of
@@ -185,26 +220,81 @@ __device__ __forceinline__ int build_entries(const DevParams &P, const DevBatch 
 
 __device__ __forceinline__ int first_species(unsigned bits) { return __ffs(bits) - 1; }
 
+// ------------------------------------------------------------ radial
+// One thread per pair: the FP64 radial expansion of every (pair, species)
+// entry (src/soap_turbo_radial.f90:281-1004), rounded to FP32 with 4 pi and
+// global_scaling folded in, into the batch's radial buffer.  The site kernels
+// read it; the contract reads the derivatives computed here by the descriptor
+// call that kept its state, as the reference keeps radial_exp_coeff and
+// radial_exp_coeff_der between get_soap and soap_contract.
+template <int AMAX>
+__global__ void __launch_bounds__(128) k_radial(const DevParams P, const DevBatch B, int do_der) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int head = (P.off_rad + P.n_species * SOAPB_RADSP_BYTES) / 16;
+  for (int t = threadIdx.x; t < head; t += 128) ((uint4 *)smem)[t] = ((const uint4 *)P.blob)[t];
+  __syncthreads();
+  const int k = blockIdx.x * 128 + threadIdx.x;
+  if (k >= B.n_pairs) return;
+  const unsigned bits = B.bits[k];
+  if (bits == 0u) return;
+  const double r = B.rjs[k];
+  // the pair's position in its CSR row decides the central-atom terms (:342-355)
+  int lo = 0, hi = B.n_sites;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (B.off[mid] <= k) lo = mid; else hi = mid;
+  }
+  const bool is_self = (B.off[lo] == k);
+  const double *sW = (const double *)(smem + P.off_W);
+  // The valid species of this pair, in order.  Species are data here, not
+  // control flow: every lane of a warp runs the same expansion with its own
+  // species' constants, so lanes of different species do not serialise.
+  unsigned todo = 0u;
+  for (int s = 0; s < P.n_species; ++s) {
+    const RadSp &RS = *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
+    if (((bits >> s) & 1u) && r < RS.rcut_hard && (!is_self || RS.do_central)) todo |= 1u << s;
+  }
+  while (todo) {
+    const int s = __ffs(todo) - 1;
+    todo &= todo - 1u;
+    const RadSp &RS = *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
+    double val[AMAX], der[AMAX];
+    radial_entry<AMAX>(P, RS, sW + s * AMAX * AMAX, r, is_self, do_der != 0, val, der);
+    const double g4 = kFourPi * RS.gscale;
+    float4 *o = (float4 *)(B.rad + ((size_t)k * P.n_species + s) * 2 * AMAX);
+#pragma unroll
+    for (int n4 = 0; n4 < AMAX / 4; ++n4)
+      o[n4] = make_float4((float)(g4 * val[4 * n4]), (float)(g4 * val[4 * n4 + 1]),
+                          (float)(g4 * val[4 * n4 + 2]), (float)(g4 * val[4 * n4 + 3]));
+    if (do_der)
+#pragma unroll
+      for (int n4 = 0; n4 < AMAX / 4; ++n4)
+        o[AMAX / 4 + n4] = make_float4((float)(g4 * der[4 * n4]), (float)(g4 * der[4 * n4 + 1]),
+                                       (float)(g4 * der[4 * n4 + 2]), (float)(g4 * der[4 * n4 + 3]));
+  }
+}
+
 // ------------------------------------------------------------ layouts
-// Shared-memory layout of the kernels (bytes); host and device agree on it.
-// The constants blob (W blocks, species constants, per-k tables, item maps)
-// comes first.  Region X holds the per-round entry staging; outside the chunk
-// loop the same bytes hold per-site arrays (c, Gp, Gu, the kept components).
+// Shared-memory layout of the site kernels (bytes); host and device agree on
+// it.  The constants blob (W blocks, species constants, per-k tables, item
+// maps, kept components, Y lists) comes first.  Region X holds the per-round
+// entry staging; outside the chunk loop the same bytes hold per-site arrays.
 struct Layout {
   size_t red, ent, wcnt, misc;
-  size_t C64, H, Rot, F;   // descriptor: FP64 c accumulators; contract: H, rotations, results
-  size_t X;                // aliased region
-  size_t R, Rd, E, U, A;   // staging inside X
-  size_t C, P, S;          // per-site arrays inside X
+  size_t C64, H, Rot, F;
+  size_t X;
+  size_t R, Rd, D, AP;   // staging inside X
+  size_t C, P, S;        // per-site arrays inside X
   size_t total;
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-
-// P_l^m to l_max+1, i_l, di_l/dr, cos(m phi), -sin(m phi), amplitude, sigma factor
-__host__ __device__ inline int ang_stride(int LC) { return (LC + 2) * (LC + 3) / 2 + 4 * (LC + 1) + 2; }
-// row stride of H (floats): the species blocks padded to AMAX, plus 4 so that
-// 128-bit loads of consecutive k rows fall in distinct banks
+// staged angular scalars per entry: i_l, di_l/dr, cos(m phi), -sin(m phi), amp, sigma factor
+__host__ __device__ inline int scal_stride(int LC) { return 4 * (LC + 1) + 3; }
+// staged P_l^m per entry (to l_max + 1 for the derivatives)
+__host__ __device__ inline int plm_stride(int LC) { return ((LC + 2) * (LC + 3) / 2) | 1; }
+// row stride of H: the species blocks padded to AMAX, plus 4 so that 128-bit
+// loads of consecutive k rows fall in distinct banks
 __host__ __device__ inline int h_stride(int n_species, int AMAX) { return n_species * AMAX + 4; }
 
 __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AMAX, int LC, int mode) {
@@ -230,13 +320,9 @@ __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AM
   size_t x = o;
   L.R = x; x += CH * AMAX * sizeof(float);
   if (mode == 1) { L.Rd = x; x += CH * AMAX * sizeof(float); }
-  x = align_up(x, 16);
-  if (mode == 0) {
-    L.E = x; x += CH * (LC + 1) * sizeof(float2);
-    L.U = x; x += CH * KS * sizeof(float);
-  } else {
-    L.A = x; x += CH * (size_t)ang_stride(LC) * sizeof(float);
-  }
+  L.D = x; x += CH * (size_t)scal_stride(LC) * sizeof(float);
+  L.AP = x;
+  x += CH * (mode == 0 ? KS : (size_t)plm_stride(LC)) * sizeof(float);
   const size_t end_stage = x;
   x = o;
   L.C = x; x += nC * sizeof(float);
@@ -259,6 +345,16 @@ __device__ __forceinline__ const RadSp &rad_of(const unsigned char *smem, const 
   return *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
 }
 
+// Persistent scheduling: every CTA takes sites from a counter until none are
+// left.  Which CTA computes a site does not change its result.
+template <int NT>
+__device__ __forceinline__ int next_site(int *ticket, int *slot) {
+  __syncthreads();
+  if (threadIdx.x == 0) *slot = atomicAdd(ticket, 1);
+  __syncthreads();
+  return *slot;
+}
+
 // ------------------------------------------------------------ descriptor
 template <int NT, int AMAX, int LC>
 __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const DevBatch B,
@@ -267,17 +363,20 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
                                                       double *__restrict__ keep_norm, int keep) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int CH = NT / 2;
-  constexpr int NPLM = (LC + 1) * (LC + 2) / 2;
   constexpr int NH = AMAX / 2;  // radial indices per c_nlm item
+  const int DS = scal_stride(LC);
+  const int O_IL = 0, O_ER = 2 * (LC + 1), O_EI = 3 * (LC + 1), O_AMP = 4 * (LC + 1);
   const Layout Ly = make_layout(P, NT, AMAX, LC, 0);
-  const double *sW = (const double *)(smem + P.off_W);
   const int *klm = (const int *)(smem + P.off_klm);
+  const float *kpref = (const float *)(smem + P.off_kpref);
   const int *citem = (const int *)(smem + P.off_citem);
+  const int *kept = (const int *)(smem + P.off_kept);
+  const double *central = (const double *)(smem + P.off_central);
   double *sRed = (double *)(smem + Ly.red);
   double *sC64 = (double *)(smem + Ly.C64);
   float *sR = (float *)(smem + Ly.R);
-  float2 *sE = (float2 *)(smem + Ly.E);
-  float *sU = (float *)(smem + Ly.U);
+  float *sD = (float *)(smem + Ly.D);
+  float *sAP = (float *)(smem + Ly.AP);
   float *sC = (float *)(smem + Ly.C);
   float *sP = (float *)(smem + Ly.P);
   float *sS = (float *)(smem + Ly.S);
@@ -285,169 +384,169 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
   int *sW_cnt = (int *)(smem + Ly.wcnt);
   int *sMisc = (int *)(smem + Ly.misc);
   int *sBase = sMisc, *sCnt = sMisc + SOAPB_MAX_SPECIES, *sNent = sMisc + 2 * SOAPB_MAX_SPECIES;
+  int *sSite = sMisc + 3 * SOAPB_MAX_SPECIES;
 
   const int tid = threadIdx.x;
-  const int site = blockIdx.x;
   const int KS = P.k_max | 1;
-  const int n_max = P.n_max, L = P.l_max;
+  const int n_max = P.n_max, L = P.l_max, nsp = P.n_species;
 
   copy_blob<NT>(P, smem);
-  for (int t = tid; t < 2 * n_max * KS; t += NT) sC64[t] = 0.0;
+  for (;;) {
+    const int site = next_site<NT>(B.ticket, sSite);
+    if (site >= B.n_sites) break;
+    for (int t = tid; t < 2 * n_max * KS; t += NT) sC64[t] = 0.0;
+    const int p_begin = B.off[site];
+    const int p_end = min(B.off[site + 1], B.n_pairs);
+    __syncthreads();
 
-  const int p_begin = B.off[site];
-  const int p_end = min(B.off[site + 1], B.n_pairs);
-  __syncthreads();
-
-  for (int chunk = p_begin; chunk < p_end; chunk += NT) {
-    int slot[SOAPB_MAX_SPECIES];
-    unsigned my_bits;
-    const int n_ent = build_entries<NT>(P, B, p_begin, chunk, p_end, false, sEnt, sW_cnt, sBase,
-                                        sCnt, sNent, slot, my_bits);
-    for (int ebase = 0; ebase < n_ent; ebase += CH) {
-      const int n_round = min(CH, n_ent - ebase);
-      // ---- A. expansions: threads [0, CH) radial (FP64), [CH, NT) angular
-      if (tid < CH) {
-        const int el = tid;
-        if (el < n_round) {
-          const int code = sEnt[ebase + el];
-          const int pl = code & 0xffffff, s = code >> 24;
-          const int k = chunk + pl;
-          const RadSp &RS = rad_of(smem, P, s);
-          double val[AMAX], der[AMAX];
-          radial_entry<AMAX>(P, RS, sW + s * AMAX * AMAX, B.rjs[k], k == p_begin, false, val, der);
-          const double g4 = kFourPi * RS.gscale;
-          float *Re = sR + (size_t)el * AMAX;
+    for (int chunk = p_begin; chunk < p_end; chunk += NT) {
+      int slot[SOAPB_MAX_SPECIES];
+      unsigned my_bits;
+      const int n_ent = build_entries<NT>(P, B, p_begin, chunk, p_end, false, sEnt, sW_cnt, sBase,
+                                          sCnt, sNent, slot, my_bits);
+      for (int ebase = 0; ebase < n_ent; ebase += CH) {
+        const int n_round = min(CH, n_ent - ebase);
+        // ---- A. angular expansion: [0, CH) the FP64 scalars, [CH, NT) the
+        // Y_lm factors amp * preflm * P_l^m and the entry's radial row
+        if (tid < CH) {
+          const int el = tid;
+          if (el < n_round) {
+            const int k = chunk + (sEnt[ebase + el] & 0xffffff);
+            double x, sq;
+            angular_stage<LC, false>(P, first_species(B.bits[k]), B.rjs[k], B.thetas[k],
+                                     B.phis[k], sD + (size_t)el * DS, O_IL, 0, O_ER, O_EI, O_AMP,
+                                     O_AMP + 1, x, sq);
+          }
+        } else {
+          const int el = tid - CH;
+          if (el < n_round) {
+            const int code = sEnt[ebase + el];
+            const int k = chunk + (code & 0xffffff), s = code >> 24;
+            const float4 *src = (const float4 *)(B.rad + ((size_t)k * nsp + s) * 2 * AMAX);
+            float4 *dst = (float4 *)(sR + (size_t)el * AMAX);
 #pragma unroll
-          for (int n = 0; n < AMAX; ++n) Re[n] = (float)(g4 * val[n]);
-        }
-      } else {
-        const int el = tid - CH;
-        if (el < n_round) {
-          const int pl = sEnt[ebase + el] & 0xffffff;
-          const int k = chunk + pl;
-          AngScalars<LC> A;
-          angular_scalars<LC>(P, first_species(B.bits[k]), B.rjs[k], B.thetas[k], B.phis[k],
-                              false, A);
-          float2 *Ee = sE + (size_t)el * (LC + 1);
-#pragma unroll
-          for (int m = 0; m <= LC; ++m) Ee[m] = make_float2((float)A.er[m], (float)A.ei[m]);
-          float ilf[LC + 1];
-#pragma unroll
-          for (int l = 0; l <= LC; ++l) ilf[l] = (float)A.il[l];
-          const float ampf = (float)A.amp, xf = (float)A.x, sqf = (float)A.sq;
-          float plm[NPLM];
-          plm_array<LC, float>(L, xf, sqf, plm);
-          float *Ue = sU + (size_t)el * KS;
-#pragma unroll
-          for (int l = 0; l <= LC; ++l) {
-            if (l > L) break;
-#pragma unroll
-            for (int m = 0; m <= l; ++m) {
-              const int kk = l * (l + 1) / 2 + m;
-              Ue[kk] = ampf * P.preflm[kk] * plm[kk] * ilf[l];
-            }
+            for (int n4 = 0; n4 < AMAX / 4; ++n4) dst[n4] = src[n4];
+            const int isp = first_species(B.bits[k]);
+            const double rj = B.rjs[k];
+            const double sig = P.sig_t[isp] + P.sig_t_c[isp] * rj;
+            const float amp = (float)(P.rcut2 / (sig * sig));
+            const double x = cos(B.thetas[k]);
+            const float xf = (float)x, sqf = (float)sqrt(1.0 - x * x);
+            float *APe = sAP + (size_t)el * KS;
+            plm_rows<LC>(L, xf, sqf, [&](int kk, float v) { APe[kk] = amp * kpref[kk] * v; });
           }
         }
-      }
-      __syncthreads();
-      // ---- B. c_nlm: item = (species, k, half of the species' radial block);
-      // FP32 partial sums over groups of 4 entries, flushed into FP64
-      const int e_hi = ebase + n_round;
-      for (int it = tid; it < P.n_citem; it += NT) {
-        const int code = citem[it];
-        const int s = code & 15, kk = (code >> 4) & 0xff, half = code >> 12;
-        const int lo = max(sBase[s], ebase), hi = min(sBase[s] + sCnt[s], e_hi);
-        if (lo >= hi) continue;
-        const RadSp &RS = rad_of(smem, P, s);
-        const int nb = RS.nbeg, a = RS.alpha, n0 = half * NH;
-        const int m = klm[kk] >> 8;
-        double dr[NH], di[NH];
-        float pr[NH], pi[NH];
-#pragma unroll
-        for (int n = 0; n < NH; ++n) {
-          dr[n] = di[n] = 0.0;
-          pr[n] = pi[n] = 0.f;
-        }
-        int cnt = 0;
-        for (int e2 = lo; e2 < hi; ++e2) {
-          const int el = e2 - ebase;
-          const float u = sU[(size_t)el * KS + kk];
-          const float2 E = sE[(size_t)el * (LC + 1) + m];
-          const float ar = u * E.x, ai = u * E.y;
-          const float *Re = sR + (size_t)el * AMAX + n0;
+        __syncthreads();
+        // ---- B. c_nlm: item = (species, k, half of the species' radial block);
+        // FP32 partial sums over groups of 4 entries, flushed into FP64
+        const int e_hi = ebase + n_round;
+        for (int it = tid; it < P.n_citem; it += NT) {
+          const int code = citem[it];
+          const int s = code & 15, kk = (code >> 4) & 0xff, half = code >> 12;
+          const int lo = max(sBase[s], ebase), hi = min(sBase[s] + sCnt[s], e_hi);
+          if (lo >= hi) continue;
+          const RadSp &RS = rad_of(smem, P, s);
+          const int nb = RS.nbeg, a = RS.alpha, n0 = half * NH;
+          const int lm = klm[kk], l = lm & 0xff, m = lm >> 8;
+          double dr[NH], di[NH];
+          float pr[NH], pi[NH];
 #pragma unroll
           for (int n = 0; n < NH; ++n) {
-            pr[n] = fmaf(Re[n], ar, pr[n]);
-            pi[n] = fmaf(Re[n], ai, pi[n]);
+            dr[n] = di[n] = 0.0;
+            pr[n] = pi[n] = 0.f;
           }
-          if (++cnt == 4) {
-            cnt = 0;
+          int cnt = 0;
+          for (int e2 = lo; e2 < hi; ++e2) {
+            const int el = e2 - ebase;
+            const float *De = sD + (size_t)el * DS;
+            const float u = sAP[(size_t)el * KS + kk] * De[O_IL + l];
+            const float ar = u * De[O_ER + m], ai = u * De[O_EI + m];
+            const float *Re = sR + (size_t)el * AMAX + n0;
 #pragma unroll
             for (int n = 0; n < NH; ++n) {
-              dr[n] += (double)pr[n];
-              di[n] += (double)pi[n];
-              pr[n] = pi[n] = 0.f;
+              pr[n] = fmaf(Re[n], ar, pr[n]);
+              pi[n] = fmaf(Re[n], ai, pi[n]);
+            }
+            if (++cnt == 4) {
+              cnt = 0;
+#pragma unroll
+              for (int n = 0; n < NH; ++n) {
+                dr[n] += (double)pr[n];
+                di[n] += (double)pi[n];
+                pr[n] = pi[n] = 0.f;
+              }
+            }
+          }
+#pragma unroll
+          for (int n = 0; n < NH; ++n) {
+            if (n0 + n < a) {
+              sC64[(size_t)(nb + n0 + n) * KS + kk] += dr[n] + (double)pr[n];
+              sC64[(size_t)(n_max + nb + n0 + n) * KS + kk] += di[n] + (double)pi[n];
             }
           }
         }
-#pragma unroll
-        for (int n = 0; n < NH; ++n) {
-          if (n0 + n < a) {
-            sC64[(size_t)(nb + n0 + n) * KS + kk] += dr[n] + (double)pr[n];
-            sC64[(size_t)(n_max + nb + n0 + n) * KS + kk] += di[n] + (double)pi[n];
-          }
-        }
+        __syncthreads();
       }
+    }
+
+    // ---- poly3gauss central-atom term (src/soap_turbo.f90:646-662)
+    if (P.basis == 1) {
+      const int mult = B.species_mult[site];
+      for (int mm = 0; mm < mult; ++mm) {
+        const int s = B.species[(size_t)site * B.max_mult + mm] - 1;
+        if (s < 0 || s >= nsp) continue;
+        const RadSp &RS = rad_of(smem, P, s);
+        for (int n = tid; n < RS.alpha; n += NT) sC64[(size_t)(RS.nbeg + n) * KS] += central[RS.nbeg + n];
+        __syncthreads();
+      }
+    }
+    __syncthreads();
+    for (int t = tid; t < 2 * n_max * KS; t += NT) sC[t] = (float)sC64[t];
+    __syncthreads();
+
+    // ---- C. power spectrum of the kept components (src/soap_turbo.f90:750-795)
+    float *pout = P.cmap_identity ? sS : sP;
+    double nrm2 = 0.0;
+    for (int q = tid; q < P.n_kept; q += NT) {
+      const int code = kept[q];
+      const int n = code & 0xff, np = (code >> 8) & 0xff, l = code >> 16;
+      const int kb = l * (l + 1) / 2;
+      const float *cn_r = sC + (size_t)n * KS + kb, *cn_i = sC + (size_t)(n_max + n) * KS + kb;
+      const float *cp_r = sC + (size_t)np * KS + kb, *cp_i = sC + (size_t)(n_max + np) * KS + kb;
+      const float acc0 = cn_r[0] * cp_r[0] + cn_i[0] * cp_i[0];
+      float acc = 0.f;
+      for (int m = 1; m <= l; ++m) acc += cn_r[m] * cp_r[m] + cn_i[m] * cp_i[m];
+      const float base = (n == np) ? 1.f : 1.41421356237309504880f;
+      const float v = base * (acc0 + 2.f * acc);
+      pout[q] = v;
+      nrm2 += (double)v * (double)v;
+    }
+    if (!P.cmap_identity) {
+      // compression through the map (:798-802)
       __syncthreads();
+      nrm2 = 0.0;
+      for (int o = tid; o < P.n_soap; o += NT) {
+        float v = 0.f;
+        for (int t = P.pi_off[o]; t < P.pi_off[o + 1]; ++t) v += P.pi_el[t] * sP[P.pi_q[t]];
+        sS[o] = v;
+        nrm2 += (double)v * (double)v;
+      }
     }
-  }
-
-  // ---- poly3gauss central-atom term (src/soap_turbo.f90:646-662)
-  if (P.basis == 1 && tid == 0) {
-    const int mult = B.species_mult[site];
-    for (int mm = 0; mm < mult; ++mm) {
-      const int s = B.species[(size_t)site * B.max_mult + mm] - 1;
-      if (s < 0 || s >= P.n_species) continue;
-      const RadSp &RS = rad_of(smem, P, s);
-      for (int n = 0; n < RS.alpha; ++n) sC64[(size_t)(RS.nbeg + n) * KS] += P.central[RS.nbeg + n];
+    nrm2 = block_sum<NT>(nrm2, sRed);  // (:805-809)
+    double norm = sqrt(nrm2);
+    if (norm < 1.0e-5) norm = 1.0;
+    const double inv = 1.0 / norm;
+    double *out = soap_out + (size_t)site * P.n_soap;
+    for (int o = tid; o < P.n_soap; o += NT) out[o] = (double)sS[o] * inv;
+    if (keep) {
+      float4 *kc = (float4 *)(keep_c + (size_t)site * 2 * n_max * KS);
+      const float4 *src = (const float4 *)sC;
+      const int n4 = (2 * n_max * KS) / 4;
+      for (int t = tid; t < n4; t += NT) kc[t] = src[t];
+      for (int t = 4 * n4 + tid; t < 2 * n_max * KS; t += NT)
+        keep_c[(size_t)site * 2 * n_max * KS + t] = sC[t];
+      if (tid == 0) keep_norm[site] = norm;
     }
-  }
-  __syncthreads();
-  for (int t = tid; t < 2 * n_max * KS; t += NT) sC[t] = (float)sC64[t];
-  __syncthreads();
-
-  // ---- C. power spectrum of the kept components (src/soap_turbo.f90:750-795)
-  for (int q = tid; q < P.n_kept; q += NT) {
-    const int code = P.kept_nnl[q];
-    const int n = code & 0xff, np = (code >> 8) & 0xff, l = code >> 16;
-    const int kb = l * (l + 1) / 2;
-    const float *cn_r = sC + (size_t)n * KS + kb, *cn_i = sC + (size_t)(n_max + n) * KS + kb;
-    const float *cp_r = sC + (size_t)np * KS + kb, *cp_i = sC + (size_t)(n_max + np) * KS + kb;
-    const float acc0 = cn_r[0] * cp_r[0] + cn_i[0] * cp_i[0];
-    float acc = 0.f;
-    for (int m = 1; m <= l; ++m) acc += cn_r[m] * cp_r[m] + cn_i[m] * cp_i[m];
-    const float base = (n == np) ? 1.f : 1.41421356237309504880f;
-    sP[q] = base * (acc0 + 2.f * acc);
-  }
-  __syncthreads();
-  // compression and norm (:798-809)
-  double nrm2 = 0.0;
-  for (int o = tid; o < P.n_soap; o += NT) {
-    float v = 0.f;
-    for (int t = P.pi_off[o]; t < P.pi_off[o + 1]; ++t) v += P.pi_el[t] * sP[P.pi_q[t]];
-    sS[o] = v;
-    nrm2 += (double)v * (double)v;
-  }
-  nrm2 = block_sum<NT>(nrm2, sRed);
-  double norm = sqrt(nrm2);
-  if (norm < 1.0e-5) norm = 1.0;
-  const double inv = 1.0 / norm;
-  double *out = soap_out + (size_t)site * P.n_soap;
-  for (int o = tid; o < P.n_soap; o += NT) out[o] = (double)sS[o] * inv;
-  if (keep) {
-    float *kc = keep_c + (size_t)site * 2 * n_max * KS;
-    for (int t = tid; t < 2 * n_max * KS; t += NT) kc[t] = sC[t];
-    if (tid == 0) keep_norm[site] = norm;
   }
 }
 
@@ -463,19 +562,20 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
   constexpr int CH = NT / 2;
   constexpr int KC = (LC + 1) * (LC + 2) / 2;
   constexpr int KJ = (KC + 15) / 16;
-  constexpr int NPLM1 = (LC + 2) * (LC + 3) / 2;
-  constexpr int AS = (LC + 2) * (LC + 3) / 2 + 4 * (LC + 1) + 2;
-  constexpr int O_IL = NPLM1, O_ILD = NPLM1 + (LC + 1), O_ER = NPLM1 + 2 * (LC + 1),
-                O_EI = NPLM1 + 3 * (LC + 1), O_AMP = NPLM1 + 4 * (LC + 1), O_SF = O_AMP + 1;
+  constexpr int GPT = 8;  // G values a thread holds while the norm dot product is reduced
   static_assert(AMAX % 4 == 0, "vector loads of H need AMAX % 4 == 0");
+  const int DS = scal_stride(LC), PS = plm_stride(LC);
+  const int O_IL = 0, O_ILD = LC + 1, O_ER = 2 * (LC + 1), O_EI = 3 * (LC + 1),
+            O_AMP = 4 * (LC + 1), O_SF = O_AMP + 1;
   const Layout Ly = make_layout(P, NT, AMAX, LC, 1);
-  const double *sW = (const double *)(smem + P.off_W);
   const int4 *kidx = (const int4 *)(smem + P.off_kidx);
   const float4 *kcoef = (const float4 *)(smem + P.off_kcoef);
   const int *klm = (const int *)(smem + P.off_klm);
   const float *kpref = (const float *)(smem + P.off_kpref);
   const int *nmap = (const int *)(smem + P.off_nmap);
   const int *hitem = (const int *)(smem + P.off_hitem);
+  const int *hloff = (const int *)(smem + P.off_hloff);
+  const int *hl = P.hl_in_blob ? (const int *)(smem + P.off_hl) : P.hl_packed;
   double *sRed = (double *)(smem + Ly.red);
   float *sH = (float *)(smem + Ly.H);
   float *sRot = (float *)(smem + Ly.Rot);
@@ -485,299 +585,343 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
   float *sGp = (float *)(smem + Ly.S);
   float *sR = (float *)(smem + Ly.R);
   float *sRd = (float *)(smem + Ly.Rd);
-  float *sA = (float *)(smem + Ly.A);
+  float *sD = (float *)(smem + Ly.D);
+  float *sPl = (float *)(smem + Ly.AP);
   int *sEnt = (int *)(smem + Ly.ent);
   int *sW_cnt = (int *)(smem + Ly.wcnt);
   int *sMisc = (int *)(smem + Ly.misc);
   int *sBase = sMisc, *sCnt = sMisc + SOAPB_MAX_SPECIES, *sNent = sMisc + 2 * SOAPB_MAX_SPECIES;
+  int *sSite = sMisc + 3 * SOAPB_MAX_SPECIES;
 
   const int tid = threadIdx.x;
-  const int site = blockIdx.x;
   const int KS = P.k_max | 1;
   const int HS = h_stride(P.n_species, AMAX);
   const size_t HPL = (size_t)KS * HS;  // H plane (re, then im)
-  const int n_max = P.n_max, k_max = P.k_max, L = P.l_max, n_soap = P.n_soap;
+  const int n_max = P.n_max, k_max = P.k_max, L = P.l_max, n_soap = P.n_soap, nsp = P.n_species;
   const int n_sites = B.n_sites;
+  const int hw = tid >> 4, hl16 = tid & 15;
+  float *sGu_eff = P.cmap_identity ? sGp : sGu;
 
   copy_blob<NT>(P, smem);
-  {
-    const float *kc = keep_c + (size_t)site * 2 * n_max * KS;
-    for (int t = tid; t < 2 * n_max * KS; t += NT) sC[t] = kc[t];
-    for (int t = tid; t < 2 * (int)HPL; t += NT) sH[t] = 0.f;
-  }
-  // ---- back through the normalisation (src/soap_turbo.f90:1783-1790)
-  const double *q = soap_in + (size_t)site * n_soap;
-  double qg = 0.0;
-  for (int o = tid; o < n_soap; o += NT)
-    qg += q[o] * (g_layout == 0 ? G[(size_t)o * n_sites + site] : G[(size_t)site * n_soap + o]);
-  qg = block_sum<NT>(qg, sRed);
-  const double inv = 1.0 / keep_norm[site];
-  for (int o = tid; o < n_soap; o += NT) {
-    const double g = g_layout == 0 ? G[(size_t)o * n_sites + site] : G[(size_t)site * n_soap + o];
-    sGp[o] = (float)((g - q[o] * qg) * inv);
-  }
-  __syncthreads();
-  // ---- back through the compression (:1791-1798), on the kept components
-  for (int t = tid; t < P.n_kept; t += NT) {
-    float v = 0.f;
-    for (int e = P.pj_off[t]; e < P.pj_off[t + 1]; ++e) v += P.pj_el[e] * sGp[P.pj_o[e]];
-    sGu[t] = v;
-  }
-  __syncthreads();
-  // ---- H(k,n) = w(m) sum_np Y(n,np,l) c(k,np) over the non-zero Y (:1800-1835);
-  // one item per (n, l) walks its Y list once for all m
-  for (int it = tid; it < P.n_hitem; it += NT) {
-    const int code = hitem[it];
-    const int n = code & 0xff, l = code >> 8;
-    const int kb = l * (l + 1) / 2;
-    float hr[LC + 1], hi[LC + 1];
+  for (;;) {
+    const int site = next_site<NT>(B.ticket + 1, sSite);
+    if (site >= n_sites) break;
+    {
+      const float4 *kc = (const float4 *)(keep_c + (size_t)site * 2 * n_max * KS);
+      const int n4 = (2 * n_max * KS) / 4;
+      for (int t = tid; t < n4; t += NT) ((float4 *)sC)[t] = kc[t];
+      for (int t = 4 * n4 + tid; t < 2 * n_max * KS; t += NT)
+        sC[t] = keep_c[(size_t)site * 2 * n_max * KS + t];
+      for (int t = tid; t < 2 * (int)HPL; t += NT) sH[t] = 0.f;
+    }
+    // ---- back through the normalisation (src/soap_turbo.f90:1783-1790); G is
+    // read once: the first GPT values per thread stay in registers
+    const double *q = soap_in + (size_t)site * n_soap;
+    double gv[GPT], qv[GPT];
+    double qg = 0.0;
 #pragma unroll
-    for (int m = 0; m <= LC; ++m) hr[m] = hi[m] = 0.f;
-    const int li = l * n_max + n;
-    for (int t = P.hl_off[li]; t < P.hl_off[li + 1]; ++t) {
-      const float y = P.hl_fac[t] * sGu[P.hl_q[t]];
-      const float *cr = sC + (size_t)P.hl_np[t] * KS + kb;
-      const float *ci = cr + (size_t)n_max * KS;
+    for (int j = 0; j < GPT; ++j) {
+      const int o = tid + j * NT;
+      gv[j] = qv[j] = 0.0;
+      if (o < n_soap) {
+        gv[j] = g_layout == 0 ? G[(size_t)o * n_sites + site] : G[(size_t)site * n_soap + o];
+        qv[j] = q[o];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < GPT; ++j) qg += qv[j] * gv[j];
+    for (int o = tid + GPT * NT; o < n_soap; o += NT) {
+      const double g = g_layout == 0 ? G[(size_t)o * n_sites + site] : G[(size_t)site * n_soap + o];
+      sGp[o] = (float)g;  // staged raw; finished below
+      qg += q[o] * g;
+    }
+    qg = block_sum<NT>(qg, sRed);
+    const double inv = 1.0 / keep_norm[site];
+#pragma unroll
+    for (int j = 0; j < GPT; ++j) {
+      const int o = tid + j * NT;
+      if (o < n_soap) sGp[o] = (float)((gv[j] - qv[j] * qg) * inv);
+    }
+    for (int o = tid + GPT * NT; o < n_soap; o += NT) sGp[o] = (float)(((double)sGp[o] - q[o] * qg) * inv);
+    __syncthreads();
+    // ---- back through the compression (:1791-1798), unless it is one-to-one
+    if (!P.cmap_identity) {
+      for (int t = tid; t < P.n_kept; t += NT) {
+        float v = 0.f;
+        for (int e = P.pj_off[t]; e < P.pj_off[t + 1]; ++e) v += P.pj_el[e] * sGp[P.pj_o[e]];
+        sGu[t] = v;
+      }
+      __syncthreads();
+    }
+    // ---- H(k,n) = w(m) sum_np Y(n,np,l) c(k,np) over the non-zero Y (:1800-1835);
+    // one item per (n, l) walks its Y list once for all m
+    for (int it = tid; it < P.n_hitem; it += NT) {
+      const int code = hitem[it];
+      const int n = code & 0xff, l = code >> 8;
+      const int kb = l * (l + 1) / 2;
+      float hr[LC + 1], hi[LC + 1];
+#pragma unroll
+      for (int m = 0; m <= LC; ++m) hr[m] = hi[m] = 0.f;
+      const int li = l * n_max + n;
+      for (int t = hloff[li]; t < hloff[li + 1]; ++t) {
+        const int e = hl[t];
+        const int np = e & 0xff, qq = (e >> 8) & 0xffff;
+        const float y = ((e >> 31) ? 2.f : 1.41421356237309504880f) * sGu_eff[qq];
+        const float *cr = sC + (size_t)np * KS + kb;
+        const float *ci = cr + (size_t)n_max * KS;
+#pragma unroll
+        for (int m = 0; m <= LC; ++m) {
+          if (m <= l) {
+            hr[m] = fmaf(y, cr[m], hr[m]);
+            hi[m] = fmaf(y, ci[m], hi[m]);
+          }
+        }
+      }
+      const int nm = nmap[n];
+      const int col = (nm & 0xff) * AMAX + (nm >> 8);
 #pragma unroll
       for (int m = 0; m <= LC; ++m) {
         if (m <= l) {
-          hr[m] = fmaf(y, cr[m], hr[m]);
-          hi[m] = fmaf(y, ci[m], hi[m]);
+          const float w = (m == 0) ? 1.f : 2.f;
+          sH[(size_t)(kb + m) * HS + col] = w * hr[m];
+          sH[HPL + (size_t)(kb + m) * HS + col] = w * hi[m];
         }
       }
     }
-    const int nm = nmap[n];
-    const int col = (nm & 0xff) * AMAX + (nm >> 8);
-#pragma unroll
-    for (int m = 0; m <= LC; ++m) {
-      if (m <= l) {
-        const float w = (m == 0) ? 1.f : 2.f;
-        sH[(size_t)(kb + m) * HS + col] = w * hr[m];
-        sH[HPL + (size_t)(kb + m) * HS + col] = w * hi[m];
-      }
-    }
-  }
-  __syncthreads();
+    __syncthreads();
 
-  const int hw = tid >> 4, hl = tid & 15;
+    const int p_begin = B.off[site];
+    const int p_end = min(B.off[site + 1], B.n_pairs);
+    double self_x = 0.0, self_y = 0.0, self_z = 0.0;
 
-  const int p_begin = B.off[site];
-  const int p_end = min(B.off[site + 1], B.n_pairs);
-  double self_x = 0.0, self_y = 0.0, self_z = 0.0;
-
-  for (int chunk = p_begin; chunk < p_end; chunk += NT) {
-    int slot[SOAPB_MAX_SPECIES];
-    unsigned my_bits;
-    const int n_ent = build_entries<NT>(P, B, p_begin, chunk, p_end, true, sEnt, sW_cnt, sBase,
-                                        sCnt, sNent, slot, my_bits);
-    for (int ebase = 0; ebase < n_ent; ebase += CH) {
-      const int n_round = min(CH, n_ent - ebase);
-      // ---- A. expansions and derivatives: [0, CH) radial, [CH, NT) angular
-      if (tid < CH) {
-        const int el = tid;
-        if (el < n_round) {
-          const int code = sEnt[ebase + el];
-          const int pl = code & 0xffffff, s = code >> 24;
-          const int k = chunk + pl;
-          const RadSp &RS = rad_of(smem, P, s);
-          double val[AMAX], der[AMAX];
-          radial_entry<AMAX>(P, RS, sW + s * AMAX * AMAX, B.rjs[k], false, true, val, der);
-          const double g4 = kFourPi * RS.gscale;
-          float *Re = sR + (size_t)el * AMAX, *Rde = sRd + (size_t)el * AMAX;
-#pragma unroll
-          for (int n = 0; n < AMAX; ++n) {
-            Re[n] = (float)(g4 * val[n]);
-            Rde[n] = (float)(g4 * der[n]);
+    for (int chunk = p_begin; chunk < p_end; chunk += NT) {
+      int slot[SOAPB_MAX_SPECIES];
+      unsigned my_bits;
+      const int n_ent = build_entries<NT>(P, B, p_begin, chunk, p_end, true, sEnt, sW_cnt, sBase,
+                                          sCnt, sNent, slot, my_bits);
+      for (int ebase = 0; ebase < n_ent; ebase += CH) {
+        const int n_round = min(CH, n_ent - ebase);
+        // ---- A. [0, CH): FP64 angular scalars with derivatives and the
+        // rotation factors; [CH, NT): P_l^m to l_max + 1 and the radial rows
+        if (tid < CH) {
+          const int el = tid;
+          if (el < n_round) {
+            const int pl = sEnt[ebase + el] & 0xffffff;
+            const int k = chunk + pl;
+            double x, sq;
+            float *De = sD + (size_t)el * DS;
+            angular_stage<LC, true>(P, first_species(B.bits[k]), B.rjs[k], B.thetas[k], B.phis[k],
+                                    De, O_IL, O_ILD, O_ER, O_EI, O_AMP, O_SF, x, sq);
+            // the rotation to Cartesian uses the same angles (:1867-1871)
+            float *rot = sRot + 4 * pl;
+            rot[0] = (float)x;
+            rot[1] = (float)sq;
+            rot[2] = De[O_ER + 1];
+            rot[3] = -De[O_EI + 1];
           }
-        }
-      } else {
-        const int el = tid - CH;
-        if (el < n_round) {
-          const int pl = sEnt[ebase + el] & 0xffffff;
-          const int k = chunk + pl;
-          AngScalars<LC> A;
-          angular_scalars<LC>(P, first_species(B.bits[k]), B.rjs[k], B.thetas[k], B.phis[k], true,
-                              A);
-          float *Ae = sA + (size_t)el * AS;
-#pragma unroll
-          for (int l = 0; l <= LC; ++l) {
-            Ae[O_IL + l] = (float)A.il[l];
-            Ae[O_ILD + l] = (float)A.ild[l];
-            Ae[O_ER + l] = (float)A.er[l];
-            Ae[O_EI + l] = (float)A.ei[l];
-          }
-          Ae[O_AMP] = (float)A.amp;
-          Ae[O_SF] = (float)A.sig_fac;
-          // the rotation to Cartesian needs the same angles (:1867-1871)
-          float *rot = sRot + 4 * pl;
-          rot[0] = (float)A.x;
-          rot[1] = (float)A.sq;
-          rot[2] = (float)A.er[1];
-          rot[3] = (float)(-A.ei[1]);
-          const float xf = (float)A.x, sqf = (float)A.sq;
-          float plm[NPLM1];
-          plm_array<LC + 1, float>(L + 1, xf, sqf, plm);
-#pragma unroll
-          for (int t = 0; t < NPLM1; ++t) Ae[t] = plm[t];
-        }
-      }
-      __syncthreads();
-      // ---- B. contraction against H: a half-warp per entry, lanes over k.
-      // Lane hl of a half-warp handles k = hl + 16 j; its k tables are loaded
-      // here rather than held through phase A, whose FP64 work needs the registers.
-      int4 kix[KJ];
-      float4 kcf[KJ];
-      int klmr[KJ];
-      float kpr[KJ];
-#pragma unroll
-      for (int j = 0; j < KJ; ++j) {
-        const int kk = hl + 16 * j;
-        const bool v = kk < k_max;
-        kix[j] = v ? kidx[kk] : make_int4(0, 0, 0, 0);
-        kcf[j] = v ? kcoef[kk] : make_float4(0.f, 0.f, 0.f, 0.f);
-        klmr[j] = v ? klm[kk] : -1;
-        kpr[j] = v ? kpref[kk] : 0.f;
-      }
-      // The loop bound is uniform per warp (both halves iterate together) so
-      // the full-mask shuffles below always see all 32 lanes.
-      for (int eb = 2 * (tid >> 5); eb < n_round; eb += NT / 16) {
-        const int el = eb + (hw & 1);
-        const bool act = el < n_round;
-        float f_rad = 0.f, f_azi = 0.f, f_pol = 0.f;
-        if (act) {
-          const int s = sEnt[ebase + el] >> 24;
-          const float *Ae = sA + (size_t)el * AS;
-          float R[AMAX], Rd[AMAX];
-#pragma unroll
-          for (int n4 = 0; n4 < AMAX / 4; ++n4) {
-            const float4 a = ((const float4 *)(sR + (size_t)el * AMAX))[n4];
-            const float4 d = ((const float4 *)(sRd + (size_t)el * AMAX))[n4];
-            R[4 * n4] = a.x; R[4 * n4 + 1] = a.y; R[4 * n4 + 2] = a.z; R[4 * n4 + 3] = a.w;
-            Rd[4 * n4] = d.x; Rd[4 * n4 + 1] = d.y; Rd[4 * n4 + 2] = d.z; Rd[4 * n4 + 3] = d.w;
-          }
-          const float amp = Ae[O_AMP], sfac = Ae[O_SF];
-          const float *Hs = sH + (size_t)s * AMAX;
-#pragma unroll
-          for (int j = 0; j < KJ; ++j) {
-            if (klmr[j] < 0) continue;
-            const int kk = hl + 16 * j;
-            const int l = klmr[j] & 0xff, m = klmr[j] >> 8;
-            const float Pk = Ae[kk];
-            const float dms = kcf[j].x * Ae[kix[j].x] + kcf[j].y * Ae[kix[j].y];
-            const float dvs = kcf[j].z * Ae[kix[j].z] + kcf[j].w * Ae[kix[j].w];
-            const float il = Ae[O_IL + l], ild = Ae[O_ILD + l];
-            const float er = Ae[O_ER + m], ei = Ae[O_EI + m];
-            const float ap = amp * kpr[j];
-            const float u = ap * Pk * il;
-            const float ur = ap * Pk * ild - sfac * u;
-            const float ua = ap * dvs * il;
-            const float up = ap * dms * il;
-            const float4 *hr4 = (const float4 *)(Hs + (size_t)kk * HS);
-            const float4 *hi4 = (const float4 *)(Hs + HPL + (size_t)kk * HS);
-            float Ur = 0.f, Ui = 0.f, Vr = 0.f, Vi = 0.f;
+        } else {
+          const int el = tid - CH;
+          if (el < n_round) {
+            const int code = sEnt[ebase + el];
+            const int k = chunk + (code & 0xffffff), s = code >> 24;
+            const float4 *src = (const float4 *)(B.rad + ((size_t)k * nsp + s) * 2 * AMAX);
+            float4 *dr = (float4 *)(sR + (size_t)el * AMAX);
+            float4 *dd = (float4 *)(sRd + (size_t)el * AMAX);
 #pragma unroll
             for (int n4 = 0; n4 < AMAX / 4; ++n4) {
-              const float4 hr = hr4[n4], hi = hi4[n4];
-              Ur = fmaf(Rd[4 * n4], hr.x, Ur); Ur = fmaf(Rd[4 * n4 + 1], hr.y, Ur);
-              Ur = fmaf(Rd[4 * n4 + 2], hr.z, Ur); Ur = fmaf(Rd[4 * n4 + 3], hr.w, Ur);
-              Ui = fmaf(Rd[4 * n4], hi.x, Ui); Ui = fmaf(Rd[4 * n4 + 1], hi.y, Ui);
-              Ui = fmaf(Rd[4 * n4 + 2], hi.z, Ui); Ui = fmaf(Rd[4 * n4 + 3], hi.w, Ui);
-              Vr = fmaf(R[4 * n4], hr.x, Vr); Vr = fmaf(R[4 * n4 + 1], hr.y, Vr);
-              Vr = fmaf(R[4 * n4 + 2], hr.z, Vr); Vr = fmaf(R[4 * n4 + 3], hr.w, Vr);
-              Vi = fmaf(R[4 * n4], hi.x, Vi); Vi = fmaf(R[4 * n4 + 1], hi.y, Vi);
-              Vi = fmaf(R[4 * n4 + 2], hi.z, Vi); Vi = fmaf(R[4 * n4 + 3], hi.w, Vi);
+              dr[n4] = src[n4];
+              dd[n4] = src[AMAX / 4 + n4];
             }
-            const float reU = er * Ur + ei * Ui;
-            const float reV = er * Vr + ei * Vi;
-            const float imV = ei * Vr - er * Vi;
-            f_rad = fmaf(u, reU, fmaf(ur, reV, f_rad));
-            f_azi = fmaf(-ua, imV, f_azi);
-            f_pol = fmaf(up, reV, f_pol);
+            const double x = cos(B.thetas[k]);
+            float *Pe = sPl + (size_t)el * PS;
+            plm_rows<LC + 1>(L + 1, (float)x, (float)sqrt(1.0 - x * x),
+                             [&](int kk, float v) { Pe[kk] = v; });
           }
         }
+        __syncthreads();
+        // ---- B. contraction against H: a half-warp per entry, lanes over k.
+        // Lane hl16 of a half-warp handles k = hl16 + 16 j; its k tables are
+        // loaded here rather than held through phase A.
+        int4 kix[KJ];
+        float4 kcf[KJ];
+        int klmr[KJ];
+        float kpr[KJ];
 #pragma unroll
-        for (int o = 8; o > 0; o >>= 1) {
-          f_rad += __shfl_xor_sync(0xffffffffu, f_rad, o);
-          f_azi += __shfl_xor_sync(0xffffffffu, f_azi, o);
-          f_pol += __shfl_xor_sync(0xffffffffu, f_pol, o);
+        for (int j = 0; j < KJ; ++j) {
+          const int kk = hl16 + 16 * j;
+          const bool v = kk < k_max;
+          kix[j] = v ? kidx[kk] : make_int4(0, 0, 0, 0);
+          kcf[j] = v ? kcoef[kk] : make_float4(0.f, 0.f, 0.f, 0.f);
+          klmr[j] = v ? klm[kk] : -1;
+          kpr[j] = v ? kpref[kk] : 0.f;
         }
-        if (act && hl == 0) {
-          float *Fe = sF + (size_t)(ebase + el) * 3;
-          Fe[0] = f_rad;
-          Fe[1] = f_azi;
-          Fe[2] = f_pol;
-        }
-      }
-      __syncthreads();
-    }
-    // ---- per pair: sum its entries, rotate to Cartesian (:1864-1875)
-    const int k = chunk + tid;
-    double px = 0.0, py = 0.0, pz = 0.0;
-    if (k < p_end && k > p_begin) {
-      if (my_bits != 0u) {
-        double fr = 0.0, fa = 0.0, fp = 0.0;
+        // The loop bound is uniform per warp (both halves iterate together) so
+        // the full-mask shuffles below always see all 32 lanes.
+        for (int eb = 2 * (tid >> 5); eb < n_round; eb += NT / 16) {
+          const int el = eb + (hw & 1);
+          const bool act = el < n_round;
+          float f_rad = 0.f, f_azi = 0.f, f_pol = 0.f;
+          if (act) {
+            const int s = sEnt[ebase + el] >> 24;
+            const float *Pe = sPl + (size_t)el * PS;
+            const float *De = sD + (size_t)el * DS;
+            float R[AMAX], Rd[AMAX];
 #pragma unroll
-        for (int s = 0; s < SOAPB_MAX_SPECIES; ++s) {
-          if (s < P.n_species && slot[s] >= 0) {
-            fr += sF[3 * slot[s] + 0];
-            fa += sF[3 * slot[s] + 1];
-            fp += sF[3 * slot[s] + 2];
+            for (int n4 = 0; n4 < AMAX / 4; ++n4) {
+              const float4 a = ((const float4 *)(sR + (size_t)el * AMAX))[n4];
+              const float4 d = ((const float4 *)(sRd + (size_t)el * AMAX))[n4];
+              R[4 * n4] = a.x; R[4 * n4 + 1] = a.y; R[4 * n4 + 2] = a.z; R[4 * n4 + 3] = a.w;
+              Rd[4 * n4] = d.x; Rd[4 * n4 + 1] = d.y; Rd[4 * n4 + 2] = d.z; Rd[4 * n4 + 3] = d.w;
+            }
+            const float amp = De[O_AMP], sfac = De[O_SF];
+            const float *Hs = sH + (size_t)s * AMAX;
+#pragma unroll
+            for (int j = 0; j < KJ; ++j) {
+              if (klmr[j] < 0) continue;
+              const int kk = hl16 + 16 * j;
+              const int l = klmr[j] & 0xff, m = klmr[j] >> 8;
+              const float Pk = Pe[kk];
+              const float dms = kcf[j].x * Pe[kix[j].x] + kcf[j].y * Pe[kix[j].y];
+              const float dvs = kcf[j].z * Pe[kix[j].z] + kcf[j].w * Pe[kix[j].w];
+              const float il = De[O_IL + l], ild = De[O_ILD + l];
+              const float er = De[O_ER + m], ei = De[O_EI + m];
+              const float ap = amp * kpr[j];
+              const float u = ap * Pk * il;
+              const float ur = ap * Pk * ild - sfac * u;
+              const float ua = ap * dvs * il;
+              const float up = ap * dms * il;
+              const float4 *hr4 = (const float4 *)(Hs + (size_t)kk * HS);
+              const float4 *hi4 = (const float4 *)(Hs + HPL + (size_t)kk * HS);
+              float Ur = 0.f, Ui = 0.f, Vr = 0.f, Vi = 0.f;
+#pragma unroll
+              for (int n4 = 0; n4 < AMAX / 4; ++n4) {
+                const float4 hr = hr4[n4], hi = hi4[n4];
+                Ur = fmaf(Rd[4 * n4], hr.x, Ur); Ur = fmaf(Rd[4 * n4 + 1], hr.y, Ur);
+                Ur = fmaf(Rd[4 * n4 + 2], hr.z, Ur); Ur = fmaf(Rd[4 * n4 + 3], hr.w, Ur);
+                Ui = fmaf(Rd[4 * n4], hi.x, Ui); Ui = fmaf(Rd[4 * n4 + 1], hi.y, Ui);
+                Ui = fmaf(Rd[4 * n4 + 2], hi.z, Ui); Ui = fmaf(Rd[4 * n4 + 3], hi.w, Ui);
+                Vr = fmaf(R[4 * n4], hr.x, Vr); Vr = fmaf(R[4 * n4 + 1], hr.y, Vr);
+                Vr = fmaf(R[4 * n4 + 2], hr.z, Vr); Vr = fmaf(R[4 * n4 + 3], hr.w, Vr);
+                Vi = fmaf(R[4 * n4], hi.x, Vi); Vi = fmaf(R[4 * n4 + 1], hi.y, Vi);
+                Vi = fmaf(R[4 * n4 + 2], hi.z, Vi); Vi = fmaf(R[4 * n4 + 3], hi.w, Vi);
+              }
+              const float reU = er * Ur + ei * Ui;
+              const float reV = er * Vr + ei * Vi;
+              const float imV = ei * Vr - er * Vi;
+              f_rad = fmaf(u, reU, fmaf(ur, reV, f_rad));
+              f_azi = fmaf(-ua, imV, f_azi);
+              f_pol = fmaf(up, reV, f_pol);
+            }
+          }
+#pragma unroll
+          for (int o = 8; o > 0; o >>= 1) {
+            f_rad += __shfl_xor_sync(0xffffffffu, f_rad, o);
+            f_azi += __shfl_xor_sync(0xffffffffu, f_azi, o);
+            f_pol += __shfl_xor_sync(0xffffffffu, f_pol, o);
+          }
+          if (act && hl16 == 0) {
+            float *Fe = sF + (size_t)(ebase + el) * 3;
+            Fe[0] = f_rad;
+            Fe[1] = f_azi;
+            Fe[2] = f_pol;
           }
         }
-        const float *rot = sRot + 4 * tid;
-        const double ct = rot[0], st = rot[1], cf = rot[2], sf = rot[3];
-        const double ir = 1.0 / B.rjs[k];
-        px = sgn * (st * cf * fr - ct * cf * ir * fp - sf * ir * fa);
-        py = sgn * (st * sf * fr - ct * sf * ir * fp + cf * ir * fa);
-        pz = sgn * (ct * fr + st * ir * fp);
+        __syncthreads();
       }
-      double *po = pair_out + (size_t)3 * k;
-      po[0] = px;
-      po[1] = py;
-      po[2] = pz;
+      // ---- per pair: sum its entries, rotate to Cartesian (:1864-1875)
+      const int k = chunk + tid;
+      double px = 0.0, py = 0.0, pz = 0.0;
+      if (k < p_end && k > p_begin) {
+        if (my_bits != 0u) {
+          double fr = 0.0, fa = 0.0, fp = 0.0;
+#pragma unroll
+          for (int s = 0; s < SOAPB_MAX_SPECIES; ++s) {
+            if (s < nsp && slot[s] >= 0) {
+              fr += sF[3 * slot[s] + 0];
+              fa += sF[3 * slot[s] + 1];
+              fp += sF[3 * slot[s] + 2];
+            }
+          }
+          const float *rot = sRot + 4 * tid;
+          const double ct = rot[0], st = rot[1], cf = rot[2], sf = rot[3];
+          const double ir = 1.0 / B.rjs[k];
+          px = sgn * (st * cf * fr - ct * cf * ir * fp - sf * ir * fa);
+          py = sgn * (st * sf * fr - ct * sf * ir * fp + cf * ir * fa);
+          pz = sgn * (ct * fr + st * ir * fp);
+        }
+        double *po = pair_out + (size_t)3 * k;
+        po[0] = px;
+        po[1] = py;
+        po[2] = pz;
+      }
+      self_x -= px;
+      self_y -= py;
+      self_z -= pz;
     }
-    self_x -= block_sum<NT>(px, sRed);
-    self_y -= block_sum<NT>(py, sRed);
-    self_z -= block_sum<NT>(pz, sRed);
-  }
-  if (tid == 0 && p_end > p_begin) {
-    double *po = pair_out + (size_t)3 * p_begin;
-    po[0] = self_x;
-    po[1] = self_y;
-    po[2] = self_z;
+    // the central pair is minus the sum of the others (:1875)
+    block_sum3<NT>(self_x, self_y, self_z, sRed);
+    if (tid == 0 && p_end > p_begin) {
+      double *po = pair_out + (size_t)3 * p_begin;
+      po[0] = self_x;
+      po[1] = self_y;
+      po[2] = self_z;
+    }
   }
 }
 
 // ------------------------------------------------------------ launchers
+template <typename K>
+static int persistent_grid(K kernel, int threads, size_t smem, int n_sites, int max_ctas) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  int g = sms * (per_sm > 0 ? per_sm : 1);
+  if (max_ctas > 0 && g > max_ctas) g = max_ctas;
+  return g < n_sites ? g : n_sites;
+}
+
 template <int NT, int AMAX, int LC>
-static cudaError_t run_descriptor(const DevParams &P, const DevBatch &B, cudaStream_t s,
+static cudaError_t run_descriptor(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
                                   double *soap, float *keep_c, double *keep_norm, int keep) {
   const size_t sm = make_layout(P, NT, AMAX, LC, 0).total;
-  cudaError_t e = cudaFuncSetAttribute(k_descriptor<NT, AMAX, LC>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  auto kern = k_descriptor<NT, AMAX, LC>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  if (P.n_sites > 0)
-    k_descriptor<NT, AMAX, LC><<<P.n_sites, NT, sm, s>>>(P, B, soap, keep_c, keep_norm, keep);
+  if (P.n_sites > 0) {
+    const int grid = persistent_grid(kern, NT, sm, P.n_sites, cfg.max_ctas);
+    kern<<<grid, NT, sm, cfg.stream>>>(P, B, soap, keep_c, keep_norm, keep);
+  }
   return cudaGetLastError();
 }
 
 template <int NT, int AMAX, int LC>
-static cudaError_t run_contract(const DevParams &P, const DevBatch &B, cudaStream_t s,
+static cudaError_t run_contract(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
                                 const double *soap, const double *G, int g_layout, double sgn,
                                 const float *keep_c, const double *keep_norm, double *pair) {
   const size_t sm = make_layout(P, NT, AMAX, LC, 1).total;
-  cudaError_t e = cudaFuncSetAttribute(k_contract<NT, AMAX, LC>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  auto kern = k_contract<NT, AMAX, LC>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  if (P.n_sites > 0)
-    k_contract<NT, AMAX, LC><<<P.n_sites, NT, sm, s>>>(P, B, soap, G, g_layout, sgn, keep_c,
-                                                       keep_norm, pair);
+  if (P.n_sites > 0) {
+    const int grid = persistent_grid(kern, NT, sm, P.n_sites, cfg.max_ctas);
+    kern<<<grid, NT, sm, cfg.stream>>>(P, B, soap, G, g_layout, sgn, keep_c, keep_norm, pair);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s) {
   const int blocks = 1 + (B.n_pairs + 255) / 256;
   k_prep<<<blocks, 256, 0, s>>>(B, P.n_species);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_radial(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der) {
+  if (B.n_pairs <= 0) return cudaSuccess;
+  const size_t sm = (size_t)P.off_rad + (size_t)P.n_species * SOAPB_RADSP_BYTES;
+  const int blocks = (B.n_pairs + 127) / 128;
+  if (P.amax_t == 8) k_radial<8><<<blocks, 128, sm, s>>>(P, B, do_der);
+  else k_radial<16><<<blocks, 128, sm, s>>>(P, B, do_der);
   return cudaGetLastError();
 }
 
@@ -791,13 +935,13 @@ cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s) {
 
 cudaError_t launch_descriptor(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
                               double *soap, float *keep_c, double *keep_norm, int keep) {
-  SOAPB_DISPATCH(run_descriptor, P, B, cfg.stream, soap, keep_c, keep_norm, keep);
+  SOAPB_DISPATCH(run_descriptor, P, B, cfg, soap, keep_c, keep_norm, keep);
 }
 
 cudaError_t launch_contract(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
                             const double *soap, const double *G, int g_layout, double sgn,
                             const float *keep_c, const double *keep_norm, double *pair) {
-  SOAPB_DISPATCH(run_contract, P, B, cfg.stream, soap, G, g_layout, sgn, keep_c, keep_norm, pair);
+  SOAPB_DISPATCH(run_contract, P, B, cfg, soap, G, g_layout, sgn, keep_c, keep_norm, pair);
 }
 
 size_t descriptor_smem(const DevParams &P, int) {
