@@ -196,7 +196,7 @@ struct soapb_context {
   // device tables
   DBuf tables;
   // arena
-  DBuf off, bits, err, keep_c, keep_norm, rad, ticket;
+  DBuf off, bits, err, keep_c, keep_norm, rad, ang, ticket;
   DBuf f64_rad, f64_rad_der, f64_ang, f64_cnk, f64_soap_un, f64_norm;
   cudaStream_t stream = 0;
   int threads = 0;
@@ -205,7 +205,7 @@ struct soapb_context {
   int keep_valid = 0, keep_sites = 0, keep_pairs = 0;
 
   ~soapb_context() {
-    for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &rad, &ticket, &f64_rad, &f64_rad_der,
+    for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &rad, &ang, &ticket, &f64_rad, &f64_rad_der,
                     &f64_ang, &f64_cnk, &f64_soap_un, &f64_norm})
       b->release();
   }
@@ -659,6 +659,8 @@ int ensure_batch(soapb_context *c, const soapb_batch *b, DevBatch &B) {
   if ((rc = c->ticket.ensure(16))) return rc;
   if ((rc = c->rad.ensure(sizeof(float) * 2 * (size_t)c->P.amax_t * c->n_species * ((size_t)b->n_atom_pairs + 1))))
     return rc;
+  if ((rc = c->ang.ensure(sizeof(float) * (size_t)ang_row_floats(c->P) * ((size_t)b->n_atom_pairs + 128))))
+    return rc;
   B.n_sites = b->n_sites;
   B.n_pairs = b->n_atom_pairs;
   B.max_mult = b->max_species_multiplicity;
@@ -673,6 +675,7 @@ int ensure_batch(soapb_context *c, const soapb_batch *b, DevBatch &B) {
   B.bits = c->bits.as<uint8_t>();
   B.err = c->err.as<unsigned long long>();
   B.rad = c->rad.as<float>();
+  B.ang = c->ang.as<float>();
   B.ticket = c->ticket.as<int>();
   return SOAPB_OK;
 }
@@ -702,11 +705,11 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
   P.n_pairs = B.n_pairs;
   P.n_sites = B.n_sites;
   if (keep) {
-    if ((rc = c->keep_c.ensure(sizeof(float) * 2 * (size_t)c->n_max * (P.k_max | 1) * ((size_t)b->n_sites + 1)))) return rc;
+    if ((rc = c->keep_c.ensure(sizeof(float) * keep_floats_per_site(P) * ((size_t)b->n_sites + 1)))) return rc;
     if ((rc = c->keep_norm.ensure(sizeof(double) * ((size_t)b->n_sites + 1)))) return rc;
   }
   LaunchCfg cfg{pick_threads(c), c->stream, c->max_ctas};
-  CU(launch_radial(P, B, c->stream, keep));
+  CU(launch_pair(P, B, c->stream, keep));
   c->launches += (b->n_atom_pairs > 0);
   CU(cudaMemsetAsync(B.ticket, 0, 2 * sizeof(int), c->stream));
   CU(launch_descriptor(P, B, cfg, d_soap, keep ? c->keep_c.as<float>() : nullptr,

@@ -95,6 +95,7 @@ struct DevBatch {
   uint8_t *bits;         // n_pairs: mask bits (prep output)
   unsigned long long *err;  // first bad pair index + 1 (0 = none)
   float *rad;            // (n_pairs, n_species, 2, amax_t): 4 pi R_n and its r-derivative
+  float *ang;            // (n_pairs, ang_row): the pair's angular row (see soapb_mixed.cu)
   int *ticket;           // work counters of the persistent site kernels
 };
 
@@ -106,7 +107,9 @@ struct LaunchCfg {
   int max_ctas;          // persistent grid cap (0 = from the occupancy)
 };
 cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s);
-cudaError_t launch_radial(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der);
+cudaError_t launch_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der);
+int ang_row_floats(const DevParams &P);
+size_t keep_floats_per_site(const DevParams &P);
 cudaError_t launch_descriptor(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
                               double *soap, float *keep_c, double *keep_norm, int keep);
 cudaError_t launch_contract(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,

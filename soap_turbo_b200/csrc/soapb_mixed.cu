@@ -220,89 +220,147 @@ __device__ __forceinline__ int build_entries(const DevParams &P, const DevBatch 
 
 __device__ __forceinline__ int first_species(unsigned bits) { return __ffs(bits) - 1; }
 
-// ------------------------------------------------------------ radial
-// One thread per pair: the FP64 radial expansion of every (pair, species)
-// entry (src/soap_turbo_radial.f90:281-1004), rounded to FP32 with 4 pi and
-// global_scaling folded in, into the batch's radial buffer.  The site kernels
-// read it; the contract reads the derivatives computed here by the descriptor
-// call that kept its state, as the reference keeps radial_exp_coeff and
-// radial_exp_coeff_der between get_soap and soap_contract.
-template <int AMAX>
-__global__ void __launch_bounds__(128) k_radial(const DevParams P, const DevBatch B, int do_der) {
+// ------------------------------------------------------------ pair rows
+// The angular row of a pair (floats), written by k_pair and read by the site
+// kernels: i_l, di_l/dr, cos(m phi), -sin(m phi) for l, m <= LC, the
+// amplitude rcut_max^2 / sigma_t^2, 2 sigma_t_scaling / sigma_t, cos(theta),
+// sqrt(1 - cos^2(theta)), then P_l^m for l <= l_max (+1 with derivatives).
+__host__ __device__ constexpr int row_il(int) { return 0; }
+__host__ __device__ constexpr int row_ild(int LC) { return LC + 1; }
+__host__ __device__ constexpr int row_er(int LC) { return 2 * (LC + 1); }
+__host__ __device__ constexpr int row_ei(int LC) { return 3 * (LC + 1); }
+__host__ __device__ constexpr int row_amp(int LC) { return 4 * (LC + 1); }
+__host__ __device__ constexpr int row_sf(int LC) { return 4 * (LC + 1) + 1; }
+__host__ __device__ constexpr int row_x(int LC) { return 4 * (LC + 1) + 2; }
+__host__ __device__ constexpr int row_sq(int LC) { return 4 * (LC + 1) + 3; }
+__host__ __device__ constexpr int row_p(int LC) { return 4 * (LC + 1) + 4; }
+__host__ __device__ constexpr int row_len(int LC) { return (row_p(LC) + (LC + 2) * (LC + 3) / 2 + 3) / 4 * 4; }
+
+int ang_row_floats(const DevParams &P) { return row_len(P.amax_t == 8 ? 8 : 12); }
+
+// ------------------------------------------------------------ pair kernel
+// One thread per pair, all FP64 work of the path:
+//  * the radial expansion of every (pair, species) entry
+//    (src/soap_turbo_radial.f90:281-1004), rounded to FP32 with 4 pi and
+//    global_scaling folded in, into the radial buffer;
+//  * the angular row (src/soap_turbo_angular.f90:267-463, 549-607), staged in
+//    shared memory and copied out with coalesced stores.
+// The site kernels only read these rows; soap_contract reads the rows of the
+// descriptor call that kept its state, as the reference keeps the radial and
+// angular expansions between get_soap and soap_contract.
+template <int AMAX, int LC>
+__global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch B, int do_der) {
   extern __shared__ __align__(16) unsigned char smem[];
+  constexpr int AW = row_len(LC);
+  // odd stride in shared memory: each thread fills its own row, so lanes must
+  // not all map to one bank
+  constexpr int AWS = AW + 1;
   const int head = (P.off_rad + P.n_species * SOAPB_RADSP_BYTES) / 16;
   for (int t = threadIdx.x; t < head; t += 128) ((uint4 *)smem)[t] = ((const uint4 *)P.blob)[t];
+  float *rows = (float *)(smem + (size_t)head * 16);
   __syncthreads();
-  const int k = blockIdx.x * 128 + threadIdx.x;
-  if (k >= B.n_pairs) return;
-  const unsigned bits = B.bits[k];
-  if (bits == 0u) return;
-  const double r = B.rjs[k];
-  // the pair's position in its CSR row decides the central-atom terms (:342-355)
-  int lo = 0, hi = B.n_sites;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (B.off[mid] <= k) lo = mid; else hi = mid;
-  }
-  const bool is_self = (B.off[lo] == k);
-  const double *sW = (const double *)(smem + P.off_W);
-  // The valid species of this pair, in order.  Species are data here, not
-  // control flow: every lane of a warp runs the same expansion with its own
-  // species' constants, so lanes of different species do not serialise.
-  unsigned todo = 0u;
-  for (int s = 0; s < P.n_species; ++s) {
-    const RadSp &RS = *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
-    if (((bits >> s) & 1u) && r < RS.rcut_hard && (!is_self || RS.do_central)) todo |= 1u << s;
-  }
-  while (todo) {
-    const int s = __ffs(todo) - 1;
-    todo &= todo - 1u;
-    const RadSp &RS = *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
-    double val[AMAX], der[AMAX];
-    radial_entry<AMAX>(P, RS, sW + s * AMAX * AMAX, r, is_self, do_der != 0, val, der);
-    const double g4 = kFourPi * RS.gscale;
-    float4 *o = (float4 *)(B.rad + ((size_t)k * P.n_species + s) * 2 * AMAX);
+  const int k0 = blockIdx.x * 128;
+  const int k = k0 + threadIdx.x;
+  if (k < B.n_pairs) {
+    const unsigned bits = B.bits[k];
+    const double r = B.rjs[k];
+    if (bits != 0u && r < P.rcut_max) {
+      float *row = rows + threadIdx.x * AWS;
+      double x, sq;
+      const int isp = __ffs(bits) - 1;
+      if (do_der)
+        angular_stage<LC, true>(P, isp, r, B.thetas[k], B.phis[k], row, row_il(LC), row_ild(LC),
+                                row_er(LC), row_ei(LC), row_amp(LC), row_sf(LC), x, sq);
+      else
+        angular_stage<LC, false>(P, isp, r, B.thetas[k], B.phis[k], row, row_il(LC), row_ild(LC),
+                                 row_er(LC), row_ei(LC), row_amp(LC), row_sf(LC), x, sq);
+      row[row_x(LC)] = (float)x;
+      row[row_sq(LC)] = (float)sq;
+      float *Pr = row + row_p(LC);
+      plm_rows<LC + 1>(P.l_max + (do_der ? 1 : 0), (float)x, (float)sq, [&](int kk, float v) { Pr[kk] = v; });
+      // the radial expansion of each valid species; the pair's position in its
+      // CSR row decides the central-atom terms (:342-355)
+      int lo = 0, hi = B.n_sites;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (B.off[mid] <= k) lo = mid; else hi = mid;
+      }
+      const bool is_self = (B.off[lo] == k);
+      const double *sW = (const double *)(smem + P.off_W);
+      unsigned todo = 0u;
+      for (int s = 0; s < P.n_species; ++s) {
+        const RadSp &RS = *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
+        if (((bits >> s) & 1u) && r < RS.rcut_hard && (!is_self || RS.do_central)) todo |= 1u << s;
+      }
+      // species are data, not control flow: lanes of different species share
+      // one expansion call
+      while (todo) {
+        const int s = __ffs(todo) - 1;
+        todo &= todo - 1u;
+        const RadSp &RS = *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
+        double val[AMAX], der[AMAX];
+        radial_entry<AMAX>(P, RS, sW + s * AMAX * AMAX, r, is_self, do_der != 0, val, der);
+        const double g4 = kFourPi * RS.gscale;
+        float4 *o = (float4 *)(B.rad + ((size_t)k * P.n_species + s) * 2 * AMAX);
 #pragma unroll
-    for (int n4 = 0; n4 < AMAX / 4; ++n4)
-      o[n4] = make_float4((float)(g4 * val[4 * n4]), (float)(g4 * val[4 * n4 + 1]),
-                          (float)(g4 * val[4 * n4 + 2]), (float)(g4 * val[4 * n4 + 3]));
-    if (do_der)
+        for (int n4 = 0; n4 < AMAX / 4; ++n4)
+          o[n4] = make_float4((float)(g4 * val[4 * n4]), (float)(g4 * val[4 * n4 + 1]),
+                              (float)(g4 * val[4 * n4 + 2]), (float)(g4 * val[4 * n4 + 3]));
+        if (do_der)
 #pragma unroll
-      for (int n4 = 0; n4 < AMAX / 4; ++n4)
-        o[AMAX / 4 + n4] = make_float4((float)(g4 * der[4 * n4]), (float)(g4 * der[4 * n4 + 1]),
-                                       (float)(g4 * der[4 * n4 + 2]), (float)(g4 * der[4 * n4 + 3]));
+          for (int n4 = 0; n4 < AMAX / 4; ++n4)
+            o[AMAX / 4 + n4] = make_float4((float)(g4 * der[4 * n4]), (float)(g4 * der[4 * n4 + 1]),
+                                           (float)(g4 * der[4 * n4 + 2]), (float)(g4 * der[4 * n4 + 3]));
+      }
+    }
+  }
+  __syncthreads();
+  const int n = min(128, B.n_pairs - k0) * AW;
+  float *dst = B.ang + (size_t)k0 * AW;
+  for (int t = threadIdx.x; t < n; t += 128) {
+    const int i = t / AW;
+    dst[t] = rows[i * AWS + (t - i * AW)];
   }
 }
 
 // ------------------------------------------------------------ layouts
-// Shared-memory layout of the site kernels (bytes); host and device agree on
-// it.  The constants blob (W blocks, species constants, per-k tables, item
+// Shared memory of the site kernels (bytes); host and device agree on it.
+// The site part of the constants blob (species constants, per-k tables, item
 // maps, kept components, Y lists) comes first.  Region X holds the per-round
 // entry staging; outside the chunk loop the same bytes hold per-site arrays.
 struct Layout {
   size_t red, ent, wcnt, misc;
   size_t C64, H, Rot, F;
   size_t X;
-  size_t R, Rd, D, AP;   // staging inside X
+  size_t R, Rd, A;       // staging inside X
   size_t C, P, S;        // per-site arrays inside X
   size_t total;
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-// staged angular scalars per entry: i_l, di_l/dr, cos(m phi), -sin(m phi), amp, sigma factor
-__host__ __device__ inline int scal_stride(int LC) { return 4 * (LC + 1) + 3; }
-// staged P_l^m per entry (to l_max + 1 for the derivatives)
-__host__ __device__ inline int plm_stride(int LC) { return ((LC + 2) * (LC + 3) / 2) | 1; }
+// staged rows are 16 floats longer than the global ones: rows stay 16-byte
+// aligned for the asynchronous copies, and the two half-warps of the VJP
+// contraction, which read neighbouring rows at the same offsets, use disjoint
+// bank halves
+__host__ __device__ inline int stage_stride(int LC) { return row_len(LC) + 16; }
 // row stride of H: the species blocks padded to AMAX, plus 4 so that 128-bit
 // loads of consecutive k rows fall in distinct banks
 __host__ __device__ inline int h_stride(int n_species, int AMAX) { return n_species * AMAX + 4; }
+// floats per site of the kept c_nlm, padded to a multiple of 4 so that every
+// site's block starts 16-byte aligned
+__host__ __device__ inline size_t keep_stride(const DevParams &P) {
+  return ((size_t)2 * P.n_max * (size_t)(P.k_max | 1) + 3) / 4 * 4;
+}
+__host__ __device__ inline size_t site_blob_bytes(const DevParams &P) {
+  return (size_t)(P.blob_bytes - P.off_rad);
+}
 
 __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AMAX, int LC, int mode) {
   Layout L{};
   const size_t KS = (size_t)(P.k_max | 1);
   const size_t nsp = (size_t)P.n_species, CH = (size_t)NT / 2;
   const size_t nC = 2 * (size_t)P.n_max * KS;
-  size_t o = (size_t)P.blob_bytes;
+  size_t o = site_blob_bytes(P);
   L.red = o;  o += 40 * sizeof(double);
   L.ent = o;  o += (size_t)NT * nsp * sizeof(int);
   L.wcnt = o; o += (size_t)SOAPB_MAX_SPECIES * (NT / 32) * sizeof(int);
@@ -320,9 +378,7 @@ __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AM
   size_t x = o;
   L.R = x; x += CH * AMAX * sizeof(float);
   if (mode == 1) { L.Rd = x; x += CH * AMAX * sizeof(float); }
-  L.D = x; x += CH * (size_t)scal_stride(LC) * sizeof(float);
-  L.AP = x;
-  x += CH * (mode == 0 ? KS : (size_t)plm_stride(LC)) * sizeof(float);
+  L.A = x; x += CH * (size_t)stage_stride(LC) * sizeof(float);
   const size_t end_stage = x;
   x = o;
   L.C = x; x += nC * sizeof(float);
@@ -335,14 +391,17 @@ __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AM
 }
 
 template <int NT>
-__device__ __forceinline__ void copy_blob(const DevParams &P, unsigned char *smem) {
-  const uint4 *src = (const uint4 *)P.blob;
+__device__ __forceinline__ void copy_site_blob(const DevParams &P, unsigned char *smem) {
+  const uint4 *src = (const uint4 *)(P.blob + P.off_rad);
   uint4 *dst = (uint4 *)smem;
-  for (int t = threadIdx.x; t < P.blob_bytes / 16; t += NT) dst[t] = src[t];
+  for (int t = threadIdx.x; t < (int)(site_blob_bytes(P) / 16); t += NT) dst[t] = src[t];
 }
 
+// Offset of a blob section inside the site kernels' shared copy.
+#define SBLOB(off) (smem + (P.off) - P.off_rad)
+
 __device__ __forceinline__ const RadSp &rad_of(const unsigned char *smem, const DevParams &P, int s) {
-  return *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
+  return *(const RadSp *)(smem + (size_t)s * SOAPB_RADSP_BYTES);
 }
 
 // Persistent scheduling: every CTA takes sites from a counter until none are
@@ -355,6 +414,42 @@ __device__ __forceinline__ int next_site(int *ticket, int *slot) {
   return *slot;
 }
 
+// 16-byte asynchronous global -> shared copy (no register staging).
+__device__ __forceinline__ void cp_async16(void *dst_smem, const void *src_gmem) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src_gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Copies the rows of entries [ebase, ebase + n_round) of a chunk into the
+// staging area (the angular rows and the radial rows), every 16-byte piece an
+// independent asynchronous copy.  The caller synchronises afterwards.
+template <int NT, int AMAX, int LC, bool DER>
+__device__ __forceinline__ void stage_entries(const DevParams &P, const DevBatch &B, const int *sEnt,
+                                              int chunk, int ebase, int n_round, float *sA,
+                                              float *sR, float *sRd) {
+  constexpr int AW4 = row_len(LC) / 4;
+  const int AS = stage_stride(LC);
+  for (int t = threadIdx.x; t < n_round * AW4; t += NT) {
+    const int el = t / AW4, j4 = t - el * AW4;
+    const int k = chunk + (sEnt[ebase + el] & 0xffffff);
+    cp_async16(sA + (size_t)el * AS + 4 * j4, B.ang + (size_t)k * (4 * AW4) + 4 * j4);
+  }
+  constexpr int R4 = AMAX / 4, RW4 = DER ? 2 * R4 : R4;
+  for (int t = threadIdx.x; t < n_round * RW4; t += NT) {
+    const int el = t / RW4, j4 = t - el * RW4;
+    const int code = sEnt[ebase + el];
+    const int k = chunk + (code & 0xffffff), s = code >> 24;
+    const float *src = B.rad + ((size_t)k * P.n_species + s) * 2 * AMAX + 4 * j4;
+    float *dst = (j4 < R4) ? sR + (size_t)el * AMAX + 4 * j4 : sRd + (size_t)el * AMAX + 4 * (j4 - R4);
+    cp_async16(dst, src);
+  }
+  cp_async_wait_all();
+}
+
 // ------------------------------------------------------------ descriptor
 template <int NT, int AMAX, int LC>
 __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const DevBatch B,
@@ -364,19 +459,17 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int CH = NT / 2;
   constexpr int NH = AMAX / 2;  // radial indices per c_nlm item
-  const int DS = scal_stride(LC);
-  const int O_IL = 0, O_ER = 2 * (LC + 1), O_EI = 3 * (LC + 1), O_AMP = 4 * (LC + 1);
+  const int AS = stage_stride(LC);
   const Layout Ly = make_layout(P, NT, AMAX, LC, 0);
-  const int *klm = (const int *)(smem + P.off_klm);
-  const float *kpref = (const float *)(smem + P.off_kpref);
-  const int *citem = (const int *)(smem + P.off_citem);
-  const int *kept = (const int *)(smem + P.off_kept);
-  const double *central = (const double *)(smem + P.off_central);
+  const int *klm = (const int *)SBLOB(off_klm);
+  const float *kpref = (const float *)SBLOB(off_kpref);
+  const int *citem = (const int *)SBLOB(off_citem);
+  const int *kept = (const int *)SBLOB(off_kept);
+  const double *central = (const double *)SBLOB(off_central);
   double *sRed = (double *)(smem + Ly.red);
   double *sC64 = (double *)(smem + Ly.C64);
   float *sR = (float *)(smem + Ly.R);
-  float *sD = (float *)(smem + Ly.D);
-  float *sAP = (float *)(smem + Ly.AP);
+  float *sA = (float *)(smem + Ly.A);
   float *sC = (float *)(smem + Ly.C);
   float *sP = (float *)(smem + Ly.P);
   float *sS = (float *)(smem + Ly.S);
@@ -388,9 +481,9 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
 
   const int tid = threadIdx.x;
   const int KS = P.k_max | 1;
-  const int n_max = P.n_max, L = P.l_max, nsp = P.n_species;
+  const int n_max = P.n_max, k_max = P.k_max, nsp = P.n_species;
 
-  copy_blob<NT>(P, smem);
+  copy_site_blob<NT>(P, smem);
   for (;;) {
     const int site = next_site<NT>(B.ticket, sSite);
     if (site >= B.n_sites) break;
@@ -406,34 +499,18 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
                                           sCnt, sNent, slot, my_bits);
       for (int ebase = 0; ebase < n_ent; ebase += CH) {
         const int n_round = min(CH, n_ent - ebase);
-        // ---- A. angular expansion: [0, CH) the FP64 scalars, [CH, NT) the
-        // Y_lm factors amp * preflm * P_l^m and the entry's radial row
-        if (tid < CH) {
-          const int el = tid;
-          if (el < n_round) {
-            const int k = chunk + (sEnt[ebase + el] & 0xffffff);
-            double x, sq;
-            angular_stage<LC, false>(P, first_species(B.bits[k]), B.rjs[k], B.thetas[k],
-                                     B.phis[k], sD + (size_t)el * DS, O_IL, 0, O_ER, O_EI, O_AMP,
-                                     O_AMP + 1, x, sq);
-          }
-        } else {
-          const int el = tid - CH;
-          if (el < n_round) {
-            const int code = sEnt[ebase + el];
-            const int k = chunk + (code & 0xffffff), s = code >> 24;
-            const float4 *src = (const float4 *)(B.rad + ((size_t)k * nsp + s) * 2 * AMAX);
-            float4 *dst = (float4 *)(sR + (size_t)el * AMAX);
-#pragma unroll
-            for (int n4 = 0; n4 < AMAX / 4; ++n4) dst[n4] = src[n4];
-            const int isp = first_species(B.bits[k]);
-            const double rj = B.rjs[k];
-            const double sig = P.sig_t[isp] + P.sig_t_c[isp] * rj;
-            const float amp = (float)(P.rcut2 / (sig * sig));
-            const double x = cos(B.thetas[k]);
-            const float xf = (float)x, sqf = (float)sqrt(1.0 - x * x);
-            float *APe = sAP + (size_t)el * KS;
-            plm_rows<LC>(L, xf, sqf, [&](int kk, float v) { APe[kk] = amp * kpref[kk] * v; });
+        // ---- A. the entries' rows, then u_k = amp * preflm_k * P_k * i_l in
+        // place of P_k (src/soap_turbo_angular.f90:590-594)
+        stage_entries<NT, AMAX, LC, false>(P, B, sEnt, chunk, ebase, n_round, sA, sR, nullptr);
+        __syncthreads();
+        {
+          int el = 0, kk = tid;
+          while (kk >= k_max) kk -= k_max, ++el;
+          for (; el < n_round;) {
+            float *Ae = sA + (size_t)el * AS;
+            Ae[row_p(LC) + kk] *= Ae[row_amp(LC)] * kpref[kk] * Ae[row_il(LC) + (klm[kk] & 0xff)];
+            kk += NT;
+            while (kk >= k_max) kk -= k_max, ++el;
           }
         }
         __syncthreads();
@@ -447,7 +524,7 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
           if (lo >= hi) continue;
           const RadSp &RS = rad_of(smem, P, s);
           const int nb = RS.nbeg, a = RS.alpha, n0 = half * NH;
-          const int lm = klm[kk], l = lm & 0xff, m = lm >> 8;
+          const int m = klm[kk] >> 8;
           double dr[NH], di[NH];
           float pr[NH], pi[NH];
 #pragma unroll
@@ -458,9 +535,9 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
           int cnt = 0;
           for (int e2 = lo; e2 < hi; ++e2) {
             const int el = e2 - ebase;
-            const float *De = sD + (size_t)el * DS;
-            const float u = sAP[(size_t)el * KS + kk] * De[O_IL + l];
-            const float ar = u * De[O_ER + m], ai = u * De[O_EI + m];
+            const float *Ae = sA + (size_t)el * AS;
+            const float u = Ae[row_p(LC) + kk];
+            const float ar = u * Ae[row_er(LC) + m], ai = u * Ae[row_ei(LC) + m];
             const float *Re = sR + (size_t)el * AMAX + n0;
 #pragma unroll
             for (int n = 0; n < NH; ++n) {
@@ -539,12 +616,10 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
     double *out = soap_out + (size_t)site * P.n_soap;
     for (int o = tid; o < P.n_soap; o += NT) out[o] = (double)sS[o] * inv;
     if (keep) {
-      float4 *kc = (float4 *)(keep_c + (size_t)site * 2 * n_max * KS);
-      const float4 *src = (const float4 *)sC;
+      float *kc = keep_c + (size_t)site * keep_stride(P);
       const int n4 = (2 * n_max * KS) / 4;
-      for (int t = tid; t < n4; t += NT) kc[t] = src[t];
-      for (int t = 4 * n4 + tid; t < 2 * n_max * KS; t += NT)
-        keep_c[(size_t)site * 2 * n_max * KS + t] = sC[t];
+      for (int t = tid; t < n4; t += NT) ((float4 *)kc)[t] = ((const float4 *)sC)[t];
+      for (int t = 4 * n4 + tid; t < 2 * n_max * KS; t += NT) kc[t] = sC[t];
       if (tid == 0) keep_norm[site] = norm;
     }
   }
@@ -564,18 +639,19 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
   constexpr int KJ = (KC + 15) / 16;
   constexpr int GPT = 8;  // G values a thread holds while the norm dot product is reduced
   static_assert(AMAX % 4 == 0, "vector loads of H need AMAX % 4 == 0");
-  const int DS = scal_stride(LC), PS = plm_stride(LC);
-  const int O_IL = 0, O_ILD = LC + 1, O_ER = 2 * (LC + 1), O_EI = 3 * (LC + 1),
-            O_AMP = 4 * (LC + 1), O_SF = O_AMP + 1;
+  const int AS = stage_stride(LC);
+  constexpr int O_IL = row_il(LC), O_ILD = row_ild(LC), O_ER = row_er(LC), O_EI = row_ei(LC),
+                O_AMP = row_amp(LC), O_SF = row_sf(LC), O_X = row_x(LC), O_SQ = row_sq(LC),
+                O_P = row_p(LC);
   const Layout Ly = make_layout(P, NT, AMAX, LC, 1);
-  const int4 *kidx = (const int4 *)(smem + P.off_kidx);
-  const float4 *kcoef = (const float4 *)(smem + P.off_kcoef);
-  const int *klm = (const int *)(smem + P.off_klm);
-  const float *kpref = (const float *)(smem + P.off_kpref);
-  const int *nmap = (const int *)(smem + P.off_nmap);
-  const int *hitem = (const int *)(smem + P.off_hitem);
-  const int *hloff = (const int *)(smem + P.off_hloff);
-  const int *hl = P.hl_in_blob ? (const int *)(smem + P.off_hl) : P.hl_packed;
+  const int4 *kidx = (const int4 *)SBLOB(off_kidx);
+  const float4 *kcoef = (const float4 *)SBLOB(off_kcoef);
+  const int *klm = (const int *)SBLOB(off_klm);
+  const float *kpref = (const float *)SBLOB(off_kpref);
+  const int *nmap = (const int *)SBLOB(off_nmap);
+  const int *hitem = (const int *)SBLOB(off_hitem);
+  const int *hloff = (const int *)SBLOB(off_hloff);
+  const int *hl = P.hl_in_blob ? (const int *)SBLOB(off_hl) : P.hl_packed;
   double *sRed = (double *)(smem + Ly.red);
   float *sH = (float *)(smem + Ly.H);
   float *sRot = (float *)(smem + Ly.Rot);
@@ -585,8 +661,7 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
   float *sGp = (float *)(smem + Ly.S);
   float *sR = (float *)(smem + Ly.R);
   float *sRd = (float *)(smem + Ly.Rd);
-  float *sD = (float *)(smem + Ly.D);
-  float *sPl = (float *)(smem + Ly.AP);
+  float *sA = (float *)(smem + Ly.A);
   int *sEnt = (int *)(smem + Ly.ent);
   int *sW_cnt = (int *)(smem + Ly.wcnt);
   int *sMisc = (int *)(smem + Ly.misc);
@@ -597,28 +672,18 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
   const int KS = P.k_max | 1;
   const int HS = h_stride(P.n_species, AMAX);
   const size_t HPL = (size_t)KS * HS;  // H plane (re, then im)
-  const int n_max = P.n_max, k_max = P.k_max, L = P.l_max, n_soap = P.n_soap, nsp = P.n_species;
+  const int n_max = P.n_max, k_max = P.k_max, n_soap = P.n_soap, nsp = P.n_species;
   const int n_sites = B.n_sites;
   const int hw = tid >> 4, hl16 = tid & 15;
   float *sGu_eff = P.cmap_identity ? sGp : sGu;
 
-  copy_blob<NT>(P, smem);
+  copy_site_blob<NT>(P, smem);
   for (;;) {
     const int site = next_site<NT>(B.ticket + 1, sSite);
     if (site >= n_sites) break;
-    {
-      const float4 *kc = (const float4 *)(keep_c + (size_t)site * 2 * n_max * KS);
-      const int n4 = (2 * n_max * KS) / 4;
-      for (int t = tid; t < n4; t += NT) ((float4 *)sC)[t] = kc[t];
-      for (int t = 4 * n4 + tid; t < 2 * n_max * KS; t += NT)
-        sC[t] = keep_c[(size_t)site * 2 * n_max * KS + t];
-      for (int t = tid; t < 2 * (int)HPL; t += NT) sH[t] = 0.f;
-    }
-    // ---- back through the normalisation (src/soap_turbo.f90:1783-1790); G is
-    // read once: the first GPT values per thread stay in registers
+    // ---- G is read first, so its latency overlaps the copies below
     const double *q = soap_in + (size_t)site * n_soap;
     double gv[GPT], qv[GPT];
-    double qg = 0.0;
 #pragma unroll
     for (int j = 0; j < GPT; ++j) {
       const int o = tid + j * NT;
@@ -628,6 +693,16 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
         qv[j] = q[o];
       }
     }
+    {
+      const float *kc = keep_c + (size_t)site * keep_stride(P);
+      const int n4 = (2 * n_max * KS) / 4;
+      for (int t = tid; t < n4; t += NT) cp_async16(sC + 4 * t, kc + 4 * t);
+      for (int t = 4 * n4 + tid; t < 2 * n_max * KS; t += NT) sC[t] = kc[t];
+      for (int t = tid; t < 2 * (int)HPL; t += NT) sH[t] = 0.f;
+      cp_async_wait_all();
+    }
+    // ---- back through the normalisation (src/soap_turbo.f90:1783-1790)
+    double qg = 0.0;
 #pragma unroll
     for (int j = 0; j < GPT; ++j) qg += qv[j] * gv[j];
     for (int o = tid + GPT * NT; o < n_soap; o += NT) {
@@ -701,47 +776,11 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
                                           sCnt, sNent, slot, my_bits);
       for (int ebase = 0; ebase < n_ent; ebase += CH) {
         const int n_round = min(CH, n_ent - ebase);
-        // ---- A. [0, CH): FP64 angular scalars with derivatives and the
-        // rotation factors; [CH, NT): P_l^m to l_max + 1 and the radial rows
-        if (tid < CH) {
-          const int el = tid;
-          if (el < n_round) {
-            const int pl = sEnt[ebase + el] & 0xffffff;
-            const int k = chunk + pl;
-            double x, sq;
-            float *De = sD + (size_t)el * DS;
-            angular_stage<LC, true>(P, first_species(B.bits[k]), B.rjs[k], B.thetas[k], B.phis[k],
-                                    De, O_IL, O_ILD, O_ER, O_EI, O_AMP, O_SF, x, sq);
-            // the rotation to Cartesian uses the same angles (:1867-1871)
-            float *rot = sRot + 4 * pl;
-            rot[0] = (float)x;
-            rot[1] = (float)sq;
-            rot[2] = De[O_ER + 1];
-            rot[3] = -De[O_EI + 1];
-          }
-        } else {
-          const int el = tid - CH;
-          if (el < n_round) {
-            const int code = sEnt[ebase + el];
-            const int k = chunk + (code & 0xffffff), s = code >> 24;
-            const float4 *src = (const float4 *)(B.rad + ((size_t)k * nsp + s) * 2 * AMAX);
-            float4 *dr = (float4 *)(sR + (size_t)el * AMAX);
-            float4 *dd = (float4 *)(sRd + (size_t)el * AMAX);
-#pragma unroll
-            for (int n4 = 0; n4 < AMAX / 4; ++n4) {
-              dr[n4] = src[n4];
-              dd[n4] = src[AMAX / 4 + n4];
-            }
-            const double x = cos(B.thetas[k]);
-            float *Pe = sPl + (size_t)el * PS;
-            plm_rows<LC + 1>(L + 1, (float)x, (float)sqrt(1.0 - x * x),
-                             [&](int kk, float v) { Pe[kk] = v; });
-          }
-        }
+        // ---- A. the entries' angular rows and radial rows
+        stage_entries<NT, AMAX, LC, true>(P, B, sEnt, chunk, ebase, n_round, sA, sR, sRd);
         __syncthreads();
         // ---- B. contraction against H: a half-warp per entry, lanes over k.
-        // Lane hl16 of a half-warp handles k = hl16 + 16 j; its k tables are
-        // loaded here rather than held through phase A.
+        // Lane hl16 of a half-warp handles k = hl16 + 16 j.
         int4 kix[KJ];
         float4 kcf[KJ];
         int klmr[KJ];
@@ -762,9 +801,18 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
           const bool act = el < n_round;
           float f_rad = 0.f, f_azi = 0.f, f_pol = 0.f;
           if (act) {
-            const int s = sEnt[ebase + el] >> 24;
-            const float *Pe = sPl + (size_t)el * PS;
-            const float *De = sD + (size_t)el * DS;
+            const int code = sEnt[ebase + el];
+            const int s = code >> 24;
+            const float *Ae = sA + (size_t)el * AS;
+            const float *Pe = Ae + O_P;
+            if (hl16 == 0) {
+              // the rotation to Cartesian uses the same angles (:1867-1871)
+              float *rot = sRot + 4 * (code & 0xffffff);
+              rot[0] = Ae[O_X];
+              rot[1] = Ae[O_SQ];
+              rot[2] = Ae[O_ER + 1];
+              rot[3] = -Ae[O_EI + 1];
+            }
             float R[AMAX], Rd[AMAX];
 #pragma unroll
             for (int n4 = 0; n4 < AMAX / 4; ++n4) {
@@ -773,7 +821,7 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
               R[4 * n4] = a.x; R[4 * n4 + 1] = a.y; R[4 * n4 + 2] = a.z; R[4 * n4 + 3] = a.w;
               Rd[4 * n4] = d.x; Rd[4 * n4 + 1] = d.y; Rd[4 * n4 + 2] = d.z; Rd[4 * n4 + 3] = d.w;
             }
-            const float amp = De[O_AMP], sfac = De[O_SF];
+            const float amp = Ae[O_AMP], sfac = Ae[O_SF];
             const float *Hs = sH + (size_t)s * AMAX;
 #pragma unroll
             for (int j = 0; j < KJ; ++j) {
@@ -783,8 +831,8 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
               const float Pk = Pe[kk];
               const float dms = kcf[j].x * Pe[kix[j].x] + kcf[j].y * Pe[kix[j].y];
               const float dvs = kcf[j].z * Pe[kix[j].z] + kcf[j].w * Pe[kix[j].w];
-              const float il = De[O_IL + l], ild = De[O_ILD + l];
-              const float er = De[O_ER + m], ei = De[O_EI + m];
+              const float il = Ae[O_IL + l], ild = Ae[O_ILD + l];
+              const float er = Ae[O_ER + m], ei = Ae[O_EI + m];
               const float ap = amp * kpr[j];
               const float u = ap * Pk * il;
               const float ur = ap * Pk * ild - sfac * u;
@@ -830,8 +878,8 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
       }
       // ---- per pair: sum its entries, rotate to Cartesian (:1864-1875)
       const int k = chunk + tid;
-      double px = 0.0, py = 0.0, pz = 0.0;
       if (k < p_end && k > p_begin) {
+        double px = 0.0, py = 0.0, pz = 0.0;
         if (my_bits != 0u) {
           double fr = 0.0, fa = 0.0, fp = 0.0;
 #pragma unroll
@@ -853,10 +901,10 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
         po[0] = px;
         po[1] = py;
         po[2] = pz;
+        self_x -= px;
+        self_y -= py;
+        self_z -= pz;
       }
-      self_x -= px;
-      self_y -= py;
-      self_z -= pz;
     }
     // the central pair is minus the sum of the others (:1875)
     block_sum3<NT>(self_x, self_y, self_z, sRed);
@@ -916,13 +964,21 @@ cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_radial(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der) {
-  if (B.n_pairs <= 0) return cudaSuccess;
-  const size_t sm = (size_t)P.off_rad + (size_t)P.n_species * SOAPB_RADSP_BYTES;
-  const int blocks = (B.n_pairs + 127) / 128;
-  if (P.amax_t == 8) k_radial<8><<<blocks, 128, sm, s>>>(P, B, do_der);
-  else k_radial<16><<<blocks, 128, sm, s>>>(P, B, do_der);
+template <int AMAX, int LC>
+static cudaError_t run_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der) {
+  const size_t sm = (size_t)P.off_rad + (size_t)P.n_species * SOAPB_RADSP_BYTES +
+                    (size_t)128 * (row_len(LC) + 1) * sizeof(float);
+  auto kern = k_pair<AMAX, LC>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  kern<<<(B.n_pairs + 127) / 128, 128, sm, s>>>(P, B, do_der);
   return cudaGetLastError();
+}
+
+cudaError_t launch_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der) {
+  if (B.n_pairs <= 0) return cudaSuccess;
+  if (P.amax_t == 8) return run_pair<8, 8>(P, B, s, do_der);
+  return run_pair<16, 12>(P, B, s, do_der);
 }
 
 // The instantiation is fixed by the definition: the host lays the constants
@@ -943,6 +999,8 @@ cudaError_t launch_contract(const DevParams &P, const DevBatch &B, const LaunchC
                             const float *keep_c, const double *keep_norm, double *pair) {
   SOAPB_DISPATCH(run_contract, P, B, cfg, soap, G, g_layout, sgn, keep_c, keep_norm, pair);
 }
+
+size_t keep_floats_per_site(const DevParams &P) { return keep_stride(P); }
 
 size_t descriptor_smem(const DevParams &P, int) {
   return make_layout(P, 128, P.amax_t, P.amax_t == 8 ? 8 : 12, 0).total;
