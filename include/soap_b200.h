@@ -191,6 +191,35 @@ int soapb_set_threads_per_site(soapb_context *ctx, int32_t threads);
 int soapb_descriptor(soapb_context *ctx, const soapb_batch *batch, double *d_soap,
                      int32_t keep_for_contract);
 
+/* Size of the static scratch array behind soapb_descriptor_noalloc (64 MiB).
+ * Every GPU that loads the library holds it until the process exits. */
+#define SOAPB_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* soapb_descriptor (without keep_for_contract) that allocates nothing: no
+ * cudaMalloc, cudaFree or allocating library routine, on any call.  It has no
+ * counterpart in the reference.  It is for callers that cannot allow a device
+ * allocation while they run -- codes that reserve the GPU's memory in their
+ * own pool at start-up, and codes whose step must not synchronise the device,
+ * which an allocation may do.  The batch's scratch (CSR offsets, mask bits,
+ * pair rows) lives in one static device array of SOAPB_NOALLOC_SCRATCH_BYTES
+ * instead of buffers that grow on demand; the context's constant tables,
+ * allocated once by soapb_create, are read as by soapb_descriptor.
+ *  - The context's device must be current.  The first call on a device looks
+ *    up the array's address (a one-time set-up); make that first call before
+ *    any stream capture.
+ *  - A batch needing more scratch than the array holds is rejected with
+ *    SOAPB_ERR_ARGUMENT and a message giving both sizes.  The need is about
+ *    (2 n_species amax + row) * 4 bytes per atom pair, with amax = 8 and a
+ *    96-float row when every alpha_max <= 8 and l_max <= 8 (577 bytes per pair
+ *    for 3 species: about 110 thousand pairs), else amax = 16 and a 128-float
+ *    row.
+ *  - All calls share the array and it keeps the last call's contents; calls
+ *    whose work overlaps on the GPU (other streams, host threads or contexts
+ *    on the same device) race on it: serialise them.
+ *  - Bad inputs are not reported through soapb_check_inputs, which reads the
+ *    context's own scratch. */
+int soapb_descriptor_noalloc(soapb_context *ctx, const soapb_batch *batch, double *d_soap);
+
 /* Force VJP on the batch of the last soapb_descriptor(keep_for_contract = 1):
  * d_pair (3, n_pairs) = sgn * G . d soap / d r, never forming soap_cart_der.
  * The pair expansions are recomputed per pair from the CSR inputs. */

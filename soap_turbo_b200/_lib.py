@@ -85,6 +85,7 @@ SIGNATURES = {
     "soapb_descriptor": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_int32]),
     "soapb_contract": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_void_p, C.c_int32,
                                  C.c_double, C.c_void_p]),
+    "soapb_descriptor_noalloc": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p]),
     "soapb_descriptor_and_vjp": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_int32,
                                            C.c_double, C.c_void_p, C.c_void_p]),
     "soapb_descriptor_fp64": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_void_p]),

@@ -152,6 +152,13 @@ class Context:
         _lib.check(self._lib.soapb_descriptor(self._h, b.c, C.c_void_p(out.data_ptr()), int(keep)))
         return out
 
+    def descriptor_noalloc(self, b: DeviceBatch, out=None):
+        """soapb_descriptor_noalloc: the descriptor with its scratch in the
+        library's static device array (no device allocation in the call)."""
+        out = self._new((b.n_sites, self.n_soap)) if out is None else out
+        _lib.check(self._lib.soapb_descriptor_noalloc(self._h, b.c, C.c_void_p(out.data_ptr())))
+        return out
+
     def contract(self, b: DeviceBatch, soap, G, sgn=1.0, g_layout=_lib.G_SITE_FASTEST, out=None):
         """pair forces (n_pairs, 3) == Fortran pair(3, n_pairs).  G is the
         reference's G(n_sites, n_soap) given as a (n_soap, n_sites) tensor

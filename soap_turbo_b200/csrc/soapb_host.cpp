@@ -878,6 +878,74 @@ int soapb_descriptor_and_vjp(soapb_context *c, const soapb_batch *b, const doubl
   return ctx_contract(c, b, d_soap, d_G, g_layout, sgn, d_pair);
 }
 
+// The descriptor with its per-call scratch carved out of the static array of
+// soapb_noalloc.cu instead of the context's growable buffers: no device memory
+// is allocated or freed here.  The kernels are soapb_descriptor's; the pair
+// kernel writes every row the site kernel reads and the prep kernel every
+// offset and mask byte, so only the work counters need clearing.
+int soapb_descriptor_noalloc(soapb_context *c, const soapb_batch *b, double *d_soap) {
+  if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
+  if (!b) return fail(SOAPB_ERR_ARGUMENT, "null batch");
+  if (b->n_sites < 0 || b->n_atom_pairs < 0) return fail(SOAPB_ERR_ARGUMENT, "negative batch size");
+  if (b->n_sites > 0 && (!b->n_neigh || !b->species_multiplicity || !b->species))
+    return fail(SOAPB_ERR_ARGUMENT, "null site arrays");
+  if (b->n_atom_pairs > 0 && (!b->mask || !b->rjs || !b->thetas || !b->phis))
+    return fail(SOAPB_ERR_ARGUMENT, "null pair arrays");
+  if (b->n_sites > 0 && !d_soap) return fail(SOAPB_ERR_ARGUMENT, "null soap output");
+  int dev = -1;
+  CU(cudaGetDevice(&dev));
+  if (dev != c->device)
+    return fail(SOAPB_ERR_ARGUMENT, "the context's device %d must be current (device %d is)", c->device, dev);
+  // sections of the scratch, each 256-byte aligned
+  const size_t np = (size_t)b->n_atom_pairs, ns = (size_t)b->n_sites;
+  auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+  const size_t o_off = 0;
+  const size_t o_bits = o_off + up(sizeof(int) * (ns + 1));
+  const size_t o_err = o_bits + up(np + 16);
+  const size_t o_ticket = o_err + 256;
+  const size_t o_rad = o_ticket + 256;
+  const size_t o_ang = o_rad + up(sizeof(float) * 2 * (size_t)c->P.amax_t * c->n_species * (np + 1));
+  const size_t need = o_ang + up(sizeof(float) * (size_t)ang_row_floats(c->P) * (np + 128));
+  if (need > (size_t)SOAPB_NOALLOC_SCRATCH_BYTES)
+    return fail(SOAPB_ERR_ARGUMENT,
+                "batch of %d sites and %d pairs needs %zu bytes of scratch; the allocation-free "
+                "descriptor holds %zu bytes (use soapb_descriptor, or split the batch)",
+                b->n_sites, b->n_atom_pairs, need, (size_t)SOAPB_NOALLOC_SCRATCH_BYTES);
+  unsigned char *base = nullptr;
+  size_t cap = 0;
+  CU(noalloc_scratch(dev, &base, &cap));
+  if (need > cap) return fail(SOAPB_ERR_ARGUMENT, "scratch array smaller than expected");
+  DevBatch B{};
+  B.n_sites = b->n_sites;
+  B.n_pairs = b->n_atom_pairs;
+  B.max_mult = b->max_species_multiplicity;
+  B.n_neigh = b->n_neigh;
+  B.species = b->species;
+  B.species_mult = b->species_multiplicity;
+  B.mask = b->mask;
+  B.rjs = b->rjs;
+  B.thetas = b->thetas;
+  B.phis = b->phis;
+  B.off = (int *)(base + o_off);
+  B.bits = (uint8_t *)(base + o_bits);
+  B.err = (unsigned long long *)(base + o_err);
+  B.ticket = (int *)(base + o_ticket);
+  B.rad = (float *)(base + o_rad);
+  B.ang = (float *)(base + o_ang);
+  int rc = run_prep(c, B);
+  if (rc) return rc;
+  DevParams P = c->P;
+  P.n_pairs = B.n_pairs;
+  P.n_sites = B.n_sites;
+  LaunchCfg cfg{pick_threads(c), c->stream, c->max_ctas};
+  CU(launch_pair(P, B, c->stream, 0));
+  c->launches += (b->n_atom_pairs > 0);
+  CU(cudaMemsetAsync(B.ticket, 0, 2 * sizeof(int), c->stream));
+  CU(launch_descriptor(P, B, cfg, d_soap, nullptr, nullptr, 0));
+  c->launches += (b->n_sites > 0);
+  return SOAPB_OK;
+}
+
 int soapb_descriptor_fp64(soapb_context *c, const soapb_batch *b, double *d_soap, double *d_cart) {
   if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
   return ctx_fp64(c, b, d_soap, d_cart);

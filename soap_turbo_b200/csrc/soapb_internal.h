@@ -118,6 +118,9 @@ cudaError_t launch_contract(const DevParams &P, const DevBatch &B, const LaunchC
 cudaError_t launch_fused(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
                          const double *G, int g_layout, double sgn, double *soap, double *pair);
 size_t descriptor_smem(const DevParams &P, int threads);
+// Device address and size of the static scratch array (soapb_noalloc.cu);
+// `device` must be current.
+cudaError_t noalloc_scratch(int device, unsigned char **addr, size_t *bytes);
 size_t contract_smem(const DevParams &P, int threads);
 size_t fused_smem(const DevParams &P, int threads);
 
