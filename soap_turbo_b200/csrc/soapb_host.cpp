@@ -441,13 +441,15 @@ int build_tables(soapb_context *c) {
   // ---- per-CTA constants of the mixed kernels (one blob, copied to shared memory)
   const int amax_t = (amax <= 8 && L <= 8) ? 8 : 16;
   const int KS = K | 1;
-  std::vector<unsigned char> blob;
-  auto put = [&](const void *src, size_t bytes) {
-    const size_t o = blob.size();
-    blob.resize((o + bytes + 15) / 16 * 16, 0);
-    if (bytes) std::memcpy(blob.data() + o, src, bytes);
+  std::vector<unsigned char> blob, blob_c;
+  auto put_in = [](std::vector<unsigned char> &b, const void *src, size_t bytes) {
+    const size_t o = b.size();
+    b.resize((o + bytes + 15) / 16 * 16, 0);
+    if (bytes) std::memcpy(b.data() + o, src, bytes);
     return (int)o;
   };
+  auto put = [&](const void *src, size_t bytes) { return put_in(blob, src, bytes); };
+  auto put_c = [&](const void *src, size_t bytes) { return put_in(blob_c, src, bytes); };
   {
     std::vector<double> Wt((size_t)c->n_species * amax_t * amax_t, 0.0);
     for (int s = 0; s < c->n_species; ++s) {
@@ -459,6 +461,7 @@ int build_tables(soapb_context *c) {
     std::vector<unsigned char> rs((size_t)c->n_species * SOAPB_RADSP_BYTES, 0);
     for (int s = 0; s < c->n_species; ++s) std::memcpy(rs.data() + (size_t)s * SOAPB_RADSP_BYTES, &P.rad[s], sizeof(RadSp));
     P.off_rad = put(rs.data(), rs.size());
+    put_c(rs.data(), rs.size());  // at offset 0 of the contract's blob
     std::vector<int4> kidx(KS, make_int4(0, 0, 0, 0));
     std::vector<float4> kcoef(KS, make_float4(0.f, 0.f, 0.f, 0.f));
     std::vector<int> klm(KS, 0);
@@ -492,14 +495,16 @@ int build_tables(soapb_context *c) {
         kidx[kk] = ix;
         kcoef[kk] = cf;
       }
-    P.off_kidx = put(kidx.data(), kidx.size() * 16);
-    P.off_kcoef = put(kcoef.data(), kcoef.size() * 16);
+    P.off_kidx = put_c(kidx.data(), kidx.size() * 16);
+    P.off_kcoef = put_c(kcoef.data(), kcoef.size() * 16);
     P.off_klm = put(klm.data(), klm.size() * 4);
     P.off_kpref = put(kpref.data(), kpref.size() * 4);
+    P.off_klm_c = put_c(klm.data(), klm.size() * 4);
+    P.off_kpref_c = put_c(kpref.data(), kpref.size() * 4);
     std::vector<int> nmap(N);
     for (int s = 0; s < c->n_species; ++s)
       for (int n = 0; n < c->alpha[s]; ++n) nmap[P.rad[s].nbeg + n] = s | (n << 8);
-    P.off_nmap = put(nmap.data(), nmap.size() * 4);
+    P.off_nmap = put_c(nmap.data(), nmap.size() * 4);
     std::vector<int> citem;
     for (int s = 0; s < c->n_species; ++s)
       for (int kk = 0; kk < K; ++kk)
@@ -516,10 +521,10 @@ int build_tables(soapb_context *c) {
     std::vector<int> hitem;
     for (auto &p : hw) hitem.push_back(p.second);
     P.n_hitem = (int)hitem.size();
-    P.off_hitem = put(hitem.data(), hitem.size() * 4);
+    P.off_hitem = put_c(hitem.data(), hitem.size() * 4);
     P.off_kept = put(kept_nnl.data(), kept_nnl.size() * 4);
     P.off_central = put(central.data(), central.size() * 8);
-    P.off_hloff = put(hl_off.data(), hl_off.size() * 4);
+    P.off_hloff = put_c(hl_off.data(), hl_off.size() * 4);
     // Y lists packed as np | q << 8 | (n == np) << 31
     if (nk >= 65536) return fail(SOAPB_ERR_ARGUMENT, "more than 65535 kept components");
     hl_packed.resize(hl_np.size());
@@ -528,7 +533,50 @@ int build_tables(soapb_context *c) {
         for (int t = hl_off[l * N + n]; t < hl_off[l * N + n + 1]; ++t)
           hl_packed[t] = (int)((unsigned)hl_np[t] | ((unsigned)hl_q[t] << 8) | ((n == hl_np[t]) ? 0x80000000u : 0u));
     P.hl_in_blob = hl_packed.size() * 4 <= 16384;
-    P.off_hl = P.hl_in_blob ? put(hl_packed.data(), hl_packed.size() * 4) : 0;
+    P.off_hl = P.hl_in_blob ? put_c(hl_packed.data(), hl_packed.size() * 4) : 0;
+    // power spectrum tiles: a column set J covering every kept (n, n') (greedy
+    // vertex cover; the species pivots for the trivial map, all n when nothing
+    // is compressed); each kept component reads P_l[row][J position]
+    {
+      std::vector<char> inJ(N, 0), covered(nk, 0);
+      for (;;) {
+        std::vector<int> deg(N, 0);
+        for (int q = 0; q < nk; ++q) {
+          if (covered[q]) continue;
+          const int n = kept_nnl[q] & 0xff, np = (kept_nnl[q] >> 8) & 0xff;
+          deg[n]++;
+          if (np != n) deg[np]++;
+        }
+        const int best = (int)(std::max_element(deg.begin(), deg.end()) - deg.begin());
+        if (deg[best] == 0) break;
+        inJ[best] = 1;
+        for (int q = 0; q < nk; ++q) {
+          const int n = kept_nnl[q] & 0xff, np = (kept_nnl[q] >> 8) & 0xff;
+          if (n == best || np == best) covered[q] = 1;
+        }
+      }
+      std::vector<int> J, jpos(N, -1);
+      for (int n = 0; n < N; ++n)
+        if (inJ[n]) {
+          jpos[n] = (int)J.size();
+          J.push_back(n);
+        }
+      P.ps_mt = (N + 15) / 16;
+      P.ps_nt = std::max(1, ((int)J.size() + 7) / 8);
+      J.resize(8 * P.ps_nt, -1);
+      const int MR = 16 * P.ps_mt, JP = 8 * P.ps_nt;
+      std::vector<int> kpos(nk);
+      for (int q = 0; q < nk; ++q) {
+        const int n = kept_nnl[q] & 0xff, np = (kept_nnl[q] >> 8) & 0xff, l = kept_nnl[q] >> 16;
+        const int row = jpos[np] >= 0 ? n : np, col = jpos[np] >= 0 ? jpos[np] : jpos[n];
+        kpos[q] = (int)((unsigned)((l * MR + row) * JP + col) | (n != np ? 0x80000000u : 0u));
+      }
+      // the tile buffer (l_max+1) x MR x JP lives in shared memory: beyond
+      // 64 KB the kernels keep the CUDA-core form of the power spectrum
+      if ((size_t)(L + 1) * MR * JP * sizeof(float) > 65536) P.ps_mt = P.ps_nt = 0;
+      P.off_psj = put(J.data(), J.size() * 4);
+      P.off_kpos = put(kpos.data(), kpos.size() * 4);
+    }
     // one-to-one compression: output q is kept component q with weight 1
     bool ident = (ns == nk) && (nz == nk);
     for (int o = 0; ident && o < ns; ++o)
@@ -538,7 +586,9 @@ int build_tables(soapb_context *c) {
   }
   P.amax_t = amax_t;
   P.blob_bytes = (int)blob.size();
+  P.blob_c_bytes = (int)blob_c.size();
   const size_t iBlob = add(blob.data(), blob.size());
+  const size_t iBlobC = add(blob_c.data(), blob_c.size());
   const size_t iHp = add(hl_packed.data(), hl_packed.size() * 4);
   int rc = c->tables.ensure(total + 256);
   if (rc) return rc;
@@ -565,6 +615,7 @@ int build_tables(soapb_context *c) {
   P.hl_fac = (const float *)at(iHf);
   P.hl_fac64 = (const double *)at(iHf64);
   P.blob = (const unsigned char *)at(iBlob);
+  P.blob_c = (const unsigned char *)at(iBlobC);
   P.hl_packed = (const int *)at(iHp);
   P.n_soap = c->n_soap;
   P.n_kept = c->n_kept;

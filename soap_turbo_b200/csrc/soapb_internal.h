@@ -58,28 +58,42 @@ struct DevParams {
   const int *hl_q;
   const float *hl_fac;
   const double *hl_fac64;
-  // Per-CTA constants of the mixed kernels, one contiguous blob copied into
-  // shared memory with 16-byte loads.  Offsets in bytes from its start.
+  // Per-CTA constants of the mixed kernels: two blobs copied into shared
+  // memory with 16-byte loads, one for the pair and descriptor kernels
+  // (blob: W blocks, then from off_rad on the descriptor's part) and one for
+  // the contract kernel (blob_c, species constants at offset 0).  Offsets in
+  // bytes from the start of the blob that holds the section.
   const unsigned char *blob;
   int blob_bytes;         // multiple of 16
+  const unsigned char *blob_c;
+  int blob_c_bytes;       // multiple of 16
   int amax_t;             // the kernel instantiation's radial block (8 or 16)
+  // in blob:
   int off_W;              // n_species blocks of amax_t^2 doubles (alpha x alpha used)
   int off_rad;            // n_species RadSp
-  int off_kidx;           // KS int4: P_l^m indices of the derivative forms
-  int off_kcoef;          // KS float4: their coefficients
   int off_klm;            // KS int: l | m << 8
   int off_kpref;          // KS float: preflm
-  int off_nmap;           // n_max int: species | local index << 8
   int off_citem;          // n_citem int: c_nlm items species | k << 4 | half << 12
-  int off_hitem;          // n_hitem int: H items n | l << 8
   int off_kept;           // n_kept int: kept_nnl
   int off_central;        // n_max double: poly3gauss central-atom term
+  // in blob_c (n_species RadSp at 0):
+  int off_kidx;           // KS int4: P_l^m indices of the derivative forms
+  int off_kcoef;          // KS float4: their coefficients
+  int off_klm_c;          // KS int: l | m << 8
+  int off_kpref_c;        // KS float: preflm
+  int off_nmap;           // n_max int: species | local index << 8
+  int off_hitem;          // n_hitem int: H items n | l << 8
   int off_hloff;          // (l_max+1)*n_max + 1 int: per (l, n) list offsets
   int off_hl;             // packed Y-list entries np | q << 8 | (n == np) << 31, when hl_in_blob
   int n_citem, n_hitem;
   int hl_in_blob;         // the packed Y lists fit in the blob (else read from hl_packed)
   const int *hl_packed;   // global copy of the packed Y lists
   int cmap_identity;      // the compression map sends kept component q to output q, weight 1
+  // power spectrum on the tensor cores: P_l[n, J] for rows n (ps_mt tiles of
+  // 16) and the column set J (ps_nt tiles of 8) that covers every kept (n, n')
+  int ps_mt, ps_nt;
+  int off_psj;            // (blob) 8 ps_nt int: the radial index of each column (-1 = padding)
+  int off_kpos;           // (blob) n_kept int: tile position (l, row, column) | (n != n') << 31
 };
 
 // Size of RadSp padded to 16 bytes, as laid out in the constants blob.

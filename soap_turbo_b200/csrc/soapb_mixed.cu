@@ -333,16 +333,16 @@ struct Layout {
   size_t C64, H, Rot, F;
   size_t X;
   size_t R, Rd, A;       // staging inside X
-  size_t C, P, S;        // per-site arrays inside X
+  size_t C, P, S, Pl;    // per-site arrays inside X
   size_t total;
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-// staged rows are 16 floats longer than the global ones: rows stay 16-byte
-// aligned for the asynchronous copies, and the two half-warps of the VJP
-// contraction, which read neighbouring rows at the same offsets, use disjoint
-// bank halves
-__host__ __device__ inline int stage_stride(int LC) { return row_len(LC) + 16; }
+// Staged rows are longer than the global ones and stay 16-byte aligned for the
+// asynchronous copies.  The contract (mode 1) pads by 16 floats so that its two
+// half-warps, which read neighbouring rows at the same offsets, use disjoint
+// bank halves; the descriptor reads one row per thread group and pads by 4.
+__host__ __device__ inline int stage_stride(int LC, int mode) { return row_len(LC) + (mode ? 16 : 4); }
 // row stride of H: the species blocks padded to AMAX, plus 4 so that 128-bit
 // loads of consecutive k rows fall in distinct banks
 __host__ __device__ inline int h_stride(int n_species, int AMAX) { return n_species * AMAX + 4; }
@@ -351,8 +351,9 @@ __host__ __device__ inline int h_stride(int n_species, int AMAX) { return n_spec
 __host__ __device__ inline size_t keep_stride(const DevParams &P) {
   return ((size_t)2 * P.n_max * (size_t)(P.k_max | 1) + 3) / 4 * 4;
 }
-__host__ __device__ inline size_t site_blob_bytes(const DevParams &P) {
-  return (size_t)(P.blob_bytes - P.off_rad);
+// bytes of constants a site kernel keeps in shared memory (mode 0 descriptor, 1 contract)
+__host__ __device__ inline size_t site_blob_bytes(const DevParams &P, int mode) {
+  return mode ? (size_t)P.blob_c_bytes : (size_t)(P.blob_bytes - P.off_rad);
 }
 
 __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AMAX, int LC, int mode) {
@@ -360,7 +361,7 @@ __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AM
   const size_t KS = (size_t)(P.k_max | 1);
   const size_t nsp = (size_t)P.n_species, CH = (size_t)NT / 2;
   const size_t nC = 2 * (size_t)P.n_max * KS;
-  size_t o = site_blob_bytes(P);
+  size_t o = site_blob_bytes(P, mode);
   L.red = o;  o += 40 * sizeof(double);
   L.ent = o;  o += (size_t)NT * nsp * sizeof(int);
   L.wcnt = o; o += (size_t)SOAPB_MAX_SPECIES * (NT / 32) * sizeof(int);
@@ -378,12 +379,16 @@ __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AM
   size_t x = o;
   L.R = x; x += CH * AMAX * sizeof(float);
   if (mode == 1) { L.Rd = x; x += CH * AMAX * sizeof(float); }
-  L.A = x; x += CH * (size_t)stage_stride(LC) * sizeof(float);
+  L.A = x; x += CH * (size_t)stage_stride(LC, mode) * sizeof(float);
   const size_t end_stage = x;
   x = o;
   L.C = x; x += nC * sizeof(float);
   L.P = x; x += (size_t)P.n_kept * sizeof(float);
   L.S = x; x += (size_t)P.n_soap * sizeof(float);
+  if (mode == 0 && P.ps_mt > 0) {
+    x = align_up(x, 16);
+    L.Pl = x; x += (size_t)(P.l_max + 1) * 16 * P.ps_mt * 8 * P.ps_nt * sizeof(float);
+  }
   const size_t end_site = x;
   o = end_stage > end_site ? end_stage : end_site;
   L.total = align_up(o, 16);
@@ -391,14 +396,15 @@ __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AM
 }
 
 template <int NT>
-__device__ __forceinline__ void copy_site_blob(const DevParams &P, unsigned char *smem) {
-  const uint4 *src = (const uint4 *)(P.blob + P.off_rad);
+__device__ __forceinline__ void copy_site_blob(const DevParams &P, unsigned char *smem, int mode) {
+  const uint4 *src = (const uint4 *)(mode ? P.blob_c : P.blob + P.off_rad);
   uint4 *dst = (uint4 *)smem;
-  for (int t = threadIdx.x; t < (int)(site_blob_bytes(P) / 16); t += NT) dst[t] = src[t];
+  for (int t = threadIdx.x; t < (int)(site_blob_bytes(P, mode) / 16); t += NT) dst[t] = src[t];
 }
 
 // Offset of a blob section inside the site kernels' shared copy.
 #define SBLOB(off) (smem + (P.off) - P.off_rad)
+#define SBLOBC(off) (smem + (P.off))
 
 __device__ __forceinline__ const RadSp &rad_of(const unsigned char *smem, const DevParams &P, int s) {
   return *(const RadSp *)(smem + (size_t)s * SOAPB_RADSP_BYTES);
@@ -432,7 +438,7 @@ __device__ __forceinline__ void stage_entries(const DevParams &P, const DevBatch
                                               int chunk, int ebase, int n_round, float *sA,
                                               float *sR, float *sRd) {
   constexpr int AW4 = row_len(LC) / 4;
-  const int AS = stage_stride(LC);
+  const int AS = stage_stride(LC, DER ? 1 : 0);
   for (int t = threadIdx.x; t < n_round * AW4; t += NT) {
     const int el = t / AW4, j4 = t - el * AW4;
     const int k = chunk + (sEnt[ebase + el] & 0xffffff);
@@ -450,6 +456,83 @@ __device__ __forceinline__ void stage_entries(const DevParams &P, const DevBatch
   cp_async_wait_all();
 }
 
+// ------------------------------------------------------------ tensor cores
+// 3xTF32 on mma.sync m16n8k8: each FP32 operand is split into a TF32 head and
+// a TF32 tail, x = hi + lo to ~22 bits, and a*b is taken as
+// lo_a*hi_b + hi_a*lo_b + hi_a*hi_b (small terms first) with FP32 accumulation.
+__device__ __forceinline__ unsigned to_tf32(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void split_tf32(float x, unsigned &hi, unsigned &lo) {
+  hi = to_tf32(x);
+  lo = to_tf32(x - __uint_as_float(hi));
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+__device__ __forceinline__ void mma_3xtf32(float (&d)[4], const float (&a)[4], const float (&b)[2]) {
+  unsigned ah[4], al[4], bh[2], bl[2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) split_tf32(a[i], ah[i], al[i]);
+#pragma unroll
+  for (int i = 0; i < 2; ++i) split_tf32(b[i], bh[i], bl[i]);
+  mma_tf32(d, al, bh);
+  mma_tf32(d, ah, bl);
+  mma_tf32(d, ah, bh);
+}
+
+// Power spectrum tiles P_l[n][j] = sum_c X_l[n][c] X_l[J_j][c] with
+// X_l[n] = (Re c_nl0, r2 Re c_nl1 .. r2 Re c_nll, Im c_nl0, r2 Im c_nl1 ..), r2 = sqrt 2,
+// i.e. P_l[n][j] = sum_m w_m Re(c_nlm conj c_{J_j}lm), w_0 = 1, w_m = 2
+// (src/soap_turbo.f90:750-795).  A warp per (l, 16-row tile, 8-column tile);
+// fragment layouts of m16n8k8: lane = 4 g + t, A rows g / g+8 and columns
+// t / t+4, B row t / t+4 and column g, D rows g / g+8 and columns 2t, 2t+1.
+template <int NT>
+__device__ __forceinline__ void ps_tensor(const DevParams &P, const float *sC, float *sPl, const int *J) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int MT = P.ps_mt, NTJ = P.ps_nt, MR = 16 * MT, JP = 8 * NTJ;
+  const int n_max = P.n_max, KS = P.k_max | 1;
+  const int per_l = MT * NTJ, n_units = (P.l_max + 1) * per_l;
+  for (int u = warp; u < n_units; u += NT / 32) {
+    const int l = u / per_l, r = u - l * per_l, mt = r / NTJ, nt = r - mt * NTJ;
+    const int kb = l * (l + 1) / 2, KL = 2 * (l + 1);
+    const int n0 = 16 * mt + g, n1 = n0 + 8, jn = J[8 * nt + g];
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int c0 = 0; c0 < KL; c0 += 8) {
+      float a[4], b[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int col = c0 + t + 4 * h;
+        float x0 = 0.f, x1 = 0.f, xj = 0.f;
+        if (col < KL) {
+          const int im = col > l, m = im ? col - l - 1 : col;
+          const float w = m ? 1.41421356237309504880f : 1.f;
+          const int off = (im ? n_max * KS : 0) + kb + m;
+          if (n0 < n_max) x0 = w * sC[n0 * KS + off];
+          if (n1 < n_max) x1 = w * sC[n1 * KS + off];
+          if (jn >= 0) xj = w * sC[jn * KS + off];
+        }
+        a[2 * h] = x0;
+        a[2 * h + 1] = x1;
+        b[h] = xj;
+      }
+      mma_3xtf32(d, a, b);
+    }
+    float *o = sPl + (size_t)(l * MR + n0) * JP + 8 * nt + 2 * t;
+    o[0] = d[0];
+    o[1] = d[1];
+    o[8 * JP] = d[2];
+    o[8 * JP + 1] = d[3];
+  }
+}
+
 // ------------------------------------------------------------ descriptor
 template <int NT, int AMAX, int LC>
 __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const DevBatch B,
@@ -459,7 +542,7 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int CH = NT / 2;
   constexpr int NH = AMAX / 2;  // radial indices per c_nlm item
-  const int AS = stage_stride(LC);
+  const int AS = stage_stride(LC, 0);
   const Layout Ly = make_layout(P, NT, AMAX, LC, 0);
   const int *klm = (const int *)SBLOB(off_klm);
   const float *kpref = (const float *)SBLOB(off_kpref);
@@ -483,7 +566,7 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
   const int KS = P.k_max | 1;
   const int n_max = P.n_max, k_max = P.k_max, nsp = P.n_species;
 
-  copy_site_blob<NT>(P, smem);
+  copy_site_blob<NT>(P, smem, 0);
   for (;;) {
     const int site = next_site<NT>(B.ticket, sSite);
     if (site >= B.n_sites) break;
@@ -584,6 +667,20 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
     // ---- C. power spectrum of the kept components (src/soap_turbo.f90:750-795)
     float *pout = P.cmap_identity ? sS : sP;
     double nrm2 = 0.0;
+    if (P.ps_mt > 0) {
+      // on the tensor cores, then gathered into the kept components with the
+      // sqrt 2 of n != n'
+      float *sPl = (float *)(smem + Ly.Pl);
+      ps_tensor<NT>(P, sC, sPl, (const int *)SBLOB(off_psj));
+      __syncthreads();
+      const int *kpos = (const int *)SBLOB(off_kpos);
+      for (int q = tid; q < P.n_kept; q += NT) {
+        const int code = kpos[q];
+        const float v = (code < 0 ? 1.41421356237309504880f : 1.f) * sPl[code & 0x7fffffff];
+        pout[q] = v;
+        nrm2 += (double)v * (double)v;
+      }
+    } else
     for (int q = tid; q < P.n_kept; q += NT) {
       const int code = kept[q];
       const int n = code & 0xff, np = (code >> 8) & 0xff, l = code >> 16;
@@ -639,19 +736,19 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
   constexpr int KJ = (KC + 15) / 16;
   constexpr int GPT = 8;  // G values a thread holds while the norm dot product is reduced
   static_assert(AMAX % 4 == 0, "vector loads of H need AMAX % 4 == 0");
-  const int AS = stage_stride(LC);
+  const int AS = stage_stride(LC, 1);
   constexpr int O_IL = row_il(LC), O_ILD = row_ild(LC), O_ER = row_er(LC), O_EI = row_ei(LC),
                 O_AMP = row_amp(LC), O_SF = row_sf(LC), O_X = row_x(LC), O_SQ = row_sq(LC),
                 O_P = row_p(LC);
   const Layout Ly = make_layout(P, NT, AMAX, LC, 1);
-  const int4 *kidx = (const int4 *)SBLOB(off_kidx);
-  const float4 *kcoef = (const float4 *)SBLOB(off_kcoef);
-  const int *klm = (const int *)SBLOB(off_klm);
-  const float *kpref = (const float *)SBLOB(off_kpref);
-  const int *nmap = (const int *)SBLOB(off_nmap);
-  const int *hitem = (const int *)SBLOB(off_hitem);
-  const int *hloff = (const int *)SBLOB(off_hloff);
-  const int *hl = P.hl_in_blob ? (const int *)SBLOB(off_hl) : P.hl_packed;
+  const int4 *kidx = (const int4 *)SBLOBC(off_kidx);
+  const float4 *kcoef = (const float4 *)SBLOBC(off_kcoef);
+  const int *klm = (const int *)SBLOBC(off_klm_c);
+  const float *kpref = (const float *)SBLOBC(off_kpref_c);
+  const int *nmap = (const int *)SBLOBC(off_nmap);
+  const int *hitem = (const int *)SBLOBC(off_hitem);
+  const int *hloff = (const int *)SBLOBC(off_hloff);
+  const int *hl = P.hl_in_blob ? (const int *)SBLOBC(off_hl) : P.hl_packed;
   double *sRed = (double *)(smem + Ly.red);
   float *sH = (float *)(smem + Ly.H);
   float *sRot = (float *)(smem + Ly.Rot);
@@ -677,7 +774,7 @@ __global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const Dev
   const int hw = tid >> 4, hl16 = tid & 15;
   float *sGu_eff = P.cmap_identity ? sGp : sGu;
 
-  copy_site_blob<NT>(P, smem);
+  copy_site_blob<NT>(P, smem, 1);
   for (;;) {
     const int site = next_site<NT>(B.ticket + 1, sSite);
     if (site >= n_sites) break;
