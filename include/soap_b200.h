@@ -182,8 +182,19 @@ int soapb_get_basis(const soapb_context *ctx, double *W, double *S);
 int soapb_n_soap(const soapb_context *ctx, int32_t *n_soap);
 /* Work on this cudaStream_t from now on (0 = legacy default stream). */
 int soapb_set_stream(soapb_context *ctx, void *stream);
-/* Work tuning: threads per site CTA (64, 128 or 256; 0 = automatic). */
+/* Work tuning: threads per site CTA (64, 128 or 256) for both site kernels;
+ * 0 returns to the autotuner's choice, or 128 before any autotuning. */
 int soapb_set_threads_per_site(soapb_context *ctx, int32_t threads);
+/* Autotuner: times the descriptor and the contract on this batch for every
+ * CTA size (64, 128, 256 threads per site) and persistent grid cap (the
+ * occupancy limit, 2 and 1 CTAs per SM), and keeps the fastest per kernel in
+ * the context.  choice (4, may be NULL) receives {descriptor threads,
+ * descriptor grid cap, contract threads, contract grid cap}, 0 meaning the
+ * occupancy limit.  A set-up call: it allocates and frees work buffers,
+ * synchronises the context's stream and discards the state kept for
+ * soapb_contract.  Results are bit-reproducible for a fixed choice; another
+ * CTA size changes the summation grouping within FP32 rounding. */
+int soapb_autotune(soapb_context *ctx, const soapb_batch *batch, int32_t *choice);
 
 /* Descriptor of one batch: d_soap (n_soap, n_sites), normalised.  With
  * keep_for_contract, the expansion coefficients c_nlm and norms stay in the

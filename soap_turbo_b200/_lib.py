@@ -91,6 +91,7 @@ SIGNATURES = {
     "soapb_descriptor_fp64": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_void_p]),
     "soapb_contract_cart_der": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_void_p,
                                           C.c_int32, C.c_double, C.c_void_p]),
+    "soapb_autotune": (C.c_int, [C.c_void_p, C.POINTER(Batch), i32p]),
     "soapb_check_inputs": (C.c_int, [C.c_void_p, i64p]),
     "soapb_launch_count": (C.c_int, [C.c_void_p, i64p]),
 }

@@ -152,6 +152,14 @@ class Context:
         _lib.check(self._lib.soapb_descriptor(self._h, b.c, C.c_void_p(out.data_ptr()), int(keep)))
         return out
 
+    def autotune(self, b: DeviceBatch) -> dict:
+        """soapb_autotune: time every CTA size and grid cap of both site
+        kernels on this batch and keep the fastest; returns the choice."""
+        ch = (C.c_int32 * 4)()
+        _lib.check(self._lib.soapb_autotune(self._h, b.c, ch))
+        return {"descriptor_threads": ch[0], "descriptor_max_ctas": ch[1],
+                "contract_threads": ch[2], "contract_max_ctas": ch[3]}
+
     def descriptor_noalloc(self, b: DeviceBatch, out=None):
         """soapb_descriptor_noalloc: the descriptor with its scratch in the
         library's static device array (no device allocation in the call)."""

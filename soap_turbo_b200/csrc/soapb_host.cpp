@@ -199,8 +199,10 @@ struct soapb_context {
   DBuf off, bits, err, keep_c, keep_norm, rad, ang, ticket;
   DBuf f64_rad, f64_rad_der, f64_ang, f64_cnk, f64_soap_un, f64_norm;
   cudaStream_t stream = 0;
-  int threads = 0;
+  int threads = 0;   // threads per site CTA chosen by the caller (0 = tuned or default)
   int max_ctas = 0;
+  // the autotuner's choice per site kernel: CTA size and persistent grid cap
+  int tune_td = 0, tune_cd = 0, tune_tc = 0, tune_cc = 0;
   int64_t launches = 0;
   int keep_valid = 0, keep_sites = 0, keep_pairs = 0;
 
@@ -742,8 +744,17 @@ int run_prep(soapb_context *c, const DevBatch &B) {
 }
 
 int pick_threads(const soapb_context *c) {
-  if (c->threads == 64 || c->threads == 128) return c->threads;
+  if (c->threads == 64 || c->threads == 128 || c->threads == 256) return c->threads;
   return 128;
+}
+
+// Launch configuration of a site kernel: the caller's CTA size if set, else
+// the autotuner's choice for that kernel, else 128 threads on the occupancy grid.
+LaunchCfg site_cfg(const soapb_context *c, bool contract) {
+  if (c->threads) return LaunchCfg{pick_threads(c), c->stream, c->max_ctas};
+  const int t = contract ? c->tune_tc : c->tune_td;
+  if (t) return LaunchCfg{t, c->stream, contract ? c->tune_cc : c->tune_cd};
+  return LaunchCfg{128, c->stream, c->max_ctas};
 }
 
 int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int keep) {
@@ -759,7 +770,7 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
     if ((rc = c->keep_c.ensure(sizeof(float) * keep_floats_per_site(P) * ((size_t)b->n_sites + 1)))) return rc;
     if ((rc = c->keep_norm.ensure(sizeof(double) * ((size_t)b->n_sites + 1)))) return rc;
   }
-  LaunchCfg cfg{pick_threads(c), c->stream, c->max_ctas};
+  LaunchCfg cfg = site_cfg(c, false);
   CU(launch_pair(P, B, c->stream, keep));
   c->launches += (b->n_atom_pairs > 0);
   CU(cudaMemsetAsync(B.ticket, 0, 2 * sizeof(int), c->stream));
@@ -785,7 +796,7 @@ int ctx_contract(soapb_context *c, const soapb_batch *b, const double *d_soap, c
   DevParams P = c->P;
   P.n_pairs = B.n_pairs;
   P.n_sites = B.n_sites;
-  LaunchCfg cfg{pick_threads(c), c->stream, c->max_ctas};
+  LaunchCfg cfg = site_cfg(c, true);
   CU(cudaMemsetAsync(B.ticket + 1, 0, sizeof(int), c->stream));
   CU(launch_contract(P, B, cfg, d_soap, d_G, g_layout, sgn, c->keep_c.as<float>(),
                      c->keep_norm.as<double>(), d_pair));
@@ -904,8 +915,8 @@ int soapb_set_stream(soapb_context *c, void *stream) {
 
 int soapb_set_threads_per_site(soapb_context *c, int32_t threads) {
   if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
-  if (threads != 0 && threads != 64 && threads != 128)
-    return fail(SOAPB_ERR_ARGUMENT, "threads per site must be 0, 64 or 128");
+  if (threads != 0 && threads != 64 && threads != 128 && threads != 256)
+    return fail(SOAPB_ERR_ARGUMENT, "threads per site must be 0, 64, 128 or 256");
   c->threads = threads;
   return SOAPB_OK;
 }
@@ -988,7 +999,7 @@ int soapb_descriptor_noalloc(soapb_context *c, const soapb_batch *b, double *d_s
   DevParams P = c->P;
   P.n_pairs = B.n_pairs;
   P.n_sites = B.n_sites;
-  LaunchCfg cfg{pick_threads(c), c->stream, c->max_ctas};
+  LaunchCfg cfg = site_cfg(c, false);
   CU(launch_pair(P, B, c->stream, 0));
   c->launches += (b->n_atom_pairs > 0);
   CU(cudaMemsetAsync(B.ticket, 0, 2 * sizeof(int), c->stream));
@@ -1024,6 +1035,81 @@ int soapb_check_inputs(soapb_context *c, int64_t *bad_pair) {
 int soapb_launch_count(const soapb_context *c, int64_t *count) {
   if (!c || !count) return fail(SOAPB_ERR_ARGUMENT, "null argument");
   *count = c->launches;
+  return SOAPB_OK;
+}
+
+int soapb_autotune(soapb_context *c, const soapb_batch *b, int32_t *choice) {
+  if (!c || !b) return fail(SOAPB_ERR_ARGUMENT, "null argument");
+  if (b->n_sites < 1) return fail(SOAPB_ERR_ARGUMENT, "autotuning needs a non-empty batch");
+  int dev = 0, sms = 0;
+  CU(cudaGetDevice(&dev));
+  CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  // work buffers of the timed calls (G = 0: the kernels' work does not depend on values)
+  struct Tmp {
+    DBuf b;
+    ~Tmp() { b.release(); }
+  } t_soap, t_G, t_pair;
+  DBuf &soap = t_soap.b, &G = t_G.b, &pair = t_pair.b;
+  int rc;
+  if ((rc = soap.ensure(sizeof(double) * (size_t)b->n_sites * c->n_soap)) ||
+      (rc = G.ensure(sizeof(double) * (size_t)b->n_sites * c->n_soap)) ||
+      (rc = pair.ensure(sizeof(double) * 3 * ((size_t)b->n_atom_pairs + 1))))
+    return rc;
+  CU(cudaMemsetAsync(G.p, 0, sizeof(double) * (size_t)b->n_sites * c->n_soap, c->stream));
+  const int saved_threads = c->threads, saved_ctas = c->max_ctas;
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  const int tcand[3] = {64, 128, 256};
+  const int ccand[3] = {0, 2 * sms, sms};
+  float best_d = 1e30f, best_c = 1e30f;
+  int td = 128, cd = 0, tc = 128, cc = 0;
+  rc = SOAPB_OK;
+  for (int it = 0; it < 3 && !rc; ++it)
+    for (int ic = 0; ic < 3 && !rc; ++ic) {
+      c->threads = tcand[it];
+      c->max_ctas = ccand[ic];
+      float md = 1e30f, mc = 1e30f;
+      for (int rep = 0; rep < 4 && !rc; ++rep) {
+        float t1 = 0.f, t2 = 0.f;
+        if (cudaEventRecord(e0, c->stream) != cudaSuccess) { rc = fail(SOAPB_ERR_CUDA, "event"); break; }
+        if ((rc = ctx_descriptor(c, b, soap.as<double>(), 1))) break;
+        if (cudaEventRecord(e1, c->stream) != cudaSuccess) { rc = fail(SOAPB_ERR_CUDA, "event"); break; }
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&t1, e0, e1) != cudaSuccess) {
+          rc = fail(SOAPB_ERR_CUDA, "event timing");
+          break;
+        }
+        cudaEventRecord(e0, c->stream);
+        if ((rc = ctx_contract(c, b, soap.as<double>(), G.as<double>(), 0, 1.0, pair.as<double>()))) break;
+        cudaEventRecord(e1, c->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&t2, e0, e1) != cudaSuccess) {
+          rc = fail(SOAPB_ERR_CUDA, "event timing");
+          break;
+        }
+        if (rep > 0) {  // the first call of a configuration is a warm-up
+          md = std::min(md, t1);
+          mc = std::min(mc, t2);
+        }
+      }
+      if (!rc && md < best_d) { best_d = md; td = tcand[it]; cd = ccand[ic]; }
+      if (!rc && mc < best_c) { best_c = mc; tc = tcand[it]; cc = ccand[ic]; }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->threads = saved_threads;
+  c->max_ctas = saved_ctas;
+  c->keep_valid = 0;  // the timed calls replaced the kept state
+  if (rc) return rc;
+  c->tune_td = td;
+  c->tune_cd = cd;
+  c->tune_tc = tc;
+  c->tune_cc = cc;
+  if (choice) {
+    choice[0] = td;
+    choice[1] = cd;
+    choice[2] = tc;
+    choice[3] = cc;
+  }
   return SOAPB_OK;
 }
 

@@ -338,6 +338,8 @@ struct Layout {
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+// entries whose rows are staged in shared memory at a time: half the CTA, at most 64
+__host__ __device__ constexpr int stage_entries_per_round(int NT) { return NT / 2 < 64 ? NT / 2 : 64; }
 // Staged rows are longer than the global ones and stay 16-byte aligned for the
 // asynchronous copies.  The contract (mode 1) pads by 16 floats so that its two
 // half-warps, which read neighbouring rows at the same offsets, use disjoint
@@ -359,7 +361,7 @@ __host__ __device__ inline size_t site_blob_bytes(const DevParams &P, int mode) 
 __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AMAX, int LC, int mode) {
   Layout L{};
   const size_t KS = (size_t)(P.k_max | 1);
-  const size_t nsp = (size_t)P.n_species, CH = (size_t)NT / 2;
+  const size_t nsp = (size_t)P.n_species, CH = (size_t)stage_entries_per_round(NT);
   const size_t nC = 2 * (size_t)P.n_max * KS;
   size_t o = site_blob_bytes(P, mode);
   L.red = o;  o += 40 * sizeof(double);
@@ -535,12 +537,12 @@ __device__ __forceinline__ void ps_tensor(const DevParams &P, const float *sC, f
 
 // ------------------------------------------------------------ descriptor
 template <int NT, int AMAX, int LC>
-__global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const DevBatch B,
+__global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, const DevBatch B,
                                                       double *__restrict__ soap_out,
                                                       float *__restrict__ keep_c,
                                                       double *__restrict__ keep_norm, int keep) {
   extern __shared__ __align__(16) unsigned char smem[];
-  constexpr int CH = NT / 2;
+  constexpr int CH = stage_entries_per_round(NT);
   constexpr int NH = AMAX / 2;  // radial indices per c_nlm item
   const int AS = stage_stride(LC, 0);
   const Layout Ly = make_layout(P, NT, AMAX, LC, 0);
@@ -724,14 +726,14 @@ __global__ void __launch_bounds__(NT, 4) k_descriptor(const DevParams P, const D
 
 // ------------------------------------------------------------ contract
 template <int NT, int AMAX, int LC>
-__global__ void __launch_bounds__(NT, 4) k_contract(const DevParams P, const DevBatch B,
+__global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, const DevBatch B,
                                                     const double *__restrict__ soap_in,
                                                     const double *__restrict__ G, int g_layout,
                                                     double sgn, const float *__restrict__ keep_c,
                                                     const double *__restrict__ keep_norm,
                                                     double *__restrict__ pair_out) {
   extern __shared__ __align__(16) unsigned char smem[];
-  constexpr int CH = NT / 2;
+  constexpr int CH = stage_entries_per_round(NT);
   constexpr int KC = (LC + 1) * (LC + 2) / 2;
   constexpr int KJ = (KC + 15) / 16;
   constexpr int GPT = 8;  // G values a thread holds while the norm dot product is reduced
@@ -1078,12 +1080,19 @@ cudaError_t launch_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, i
   return run_pair<16, 12>(P, B, s, do_der);
 }
 
-// The instantiation is fixed by the definition: the host lays the constants
-// blob out for amax_t (8 when every alpha <= 8 and l_max <= 8, else 16).
-#define SOAPB_DISPATCH(FN, ...)                          \
-  do {                                                   \
-    if (P.amax_t == 8) return FN<128, 8, 8>(__VA_ARGS__); \
-    return FN<128, 16, 12>(__VA_ARGS__);                 \
+// The radial block is fixed by the definition: the host lays the constants
+// blob out for amax_t (8 when every alpha <= 8 and l_max <= 8, else 16).  The
+// CTA size (threads per site) is a launch choice: 64, 128 or 256.
+#define SOAPB_DISPATCH_NT(FN, NT, ...)                    \
+  do {                                                    \
+    if (P.amax_t == 8) return FN<NT, 8, 8>(__VA_ARGS__);  \
+    return FN<NT, 16, 12>(__VA_ARGS__);                   \
+  } while (0)
+#define SOAPB_DISPATCH(FN, ...)                                             \
+  do {                                                                      \
+    if (cfg.threads == 64) SOAPB_DISPATCH_NT(FN, 64, __VA_ARGS__);          \
+    if (cfg.threads == 256) SOAPB_DISPATCH_NT(FN, 256, __VA_ARGS__);        \
+    SOAPB_DISPATCH_NT(FN, 128, __VA_ARGS__);                                \
   } while (0)
 
 cudaError_t launch_descriptor(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
@@ -1099,11 +1108,11 @@ cudaError_t launch_contract(const DevParams &P, const DevBatch &B, const LaunchC
 
 size_t keep_floats_per_site(const DevParams &P) { return keep_stride(P); }
 
-size_t descriptor_smem(const DevParams &P, int) {
-  return make_layout(P, 128, P.amax_t, P.amax_t == 8 ? 8 : 12, 0).total;
+size_t descriptor_smem(const DevParams &P, int threads) {
+  return make_layout(P, threads, P.amax_t, P.amax_t == 8 ? 8 : 12, 0).total;
 }
-size_t contract_smem(const DevParams &P, int) {
-  return make_layout(P, 128, P.amax_t, P.amax_t == 8 ? 8 : 12, 1).total;
+size_t contract_smem(const DevParams &P, int threads) {
+  return make_layout(P, threads, P.amax_t, P.amax_t == 8 ? 8 : 12, 1).total;
 }
 
 }  // namespace soapb
