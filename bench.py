@@ -188,7 +188,7 @@ def algorithmic_flops(w):
     n_keep = 69
     F_ps = nl.n_sites * 4.0 * K * n_keep
     F_H = nl.n_sites * 4.0 * N * N * K
-    return {"descriptor": F_cnk + F_W / 2 + F_ps, "contract": F_W / 2 + F_H + F_vjp,
+    return {"pair": F_W, "descriptor": F_cnk + F_ps, "contract": F_H + F_vjp,
             "total": F_cnk + F_W + F_ps + F_H + F_vjp}
 
 
@@ -203,7 +203,8 @@ def algorithmic_bytes(w):
     desc = nl.n_pairs * per_pair_in + nl.n_sites * (8 + 8 * n_soap + 8 * hp.n_max * K + 8)
     con = (nl.n_pairs * (per_pair_in + 24) +
            nl.n_sites * (8 + 16 * n_soap + 8 * hp.n_max * K + 8))
-    return {"descriptor": float(desc), "contract": float(con)}
+    return {"pair": float(nl.n_pairs * per_pair_in), "descriptor": float(desc),
+            "contract": float(con)}
 
 
 def hbm_peak():
@@ -213,13 +214,14 @@ def hbm_peak():
     return 6650.0
 
 
-def fp32_peak_tflops(torch):
-    """FP32 CUDA-core peak measured here: cuBLAS SGEMM with TF32 disabled."""
+def gemm_peak_tflops(torch, dtype):
+    """CUDA-core peak measured here: cuBLAS SGEMM with TF32 disabled (FP32)
+    or DGEMM (FP64), 8192^3, best of 4."""
     prev = torch.backends.cuda.matmul.allow_tf32
     torch.backends.cuda.matmul.allow_tf32 = False
     n = 8192
-    a = torch.randn(n, n, device="cuda")
-    b = torch.randn(n, n, device="cuda")
+    a = torch.randn(n, n, device="cuda", dtype=dtype)
+    b = torch.randn(n, n, device="cuda", dtype=dtype)
     for _ in range(2):
         a @ b
     torch.cuda.synchronize()
@@ -268,6 +270,8 @@ def run_ours(args):
         p = ctx.contract(b, s, G)
         return s, p
 
+    # the project's autotuner picks CTA size and persistent grid cap per site kernel
+    tune = ctx.autotune(b)
     for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize()
@@ -276,6 +280,7 @@ def run_ours(args):
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     launches0 = ctx.launch_count
+    ctx.kernel_timing(4 * K + 8)  # events around every kernel launch of the timed steps
     if ws > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -292,6 +297,10 @@ def run_ours(args):
     if ws > 1:
         torch.distributed.barrier()
     launches = ctx.launch_count - launches0
+    ktimes = ctx.kernel_times()
+    ctx.kernel_timing(0)
+    kernel_ms = {k: (ktimes[k][1] / ktimes[k][0] if ktimes[k][0] else 0.0)
+                 for k in ("prep", "pair", "descriptor", "contract")}
     t_desc = [e0.elapsed_time(e1) for e0, e1, _ in ev]
     t_con = [e1.elapsed_time(e2) for _, e1, e2 in ev]
     ms_step = (sum(t_desc) + sum(t_con)) / K
@@ -302,7 +311,8 @@ def run_ours(args):
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "envs/s", "n_gpus": ws,
                               "steps": K, "warmup": args.warmup, "ms_per_step": ms_step_max,
-                              "kernels_ms": {"descriptor": sum(t_desc) / K, "contract": sum(t_con) / K},
+                              "calls_ms": {"descriptor": sum(t_desc) / K, "contract": sum(t_con) / K},
+                              "kernel_ms": kernel_ms, "autotune": tune,
                               "quick": True, "gpu_launches": int(launches)}), flush=True)
         if ws > 1:
             torch.distributed.barrier()
@@ -371,13 +381,17 @@ def run_ours(args):
            h_ph.nbytes + h_soap.nbytes + h_G.nbytes)
     d2h = h_soap.nbytes + h_pair.nbytes
 
-    # ---- roofline of the dominant kernel (the adjoint contract)
+    # ---- roofline of the dominant kernel: the one with the largest device time
+    # per step, timed by events around each of its launches in the timed steps
     flops = algorithmic_flops(w)
     t_con_avg = sum(t_con) / K * 1e-3
     t_desc_avg = sum(t_desc) / K * 1e-3
-    dominant = "contract" if t_con_avg >= t_desc_avg else "descriptor"
-    t_dom = max(t_con_avg, t_desc_avg)
-    peak = fp32_peak_tflops(torch)
+    dominant = max(("pair", "descriptor", "contract"), key=lambda k: kernel_ms[k])
+    t_dom = kernel_ms[dominant] * 1e-3
+    peak32 = gemm_peak_tflops(torch, torch.float32)
+    peak64 = gemm_peak_tflops(torch, torch.float64)
+    # the pair kernel's arithmetic is FP64 (radial integrals, W transform)
+    peak = peak64 if dominant == "pair" else peak32
     achieved = flops[dominant] / t_dom / 1e12
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
@@ -406,7 +420,9 @@ def run_ours(args):
                                     "over groups of 4 pairs",
                        "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"site shards, {ws} GPU(s), no data-path collective"},
-            "kernels_ms": {"descriptor": t_desc_avg * 1e3, "contract": t_con_avg * 1e3},
+            "calls_ms": {"descriptor": t_desc_avg * 1e3, "contract": t_con_avg * 1e3},
+            "kernel_ms": kernel_ms,
+            "autotune": tune,
             "fp64_plain": {"value": nl.n_sites * ws / (ms64 * 1e-3), "unit": "envs/s",
                            "ms_per_step": ms64,
                            "what": "FP64 staged like the reference: radial, angular, c_nlm, power "
@@ -417,16 +433,23 @@ def run_ours(args):
                     "d2h_bytes_per_step": int(d2h),
                     "path": "soapb_get_soap(contract=1) + soapb_soap_contract on pinned host arrays"},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "fp32", "kernel": "k_" + dominant, "achieved": achieved,
+            "roofline": {"bound": "fp64" if dominant == "pair" else "fp32",
+                         "kernel": "k_" + dominant, "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": traffic,
                          "flops_per_launch": flops[dominant],
-                         "peak_source": "FP32 CUDA-core rate measured in this run (cuBLAS SGEMM "
-                                        "8192^3, TF32 off); MEASURED_PEAKS.json has HBM and bf16 "
-                                        "tensor peaks only",
-                         "hbm": {"algorithmic_bytes_per_launch": algorithmic_bytes(w)[dominant],
-                                 "algorithmic_GBps": algorithmic_bytes(w)[dominant] / t_dom / 1e9,
-                                 "peak_GBps": hbm_peak()}},
+                         "launch_ms": kernel_ms[dominant],
+                         "peak_source": "CUDA-core rate measured in this run (cuBLAS "
+                                        + ("DGEMM" if dominant == "pair" else "SGEMM, TF32 off")
+                                        + " 8192^3); MEASURED_PEAKS.json has HBM and bf16 "
+                                          "tensor peaks only",
+                         "peaks_measured_tflops": {"fp32": peak32, "fp64": peak64},
+                         "step": {"algorithmic_flops": flops["total"],
+                                  "achieved_tflops": flops["total"] / (ms_step_max * 1e-3) / 1e12,
+                                  "frac_of_fp32": flops["total"] / (ms_step_max * 1e-3) / 1e12 / peak32},
+                         "hbm": {"algorithmic_bytes_per_launch": algorithmic_bytes(w).get(dominant),
+                                 "algorithmic_GBps": (algorithmic_bytes(w).get(dominant) or 0.0) / t_dom / 1e9,
+                                 "peak_GBps": hbm_peak(), "peak_source": "measured (MEASURED_PEAKS.json)"}},
             "clocks": clk.summary(),
         }
         if ws == 1:

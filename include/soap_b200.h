@@ -260,6 +260,27 @@ int soapb_check_inputs(soapb_context *ctx, int64_t *bad_pair);
 /* Number of kernel launches issued by this context since creation. */
 int soapb_launch_count(const soapb_context *ctx, int64_t *count);
 
+/* Device timing per kernel, the context-layer form of get_soap's do_timing
+ * (src/soap_turbo.f90:139-169 argument do_timing, whose cpu_time table the
+ * drop-in layer prints as GPU times).  soapb_kernel_timing(ctx, capacity)
+ * brackets each of the next `capacity` launches of the kernels below with CUDA
+ * events on the context's stream (0 switches timing off); it is a set-up call
+ * (it creates events) and must not be made during stream capture, and no timed
+ * call may be captured.  soapb_kernel_times waits for the last timed launch,
+ * returns per kernel kind the number of timed launches and their summed device
+ * milliseconds (count[4], total_ms[4], indexed by SOAPB_KERNEL_*), the number
+ * of launches the full ring could not time (dropped, may be NULL), and empties
+ * the ring. */
+enum {
+  SOAPB_KERNEL_PREP = 0,       /* CSR offsets, mask bits, input checks     */
+  SOAPB_KERNEL_PAIR = 1,       /* FP64 radial and angular rows per pair    */
+  SOAPB_KERNEL_DESCRIPTOR = 2, /* c_nlm, power spectrum, norm per site     */
+  SOAPB_KERNEL_CONTRACT = 3,   /* force VJP per site                       */
+  SOAPB_KERNEL_KINDS = 4
+};
+int soapb_kernel_timing(soapb_context *ctx, int32_t capacity);
+int soapb_kernel_times(soapb_context *ctx, int64_t *count, double *total_ms, int64_t *dropped);
+
 #ifdef __cplusplus
 }
 #endif

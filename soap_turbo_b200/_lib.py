@@ -94,7 +94,10 @@ SIGNATURES = {
     "soapb_autotune": (C.c_int, [C.c_void_p, C.POINTER(Batch), i32p]),
     "soapb_check_inputs": (C.c_int, [C.c_void_p, i64p]),
     "soapb_launch_count": (C.c_int, [C.c_void_p, i64p]),
+    "soapb_kernel_timing": (C.c_int, [C.c_void_p, C.c_int32]),
+    "soapb_kernel_times": (C.c_int, [C.c_void_p, i64p, f64p, i64p]),
 }
+KERNEL_KINDS = ("prep", "pair", "descriptor", "contract")
 
 _lib = None
 

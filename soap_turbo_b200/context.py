@@ -135,6 +135,22 @@ class Context:
         _lib.check(self._lib.soapb_launch_count(self._h, C.byref(v)))
         return v.value
 
+    def kernel_timing(self, capacity: int):
+        """soapb_kernel_timing: time the next `capacity` kernel launches with
+        CUDA events on the context's stream (0 switches timing off)."""
+        _lib.check(self._lib.soapb_kernel_timing(self._h, int(capacity)))
+
+    def kernel_times(self) -> dict:
+        """soapb_kernel_times: {kernel: (launches, total device ms)} of the
+        launches timed since the last read, plus "dropped"."""
+        cnt = (C.c_int64 * 4)()
+        tot = (C.c_double * 4)()
+        drop = C.c_int64(0)
+        _lib.check(self._lib.soapb_kernel_times(self._h, cnt, tot, C.byref(drop)))
+        out = {k: (int(cnt[i]), float(tot[i])) for i, k in enumerate(_lib.KERNEL_KINDS)}
+        out["dropped"] = int(drop.value)
+        return out
+
     def check_inputs(self):
         bad = C.c_int64(-1)
         _lib.check(self._lib.soapb_check_inputs(self._h, C.byref(bad)))

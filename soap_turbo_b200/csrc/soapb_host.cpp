@@ -205,8 +205,23 @@ struct soapb_context {
   int tune_td = 0, tune_cd = 0, tune_tc = 0, tune_cc = 0;
   int64_t launches = 0;
   int keep_valid = 0, keep_sites = 0, keep_pairs = 0;
+  // device timing of the kernels (soapb_kernel_timing): an event pair around
+  // each timed launch, tkind[i] the kernel of pair i, tn pairs recorded so far
+  std::vector<cudaEvent_t> tev;
+  std::vector<int> tkind;
+  int tn = 0;
+  int64_t tdropped = 0;
+
+  void timing_release() {
+    for (cudaEvent_t e : tev) cudaEventDestroy(e);
+    tev.clear();
+    tkind.clear();
+    tn = 0;
+    tdropped = 0;
+  }
 
   ~soapb_context() {
+    timing_release();
     for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &rad, &ang, &ticket, &f64_rad, &f64_rad_der,
                     &f64_ang, &f64_cnk, &f64_soap_un, &f64_norm})
       b->release();
@@ -733,12 +748,35 @@ int ensure_batch(soapb_context *c, const soapb_batch *b, DevBatch &B) {
   return SOAPB_OK;
 }
 
+// Brackets one kernel launch with the timing events when timing is on; a
+// launch beyond the ring's capacity is counted as dropped.
+struct TimedLaunch {
+  soapb_context *c;
+  int slot = -1;
+  TimedLaunch(soapb_context *ctx, int kind) : c(ctx) {
+    if (c->tev.empty()) return;
+    if (2 * (size_t)c->tn + 1 >= c->tev.size()) {
+      ++c->tdropped;
+      return;
+    }
+    slot = c->tn++;
+    c->tkind[slot] = kind;
+    cudaEventRecord(c->tev[2 * (size_t)slot], c->stream);
+  }
+  ~TimedLaunch() {
+    if (slot >= 0) cudaEventRecord(c->tev[2 * (size_t)slot + 1], c->stream);
+  }
+};
+
 int run_prep(soapb_context *c, const DevBatch &B) {
   CU(cudaMemsetAsync(B.err, 0xff, sizeof(unsigned long long), c->stream));
   DevParams P = c->P;
   P.n_pairs = B.n_pairs;
   P.n_sites = B.n_sites;
-  CU(launch_prep(P, B, c->stream));
+  {
+    TimedLaunch tl(c, SOAPB_KERNEL_PREP);
+    CU(launch_prep(P, B, c->stream));
+  }
   c->launches += 1;
   return SOAPB_OK;
 }
@@ -771,11 +809,17 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
     if ((rc = c->keep_norm.ensure(sizeof(double) * ((size_t)b->n_sites + 1)))) return rc;
   }
   LaunchCfg cfg = site_cfg(c, false);
-  CU(launch_pair(P, B, c->stream, keep));
+  if (b->n_atom_pairs > 0) {
+    TimedLaunch tl(c, SOAPB_KERNEL_PAIR);
+    CU(launch_pair(P, B, c->stream, keep));
+  }
   c->launches += (b->n_atom_pairs > 0);
   CU(cudaMemsetAsync(B.ticket, 0, 2 * sizeof(int), c->stream));
-  CU(launch_descriptor(P, B, cfg, d_soap, keep ? c->keep_c.as<float>() : nullptr,
-                       keep ? c->keep_norm.as<double>() : nullptr, keep));
+  if (b->n_sites > 0) {
+    TimedLaunch tl(c, SOAPB_KERNEL_DESCRIPTOR);
+    CU(launch_descriptor(P, B, cfg, d_soap, keep ? c->keep_c.as<float>() : nullptr,
+                         keep ? c->keep_norm.as<double>() : nullptr, keep));
+  }
   c->launches += (b->n_sites > 0);
   c->keep_valid = keep;
   c->keep_sites = b->n_sites;
@@ -798,8 +842,11 @@ int ctx_contract(soapb_context *c, const soapb_batch *b, const double *d_soap, c
   P.n_sites = B.n_sites;
   LaunchCfg cfg = site_cfg(c, true);
   CU(cudaMemsetAsync(B.ticket + 1, 0, sizeof(int), c->stream));
-  CU(launch_contract(P, B, cfg, d_soap, d_G, g_layout, sgn, c->keep_c.as<float>(),
-                     c->keep_norm.as<double>(), d_pair));
+  if (b->n_sites > 0) {
+    TimedLaunch tl(c, SOAPB_KERNEL_CONTRACT);
+    CU(launch_contract(P, B, cfg, d_soap, d_G, g_layout, sgn, c->keep_c.as<float>(),
+                       c->keep_norm.as<double>(), d_pair));
+  }
   c->launches += (b->n_sites > 0);
   return SOAPB_OK;
 }
@@ -1035,6 +1082,43 @@ int soapb_check_inputs(soapb_context *c, int64_t *bad_pair) {
 int soapb_launch_count(const soapb_context *c, int64_t *count) {
   if (!c || !count) return fail(SOAPB_ERR_ARGUMENT, "null argument");
   *count = c->launches;
+  return SOAPB_OK;
+}
+
+int soapb_kernel_timing(soapb_context *c, int32_t capacity) {
+  if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
+  if (capacity < 0 || capacity > (1 << 20)) return fail(SOAPB_ERR_ARGUMENT, "timing capacity out of range");
+  c->timing_release();
+  if (capacity == 0) return SOAPB_OK;
+  c->tev.resize(2 * (size_t)capacity + 2, nullptr);
+  c->tkind.assign((size_t)capacity + 1, 0);
+  for (cudaEvent_t &e : c->tev) {
+    const cudaError_t st = cudaEventCreate(&e);
+    if (st != cudaSuccess) {
+      e = nullptr;
+      c->timing_release();
+      return cuda_fail(st, "cudaEventCreate");
+    }
+  }
+  return SOAPB_OK;
+}
+
+int soapb_kernel_times(soapb_context *c, int64_t *count, double *total_ms, int64_t *dropped) {
+  if (!c || !count || !total_ms) return fail(SOAPB_ERR_ARGUMENT, "null argument");
+  for (int k = 0; k < SOAPB_KERNEL_KINDS; ++k) {
+    count[k] = 0;
+    total_ms[k] = 0.0;
+  }
+  if (dropped) *dropped = c->tdropped;
+  if (c->tn > 0) CU(cudaEventSynchronize(c->tev[2 * (size_t)c->tn - 1]));
+  for (int i = 0; i < c->tn; ++i) {
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, c->tev[2 * (size_t)i], c->tev[2 * (size_t)i + 1]));
+    count[c->tkind[i]] += 1;
+    total_ms[c->tkind[i]] += ms;
+  }
+  c->tn = 0;
+  c->tdropped = 0;
   return SOAPB_OK;
 }
 
