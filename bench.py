@@ -277,33 +277,36 @@ def run_ours(args):
     torch.cuda.synchronize()
 
     K = args.steps
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-           torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(K)]
     launches0 = ctx.launch_count
-    ctx.kernel_timing(4 * K + 8)  # events around every kernel launch of the timed steps
     if ws > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     with ClockSampler(dev.index) as clk:
         for i in range(K):
             flush.fill_(float(i))
-            e0, e1, e2 = ev[i]
+            e0, e1 = ev[i]
             e0.record(stream)
-            s = ctx.descriptor(b, keep=True)
+            s, p = step()
             e1.record(stream)
-            p = ctx.contract(b, s, G)
-            e2.record(stream)
         torch.cuda.synchronize()
     if ws > 1:
         torch.distributed.barrier()
     launches = ctx.launch_count - launches0
+
+    # per-kernel device times: the same K steps again with CUDA events around
+    # every kernel launch (kept out of the headline loop: each event between two
+    # dependent kernels costs the step ~2 us)
+    ctx.kernel_timing(4 * K + 8)
+    for i in range(K):
+        flush.fill_(float(i))
+        step()
     ktimes = ctx.kernel_times()
     ctx.kernel_timing(0)
     kernel_ms = {k: (ktimes[k][1] / ktimes[k][0] if ktimes[k][0] else 0.0)
                  for k in ("prep", "pair", "descriptor", "contract")}
-    t_desc = [e0.elapsed_time(e1) for e0, e1, _ in ev]
-    t_con = [e1.elapsed_time(e2) for _, e1, e2 in ev]
-    ms_step = (sum(t_desc) + sum(t_con)) / K
+    ms_step = sum(e0.elapsed_time(e1) for e0, e1 in ev) / K
     ms_step_max = shard.max_over_ranks(ms_step, device=dev)
     value = ws * nl.n_sites / (ms_step_max * 1e-3)
 
@@ -311,7 +314,6 @@ def run_ours(args):
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "envs/s", "n_gpus": ws,
                               "steps": K, "warmup": args.warmup, "ms_per_step": ms_step_max,
-                              "calls_ms": {"descriptor": sum(t_desc) / K, "contract": sum(t_con) / K},
                               "kernel_ms": kernel_ms, "autotune": tune,
                               "quick": True, "gpu_launches": int(launches)}), flush=True)
         if ws > 1:
@@ -384,8 +386,6 @@ def run_ours(args):
     # ---- roofline of the dominant kernel: the one with the largest device time
     # per step, timed by events around each of its launches in the timed steps
     flops = algorithmic_flops(w)
-    t_con_avg = sum(t_con) / K * 1e-3
-    t_desc_avg = sum(t_desc) / K * 1e-3
     dominant = max(("pair", "descriptor", "contract"), key=lambda k: kernel_ms[k])
     t_dom = kernel_ms[dominant] * 1e-3
     peak32 = gemm_peak_tflops(torch, torch.float32)
@@ -420,8 +420,8 @@ def run_ours(args):
                                     "over groups of 4 pairs",
                        "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"site shards, {ws} GPU(s), no data-path collective"},
-            "calls_ms": {"descriptor": t_desc_avg * 1e3, "contract": t_con_avg * 1e3},
             "kernel_ms": kernel_ms,
+            "kernel_ms_how": "a second pass of the K steps with CUDA events around each kernel launch",
             "autotune": tune,
             "fp64_plain": {"value": nl.n_sites * ws / (ms64 * 1e-3), "unit": "envs/s",
                            "ms_per_step": ms64,

@@ -233,11 +233,12 @@ int soapb_descriptor_noalloc(soapb_context *ctx, const soapb_batch *batch, doubl
 
 /* Force VJP on the batch of the last soapb_descriptor(keep_for_contract = 1):
  * d_pair (3, n_pairs) = sgn * G . d soap / d r, never forming soap_cart_der.
- * The pair expansions are recomputed per pair from the CSR inputs. */
+ * It reads the pair expansions and c_nlm that descriptor call kept, as the
+ * reference's soap_contract reads the state its get_soap kept. */
 int soapb_contract(soapb_context *ctx, const soapb_batch *batch, const double *d_soap,
                    const double *d_G, int32_t g_layout, double sgn, double *d_pair);
 
-/* Descriptor and force VJP in one kernel, for an upstream gradient known up
+/* Descriptor and force VJP in one call, for an upstream gradient known up
  * front (e.g. a linear model): same outputs as the two calls above. */
 int soapb_descriptor_and_vjp(soapb_context *ctx, const soapb_batch *batch, const double *d_G,
                              int32_t g_layout, double sgn, double *d_soap, double *d_pair);

@@ -196,7 +196,7 @@ struct soapb_context {
   // device tables
   DBuf tables;
   // arena
-  DBuf off, bits, err, keep_c, keep_norm, rad, ang, ticket;
+  DBuf off, bits, err, keep_c, keep_norm, rad, ang;
   DBuf f64_rad, f64_rad_der, f64_ang, f64_cnk, f64_soap_un, f64_norm;
   cudaStream_t stream = 0;
   int threads = 0;   // threads per site CTA chosen by the caller (0 = tuned or default)
@@ -222,7 +222,7 @@ struct soapb_context {
 
   ~soapb_context() {
     timing_release();
-    for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &rad, &ang, &ticket, &f64_rad, &f64_rad_der,
+    for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &rad, &ang, &f64_rad, &f64_rad_der,
                     &f64_ang, &f64_cnk, &f64_soap_un, &f64_norm})
       b->release();
   }
@@ -723,8 +723,7 @@ int ensure_batch(soapb_context *c, const soapb_batch *b, DevBatch &B) {
   int rc;
   if ((rc = c->off.ensure(sizeof(int) * ((size_t)b->n_sites + 1)))) return rc;
   if ((rc = c->bits.ensure((size_t)b->n_atom_pairs + 16))) return rc;
-  if ((rc = c->err.ensure(16))) return rc;
-  if ((rc = c->ticket.ensure(16))) return rc;
+  if ((rc = c->err.ensure(8 * (size_t)prep_err_words(b->n_sites)))) return rc;
   if ((rc = c->rad.ensure(sizeof(float) * 2 * (size_t)c->P.amax_t * c->n_species * ((size_t)b->n_atom_pairs + 1))))
     return rc;
   if ((rc = c->ang.ensure(sizeof(float) * (size_t)ang_row_floats(c->P) * ((size_t)b->n_atom_pairs + 128))))
@@ -744,7 +743,14 @@ int ensure_batch(soapb_context *c, const soapb_batch *b, DevBatch &B) {
   B.err = c->err.as<unsigned long long>();
   B.rad = c->rad.as<float>();
   B.ang = c->ang.as<float>();
-  B.ticket = c->ticket.as<int>();
+  B.ticket = (int *)(B.err + prep_err_words(b->n_sites) - 1);
+  return SOAPB_OK;
+}
+
+// Clears the error word, the scan state and the work counters before a prep
+// launch (the FP64 path's k_prep, or the mixed path's k_pair): one memset.
+int clear_prep_state(soapb_context *c, const DevBatch &B) {
+  CU(cudaMemsetAsync(B.err, 0, 8 * (size_t)prep_err_words(B.n_sites), c->stream));
   return SOAPB_OK;
 }
 
@@ -768,8 +774,9 @@ struct TimedLaunch {
   }
 };
 
-int run_prep(soapb_context *c, const DevBatch &B) {
-  CU(cudaMemsetAsync(B.err, 0xff, sizeof(unsigned long long), c->stream));
+int run_prep(soapb_context *c, DevBatch &B) {
+  int rc = clear_prep_state(c, B);
+  if (rc) return rc;
   DevParams P = c->P;
   P.n_pairs = B.n_pairs;
   P.n_sites = B.n_sites;
@@ -800,7 +807,7 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
   int rc = ensure_batch(c, b, B);
   if (rc) return rc;
   if (b->n_sites > 0 && !d_soap) return fail(SOAPB_ERR_ARGUMENT, "null soap output");
-  if ((rc = run_prep(c, B))) return rc;
+  if ((rc = clear_prep_state(c, B))) return rc;
   DevParams P = c->P;
   P.n_pairs = B.n_pairs;
   P.n_sites = B.n_sites;
@@ -809,12 +816,13 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
     if ((rc = c->keep_norm.ensure(sizeof(double) * ((size_t)b->n_sites + 1)))) return rc;
   }
   LaunchCfg cfg = site_cfg(c, false);
-  if (b->n_atom_pairs > 0) {
+  // the pair kernel also scans n_neigh into the CSR offsets, packs the mask
+  // and checks the inputs
+  if (b->n_atom_pairs > 0 || b->n_sites > 0) {
     TimedLaunch tl(c, SOAPB_KERNEL_PAIR);
     CU(launch_pair(P, B, c->stream, keep));
+    c->launches += 1;
   }
-  c->launches += (b->n_atom_pairs > 0);
-  CU(cudaMemsetAsync(B.ticket, 0, 2 * sizeof(int), c->stream));
   if (b->n_sites > 0) {
     TimedLaunch tl(c, SOAPB_KERNEL_DESCRIPTOR);
     CU(launch_descriptor(P, B, cfg, d_soap, keep ? c->keep_c.as<float>() : nullptr,
@@ -841,7 +849,6 @@ int ctx_contract(soapb_context *c, const soapb_batch *b, const double *d_soap, c
   P.n_pairs = B.n_pairs;
   P.n_sites = B.n_sites;
   LaunchCfg cfg = site_cfg(c, true);
-  CU(cudaMemsetAsync(B.ticket + 1, 0, sizeof(int), c->stream));
   if (b->n_sites > 0) {
     TimedLaunch tl(c, SOAPB_KERNEL_CONTRACT);
     CU(launch_contract(P, B, cfg, d_soap, d_G, g_layout, sgn, c->keep_c.as<float>(),
@@ -1011,8 +1018,7 @@ int soapb_descriptor_noalloc(soapb_context *c, const soapb_batch *b, double *d_s
   const size_t o_off = 0;
   const size_t o_bits = o_off + up(sizeof(int) * (ns + 1));
   const size_t o_err = o_bits + up(np + 16);
-  const size_t o_ticket = o_err + 256;
-  const size_t o_rad = o_ticket + 256;
+  const size_t o_rad = o_err + up(8 * (size_t)prep_err_words(b->n_sites));
   const size_t o_ang = o_rad + up(sizeof(float) * 2 * (size_t)c->P.amax_t * c->n_species * (np + 1));
   const size_t need = o_ang + up(sizeof(float) * (size_t)ang_row_floats(c->P) * (np + 128));
   if (need > (size_t)SOAPB_NOALLOC_SCRATCH_BYTES)
@@ -1038,19 +1044,20 @@ int soapb_descriptor_noalloc(soapb_context *c, const soapb_batch *b, double *d_s
   B.off = (int *)(base + o_off);
   B.bits = (uint8_t *)(base + o_bits);
   B.err = (unsigned long long *)(base + o_err);
-  B.ticket = (int *)(base + o_ticket);
+  B.ticket = (int *)(B.err + prep_err_words(b->n_sites) - 1);
   B.rad = (float *)(base + o_rad);
   B.ang = (float *)(base + o_ang);
-  int rc = run_prep(c, B);
+  int rc = clear_prep_state(c, B);
   if (rc) return rc;
   DevParams P = c->P;
   P.n_pairs = B.n_pairs;
   P.n_sites = B.n_sites;
   LaunchCfg cfg = site_cfg(c, false);
-  CU(launch_pair(P, B, c->stream, 0));
-  c->launches += (b->n_atom_pairs > 0);
-  CU(cudaMemsetAsync(B.ticket, 0, 2 * sizeof(int), c->stream));
-  CU(launch_descriptor(P, B, cfg, d_soap, nullptr, nullptr, 0));
+  if (b->n_atom_pairs > 0 || b->n_sites > 0) {
+    CU(launch_pair(P, B, c->stream, 0));
+    c->launches += 1;
+  }
+  if (b->n_sites > 0) CU(launch_descriptor(P, B, cfg, d_soap, nullptr, nullptr, 0));
   c->launches += (b->n_sites > 0);
   return SOAPB_OK;
 }
@@ -1070,11 +1077,13 @@ int soapb_check_inputs(soapb_context *c, int64_t *bad_pair) {
   if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
   if (bad_pair) *bad_pair = -1;
   if (!c->err.p) return SOAPB_OK;
-  unsigned long long v = 0;
-  CU(cudaMemcpyAsync(&v, c->err.p, sizeof v, cudaMemcpyDeviceToHost, c->stream));
+  unsigned long long w = 0;
+  CU(cudaMemcpyAsync(&w, c->err.p, sizeof w, cudaMemcpyDeviceToHost, c->stream));
   CU(cudaStreamSynchronize(c->stream));
+  const unsigned long long v = prep_error_code(w);
   if (v == ~0ull) return SOAPB_OK;
-  if (v == (1ull << 62)) return fail(SOAPB_ERR_INPUT, "n_neigh is negative or does not sum to n_atom_pairs");
+  if (v == (1ull << 33)) return fail(SOAPB_ERR_INPUT, "n_neigh is negative or does not sum to n_atom_pairs");
+  if (v > (1ull << 33)) return fail(SOAPB_ERR_CUDA, "the CSR offset scan gave up waiting for a preceding tile");
   if (bad_pair) *bad_pair = (int64_t)v;
   return fail(SOAPB_ERR_INPUT, "non-finite or negative pair input at pair %llu", v);
 }

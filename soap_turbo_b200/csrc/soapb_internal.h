@@ -107,10 +107,13 @@ struct DevBatch {
   const double *rjs, *thetas, *phis;
   int *off;              // n_sites + 1 (prep output)
   uint8_t *bits;         // n_pairs: mask bits (prep output)
-  unsigned long long *err;  // first bad pair index + 1 (0 = none)
+  unsigned long long *err;  // prep_err_words(n_sites) words, cleared before each prep launch:
+                            // the first input error, the prep scan's state and (last
+                            // word) the site kernels' work counters
   float *rad;            // (n_pairs, n_species, 2, amax_t): 4 pi R_n and its r-derivative
   float *ang;            // (n_pairs, ang_row): the pair's angular row (see soapb_mixed.cu)
-  int *ticket;           // work counters of the persistent site kernels
+  int *ticket;           // work counters of the persistent site kernels, in the last word
+                         // of err (the kernels put them back to 0 when they finish)
 };
 
 // Kernel launchers (soapb_mixed.cu, soapb_fp64.cu)
@@ -121,6 +124,12 @@ struct LaunchCfg {
   int max_ctas;          // persistent grid cap (0 = from the occupancy)
 };
 cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s);
+// 64-bit words of DevBatch::err for a batch of n_sites; the launcher's caller
+// clears them before each prep launch
+int prep_err_words(int n_sites);
+// The error code in err[0]: a bad pair's index, a value >= 2^33 for CSR and
+// scan failures, or all ones when the launch found no error.
+unsigned long long prep_error_code(unsigned long long word);
 cudaError_t launch_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der);
 int ang_row_floats(const DevParams &P);
 size_t keep_floats_per_site(const DevParams &P);
@@ -129,14 +138,11 @@ cudaError_t launch_descriptor(const DevParams &P, const DevBatch &B, const Launc
 cudaError_t launch_contract(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
                             const double *soap, const double *G, int g_layout, double sgn,
                             const float *keep_c, const double *keep_norm, double *pair);
-cudaError_t launch_fused(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
-                         const double *G, int g_layout, double sgn, double *soap, double *pair);
 size_t descriptor_smem(const DevParams &P, int threads);
 // Device address and size of the static scratch array (soapb_noalloc.cu);
 // `device` must be current.
 cudaError_t noalloc_scratch(int device, unsigned char **addr, size_t *bytes);
 size_t contract_smem(const DevParams &P, int threads);
-size_t fused_smem(const DevParams &P, int threads);
 
 // Plain FP64 staged path
 struct Fp64Work {

@@ -31,61 +31,144 @@ namespace soapb {
 constexpr double kFourPi = 12.566370614359172954;
 
 // ------------------------------------------------------------------ prep
-// Block 0 scans n_neigh into CSR offsets; the other blocks pack the mask into
-// per-pair species bits and check the pair inputs.
-__global__ void k_prep(DevBatch B, int n_species) {
-  if (blockIdx.x == 0) {
-    __shared__ int warp_tot[32];
-    __shared__ int carry;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (int base = 0; base < B.n_sites; base += blockDim.x) {
-      const int i = base + threadIdx.x;
-      int v = (i < B.n_sites) ? B.n_neigh[i] : 0;
-      if (v < 0) {
-        atomicMin(B.err, (unsigned long long)(1ull << 62));
-        v = 0;
-      }
-      int x = v;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-      }
-      if (lane == 31) warp_tot[warp] = x;
-      __syncthreads();
-      if (warp == 0) {
-        int t = (lane < (int)(blockDim.x >> 5)) ? warp_tot[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int y = __shfl_up_sync(0xffffffffu, t, o);
-          if (lane >= o) t += y;
-        }
-        warp_tot[lane] = t;  // inclusive over warps
-      }
-      __syncthreads();
-      const int excl = carry + (warp > 0 ? warp_tot[warp - 1] : 0) + x - v;
-      if (i < B.n_sites) B.off[i] = excl;
-      __syncthreads();
-      if (threadIdx.x == blockDim.x - 1) carry = excl + v;
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-      B.off[B.n_sites] = carry;
-      if (carry != B.n_pairs) atomicMin(B.err, (unsigned long long)(1ull << 62));
-    }
+// CSR offsets, per-pair mask bits and input checks.  DevBatch::err holds
+// prep_err_words(n_sites) 64-bit words, all cleared by one memset before the
+// prep launch:
+//   err[0]     the first input error: 2^34 - code under atomicMax, so the
+//              smallest code wins (0 = none); code = a bad pair's index, or
+//              kErrCsr / kErrScan;
+//   err[1]     the scan's tile counter (low 32 bits);
+//   err[2 + t] scan tile t's status: flag << 32 | sum, flag 1 = the tile's own
+//              sum, 2 = the inclusive prefix up to the tile (0 = not yet);
+//   the last word: the two work counters of the persistent site kernels.
+// n_neigh is scanned in tiles of 2048 sites with a decoupled look-back: each
+// tile publishes its sum, then walks back over its predecessors until it meets
+// an inclusive prefix.  A tile takes its index from the counter, so every
+// predecessor it waits for has already started; the wait is bounded.
+constexpr int kScanTile = 2048;
+constexpr unsigned long long kErrCsr = 1ull << 33;        // n_neigh negative or sum != n_pairs
+constexpr unsigned long long kErrScan = (1ull << 33) + 1;  // look-back wait gave up
+constexpr unsigned long long kErrTop = 1ull << 34;
+
+__host__ __device__ inline int prep_scan_tiles(int n_sites) { return (n_sites + kScanTile - 1) / kScanTile; }
+
+__device__ __forceinline__ void prep_error(const DevBatch &B, unsigned long long code) {
+  atomicMax(B.err, kErrTop - code);
+}
+
+// One scan tile per calling block (NTH threads); sv: kScanTile ints of shared memory.
+template <int NTH>
+__device__ __forceinline__ void prep_scan_tile(const DevBatch &B, int scan_tiles, int *sv) {
+  constexpr int ITEMS = kScanTile / NTH;
+  __shared__ int wtot[NTH / 32];
+  __shared__ int s_tile, s_excl;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  unsigned *counter = (unsigned *)(B.err + 1);
+  unsigned long long *status = B.err + 2;
+  if (tid == 0) s_tile = (int)atomicAdd(counter, 1u);
+  __syncthreads();
+  const int tile = s_tile;
+  if (tile >= scan_tiles) {
+    if (tid == 0) prep_error(B, kErrScan);
     return;
   }
-  const int k = (blockIdx.x - 1) * blockDim.x + threadIdx.x;
-  if (k >= B.n_pairs) return;
+  const int base = tile * kScanTile;
+  bool bad = false;
+#pragma unroll
+  for (int j = 0; j < ITEMS; ++j) {
+    const int i = base + j * NTH + tid;
+    int v = i < B.n_sites ? B.n_neigh[i] : 0;
+    if (v < 0) {
+      bad = true;
+      v = 0;
+    }
+    sv[j * NTH + tid] = v;
+  }
+  if (bad) prep_error(B, kErrCsr);
+  __syncthreads();
+  int loc[ITEMS], sum = 0;
+#pragma unroll
+  for (int j = 0; j < ITEMS; ++j) {
+    loc[j] = sum;
+    sum += sv[tid * ITEMS + j];
+  }
+  int x = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wtot[warp] = x;
+  __syncthreads();
+  int wpre = 0, total = 0;
+#pragma unroll
+  for (int w = 0; w < NTH / 32; ++w) {
+    if (w < warp) wpre += wtot[w];
+    total += wtot[w];
+  }
+  const int tpre = wpre + x - sum;  // exclusive prefix of this thread's items in the tile
+  if (tid == 0) {
+    volatile unsigned long long *vs = status;
+    long long excl = 0;
+    if (tile == 0) {
+      vs[0] = (2ull << 32) | (unsigned)total;
+    } else {
+      vs[tile] = (1ull << 32) | (unsigned)total;
+      int j = tile - 1, spins = 0;
+      while (j >= 0) {
+        const unsigned long long w = vs[j];
+        const unsigned f = (unsigned)(w >> 32);
+        if (f == 1u || f == 2u) {
+          excl += (unsigned)w;
+          if (f == 2u) break;
+          --j;
+        } else if (++spins > (1 << 20)) {
+          prep_error(B, kErrScan);
+          break;
+        } else {
+          __nanosleep(64);
+        }
+      }
+      vs[tile] = (2ull << 32) | (unsigned)(excl + total);
+    }
+    s_excl = (int)excl;
+  }
+  __syncthreads();
+  const int e0 = s_excl + tpre;
+#pragma unroll
+  for (int j = 0; j < ITEMS; ++j) {
+    const int i = base + tid * ITEMS + j;
+    if (i < B.n_sites) B.off[i] = e0 + loc[j];
+  }
+  if (tile == scan_tiles - 1 && tid == 0) {
+    const long long all = (long long)s_excl + total;
+    B.off[B.n_sites] = (int)all;
+    if (all != (long long)B.n_pairs) prep_error(B, kErrCsr);
+  }
+}
+
+// The species bits of pair k from the reference's mask(n_pairs, n_species),
+// written to B.bits, with the pair's inputs checked.
+__device__ __forceinline__ unsigned prep_pair(const DevBatch &B, int k, int n_species) {
   unsigned bits = 0;
   for (int s = 0; s < n_species; ++s)
     if (B.mask[(size_t)s * B.n_pairs + k]) bits |= 1u << s;
   B.bits[k] = (uint8_t)bits;
   const double r = B.rjs[k], t = B.thetas[k], f = B.phis[k];
-  if (!(r >= 0.0) || !isfinite(r) || !isfinite(t) || !isfinite(f))
-    atomicMin(B.err, (unsigned long long)k);
+  if (!(r >= 0.0) || !isfinite(r) || !isfinite(t) || !isfinite(f)) prep_error(B, (unsigned long long)k);
+  return bits;
+}
+
+// The prep kernel of the plain FP64 path: scan tiles first, then one thread per pair.
+constexpr int kPrepThreads = 256;
+__global__ void __launch_bounds__(kPrepThreads) k_prep(DevBatch B, int n_species, int scan_tiles) {
+  if ((int)blockIdx.x < scan_tiles) {
+    __shared__ int sv[kScanTile];
+    prep_scan_tile<kPrepThreads>(B, scan_tiles, sv);
+    return;
+  }
+  const int k = ((int)blockIdx.x - scan_tiles) * kPrepThreads + threadIdx.x;
+  if (k < B.n_pairs) prep_pair(B, k, n_species);
 }
 
 // ------------------------------------------------------------- utilities
@@ -148,20 +231,23 @@ __device__ __forceinline__ void block_sum3(double &a, double &b, double &c, doub
 }
 
 // Builds the entry list of one chunk of NT pairs.  Returns, per thread, the
-// radial-valid species bits of its own pair and (in slot[]) the entry slot of
-// each of them.  Shared: ent[] = chunk-local pair | species << 24, and
-// sbase/scnt per species.
+// radial-valid species bits of its own pair, its distance (my_r) and (in
+// slot[]) the entry slot of each of them.  Shared: ent[] = chunk-local pair |
+// species << 24, and sbase/scnt per species.
 template <int NT>
 __device__ __forceinline__ int build_entries(const DevParams &P, const DevBatch &B, int p_begin,
                                              int chunk, int p_end, bool vjp, int *ent, int *wcnt,
                                              int *sbase, int *scnt, int *n_ent_out,
-                                             int (&slot)[SOAPB_MAX_SPECIES], unsigned &my_bits) {
+                                             int (&slot)[SOAPB_MAX_SPECIES], unsigned &my_bits,
+                                             double &my_r) {
   constexpr int NW = NT / 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int k = chunk + tid;
   unsigned rb = 0;
+  my_r = 1.0;
   if (k < p_end) {
     const double r = B.rjs[k];
+    my_r = r;
     const unsigned bits = B.bits[k];
     const int j = k - p_begin;
 #pragma unroll
@@ -249,8 +335,13 @@ int ang_row_floats(const DevParams &P) { return row_len(P.amax_t == 8 ? 8 : 12);
 // descriptor call that kept its state, as the reference keeps the radial and
 // angular expansions between get_soap and soap_contract.
 template <int AMAX, int LC>
-__global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch B, int do_der) {
+__global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch B, int do_der,
+                                              int scan_tiles) {
   extern __shared__ __align__(16) unsigned char smem[];
+  if ((int)blockIdx.x < scan_tiles) {
+    prep_scan_tile<128>(B, scan_tiles, (int *)smem);
+    return;
+  }
   constexpr int AW = row_len(LC);
   // odd stride in shared memory: each thread fills its own row, so lanes must
   // not all map to one bank
@@ -259,10 +350,10 @@ __global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch 
   for (int t = threadIdx.x; t < head; t += 128) ((uint4 *)smem)[t] = ((const uint4 *)P.blob)[t];
   float *rows = (float *)(smem + (size_t)head * 16);
   __syncthreads();
-  const int k0 = blockIdx.x * 128;
+  const int k0 = ((int)blockIdx.x - scan_tiles) * 128;
   const int k = k0 + threadIdx.x;
   if (k < B.n_pairs) {
-    const unsigned bits = B.bits[k];
+    const unsigned bits = prep_pair(B, k, P.n_species);
     const double r = B.rjs[k];
     if (bits != 0u && r < P.rcut_max) {
       float *row = rows + threadIdx.x * AWS;
@@ -278,19 +369,14 @@ __global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch 
       row[row_sq(LC)] = (float)sq;
       float *Pr = row + row_p(LC);
       plm_rows<LC + 1>(P.l_max + (do_der ? 1 : 0), (float)x, (float)sq, [&](int kk, float v) { Pr[kk] = v; });
-      // the radial expansion of each valid species; the pair's position in its
-      // CSR row decides the central-atom terms (:342-355)
-      int lo = 0, hi = B.n_sites;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (B.off[mid] <= k) lo = mid; else hi = mid;
-      }
-      const bool is_self = (B.off[lo] == k);
+      // the radial expansion of each species in range, as for a neighbour: the
+      // central pair's expansion (:342-355) differs only by the factor
+      // central_weight (:638-646), which the descriptor applies to that entry
       const double *sW = (const double *)(smem + P.off_W);
       unsigned todo = 0u;
       for (int s = 0; s < P.n_species; ++s) {
         const RadSp &RS = *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
-        if (((bits >> s) & 1u) && r < RS.rcut_hard && (!is_self || RS.do_central)) todo |= 1u << s;
+        if (((bits >> s) & 1u) && r < RS.rcut_hard) todo |= 1u << s;
       }
       // species are data, not control flow: lanes of different species share
       // one expansion call
@@ -299,7 +385,7 @@ __global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch 
         todo &= todo - 1u;
         const RadSp &RS = *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
         double val[AMAX], der[AMAX];
-        radial_entry<AMAX>(P, RS, sW + s * AMAX * AMAX, r, is_self, do_der != 0, val, der);
+        radial_entry<AMAX>(P, RS, sW + s * AMAX * AMAX, r, false, do_der != 0, val, der);
         const double g4 = kFourPi * RS.gscale;
         float4 *o = (float4 *)(B.rad + ((size_t)k * P.n_species + s) * 2 * AMAX);
 #pragma unroll
@@ -413,13 +499,44 @@ __device__ __forceinline__ const RadSp &rad_of(const unsigned char *smem, const 
 }
 
 // Persistent scheduling: every CTA takes sites from a counter until none are
-// left.  Which CTA computes a site does not change its result.
-template <int NT>
-__device__ __forceinline__ int next_site(int *ticket, int *slot) {
+// left; which CTA computes a site does not change its result.  The next site
+// is fetched ahead, so that neither the ticket nor the CSR bounds are a round
+// trip between two sites: thread 0 takes the next ticket when a site starts,
+// loads that site's bounds part-way through (ahead_bounds) and hands the three
+// values to the CTA in cur[] when the site ends (ahead_publish, which also
+// synchronises).  The first site is fetched by first_site.
+// Each CTA takes tickets until one is past the last site, so a launch hands out
+// exactly n_sites + gridDim.x of them; the CTA holding the last one puts the
+// counter back to 0 for the next launch.
+__device__ __forceinline__ int take_ticket(int *ticket, int n_sites) {
+  const int t = atomicAdd(ticket, 1);
+  if (t == n_sites + (int)gridDim.x - 1) atomicExch(ticket, 0);
+  return t;
+}
+__device__ __forceinline__ void first_site(const DevBatch &B, int *ticket, int *cur) {
+  if (threadIdx.x == 0) {
+    const int s0 = take_ticket(ticket, B.n_sites);
+    cur[0] = s0;
+    cur[1] = s0 < B.n_sites ? B.off[s0] : 0;
+    cur[2] = s0 < B.n_sites ? B.off[s0 + 1] : 0;
+  }
   __syncthreads();
-  if (threadIdx.x == 0) *slot = atomicAdd(ticket, 1);
+}
+__device__ __forceinline__ void ahead_bounds(const DevBatch &B, int nx, int &nx0, int &nx1) {
+  if (threadIdx.x == 0 && nx < B.n_sites) {
+    nx0 = B.off[nx];
+    nx1 = B.off[nx + 1];
+  }
+}
+// Callers guarantee a __syncthreads between their reads of cur[] at the top of
+// the site and this call.
+__device__ __forceinline__ void ahead_publish(int *cur, int nx, int nx0, int nx1) {
+  if (threadIdx.x == 0) {
+    cur[0] = nx;
+    cur[1] = nx0;
+    cur[2] = nx1;
+  }
   __syncthreads();
-  return *slot;
 }
 
 // 16-byte asynchronous global -> shared copy (no register staging).
@@ -569,19 +686,23 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
   const int n_max = P.n_max, k_max = P.k_max, nsp = P.n_species;
 
   copy_site_blob<NT>(P, smem, 0);
+  first_site(B, B.ticket, sSite);
   for (;;) {
-    const int site = next_site<NT>(B.ticket, sSite);
+    const int site = sSite[0];
     if (site >= B.n_sites) break;
+    const int p_begin = sSite[1];
+    const int p_end = min(sSite[2], B.n_pairs);
+    int nx = 0, nx0 = 0, nx1 = 0;
+    if (tid == 0) nx = take_ticket(B.ticket, B.n_sites);  // the next site, fetched ahead
     for (int t = tid; t < 2 * n_max * KS; t += NT) sC64[t] = 0.0;
-    const int p_begin = B.off[site];
-    const int p_end = min(B.off[site + 1], B.n_pairs);
     __syncthreads();
 
     for (int chunk = p_begin; chunk < p_end; chunk += NT) {
       int slot[SOAPB_MAX_SPECIES];
       unsigned my_bits;
+      double my_r;
       const int n_ent = build_entries<NT>(P, B, p_begin, chunk, p_end, false, sEnt, sW_cnt, sBase,
-                                          sCnt, sNent, slot, my_bits);
+                                          sCnt, sNent, slot, my_bits, my_r);
       for (int ebase = 0; ebase < n_ent; ebase += CH) {
         const int n_round = min(CH, n_ent - ebase);
         // ---- A. the entries' rows, then u_k = amp * preflm_k * P_k * i_l in
@@ -598,6 +719,16 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
             while (kk >= k_max) kk -= k_max, ++el;
           }
         }
+        // the central pair's entries carry central_weight (:638-646); the pair
+        // kernel expanded every pair as a neighbour
+        if (chunk == p_begin)
+          for (int el = tid; el < n_round; el += NT) {
+            const int code = sEnt[ebase + el];
+            const double cw = rad_of(smem, P, code >> 24).cw;
+            if ((code & 0xffffff) == 0 && cw != 1.0)
+#pragma unroll
+              for (int n = 0; n < AMAX; ++n) sR[(size_t)el * AMAX + n] *= (float)cw;
+          }
         __syncthreads();
         // ---- B. c_nlm: item = (species, k, half of the species' radial block);
         // FP32 partial sums over groups of 4 entries, flushed into FP64
@@ -651,6 +782,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
       }
     }
 
+    ahead_bounds(B, nx, nx0, nx1);
     // ---- poly3gauss central-atom term (src/soap_turbo.f90:646-662)
     if (P.basis == 1) {
       const int mult = B.species_mult[site];
@@ -721,6 +853,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
       for (int t = 4 * n4 + tid; t < 2 * n_max * KS; t += NT) kc[t] = sC[t];
       if (tid == 0) keep_norm[site] = norm;
     }
+    ahead_publish(sSite, nx, nx0, nx1);
   }
 }
 
@@ -777,10 +910,16 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
   float *sGu_eff = P.cmap_identity ? sGp : sGu;
 
   copy_site_blob<NT>(P, smem, 1);
+  first_site(B, B.ticket + 1, sSite);
   for (;;) {
-    const int site = next_site<NT>(B.ticket + 1, sSite);
+    const int site = sSite[0];
     if (site >= n_sites) break;
-    // ---- G is read first, so its latency overlaps the copies below
+    const int p_begin = sSite[1];
+    const int p_end = min(sSite[2], B.n_pairs);
+    int nx = 0, nx0 = 0, nx1 = 0;
+    if (tid == 0) nx = take_ticket(B.ticket + 1, n_sites);  // the next site, fetched ahead
+    // ---- every per-site load is issued here, so their latencies overlap
+    const double knorm = keep_norm[site];
     const double *q = soap_in + (size_t)site * n_soap;
     double gv[GPT], qv[GPT];
 #pragma unroll
@@ -810,7 +949,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
       qg += q[o] * g;
     }
     qg = block_sum<NT>(qg, sRed);
-    const double inv = 1.0 / keep_norm[site];
+    const double inv = 1.0 / knorm;
 #pragma unroll
     for (int j = 0; j < GPT; ++j) {
       const int o = tid + j * NT;
@@ -863,16 +1002,16 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
       }
     }
     __syncthreads();
+    ahead_bounds(B, nx, nx0, nx1);
 
-    const int p_begin = B.off[site];
-    const int p_end = min(B.off[site + 1], B.n_pairs);
     double self_x = 0.0, self_y = 0.0, self_z = 0.0;
 
     for (int chunk = p_begin; chunk < p_end; chunk += NT) {
       int slot[SOAPB_MAX_SPECIES];
       unsigned my_bits;
+      double my_r;
       const int n_ent = build_entries<NT>(P, B, p_begin, chunk, p_end, true, sEnt, sW_cnt, sBase,
-                                          sCnt, sNent, slot, my_bits);
+                                          sCnt, sNent, slot, my_bits, my_r);
       for (int ebase = 0; ebase < n_ent; ebase += CH) {
         const int n_round = min(CH, n_ent - ebase);
         // ---- A. the entries' angular rows and radial rows
@@ -991,7 +1130,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
           }
           const float *rot = sRot + 4 * tid;
           const double ct = rot[0], st = rot[1], cf = rot[2], sf = rot[3];
-          const double ir = 1.0 / B.rjs[k];
+          const double ir = 1.0 / my_r;
           px = sgn * (st * cf * fr - ct * cf * ir * fp - sf * ir * fa);
           py = sgn * (st * sf * fr - ct * sf * ir * fp + cf * ir * fa);
           pz = sgn * (ct * fr + st * ir * fp);
@@ -1013,6 +1152,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
       po[1] = self_y;
       po[2] = self_z;
     }
+    ahead_publish(sSite, nx, nx0, nx1);
   }
 }
 
@@ -1057,25 +1197,34 @@ static cudaError_t run_contract(const DevParams &P, const DevBatch &B, const Lau
   return cudaGetLastError();
 }
 
+int prep_err_words(int n_sites) { return 3 + prep_scan_tiles(n_sites); }
+
+unsigned long long prep_error_code(unsigned long long word) {
+  return word == 0 ? ~0ull : kErrTop - word;
+}
+
 cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s) {
-  const int blocks = 1 + (B.n_pairs + 255) / 256;
-  k_prep<<<blocks, 256, 0, s>>>(B, P.n_species);
+  const int tiles = prep_scan_tiles(B.n_sites);
+  const int blocks = tiles + (B.n_pairs + kPrepThreads - 1) / kPrepThreads;
+  if (blocks > 0) k_prep<<<blocks, kPrepThreads, 0, s>>>(B, P.n_species, tiles);
   return cudaGetLastError();
 }
 
 template <int AMAX, int LC>
 static cudaError_t run_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der) {
-  const size_t sm = (size_t)P.off_rad + (size_t)P.n_species * SOAPB_RADSP_BYTES +
-                    (size_t)128 * (row_len(LC) + 1) * sizeof(float);
+  size_t sm = (size_t)P.off_rad + (size_t)P.n_species * SOAPB_RADSP_BYTES +
+              (size_t)128 * (row_len(LC) + 1) * sizeof(float);
+  if (sm < kScanTile * sizeof(int)) sm = kScanTile * sizeof(int);  // scan tiles reuse it
   auto kern = k_pair<AMAX, LC>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  kern<<<(B.n_pairs + 127) / 128, 128, sm, s>>>(P, B, do_der);
+  const int tiles = prep_scan_tiles(B.n_sites);
+  const int blocks = tiles + (B.n_pairs + 127) / 128;
+  if (blocks > 0) kern<<<blocks, 128, sm, s>>>(P, B, do_der, tiles);
   return cudaGetLastError();
 }
 
 cudaError_t launch_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der) {
-  if (B.n_pairs <= 0) return cudaSuccess;
   if (P.amax_t == 8) return run_pair<8, 8>(P, B, s, do_der);
   return run_pair<16, 12>(P, B, s, do_der);
 }
