@@ -384,6 +384,7 @@ __device__ __forceinline__ void angular_stage(const DevParams &P, int i_sp, doub
   const double sc = P.sig_t_c[i_sp];
   const double c1 = 2.0 * rj / (sig * sig), c2 = 1.0 - sc * rj / sig;
   const bool dz = !(rj >= 1.0e-5);
+  const double irj = dz ? 0.0 : 1.0 / rj;  // one division for every l below
   double fact = 1.0, il_prev = 0.0, il0 = 0.0;
 #pragma unroll
   for (int l = 0; l <= LC + 1; ++l) {
@@ -411,7 +412,7 @@ __device__ __forceinline__ void angular_stage(const DevParams &P, int i_sp, doub
       if (l == 0) il0 = il;
       if (l == 1 && L >= 0) out[o_ild + 0] = dz ? 0.f : (float)(c1 * (il - il0) * c2);
       if (l >= 1 && l <= L && l <= LC)
-        out[o_ild + l] = dz ? 0.f : (float)(((-c1 - (double)(2 * l + 2) / rj) * il + c1 * il_prev) * c2);
+        out[o_ild + l] = dz ? 0.f : (float)(((-c1 - (double)(2 * l + 2) * irj) * il + c1 * il_prev) * c2);
     }
     il_prev = il;
   }

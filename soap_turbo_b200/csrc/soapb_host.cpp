@@ -529,11 +529,19 @@ int build_tables(soapb_context *c) {
           if (half * (amax_t / 2) < c->alpha[s]) citem.push_back(s | (kk << 4) | (half << 12));
     P.n_citem = (int)citem.size();
     P.off_citem = put(citem.data(), citem.size() * 4);
-    // H items (n, l), heaviest first so a strided assignment balances
+    // H items (n, l, m0): m = m0 .. m0 + 2 (the contract kernel's kHM) of one
+    // (n, l) Y list, which costs the list's length per m; empty lists give no
+    // item.  Heaviest first, so that a strided assignment over the CTA's
+    // threads balances.
+    constexpr int kHM = 3;
     std::vector<std::pair<long, int>> hw;
     for (int l = 0; l <= L; ++l)
-      for (int n = 0; n < N; ++n)
-        hw.push_back({-(long)(hl_off[l * N + n + 1] - hl_off[l * N + n]) * (l + 1), n | (l << 8)});
+      for (int n = 0; n < N; ++n) {
+        const long len = hl_off[l * N + n + 1] - hl_off[l * N + n];
+        if (len == 0) continue;
+        for (int m0 = 0; m0 <= l; m0 += kHM)
+          hw.push_back({-len * std::min(kHM, l + 1 - m0), n | (l << 8) | (m0 << 16)});
+      }
     std::stable_sort(hw.begin(), hw.end());
     std::vector<int> hitem;
     for (auto &p : hw) hitem.push_back(p.second);

@@ -424,8 +424,12 @@ struct Layout {
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-// entries whose rows are staged in shared memory at a time: half the CTA, at most 64
-__host__ __device__ constexpr int stage_entries_per_round(int NT) { return NT / 2 < 64 ? NT / 2 : 64; }
+// entries whose rows are staged in shared memory at a time: half the CTA, at
+// most 64 for the descriptor (mode 0) and 32 for the contract (mode 1), whose
+// longer staged rows would otherwise cost it a CTA per SM
+__host__ __device__ constexpr int stage_entries_per_round(int NT, int mode) {
+  return NT / 2 < (mode ? 32 : 64) ? NT / 2 : (mode ? 32 : 64);
+}
 // Staged rows are longer than the global ones and stay 16-byte aligned for the
 // asynchronous copies.  The contract (mode 1) pads by 16 floats so that its two
 // half-warps, which read neighbouring rows at the same offsets, use disjoint
@@ -447,7 +451,7 @@ __host__ __device__ inline size_t site_blob_bytes(const DevParams &P, int mode) 
 __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AMAX, int LC, int mode) {
   Layout L{};
   const size_t KS = (size_t)(P.k_max | 1);
-  const size_t nsp = (size_t)P.n_species, CH = (size_t)stage_entries_per_round(NT);
+  const size_t nsp = (size_t)P.n_species, CH = (size_t)stage_entries_per_round(NT, mode);
   const size_t nC = 2 * (size_t)P.n_max * KS;
   size_t o = site_blob_bytes(P, mode);
   L.red = o;  o += 40 * sizeof(double);
@@ -659,7 +663,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
                                                       float *__restrict__ keep_c,
                                                       double *__restrict__ keep_norm, int keep) {
   extern __shared__ __align__(16) unsigned char smem[];
-  constexpr int CH = stage_entries_per_round(NT);
+  constexpr int CH = stage_entries_per_round(NT, 0);
   constexpr int NH = AMAX / 2;  // radial indices per c_nlm item
   const int AS = stage_stride(LC, 0);
   const Layout Ly = make_layout(P, NT, AMAX, LC, 0);
@@ -858,6 +862,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
 }
 
 // ------------------------------------------------------------ contract
+constexpr int kHM = 3;  // m values per H item (the host's items must agree)
+
 template <int NT, int AMAX, int LC>
 __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, const DevBatch B,
                                                     const double *__restrict__ soap_in,
@@ -866,7 +872,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
                                                     const double *__restrict__ keep_norm,
                                                     double *__restrict__ pair_out) {
   extern __shared__ __align__(16) unsigned char smem[];
-  constexpr int CH = stage_entries_per_round(NT);
+  constexpr int CH = stage_entries_per_round(NT, 1);
   constexpr int KC = (LC + 1) * (LC + 2) / 2;
   constexpr int KJ = (KC + 15) / 16;
   constexpr int GPT = 8;  // G values a thread holds while the norm dot product is reduced
@@ -910,6 +916,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
   float *sGu_eff = P.cmap_identity ? sGp : sGu;
 
   copy_site_blob<NT>(P, smem, 1);
+  for (int t = tid; t < 2 * (int)HPL; t += NT) sH[t] = 0.f;  // entries no item writes stay 0
   first_site(B, B.ticket + 1, sSite);
   for (;;) {
     const int site = sSite[0];
@@ -936,7 +943,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
       const int n4 = (2 * n_max * KS) / 4;
       for (int t = tid; t < n4; t += NT) cp_async16(sC + 4 * t, kc + 4 * t);
       for (int t = 4 * n4 + tid; t < 2 * n_max * KS; t += NT) sC[t] = kc[t];
-      for (int t = tid; t < 2 * (int)HPL; t += NT) sH[t] = 0.f;
       cp_async_wait_all();
     }
     // ---- back through the normalisation (src/soap_turbo.f90:1783-1790)
@@ -967,14 +973,16 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
       __syncthreads();
     }
     // ---- H(k,n) = w(m) sum_np Y(n,np,l) c(k,np) over the non-zero Y (:1800-1835);
-    // one item per (n, l) walks its Y list once for all m
+    // one item per (n, l, m0) walks its Y list once for m = m0 .. m0 + kHM - 1
+    // (up to l); the host orders the items heaviest first.  Every H entry an
+    // item writes is rewritten at every site; the others stay 0.
     for (int it = tid; it < P.n_hitem; it += NT) {
       const int code = hitem[it];
-      const int n = code & 0xff, l = code >> 8;
-      const int kb = l * (l + 1) / 2;
-      float hr[LC + 1], hi[LC + 1];
+      const int n = code & 0xff, l = (code >> 8) & 0xff, m0 = code >> 16;
+      const int kb = l * (l + 1) / 2 + m0, mn = min(kHM, l + 1 - m0);
+      float hr[kHM], hi[kHM];
 #pragma unroll
-      for (int m = 0; m <= LC; ++m) hr[m] = hi[m] = 0.f;
+      for (int j = 0; j < kHM; ++j) hr[j] = hi[j] = 0.f;
       const int li = l * n_max + n;
       for (int t = hloff[li]; t < hloff[li + 1]; ++t) {
         const int e = hl[t];
@@ -983,21 +991,21 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
         const float *cr = sC + (size_t)np * KS + kb;
         const float *ci = cr + (size_t)n_max * KS;
 #pragma unroll
-        for (int m = 0; m <= LC; ++m) {
-          if (m <= l) {
-            hr[m] = fmaf(y, cr[m], hr[m]);
-            hi[m] = fmaf(y, ci[m], hi[m]);
+        for (int j = 0; j < kHM; ++j) {
+          if (j < mn) {
+            hr[j] = fmaf(y, cr[j], hr[j]);
+            hi[j] = fmaf(y, ci[j], hi[j]);
           }
         }
       }
       const int nm = nmap[n];
       const int col = (nm & 0xff) * AMAX + (nm >> 8);
 #pragma unroll
-      for (int m = 0; m <= LC; ++m) {
-        if (m <= l) {
-          const float w = (m == 0) ? 1.f : 2.f;
-          sH[(size_t)(kb + m) * HS + col] = w * hr[m];
-          sH[HPL + (size_t)(kb + m) * HS + col] = w * hi[m];
+      for (int j = 0; j < kHM; ++j) {
+        if (j < mn) {
+          const float w = (m0 + j == 0) ? 1.f : 2.f;
+          sH[(size_t)(kb + j) * HS + col] = w * hr[j];
+          sH[HPL + (size_t)(kb + j) * HS + col] = w * hi[j];
         }
       }
     }
