@@ -353,16 +353,19 @@ __device__ __forceinline__ void plm_array(int lmax, T x, T sq, T (&p)[(LC + 1) *
 
 // ---------------------------------------------------------------- streamed angular stage
 // The same quantities as angular_scalars, written in FP32 to `out` as each one
-// appears so that only the last two terms of each recursion are live in FP64:
-//   out[o_il + l], out[o_ild + l] (DER), out[o_er + m], out[o_ei + m], out[o_amp],
-//   out[o_sf]; cos(theta) and sqrt(1 - cos^2) are returned in x, sq.
+// appears so that only the last two terms of each recursion are live in FP64.
+// The amplitude rcut_max^2 / sigma_t^2 is folded into i_l and its derivative:
+//   out[o_il + l] = amp i_l, out[o_ild + l] = amp d i_l / dr (DER),
+//   out[o_er + m], out[o_ei + m], out[o_amp] = amp, out[o_sf];
+// cos(theta) and sqrt(1 - cos^2) are returned in x, sq.
 template <int LC, bool DER>
 __device__ __forceinline__ void angular_stage(const DevParams &P, int i_sp, double rj, double theta,
                                               double phi, float *out, int o_il, int o_ild, int o_er,
                                               int o_ei, int o_amp, int o_sf, double &x, double &sq) {
   const int L = P.l_max;
   const double sig = P.sig_t[i_sp] + P.sig_t_c[i_sp] * rj;               // :579-580
-  out[o_amp] = (float)(P.rcut2 / (sig * sig));
+  const double amp = P.rcut2 / (sig * sig);
+  out[o_amp] = (float)amp;
   x = cos(theta);
   sq = sqrt(1.0 - x * x);
   // i_l(x^2) exp(-x^2) (src/soap_turbo_angular.f90:361-422) and its radial
@@ -407,12 +410,13 @@ __device__ __forceinline__ void angular_stage(const DevParams &P, int i_sp, doub
       flm1 = fl;
       il = fl;
     }
-    if (l <= LC) out[o_il + l] = (float)il;
+    if (l <= LC) out[o_il + l] = (float)(amp * il);
     if (DER) {
       if (l == 0) il0 = il;
-      if (l == 1 && L >= 0) out[o_ild + 0] = dz ? 0.f : (float)(c1 * (il - il0) * c2);
+      if (l == 1 && L >= 0) out[o_ild + 0] = dz ? 0.f : (float)(amp * (c1 * (il - il0) * c2));
       if (l >= 1 && l <= L && l <= LC)
-        out[o_ild + l] = dz ? 0.f : (float)(((-c1 - (double)(2 * l + 2) * irj) * il + c1 * il_prev) * c2);
+        out[o_ild + l] =
+            dz ? 0.f : (float)(amp * (((-c1 - (double)(2 * l + 2) * irj) * il + c1 * il_prev) * c2));
     }
     il_prev = il;
   }

@@ -475,6 +475,12 @@ int build_tables(soapb_context *c) {
         for (int i = 0; i < a; ++i) Wt[(size_t)s * amax_t * amax_t + j * a + i] = c->W[(size_t)(b + j) * N + (b + i)];
     }
     P.off_W = put(Wt.data(), Wt.size() * 8);
+    // preflm to l_max + 1: the pair kernel stores preflm_k P_k in the rows
+    const int KX = (L + 2) * (L + 3) / 2;
+    std::vector<double> pfx(KX);
+    preflm(L + 1, pfx.data());
+    std::vector<float> kpx(pfx.begin(), pfx.end());
+    P.off_kpx = put(kpx.data(), kpx.size() * 4);
     std::vector<unsigned char> rs((size_t)c->n_species * SOAPB_RADSP_BYTES, 0);
     for (int s = 0; s < c->n_species; ++s) std::memcpy(rs.data() + (size_t)s * SOAPB_RADSP_BYTES, &P.rad[s], sizeof(RadSp));
     P.off_rad = put(rs.data(), rs.size());
@@ -482,42 +488,41 @@ int build_tables(soapb_context *c) {
     std::vector<int4> kidx(KS, make_int4(0, 0, 0, 0));
     std::vector<float4> kcoef(KS, make_float4(0.f, 0.f, 0.f, 0.f));
     std::vector<int> klm(KS, 0);
-    std::vector<float> kpref(KS, 0.f);
     for (int l = 0; l <= L; ++l)
       for (int m = 0; m <= l; ++m) {
         const int kk = l * (l + 1) / 2 + m;
         klm[kk] = l | (m << 8);
-        kpref[kk] = (float)pf[kk];
         // sin(t) dP/dx and -m P/sin(t) from P_l^{m-1}, P_l^{m+1}, P_{l+1}^{m-1}, P_{l+1}^{m+1}
-        // (src/soap_turbo_angular.f90:194-246)
+        // (src/soap_turbo_angular.f90:194-246); the rows hold preflm_j P_j, so
+        // each coefficient carries preflm_kk / preflm_j of the value it scales
         int4 ix = make_int4(kk, kk, kk, kk);
-        float4 cf = make_float4(0.f, 0.f, 0.f, 0.f);
+        double cx = 0.0, cy = 0.0, cz = 0.0, cq = 0.0;
         if (m == 0) {
           if (l > 0) {
             ix.x = ix.y = l * (l + 1) / 2 + 1;
-            cf.x = cf.y = -0.5f;
+            cx = cy = -0.5;
           }
         } else {
           ix.x = kk - 1;
-          cf.x = 0.5f * (float)((l + m) * (l - m + 1));
+          cx = 0.5 * (double)((l + m) * (l - m + 1));
           if (m != l) {
             ix.y = kk + 1;
-            cf.y = -0.5f;
+            cy = -0.5;
           }
           ix.z = (l + 1) * (l + 2) / 2 + m - 1;
-          cf.z = 0.5f * (float)((l - m + 1) * (l - m + 2));
+          cz = 0.5 * (double)((l - m + 1) * (l - m + 2));
           ix.w = (l + 1) * (l + 2) / 2 + m + 1;
-          cf.w = 0.5f;
+          cq = 0.5;
         }
+        const float4 cf = make_float4((float)(cx * pfx[kk] / pfx[ix.x]), (float)(cy * pfx[kk] / pfx[ix.y]),
+                                      (float)(cz * pfx[kk] / pfx[ix.z]), (float)(cq * pfx[kk] / pfx[ix.w]));
         kidx[kk] = ix;
         kcoef[kk] = cf;
       }
     P.off_kidx = put_c(kidx.data(), kidx.size() * 16);
     P.off_kcoef = put_c(kcoef.data(), kcoef.size() * 16);
     P.off_klm = put(klm.data(), klm.size() * 4);
-    P.off_kpref = put(kpref.data(), kpref.size() * 4);
     P.off_klm_c = put_c(klm.data(), klm.size() * 4);
-    P.off_kpref_c = put_c(kpref.data(), kpref.size() * 4);
     std::vector<int> nmap(N);
     for (int s = 0; s < c->n_species; ++s)
       for (int n = 0; n < c->alpha[s]; ++n) nmap[P.rad[s].nbeg + n] = s | (n << 8);

@@ -70,9 +70,9 @@ struct DevParams {
   int amax_t;             // the kernel instantiation's radial block (8 or 16)
   // in blob:
   int off_W;              // n_species blocks of amax_t^2 doubles (alpha x alpha used)
+  int off_kpx;            // (l_max+2)(l_max+3)/2 float: preflm to l_max + 1 (pair kernel)
   int off_rad;            // n_species RadSp
   int off_klm;            // KS int: l | m << 8
-  int off_kpref;          // KS float: preflm
   int off_citem;          // n_citem int: c_nlm items species | k << 4 | half << 12
   int off_kept;           // n_kept int: kept_nnl
   int off_central;        // n_max double: poly3gauss central-atom term
@@ -80,7 +80,6 @@ struct DevParams {
   int off_kidx;           // KS int4: P_l^m indices of the derivative forms
   int off_kcoef;          // KS float4: their coefficients
   int off_klm_c;          // KS int: l | m << 8
-  int off_kpref_c;        // KS float: preflm
   int off_nmap;           // n_max int: species | local index << 8
   int off_hitem;          // n_hitem int: H items n | l << 8
   int off_hloff;          // (l_max+1)*n_max + 1 int: per (l, n) list offsets

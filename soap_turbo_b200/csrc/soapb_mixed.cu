@@ -308,9 +308,11 @@ __device__ __forceinline__ int first_species(unsigned bits) { return __ffs(bits)
 
 // ------------------------------------------------------------ pair rows
 // The angular row of a pair (floats), written by k_pair and read by the site
-// kernels: i_l, di_l/dr, cos(m phi), -sin(m phi) for l, m <= LC, the
-// amplitude rcut_max^2 / sigma_t^2, 2 sigma_t_scaling / sigma_t, cos(theta),
-// sqrt(1 - cos^2(theta)), then P_l^m for l <= l_max (+1 with derivatives).
+// kernels: amp i_l, amp di_l/dr, cos(m phi), -sin(m phi) for l, m <= LC, the
+// amplitude amp = rcut_max^2 / sigma_t^2, 2 sigma_t_scaling / sigma_t,
+// cos(theta), sqrt(1 - cos^2(theta)), then preflm_k P_l^m for l <= l_max (+1
+// with derivatives), k = l(l+1)/2 + m.  So u_k = amp preflm_k P_k i_l of
+// src/soap_turbo_angular.f90:590-594 is one product of two row values.
 __host__ __device__ constexpr int row_il(int) { return 0; }
 __host__ __device__ constexpr int row_ild(int LC) { return LC + 1; }
 __host__ __device__ constexpr int row_er(int LC) { return 2 * (LC + 1); }
@@ -368,7 +370,9 @@ __global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch 
       row[row_x(LC)] = (float)x;
       row[row_sq(LC)] = (float)sq;
       float *Pr = row + row_p(LC);
-      plm_rows<LC + 1>(P.l_max + (do_der ? 1 : 0), (float)x, (float)sq, [&](int kk, float v) { Pr[kk] = v; });
+      const float *kpx = (const float *)(smem + P.off_kpx);
+      plm_rows<LC + 1>(P.l_max + (do_der ? 1 : 0), (float)x, (float)sq,
+                       [&](int kk, float v) { Pr[kk] = v * kpx[kk]; });
       // the radial expansion of each species in range, as for a neighbour: the
       // central pair's expansion (:342-355) differs only by the factor
       // central_weight (:638-646), which the descriptor applies to that entry
@@ -668,7 +672,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
   const int AS = stage_stride(LC, 0);
   const Layout Ly = make_layout(P, NT, AMAX, LC, 0);
   const int *klm = (const int *)SBLOB(off_klm);
-  const float *kpref = (const float *)SBLOB(off_kpref);
   const int *citem = (const int *)SBLOB(off_citem);
   const int *kept = (const int *)SBLOB(off_kept);
   const double *central = (const double *)SBLOB(off_central);
@@ -687,7 +690,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
 
   const int tid = threadIdx.x;
   const int KS = P.k_max | 1;
-  const int n_max = P.n_max, k_max = P.k_max, nsp = P.n_species;
+  const int n_max = P.n_max, nsp = P.n_species;
 
   copy_site_blob<NT>(P, smem, 0);
   first_site(B, B.ticket, sSite);
@@ -709,23 +712,12 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
                                           sCnt, sNent, slot, my_bits, my_r);
       for (int ebase = 0; ebase < n_ent; ebase += CH) {
         const int n_round = min(CH, n_ent - ebase);
-        // ---- A. the entries' rows, then u_k = amp * preflm_k * P_k * i_l in
-        // place of P_k (src/soap_turbo_angular.f90:590-594)
+        // ---- A. the entries' rows
         stage_entries<NT, AMAX, LC, false>(P, B, sEnt, chunk, ebase, n_round, sA, sR, nullptr);
         __syncthreads();
-        {
-          int el = 0, kk = tid;
-          while (kk >= k_max) kk -= k_max, ++el;
-          for (; el < n_round;) {
-            float *Ae = sA + (size_t)el * AS;
-            Ae[row_p(LC) + kk] *= Ae[row_amp(LC)] * kpref[kk] * Ae[row_il(LC) + (klm[kk] & 0xff)];
-            kk += NT;
-            while (kk >= k_max) kk -= k_max, ++el;
-          }
-        }
         // the central pair's entries carry central_weight (:638-646); the pair
         // kernel expanded every pair as a neighbour
-        if (chunk == p_begin)
+        if (chunk == p_begin) {
           for (int el = tid; el < n_round; el += NT) {
             const int code = sEnt[ebase + el];
             const double cw = rad_of(smem, P, code >> 24).cw;
@@ -733,7 +725,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
 #pragma unroll
               for (int n = 0; n < AMAX; ++n) sR[(size_t)el * AMAX + n] *= (float)cw;
           }
-        __syncthreads();
+          __syncthreads();
+        }
         // ---- B. c_nlm: item = (species, k, half of the species' radial block);
         // FP32 partial sums over groups of 4 entries, flushed into FP64
         const int e_hi = ebase + n_round;
@@ -744,7 +737,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
           if (lo >= hi) continue;
           const RadSp &RS = rad_of(smem, P, s);
           const int nb = RS.nbeg, a = RS.alpha, n0 = half * NH;
-          const int m = klm[kk] >> 8;
+          const int l = klm[kk] & 0xff, m = klm[kk] >> 8;
           double dr[NH], di[NH];
           float pr[NH], pi[NH];
 #pragma unroll
@@ -756,7 +749,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
           for (int e2 = lo; e2 < hi; ++e2) {
             const int el = e2 - ebase;
             const float *Ae = sA + (size_t)el * AS;
-            const float u = Ae[row_p(LC) + kk];
+            // u_k = (preflm_k P_k) (amp i_l) (src/soap_turbo_angular.f90:590-594)
+            const float u = Ae[row_p(LC) + kk] * Ae[row_il(LC) + l];
             const float ar = u * Ae[row_er(LC) + m], ai = u * Ae[row_ei(LC) + m];
             const float *Re = sR + (size_t)el * AMAX + n0;
 #pragma unroll
@@ -879,13 +873,12 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
   static_assert(AMAX % 4 == 0, "vector loads of H need AMAX % 4 == 0");
   const int AS = stage_stride(LC, 1);
   constexpr int O_IL = row_il(LC), O_ILD = row_ild(LC), O_ER = row_er(LC), O_EI = row_ei(LC),
-                O_AMP = row_amp(LC), O_SF = row_sf(LC), O_X = row_x(LC), O_SQ = row_sq(LC),
+                O_SF = row_sf(LC), O_X = row_x(LC), O_SQ = row_sq(LC),
                 O_P = row_p(LC);
   const Layout Ly = make_layout(P, NT, AMAX, LC, 1);
   const int4 *kidx = (const int4 *)SBLOBC(off_kidx);
   const float4 *kcoef = (const float4 *)SBLOBC(off_kcoef);
   const int *klm = (const int *)SBLOBC(off_klm_c);
-  const float *kpref = (const float *)SBLOBC(off_kpref_c);
   const int *nmap = (const int *)SBLOBC(off_nmap);
   const int *hitem = (const int *)SBLOBC(off_hitem);
   const int *hloff = (const int *)SBLOBC(off_hloff);
@@ -1030,7 +1023,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
         int4 kix[KJ];
         float4 kcf[KJ];
         int klmr[KJ];
-        float kpr[KJ];
 #pragma unroll
         for (int j = 0; j < KJ; ++j) {
           const int kk = hl16 + 16 * j;
@@ -1038,7 +1030,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
           kix[j] = v ? kidx[kk] : make_int4(0, 0, 0, 0);
           kcf[j] = v ? kcoef[kk] : make_float4(0.f, 0.f, 0.f, 0.f);
           klmr[j] = v ? klm[kk] : -1;
-          kpr[j] = v ? kpref[kk] : 0.f;
         }
         // The loop bound is uniform per warp (both halves iterate together) so
         // the full-mask shuffles below always see all 32 lanes.
@@ -1067,7 +1058,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
               R[4 * n4] = a.x; R[4 * n4 + 1] = a.y; R[4 * n4 + 2] = a.z; R[4 * n4 + 3] = a.w;
               Rd[4 * n4] = d.x; Rd[4 * n4 + 1] = d.y; Rd[4 * n4 + 2] = d.z; Rd[4 * n4 + 3] = d.w;
             }
-            const float amp = Ae[O_AMP], sfac = Ae[O_SF];
+            const float sfac = Ae[O_SF];
             const float *Hs = sH + (size_t)s * AMAX;
 #pragma unroll
             for (int j = 0; j < KJ; ++j) {
@@ -1077,13 +1068,14 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
               const float Pk = Pe[kk];
               const float dms = kcf[j].x * Pe[kix[j].x] + kcf[j].y * Pe[kix[j].y];
               const float dvs = kcf[j].z * Pe[kix[j].z] + kcf[j].w * Pe[kix[j].w];
+              // rows hold amp i_l, amp di_l/dr and preflm_k P_k; kcoef carries the
+              // preflm ratios of the derivative combinations
               const float il = Ae[O_IL + l], ild = Ae[O_ILD + l];
               const float er = Ae[O_ER + m], ei = Ae[O_EI + m];
-              const float ap = amp * kpr[j];
-              const float u = ap * Pk * il;
-              const float ur = ap * Pk * ild - sfac * u;
-              const float ua = ap * dvs * il;
-              const float up = ap * dms * il;
+              const float u = Pk * il;
+              const float ur = Pk * ild - sfac * u;
+              const float ua = dvs * il;
+              const float up = dms * il;
               const float4 *hr4 = (const float4 *)(Hs + (size_t)kk * HS);
               const float4 *hi4 = (const float4 *)(Hs + HPL + (size_t)kk * HS);
               float Ur = 0.f, Ui = 0.f, Vr = 0.f, Vi = 0.f;
