@@ -122,8 +122,10 @@ int soapb_set_basis_matrices(int32_t n_max, const double *W, const double *S);
 
 /* get_compress_indices (src/soap_turbo_compress.f90:44).  what_to_do =
  * "get_dim" fills dim and P_nonzero only; "set_indices" also fills P_i, P_j
- * (1-based) and P_el, each of capacity P_nonzero.  Supported mode: "trivial"
- * ("Trivial"); other modes return SOAPB_ERR_COMPRESS_MODE. */
+ * (1-based) and P_el, each of capacity P_nonzero.  Modes: "trivial"
+ * ("Trivial", :86-119) and Darby's "nu_R_nu_S" with nu_R, nu_S in 0..2
+ * ("0_0" .. "2_2", :120-303; every species must have the same alpha_max,
+ * else SOAPB_ERR_COMPRESS_MODE).  Other modes return SOAPB_ERR_COMPRESS_MODE. */
 int soapb_get_compress_indices(const char *compress_mode, int32_t n_species,
                                const int32_t *alpha_max, int32_t l_max, int32_t *dim,
                                int32_t *P_nonzero, int32_t *P_i, int32_t *P_j, double *P_el,

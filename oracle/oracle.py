@@ -70,6 +70,8 @@ def lib():
         _lib.or_overlap_poly3.argtypes = [C.c_int, _f64p]
         _lib.or_overlap_poly3gauss.argtypes = [C.c_int, C.c_double, C.c_double, _f64p]
         _lib.or_compress_trivial.argtypes = [C.c_int, _i32p, C.c_int, _i32p, _i32p, _f64p]
+        _lib.or_compress_darby.argtypes = [C.c_int, _i32p, C.c_int, C.c_int, C.c_int, _i32p,
+                                           _i32p, _i32p, _f64p]
         _lib.or_radial_eval.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.c_double, C.c_double, _f64p, C.c_int, C.c_int,
                                         C.c_double, C.c_int, C.c_int, C.c_int, _f64p, _f64p, _f64p]
@@ -175,6 +177,30 @@ def compress_trivial(alpha_max, l_max):
     return P_i, P_j, P_el
 
 
+DARBY_MODES = ("0_0", "0_1", "0_2", "1_0", "1_1", "1_2", "2_0", "2_1", "2_2")
+
+
+def compress_darby(mode, alpha_max, l_max):
+    """get_compress_indices for the Darby modes "nu_R_nu_S"
+    (src/soap_turbo_compress.f90:120-303): (dim, P_i, P_j, P_el), 1-based."""
+    nu_R, nu_S = int(mode[0]), int(mode[2])
+    am = np.ascontiguousarray(alpha_max, dtype=np.int32)
+    dim = C.c_int(0)
+    n = lib().or_compress_darby(len(am), _p(am, _i32p), l_max, nu_R, nu_S, C.byref(dim),
+                                None, None, None)
+    if n == -2:
+        raise ValueError(f"compress_mode={mode} requires all species to have the same number "
+                         "of radial basis functions")
+    if n < 0:
+        raise MemoryError("compression lookup does not fit")
+    P_i = np.zeros(n, dtype=np.int32)
+    P_j = np.zeros(n, dtype=np.int32)
+    P_el = np.zeros(n)
+    lib().or_compress_darby(len(am), _p(am, _i32p), l_max, nu_R, nu_S, C.byref(dim),
+                            _p(P_i, _i32p), _p(P_j, _i32p), _p(P_el, _f64p))
+    return dim.value, P_i, P_j, P_el
+
+
 # ---------------------------------------------------------------- get_soap
 class Result:
     """soap (n_sites, n_soap) == Fortran soap(n_soap, n_sites); the state
@@ -230,6 +256,8 @@ class Result:
 def compress_arrays(hyper):
     if hyper.compress_mode in ("trivial", "Trivial"):
         return compress_trivial(hyper.alpha_max, hyper.l_max)
+    if hyper.compress_mode in DARBY_MODES:
+        return compress_darby(hyper.compress_mode, hyper.alpha_max, hyper.l_max)[1:]
     return None
 
 

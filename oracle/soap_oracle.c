@@ -1057,6 +1057,87 @@ int or_compress_trivial(int n_species, const int *alpha_max, int l_max, int *P_i
   return counter;
 }
 
+/* get_compress_indices, the Darby branch (compress_mode "nu_R_nu_S", nu_R, nu_S
+ * in 0..2), src/soap_turbo_compress.f90:120-303, followed step by step: the
+ * combined (species, radial) index ns, the limits N1, N2, S1, S2, the
+ * symmetric (nu_R, nu_S both even) and the general recipe, and the
+ * dense_to_sparse lookup that numbers the non-zero entries in the order they
+ * are met.  Every species must have the same alpha (:134-141; returns -2).
+ * With P_i == NULL only P_nonzero is returned; *dim gets the compressed size. */
+int or_compress_darby(int n_species, const int *alpha_max, int l_max, int nu_R, int nu_S, int *dim,
+                      int *P_i, int *P_j, double *P_el) {
+  for (int i = 0; i < n_species; i++)
+    if (alpha_max[i] != alpha_max[0]) return -2;
+  const int A = alpha_max[0], NS = n_species * A, L1 = l_max + 1;
+  int *ns_s = (int *)malloc(sizeof(int) * NS), *ns_n = (int *)malloc(sizeof(int) * NS);
+  for (int i = 0, k = 0; i < n_species; i++)
+    for (int n = 0; n < A; n++, k++) { ns_s[k] = i; ns_n[k] = n; }
+  const int sym = (nu_R % 2 == 0) && (nu_S % 2 == 0);
+  const int N1 = nu_R > 0 ? A : 1, N2 = nu_R == 2 ? A : 1;
+  const int S1 = nu_S > 0 ? n_species : 1, S2 = nu_S == 2 ? n_species : 1;
+  const long n_unc = (long)NS * (NS + 1) / 2 * L1;
+  const long n_comp = sym ? (long)N1 * S1 * (N1 * S1 + 1) / 2 * L1 : (long)N1 * S1 * N2 * S2 * L1;
+  int *d2s = (int *)calloc((size_t)n_comp * n_unc, sizeof(int)); /* dense_to_sparse(comp, ind) */
+  if (!d2s) { free(ns_s); free(ns_n); return -3; }
+  int counter = 0;
+  long ind = 0;
+#define D2S(c, u) d2s[(size_t)(c) * n_unc + (u)]
+  for (int i = 0; i < NS; i++) {
+    const int z1 = ns_s[i] % S1, a1 = ns_n[i] % N1;
+    for (int j = 0; j < NS; j++) {
+      const int z2 = ns_s[j] % S2, a2 = ns_n[j] % N2;
+      if (j < i) continue; /* the original power spectrum is symmetric */
+      for (int l = 0; l <= l_max; l++) {
+        if (sym) {
+          int ic = z1 * N1 + a1, jc = z2 * N2 + a2;
+          if (jc < ic) { const int t = ic; ic = jc; jc = t; }
+          const long comp = ((long)ic * (2 * N1 * S1 + 1 - ic) * L1) / 2 + (long)(jc - ic) * L1 + l;
+          if (D2S(comp, ind) == 0) D2S(comp, ind) = ++counter;
+          const int k = D2S(comp, ind);
+          if (P_i) {
+            P_el[k - 1] += (i != j && ic == jc) ? sqrt(2.0) : 1.0;
+            P_i[k - 1] = (int)comp + 1;
+            P_j[k - 1] = (int)ind + 1;
+          }
+        } else {
+          const int ic = z1 * N1 + a1, jc = z2 * N2 + a2;
+          /* the compressed indices of the symmetric term that is skipped */
+          const int ic2 = (ns_s[j] % S1) * N1 + ns_n[j] % N1, jc2 = (ns_s[i] % S2) * N2 + ns_n[i] % N2;
+          const long comp = ((long)ic * S2 * N2 + jc) * L1 + l;
+          const long comp2 = ((long)ic2 * S2 * N2 + jc2) * L1 + l;
+          if (D2S(comp, ind) == 0) D2S(comp, ind) = ++counter;
+          const int k = D2S(comp, ind);
+          if (D2S(comp2, ind) == 0 && i != j && comp != comp2) D2S(comp2, ind) = ++counter;
+          const int k2 = D2S(comp2, ind);
+          if (P_i) {
+            if (i == j) {
+              P_el[k - 1] += 1.0;
+              P_i[k - 1] = (int)comp + 1;
+              P_j[k - 1] = (int)ind + 1;
+            } else if (comp == comp2) {
+              P_el[k - 1] += sqrt(2.0);
+              P_i[k - 1] = (int)comp + 1;
+              P_j[k - 1] = (int)ind + 1;
+            } else {
+              P_el[k - 1] += 1.0 / sqrt(2.0);
+              P_i[k - 1] = (int)comp + 1;
+              P_j[k - 1] = (int)ind + 1;
+              P_el[k2 - 1] += 1.0 / sqrt(2.0);
+              P_i[k2 - 1] = (int)comp2 + 1;
+              P_j[k2 - 1] = (int)ind + 1;
+            }
+          }
+        }
+        ind++;
+      }
+    }
+  }
+#undef D2S
+  free(d2s); free(ns_s); free(ns_n);
+  *dim = (int)n_comp;
+  return counter;
+}
+
 int or_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -68,9 +68,11 @@ class Context:
                  "amplitude_scaling", "central_weight")
         for nm in names:
             keep[nm] = _f64(getattr(hyper, nm), n)
-        if compress is None and getattr(hyper, "compress_mode", "None") in ("trivial", "Trivial"):
+        mode = getattr(hyper, "compress_mode", "None")
+        if compress is None and mode not in (None, "", "None"):
+            # trivial or a Darby mode "nu_R_nu_S"; others raise, as the reference stops
             from .descriptor import get_compress_indices
-            _, _, P_i, P_j, P_el = get_compress_indices("trivial", hyper.alpha_max, hyper.l_max)
+            _, _, P_i, P_j, P_el = get_compress_indices(mode, hyper.alpha_max, hyper.l_max)
             compress = (P_i, P_j, P_el)
         h = _lib.Hyper()
         h.n_species = n

@@ -1229,6 +1229,83 @@ int soapb_orthonormalization_matrix(int32_t basis, int32_t alpha_max, double ato
   return species_basis(basis, alpha_max, atom_sigma_r, rcut_hard, S, W);
 }
 
+namespace {
+
+// get_compress_indices, the compression recipes of James Darby
+// (src/soap_turbo_compress.f90:120-303): nu_R (radially sensitive) and nu_S
+// (species sensitive) correlation indices in 0..2.  Every species must have
+// the same alpha (:134-141).  The combined index runs over (species, n); for
+// each uncompressed component (i <= j, l), numbered ind in that order, the
+// reference numbers the non-zero entries through a dense (compressed x
+// uncompressed) lookup that is only ever read in column ind, so the number
+// assigned is simply the next one, and a second entry (the skipped symmetric
+// term of the general recipe) exists iff i != j and its compressed index
+// differs.  P_el is zeroed first and accumulated, as in the reference.
+int darby_indices(const char *mode, int nu_R, int nu_S, int n_species, const int32_t *alpha_max, int l_max,
+                  bool set, int32_t *dim, int32_t *P_nonzero, int32_t *P_i, int32_t *P_j, double *P_el) {
+  for (int i = 0; i < n_species; ++i)
+    if (alpha_max[i] != alpha_max[0])
+      return fail(SOAPB_ERR_COMPRESS_MODE,
+                  "ERROR: compress_mode=%s requires all species to have the same number of radial "
+                  "basis functions!",
+                  mode);
+  const int A = alpha_max[0], NS = n_species * A, L1 = l_max + 1;
+  const bool sym = nu_R % 2 == 0 && nu_S % 2 == 0;
+  const int N1 = nu_R > 0 ? A : 1, N2 = nu_R == 2 ? A : 1;
+  const int S1 = nu_S > 0 ? n_species : 1, S2 = nu_S == 2 ? n_species : 1;
+  const long n_comp = sym ? (long)N1 * S1 * (N1 * S1 + 1) / 2 * L1 : (long)N1 * S1 * N2 * S2 * L1;
+  if (n_comp > INT32_MAX) return fail(SOAPB_ERR_ARGUMENT, "compressed dimension too large");
+  const int cap = *P_nonzero;
+  if (set)
+    for (int t = 0; t < cap; ++t) {
+      P_i[t] = 0;
+      P_j[t] = 0;
+      P_el[t] = 0.0;
+    }
+  long counter = 0, ind = 0;
+  auto put = [&](long comp, double el) {  // the next entry number, 1-based
+    ++counter;
+    if (set) {
+      if (counter > cap) return false;
+      P_el[counter - 1] += el;
+      P_i[counter - 1] = (int32_t)(comp + 1);
+      P_j[counter - 1] = (int32_t)(ind + 1);
+    }
+    return true;
+  };
+  const double r2 = std::sqrt(2.0), ir2 = 1.0 / std::sqrt(2.0);
+  for (int i = 0; i < NS; ++i) {
+    const int si = i / A, ni = i % A;
+    for (int j = i; j < NS; ++j) {
+      const int sj = j / A, nj = j % A;
+      for (int l = 0; l <= l_max; ++l) {
+        bool ok;
+        if (sym) {
+          int ic = (si % S1) * N1 + ni % N1, jc = (sj % S2) * N2 + nj % N2;
+          if (jc < ic) std::swap(ic, jc);
+          const long comp = ((long)ic * (2 * N1 * S1 + 1 - ic) * L1) / 2 + (long)(jc - ic) * L1 + l;
+          ok = put(comp, (i != j && ic == jc) ? r2 : 1.0);
+        } else {
+          const int ic = (si % S1) * N1 + ni % N1, jc = (sj % S2) * N2 + nj % N2;
+          const int ic2 = (sj % S1) * N1 + nj % N1, jc2 = (si % S2) * N2 + ni % N2;
+          const long comp = ((long)ic * S2 * N2 + jc) * L1 + l;
+          const long comp2 = ((long)ic2 * S2 * N2 + jc2) * L1 + l;
+          if (i == j) ok = put(comp, 1.0);
+          else if (comp == comp2) ok = put(comp, r2);
+          else ok = put(comp, ir2) && put(comp2, ir2);
+        }
+        if (!ok) return fail(SOAPB_ERR_ARGUMENT, "index arrays too short");
+        ++ind;
+      }
+    }
+  }
+  *dim = (int32_t)n_comp;
+  *P_nonzero = (int32_t)counter;
+  return SOAPB_OK;
+}
+
+}  // namespace
+
 int soapb_get_compress_indices(const char *compress_mode, int32_t n_species, const int32_t *alpha_max,
                                int32_t l_max, int32_t *dim, int32_t *P_nonzero, int32_t *P_i,
                                int32_t *P_j, double *P_el, const char *what_to_do) {
@@ -1238,9 +1315,15 @@ int soapb_get_compress_indices(const char *compress_mode, int32_t n_species, con
   if (!std::strcmp(what_to_do, "get_dim")) set = false;
   else if (!std::strcmp(what_to_do, "set_indices")) set = true;
   else return fail(SOAPB_ERR_ARGUMENT, "ERROR: incorrect what_to_do in get_compress_indices() subroutine!");
+  if (n_species < 1) return fail(SOAPB_ERR_ARGUMENT, "n_species must be >= 1");
+  if (set && (!P_i || !P_j || !P_el)) return fail(SOAPB_ERR_ARGUMENT, "null index arrays");
+  const bool darby = std::strlen(compress_mode) == 3 && compress_mode[1] == '_' &&
+                     compress_mode[0] >= '0' && compress_mode[0] <= '2' && compress_mode[2] >= '0' &&
+                     compress_mode[2] <= '2';
+  if (darby) return darby_indices(compress_mode, compress_mode[0] - '0', compress_mode[2] - '0', n_species,
+                                  alpha_max, l_max, set, dim, P_nonzero, P_i, P_j, P_el);
   if (std::strcmp(compress_mode, "trivial") && std::strcmp(compress_mode, "Trivial"))
     return fail(SOAPB_ERR_COMPRESS_MODE, "ERROR: I don't understand compress_mode = %s", compress_mode);
-  if (n_species < 1) return fail(SOAPB_ERR_ARGUMENT, "n_species must be >= 1");
   // trivial recipe (src/soap_turbo_compress.f90:86-119)
   std::vector<int> pivot(n_species);
   pivot[0] = 1;
@@ -1249,7 +1332,6 @@ int soapb_get_compress_indices(const char *compress_mode, int32_t n_species, con
     pivot[i + 1] = pivot[i] + alpha_max[i];
     n_max += alpha_max[i + 1];
   }
-  if (set && (!P_i || !P_j || !P_el)) return fail(SOAPB_ERR_ARGUMENT, "null index arrays");
   int counter = 0, k = 1;
   for (int n = 1; n <= n_max; ++n)
     for (int m = n; m <= n_max; ++m)

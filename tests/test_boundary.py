@@ -87,9 +87,58 @@ def test_compress_indices_bit_exact(am, L):
     assert (dim2, nz2) == (dim, nz)
 
 
+DARBY = ("0_0", "0_1", "0_2", "1_0", "1_1", "1_2", "2_0", "2_1", "2_2")
+
+
+@pytest.mark.parametrize("mode", DARBY)
+@pytest.mark.parametrize("am,L", [([4], 3), ([3, 3], 2), ([8, 8, 8], 8), ([2, 2, 2, 2], 4)])
+def test_darby_indices_bit_exact(mode, am, L):
+    """The library's Darby maps against the oracle's literal restatement
+    (dense lookup and all) of src/soap_turbo_compress.f90:120-303."""
+    dim, nz, P_i, P_j, P_el = D.get_compress_indices(mode, am, L)
+    qdim, Q_i, Q_j, Q_el = O.compress_darby(mode, am, L)
+    assert dim == qdim and nz == Q_i.shape[0]
+    np.testing.assert_array_equal(P_i, Q_i)
+    np.testing.assert_array_equal(P_j, Q_j)
+    np.testing.assert_array_equal(P_el, Q_el)
+    assert P_i.min() >= 1 and P_i.max() == dim
+    n_unc = sum(am) * (sum(am) + 1) // 2 * (L + 1)
+    assert P_j.min() >= 1 and P_j.max() == n_unc
+    assert (dim, nz) == D.get_compress_indices(mode, am, L, what_to_do="get_dim")[:2]
+
+
+def test_darby_2_2_keeps_every_component_once():
+    """nu_R = nu_S = 2 is the full power spectrum: the map is the identity."""
+    dim, nz, P_i, P_j, P_el = D.get_compress_indices("2_2", [3, 3], 2)
+    assert dim == nz == 6 * 7 // 2 * 3
+    np.testing.assert_array_equal(P_i, P_j)
+    np.testing.assert_array_equal(P_el, np.ones(nz))
+
+
+def test_darby_0_0_sums_every_radial_pair_per_l():
+    """nu_R = nu_S = 0 keeps one component per l: each uncompressed (n <= n')
+    enters it once, with sqrt 2 off the diagonal."""
+    am, L = [2, 2], 3
+    dim, nz, P_i, P_j, P_el = D.get_compress_indices("0_0", am, L)
+    N = sum(am)
+    assert dim == L + 1 and nz == N * (N + 1) // 2 * (L + 1)
+    ls = (P_j - 1) % (L + 1)
+    np.testing.assert_array_equal(P_i - 1, ls)
+    diag = []
+    for n in range(N):
+        for m in range(n, N):
+            diag += [n == m] * (L + 1)
+    np.testing.assert_array_equal(P_el, np.where(np.asarray(diag)[P_j - 1], 1.0, np.sqrt(2.0)))
+
+
 def test_compress_errors():
     with pytest.raises(_lib.SoapError) as e:
-        D.get_compress_indices("2_2", [8, 8], 8)
+        D.get_compress_indices("2_2", [8, 6], 8)  # Darby modes need equal alpha_max
+    assert e.value.code == 4
+    with pytest.raises(ValueError):
+        O.compress_darby("2_2", [8, 6], 8)
+    with pytest.raises(_lib.SoapError) as e:
+        D.get_compress_indices("3_0", [8], 8)
     assert e.value.code == 4
     with pytest.raises(_lib.SoapError) as e:
         D.get_compress_indices("bogus", [8], 8)
