@@ -260,6 +260,35 @@ int soapb_contract_cart_der(soapb_context *ctx, const soapb_batch *batch, const 
  * pair index in *bad_pair (or -1). */
 int soapb_check_inputs(soapb_context *ctx, int64_t *bad_pair);
 
+/* Neighbour list of one periodic structure, built on the device in the
+ * layout get_soap takes -- the step before get_soap, which soap_turbo leaves
+ * to its callers; the species and mask follow its assign_species_multiplicity
+ * (src/soap_turbo.f90:2099-2221, mask lines 2188-2214, whose loop runs over
+ * the central atom's multiplicity).
+ *   d_positions (3, n_atoms)       Cartesian, Angstrom (x fastest)
+ *   lattice     (3, 3) on the host the cell vectors a, b, c: lattice[3*i + k]
+ *                                  = component k of vector i; periodic along all three
+ *   d_atom_species (max_mult, n_atoms)  1-based species of each atom, 0 beyond its
+ *                                  multiplicity; d_atom_mult (n_atoms)
+ *   d_sites (n_sites)              0-based atom index of each central site
+ *   rcut                           <= 0: the context's largest rcut_hard
+ * Each row holds the site itself first (rjs = 0, theta = phi = 0), then every
+ * periodic image of every atom closer than rcut, ordered by atom index, then
+ * distance (rounded to FP32), then lattice translation -- an order that
+ * depends on the inputs only; theta = acos(dz/r), phi = atan2(dy, dx) of
+ * r_image - r_site.
+ * `batch` receives device pointers into buffers the context owns, valid until
+ * the next call (use it with soapb_descriptor and friends); d_neigh_atom (may
+ * be NULL) receives the atom index of every pair.  The call waits for the
+ * context's stream (the pair count sizes the outputs).  Errors: a site index
+ * out of range or a non-finite position (SOAPB_ERR_INPUT), more than 1024
+ * neighbours of one site or an rcut reaching more than 100 cells along an
+ * axis (SOAPB_ERR_ARGUMENT). */
+int soapb_build_neighbors(soapb_context *ctx, int32_t n_atoms, const double *d_positions,
+                          const double *lattice, const int32_t *d_atom_species, int32_t max_mult,
+                          const int32_t *d_atom_mult, int32_t n_sites, const int32_t *d_sites,
+                          double rcut, soapb_batch *batch, const int32_t **d_neigh_atom);
+
 /* Number of kernel launches issued by this context since creation. */
 int soapb_launch_count(const soapb_context *ctx, int64_t *count);
 

@@ -94,6 +94,9 @@ SIGNATURES = {
     "soapb_autotune": (C.c_int, [C.c_void_p, C.POINTER(Batch), i32p]),
     "soapb_check_inputs": (C.c_int, [C.c_void_p, i64p]),
     "soapb_launch_count": (C.c_int, [C.c_void_p, i64p]),
+    "soapb_build_neighbors": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, f64p, C.c_void_p,
+                                        C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_double,
+                                        C.POINTER(Batch), C.POINTER(C.c_void_p)]),
     "soapb_kernel_timing": (C.c_int, [C.c_void_p, C.c_int32]),
     "soapb_kernel_times": (C.c_int, [C.c_void_p, i64p, f64p, i64p]),
 }

@@ -54,6 +54,50 @@ class DeviceBatch:
             self.thetas, self.phis))
 
 
+class _DeviceView:
+    """A device array owned by the library, seen through __cuda_array_interface__."""
+
+    def __init__(self, ptr, shape, typestr):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr,
+                                         "data": (int(ptr or 0), False), "version": 2}
+
+
+class BuiltBatch:
+    """The neighbour list soapb_build_neighbors built in a context's buffers:
+    usable as a batch of that context until its next build."""
+
+    def __init__(self, c_batch, neigh_atom_ptr, n_species):
+        self._c = c_batch
+        self.n_sites = int(c_batch.n_sites)
+        self.n_pairs = int(c_batch.n_atom_pairs)
+        self.max_mult = int(c_batch.max_species_multiplicity)
+        self._neigh_atom = neigh_atom_ptr
+        self._n_species = n_species
+
+    @property
+    def c(self):
+        return C.byref(self._c)
+
+    def arrays(self) -> dict:
+        """Host copies of the list, in synthetic.NeighbourList's layout."""
+        b, ns, npair = self._c, self.n_sites, self.n_pairs
+
+        def get(ptr, shape, ts, dt):
+            if int(np.prod(shape)) == 0:
+                return np.zeros(shape, dtype=dt)
+            return torch.as_tensor(_DeviceView(ptr, shape, ts), device="cuda").cpu().numpy().copy()
+        return {
+            "n_neigh": get(b.n_neigh, (ns,), "<i4", np.int32),
+            "rjs": get(b.rjs, (npair,), "<f8", np.float64),
+            "thetas": get(b.thetas, (npair,), "<f8", np.float64),
+            "phis": get(b.phis, (npair,), "<f8", np.float64),
+            "mask": get(b.mask, (self._n_species, npair), "|u1", np.uint8),
+            "species": get(b.species, (ns, self.max_mult), "<i4", np.int32),
+            "species_multiplicity": get(b.species_multiplicity, (ns,), "<i4", np.int32),
+            "neigh_atom": get(self._neigh_atom, (npair,), "<i4", np.int32),
+        }
+
+
 class Context:
     def __init__(self, hyper, *, legacy_filter_seed=True, compress=None, device=None):
         """``hyper``: a synthetic.Hyper-like object (alpha_max, l_max, per-species
@@ -136,6 +180,31 @@ class Context:
         v = C.c_int64(0)
         _lib.check(self._lib.soapb_launch_count(self._h, C.byref(v)))
         return v.value
+
+    def build_neighbors(self, positions, lattice, atom_species, sites, atom_mult=None,
+                        rcut=0.0) -> BuiltBatch:
+        """soapb_build_neighbors: the CSR neighbour list of one periodic
+        structure, built on the GPU.  positions: (n_atoms, 3) float64 CUDA
+        tensor; lattice: 3x3 host array, rows = cell vectors; atom_species:
+        (n_atoms, max_mult) int32 CUDA tensor of 1-based species (0 beyond an
+        atom's multiplicity); sites: (n_sites,) int32 CUDA tensor of atom
+        indices; atom_mult: (n_atoms,) int32 (default: the non-zero entries)."""
+        pos = positions.contiguous()
+        sp = atom_species.to(torch.int32).contiguous()
+        if sp.dim() == 1:
+            sp = sp.reshape(-1, 1)
+        if atom_mult is None:
+            atom_mult = (sp > 0).sum(dim=1).to(torch.int32)
+        am = atom_mult.to(torch.int32).contiguous()
+        st = sites.to(torch.int32).contiguous()
+        lat = np.ascontiguousarray(lattice, dtype=np.float64).reshape(9)
+        out = _lib.Batch()
+        na = C.c_void_p()
+        _lib.check(self._lib.soapb_build_neighbors(
+            self._h, int(pos.shape[0]), C.c_void_p(pos.data_ptr()), lat.ctypes.data_as(_lib.f64p),
+            C.c_void_p(sp.data_ptr()), int(sp.shape[1]), C.c_void_p(am.data_ptr()),
+            int(st.shape[0]), C.c_void_p(st.data_ptr()), float(rcut), C.byref(out), C.byref(na)))
+        return BuiltBatch(out, na.value, len(self.hyper.alpha_max))
 
     def kernel_timing(self, capacity: int):
         """soapb_kernel_timing: time the next `capacity` kernel launches with

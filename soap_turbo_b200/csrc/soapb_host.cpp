@@ -198,6 +198,9 @@ struct soapb_context {
   // arena
   DBuf off, bits, err, keep_c, keep_norm, rad, ang;
   DBuf f64_rad, f64_rad_der, f64_ang, f64_cnk, f64_soap_un, f64_norm;
+  // neighbour-list builder: cell list, counts and the batch it hands out
+  DBuf nb_acell, nb_ccount, nb_cstart, nb_cfill, nb_catoms, nb_counts, nb_off, nb_state;
+  DBuf nb_rjs, nb_th, nb_ph, nb_mask, nb_natom, nb_nneigh, nb_species, nb_smult;
   cudaStream_t stream = 0;
   int threads = 0;   // threads per site CTA chosen by the caller (0 = tuned or default)
   int max_ctas = 0;
@@ -223,7 +226,9 @@ struct soapb_context {
   ~soapb_context() {
     timing_release();
     for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &rad, &ang, &f64_rad, &f64_rad_der,
-                    &f64_ang, &f64_cnk, &f64_soap_un, &f64_norm})
+                    &f64_ang, &f64_cnk, &f64_soap_un, &f64_norm, &nb_acell, &nb_ccount, &nb_cstart,
+                    &nb_cfill, &nb_catoms, &nb_counts, &nb_off, &nb_state, &nb_rjs, &nb_th, &nb_ph,
+                    &nb_mask, &nb_natom, &nb_nneigh, &nb_species, &nb_smult})
       b->release();
   }
 };
@@ -1099,6 +1104,130 @@ int soapb_check_inputs(soapb_context *c, int64_t *bad_pair) {
   if (v > (1ull << 33)) return fail(SOAPB_ERR_CUDA, "the CSR offset scan gave up waiting for a preceding tile");
   if (bad_pair) *bad_pair = (int64_t)v;
   return fail(SOAPB_ERR_INPUT, "non-finite or negative pair input at pair %llu", v);
+}
+
+int soapb_build_neighbors(soapb_context *c, int32_t n_atoms, const double *d_positions, const double *lattice,
+                          const int32_t *d_atom_species, int32_t max_mult, const int32_t *d_atom_mult,
+                          int32_t n_sites, const int32_t *d_sites, double rcut, soapb_batch *out,
+                          const int32_t **d_neigh_atom) {
+  if (!c || !lattice || !out) return fail(SOAPB_ERR_ARGUMENT, "null argument");
+  if (n_atoms < 1 || n_sites < 0 || max_mult < 1) return fail(SOAPB_ERR_ARGUMENT, "bad sizes");
+  if (!d_positions || !d_atom_species || !d_atom_mult || (n_sites > 0 && !d_sites))
+    return fail(SOAPB_ERR_ARGUMENT, "null device array");
+  if (!(rcut > 0.0)) rcut = c->P.rcut_max;
+  NbGeom g{};
+  for (int t = 0; t < 9; ++t) g.lat[t] = lattice[t];
+  // inverse of the row-vector cell matrix, the cell's volume and plane spacings
+  const double *A = g.lat;
+  const double cof[9] = {A[4] * A[8] - A[5] * A[7], A[5] * A[6] - A[3] * A[8], A[3] * A[7] - A[4] * A[6],
+                         A[2] * A[7] - A[1] * A[8], A[0] * A[8] - A[2] * A[6], A[1] * A[6] - A[0] * A[7],
+                         A[1] * A[5] - A[2] * A[4], A[2] * A[3] - A[0] * A[5], A[0] * A[4] - A[1] * A[3]};
+  const double det = A[0] * cof[0] + A[1] * cof[1] + A[2] * cof[2];
+  double lmax = 0.0;
+  for (int t = 0; t < 9; ++t) lmax = std::max(lmax, std::fabs(A[t]));
+  if (!(std::fabs(det) > 1e-12 * lmax * lmax * lmax)) return fail(SOAPB_ERR_ARGUMENT, "singular cell");
+  for (int r = 0; r < 3; ++r)
+    for (int col = 0; col < 3; ++col) g.inv[r * 3 + col] = cof[col * 3 + r] / det;
+  for (int d = 0; d < 3; ++d) {
+    // plane spacing along axis d: |det| / |a_e x a_f|, the norm of row d of the cofactors
+    const double *cr = cof + 3 * d;
+    const double width = std::fabs(det) / std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    g.nc[d] = (int)std::max(1.0, std::min(1024.0, std::floor(width / rcut)));
+    g.R[d] = (int)std::ceil(rcut * g.nc[d] / width);
+    if (g.R[d] > kNbMaxReach)
+      return fail(SOAPB_ERR_ARGUMENT, "rcut = %g reaches more than %d cells along a cell axis", rcut, kNbMaxReach);
+  }
+  // no more cells than atoms need: coarser cells only widen the stencil's reach by nothing
+  while ((long)g.nc[0] * g.nc[1] * g.nc[2] > std::max(64L, 2L * n_atoms)) {
+    const int d = (g.nc[0] >= g.nc[1] && g.nc[0] >= g.nc[2]) ? 0 : (g.nc[1] >= g.nc[2] ? 1 : 2);
+    g.nc[d] = (g.nc[d] + 1) / 2;
+  }
+  for (int d = 0; d < 3; ++d) {
+    const double *cr = cof + 3 * d;
+    const double width = std::fabs(det) / std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    g.R[d] = (int)std::ceil(rcut * g.nc[d] / width);
+  }
+  g.rcut2 = rcut * rcut;
+  g.n_atoms = n_atoms;
+  g.n_sites = n_sites;
+  g.max_mult = max_mult;
+  g.n_species = c->n_species;
+  const int n_cells = g.nc[0] * g.nc[1] * g.nc[2];
+  const size_t w_cells = (size_t)prep_err_words(n_cells), w_sites = (size_t)prep_err_words(n_sites);
+  int rc;
+  if ((rc = c->nb_acell.ensure(sizeof(int4) * (size_t)n_atoms)) ||
+      (rc = c->nb_ccount.ensure(sizeof(int) * ((size_t)n_cells + 1))) ||
+      (rc = c->nb_cstart.ensure(sizeof(int) * ((size_t)n_cells + 1))) ||
+      (rc = c->nb_cfill.ensure(sizeof(int) * (size_t)n_cells)) ||
+      (rc = c->nb_catoms.ensure(sizeof(int) * (size_t)n_atoms)) ||
+      (rc = c->nb_counts.ensure(sizeof(int) * ((size_t)n_sites + 1))) ||
+      (rc = c->nb_off.ensure(sizeof(int) * ((size_t)n_sites + 1))) ||
+      (rc = c->nb_state.ensure(8 * (1 + w_cells + w_sites))))
+    return rc;
+  unsigned long long *st = c->nb_state.as<unsigned long long>();
+  cudaStream_t s = c->stream;
+  CU(cudaMemsetAsync(c->nb_ccount.p, 0, sizeof(int) * ((size_t)n_cells + 1), s));
+  CU(cudaMemsetAsync(c->nb_cfill.p, 0, sizeof(int) * (size_t)n_cells, s));
+  CU(cudaMemsetAsync(st, 0, 8 * (1 + w_cells + w_sites), s));
+  int4 *acell = c->nb_acell.as<int4>();
+  int *cstart = c->nb_cstart.as<int>(), *catoms = c->nb_catoms.as<int>();
+  CU(launch_nb_bin(g, d_positions, acell, c->nb_ccount.as<int>(), st, s));
+  CU(launch_scan(c->nb_ccount.as<int>(), n_cells, cstart, st + 1, s));
+  CU(launch_nb_place(g, acell, cstart, c->nb_cfill.as<int>(), catoms, s));
+  CU(launch_nb_count(g, d_positions, d_sites, acell, cstart, catoms, c->nb_counts.as<int>(), st, s));
+  CU(launch_scan(c->nb_counts.as<int>(), n_sites, c->nb_off.as<int>(), st + 1 + w_cells, s));
+  c->launches += 4 + (n_sites > 0);
+  int total = 0;
+  if (n_sites > 0) CU(cudaMemcpyAsync(&total, c->nb_off.as<int>() + n_sites, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (total < 0) return fail(SOAPB_ERR_ARGUMENT, "more than 2^31 pairs");
+  const size_t np = (size_t)total;
+  if ((rc = c->nb_rjs.ensure(8 * (np + 1))) || (rc = c->nb_th.ensure(8 * (np + 1))) ||
+      (rc = c->nb_ph.ensure(8 * (np + 1))) || (rc = c->nb_mask.ensure((size_t)c->n_species * np + 16)) ||
+      (rc = c->nb_natom.ensure(4 * (np + 1))) || (rc = c->nb_nneigh.ensure(4 * ((size_t)n_sites + 1))) ||
+      (rc = c->nb_species.ensure(4 * ((size_t)max_mult * n_sites + 1))) ||
+      (rc = c->nb_smult.ensure(4 * ((size_t)n_sites + 1))))
+    return rc;
+  NbOut o{};
+  o.n_pairs = total;
+  o.rjs = c->nb_rjs.as<double>();
+  o.thetas = c->nb_th.as<double>();
+  o.phis = c->nb_ph.as<double>();
+  o.mask = c->nb_mask.as<uint8_t>();
+  o.neigh_atom = c->nb_natom.as<int>();
+  o.n_neigh = c->nb_nneigh.as<int>();
+  o.species = c->nb_species.as<int>();
+  o.species_mult = c->nb_smult.as<int>();
+  CU(launch_nb_fill(g, d_positions, d_sites, d_atom_species, d_atom_mult, acell, cstart, catoms,
+                    c->nb_off.as<int>(), o, st, s));
+  c->launches += (n_sites > 0);
+  unsigned long long w[3] = {0, 0, 0};
+  CU(cudaMemcpyAsync(&w[0], st, 8, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(&w[1], st + 1, 8, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(&w[2], st + 1 + w_cells, 8, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (w[1] || w[2]) return fail(SOAPB_ERR_CUDA, "the neighbour-list scan gave up waiting for a preceding tile");
+  if (w[0]) {
+    const unsigned long long code = kErrTop - w[0];
+    if (code == kErrWrap)
+      return fail(SOAPB_ERR_INPUT, "an atom position is not finite or lies more than %d cells outside the cell",
+                  kNbMaxWrap);
+    if (code < (1ull << 32)) return fail(SOAPB_ERR_INPUT, "sites(%llu) is not an atom index", code + 1);
+    return fail(SOAPB_ERR_ARGUMENT, "site %llu has more than %d neighbours within rcut = %g",
+                code - (1ull << 32) + 1, kNbCap, rcut);
+  }
+  out->n_sites = n_sites;
+  out->n_atom_pairs = total;
+  out->max_species_multiplicity = max_mult;
+  out->n_neigh = o.n_neigh;
+  out->species = o.species;
+  out->species_multiplicity = o.species_mult;
+  out->mask = o.mask;
+  out->rjs = o.rjs;
+  out->thetas = o.thetas;
+  out->phis = o.phis;
+  if (d_neigh_atom) *d_neigh_atom = o.neigh_atom;
+  return SOAPB_OK;
 }
 
 int soapb_launch_count(const soapb_context *c, int64_t *count) {

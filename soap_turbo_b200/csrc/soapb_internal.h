@@ -143,6 +143,45 @@ size_t descriptor_smem(const DevParams &P, int threads);
 cudaError_t noalloc_scratch(int device, unsigned char **addr, size_t *bytes);
 size_t contract_smem(const DevParams &P, int threads);
 
+// Error codes reported through an error word (kErrTop - code under atomicMax,
+// so the smallest code wins; 0 = none): a pair or site index below 2^32, else
+constexpr unsigned long long kErrCsr = 1ull << 33;        // n_neigh negative or sum != n_pairs
+constexpr unsigned long long kErrScan = (1ull << 33) + 1;  // the scan's look-back wait gave up
+constexpr unsigned long long kErrWrap = (1ull << 33) + 2;  // an atom far outside the cell
+constexpr unsigned long long kErrTop = 1ull << 34;
+
+// Neighbour-list builder (soapb_neigh.cu)
+constexpr int kNbCap = 1024;  // neighbours within rcut of one site the fill pass can sort
+constexpr int kNbMaxWrap = 200;  // |lattice translation| that wraps an atom into the cell
+constexpr int kNbMaxReach = 100; // cells a site may visit on each side
+struct NbGeom {
+  double lat[9];   // cell vectors a, b, c as rows (Cartesian)
+  double inv[9];   // inverse: fractional s = r . inv (row vectors)
+  int nc[3];       // cells along each axis (each at least rcut wide)
+  int R[3];        // cells visited on each side of a site's own
+  double rcut2;
+  int n_atoms, n_sites, max_mult, n_species;
+};
+struct NbOut {     // get_soap's inputs, plus the atom behind every pair
+  int n_pairs;
+  double *rjs, *thetas, *phis;
+  uint8_t *mask;   // (n_species, n_pairs)
+  int *neigh_atom, *n_neigh, *species, *species_mult;
+};
+cudaError_t launch_nb_bin(const NbGeom &g, const double *pos, int4 *atom_cell, int *cell_count,
+                          unsigned long long *err, cudaStream_t s);
+cudaError_t launch_nb_place(const NbGeom &g, const int4 *atom_cell, const int *cell_start, int *cell_fill,
+                            int *cell_atoms, cudaStream_t s);
+cudaError_t launch_nb_count(const NbGeom &g, const double *pos, const int *sites, const int4 *atom_cell,
+                            const int *cell_start, const int *cell_atoms, int *counts, unsigned long long *err,
+                            cudaStream_t s);
+cudaError_t launch_nb_fill(const NbGeom &g, const double *pos, const int *sites, const int *atom_species,
+                           const int *atom_mult, const int4 *atom_cell, const int *cell_start, const int *cell_atoms,
+                           const int *off, const NbOut &o, unsigned long long *err, cudaStream_t s);
+// Exclusive scan of n counts into off (n + 1 entries); state: prep_err_words(n)
+// words cleared beforehand.
+cudaError_t launch_scan(const int *counts, int n, int *off, unsigned long long *state, cudaStream_t s);
+
 // Plain FP64 staged path
 struct Fp64Work {
   double *rad, *rad_der;   // (n_pairs, n_max)

@@ -25,128 +25,13 @@
 #include <cstdio>
 
 #include "soapb_device.cuh"
+#include "soapb_scan.cuh"
 
 namespace soapb {
 
 constexpr double kFourPi = 12.566370614359172954;
 
 // ------------------------------------------------------------------ prep
-// CSR offsets, per-pair mask bits and input checks.  DevBatch::err holds
-// prep_err_words(n_sites) 64-bit words, all cleared by one memset before the
-// prep launch:
-//   err[0]     the first input error: 2^34 - code under atomicMax, so the
-//              smallest code wins (0 = none); code = a bad pair's index, or
-//              kErrCsr / kErrScan;
-//   err[1]     the scan's tile counter (low 32 bits);
-//   err[2 + t] scan tile t's status: flag << 32 | sum, flag 1 = the tile's own
-//              sum, 2 = the inclusive prefix up to the tile (0 = not yet);
-//   the last word: the two work counters of the persistent site kernels.
-// n_neigh is scanned in tiles of 2048 sites with a decoupled look-back: each
-// tile publishes its sum, then walks back over its predecessors until it meets
-// an inclusive prefix.  A tile takes its index from the counter, so every
-// predecessor it waits for has already started; the wait is bounded.
-constexpr int kScanTile = 2048;
-constexpr unsigned long long kErrCsr = 1ull << 33;        // n_neigh negative or sum != n_pairs
-constexpr unsigned long long kErrScan = (1ull << 33) + 1;  // look-back wait gave up
-constexpr unsigned long long kErrTop = 1ull << 34;
-
-__host__ __device__ inline int prep_scan_tiles(int n_sites) { return (n_sites + kScanTile - 1) / kScanTile; }
-
-__device__ __forceinline__ void prep_error(const DevBatch &B, unsigned long long code) {
-  atomicMax(B.err, kErrTop - code);
-}
-
-// One scan tile per calling block (NTH threads); sv: kScanTile ints of shared memory.
-template <int NTH>
-__device__ __forceinline__ void prep_scan_tile(const DevBatch &B, int scan_tiles, int *sv) {
-  constexpr int ITEMS = kScanTile / NTH;
-  __shared__ int wtot[NTH / 32];
-  __shared__ int s_tile, s_excl;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  unsigned *counter = (unsigned *)(B.err + 1);
-  unsigned long long *status = B.err + 2;
-  if (tid == 0) s_tile = (int)atomicAdd(counter, 1u);
-  __syncthreads();
-  const int tile = s_tile;
-  if (tile >= scan_tiles) {
-    if (tid == 0) prep_error(B, kErrScan);
-    return;
-  }
-  const int base = tile * kScanTile;
-  bool bad = false;
-#pragma unroll
-  for (int j = 0; j < ITEMS; ++j) {
-    const int i = base + j * NTH + tid;
-    int v = i < B.n_sites ? B.n_neigh[i] : 0;
-    if (v < 0) {
-      bad = true;
-      v = 0;
-    }
-    sv[j * NTH + tid] = v;
-  }
-  if (bad) prep_error(B, kErrCsr);
-  __syncthreads();
-  int loc[ITEMS], sum = 0;
-#pragma unroll
-  for (int j = 0; j < ITEMS; ++j) {
-    loc[j] = sum;
-    sum += sv[tid * ITEMS + j];
-  }
-  int x = sum;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) wtot[warp] = x;
-  __syncthreads();
-  int wpre = 0, total = 0;
-#pragma unroll
-  for (int w = 0; w < NTH / 32; ++w) {
-    if (w < warp) wpre += wtot[w];
-    total += wtot[w];
-  }
-  const int tpre = wpre + x - sum;  // exclusive prefix of this thread's items in the tile
-  if (tid == 0) {
-    volatile unsigned long long *vs = status;
-    long long excl = 0;
-    if (tile == 0) {
-      vs[0] = (2ull << 32) | (unsigned)total;
-    } else {
-      vs[tile] = (1ull << 32) | (unsigned)total;
-      int j = tile - 1, spins = 0;
-      while (j >= 0) {
-        const unsigned long long w = vs[j];
-        const unsigned f = (unsigned)(w >> 32);
-        if (f == 1u || f == 2u) {
-          excl += (unsigned)w;
-          if (f == 2u) break;
-          --j;
-        } else if (++spins > (1 << 20)) {
-          prep_error(B, kErrScan);
-          break;
-        } else {
-          __nanosleep(64);
-        }
-      }
-      vs[tile] = (2ull << 32) | (unsigned)(excl + total);
-    }
-    s_excl = (int)excl;
-  }
-  __syncthreads();
-  const int e0 = s_excl + tpre;
-#pragma unroll
-  for (int j = 0; j < ITEMS; ++j) {
-    const int i = base + tid * ITEMS + j;
-    if (i < B.n_sites) B.off[i] = e0 + loc[j];
-  }
-  if (tile == scan_tiles - 1 && tid == 0) {
-    const long long all = (long long)s_excl + total;
-    B.off[B.n_sites] = (int)all;
-    if (all != (long long)B.n_pairs) prep_error(B, kErrCsr);
-  }
-}
-
 // The species bits of pair k from the reference's mask(n_pairs, n_species),
 // written to B.bits, with the pair's inputs checked.
 __device__ __forceinline__ unsigned prep_pair(const DevBatch &B, int k, int n_species) {
