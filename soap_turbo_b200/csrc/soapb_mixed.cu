@@ -31,14 +31,6 @@ namespace soapb {
 
 constexpr double kFourPi = 12.566370614359172954;
 
-// Programmatic dependent launch: the site kernels are launched so that they
-// may start while the kernel before them drains.  A kernel lets its dependent
-// be scheduled early (pdl_release, which only allows scheduling) and a
-// dependent waits for its predecessor to complete, with its memory visible,
-// before it reads what that kernel wrote (pdl_wait; immediate when the kernel
-// was launched without the attribute).
-__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
 
 
 // ------------------------------------------------------------------ prep
@@ -235,7 +227,6 @@ template <int AMAX, int LC>
 __global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch B, int do_der,
                                               int scan_tiles) {
   extern __shared__ __align__(16) unsigned char smem[];
-  pdl_release();
   if ((int)blockIdx.x < scan_tiles) {
     prep_scan_tile<128>(B, scan_tiles, (int *)smem);
     return;
@@ -301,11 +292,14 @@ __global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch 
     }
   }
   __syncthreads();
-  const int n = min(128, B.n_pairs - k0) * AW;
-  float *dst = B.ang + (size_t)k0 * AW;
-  for (int t = threadIdx.x; t < n; t += 128) {
-    const int i = t / AW;
-    dst[t] = rows[i * AWS + (t - i * AW)];
+  // coalesced 16-byte stores of the CTA's rows (AW is a multiple of 4 floats)
+  constexpr int AW4 = AW / 4;
+  const int n4 = min(128, B.n_pairs - k0) * AW4;
+  float4 *dst = (float4 *)(B.ang + (size_t)k0 * AW);
+  for (int t = threadIdx.x; t < n4; t += 128) {
+    const int i = t / AW4;
+    const float *src = rows + i * AWS + 4 * (t - i * AW4);
+    dst[t] = make_float4(src[0], src[1], src[2], src[3]);
   }
 }
 
@@ -588,9 +582,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
   const int KS = P.k_max | 1;
   const int n_max = P.n_max, nsp = P.n_species;
 
-  pdl_release();
   copy_site_blob<NT>(P, smem, 0);
-  pdl_wait();  // the pair kernel's rows, offsets and mask bits
   first_site(B, B.ticket, sSite);
   for (;;) {
     const int site = sSite[0];
@@ -808,7 +800,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
 
   copy_site_blob<NT>(P, smem, 1);
   for (int t = tid; t < 2 * (int)HPL; t += NT) sH[t] = 0.f;  // entries no item writes stay 0
-  pdl_wait();  // the descriptor's soap, kept c_nlm and norms
   first_site(B, B.ticket + 1, sSite);
   for (;;) {
     const int site = sSite[0];
@@ -1056,24 +1047,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
 }
 
 // ------------------------------------------------------------ launchers
-// A launch with programmatic stream serialization: the kernel may be scheduled
-// before the previous kernel in the stream completes (see pdl_wait).
-template <typename... KArgs, typename... Args>
-static cudaError_t launch_dependent(void (*kern)(KArgs...), int grid, int threads, size_t smem,
-                                    cudaStream_t s, Args... args) {
-  cudaLaunchConfig_t lc = {};
-  lc.gridDim = dim3(grid);
-  lc.blockDim = dim3(threads);
-  lc.dynamicSmemBytes = smem;
-  lc.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  lc.attrs = at;
-  lc.numAttrs = 1;
-  return cudaLaunchKernelEx(&lc, kern, args...);
-}
-
 template <typename K>
 static int persistent_grid(K kernel, int threads, size_t smem, int n_sites, int max_ctas) {
   int dev = 0, sms = 0, per_sm = 0;
@@ -1094,8 +1067,7 @@ static cudaError_t run_descriptor(const DevParams &P, const DevBatch &B, const L
   if (e != cudaSuccess) return e;
   if (P.n_sites > 0) {
     const int grid = persistent_grid(kern, NT, sm, P.n_sites, cfg.max_ctas);
-    e = launch_dependent(kern, grid, NT, sm, cfg.stream, P, B, soap, keep_c, keep_norm, keep);
-    if (e != cudaSuccess) return e;
+    kern<<<grid, NT, sm, cfg.stream>>>(P, B, soap, keep_c, keep_norm, keep);
   }
   return cudaGetLastError();
 }
@@ -1110,8 +1082,7 @@ static cudaError_t run_contract(const DevParams &P, const DevBatch &B, const Lau
   if (e != cudaSuccess) return e;
   if (P.n_sites > 0) {
     const int grid = persistent_grid(kern, NT, sm, P.n_sites, cfg.max_ctas);
-    e = launch_dependent(kern, grid, NT, sm, cfg.stream, P, B, soap, G, g_layout, sgn, keep_c, keep_norm, pair);
-    if (e != cudaSuccess) return e;
+    kern<<<grid, NT, sm, cfg.stream>>>(P, B, soap, G, g_layout, sgn, keep_c, keep_norm, pair);
   }
   return cudaGetLastError();
 }
