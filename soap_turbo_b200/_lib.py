@@ -15,6 +15,7 @@ i32p = C.POINTER(C.c_int32)
 i64p = C.POINTER(C.c_int64)
 f64p = C.POINTER(C.c_double)
 u8p = C.POINTER(C.c_uint8)
+vp = C.c_void_p
 
 SOAPB_OK = 0
 ERRORS = {
@@ -60,12 +61,14 @@ class Batch(C.Structure):
 SIGNATURES = {
     "soapb_last_error": (C.c_char_p, []),
     "soapb_version": (C.c_char_p, []),
+    # the drop-in calls take their host arrays as addresses (ndarray.ctypes.data):
+    # per-call conversions dominate their Python overhead otherwise
     "soapb_get_soap": (C.c_int, [
-        C.c_int32, i32p, C.c_int32, i32p, C.c_int32, i32p, C.c_int32, u8p, f64p, f64p, f64p,
-        i32p, C.c_int32, f64p, f64p, f64p, f64p, f64p, f64p, f64p, f64p, f64p, C.c_int32, f64p,
-        C.c_char_p, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, i32p, i32p, f64p,
-        f64p, C.c_int32, f64p, C.c_int32]),
-    "soapb_soap_contract": (C.c_int, [f64p, f64p, C.c_double, f64p, C.c_int32, C.c_int32,
+        C.c_int32, vp, C.c_int32, vp, C.c_int32, vp, C.c_int32, vp, vp, vp, vp,
+        vp, C.c_int32, vp, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int32, vp,
+        C.c_char_p, C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp,
+        vp, C.c_int32, vp, C.c_int32]),
+    "soapb_soap_contract": (C.c_int, [vp, vp, C.c_double, vp, C.c_int32, C.c_int32,
                                       C.c_int32]),
     "soapb_set_legacy_filter_seed": (C.c_int, [C.c_int32]),
     "soapb_get_legacy_filter_seed": (C.c_int, [i32p]),

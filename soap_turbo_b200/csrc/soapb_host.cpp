@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -762,6 +763,8 @@ int ensure_batch(soapb_context *c, const soapb_batch *b, DevBatch &B) {
   B.rad = c->rad.as<float>();
   B.ang = c->ang.as<float>();
   B.ticket = (int *)(B.err + prep_err_words(b->n_sites) - 1);
+  B.site_lo = 0;
+  B.site_hi = b->n_sites;
   return SOAPB_OK;
 }
 
@@ -820,7 +823,29 @@ LaunchCfg site_cfg(const soapb_context *c, bool contract) {
   return LaunchCfg{128, c->stream, c->max_ctas};
 }
 
-int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int keep) {
+// Status of the inputs from the prep error word a launch left (see soapb_scan.cuh).
+int input_status(unsigned long long w, int64_t *bad_pair) {
+  if (bad_pair) *bad_pair = -1;
+  const unsigned long long v = prep_error_code(w);
+  if (v == ~0ull) return SOAPB_OK;
+  if (v == (1ull << 33)) return fail(SOAPB_ERR_INPUT, "n_neigh is negative or does not sum to n_atom_pairs");
+  if (v > (1ull << 33)) return fail(SOAPB_ERR_CUDA, "the CSR offset scan gave up waiting for a preceding tile");
+  if (bad_pair) *bad_pair = (int64_t)v;
+  return fail(SOAPB_ERR_INPUT, "non-finite or negative pair input at pair %llu", v);
+}
+
+// Site chunks for the drop-in layer's overlap of copies with the site kernels:
+// the site kernel runs once per chunk [bounds[i], bounds[i + 1]); before(i) runs
+// before chunk i's launch (to make the stream wait for its inputs) and after(i)
+// after it (to start the copy of its outputs).
+struct SiteChunks {
+  int n = 1;
+  const int *bounds = nullptr;
+  std::function<int(int)> before, after;
+};
+
+int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int keep,
+                   const SiteChunks *ch = nullptr) {
   DevBatch B{};
   int rc = ensure_batch(c, b, B);
   if (rc) return rc;
@@ -841,12 +866,19 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
     CU(launch_pair(P, B, c->stream, keep));
     c->launches += 1;
   }
-  if (b->n_sites > 0) {
-    TimedLaunch tl(c, SOAPB_KERNEL_DESCRIPTOR);
-    CU(launch_descriptor(P, B, cfg, d_soap, keep ? c->keep_c.as<float>() : nullptr,
-                         keep ? c->keep_norm.as<double>() : nullptr, keep));
+  const int nch = (ch && b->n_sites > 0) ? ch->n : 1;
+  for (int i = 0; i < nch && b->n_sites > 0; ++i) {
+    B.site_lo = ch ? ch->bounds[i] : 0;
+    B.site_hi = ch ? ch->bounds[i + 1] : b->n_sites;
+    if (ch && ch->before && (rc = ch->before(i))) return rc;
+    {
+      TimedLaunch tl(c, SOAPB_KERNEL_DESCRIPTOR);
+      CU(launch_descriptor(P, B, cfg, d_soap, keep ? c->keep_c.as<float>() : nullptr,
+                           keep ? c->keep_norm.as<double>() : nullptr, keep));
+    }
+    c->launches += 1;
+    if (ch && ch->after && (rc = ch->after(i))) return rc;
   }
-  c->launches += (b->n_sites > 0);
   c->keep_valid = keep;
   c->keep_sites = b->n_sites;
   c->keep_pairs = b->n_atom_pairs;
@@ -854,7 +886,7 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
 }
 
 int ctx_contract(soapb_context *c, const soapb_batch *b, const double *d_soap, const double *d_G,
-                 int g_layout, double sgn, double *d_pair) {
+                 int g_layout, double sgn, double *d_pair, const SiteChunks *ch = nullptr) {
   if (!c->keep_valid || c->keep_sites != b->n_sites || c->keep_pairs != b->n_atom_pairs)
     return fail(SOAPB_ERR_CONTRACT_STATE,
                 "ERROR: soap_contract needs get_soap called with contract = .true. first");
@@ -867,12 +899,19 @@ int ctx_contract(soapb_context *c, const soapb_batch *b, const double *d_soap, c
   P.n_pairs = B.n_pairs;
   P.n_sites = B.n_sites;
   LaunchCfg cfg = site_cfg(c, true);
-  if (b->n_sites > 0) {
-    TimedLaunch tl(c, SOAPB_KERNEL_CONTRACT);
-    CU(launch_contract(P, B, cfg, d_soap, d_G, g_layout, sgn, c->keep_c.as<float>(),
-                       c->keep_norm.as<double>(), d_pair));
+  const int nch = (ch && b->n_sites > 0) ? ch->n : 1;
+  for (int i = 0; i < nch && b->n_sites > 0; ++i) {
+    B.site_lo = ch ? ch->bounds[i] : 0;
+    B.site_hi = ch ? ch->bounds[i + 1] : b->n_sites;
+    if (ch && ch->before && (rc = ch->before(i))) return rc;
+    {
+      TimedLaunch tl(c, SOAPB_KERNEL_CONTRACT);
+      CU(launch_contract(P, B, cfg, d_soap, d_G, g_layout, sgn, c->keep_c.as<float>(),
+                         c->keep_norm.as<double>(), d_pair));
+    }
+    c->launches += 1;
+    if (ch && ch->after && (rc = ch->after(i))) return rc;
   }
-  c->launches += (b->n_sites > 0);
   return SOAPB_OK;
 }
 
@@ -1063,6 +1102,8 @@ int soapb_descriptor_noalloc(soapb_context *c, const soapb_batch *b, double *d_s
   B.bits = (uint8_t *)(base + o_bits);
   B.err = (unsigned long long *)(base + o_err);
   B.ticket = (int *)(B.err + prep_err_words(b->n_sites) - 1);
+  B.site_lo = 0;
+  B.site_hi = b->n_sites;
   B.rad = (float *)(base + o_rad);
   B.ang = (float *)(base + o_ang);
   int rc = clear_prep_state(c, B);
@@ -1098,12 +1139,7 @@ int soapb_check_inputs(soapb_context *c, int64_t *bad_pair) {
   unsigned long long w = 0;
   CU(cudaMemcpyAsync(&w, c->err.p, sizeof w, cudaMemcpyDeviceToHost, c->stream));
   CU(cudaStreamSynchronize(c->stream));
-  const unsigned long long v = prep_error_code(w);
-  if (v == ~0ull) return SOAPB_OK;
-  if (v == (1ull << 33)) return fail(SOAPB_ERR_INPUT, "n_neigh is negative or does not sum to n_atom_pairs");
-  if (v > (1ull << 33)) return fail(SOAPB_ERR_CUDA, "the CSR offset scan gave up waiting for a preceding tile");
-  if (bad_pair) *bad_pair = (int64_t)v;
-  return fail(SOAPB_ERR_INPUT, "non-finite or negative pair input at pair %llu", v);
+  return input_status(w, bad_pair);
 }
 
 int soapb_build_neighbors(soapb_context *c, int32_t n_atoms, const double *d_positions, const double *lattice,
@@ -1500,7 +1536,35 @@ struct DropIn {
   soapb_batch batch{};
   int ct_ready = 0, ct_fp64 = 0, ct_n_sites = 0, ct_n_pairs = 0, ct_n_soap = 0;
   cudaStream_t stream = nullptr;
+  // overlap of host copies with the site kernels (mixed path): the sites go in
+  // chunks, each chunk's outputs copied back (and, in soap_contract, its inputs
+  // copied in) on their own streams while the next chunk computes
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  std::vector<cudaEvent_t> evs;
+  std::vector<int> chunk;                  // site chunk bounds of the last get_soap
+  std::vector<long long> host_off;         // its CSR offsets
+  unsigned long long *err_host = nullptr;  // pinned copy of the prep error word
 };
+
+// Site chunks of a drop-in call: about 384 sites each, at most 8 (1 chunk for
+// small batches, and with do_timing, whose per-phase times need the phases apart).
+void plan_chunks(DropIn &d, int n_sites, bool whole) {
+  const int n = whole ? 1 : std::max(1, std::min(8, n_sites / 384));
+  d.chunk.resize(n + 1);
+  for (int i = 0; i <= n; ++i) d.chunk[i] = (int)((long long)n_sites * i / n);
+}
+
+int dropin_streams(DropIn &d, int n_events) {
+  if (!d.copy_in) CU(cudaStreamCreateWithFlags(&d.copy_in, cudaStreamNonBlocking));
+  if (!d.copy_out) CU(cudaStreamCreateWithFlags(&d.copy_out, cudaStreamNonBlocking));
+  if (!d.err_host) CU(cudaMallocHost((void **)&d.err_host, sizeof(unsigned long long)));
+  while ((int)d.evs.size() < n_events) {
+    cudaEvent_t e;
+    CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    d.evs.push_back(e);
+  }
+  return SOAPB_OK;
+}
 
 DropIn &dropin() {
   static DropIn d;
@@ -1610,10 +1674,13 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
   if (n_sites > 0 && !n_neigh) return fail(SOAPB_ERR_ARGUMENT, "null n_neigh");
   // CSR check on the host: the kernels trust the offsets
   long long total = 0;
+  d.host_off.resize((size_t)n_sites + 1);
   for (int i = 0; i < n_sites; ++i) {
     if (n_neigh[i] < 0) return fail(SOAPB_ERR_INPUT, "n_neigh(%d) is negative", i + 1);
+    d.host_off[i] = total;
     total += n_neigh[i];
   }
+  d.host_off[n_sites] = total;
   if (total != n_atom_pairs)
     return fail(SOAPB_ERR_INPUT, "sum(n_neigh) = %lld but n_atom_pairs = %d", total, n_atom_pairs);
   for (int i = 0; i < n_sites; ++i)
@@ -1703,23 +1770,50 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
   bt.phis = d.phis.as<double>();
   if (do_timing) cudaEventRecord(ev[1], s);
   const bool keep_cart = fp64 && do_derivatives;  // FP64 contract works on soap_cart_der
+  bool soap_copied = false;
   if (fp64) {
     if (keep_cart && (rc = d.cart.ensure(8 * ((size_t)n_atom_pairs * n_soap * 3 + 1)))) return rc;
     rc = soapb_descriptor_fp64(c, &bt, d.soap.as<double>(), keep_cart ? d.cart.as<double>() : nullptr);
   } else {
-    rc = soapb_descriptor(c, &bt, d.soap.as<double>(), do_derivatives && contract);
+    // each chunk's soap rows go back while the next chunk computes
+    plan_chunks(d, n_sites, do_timing != 0);
+    const int nch = (int)d.chunk.size() - 1;
+    if ((rc = dropin_streams(d, 2 * nch))) return rc;
+    SiteChunks ch;
+    ch.n = nch;
+    ch.bounds = d.chunk.data();
+    if (!do_timing)
+      ch.after = [&](int i) -> int {
+        const size_t lo = (size_t)d.chunk[i], hi = (size_t)d.chunk[i + 1];
+        CU(cudaEventRecord(d.evs[i], s));
+        CU(cudaStreamWaitEvent(d.copy_out, d.evs[i], 0));
+        CU(cudaMemcpyAsync(soap + lo * n_soap, d.soap.as<double>() + lo * n_soap, 8 * (hi - lo) * n_soap,
+                           cudaMemcpyDeviceToHost, d.copy_out));
+        return SOAPB_OK;
+      };
+    rc = ctx_descriptor(c, &bt, d.soap.as<double>(), do_derivatives && contract, &ch);
+    soap_copied = !do_timing;
   }
-  if (rc) return rc;
+  if (rc) {
+    if (soap_copied) cudaStreamSynchronize(d.copy_out);  // no copy into soap outlives the call
+    return rc;
+  }
   if (do_timing) cudaEventRecord(ev[2], s);
-  if (n_sites > 0)
+  if (n_sites > 0 && !soap_copied)
     CU(cudaMemcpyAsync(soap, d.soap.p, 8 * (size_t)n_sites * n_soap, cudaMemcpyDeviceToHost, s));
   if (want_cart && n_atom_pairs > 0)
     CU(cudaMemcpyAsync(soap_cart_der, d.cart.p, 8 * (size_t)n_atom_pairs * n_soap * 3,
                        cudaMemcpyDeviceToHost, s));
   if (do_timing) cudaEventRecord(ev[3], s);
-  CU(cudaStreamSynchronize(s));
-  int64_t bad = -1;
-  if ((rc = soapb_check_inputs(c, &bad))) return rc;
+  // the prep error word comes back with the same wait
+  if ((rc = dropin_streams(d, 0))) return rc;
+  *d.err_host = 0;
+  if (c->err.p) CU(cudaMemcpyAsync(d.err_host, c->err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  const cudaError_t es = cudaStreamSynchronize(s);
+  const cudaError_t eo = soap_copied ? cudaStreamSynchronize(d.copy_out) : cudaSuccess;
+  CU(es);
+  CU(eo);
+  if ((rc = input_status(*d.err_host, nullptr))) return rc;
   if (do_timing) {
     float t01, t12, t23;
     cudaEventElapsedTime(&t01, ev[0], ev[1]);
@@ -1753,19 +1847,59 @@ int soapb_soap_contract(const double *soap, const double *G, double sgn, double 
   if (n_sites > 0 && (!soap || !G || !pair)) return fail(SOAPB_ERR_ARGUMENT, "null pointer");
   cudaStream_t s = d.stream;
   int rc;
-  if ((rc = upload(d.soap, soap, (size_t)n_sites * n_soap, s))) return rc;
-  if ((rc = upload(d.G, G, (size_t)n_sites * n_soap, s))) return rc;
   if ((rc = d.pair.ensure(8 * (3 * (size_t)n_atom_pairs + 1)))) return rc;
-  if (d.ct_fp64)
-    rc = soapb_contract_cart_der(d.ctx, &d.batch, d.cart.as<double>(), d.G.as<double>(),
-                                 SOAPB_G_SITE_FASTEST, sgn, d.pair.as<double>());
-  else
-    rc = soapb_contract(d.ctx, &d.batch, d.soap.as<double>(), d.G.as<double>(), SOAPB_G_SITE_FASTEST,
-                        sgn, d.pair.as<double>());
+  if (d.ct_fp64) {
+    if ((rc = upload(d.soap, soap, (size_t)n_sites * n_soap, s))) return rc;
+    if ((rc = upload(d.G, G, (size_t)n_sites * n_soap, s))) return rc;
+    if ((rc = soapb_contract_cart_der(d.ctx, &d.batch, d.cart.as<double>(), d.G.as<double>(),
+                                      SOAPB_G_SITE_FASTEST, sgn, d.pair.as<double>())))
+      return rc;
+    if (n_atom_pairs > 0)
+      CU(cudaMemcpyAsync(pair, d.pair.p, 24 * (size_t)n_atom_pairs, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    return SOAPB_OK;
+  }
+  // per site chunk: soap rows and G columns in on copy_in, the contract on the
+  // compute stream once they are there, the chunk's pair forces out on copy_out
+  if ((rc = d.soap.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
+  if ((rc = d.G.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
+  if ((int)d.chunk.size() < 2 || d.chunk.back() != n_sites) plan_chunks(d, n_sites, false);
+  const int nch = (int)d.chunk.size() - 1;
+  if ((rc = dropin_streams(d, 2 * nch))) return rc;
+  double *dS = d.soap.as<double>(), *dG = d.G.as<double>(), *dP = d.pair.as<double>();
+  CU(cudaEventRecord(d.evs[0], s));  // the copies in must not overwrite what earlier work still reads
+  CU(cudaStreamWaitEvent(d.copy_in, d.evs[0], 0));
+  for (int i = 0; i < nch && n_sites > 0; ++i) {
+    const size_t lo = (size_t)d.chunk[i], hi = (size_t)d.chunk[i + 1];
+    CU(cudaMemcpyAsync(dS + lo * n_soap, soap + lo * n_soap, 8 * (hi - lo) * n_soap, cudaMemcpyHostToDevice,
+                       d.copy_in));
+    CU(cudaMemcpy2DAsync(dG + lo, 8 * (size_t)n_sites, G + lo, 8 * (size_t)n_sites, 8 * (hi - lo), n_soap,
+                         cudaMemcpyHostToDevice, d.copy_in));
+    CU(cudaEventRecord(d.evs[i], d.copy_in));
+  }
+  SiteChunks ch;
+  ch.n = nch;
+  ch.bounds = d.chunk.data();
+  ch.before = [&](int i) -> int {
+    CU(cudaStreamWaitEvent(s, d.evs[i], 0));
+    return SOAPB_OK;
+  };
+  ch.after = [&](int i) -> int {
+    const long long p0 = d.host_off[d.chunk[i]], p1 = d.host_off[d.chunk[i + 1]];
+    CU(cudaEventRecord(d.evs[nch + i], s));
+    CU(cudaStreamWaitEvent(d.copy_out, d.evs[nch + i], 0));
+    if (p1 > p0)
+      CU(cudaMemcpyAsync(pair + 3 * p0, dP + 3 * p0, 24 * (size_t)(p1 - p0), cudaMemcpyDeviceToHost, d.copy_out));
+    return SOAPB_OK;
+  };
+  rc = ctx_contract(d.ctx, &d.batch, dS, dG, SOAPB_G_SITE_FASTEST, sgn, dP, &ch);
+  // whatever ran, no copy may still be in flight when this returns
+  const cudaError_t e1 = cudaStreamSynchronize(d.copy_in), e2 = cudaStreamSynchronize(s),
+                    e3 = cudaStreamSynchronize(d.copy_out);
   if (rc) return rc;
-  if (n_atom_pairs > 0)
-    CU(cudaMemcpyAsync(pair, d.pair.p, 24 * (size_t)n_atom_pairs, cudaMemcpyDeviceToHost, s));
-  CU(cudaStreamSynchronize(s));
+  CU(e1);
+  CU(e2);
+  CU(e3);
   return SOAPB_OK;
 }
 

@@ -113,6 +113,7 @@ struct DevBatch {
   float *ang;            // (n_pairs, ang_row): the pair's angular row (see soapb_mixed.cu)
   int *ticket;           // work counters of the persistent site kernels, in the last word
                          // of err (the kernels put them back to 0 when they finish)
+  int site_lo, site_hi;  // the sites a site-kernel launch processes (all: 0, n_sites)
 };
 
 // Kernel launchers (soapb_mixed.cu, soapb_fp64.cu)

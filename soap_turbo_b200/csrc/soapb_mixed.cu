@@ -403,25 +403,27 @@ __device__ __forceinline__ const RadSp &rad_of(const unsigned char *smem, const 
 // loads that site's bounds part-way through (ahead_bounds) and hands the three
 // values to the CTA in cur[] when the site ends (ahead_publish, which also
 // synchronises).  The first site is fetched by first_site.
-// Each CTA takes tickets until one is past the last site, so a launch hands out
-// exactly n_sites + gridDim.x of them; the CTA holding the last one puts the
-// counter back to 0 for the next launch.
-__device__ __forceinline__ int take_ticket(int *ticket, int n_sites) {
+// A launch processes the sites [site_lo, site_hi) of the batch.  Each CTA takes
+// tickets until one is past the last site, so a launch hands out exactly
+// (site_hi - site_lo) + gridDim.x of them; the CTA holding the last one puts
+// the counter back to 0 for the next launch.  Returns the site (>= site_hi: none left).
+__device__ __forceinline__ int take_ticket(const DevBatch &B, int *ticket) {
+  const int n = B.site_hi - B.site_lo;
   const int t = atomicAdd(ticket, 1);
-  if (t == n_sites + (int)gridDim.x - 1) atomicExch(ticket, 0);
-  return t;
+  if (t == n + (int)gridDim.x - 1) atomicExch(ticket, 0);
+  return B.site_lo + min(t, n);
 }
 __device__ __forceinline__ void first_site(const DevBatch &B, int *ticket, int *cur) {
   if (threadIdx.x == 0) {
-    const int s0 = take_ticket(ticket, B.n_sites);
+    const int s0 = take_ticket(B, ticket);
     cur[0] = s0;
-    cur[1] = s0 < B.n_sites ? B.off[s0] : 0;
-    cur[2] = s0 < B.n_sites ? B.off[s0 + 1] : 0;
+    cur[1] = s0 < B.site_hi ? B.off[s0] : 0;
+    cur[2] = s0 < B.site_hi ? B.off[s0 + 1] : 0;
   }
   __syncthreads();
 }
 __device__ __forceinline__ void ahead_bounds(const DevBatch &B, int nx, int &nx0, int &nx1) {
-  if (threadIdx.x == 0 && nx < B.n_sites) {
+  if (threadIdx.x == 0 && nx < B.site_hi) {
     nx0 = B.off[nx];
     nx1 = B.off[nx + 1];
   }
@@ -586,11 +588,11 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
   first_site(B, B.ticket, sSite);
   for (;;) {
     const int site = sSite[0];
-    if (site >= B.n_sites) break;
+    if (site >= B.site_hi) break;
     const int p_begin = sSite[1];
     const int p_end = min(sSite[2], B.n_pairs);
     int nx = 0, nx0 = 0, nx1 = 0;
-    if (tid == 0) nx = take_ticket(B.ticket, B.n_sites);  // the next site, fetched ahead
+    if (tid == 0) nx = take_ticket(B, B.ticket);  // the next site, fetched ahead
     for (int t = tid; t < 2 * n_max * KS; t += NT) sC64[t] = 0.0;
     __syncthreads();
 
@@ -803,11 +805,11 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
   first_site(B, B.ticket + 1, sSite);
   for (;;) {
     const int site = sSite[0];
-    if (site >= n_sites) break;
+    if (site >= B.site_hi) break;
     const int p_begin = sSite[1];
     const int p_end = min(sSite[2], B.n_pairs);
     int nx = 0, nx0 = 0, nx1 = 0;
-    if (tid == 0) nx = take_ticket(B.ticket + 1, n_sites);  // the next site, fetched ahead
+    if (tid == 0) nx = take_ticket(B, B.ticket + 1);  // the next site, fetched ahead
     // ---- every per-site load is issued here, so their latencies overlap
     const double knorm = keep_norm[site];
     const double *q = soap_in + (size_t)site * n_soap;
@@ -1065,8 +1067,8 @@ static cudaError_t run_descriptor(const DevParams &P, const DevBatch &B, const L
   auto kern = k_descriptor<NT, AMAX, LC>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  if (P.n_sites > 0) {
-    const int grid = persistent_grid(kern, NT, sm, P.n_sites, cfg.max_ctas);
+  if (B.site_hi > B.site_lo) {
+    const int grid = persistent_grid(kern, NT, sm, B.site_hi - B.site_lo, cfg.max_ctas);
     kern<<<grid, NT, sm, cfg.stream>>>(P, B, soap, keep_c, keep_norm, keep);
   }
   return cudaGetLastError();
@@ -1080,8 +1082,8 @@ static cudaError_t run_contract(const DevParams &P, const DevBatch &B, const Lau
   auto kern = k_contract<NT, AMAX, LC>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  if (P.n_sites > 0) {
-    const int grid = persistent_grid(kern, NT, sm, P.n_sites, cfg.max_ctas);
+  if (B.site_hi > B.site_lo) {
+    const int grid = persistent_grid(kern, NT, sm, B.site_hi - B.site_lo, cfg.max_ctas);
     kern<<<grid, NT, sm, cfg.stream>>>(P, B, soap, G, g_layout, sgn, keep_c, keep_norm, pair);
   }
   return cudaGetLastError();

@@ -26,7 +26,14 @@ def _p(a, t):
     return a.ctypes.data_as(t)
 
 
+def _a(a):
+    """The array's address, for the drop-in calls' void-pointer arguments."""
+    return a.ctypes.data
+
+
 def _per_species(v, n):
+    if isinstance(v, (float, int)):
+        return np.full(n, float(v))
     v = np.atleast_1d(np.asarray(v, dtype=_f64))
     if v.shape[0] == 1 and n > 1:
         v = np.repeat(v, n)
@@ -77,16 +84,14 @@ def get_soap(n_sites, n_neigh, n_species, species, species_multiplicity, n_atom_
     if soap_cart_der is not None:
         if not (soap_cart_der.dtype == _f64 and soap_cart_der.flags.f_contiguous):
             raise TypeError("soap_cart_der must be a Fortran-ordered float64 array")
-        cart_ptr = _p(soap_cart_der, _lib.f64p)
+        cart_ptr = _a(soap_cart_der)
     _lib.check(lib.soapb_get_soap(
-        int(n_sites), _p(n_neigh, _lib.i32p), int(n_species), _p(species, _lib.i32p),
-        int(species.shape[0]), _p(species_multiplicity, _lib.i32p), int(n_atom_pairs),
-        _p(mask_u8, _lib.u8p), _p(rjs, _lib.f64p), _p(thetas, _lib.f64p), _p(phis, _lib.f64p),
-        _p(alpha_max, _lib.i32p), int(l_max), *[_p(v, _lib.f64p) for v in ps[:9]],
-        int(radial_enhancement), _p(cw, _lib.f64p), basis.encode(), scaling_mode.encode(),
-        int(bool(do_timing)), int(bool(do_derivatives)), int(bool(compress_soap)),
-        int(compress_P_nonzero), _p(P_i, _lib.i32p), _p(P_j, _lib.i32p), _p(P_el, _lib.f64p),
-        _p(soap, _lib.f64p), int(soap.shape[0]), cart_ptr, int(bool(contract))))
+        int(n_sites), _a(n_neigh), int(n_species), _a(species), int(species.shape[0]),
+        _a(species_multiplicity), int(n_atom_pairs), _a(mask_u8), _a(rjs), _a(thetas), _a(phis),
+        _a(alpha_max), int(l_max), *[_a(v) for v in ps[:9]], int(radial_enhancement), _a(cw),
+        basis.encode(), scaling_mode.encode(), int(bool(do_timing)), int(bool(do_derivatives)),
+        int(bool(compress_soap)), int(compress_P_nonzero), _a(P_i), _a(P_j), _a(P_el), _a(soap),
+        int(soap.shape[0]), cart_ptr, int(bool(contract))))
 
 
 def soap_contract(soap, G, sgn, pair):
@@ -97,9 +102,8 @@ def soap_contract(soap, G, sgn, pair):
     G = _f(G, _f64)
     if not (isinstance(pair, np.ndarray) and pair.dtype == _f64 and pair.flags.f_contiguous):
         raise TypeError("pair must be a Fortran-ordered float64 array (written in place)")
-    _lib.check(lib.soapb_soap_contract(_p(soap, _lib.f64p), _p(G, _lib.f64p), float(sgn),
-                                       _p(pair, _lib.f64p), int(soap.shape[1]), int(soap.shape[0]),
-                                       int(pair.shape[1])))
+    _lib.check(lib.soapb_soap_contract(_a(soap), _a(G), float(sgn), _a(pair), int(soap.shape[1]),
+                                       int(soap.shape[0]), int(pair.shape[1])))
 
 
 def get_compress_indices(compress_mode, alpha_max, l_max, what_to_do="set_indices"):

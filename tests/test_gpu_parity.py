@@ -153,6 +153,46 @@ def test_dropin_get_soap_and_contract(name):
         D.set_basis_matrices(None)
 
 
+@pytest.mark.parametrize("pinned", [True, False])
+def test_dropin_site_chunks_match_the_context_layer(pinned):
+    """The drop-in layer runs batches of 768 sites or more in site chunks whose
+    copies overlap the kernels (1703 sites here: four chunks); every site's
+    result is computed the same way, so soap and pair equal the single-launch
+    context calls bit for bit, from pinned or pageable host arrays."""
+    import torch
+    w = syn.config(2, seed=41)
+    nl = w.nl
+    assert nl.n_sites >= 4 * 384
+    ctx = Context(w.hyper)
+    W, S = ctx.basis()
+    b = ctx.batch(nl)
+    s_ctx = ctx.descriptor(b, keep=True)
+    G = np.random.default_rng(5).standard_normal((ctx.n_soap, nl.n_sites))
+    p_ctx = ctx.contract(b, s_ctx, torch.as_tensor(G).cuda()).cpu().numpy()
+    s_ctx = s_ctx.cpu().numpy()
+
+    def host(a):
+        if not pinned:
+            return np.asfortranarray(a)
+        t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+        out = t.numpy().reshape(a.shape, order="F")
+        out[...] = a
+        host.keep.append(t)
+        return out
+    host.keep = []
+    D.set_basis_matrices(W, S)
+    try:
+        for _ in range(2):  # a second step reuses the streams, events and buffers
+            soap = host(np.zeros((ctx.n_soap, nl.n_sites)))
+            D.get_soap(**_dropin_args(w, soap), contract=True)
+            np.testing.assert_array_equal(soap.T, s_ctx)
+            pair = host(np.zeros((3, nl.n_pairs)))
+            D.soap_contract(soap, host(G.T), 1.0, pair)
+            np.testing.assert_array_equal(pair.T, p_ctx)
+    finally:
+        D.set_basis_matrices(None)
+
+
 def test_dropin_soap_cart_der_is_fp64():
     w = WORKLOADS["config1"]()
     r = Run(w, cart=True)
