@@ -52,6 +52,12 @@ def lib():
         _lib.or_get_soap.restype = C.c_int
         _lib.or_get_soap.argtypes = [C.POINTER(_Args), C.c_int, _f64p, _f64p, C.POINTER(C.c_void_p)]
         _lib.or_soap_contract.argtypes = [C.c_void_p, _f64p, _f64p, C.c_double, _f64p]
+        _lib.or_get_soap2.restype = C.c_int
+        _lib.or_get_soap2.argtypes = [C.POINTER(_Args), C.c_int, C.c_int, _f64p, _f64p,
+                                      C.POINTER(C.c_void_p)]
+        _lib.or_central_hessian.restype = C.c_int
+        _lib.or_central_hessian.argtypes = [C.POINTER(_Args), C.c_void_p, _f64p, C.c_int, _f64p,
+                                            _f64p, _f64p]
         _lib.or_ctx_free.argtypes = [C.c_void_p]
         for name in ("or_ctx_cnk", "or_ctx_rad", "or_ctx_rad_der", "or_ctx_norm"):
             getattr(_lib, name).restype = _f64p
@@ -74,7 +80,8 @@ def lib():
                                            _i32p, _i32p, _f64p]
         _lib.or_radial_eval.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.c_double, C.c_double, _f64p, C.c_int, C.c_int,
-                                        C.c_double, C.c_int, C.c_int, C.c_int, _f64p, _f64p, _f64p]
+                                        C.c_double, C.c_int, C.c_int, C.c_int, _f64p, _f64p, _f64p,
+                                        _f64p]
         _lib.or_num_threads.restype = C.c_int
     return _lib
 
@@ -150,20 +157,26 @@ def preflm(lmax):
     return out
 
 
-def radial_eval(hyper, species: int, W_block, r, legacy_seed=True, is_central=False):
+def radial_eval(hyper, species: int, W_block, r, legacy_seed=True, is_central=False, der2=False):
+    """The radial expansion of one species at distances r: (values, r-derivatives)
+    and, with der2 (unified seed only), the second r-derivatives as well."""
     a = hyper.alpha_max[species]
     r = np.ascontiguousarray(r, dtype=np.float64)
     out = np.zeros((r.shape[0], a))
     der = np.zeros((r.shape[0], a))
+    d2 = np.zeros((r.shape[0], a)) if der2 else None
     Wb = np.asfortranarray(W_block, dtype=np.float64)
-    lib().or_radial_eval(
+    rc = lib().or_radial_eval(
         1 if hyper.basis == "poly3gauss" else 0, a, hyper.arr("rcut_soft")[species],
         hyper.arr("rcut_hard")[species], hyper.arr("atom_sigma_r")[species],
         hyper.arr("atom_sigma_r_scaling")[species], hyper.arr("amplitude_scaling")[species],
         hyper.arr("nf")[species], _p(Wb, _f64p), 1 if hyper.scaling_mode == "polynomial" else 0,
         hyper.radial_enhancement, hyper.arr("central_weight")[species], int(is_central),
-        int(legacy_seed), r.shape[0], _p(r, _f64p), _p(out, _f64p), _p(der, _f64p))
-    return out, der
+        int(legacy_seed), r.shape[0], _p(r, _f64p), _p(out, _f64p), _p(der, _f64p),
+        _p(d2, _f64p) if der2 else None)
+    if rc:
+        raise ValueError("second radial derivatives need the unified filter seed")
+    return (out, der, d2) if der2 else (out, der)
 
 
 def compress_trivial(alpha_max, l_max):
@@ -224,6 +237,24 @@ class Result:
             raise RuntimeError("oracle soap_contract needs derivatives")
         return pair
 
+    def central_hessian(self, vecs: np.ndarray):
+        """get_soap_central_hessian (src/soap_turbo.f90:1151-1700) on this
+        state (get_soap with hessian=True).  vecs: (n_sites, n_vec, n_soap),
+        the reference's vecs(n_soap, n_vec, n_sites).  Returns (hess, err):
+        hess (n_pairs, n_vec, 3, 3) with hess[k, v, b, a] the reference's
+        hess(a, b, v, k) (a: central atom, b: neighbour), and the self-test's
+        relative error of the rebuilt first derivative."""
+        vecs = np.ascontiguousarray(vecs, dtype=np.float64)
+        n_vec = vecs.shape[1]
+        soap = np.ascontiguousarray(self.soap)
+        hess = np.zeros((self._keep["n_pairs"], n_vec, 3, 3))
+        err = C.c_double(0.0)
+        rc = lib().or_central_hessian(C.byref(self._keep["args"]), self._ctx, _p(soap, _f64p), n_vec,
+                                      _p(vecs, _f64p), _p(hess, _f64p), C.byref(err))
+        if rc:
+            raise RuntimeError("central_hessian needs get_soap(..., hessian=True)")
+        return hess, err.value
+
     def cnk(self):
         c = self._keep
         ptr = lib().or_ctx_cnk(self._ctx)
@@ -262,9 +293,11 @@ def compress_arrays(hyper):
 
 
 def get_soap(hyper, nl, W, S, do_derivatives=True, cart_der=False, legacy_filter_seed=True,
-             compress=None) -> Result:
+             compress=None, hessian=False) -> Result:
     """Run the oracle get_soap.  ``cart_der`` materialises soap_cart_der
-    (contract = .false.); the expansion is always kept for ``contract``."""
+    (contract = .false.); the expansion is always kept for ``contract``;
+    ``hessian`` also keeps the second radial derivatives central_hessian needs
+    (the reference's soap_hessian_enabled; unified filter seed only)."""
     n_species = hyper.n_species
     if compress is None:
         compress = compress_arrays(hyper)
@@ -321,10 +354,10 @@ def get_soap(hyper, nl, W, S, do_derivatives=True, cart_der=False, legacy_filter
     soap = np.zeros((nl.n_sites, n_soap))
     cart = np.zeros((nl.n_pairs, n_soap, 3)) if (do_derivatives and cart_der) else None
     ctx = C.c_void_p()
-    rc = lib().or_get_soap(C.byref(a), int(do_derivatives), _p(soap, _f64p),
-                           _p(cart, _f64p) if cart is not None else None, C.byref(ctx))
+    rc = lib().or_get_soap2(C.byref(a), int(do_derivatives), int(bool(hessian)), _p(soap, _f64p),
+                            _p(cart, _f64p) if cart is not None else None, C.byref(ctx))
     if rc < 0:
         raise RuntimeError(f"oracle get_soap failed ({rc})")
     keep.update(n_sites=nl.n_sites, n_pairs=nl.n_pairs, n_max=n_max,
-                k_max=(hyper.l_max + 1) * (hyper.l_max + 2) // 2, arrays=arrays)
+                k_max=(hyper.l_max + 1) * (hyper.l_max + 2) // 2, arrays=arrays, args=a)
     return Result(soap, cart, ctx.value, keep)

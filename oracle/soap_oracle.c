@@ -31,6 +31,7 @@
  *   species(max_mult, n_sites)         -> species[i*max_mult + m]  (1-based)
  *   W, S (n_max, n_max)                -> W[col*n_max + row]
  */
+#include <complex.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -337,11 +338,11 @@ int or_inverse_sqrt(int a, const double *S, double *W) {
 /* src/soap_turbo_radial.f90:281-1004, one pair at a time.                   */
 /* ------------------------------------------------------------------------ */
 typedef struct {
-  int alpha, n_poly, n_hi, with_gauss, unified, has_filter, do_der;
+  int alpha, n_poly, n_hi, with_gauss, unified, has_filter, do_der, do_der2;
   double rcut_soft, atom_sigma, c, dr, sqrt_rcut, inv_sqrt_rcut, inv_rcut;
   double q, drnf, sigma_sq0, N_gauss, inv_Nm2, amp_scaling, cw;
   int do_central, scaling_poly, radial_enhancement;
-  double Nv[32], ra[32], rb[32], rc[32], R1[32], R2[32]; /* index n+4 */
+  double Nv[32], ra[32], rb[32], rc[32], R1[32], R2[32], R3[32], R4[32]; /* index n+4 */
   const double *W; int ldw;                                /* alpha x alpha block */
 } or_radial_setup;
 
@@ -392,48 +393,77 @@ static void or_radial_init(or_radial_setup *s, int alpha, double rcut_soft_in, d
   }
 }
 
+/* Second radial derivatives as well (src/soap_turbo_radial.f90:489-491,
+ * 520-525): the recursions run to alpha + 4.  Only with the unified filter
+ * seed (:318-328); returns -1 otherwise. */
+static int or_radial_enable_der2(or_radial_setup *s) {
+  if (!s->unified || !s->do_der) return -1;
+  s->do_der2 = 1;
+  s->n_hi = s->n_poly + 4;
+  for (int n = -1; n <= s->n_hi; n++) {
+    s->ra[NI(n)] = (double)(n + 1) * s->Nv[NI(n - 2)] / s->Nv[NI(n)];
+    s->rb[NI(n)] = s->Nv[NI(n - 1)] / s->Nv[NI(n)];
+    s->rc[NI(n)] = 1.0 / s->Nv[NI(n)];
+  }
+  s->ra[NI(-1)] = 0.0;
+  for (int n = 1; n <= s->n_poly; n++) {
+    s->R3[NI(n)] = s->Nv[NI(n + 3)] / s->Nv[NI(n)];
+    s->R4[NI(n)] = s->Nv[NI(n + 4)] / s->Nv[NI(n)];
+  }
+  return 0;
+}
+
 /* One pair of process_block (src/soap_turbo_radial.f90:550-1002).  rj_in is
  * the unscaled distance.  Writes alpha values to out (and der if do_der). */
-static void or_radial_pair(const or_radial_setup *s, double rj_in, int is_central, double *out, double *der) {
+static void or_radial_pair(const or_radial_setup *s, double rj_in, int is_central, double *out, double *der,
+                           double *der2) {
   const double pi = acos(-1.0), sq2 = sqrt(2.0), isq2 = 1.0 / sq2;
   const double sqpi2 = sqrt(pi / 2.0), sq2pi = sqrt(2.0 / pi), sq8pi = sqrt(8.0 / pi);
   const int a = s->alpha, n_hi = s->n_hi, n_poly = s->n_poly;
   const double c = s->c, rs = s->rcut_soft, dr = s->dr;
-  double T1[40], T2[40], pol[40], DT[40], dtot[40];
+  double T1[40], T2[40], pol[40], DT[40], dtot[40], D2T[40], d2tot[40];
   double rj = rj_in * s->inv_rcut;
-  for (int i = 0; i < 40; i++) { T1[i] = T2[i] = pol[i] = DT[i] = dtot[i] = 0.0; }
+  for (int i = 0; i < 40; i++) { T1[i] = T2[i] = pol[i] = DT[i] = dtot[i] = D2T[i] = d2tot[i] = 0.0; }
 
   double sig = s->atom_sigma + c * rj, s2 = sig * sig;               /* :560-570 */
   double isig = 1.0 / sig, is2 = isig * isig, is3 = is2 * isig;
 
-  double amp, ampd;                                                  /* :589-635 */
+  double amp, ampd, ampd2;                                           /* :589-635 */
   if (!s->scaling_poly) {
-    amp = 1.0; ampd = 0.0;
+    amp = 1.0; ampd = 0.0; ampd2 = 0.0;
   } else if (s->amp_scaling == 0.0) {
-    amp = isig; ampd = -c * is2;
+    amp = isig; ampd = -c * is2; ampd2 = 2.0 * c * c * is3;
   } else if (s->amp_scaling == 1.0) {
     double h = 1.0 + 2.0 * (rj * rj * rj) - 3.0 * rj * rj;
-    double hp = 6.0 * rj * rj - 6.0 * rj;
+    double hp = 6.0 * rj * rj - 6.0 * rj, hpp = 12.0 * rj - 6.0;
     double g = isig * h;
     amp = (h <= 1.0e-10) ? 0.0 : g;
     ampd = (h <= 1.0e-10) ? 0.0 : hp * isig - c * isig * g;
+    ampd2 = (h <= 1.0e-10) ? 0.0 : hpp * isig - 2.0 * c * hp * is2 + 2.0 * c * c * h * is3;
   } else {
     double h = 1.0 + 2.0 * (rj * rj * rj) - 3.0 * rj * rj;
-    if (h <= 1.0e-10) { amp = 0.0; ampd = 0.0; }
+    if (h <= 1.0e-10) { amp = 0.0; ampd = 0.0; ampd2 = 0.0; }
     else {
-      double hp = 6.0 * rj * rj - 6.0 * rj, aa = s->amp_scaling;
+      double hp = 6.0 * rj * rj - 6.0 * rj, hpp = 12.0 * rj - 6.0, aa = s->amp_scaling;
       amp = isig * pow(h, aa);
       ampd = aa * pow(h, aa - 1.0) * hp * isig - c * isig * amp;
+      ampd2 = (aa * (aa - 1.0) * pow(h, aa - 2.0) * hp * hp + aa * pow(h, aa - 1.0) * hpp) * isig
+              - 2.0 * c * aa * pow(h, aa - 1.0) * hp * is2 + 2.0 * c * c * pow(h, aa) * is3;
     }
   }
-  if (s->do_central && s->cw != 1.0 && is_central) { amp *= s->cw; ampd *= s->cw; } /* :638-646 */
+  if (s->do_central && s->cw != 1.0 && is_central) {                 /* :638-646 */
+    amp *= s->cw; ampd *= s->cw; ampd2 *= s->cw;
+  }
   if (s->radial_enhancement == 1) {                                  /* :651-670 */
     double g = rj + sq2pi * sig, f = 1.0 + sq2pi * c;
+    ampd2 = ampd2 * g + 2.0 * ampd * f;
     ampd = amp * f + ampd * g;
     amp = amp * g;
   } else if (s->radial_enhancement == 2) {
     double g = rj * rj + s2 + sq8pi * sig * rj;
     double f = 2.0 * rj + 2.0 * sig * c + sq8pi * sig + sq8pi * rj * c;
+    double h = 2.0 + 2.0 * c * c + 2.0 * sq8pi * c;
+    ampd2 = ampd2 * g + 2.0 * ampd * f + amp * h;
     ampd = amp * f + ampd * g;
     amp = amp * g;
   }
@@ -501,6 +531,19 @@ static void or_radial_pair(const or_radial_setup *s, double rj_in, int is_centra
     double g2 = c * is3;
     for (int n = 1; n <= n_poly; n++)
       DT[NI(n)] = g0 * pol[NI(n)] + s->R1[NI(n)] * g1 * pol[NI(n + 1)] + s->R2[NI(n)] * g2 * pol[NI(n + 2)];
+    if (s->do_der2) {                                                /* :838-861 */
+      double is4 = is2 * is2, is5 = is4 * isig, is6 = is4 * is2;
+      double k0 = -is2, k1 = -4.0 * c * is3, k2 = (1.0 - 3.0 * c * c) * is4, k3 = 2.0 * c * is5,
+             k4 = c * c * is6;
+      double B0 = k0 + k1 * f + k2 * f * f + k3 * f * f * f + k4 * f * f * f * f;
+      double B1 = -(k1 + 2.0 * k2 * f + 3.0 * k3 * f * f + 4.0 * k4 * f * f * f);
+      double B2 = k2 + 3.0 * k3 * f + 6.0 * k4 * f * f;
+      double B3 = -(k3 + 4.0 * k4 * f);
+      double B4 = k4;
+      for (int n = 1; n <= n_poly; n++)
+        D2T[NI(n)] = B0 * pol[NI(n)] + s->R1[NI(n)] * B1 * pol[NI(n + 1)] + s->R2[NI(n)] * B2 * pol[NI(n + 2)]
+                     + s->R3[NI(n)] * B3 * pol[NI(n + 3)] + s->R4[NI(n)] * B4 * pol[NI(n + 4)];
+    }
   }
 
   if (s->with_gauss) {                                               /* :875-908 */
@@ -516,6 +559,13 @@ static void or_radial_pair(const or_radial_setup *s, double rj_in, int is_centra
       double M1 = sc0 * ge - pp * M0;
       double M2 = sc0 * ge * (-rj) - pp * M1 + sc0 * M0;
       DT[NI(a)] = M1 * is2 + c * M2 * is3;
+      if (s->do_der2) {                                              /* :895-905 */
+        double M3 = sc0 * ge * rj * rj - pp * M2 + 2.0 * sc0 * M1;
+        double M4 = sc0 * ge * (-rj * rj * rj) - pp * M3 + 3.0 * sc0 * M2;
+        double is4 = is2 * is2, is5 = is4 * isig, is6 = is4 * is2;
+        D2T[NI(a)] = -M0 * is2 - 4.0 * c * M1 * is3 + (1.0 - 3.0 * c * c) * M2 * is4
+                     + 2.0 * c * M3 * is5 + c * c * M4 * is6;
+      }
     }
   }
 
@@ -525,6 +575,15 @@ static void or_radial_pair(const or_radial_setup *s, double rj_in, int is_centra
       double acc = s->W[0 * s->ldw + (n - 1)] * dtot[NI(1)];
       for (int m = 2; m <= a; m++) acc = acc + s->W[(m - 1) * s->ldw + (n - 1)] * dtot[NI(m)];
       der[n - 1] = acc * s->inv_sqrt_rcut;
+    }
+    if (s->do_der2 && der2) {                                        /* :917-956 */
+      for (int n = 1; n <= a; n++)
+        d2tot[NI(n)] = amp * D2T[NI(n)] + 2.0 * ampd * DT[NI(n)] + ampd2 * pol[NI(n)];
+      for (int n = 1; n <= a; n++) {
+        double acc = s->W[0 * s->ldw + (n - 1)] * d2tot[NI(1)];
+        for (int m = 2; m <= a; m++) acc = acc + s->W[(m - 1) * s->ldw + (n - 1)] * d2tot[NI(m)];
+        der2[n - 1] = acc * s->inv_sqrt_rcut * s->inv_rcut;
+      }
     }
   }
   for (int n = 1; n <= a; n++) {                                     /* :962-976 */
@@ -540,7 +599,7 @@ static void or_radial_pair(const or_radial_setup *s, double rj_in, int is_centra
 typedef struct {
   int n_sites, n_pairs, n_max, k_max, l_max, n_soap, n_soap_unc, compress, P_nonzero;
   int *k_first;
-  double *rad, *rad_der;                          /* (n_max, n_pairs) */
+  double *rad, *rad_der, *rad_der2;               /* (n_max, n_pairs); der2 only for the Hessian */
   double *ang, *ang_r, *ang_a, *ang_p;            /* complex (k_max, n_pairs): re,im interleaved */
   double *cnk;                                    /* complex (k_max, n_max, n_sites) */
   double *sqrt_dot_p;                             /* n_sites */
@@ -551,7 +610,7 @@ typedef struct {
 
 void or_ctx_free(or_ctx *c) {
   if (!c) return;
-  free(c->k_first); free(c->rad); free(c->rad_der);
+  free(c->k_first); free(c->rad); free(c->rad_der); free(c->rad_der2);
   free(c->ang); free(c->ang_r); free(c->ang_a); free(c->ang_p);
   free(c->cnk); free(c->sqrt_dot_p); free(c->skip);
   free(c);
@@ -571,7 +630,17 @@ static void species_blocks(const or_args *a, int *i_beg, int *n_max) {
  *   ctx_out:       when non-NULL, receives the state soap_contract needs
  *                  (the reference's contract = .true.; :1008-1035)
  * Returns n_soap, or a negative code. */
+int or_get_soap2(const or_args *a, int do_derivatives, int do_der2, double *soap, double *soap_cart_der,
+                 or_ctx **ctx_out);
 int or_get_soap(const or_args *a, int do_derivatives, double *soap, double *soap_cart_der, or_ctx **ctx_out) {
+  return or_get_soap2(a, do_derivatives, 0, soap, soap_cart_der, ctx_out);
+}
+
+/* get_soap with, when do_der2, the second radial derivatives the central-atom
+ * Hessian needs (soap_hessian_enabled, src/soap_turbo.f90:76, 228, 457-522);
+ * returns -2 with the legacy filter seed (src/soap_turbo_radial.f90:318-328). */
+int or_get_soap2(const or_args *a, int do_derivatives, int do_der2, double *soap, double *soap_cart_der,
+                 or_ctx **ctx_out) {
   const double pi = acos(-1.0);
   int i_beg[64], n_max;
   if (a->n_species > 64) return -1;
@@ -580,6 +649,7 @@ int or_get_soap(const or_args *a, int do_derivatives, double *soap, double *soap
   const int n_pairs = a->n_pairs, n_sites = a->n_sites;
   const int n_soap_unc = n_max * (n_max + 1) / 2 * (l_max + 1);      /* :396 */
   const int need_der = do_derivatives;
+  if (do_der2 && (!do_derivatives || a->legacy_filter_seed)) return -2;
 
   or_ctx *c = (or_ctx *)calloc(1, sizeof(or_ctx));
   c->n_sites = n_sites; c->n_pairs = n_pairs; c->n_max = n_max; c->k_max = k_max; c->l_max = l_max;
@@ -587,6 +657,7 @@ int or_get_soap(const or_args *a, int do_derivatives, double *soap, double *soap
   c->k_first = (int *)malloc(sizeof(int) * (n_sites + 1));
   c->rad = (double *)calloc((size_t)n_max * n_pairs + 1, sizeof(double));
   c->rad_der = (double *)calloc((size_t)n_max * n_pairs + 1, sizeof(double));
+  if (do_der2) c->rad_der2 = (double *)calloc((size_t)n_max * n_pairs + 1, sizeof(double));
   c->ang = (double *)calloc((size_t)2 * k_max * n_pairs + 1, sizeof(double));
   if (need_der) {
     c->ang_r = (double *)calloc((size_t)2 * k_max * n_pairs + 1, sizeof(double));
@@ -612,6 +683,7 @@ int or_get_soap(const or_args *a, int do_derivatives, double *soap, double *soap
                    a->W + (size_t)i_beg[sp] * n_max + i_beg[sp], n_max, a->scaling_poly,
                    a->radial_enhancement, need_der, do_central, a->central_weight[sp], with_gauss,
                    a->legacy_filter_seed);
+    if (do_der2) or_radial_enable_der2(&st);
     const double gsc = a->global_scaling[sp];
     #pragma omp parallel for schedule(dynamic, 16)
     for (int i = 0; i < n_sites; i++) {
@@ -619,15 +691,17 @@ int or_get_soap(const or_args *a, int do_derivatives, double *soap, double *soap
         int k = c->k_first[i] + j;
         double *out = c->rad + (size_t)k * n_max + i_beg[sp];
         double *der = c->rad_der + (size_t)k * n_max + i_beg[sp];
-        for (int n = 0; n < alpha; n++) { out[n] = 0.0; der[n] = 0.0; }   /* :328-340 */
+        double *der2 = do_der2 ? c->rad_der2 + (size_t)k * n_max + i_beg[sp] : NULL;
+        for (int n = 0; n < alpha; n++) { out[n] = 0.0; der[n] = 0.0; if (der2) der2[n] = 0.0; } /* :328-340 */
         if (j == 0 && !do_central) continue;                               /* :342-355 */
         if (a->rjs[k] >= a->rcut_hard[sp]) continue;
         if (!a->mask[(size_t)sp * n_pairs + k]) continue;
-        double o[32], d[32];
-        or_radial_pair(&st, a->rjs[k], j == 0, o, d);
+        double o[32], d[32], d2[32];
+        or_radial_pair(&st, a->rjs[k], j == 0, o, d, der2 ? d2 : NULL);
         for (int n = 0; n < alpha; n++) {
           out[n] = o[n] * gsc;                                             /* :510-511, :532-533 */
           if (need_der) der[n] = d[n] * gsc;
+          if (der2) der2[n] = d2[n] * gsc;
         }
       }
     }
@@ -1004,22 +1078,401 @@ int or_soap_contract(const or_ctx *c, const double *soap, const double *G, doubl
   return 0;
 }
 
+/* ------------------------------------------------------------------------ */
+/* get_soap_central_hessian, src/soap_turbo.f90:1151-1700, on the state of    */
+/* or_get_soap2(do_derivatives = 1, do_der2 = 1).                            */
+/* ------------------------------------------------------------------------ */
+typedef double complex cplx;
+
+/* The unnormalised, compressed spherical derivatives of site i's p for pair
+ * k2 (soap_rad/azi/pol_der, src/soap_turbo.f90:1927-2075), as get_soap builds
+ * them before the normalisation. */
+static void hs_pair_sph(const or_args *a, const or_ctx *c, int i, int k2, double *trad, double *tazi,
+                        double *tpol, double *drad, double *dazi, double *dpol, double *P, double *Q,
+                        double *Qa, double *Qo) {
+  const int n_max = c->n_max, k_max = c->k_max, l_max = c->l_max, L1 = l_max + 1, n_soap = c->n_soap;
+  const double fourpi = 4.0 * acos(-1.0), sq2 = sqrt(2.0);
+  const double *ci = c->cnk + (size_t)2 * k_max * n_max * i;
+  const double *A = c->ang + (size_t)2 * k_max * k2, *Ar = c->ang_r + (size_t)2 * k_max * k2;
+  const double *Aa = c->ang_a + (size_t)2 * k_max * k2, *Ap = c->ang_p + (size_t)2 * k_max * k2;
+  for (int n = 0; n < n_max; n++)
+    for (int l = 0; l <= l_max; l++) {
+      double ap = 0, aq = 0, aa = 0, ao = 0;
+      for (int m = 0; m <= l; m++) {
+        int kk = kidx(l, m);
+        double w = (m == 0) ? 1.0 : 2.0;
+        double cr = ci[(size_t)2 * (k_max * n + kk)], cim = ci[(size_t)2 * (k_max * n + kk) + 1];
+        ap = ap + w * (A[2 * kk] * cr + A[2 * kk + 1] * cim);
+        aq = aq + w * (Ar[2 * kk] * cr + Ar[2 * kk + 1] * cim);
+        aa = aa + w * (Aa[2 * kk] * cr + Aa[2 * kk + 1] * cim);
+        ao = ao + w * (Ap[2 * kk] * cr + Ap[2 * kk + 1] * cim);
+      }
+      P[n * L1 + l] = ap; Q[n * L1 + l] = aq; Qa[n * L1 + l] = aa; Qo[n * L1 + l] = ao;
+    }
+  int counter = 0;
+  for (int n = 0; n < n_max; n++) {
+    double rn = c->rad[(size_t)k2 * n_max + n], rdn = c->rad_der[(size_t)k2 * n_max + n];
+    for (int np = n; np < n_max; np++) {
+      double rnp = c->rad[(size_t)k2 * n_max + np], rdnp = c->rad_der[(size_t)k2 * n_max + np];
+      double pre = fourpi * ((n == np) ? 1.0 : sq2);
+      for (int l = 0; l <= l_max; l++) {
+        int cidx = counter++;
+        if (c->skip[cidx]) { trad[cidx] = tazi[cidx] = tpol[cidx] = 0.0; continue; }
+        trad[cidx] = pre * (rdn * P[np * L1 + l] + rn * Q[np * L1 + l] + rdnp * P[n * L1 + l] + rnp * Q[n * L1 + l]);
+        tazi[cidx] = pre * (rn * Qa[np * L1 + l] + rnp * Qa[n * L1 + l]);
+        tpol[cidx] = pre * (rn * Qo[np * L1 + l] + rnp * Qo[n * L1 + l]);
+      }
+    }
+  }
+  if (c->compress) {
+    for (int s = 0; s < n_soap; s++) drad[s] = dazi[s] = dpol[s] = 0.0;
+    for (int t = 0; t < a->P_nonzero; t++) {
+      int pi_ = a->P_i[t] - 1, pj = a->P_j[t] - 1;
+      drad[pi_] = drad[pi_] + a->P_el[t] * trad[pj];
+      dazi[pi_] = dazi[pi_] + a->P_el[t] * tazi[pj];
+      dpol[pi_] = dpol[pi_] + a->P_el[t] * tpol[pj];
+    }
+  } else {
+    for (int s = 0; s < n_soap; s++) { drad[s] = trad[s]; dazi[s] = tazi[s]; dpol[s] = tpol[s]; }
+  }
+}
+
+/* hess(a, b, v, k2) = sum_d vecs(d, v, i) d^2 q_d / dr_ia dr_jb for pair k2 =
+ * (site i, neighbour j), a of the central atom and b of the neighbour; the self
+ * pair's block is minus the sum of the others (:1488-1495).  Layouts (C):
+ * vecs[(i * n_vec + v) * n_soap + d], hess[((k2 * n_vec + v) * 3 + b) * 3 + a].
+ * selftest_err (may be NULL) receives the largest relative gap between the
+ * first derivative rebuilt from the same contraction and the one from the
+ * spherical derivatives (soap_hessian_selftest, :1395-1412).  Returns 0, or -1
+ * without second radial derivatives in ctx. */
+int or_central_hessian(const or_args *a, const or_ctx *c, const double *soap, int n_vec, const double *vecs,
+                       double *hess, double *selftest_err) {
+  if (!c->rad_der2 || !c->ang_r) return -1;
+  const int n_sites = c->n_sites, n_max = c->n_max, k_max = c->k_max, l_max = c->l_max;
+  const int n_soap = c->n_soap, n_soap_unc = c->n_soap_unc, nv = n_vec + 1, n_pairs = c->n_pairs;
+  const double pi = acos(-1.0), fourpi = 4.0 * pi, sqrt2 = sqrt(2.0);
+  double rcut_max = 0.0;
+  for (int sp = 0; sp < a->n_species; sp++) if (a->rcut_hard[sp] > rcut_max) rcut_max = a->rcut_hard[sp];
+  int *lofk = (int *)malloc(sizeof(int) * k_max), *mofk = (int *)malloc(sizeof(int) * k_max);
+  double *wm = (double *)malloc(sizeof(double) * k_max), *preflm = (double *)malloc(sizeof(double) * k_max);
+  double *Ck = (double *)malloc(sizeof(double) * k_max);
+  for (int l = 0, k = 0; l <= l_max; l++)
+    for (int m = 0; m <= l; m++, k++) { lofk[k] = l; mofk[k] = m; wm[k] = m > 0 ? 2.0 : 1.0; }
+  or_preflm(l_max, preflm);
+  for (int k = 0; k < k_max; k++) Ck[k] = (mofk[k] % 2 == 0) ? preflm[k] : -preflm[k];   /* :1264-1271 */
+  for (size_t t = 0; t < (size_t)9 * n_vec * n_pairs; t++) hess[t] = 0.0;
+  double chk_err = 0.0, chk_ref = 0.0;
+
+  #pragma omp parallel reduction(max : chk_err, chk_ref)
+  {
+    cplx *Gacc = (cplx *)malloc(sizeof(cplx) * n_max * k_max * 3);
+    cplx *Zv = (cplx *)malloc(sizeof(cplx) * n_max * k_max * nv);
+    cplx *ZGv = (cplx *)malloc(sizeof(cplx) * n_max * k_max * 3 * nv);
+    double *Smat = (double *)malloc(sizeof(double) * n_max * n_max * (l_max + 1));
+    double *vunc = (double *)malloc(sizeof(double) * (n_soap_unc + 1)), *pvec = (double *)malloc(sizeof(double) * n_soap);
+    double *dp1 = (double *)malloc(sizeof(double) * n_soap * 3), *dp2 = (double *)malloc(sizeof(double) * n_soap * 3);
+    double *trad = (double *)malloc(sizeof(double) * (n_soap_unc + 1)), *tazi = (double *)malloc(sizeof(double) * (n_soap_unc + 1));
+    double *tpol = (double *)malloc(sizeof(double) * (n_soap_unc + 1));
+    double *drad = (double *)malloc(sizeof(double) * n_soap), *dazi = (double *)malloc(sizeof(double) * n_soap);
+    double *dpol = (double *)malloc(sizeof(double) * n_soap);
+    double *Pb = (double *)malloc(sizeof(double) * n_max * (l_max + 1) * 4);
+    double *il = (double *)malloc(sizeof(double) * (l_max + 4)), *dilz = (double *)malloc(sizeof(double) * (l_max + 1));
+    double *d2ilz = (double *)malloc(sizeof(double) * (l_max + 1));
+    double *Fl = (double *)malloc(sizeof(double) * (l_max + 1)), *Fl1 = (double *)malloc(sizeof(double) * (l_max + 1));
+    double *Fl2 = (double *)malloc(sizeof(double) * (l_max + 1)), *Qt = (double *)malloc(sizeof(double) * k_max);
+    cplx *Om = (cplx *)malloc(sizeof(cplx) * k_max), *dOm = (cplx *)malloc(sizeof(cplx) * 3 * k_max);
+    cplx *d2Om = (cplx *)malloc(sizeof(cplx) * 9 * k_max), *wpow = (cplx *)malloc(sizeof(cplx) * (l_max + 3));
+    double *hv = (double *)malloc(sizeof(double) * 9 * nv), *hsum = (double *)malloc(sizeof(double) * 9 * (n_vec + 1));
+    double *u2rec = (double *)malloc(sizeof(double) * 3 * nv);
+    double nh[3], tvec[3], thes[9], rr = 0, invr = 0;
+    cplx wvec[3], whes[9];
+
+    /* F_l, Omega, dOmega and (want2) d2Omega of one pair (pair_geometry, :1537-1652) */
+#define PAIR_GEOMETRY(kk, good, want2)                                                                       \
+    do {                                                                                                     \
+      good = 0;                                                                                              \
+      rr = a->rjs[kk];                                                                                       \
+      if (rr >= rcut_max || rr < 1.0e-10) break;                                                            \
+      int isp = -1;                                                                                          \
+      for (int q = 0; q < a->n_species; q++) if (a->mask[(size_t)q * n_pairs + (kk)]) { isp = q; break; }    \
+      if (isp < 0) break;                                                                                    \
+      good = 1;                                                                                              \
+      invr = 1.0 / rr;                                                                                       \
+      const double invr2 = invr * invr;                                                                      \
+      const double sscal = a->atom_sigma_t_scaling[isp], sig = a->atom_sigma_t[isp] + sscal * rr;           \
+      const double amp = rcut_max * rcut_max / (sig * sig), ampd = -2.0 * sscal / sig * amp;                 \
+      const double ampdd = 6.0 * sscal * sscal / (sig * sig) * amp;                                          \
+      const double xarg = rr / sig, zz = xarg * xarg, invz = 1.0 / zz;                                      \
+      or_ilexp_array(l_max + 2, xarg, il);                                                                   \
+      for (int l = 0; l <= l_max; l++) {                                                                     \
+        const double rl = (double)l;                                                                         \
+        dilz[l] = il[l + 1] + (rl * invz - 1.0) * il[l];                                                     \
+        d2ilz[l] = il[l + 2] + ((double)(2 * l + 1) * invz - 2.0) * il[l + 1]                               \
+                   + (rl * (rl - 1.0) * invz * invz - 2.0 * rl * invz + 1.0) * il[l];                        \
+      }                                                                                                      \
+      const double zp = 2.0 * rr / (sig * sig) - 2.0 * rr * rr * sscal / (sig * sig * sig);                \
+      const double zp2 = 2.0 / (sig * sig) - 8.0 * rr * sscal / (sig * sig * sig)                           \
+                         + 6.0 * rr * rr * sscal * sscal / (sig * sig * sig * sig);                           \
+      for (int l = 0; l <= l_max; l++) {                                                                     \
+        const double f0_ = il[l], f1_ = dilz[l] * zp, f2_ = d2ilz[l] * zp * zp + dilz[l] * zp2;             \
+        Fl[l] = amp * f0_;                                                                                   \
+        Fl1[l] = ampd * f0_ + amp * f1_;                                                                     \
+        Fl2[l] = ampdd * f0_ + 2.0 * ampd * f1_ + amp * f2_;                                                 \
+      }                                                                                                      \
+      const double sin_t = sin(a->thetas[kk]), cos_t = cos(a->thetas[kk]);                                   \
+      const double sin_f = sin(a->phis[kk]), cos_f = cos(a->phis[kk]);                                       \
+      nh[0] = sin_t * cos_f; nh[1] = sin_t * sin_f; nh[2] = cos_t;                                           \
+      const double tt = nh[2];                                                                               \
+      const cplx wc = nh[0] - I * nh[1];                                                                     \
+      const cplx ec[3] = {1.0, -I, 0.0};                                                                     \
+      for (int q = 0; q < 3; q++) { tvec[q] = -tt * nh[q] * invr; wvec[q] = -wc * nh[q] * invr; }          \
+      tvec[2] = tvec[2] + invr;                                                                              \
+      for (int q = 0; q < 3; q++) wvec[q] = wvec[q] + ec[q] * invr;                                          \
+      if (want2) {                                                                                           \
+        for (int bb = 0; bb < 3; bb++)                                                                       \
+          for (int aa = 0; aa < 3; aa++) {                                                                   \
+            thes[bb * 3 + aa] = (3.0 * tt * nh[aa] * nh[bb]) * invr2;                                        \
+            whes[bb * 3 + aa] = (3.0 * wc * nh[aa] * nh[bb] - ec[aa] * nh[bb] - ec[bb] * nh[aa]) * invr2;    \
+          }                                                                                                  \
+        for (int aa = 0; aa < 3; aa++) {                                                                     \
+          thes[aa * 3 + 2] = thes[aa * 3 + 2] - nh[aa] * invr2;                                              \
+          thes[2 * 3 + aa] = thes[2 * 3 + aa] - nh[aa] * invr2;                                              \
+          thes[aa * 3 + aa] = thes[aa * 3 + aa] - tt * invr2;                                                \
+          whes[aa * 3 + aa] = whes[aa * 3 + aa] - wc * invr2;                                                \
+        }                                                                                                    \
+      }                                                                                                      \
+      Qt[0] = 1.0;                                                                                           \
+      if (l_max >= 1) { Qt[1] = tt; Qt[2] = 1.0; }                                                          \
+      for (int ll = 2; ll <= l_max; ll++) {                                                                  \
+        const int kbb = ll * (ll + 1) / 2;                                                                   \
+        for (int mm = 0; mm <= ll - 2; mm++) {                                                               \
+          const int kq = kbb + mm;                                                                           \
+          Qt[kq] = ((double)(2 * ll - 1) * tt * Qt[kq - ll] - (double)(ll + mm - 1) * Qt[kq - 2 * ll + 1])   \
+                   / (double)(ll - mm);                                                                      \
+        }                                                                                                    \
+        Qt[kbb + ll - 1] = (double)(2 * ll - 1) * tt * Qt[kbb + ll - 1 - ll];                                \
+        Qt[kbb + ll] = (double)(2 * ll - 1) * Qt[kbb + ll - ll - 1];                                         \
+      }                                                                                                      \
+      wpow[0] = 0.0; wpow[1] = 0.0; wpow[2] = 1.0;  /* wpow[m + 2] = w^m */                                \
+      for (int mm = 1; mm <= l_max; mm++) wpow[mm + 2] = wpow[mm + 1] * wc;                                  \
+      for (int kq = 0; kq < k_max; kq++) {                                                                   \
+        const int ll = lofk[kq], mm = mofk[kq];                                                              \
+        const double q0 = Qt[kq], q1 = (mm + 1 <= ll) ? Qt[kq + 1] : 0.0, q2 = (mm + 2 <= ll) ? Qt[kq + 2] : 0.0; \
+        Om[kq] = Ck[kq] * q0 * wpow[mm + 2];                                                                 \
+        for (int aa = 0; aa < 3; aa++)                                                                       \
+          dOm[kq * 3 + aa] = Ck[kq] * (q1 * tvec[aa] * wpow[mm + 2] + q0 * (double)mm * wpow[mm + 1] * wvec[aa]); \
+        if (want2)                                                                                           \
+          for (int bb = 0; bb < 3; bb++)                                                                     \
+            for (int aa = 0; aa < 3; aa++)                                                                   \
+              d2Om[(kq * 3 + bb) * 3 + aa] =                                                                 \
+                  Ck[kq] * (q2 * tvec[aa] * tvec[bb] * wpow[mm + 2] + q1 * thes[bb * 3 + aa] * wpow[mm + 2]   \
+                            + q1 * (double)mm * wpow[mm + 1] * (tvec[aa] * wvec[bb] + tvec[bb] * wvec[aa])  \
+                            + q0 * (double)(mm * (mm - 1)) * wpow[mm] * wvec[aa] * wvec[bb]                  \
+                            + q0 * (double)mm * wpow[mm + 1] * whes[bb * 3 + aa]);                           \
+      }                                                                                                      \
+    } while (0)
+
+    /* the Cartesian, unnormalised derivative of the compressed p for one pair (pair_dp, :1520-1534) */
+#define PAIR_DP(kk, i_, d)                                                                                   \
+    do {                                                                                                     \
+      hs_pair_sph(a, c, i_, kk, trad, tazi, tpol, drad, dazi, dpol, Pb, Pb + n_max * (l_max + 1),           \
+                  Pb + 2 * n_max * (l_max + 1), Pb + 3 * n_max * (l_max + 1));                               \
+      const double st_ = sin(a->thetas[kk]), ct_ = cos(a->thetas[kk]);                                       \
+      const double sf_ = sin(a->phis[kk]), cf_ = cos(a->phis[kk]), ir_ = 1.0 / a->rjs[kk];                   \
+      const double cxr = st_ * cf_, cyr = st_ * sf_, czr = ct_;                                              \
+      const double pxr = -ct_ * cf_ * ir_, pyr = -ct_ * sf_ * ir_, pzr = st_ * ir_;                          \
+      const double axr = -sf_ * ir_, ayr = cf_ * ir_;                                                        \
+      for (int kq = 0; kq < n_soap; kq++) {                                                                  \
+        (d)[kq * 3 + 0] = cxr * drad[kq] + pxr * dpol[kq] + axr * dazi[kq];                                  \
+        (d)[kq * 3 + 1] = cyr * drad[kq] + pyr * dpol[kq] + ayr * dazi[kq];                                  \
+        (d)[kq * 3 + 2] = czr * drad[kq] + pzr * dpol[kq];                                                   \
+      }                                                                                                      \
+    } while (0)
+
+    #pragma omp for schedule(dynamic, 4)
+    for (int i = 0; i < n_sites; i++) {
+      const int k3 = c->k_first[i];
+      const double sv = c->sqrt_dot_p[i], invs = 1.0 / sv, invs3 = invs / (sv * sv), invs5 = invs3 / (sv * sv);
+      for (int q = 0; q < n_soap; q++) pvec[q] = soap[(size_t)n_soap * i + q] * sv;
+      const double *ci = c->cnk + (size_t)2 * k_max * n_max * i;
+      int good;
+      /* ---- pass A (:1305-1334) */
+      for (int t = 0; t < n_max * k_max * 3; t++) Gacc[t] = 0.0;
+      for (int t = 0; t < n_soap * 3; t++) dp1[t] = 0.0;
+      for (int j = 1; j < a->n_neigh[i]; j++) {
+        const int k2 = k3 + j;
+        PAIR_GEOMETRY(k2, good, 0);
+        if (!good) continue;
+        PAIR_DP(k2, i, dp2);
+        for (int t = 0; t < n_soap * 3; t++) dp1[t] = dp1[t] - dp2[t];
+        for (int k = 0; k < k_max; k++) {
+          const int l = lofk[k];
+          const double f0 = Fl[l], f1 = Fl1[l];
+          for (int n = 0; n < n_max; n++) {
+            const double r0 = fourpi * c->rad[(size_t)k2 * n_max + n], r1 = fourpi * c->rad_der[(size_t)k2 * n_max + n];
+            const double g0 = r0 * f0, g1 = r1 * f0 + r0 * f1;
+            for (int q = 0; q < 3; q++)
+              Gacc[(n * k_max + k) * 3 + q] = Gacc[(n * k_max + k) * 3 + q] + g1 * nh[q] * Om[k] + g0 * dOm[k * 3 + q];
+          }
+        }
+      }
+      /* ---- the weight vectors, uncompressed, and their S matrices (:1336-1376) */
+      for (int v = 0; v < nv; v++) {
+        const double *vin = v < n_vec ? vecs + ((size_t)i * n_vec + v) * n_soap : pvec;
+        for (int t = 0; t < n_soap_unc; t++) vunc[t] = 0.0;
+        if (c->compress) {
+          for (int t = 0; t < a->P_nonzero; t++)
+            vunc[a->P_j[t] - 1] = vunc[a->P_j[t] - 1] + a->P_el[t] * vin[a->P_i[t] - 1];
+        } else {
+          for (int t = 0; t < n_soap; t++) vunc[t] = vin[t];
+        }
+        for (int t = 0; t < n_soap_unc; t++) if (c->skip[t]) vunc[t] = 0.0;
+        for (int t = 0; t < n_max * n_max * (l_max + 1); t++) Smat[t] = 0.0;
+        int counter = 0;
+        for (int n = 0; n < n_max; n++)
+          for (int np = n; np < n_max; np++)
+            for (int l = 0; l <= l_max; l++) {
+              const double vu = vunc[counter++];
+              if (n == np) Smat[(l * n_max + n) * n_max + n] = 2.0 * vu;
+              else {
+                Smat[(l * n_max + np) * n_max + n] = sqrt2 * vu;
+                Smat[(l * n_max + n) * n_max + np] = Smat[(l * n_max + np) * n_max + n];
+              }
+            }
+        for (int k = 0; k < k_max; k++) {
+          const int l = lofk[k];
+          for (int n = 0; n < n_max; n++) {
+            cplx zc = 0.0, b0[3] = {0.0, 0.0, 0.0};
+            for (int np = 0; np < n_max; np++) {
+              const double smv = Smat[(l * n_max + np) * n_max + n];
+              zc = zc + smv * (ci[(size_t)2 * (k_max * np + k)] + I * ci[(size_t)2 * (k_max * np + k) + 1]);
+              for (int q = 0; q < 3; q++) b0[q] = b0[q] + smv * Gacc[(np * k_max + k) * 3 + q];
+            }
+            Zv[(v * n_max + n) * k_max + k] = zc;
+            for (int q = 0; q < 3; q++) ZGv[((v * n_max + n) * k_max + k) * 3 + q] = b0[q];
+          }
+        }
+      }
+      /* ---- pass B (:1378-1486) */
+      for (int t = 0; t < 9 * n_vec; t++) hsum[t] = 0.0;
+      for (int j = 1; j < a->n_neigh[i]; j++) {
+        const int k2 = k3 + j;
+        PAIR_GEOMETRY(k2, good, 1);
+        if (!good) continue;
+        PAIR_DP(k2, i, dp2);
+        for (int t = 0; t < 9 * nv; t++) hv[t] = 0.0;
+        for (int t = 0; t < 3 * nv; t++) u2rec[t] = 0.0;
+        for (int k = 0; k < k_max; k++) {
+          const int l = lofk[k];
+          const double f0 = Fl[l], f1 = Fl1[l], f2 = Fl2[l], wmk = wm[k];
+          for (int v = 0; v < nv; v++) {
+            cplx a0 = 0.0, a1 = 0.0, a2 = 0.0, b0[3] = {0.0, 0.0, 0.0}, b1[3] = {0.0, 0.0, 0.0};
+            for (int n = 0; n < n_max; n++) {
+              const double r0 = c->rad[(size_t)k2 * n_max + n], r1 = c->rad_der[(size_t)k2 * n_max + n];
+              const double r2 = c->rad_der2[(size_t)k2 * n_max + n];
+              const cplx zc = conj(Zv[(v * n_max + n) * k_max + k]);
+              a0 = a0 + r0 * zc;
+              a1 = a1 + r1 * zc;
+              a2 = a2 + r2 * zc;
+              for (int q = 0; q < 3; q++) {
+                const cplx gc = conj(ZGv[((v * n_max + n) * k_max + k) * 3 + q]);
+                b0[q] = b0[q] + r0 * gc;
+                b1[q] = b1[q] + r1 * gc;
+              }
+            }
+            const cplx z0 = fourpi * f0 * a0, z1 = fourpi * (f0 * a1 + f1 * a0);
+            const cplx z2 = fourpi * (f0 * a2 + 2.0 * f1 * a1 + f2 * a0);
+            cplx gg0[3], gg1[3];
+            for (int q = 0; q < 3; q++) {
+              gg0[q] = fourpi * f0 * b0[q];
+              gg1[q] = fourpi * (f0 * b1[q] + f1 * b0[q]);
+            }
+            for (int bb = 0; bb < 3; bb++) u2rec[v * 3 + bb] += wmk * creal(z1 * nh[bb] * Om[k] + z0 * dOm[k * 3 + bb]);
+            for (int bb = 0; bb < 3; bb++)
+              for (int aa = 0; aa < 3; aa++) {
+                cplx tE = (z2 - z1 * invr) * nh[aa] * nh[bb] * Om[k] + z1 * (nh[aa] * dOm[k * 3 + bb] + nh[bb] * dOm[k * 3 + aa])
+                          + z0 * d2Om[(k * 3 + bb) * 3 + aa];
+                if (aa == bb) tE = tE + z1 * invr * Om[k];
+                const cplx tD = gg1[aa] * nh[bb] * Om[k] + gg0[aa] * dOm[k * 3 + bb];
+                hv[(v * 3 + bb) * 3 + aa] = hv[(v * 3 + bb) * 3 + aa] - wmk * (creal(tE) + creal(tD));
+              }
+          }
+        }
+        for (int v = 0; v < nv; v++) {
+          const double *wv = v < n_vec ? vecs + ((size_t)i * n_vec + v) * n_soap : pvec;
+          for (int bb = 0; bb < 3; bb++) {
+            double refd = 0.0;
+            for (int q = 0; q < n_soap; q++) refd += wv[q] * dp2[q * 3 + bb];
+            const double e = fabs(u2rec[v * 3 + bb] - refd);
+            if (e > chk_err) chk_err = e;
+            if (fabs(refd) > chk_ref) chk_ref = fabs(refd);
+          }
+        }
+        /* ---- normalisation (:1414-1484) */
+        double t1[3], t2[3], c12[9];
+        for (int q = 0; q < 3; q++) {
+          t1[q] = 0.0; t2[q] = 0.0;
+          for (int s2 = 0; s2 < n_soap; s2++) { t1[q] += pvec[s2] * dp1[s2 * 3 + q]; t2[q] += pvec[s2] * dp2[s2 * 3 + q]; }
+        }
+        for (int bb = 0; bb < 3; bb++)
+          for (int aa = 0; aa < 3; aa++) {
+            double acc = 0.0;
+            for (int s2 = 0; s2 < n_soap; s2++) acc += dp1[s2 * 3 + aa] * dp2[s2 * 3 + bb];
+            c12[bb * 3 + aa] = acc;
+          }
+        for (int v = 0; v < n_vec; v++) {
+          const double *wv = vecs + ((size_t)i * n_vec + v) * n_soap;
+          double wp = 0.0, u1[3] = {0, 0, 0}, u2[3] = {0, 0, 0};
+          for (int s2 = 0; s2 < n_soap; s2++) {
+            wp += wv[s2] * pvec[s2];
+            for (int q = 0; q < 3; q++) { u1[q] += wv[s2] * dp1[s2 * 3 + q]; u2[q] += wv[s2] * dp2[s2 * 3 + q]; }
+          }
+          for (int bb = 0; bb < 3; bb++)
+            for (int aa = 0; aa < 3; aa++) {
+              const double h = hv[(v * 3 + bb) * 3 + aa] * invs - (u1[aa] * t2[bb] + u2[bb] * t1[aa]) * invs3
+                               - wp * (c12[bb * 3 + aa] + hv[(n_vec * 3 + bb) * 3 + aa]) * invs3
+                               + 3.0 * wp * t1[aa] * t2[bb] * invs5;
+              hess[(((size_t)k2 * n_vec + v) * 3 + bb) * 3 + aa] = h;
+              hsum[(v * 3 + bb) * 3 + aa] += h;
+            }
+        }
+      }
+      for (int v = 0; v < n_vec; v++)
+        for (int t = 0; t < 9; t++) hess[((size_t)k3 * n_vec + v) * 9 + t] = -hsum[v * 9 + t];
+    }
+#undef PAIR_GEOMETRY
+#undef PAIR_DP
+    free(Gacc); free(Zv); free(ZGv); free(Smat); free(vunc); free(pvec); free(dp1); free(dp2);
+    free(trad); free(tazi); free(tpol); free(drad); free(dazi); free(dpol); free(Pb);
+    free(il); free(dilz); free(d2ilz); free(Fl); free(Fl1); free(Fl2); free(Qt);
+    free(Om); free(dOm); free(d2Om); free(wpow); free(hv); free(hsum); free(u2rec);
+  }
+  if (selftest_err) *selftest_err = chk_err / (chk_ref > 1e-300 ? chk_ref : 1e-300);
+  free(lofk); free(mofk); free(wm); free(preflm); free(Ck);
+  return 0;
+}
+
 /* The radial expansion of one species at a list of distances (the columns a
  * masked, in-cutoff pair would get; src/soap_turbo_radial.f90:394-1004,
  * global_scaling not applied).  W is the species' alpha x alpha block. */
 int or_radial_eval(int basis, int alpha, double rcut_soft, double rcut_hard, double sigma,
                    double sigma_scaling, double amp_scaling, double nf, const double *W,
                    int scaling_poly, int radial_enhancement, double central_weight, int is_central,
-                   int legacy_seed, int n, const double *r, double *out, double *der) {
+                   int legacy_seed, int n, const double *r, double *out, double *der, double *der2) {
   or_radial_setup st;
   int with_gauss = basis == 1;
   int do_central = with_gauss ? 0 : (central_weight != 0.0);
   or_radial_init(&st, alpha, rcut_soft, rcut_hard, sigma, sigma_scaling, amp_scaling, nf, W, alpha,
                  scaling_poly, radial_enhancement, 1, do_central, central_weight, with_gauss, legacy_seed);
+  if (der2 && or_radial_enable_der2(&st)) return -1;  /* second derivatives need the unified seed */
   for (int t = 0; t < n; t++) {
-    double o[32], d[32];
-    or_radial_pair(&st, r[t], is_central, o, d);
-    for (int q = 0; q < alpha; q++) { out[(size_t)t * alpha + q] = o[q]; der[(size_t)t * alpha + q] = d[q]; }
+    double o[32], d[32], d2[32];
+    or_radial_pair(&st, r[t], is_central, o, d, der2 ? d2 : NULL);
+    for (int q = 0; q < alpha; q++) {
+      out[(size_t)t * alpha + q] = o[q];
+      der[(size_t)t * alpha + q] = d[q];
+      if (der2) der2[(size_t)t * alpha + q] = d2[q];
+    }
   }
   return 0;
 }

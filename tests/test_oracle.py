@@ -266,3 +266,76 @@ def test_oracle_vjp_against_finite_differences(cfg1):
             m[a, c] -= h
             fd = (L(p) - L(m)) / (2 * h)
             assert abs(fd - F[a, c]) < 1e-6 * np.abs(F).max()
+
+
+# ---------------------------------------------------------------- central-atom Hessian
+def _hessian_case(seed=3, n_atoms=24):
+    hp = syn.Hyper(alpha_max=[4, 4], l_max=4, basis="poly3gauss", atom_sigma_t_scaling=0.05,
+                   atom_sigma_r_scaling=0.05)
+    st = syn.random_structure(n_atoms, density=0.1, d_min=1.0, fractions=(0.5, 0.5), seed=seed)
+    nl = syn.neighbour_list(st, 5.0, 2)
+    W, S = O.basis_matrices(hp)
+    return hp, nl, W, S
+
+
+@pytest.mark.parametrize("basis,enh", [("poly3", 0), ("poly3gauss", 0), ("poly3", 2), ("poly3gauss", 1)])
+def test_radial_second_derivative_matches_finite_differences(basis, enh):
+    """d^2 R/dr^2 of the unified seed (src/soap_turbo_radial.f90:838-861,
+    895-905, 917-956) against central differences of dR/dr; the attainable
+    agreement is set by W's conditioning (~1e6), hence h = 1e-3."""
+    hp = syn.Hyper(alpha_max=[8], basis=basis, radial_enhancement=enh, atom_sigma_r_scaling=0.1)
+    W, _ = O.basis_matrices(hp)
+    r = np.linspace(0.5, 4.95, 37)
+    h = 1e-3
+    _, d, d2 = O.radial_eval(hp, 0, W, r, legacy_seed=False, der2=True)
+    _, dp = O.radial_eval(hp, 0, W, r + h, legacy_seed=False)
+    _, dm = O.radial_eval(hp, 0, W, r - h, legacy_seed=False)
+    assert np.abs(d2 - (dp - dm) / (2 * h)).max() <= 2e-5 * np.abs(d2).max()
+    with pytest.raises(ValueError):  # refused with the legacy seed (:318-328)
+        O.radial_eval(hp, 0, W, r, legacy_seed=True, der2=True)
+
+
+def test_central_hessian_against_finite_differences():
+    """hess(a, b, v, k) = sum_d vecs(d, v, i) d^2 q_d / dr_ia dr_jb against central
+    differences, in pair k's displacement, of the central atom's VJP (the self
+    entry of soap_contract with G = the site's vecs)."""
+    import copy
+    hp, nl, W, S = _hessian_case()
+    ref = O.get_soap(hp, nl, W, S, do_derivatives=True, legacy_filter_seed=False, hessian=True)
+    n_soap = ref.soap.shape[1]
+    vecs = np.random.default_rng(3).standard_normal((nl.n_sites, 2, n_soap))
+    hess, err = ref.central_hessian(vecs)
+    assert err < 1e-12  # the rebuilt first derivative (soap_hessian_selftest)
+    off = np.concatenate([[0], np.cumsum(nl.n_neigh)])
+    h = 1e-5
+    for i, j in ((0, 3), (5, 1), (7, 10)):
+        k = off[i] + j
+        for b in range(3):
+            num = []
+            for sgn in (1, -1):
+                nlx = copy.deepcopy(nl)
+                d = nl.disp[k].copy()
+                d[b] += sgn * h
+                r = np.linalg.norm(d)
+                nlx.rjs[k], nlx.thetas[k], nlx.phis[k] = r, np.arccos(np.clip(d[2] / r, -1, 1)), np.arctan2(d[1], d[0])
+                rx = O.get_soap(hp, nlx, W, S, do_derivatives=True, legacy_filter_seed=False)
+                G = np.zeros((n_soap, nl.n_sites))
+                G[:, i] = vecs[i, 0]
+                num.append(rx.contract(G, 1.0)[off[i]])
+            fd = (num[0] - num[1]) / (2 * h)
+            assert np.abs(fd - hess[k, 0, b, :]).max() <= 1e-6 * np.abs(hess[k, 0]).max()
+
+
+def test_central_hessian_self_block_and_state():
+    hp, nl, W, S = _hessian_case(seed=5)
+    ref = O.get_soap(hp, nl, W, S, do_derivatives=True, legacy_filter_seed=False, hessian=True)
+    vecs = np.random.default_rng(1).standard_normal((nl.n_sites, 3, ref.soap.shape[1]))
+    hess, _ = ref.central_hessian(vecs)
+    off = np.concatenate([[0], np.cumsum(nl.n_neigh)])
+    for i in range(nl.n_sites):  # a rigid shift leaves q alone: each row of blocks sums to zero
+        np.testing.assert_allclose(hess[off[i]:off[i + 1]].sum(axis=0), 0.0, atol=1e-12 * np.abs(hess).max())
+    plain = O.get_soap(hp, nl, W, S, do_derivatives=True, legacy_filter_seed=False)
+    with pytest.raises(RuntimeError):
+        plain.central_hessian(vecs)
+    with pytest.raises(RuntimeError):  # second radial derivatives need the unified seed
+        O.get_soap(hp, nl, W, S, do_derivatives=True, legacy_filter_seed=True, hessian=True)
