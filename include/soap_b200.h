@@ -51,7 +51,9 @@ enum {
   SOAPB_ERR_CUDA = 6,            /* CUDA runtime failure                                 */
   SOAPB_ERR_NO_DEVICE = 7,       /* no usable sm_100 device                              */
   SOAPB_ERR_INPUT = 8,           /* non-finite or negative distance, bad CSR, bad mask   */
-  SOAPB_ERR_BASIS_MATRIX = 9     /* overlap matrix not positive definite                 */
+  SOAPB_ERR_BASIS_MATRIX = 9,    /* overlap matrix not positive definite                 */
+  SOAPB_ERR_HESSIAN_STATE = 10   /* get_soap_central_hessian without a matching get_soap
+                                    (src/soap_turbo.f90:1206-1227)                       */
 };
 
 enum { SOAPB_BASIS_POLY3 = 0, SOAPB_BASIS_POLY3GAUSS = 1 };
@@ -111,6 +113,39 @@ int soapb_soap_contract(const double *soap, const double *G, double sgn, double 
 /* Module flag legacy_filter_seed (src/soap_turbo_radial.f90:67); default 1. */
 int soapb_set_legacy_filter_seed(int32_t legacy);
 int soapb_get_legacy_filter_seed(int32_t *legacy);
+
+/* Module flag soap_hessian_enabled (src/soap_turbo.f90:76); default 0.  With
+ * it set, soapb_get_soap called with do_derivatives records the batch for
+ * soapb_get_soap_central_hessian; it then needs legacy_filter_seed = 0 (else
+ * soapb_get_soap returns SOAPB_ERR_ARGUMENT, as the reference's radial kernel
+ * stops, src/soap_turbo_radial.f90:318-323). */
+int soapb_set_soap_hessian_enabled(int32_t enabled);
+int soapb_get_soap_hessian_enabled(int32_t *enabled);
+
+/* get_soap_central_hessian (src/soap_turbo.f90:1151-1160), same arguments plus
+ * n_soap = size(soap,1):
+ *   hess(3, 3, n_vec, n_atom_pairs)  hess[((k*n_vec + v)*3 + b)*3 + a]
+ *     = sum_d vecs(d, v, i) d^2 soap(d, i) / dr_ia dr_jb
+ * for pair k = (site i, neighbour j), a of the central atom and b of the
+ * neighbour; the self pair's block is minus the sum of the others.
+ *   vecs(n_soap, n_vec, n_sites)     vecs[(i*n_vec + v)*n_soap + d]
+ *   soap                             the normalised descriptor get_soap returned
+ * It must follow a soapb_get_soap on the same batch with do_derivatives and
+ * soap_hessian_enabled set (else SOAPB_ERR_HESSIAN_STATE, as the reference
+ * stops).  The descriptor definition, species and neighbour geometry are the
+ * ones that get_soap call kept on the device (the reference reads its kept
+ * buffers the same way); the geometry, cutoff, sigma and compression arguments
+ * here are accepted for the reference's argument list and not read again.
+ * Computed in FP64. */
+int soapb_get_soap_central_hessian(int32_t n_sites, const int32_t *n_neigh, int32_t n_atom_pairs,
+                                   int32_t n_species, const uint8_t *mask, const double *rjs,
+                                   const double *thetas, const double *phis, int32_t l_max,
+                                   const double *rcut_hard, const double *atom_sigma_t,
+                                   const double *atom_sigma_t_scaling, int32_t compress_soap,
+                                   int32_t compress_P_nonzero, const int32_t *compress_P_i,
+                                   const int32_t *compress_P_j, const double *compress_P_el,
+                                   const double *soap, int32_t n_soap, int32_t n_vec, const double *vecs,
+                                   double *hess);
 
 /* Arithmetic of the drop-in layer (SOAPB_PREC_*); default mixed. */
 int soapb_set_precision(int32_t precision);
@@ -250,6 +285,15 @@ int soapb_descriptor_and_vjp(soapb_context *ctx, const soapb_batch *batch, const
  * with the self column minus the sum of the others. */
 int soapb_descriptor_fp64(soapb_context *ctx, const soapb_batch *batch, double *d_soap,
                           double *d_cart);
+
+/* Central-atom Hessian contracted with weight vectors (the context form of
+ * soapb_get_soap_central_hessian): d_vecs (n_soap, n_vec, n_sites), d_hess
+ * (3, 3, n_vec, n_pairs), layouts as there.  FP64; it recomputes the FP64
+ * expansion state of the batch, so it needs no earlier call.  d_soap is the
+ * normalised descriptor the weights were formed against (NULL: the FP64 one
+ * this call computes).  Needs legacy_filter_seed = 0 (SOAPB_ERR_ARGUMENT). */
+int soapb_central_hessian(soapb_context *ctx, const soapb_batch *batch, const double *d_soap,
+                          int32_t n_vec, const double *d_vecs, double *d_hess);
 
 /* pair = sgn * G . soap_cart_der over a materialised soap_cart_der. */
 int soapb_contract_cart_der(soapb_context *ctx, const soapb_batch *batch, const double *d_cart,

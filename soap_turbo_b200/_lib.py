@@ -22,6 +22,7 @@ ERRORS = {
     1: "SOAPB_ERR_ARGUMENT", 2: "SOAPB_ERR_ALPHA_TOO_LARGE", 3: "SOAPB_ERR_CONTRACT_STATE",
     4: "SOAPB_ERR_COMPRESS_MODE", 5: "SOAPB_ERR_BASIS", 6: "SOAPB_ERR_CUDA",
     7: "SOAPB_ERR_NO_DEVICE", 8: "SOAPB_ERR_INPUT", 9: "SOAPB_ERR_BASIS_MATRIX",
+    10: "SOAPB_ERR_HESSIAN_STATE",
 }
 BASIS = {"poly3": 0, "poly3gauss": 1}
 PREC_MIXED, PREC_FP64 = 0, 1
@@ -72,6 +73,11 @@ SIGNATURES = {
                                       C.c_int32]),
     "soapb_set_legacy_filter_seed": (C.c_int, [C.c_int32]),
     "soapb_get_legacy_filter_seed": (C.c_int, [i32p]),
+    "soapb_set_soap_hessian_enabled": (C.c_int, [C.c_int32]),
+    "soapb_get_soap_hessian_enabled": (C.c_int, [i32p]),
+    "soapb_get_soap_central_hessian": (C.c_int, [
+        C.c_int32, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, C.c_int32, vp, vp, vp, C.c_int32,
+        C.c_int32, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp]),
     "soapb_set_precision": (C.c_int, [C.c_int32]),
     "soapb_set_basis_matrices": (C.c_int, [C.c_int32, f64p, f64p]),
     "soapb_get_compress_indices": (C.c_int, [C.c_char_p, C.c_int32, i32p, C.c_int32, i32p, i32p,
@@ -94,6 +100,8 @@ SIGNATURES = {
     "soapb_descriptor_fp64": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_void_p]),
     "soapb_contract_cart_der": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_void_p,
                                           C.c_int32, C.c_double, C.c_void_p]),
+    "soapb_central_hessian": (C.c_int, [C.c_void_p, C.POINTER(Batch), C.c_void_p, C.c_int32,
+                                        C.c_void_p, C.c_void_p]),
     "soapb_autotune": (C.c_int, [C.c_void_p, C.POINTER(Batch), i32p]),
     "soapb_check_inputs": (C.c_int, [C.c_void_p, i64p]),
     "soapb_launch_count": (C.c_int, [C.c_void_p, i64p]),

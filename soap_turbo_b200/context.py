@@ -282,6 +282,19 @@ class Context:
             C.c_void_p(cart_t.data_ptr()) if cart_t is not None else None))
         return soap, cart_t
 
+    def central_hessian(self, b: DeviceBatch, vecs, soap=None, out=None):
+        """soapb_central_hessian: vecs (n_sites, n_vec, n_soap) == Fortran
+        vecs(n_soap, n_vec, n_sites); returns hess (n_pairs, n_vec, 3, 3) ==
+        Fortran hess(3, 3, n_vec, n_pairs), element [k, v, b, a].  soap: the
+        normalised descriptor the weights were formed against (None: the FP64
+        one the call computes)."""
+        n_vec = int(vecs.shape[1])
+        out = self._new((b.n_pairs, n_vec, 3, 3)) if out is None else out
+        _lib.check(self._lib.soapb_central_hessian(
+            self._h, b.c, C.c_void_p(soap.data_ptr()) if soap is not None else None, n_vec,
+            C.c_void_p(vecs.data_ptr()), C.c_void_p(out.data_ptr())))
+        return out
+
     def contract_cart_der(self, b: DeviceBatch, cart, G, sgn=1.0, g_layout=_lib.G_SITE_FASTEST,
                           out=None):
         out = self._new((b.n_pairs, 3)) if out is None else out

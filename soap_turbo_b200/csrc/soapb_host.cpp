@@ -199,6 +199,9 @@ struct soapb_context {
   // arena
   DBuf off, bits, err, keep_c, keep_norm, rad, ang;
   DBuf f64_rad, f64_rad_der, f64_ang, f64_cnk, f64_soap_un, f64_norm;
+  // central-atom Hessian: second radial derivatives, per-CTA scratch, the
+  // descriptor it recomputes, its work counter
+  DBuf hs_rad_der2, hs_scratch, hs_soap, hs_ticket;
   // neighbour-list builder: cell list, counts and the batch it hands out
   DBuf nb_acell, nb_ccount, nb_cstart, nb_cfill, nb_catoms, nb_counts, nb_off, nb_state;
   DBuf nb_rjs, nb_th, nb_ph, nb_mask, nb_natom, nb_nneigh, nb_species, nb_smult;
@@ -227,7 +230,8 @@ struct soapb_context {
   ~soapb_context() {
     timing_release();
     for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &rad, &ang, &f64_rad, &f64_rad_der,
-                    &f64_ang, &f64_cnk, &f64_soap_un, &f64_norm, &nb_acell, &nb_ccount, &nb_cstart,
+                    &f64_ang, &f64_cnk, &f64_soap_un, &f64_norm, &hs_rad_der2, &hs_scratch, &hs_soap,
+                    &hs_ticket, &nb_acell, &nb_ccount, &nb_cstart,
                     &nb_cfill, &nb_catoms, &nb_counts, &nb_off, &nb_state, &nb_rjs, &nb_th, &nb_ph,
                     &nb_mask, &nb_natom, &nb_nneigh, &nb_species, &nb_smult})
       b->release();
@@ -939,6 +943,49 @@ int ctx_fp64(soapb_context *c, const soapb_batch *b, double *d_soap, double *d_c
   return SOAPB_OK;
 }
 
+// get_soap_central_hessian (src/soap_turbo.f90:1151-1700) on one batch: the
+// FP64 descriptor path with derivatives rebuilds the expansion state, then the
+// second radial derivatives and the Hessian kernel.  d_soap (the normalised
+// descriptor the caller holds) may be null: the recomputed one is used.
+int ctx_hessian(soapb_context *c, const soapb_batch *b, const double *d_soap, int n_vec, const double *d_vecs,
+                double *d_hess) {
+  if (c->legacy)
+    return fail(SOAPB_ERR_ARGUMENT,
+                "ERROR: the second radial derivatives need legacy_filter_seed = .false.; with the legacy "
+                "seed the filter integrals are not the ones the recursion differentiates");
+  if (n_vec < 0) return fail(SOAPB_ERR_ARGUMENT, "n_vec must be >= 0");
+  DevBatch B{};
+  int rc = ensure_batch(c, b, B);
+  if (rc) return rc;
+  if (n_vec == 0) return SOAPB_OK;
+  if (b->n_sites > 0 && !d_vecs) return fail(SOAPB_ERR_ARGUMENT, "null vecs");
+  if (b->n_atom_pairs > 0 && !d_hess) return fail(SOAPB_ERR_ARGUMENT, "null hess");
+  if ((rc = run_prep(c, B))) return rc;
+  DevParams P = c->P;
+  P.n_pairs = B.n_pairs;
+  P.n_sites = B.n_sites;
+  const size_t np = (size_t)b->n_atom_pairs + 1, ns = (size_t)b->n_sites + 1;
+  if ((rc = c->f64_rad.ensure(8 * np * c->n_max))) return rc;
+  if ((rc = c->f64_rad_der.ensure(8 * np * c->n_max))) return rc;
+  if ((rc = c->f64_ang.ensure(16 * np * P.k_max * 4))) return rc;
+  if ((rc = c->f64_cnk.ensure(16 * ns * c->n_max * P.k_max))) return rc;
+  if ((rc = c->f64_soap_un.ensure(8 * ns * c->n_soap))) return rc;
+  if ((rc = c->f64_norm.ensure(8 * ns))) return rc;
+  if ((rc = c->hs_rad_der2.ensure(8 * np * c->n_max))) return rc;
+  if ((rc = c->hs_soap.ensure(8 * ns * c->n_soap))) return rc;
+  if ((rc = c->hs_ticket.ensure(16))) return rc;
+  const int grid = std::max(1, std::min(hess_grid(P, n_vec), b->n_sites));
+  if ((rc = c->hs_scratch.ensure(8 * (size_t)grid * hess_scratch_doubles(P, n_vec)))) return rc;
+  Fp64Work w{c->f64_rad.as<double>(), c->f64_rad_der.as<double>(), c->f64_ang.as<double>(),
+             c->f64_cnk.as<double>(), c->f64_soap_un.as<double>(), c->f64_norm.as<double>()};
+  int nl = 0;
+  CU(launch_fp64_descriptor(P, B, c->stream, w, 1, c->hs_soap.as<double>(), nullptr, &nl));
+  CU(launch_hessian(P, B, c->stream, w, c->hs_rad_der2.as<double>(), d_soap ? d_soap : c->hs_soap.as<double>(),
+                    n_vec, d_vecs, d_hess, c->hs_scratch.as<double>(), grid, c->hs_ticket.as<int>(), &nl));
+  c->launches += nl;
+  return SOAPB_OK;
+}
+
 int ctx_contract_cart(soapb_context *c, const soapb_batch *b, const double *d_cart, const double *d_G,
                       int g_layout, double sgn, double *d_pair) {
   DevBatch B{};
@@ -1124,6 +1171,12 @@ int soapb_descriptor_noalloc(soapb_context *c, const soapb_batch *b, double *d_s
 int soapb_descriptor_fp64(soapb_context *c, const soapb_batch *b, double *d_soap, double *d_cart) {
   if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
   return ctx_fp64(c, b, d_soap, d_cart);
+}
+
+int soapb_central_hessian(soapb_context *c, const soapb_batch *b, const double *d_soap, int32_t n_vec,
+                          const double *d_vecs, double *d_hess) {
+  if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
+  return ctx_hessian(c, b, d_soap, n_vec, d_vecs, d_hess);
 }
 
 int soapb_contract_cart_der(soapb_context *c, const soapb_batch *b, const double *d_cart,
@@ -1532,9 +1585,13 @@ struct DropIn {
   std::vector<double> user_W, user_S;  // caller-supplied basis, if any
   bool warned_poly3 = false, warned_gauss = false;
   // device copies of the last batch
-  DBuf n_neigh, species, species_mult, mask, rjs, thetas, phis, soap, G, pair, cart;
+  DBuf n_neigh, species, species_mult, mask, rjs, thetas, phis, soap, G, pair, cart, vecs, hess;
   soapb_batch batch{};
   int ct_ready = 0, ct_fp64 = 0, ct_n_sites = 0, ct_n_pairs = 0, ct_n_soap = 0;
+  // soap_hessian_enabled and what get_soap_central_hessian checks against
+  // (src/soap_turbo.f90:76, 93-95)
+  int hessian_enabled = 0;
+  int hs_ready = 0, hs_n_sites = 0, hs_n_pairs = 0, hs_l_max = -1, hs_n_soap = 0;
   cudaStream_t stream = nullptr;
   // overlap of host copies with the site kernels (mixed path): the sites go in
   // chunks, each chunk's outputs copied back (and, in soap_contract, its inputs
@@ -1623,6 +1680,21 @@ int soapb_get_legacy_filter_seed(int32_t *legacy) {
   return SOAPB_OK;
 }
 
+int soapb_set_soap_hessian_enabled(int32_t enabled) {
+  DropIn &d = dropin();
+  std::lock_guard<std::mutex> g(d.mu);
+  d.hessian_enabled = enabled ? 1 : 0;
+  return SOAPB_OK;
+}
+
+int soapb_get_soap_hessian_enabled(int32_t *enabled) {
+  if (!enabled) return fail(SOAPB_ERR_ARGUMENT, "null argument");
+  DropIn &d = dropin();
+  std::lock_guard<std::mutex> g(d.mu);
+  *enabled = d.hessian_enabled;
+  return SOAPB_OK;
+}
+
 int soapb_set_precision(int32_t precision) {
   if (precision != SOAPB_PREC_MIXED && precision != SOAPB_PREC_FP64)
     return fail(SOAPB_ERR_ARGUMENT, "precision must be SOAPB_PREC_MIXED or SOAPB_PREC_FP64");
@@ -1665,6 +1737,14 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
   DropIn &d = dropin();
   std::lock_guard<std::mutex> g(d.mu);
   d.ct_ready = 0;
+  d.hs_ready = 0;
+  // the second derivatives only come with the first ones, and only with the
+  // corrected filter seed (src/soap_turbo.f90:228; src/soap_turbo_radial.f90:318-323)
+  const bool do_hessian = d.hessian_enabled && do_derivatives;
+  if (do_hessian && d.legacy)
+    return fail(SOAPB_ERR_ARGUMENT,
+                "ERROR: soap_hessian_enabled needs legacy_filter_seed = .false. (the second radial "
+                "derivatives are taken with the corrected filter seed)");
   if (!basis || !scaling_mode) return fail(SOAPB_ERR_ARGUMENT, "null basis or scaling_mode");
   int b;
   if (!std::strcmp(basis, "poly3")) b = SOAPB_BASIS_POLY3;
@@ -1826,6 +1906,13 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
     std::printf("  *) Device to host copies: %8.3f ms |\n", t23);
     for (auto &e : ev) cudaEventDestroy(e);
   }
+  if (do_hessian) {
+    d.hs_ready = 1;
+    d.hs_n_sites = n_sites;
+    d.hs_n_pairs = n_atom_pairs;
+    d.hs_l_max = l_max;
+    d.hs_n_soap = n_soap;
+  }
   if (do_derivatives && contract) {
     d.ct_ready = 1;
     d.ct_fp64 = fp64;
@@ -1901,6 +1988,49 @@ int soapb_soap_contract(const double *soap, const double *G, double sgn, double 
   CU(e2);
   CU(e3);
   return SOAPB_OK;
+}
+
+int soapb_get_soap_central_hessian(int32_t n_sites, const int32_t *n_neigh, int32_t n_atom_pairs,
+                                   int32_t n_species, const uint8_t *mask, const double *rjs,
+                                   const double *thetas, const double *phis, int32_t l_max,
+                                   const double *rcut_hard, const double *atom_sigma_t,
+                                   const double *atom_sigma_t_scaling, int32_t compress_soap,
+                                   int32_t compress_P_nonzero, const int32_t *compress_P_i,
+                                   const int32_t *compress_P_j, const double *compress_P_el,
+                                   const double *soap, int32_t n_soap, int32_t n_vec, const double *vecs,
+                                   double *hess) {
+  (void)n_neigh; (void)n_species; (void)mask; (void)rjs; (void)thetas; (void)phis; (void)rcut_hard;
+  (void)atom_sigma_t; (void)atom_sigma_t_scaling; (void)compress_soap; (void)compress_P_nonzero;
+  (void)compress_P_i; (void)compress_P_j; (void)compress_P_el;
+  DropIn &d = dropin();
+  std::lock_guard<std::mutex> g(d.mu);
+  // state check (src/soap_turbo.f90:1206-1227)
+  if (!d.hs_ready || !d.ctx)
+    return fail(SOAPB_ERR_HESSIAN_STATE,
+                "ERROR: get_soap_central_hessian was called without a matching get_soap. Set "
+                "soap_hessian_enabled = .true. and call get_soap with do_derivatives = .true. first.");
+  if (n_sites != d.hs_n_sites || n_atom_pairs != d.hs_n_pairs || l_max != d.hs_l_max || n_soap != d.hs_n_soap)
+    return fail(SOAPB_ERR_HESSIAN_STATE,
+                "ERROR: get_soap_central_hessian was called on a different batch than the get_soap that "
+                "filled the buffers it reads.");
+  if (n_vec < 0) return fail(SOAPB_ERR_ARGUMENT, "n_vec must be >= 0");
+  if (n_vec == 0 || n_atom_pairs == 0) return SOAPB_OK;
+  if (!soap || !vecs || !hess) return fail(SOAPB_ERR_ARGUMENT, "null pointer");
+  cudaStream_t s = d.stream;
+  int rc;
+  const size_t nsv = (size_t)n_sites * n_soap;
+  if ((rc = upload(d.soap, soap, nsv, s))) return rc;
+  if ((rc = upload(d.vecs, vecs, nsv * n_vec, s))) return rc;
+  if ((rc = d.hess.ensure(8 * (9 * (size_t)n_vec * n_atom_pairs + 1)))) return rc;
+  if ((rc = ctx_hessian(d.ctx, &d.batch, d.soap.as<double>(), n_vec, d.vecs.as<double>(), d.hess.as<double>())))
+    return rc;
+  CU(cudaMemcpyAsync(hess, d.hess.p, 72 * (size_t)n_vec * n_atom_pairs, cudaMemcpyDeviceToHost, s));
+  if ((rc = dropin_streams(d, 0))) return rc;
+  *d.err_host = 0;
+  if (d.ctx->err.p)
+    CU(cudaMemcpyAsync(d.err_host, d.ctx->err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  return input_status(*d.err_host, nullptr);
 }
 
 }  // extern "C"

@@ -1,11 +1,13 @@
 """The reference's host interface for the descriptor path, on the GPU.
 
-``get_soap`` and ``soap_contract`` take the arguments of soap_turbo's Fortran
-routines (src/soap_turbo.f90:139-169 and :1723-1730) in the same order, with
+``get_soap``, ``soap_contract`` and ``get_soap_central_hessian`` take the
+arguments of soap_turbo's Fortran routines (src/soap_turbo.f90:139-169,
+:1723-1730 and :1151-1160) in the same order, with
 numpy arrays in the same (Fortran) shapes, and write their outputs in place
 like the Fortran ``intent(inout)`` / ``intent(out)`` arguments.  They call the
 drop-in layer of libsoapb200.so, which keeps the reference's module state:
-the basis cache, ``legacy_filter_seed`` and the contract state.
+the basis cache, ``legacy_filter_seed``, ``soap_hessian_enabled`` and the
+contract and Hessian state.
 """
 from __future__ import annotations
 
@@ -104,6 +106,40 @@ def soap_contract(soap, G, sgn, pair):
         raise TypeError("pair must be a Fortran-ordered float64 array (written in place)")
     _lib.check(lib.soapb_soap_contract(_a(soap), _a(G), float(sgn), _a(pair), int(soap.shape[1]),
                                        int(soap.shape[0]), int(pair.shape[1])))
+
+
+def get_soap_central_hessian(n_sites, n_neigh, n_atom_pairs, n_species, mask, rjs, thetas, phis,
+                             l_max, rcut_hard, atom_sigma_t, atom_sigma_t_scaling, compress_soap,
+                             compress_P_nonzero, compress_P_i, compress_P_j, compress_P_el, soap,
+                             n_vec, vecs, hess):
+    """get_soap_central_hessian (src/soap_turbo.f90:1151-1160): soap (n_soap,
+    n_sites) as get_soap returned it, vecs (n_soap, n_vec, n_sites), hess (3, 3,
+    n_vec, n_atom_pairs) written in place: hess[a, b, v, k] = sum_d vecs[d, v, i]
+    d^2 soap[d, i] / dr_ia dr_jb.  Follows a get_soap on the same batch with
+    do_derivatives and soap_hessian_enabled set."""
+    lib = _lib.load()
+    soap = _f(soap, _f64)
+    vecs = _f(vecs, _f64)
+    if not (isinstance(hess, np.ndarray) and hess.dtype == _f64 and hess.flags.f_contiguous):
+        raise TypeError("hess must be a Fortran-ordered float64 array (written in place)")
+    if hess.size != 9 * int(n_vec) * int(n_atom_pairs) or vecs.size != soap.size * int(n_vec):
+        raise ValueError("hess must be (3, 3, n_vec, n_atom_pairs) and vecs (n_soap, n_vec, n_sites)")
+    _lib.check(lib.soapb_get_soap_central_hessian(
+        int(n_sites), None, int(n_atom_pairs), int(n_species), None, None, None, None, int(l_max),
+        None, None, None, int(bool(compress_soap)), int(compress_P_nonzero), None, None, None,
+        _a(soap), int(soap.shape[0]), int(n_vec), _a(vecs), _a(hess)))
+
+
+def set_soap_hessian_enabled(enabled: bool):
+    """The reference's module flag soap_hessian_enabled (src/soap_turbo.f90:76)."""
+    _lib.check(_lib.load().soapb_set_soap_hessian_enabled(int(bool(enabled))))
+
+
+def get_soap_hessian_enabled() -> bool:
+    import ctypes as C
+    v = C.c_int32(0)
+    _lib.check(_lib.load().soapb_get_soap_hessian_enabled(C.byref(v)))
+    return bool(v.value)
 
 
 def get_compress_indices(compress_mode, alpha_max, l_max, what_to_do="set_indices"):

@@ -205,3 +205,27 @@ def test_get_soap_without_a_gpu_fails_loudly():
     with pytest.raises(_lib.SoapError) as e:
         D.get_soap(**_tiny_call())
     assert e.value.code == 7
+
+
+def test_central_hessian_state_checks_on_the_host():
+    """get_soap_central_hessian without a matching get_soap stops the reference
+    (src/soap_turbo.f90:1206-1227); soap_hessian_enabled with the legacy filter
+    seed is refused before any device work (src/soap_turbo_radial.f90:318-323)."""
+    args = _tiny_call()
+    n_soap, n_sites, n_pairs = 324, args["n_sites"], args["n_atom_pairs"]
+    hess = np.zeros((3, 3, 1, n_pairs), order="F")
+    with pytest.raises(_lib.SoapError) as e:
+        D.get_soap_central_hessian(
+            n_sites, args["n_neigh"], n_pairs, 1, args["mask"], args["rjs"], args["thetas"],
+            args["phis"], 8, 5.0, 0.5, 0.0, False, 0, None, None, None,
+            np.zeros((n_soap, n_sites), order="F"), 1, np.zeros((n_soap, 1, n_sites), order="F"), hess)
+    assert e.value.code == 10
+    assert not D.get_soap_hessian_enabled()
+    D.set_soap_hessian_enabled(True)
+    try:
+        assert D.get_legacy_filter_seed()
+        with pytest.raises(_lib.SoapError) as e:
+            D.get_soap(**_tiny_call(do_derivatives=True))
+        assert e.value.code == 1 and "legacy_filter_seed" in str(e.value)
+    finally:
+        D.set_soap_hessian_enabled(False)
