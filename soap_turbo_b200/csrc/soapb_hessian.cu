@@ -8,15 +8,13 @@
 //
 // k64_radial_d2 adds the second radial derivatives to the plain FP64 path's
 // state (src/soap_turbo_radial.f90:838-861, 895-905, 917-956; unified filter
-// seed only); k64_hess is persistent, one CTA per site at a time, and follows
-// the reference's two passes: pass A builds G (the central-atom gradient of
-// the expansion) and the unnormalised central derivative dp1, the weight
-// vectors are spread back through the compression into their S matrices and
-// contracted with c_nlm and G (Z, ZG), and pass B contracts every pair's
-// radial values and first and second derivatives against them and applies the
-// normalisation.  The angular factor Omega = C_k Q_l^m(t) w^m and its Cartesian
-// gradient and Hessian are rebuilt per pair (Q_l^m = d^m P_l / dt^m, w = x - iy
-// over r), as the reference does.  Every reduction runs in a fixed order.
+// seed only); k64_hgeo writes one geometry record per pair (pair_geometry,
+// src/soap_turbo.f90:1537-1652); k64_hess is persistent, one CTA per site at a
+// time, and follows the reference's two passes around the weight vectors' S
+// matrices (see the kernel).  The angular factor Omega = C_k Q_l^m(t) w^m and
+// its Cartesian gradient and Hessian are rebuilt from the record where needed
+// (Q_l^m = d^m P_l / dt^m, w = (x - iy)/r), as the reference does.  Every sum
+// runs in a fixed order, so results repeat bit for bit.
 #include "soapb_device.cuh"
 
 namespace soapb {
@@ -25,7 +23,8 @@ namespace {
 
 constexpr double kPi = 3.14159265358979323846;
 constexpr int kHessThreads = 256;
-constexpr int kHessVB = 8;  // weight vectors contracted per pass over a pair's k
+constexpr int kHessS = 26;  // k-sums per weight vector in pass B
+constexpr int kHessPC = 8;  // pairs per chunk of pass A
 
 #define CU_RET(x)                         \
   do {                                    \
@@ -43,7 +42,6 @@ __device__ __forceinline__ dcx operator*(dcx a, dcx b) {
   return cx(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
 }
 __device__ __forceinline__ dcx operator*(double s, dcx a) { return cx(s * a.re, s * a.im); }
-__device__ __forceinline__ dcx conjg(dcx a) { return cx(a.re, -a.im); }
 
 __device__ __forceinline__ double nv_tab(int n) { return n == -3 ? 1.0 : sqrt(1.0 / (double)(2 * n + 5)); }
 
@@ -212,17 +210,39 @@ __global__ void k64_radial_d2(const DevParams P, const DevBatch B, double *rad_d
   }
 }
 
-// Shared per-pair quantities of the Hessian kernel (pair_geometry,
-// src/soap_turbo.f90:1537-1652): written by pair_setup, read by all threads.
-struct PairGeo {
-  int good;
-  double nh[3], invr;
-  double tvec[3], thes[9];
-  dcx wvec[3], whes[9];
-  double Fl[SOAPB_MAX_LMAX + 1], Fl1[SOAPB_MAX_LMAX + 1], Fl2[SOAPB_MAX_LMAX + 1];
-  double Qt[SOAPB_KMAX_CAP];
-  dcx wpow[SOAPB_MAX_LMAX + 3];  // wpow[m + 2] = w^m, w^-1 = w^-2 = 0
+// Per-pair record of the Hessian (pair_geometry, src/soap_turbo.f90:1537-1652),
+// written once by k64_hgeo and read by k64_hess: offsets in doubles.
+struct GeoLayout {
+  int nh, invr, F, F1, F2, t, th, w, wh, Q, wp, size;
+  __host__ __device__ explicit GeoLayout(int L) {
+    const int L1 = L + 1, K = L1 * (L1 + 1) / 2;
+    nh = 0;
+    invr = 3;
+    F = 4;
+    F1 = F + L1;
+    F2 = F1 + L1;
+    t = F2 + L1;
+    th = t + 3;
+    w = th + 9;   // 3 complex
+    wh = w + 6;   // 9 complex
+    Q = wh + 18;  // K: Q_l^m(t) = d^m P_l / dt^m
+    wp = Q + K;   // L + 3 complex: w^m at m + 2, w^-2 = w^-1 = 0
+    size = wp + 2 * (L + 3);
+    size += size & 1;
+  }
 };
+
+__device__ __forceinline__ dcx ldc(const double *p) { return cx(p[0], p[1]); }
+__device__ __forceinline__ void stc(double *p, dcx v) {
+  p[0] = v.re;
+  p[1] = v.im;
+}
+
+__device__ __forceinline__ int l_of_k(int k) {
+  int l = 0;
+  while ((l + 1) * (l + 2) / 2 <= k) ++l;
+  return l;
+}
 
 // get_ilexp (src/soap_turbo_angular.f90:361-422) to lmax, for the F_l of the Hessian
 __device__ void ilexp_to(int lmax, double x, double *out) {
@@ -253,19 +273,24 @@ __device__ void ilexp_to(int lmax, double x, double *out) {
   }
 }
 
-// The scalar part of pair_geometry, one thread: F_l and its derivatives, the
-// unit vector, the gradients and Hessians of t = cos(theta) and w, Q_l^m, w^m.
-__device__ void pair_setup(const DevParams &P, const DevBatch &B, int kk, bool want2, PairGeo &G) {
-  G.good = 0;
-  const double rr = B.rjs[kk];
-  if (rr >= P.rcut_max || rr < 1.0e-10) return;
-  const unsigned bits = B.bits[kk];
-  if (bits == 0u) return;
-  const int isp = __ffs(bits) - 1;
-  G.good = 1;
+// ---- pair geometry, one thread per pair: F_l and its first two r-derivatives,
+// the unit vector, the gradients and Hessians of t = cos(theta) and
+// w = (x - iy)/r, Q_l^m(t) and w^m.  good[k] = 0 for pairs the Hessian skips
+// (beyond rcut_max, at the origin, or in no species).
+__global__ void k64_hgeo(const DevParams P, const DevBatch B, double *geo, int *good) {
+  const int kk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kk >= B.n_pairs) return;
   const int L = P.l_max;
+  const GeoLayout Lg(L);
+  double *g = geo + (size_t)kk * Lg.size;
+  const double rr = B.rjs[kk];
+  const unsigned bits = B.bits[kk];
+  const bool ok = rr < P.rcut_max && rr >= 1.0e-10 && bits != 0u;
+  good[kk] = ok ? 1 : 0;
+  if (!ok) return;
+  const int isp = __ffs(bits) - 1;
   const double invr = 1.0 / rr, invr2 = invr * invr;
-  G.invr = invr;
+  g[Lg.invr] = invr;
   const double sscal = P.sig_t_c[isp], sig = P.sig_t[isp] + sscal * rr;
   const double amp = P.rcut2 / (sig * sig), ampd = -2.0 * sscal / sig * amp;
   const double ampdd = 6.0 * sscal * sscal / (sig * sig) * amp;
@@ -281,157 +306,117 @@ __device__ void pair_setup(const DevParams &P, const DevBatch &B, int kk, bool w
     const double d2il = il[l + 2] + ((double)(2 * l + 1) * invz - 2.0) * il[l + 1] +
                         (rl * (rl - 1.0) * invz * invz - 2.0 * rl * invz + 1.0) * il[l];
     const double f0 = il[l], f1 = dil * zp, f2 = d2il * zp * zp + dil * zp2;
-    G.Fl[l] = amp * f0;
-    G.Fl1[l] = ampd * f0 + amp * f1;
-    G.Fl2[l] = ampdd * f0 + 2.0 * ampd * f1 + amp * f2;
+    g[Lg.F + l] = amp * f0;
+    g[Lg.F1 + l] = ampd * f0 + amp * f1;
+    g[Lg.F2 + l] = ampdd * f0 + 2.0 * ampd * f1 + amp * f2;
   }
+  double nh[3];
   const double sin_t = sin(B.thetas[kk]), cos_t = cos(B.thetas[kk]);
   const double sin_f = sin(B.phis[kk]), cos_f = cos(B.phis[kk]);
-  G.nh[0] = sin_t * cos_f;
-  G.nh[1] = sin_t * sin_f;
-  G.nh[2] = cos_t;
-  const double tt = G.nh[2];
-  const dcx wc = cx(G.nh[0], -G.nh[1]);
+  nh[0] = sin_t * cos_f;
+  nh[1] = sin_t * sin_f;
+  nh[2] = cos_t;
+  for (int q = 0; q < 3; ++q) g[Lg.nh + q] = nh[q];
+  const double tt = nh[2];
+  const dcx wc = cx(nh[0], -nh[1]);
   const dcx ec[3] = {cx(1.0, 0.0), cx(0.0, -1.0), cx(0.0, 0.0)};
   for (int q = 0; q < 3; ++q) {
-    G.tvec[q] = -tt * G.nh[q] * invr;
-    G.wvec[q] = (-G.nh[q] * invr) * wc;
+    g[Lg.t + q] = -tt * nh[q] * invr + (q == 2 ? invr : 0.0);
+    stc(g + Lg.w + 2 * q, (-nh[q] * invr) * wc + invr * ec[q]);
   }
-  G.tvec[2] = G.tvec[2] + invr;
-  for (int q = 0; q < 3; ++q) G.wvec[q] = G.wvec[q] + invr * ec[q];
-  if (want2) {
-    for (int bb = 0; bb < 3; ++bb)
-      for (int aa = 0; aa < 3; ++aa) {
-        G.thes[bb * 3 + aa] = (3.0 * tt * G.nh[aa] * G.nh[bb]) * invr2;
-        G.whes[bb * 3 + aa] = invr2 * ((3.0 * G.nh[aa] * G.nh[bb]) * wc - G.nh[bb] * ec[aa] - G.nh[aa] * ec[bb]);
-      }
+  for (int bb = 0; bb < 3; ++bb)
     for (int aa = 0; aa < 3; ++aa) {
-      G.thes[aa * 3 + 2] = G.thes[aa * 3 + 2] - G.nh[aa] * invr2;
-      G.thes[2 * 3 + aa] = G.thes[2 * 3 + aa] - G.nh[aa] * invr2;
-      G.thes[aa * 3 + aa] = G.thes[aa * 3 + aa] - tt * invr2;
-      G.whes[aa * 3 + aa] = G.whes[aa * 3 + aa] - invr2 * wc;
+      double th = (3.0 * tt * nh[aa] * nh[bb]) * invr2;
+      dcx wh = invr2 * ((3.0 * nh[aa] * nh[bb]) * wc - nh[bb] * ec[aa] - nh[aa] * ec[bb]);
+      if (bb == 2) th = th - nh[aa] * invr2;
+      if (aa == 2) th = th - nh[bb] * invr2;
+      if (aa == bb) {
+        th = th - tt * invr2;
+        wh = wh - invr2 * wc;
+      }
+      g[Lg.th + bb * 3 + aa] = th;
+      stc(g + Lg.wh + 2 * (bb * 3 + aa), wh);
     }
-  }
-  G.Qt[0] = 1.0;
+  double *Qt = g + Lg.Q;
+  Qt[0] = 1.0;
   if (L >= 1) {
-    G.Qt[1] = tt;
-    G.Qt[2] = 1.0;
+    Qt[1] = tt;
+    Qt[2] = 1.0;
   }
   for (int ll = 2; ll <= L; ++ll) {
     const int kbb = ll * (ll + 1) / 2;
     for (int mm = 0; mm <= ll - 2; ++mm) {
       const int kq = kbb + mm;
-      G.Qt[kq] = ((double)(2 * ll - 1) * tt * G.Qt[kq - ll] - (double)(ll + mm - 1) * G.Qt[kq - 2 * ll + 1]) /
-                 (double)(ll - mm);
+      Qt[kq] = ((double)(2 * ll - 1) * tt * Qt[kq - ll] - (double)(ll + mm - 1) * Qt[kq - 2 * ll + 1]) /
+               (double)(ll - mm);
     }
-    G.Qt[kbb + ll - 1] = (double)(2 * ll - 1) * tt * G.Qt[kbb - 1];
-    G.Qt[kbb + ll] = (double)(2 * ll - 1) * G.Qt[kbb - 1];
+    Qt[kbb + ll - 1] = (double)(2 * ll - 1) * tt * Qt[kbb - 1];
+    Qt[kbb + ll] = (double)(2 * ll - 1) * Qt[kbb - 1];
   }
-  G.wpow[0] = cx(0.0, 0.0);
-  G.wpow[1] = cx(0.0, 0.0);
-  G.wpow[2] = cx(1.0, 0.0);
-  for (int mm = 1; mm <= L; ++mm) G.wpow[mm + 2] = G.wpow[mm + 1] * wc;
+  dcx wpow = cx(1.0, 0.0);
+  stc(g + Lg.wp, cx(0.0, 0.0));
+  stc(g + Lg.wp + 2, cx(0.0, 0.0));
+  stc(g + Lg.wp + 4, wpow);
+  for (int mm = 1; mm <= L; ++mm) {
+    wpow = wpow * wc;
+    stc(g + Lg.wp + 2 * (mm + 2), wpow);
+  }
 }
 
-// Omega, dOmega and (want2) d2Omega of component kq (:1620-1650); Ck the signed prefactor.
-__device__ __forceinline__ void omega_k(const PairGeo &G, int kq, int ll, int mm, double Ck, bool want2, dcx &Om,
-                                        dcx *dOm, dcx *d2Om) {
-  const double q0 = G.Qt[kq], q1 = (mm + 1 <= ll) ? G.Qt[kq + 1] : 0.0, q2 = (mm + 2 <= ll) ? G.Qt[kq + 2] : 0.0;
-  const dcx w0 = G.wpow[mm + 2], w1 = G.wpow[mm + 1], w2 = G.wpow[mm];
+// Omega, dOmega and (want2) d2Omega of component kq from a pair record
+// (:1620-1650); Ck the signed prefactor (-1)^m preflm.
+__device__ __forceinline__ void omega_k(const double *g, const GeoLayout &Lg, int kq, int ll, int mm, double Ck,
+                                        bool want2, dcx &Om, dcx *dOm, dcx *d2Om) {
+  const double *Qt = g + Lg.Q;
+  const double q0 = Qt[kq], q1 = (mm + 1 <= ll) ? Qt[kq + 1] : 0.0, q2 = (mm + 2 <= ll) ? Qt[kq + 2] : 0.0;
+  const dcx w0 = ldc(g + Lg.wp + 2 * (mm + 2)), w1 = ldc(g + Lg.wp + 2 * (mm + 1)), w2 = ldc(g + Lg.wp + 2 * mm);
+  const double *tv = g + Lg.t;
+  dcx wv[3];
+  for (int aa = 0; aa < 3; ++aa) wv[aa] = ldc(g + Lg.w + 2 * aa);
   Om = (Ck * q0) * w0;
-  for (int aa = 0; aa < 3; ++aa) dOm[aa] = Ck * ((q1 * G.tvec[aa]) * w0 + (q0 * (double)mm) * (w1 * G.wvec[aa]));
+  for (int aa = 0; aa < 3; ++aa) dOm[aa] = Ck * ((q1 * tv[aa]) * w0 + (q0 * (double)mm) * (w1 * wv[aa]));
   if (want2)
     for (int bb = 0; bb < 3; ++bb)
       for (int aa = 0; aa < 3; ++aa)
         d2Om[bb * 3 + aa] =
-            Ck * ((q2 * G.tvec[aa] * G.tvec[bb]) * w0 + (q1 * G.thes[bb * 3 + aa]) * w0 +
-                  (q1 * (double)mm) * (w1 * (G.tvec[aa] * G.wvec[bb] + G.tvec[bb] * G.wvec[aa])) +
-                  (q0 * (double)(mm * (mm - 1))) * (w2 * (G.wvec[aa] * G.wvec[bb])) +
-                  (q0 * (double)mm) * (w1 * G.whes[bb * 3 + aa]));
+            Ck * ((q2 * tv[aa] * tv[bb]) * w0 + (q1 * g[Lg.th + bb * 3 + aa]) * w0 +
+                  (q1 * (double)mm) * (w1 * (tv[aa] * wv[bb] + tv[bb] * wv[aa])) +
+                  (q0 * (double)(mm * (mm - 1))) * (w2 * (wv[aa] * wv[bb])) +
+                  (q0 * (double)mm) * (w1 * ldc(g + Lg.wh + 2 * (bb * 3 + aa))));
 }
 
-// Per-CTA global scratch of the Hessian kernel (doubles), see hess_scratch_doubles
+// One (b, a) element of the second-derivative block from the k-sums S of a
+// weight vector (layout: S1, S2, S3[3], S4 upper triangle[6], S5[3], S6[3][3], S7[3]).
+__device__ __forceinline__ double hv_block(const double *S, const double *nh, double invr, int aa, int bb) {
+  const int lo = aa < bb ? aa : bb, hi = aa < bb ? bb : aa;
+  const int tri = lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
+  return -(nh[aa] * nh[bb] * S[0] + (aa == bb ? invr * S[1] : 0.0) + nh[aa] * S[2 + bb] + nh[bb] * S[2 + aa] +
+           S[5 + tri] + nh[bb] * S[11 + aa] + S[14 + aa * 3 + bb]);
+}
+
+// Per-CTA global scratch of the Hessian kernel (hess_scratch_doubles)
 struct HessScratch {
-  dcx *Gacc;      // (n_max, k_max, 3)
-  dcx *Zv, *ZGv;  // (nv, n_max, k_max), (nv, n_max, k_max, 3)
-  double *dp1, *dp2;  // (n_soap, 3)
-  double *kept3;  // (3, n_kept): one pair's spherical derivatives of the kept components
+  double *Gacc;   // (n_max, k_max, 3) complex: G = sum_j d c_nlm / d r_j
+  double *Zv;     // (n_vec + 4, n_max, k_max) complex: S_v c for every weight vector
+  double *ZGv;    // (n_vec + 1, n_max, k_max, 3) complex: S_v G for the Hessian's vectors
+  double *dp1;    // (n_soap, 3): d p / d r_i, unnormalised
+  double *kept3;  // (3, n_kept)
   double *vk;     // (n_kept): a weight vector spread through the compression
 };
 
-__device__ HessScratch carve(double *base, const DevParams &P, int nv) {
+__device__ HessScratch carve(double *base, const DevParams &P, int n_vec) {
   const size_t nk = (size_t)P.n_max * P.k_max;
   HessScratch h;
-  h.Gacc = (dcx *)base;
-  h.Zv = h.Gacc + 3 * nk;
-  h.ZGv = h.Zv + (size_t)nv * nk;
-  h.dp1 = (double *)(h.ZGv + 3 * (size_t)nv * nk);
-  h.dp2 = h.dp1 + 3 * (size_t)P.n_soap;
-  h.kept3 = h.dp2 + 3 * (size_t)P.n_soap;
+  h.Gacc = base;
+  h.Zv = h.Gacc + 6 * nk;
+  h.ZGv = h.Zv + 2 * (size_t)(n_vec + 4) * nk;
+  h.dp1 = h.ZGv + 6 * (size_t)(n_vec + 1) * nk;
+  h.kept3 = h.dp1 + 3 * (size_t)P.n_soap;
   h.vk = h.kept3 + 3 * (size_t)P.n_kept;
   return h;
 }
 
-// The Cartesian, unnormalised derivative of the site's compressed p for pair
-// kk (pair_dp, :1520-1534, on soap_rad/azi/pol_der, :1927-2075) into dp (n_soap, 3).
-__device__ void pair_dp(const DevParams &P, const DevBatch &B, int kk, const double *rad, const double *rad_der,
-                        const double2 *ang, const double2 *c, double *sPQ, double *kept3, double *dp) {
-  const int N = P.n_max, K = P.k_max, L1 = P.l_max + 1, nk = P.n_kept;
-  const size_t plane = (size_t)B.n_pairs * K;
-  const double2 *A = ang + (size_t)kk * K;
-  for (int it = threadIdx.x; it < N * L1; it += blockDim.x) {
-    const int n = it / L1, l = it - n * L1;
-    double ap = 0.0, aq = 0.0, aa = 0.0, ao = 0.0;
-    for (int m = 0; m <= l; ++m) {
-      const int k = l * (l + 1) / 2 + m;
-      const double w = (m == 0) ? 1.0 : 2.0;
-      const double2 cc = c[(size_t)n * K + k];
-      const double2 a0 = A[k], a1 = A[plane + k], a2 = A[2 * plane + k], a3 = A[3 * plane + k];
-      ap = ap + w * (a0.x * cc.x + a0.y * cc.y);
-      aq = aq + w * (a1.x * cc.x + a1.y * cc.y);
-      aa = aa + w * (a2.x * cc.x + a2.y * cc.y);
-      ao = ao + w * (a3.x * cc.x + a3.y * cc.y);
-    }
-    sPQ[it] = ap;
-    sPQ[N * L1 + it] = aq;
-    sPQ[2 * N * L1 + it] = aa;
-    sPQ[3 * N * L1 + it] = ao;
-  }
-  __syncthreads();
-  const double *Pm = sPQ, *Qm = sPQ + N * L1, *Qa = sPQ + 2 * N * L1, *Qo = sPQ + 3 * N * L1;
-  for (int q = threadIdx.x; q < nk; q += blockDim.x) {
-    const int code = P.kept_nnl[q];
-    const int n = code & 0xff, np = (code >> 8) & 0xff, l = code >> 16;
-    const double rn = rad[(size_t)kk * N + n], rdn = rad_der[(size_t)kk * N + n];
-    const double rnp = rad[(size_t)kk * N + np], rdnp = rad_der[(size_t)kk * N + np];
-    const double pre = 4.0 * kPi * ((n == np) ? 1.0 : sqrt(2.0));
-    kept3[q] = pre * (rdn * Pm[np * L1 + l] + rn * Qm[np * L1 + l] + rdnp * Pm[n * L1 + l] + rnp * Qm[n * L1 + l]);
-    kept3[nk + q] = pre * (rn * Qa[np * L1 + l] + rnp * Qa[n * L1 + l]);
-    kept3[2 * nk + q] = pre * (rn * Qo[np * L1 + l] + rnp * Qo[n * L1 + l]);
-  }
-  __syncthreads();
-  const double st = sin(B.thetas[kk]), ct = cos(B.thetas[kk]), sf = sin(B.phis[kk]), cf = cos(B.phis[kk]);
-  const double ir = 1.0 / B.rjs[kk];
-  const double cxr = st * cf, cyr = st * sf, czr = ct, pxr = -ct * cf * ir, pyr = -ct * sf * ir, pzr = st * ir;
-  const double axr = -sf * ir, ayr = cf * ir;
-  for (int o = threadIdx.x; o < P.n_soap; o += blockDim.x) {
-    double dr = 0.0, da = 0.0, dpl = 0.0;
-    for (int t = P.pi_off[o]; t < P.pi_off[o + 1]; ++t) {
-      const double e = P.pi_el64[t];
-      const int q = P.pi_q[t];
-      dr = dr + e * kept3[q];
-      da = da + e * kept3[nk + q];
-      dpl = dpl + e * kept3[2 * nk + q];
-    }
-    dp[3 * o + 0] = cxr * dr + pxr * dpl + axr * da;
-    dp[3 * o + 1] = cyr * dr + pyr * dpl + ayr * da;
-    dp[3 * o + 2] = czr * dr + pzr * dpl;
-  }
-  __syncthreads();
-}
-
-// Warp-wise dot products of length n over fixed lane strides and a fixed
-// shuffle tree: x . y (both with element stride sx, sy).
+// Warp-wise dot product over fixed lane strides and a fixed shuffle tree.
 __device__ __forceinline__ double warp_dot(const double *x, int sx, const double *y, int sy, int n) {
   const int lane = threadIdx.x & 31;
   double s = 0.0;
@@ -440,26 +425,57 @@ __device__ __forceinline__ double warp_dot(const double *x, int sx, const double
   return s;
 }
 
+// Weight vectors of one site: v < n_vec the caller's, v = n_vec the site's
+// unnormalised p, v = n_vec + 1 + a the column a of dp1.  Of the first n_vec + 1
+// the Hessian is formed; the last three give dp1 . dp_j.
+__device__ __forceinline__ double weight(const double *vecs, const double *soap_i, double sv, const double *dp1,
+                                         int n_vec, int ns, int site, int v, int o) {
+  if (v < n_vec) return vecs[((size_t)site * n_vec + v) * ns + o];
+  if (v == n_vec) return soap_i[o] * sv;
+  return dp1[3 * o + (v - n_vec - 1)];
+}
+
+// ---- the Hessian, persistent, one CTA per site at a time.  Per site:
+//  A  G(n,k) = sum_j d/dr_j [4 pi R_n F_l Omega_k] (:1305-1334), a fixed-order
+//     sum over the site's pairs of R'_n A_j + R_n B_j, with the pairs' angular
+//     factors A_j, B_j built in shared memory chunk by chunk; then
+//     dp1 = d p / d r_i = -(d p / d c) G component by component of p (the
+//     reference sums -dp_j over the pairs; the two agree to rounding, since
+//     sum_j d c / d r_j = G);
+//  Z  every weight vector v spread back through the compression into its
+//     S_v(n, n', l) and applied to c_nlm (Z_v) and to G (ZG_v) (:1336-1376);
+//  B  one warp per pair, lanes over k: Z_v and ZG_v contracted with the pair's
+//     R_n, R'_n, R''_n and Omega, dOmega, d2Omega (:1378-1412) give the second
+//     derivative hv and the first derivative v . dp_j (what the reference's
+//     self-test rebuilds, here the value used), and from them the
+//     normalisation (:1414-1484).
+// Sums run in a fixed order (pairs to warps by index, a fixed shuffle tree,
+// k rounds in order, warps in index order).
 __global__ void __launch_bounds__(kHessThreads) k64_hess(const DevParams P, const DevBatch B, const double *rad,
                                                          const double *rad_der, const double *rad_der2,
-                                                         const double2 *ang, const double2 *cnk,
+                                                         const double *geo, const int *good, const double2 *cnk,
                                                          const double *norm, const double *soap, int n_vec,
                                                          const double *vecs, double *hess, double *scratch,
                                                          size_t scratch_per_cta, int *ticket) {
   extern __shared__ __align__(16) double sm[];
-  __shared__ PairGeo G;
   __shared__ int s_site;
-  const int N = P.n_max, K = P.k_max, L1 = P.l_max + 1, ns = P.n_soap, nv = n_vec + 1;
+  const int N = P.n_max, K = P.k_max, ns = P.n_soap, nk = P.n_kept;
+  const int nvh = n_vec + 1, nva = n_vec + 4;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, n_warps = kHessThreads / 32;
-  // shared: pvec (ns), sPQ (4 N L1), per-k partial sums (K, kHessVB, 9), hv (nv, 9),
-  // hsum (n_vec, 9), dots (15 + 7 n_vec)
-  double *pvec = sm;
-  double *sPQ = pvec + ns;
-  double *part = sPQ + 4 * N * L1;
-  double *hv = part + (size_t)K * kHessVB * 9;
-  double *hsum = hv + 9 * nv;
-  double *dots = hsum + 9 * n_vec;
-  const HessScratch h = carve(scratch + scratch_per_cta * blockIdx.x, P, nv);
+  const GeoLayout Lg(P.l_max);
+  // shared: the site's dot products (3 + 4 n_vec), then a region used by pass
+  // A (a chunk of kHessPC pairs: their A, B factors (K, 12) and R, R' rows) and
+  // by pass B (per warp: the k-sums of its pair (n_vec + 4, kHessS), its radial
+  // rows (3 n_max) and its running hsum (n_vec, 9))
+  const int sd = 3 + 4 * n_vec + ((3 + 4 * n_vec) & 1);
+  const int per_warp = kHessS * nva + 3 * N + 9 * n_vec;
+  double *sdot = sm;
+  double *cab = sm + sd;
+  double *crr = cab + (size_t)kHessPC * K * 12;
+  double *wsum = sm + sd + (size_t)warp * per_warp;
+  double *wrad = wsum + kHessS * nva;
+  double *whs = wrad + 3 * N;
+  const HessScratch h = carve(scratch + scratch_per_cta * blockIdx.x, P, n_vec);
   const double fourpi = 4.0 * kPi;
 
   for (;;) {
@@ -471,194 +487,291 @@ __global__ void __launch_bounds__(kHessThreads) k64_hess(const DevParams P, cons
     const int p0 = B.off[site], p1 = min(B.off[site + 1], B.n_pairs);
     const double sv = norm[site], invs = 1.0 / sv, invs3 = invs / (sv * sv), invs5 = invs3 / (sv * sv);
     const double2 *c = cnk + (size_t)site * N * K;
-    for (int q = tid; q < ns; q += kHessThreads) pvec[q] = soap[(size_t)site * ns + q] * sv;
-    // ---- pass A: G and the unnormalised central-atom derivative (:1305-1334)
-    for (int t = tid; t < 3 * N * K; t += kHessThreads) h.Gacc[t] = cx(0.0, 0.0);
-    for (int t = tid; t < 3 * ns; t += kHessThreads) h.dp1[t] = 0.0;
-    __syncthreads();
-    for (int k2 = p0 + 1; k2 < p1; ++k2) {
-      if (tid == 0) pair_setup(P, B, k2, false, G);
+    const double *soap_i = soap + (size_t)site * ns;
+    // ---- A: G, threads over (n, k), the pairs in CSR order in chunks of kHessPC:
+    // A(j, k, q) = 4 pi F_l nh_q Omega_k, B = 4 pi (F'_l nh_q Omega_k + F_l dOmega_kq),
+    // G(n, k, q) = sum_j R'_n(j) A(j, k, q) + R_n(j) B(j, k, q) (:1320-1331)
+    for (int t = tid; t < 6 * N * K; t += kHessThreads) h.Gacc[t] = 0.0;
+    for (int jc = p0 + 1; jc < p1; jc += kHessPC) {
+      const int nc = min(kHessPC, p1 - jc);
       __syncthreads();
-      if (!G.good) continue;
-      pair_dp(P, B, k2, rad, rad_der, ang, c, sPQ, h.kept3, h.dp2);
-      for (int t = tid; t < 3 * ns; t += kHessThreads) h.dp1[t] = h.dp1[t] - h.dp2[t];
-      for (int it = tid; it < N * K; it += kHessThreads) {
-        const int n = it / K, k = it - n * K;
-        int l = 0;
-        while ((l + 1) * (l + 2) / 2 <= k) ++l;
-        const int m = k - l * (l + 1) / 2;
+      for (int t = tid; t < nc * 2 * N; t += kHessThreads) {
+        const int pp = t / (2 * N), r = t - pp * 2 * N;
+        crr[t] = (r < N ? rad : rad_der)[(size_t)(jc + pp) * N + (r < N ? r : r - N)];
+      }
+      for (int t = tid; t < nc * K; t += kHessThreads) {
+        const int pp = t / K, k = t - pp * K, j = jc + pp;
+        double *o = cab + (size_t)t * 12;
+        if (!good[j]) {
+          for (int e = 0; e < 12; ++e) o[e] = 0.0;
+          continue;
+        }
+        const double *g = geo + (size_t)j * Lg.size;
+        const int l = l_of_k(k), m = k - l * (l + 1) / 2;
         dcx Om, dOm[3];
-        omega_k(G, k, l, m, (m & 1) ? -P.preflm64[k] : P.preflm64[k], false, Om, dOm, nullptr);
-        const double r0 = fourpi * rad[(size_t)k2 * N + n], r1 = fourpi * rad_der[(size_t)k2 * N + n];
-        const double g0 = r0 * G.Fl[l], g1 = r1 * G.Fl[l] + r0 * G.Fl1[l];
-        for (int q = 0; q < 3; ++q) h.Gacc[(size_t)it * 3 + q] = h.Gacc[(size_t)it * 3 + q] + (g1 * G.nh[q]) * Om + g0 * dOm[q];
+        omega_k(g, Lg, k, l, m, (m & 1) ? -P.preflm64[k] : P.preflm64[k], false, Om, dOm, nullptr);
+        const double f0 = fourpi * g[Lg.F + l], f1 = fourpi * g[Lg.F1 + l];
+        for (int q = 0; q < 3; ++q) {
+          const double nq = g[Lg.nh + q];
+          stc(o + 4 * q, (f0 * nq) * Om);
+          stc(o + 4 * q + 2, (f1 * nq) * Om + f0 * dOm[q]);
+        }
       }
       __syncthreads();
+      for (int it = tid; it < N * K; it += kHessThreads) {
+        const int n = it / K, k = it - n * K;
+        double *ga = h.Gacc + (size_t)it * 6;
+        dcx gq[3] = {ldc(ga), ldc(ga + 2), ldc(ga + 4)};
+        for (int pp = 0; pp < nc; ++pp) {
+          const double r0 = crr[pp * 2 * N + n], r1 = crr[pp * 2 * N + N + n];
+          const double *a = cab + ((size_t)pp * K + k) * 12;
+          for (int q = 0; q < 3; ++q) gq[q] = gq[q] + r1 * ldc(a + 4 * q) + r0 * ldc(a + 4 * q + 2);
+        }
+        for (int q = 0; q < 3; ++q) stc(ga + 2 * q, gq[q]);
+      }
     }
-    // ---- the weight vectors spread back through the compression, their S
-    // matrices applied to c_nlm and G (:1336-1376), through the Y lists
-    for (int v = 0; v < nv; ++v) {
-      const double *vin = v < n_vec ? vecs + ((size_t)site * n_vec + v) * ns : pvec;
-      for (int q = tid; q < P.n_kept; q += kHessThreads) {
+    __syncthreads();
+    // dp1 in the kept components, then through the compression map
+    for (int q = tid; q < nk; q += kHessThreads) {
+      const int code = P.kept_nnl[q];
+      const int n = code & 0xff, np = (code >> 8) & 0xff, l = code >> 16;
+      const double base = (n == np) ? 1.0 : sqrt(2.0);
+      double d[3] = {0.0, 0.0, 0.0};
+      for (int m = 0; m <= l; ++m) {
+        const int k = l * (l + 1) / 2 + m;
+        const double w = base * ((m > 0) ? 2.0 : 1.0);
+        const double2 a = c[(size_t)n * K + k], b = c[(size_t)np * K + k];
+        const double *ga = h.Gacc + ((size_t)n * K + k) * 6, *gb = h.Gacc + ((size_t)np * K + k) * 6;
+        for (int e = 0; e < 3; ++e)
+          d[e] = d[e] - w * (ga[2 * e] * b.x + ga[2 * e + 1] * b.y + a.x * gb[2 * e] + a.y * gb[2 * e + 1]);
+      }
+      for (int e = 0; e < 3; ++e) h.kept3[(size_t)e * nk + q] = d[e];
+    }
+    __syncthreads();
+    for (int o = tid; o < ns; o += kHessThreads) {
+      double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+      for (int t = P.pi_off[o]; t < P.pi_off[o + 1]; ++t) {
+        const double e = P.pi_el64[t];
+        const int q = P.pi_q[t];
+        d0 = d0 + e * h.kept3[q];
+        d1 = d1 + e * h.kept3[nk + q];
+        d2 = d2 + e * h.kept3[2 * nk + q];
+      }
+      h.dp1[3 * o] = d0;
+      h.dp1[3 * o + 1] = d1;
+      h.dp1[3 * o + 2] = d2;
+    }
+    __syncthreads();
+    // the site's dot products: t1 (3), then per v wp, u1 (3)
+    for (int d = warp; d < 3 + 4 * n_vec; d += n_warps) {
+      double r;
+      if (d < 3) r = sv * warp_dot(soap_i, 1, h.dp1 + d, 3, ns);
+      else {
+        const int v = (d - 3) >> 2, e = (d - 3) & 3;
+        const double *wv = vecs + ((size_t)site * n_vec + v) * ns;
+        r = (e == 0) ? sv * warp_dot(wv, 1, soap_i, 1, ns) : warp_dot(wv, 1, h.dp1 + (e - 1), 3, ns);
+      }
+      if (lane == 0) sdot[d] = r;
+    }
+    // ---- Z: S_v applied to c and G through the per-(l, n) lists of the kept
+    // components (2 v on the diagonal, sqrt 2 v off it, np ascending)
+    for (int v = 0; v < nva; ++v) {
+      for (int q = tid; q < nk; q += kHessThreads) {
         double s = 0.0;
-        for (int t = P.pj_off[q]; t < P.pj_off[q + 1]; ++t) s = s + P.pj_el64[t] * vin[P.pj_o[t]];
+        for (int t = P.pj_off[q]; t < P.pj_off[q + 1]; ++t)
+          s = s + P.pj_el64[t] * weight(vecs, soap_i, sv, h.dp1, n_vec, ns, site, v, P.pj_o[t]);
         h.vk[q] = s;
       }
       __syncthreads();
       for (int it = tid; it < N * K; it += kHessThreads) {
-        const int n = it / K, k = it - n * K;
-        int l = 0;
-        while ((l + 1) * (l + 2) / 2 <= k) ++l;
-        // S(n, np, l) from the kept component (min, max, l): 2 v on the
-        // diagonal, sqrt 2 v off it; the list runs over np ascending
+        const int n = it / K, k = it - n * K, l = l_of_k(k);
         dcx zc = cx(0.0, 0.0), b0[3] = {cx(0.0, 0.0), cx(0.0, 0.0), cx(0.0, 0.0)};
         for (int t = P.hl_off[l * N + n]; t < P.hl_off[l * N + n + 1]; ++t) {
           const int np = P.hl_np[t];
           const double smv = P.hl_fac64[t] * h.vk[P.hl_q[t]];
           const double2 cc = c[(size_t)np * K + k];
           zc = zc + cx(smv * cc.x, smv * cc.y);
-          for (int q = 0; q < 3; ++q) b0[q] = b0[q] + smv * h.Gacc[((size_t)np * K + k) * 3 + q];
+          if (v < nvh)
+            for (int q = 0; q < 3; ++q) b0[q] = b0[q] + smv * ldc(h.Gacc + ((size_t)np * K + k) * 6 + 2 * q);
         }
-        h.Zv[((size_t)v * N + n) * K + k] = zc;
-        for (int q = 0; q < 3; ++q) h.ZGv[(((size_t)v * N + n) * K + k) * 3 + q] = b0[q];
+        stc(h.Zv + (((size_t)v * N + n) * K + k) * 2, zc);
+        if (v < nvh)
+          for (int q = 0; q < 3; ++q) stc(h.ZGv + ((((size_t)v * N + n) * K + k) * 3 + q) * 2, b0[q]);
       }
       __syncthreads();
     }
-    // ---- pass B: per pair, the contraction and the normalisation (:1378-1486)
-    for (int t = tid; t < 9 * n_vec; t += kHessThreads) hsum[t] = 0.0;
-    __syncthreads();
-    for (int k2 = p0 + 1; k2 < p1; ++k2) {
-      if (tid == 0) pair_setup(P, B, k2, true, G);
-      __syncthreads();
-      if (!G.good) continue;
-      pair_dp(P, B, k2, rad, rad_der, ang, c, sPQ, h.kept3, h.dp2);
-      for (int vb = 0; vb < nv; vb += kHessVB) {
-        const int nvb = min(kHessVB, nv - vb);
-        for (int it = tid; it < K * nvb; it += kHessThreads) {
-          const int k = it / nvb, v = vb + (it - (it / nvb) * nvb);
-          int l = 0;
-          while ((l + 1) * (l + 2) / 2 <= k) ++l;
-          const int m = k - l * (l + 1) / 2;
-          dcx Om, dOm[3], d2Om[9];
-          omega_k(G, k, l, m, (m & 1) ? -P.preflm64[k] : P.preflm64[k], true, Om, dOm, d2Om);
+    // ---- B: one warp per pair, lanes over k (rounds of 32).  Per weight vector
+    // the k-sums below give the block (:1378-1412, reassociated over k):
+    //   S1 = sum w Re[(z2 - z1/r) Om]   S2 = sum w Re[z1 Om]    S3_b = sum w Re[z1 dOm_b]
+    //   S4_ab = sum w Re[z0 d2Om_ab]    S5_a = sum w Re[gg1_a Om]
+    //   S6_ab = sum w Re[gg0_a dOm_b]   S7_b = sum w Re[z0 dOm_b]
+    //   hv(b, a) = -(n_a n_b S1 + [a = b] S2 / r + n_a S3_b + n_b S3_a + S4_ab + n_b S5_a + S6_ab)
+    //   v . dp_j (b) = n_b S2 + S7_b
+    for (int t = lane; t < 9 * n_vec; t += 32) whs[t] = 0.0;
+    for (int j = p0 + 1 + warp; j < p1; j += n_warps) {
+      if (!good[j]) continue;
+      const double *g = geo + (size_t)j * Lg.size;
+      for (int t = lane; t < 3 * N; t += 32) {
+        const int w = t / N, n = t - w * N;
+        wrad[t] = (w == 0 ? rad : (w == 1 ? rad_der : rad_der2))[(size_t)j * N + n];
+      }
+      for (int t = lane; t < kHessS * nva; t += 32) wsum[t] = 0.0;
+      __syncwarp();
+      for (int k0 = 0; k0 < K; k0 += 32) {
+        const int k = k0 + lane;
+        const bool act = k < K;
+        const int kc = act ? k : 0;
+        const int l = l_of_k(kc), m = kc - l * (l + 1) / 2;
+        dcx Om, dOm[3], d2Om[9];
+        omega_k(g, Lg, kc, l, m, (m & 1) ? -P.preflm64[kc] : P.preflm64[kc], true, Om, dOm, d2Om);
+        const double wmk = act ? ((m > 0) ? 2.0 : 1.0) : 0.0;
+        const double f0 = fourpi * g[Lg.F + l], f1 = fourpi * g[Lg.F1 + l], f2 = fourpi * g[Lg.F2 + l];
+        for (int v = 0; v < nva; ++v) {
+          const bool full = v < nvh;
           dcx a0 = cx(0.0, 0.0), a1 = a0, a2 = a0, b0[3] = {a0, a0, a0}, b1[3] = {a0, a0, a0};
-          for (int n = 0; n < N; ++n) {
-            const double r0 = rad[(size_t)k2 * N + n], r1 = rad_der[(size_t)k2 * N + n];
-            const double r2 = rad_der2[(size_t)k2 * N + n];
-            const dcx zc = conjg(h.Zv[((size_t)v * N + n) * K + k]);
-            a0 = a0 + r0 * zc;
-            a1 = a1 + r1 * zc;
-            a2 = a2 + r2 * zc;
-            for (int q = 0; q < 3; ++q) {
-              const dcx gc = conjg(h.ZGv[(((size_t)v * N + n) * K + k) * 3 + q]);
-              b0[q] = b0[q] + r0 * gc;
-              b1[q] = b1[q] + r1 * gc;
+          if (act) {
+            const double2 *zv = (const double2 *)h.Zv + (size_t)v * N * K + k;
+            const double2 *zg = (const double2 *)h.ZGv + ((size_t)v * N * K + k) * 3;
+            for (int n = 0; n < N; ++n) {
+              const double2 zz = zv[(size_t)n * K];
+              const dcx zc = cx(zz.x, -zz.y);
+              const double r0 = wrad[n], r1 = wrad[N + n];
+              a0 = a0 + r0 * zc;
+              a1 = a1 + r1 * zc;
+              if (full) {
+                a2 = a2 + wrad[2 * N + n] * zc;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                  const double2 gz = zg[(size_t)n * K * 3 + q];
+                  const dcx gc = cx(gz.x, -gz.y);
+                  b0[q] = b0[q] + r0 * gc;
+                  b1[q] = b1[q] + r1 * gc;
+                }
+              }
             }
           }
-          const double f0 = G.Fl[l], f1 = G.Fl1[l], f2 = G.Fl2[l], wmk = (m > 0) ? 2.0 : 1.0;
-          const dcx z0 = (fourpi * f0) * a0, z1 = fourpi * (f0 * a1 + f1 * a0);
-          const dcx z2 = fourpi * (f0 * a2 + (2.0 * f1) * a1 + f2 * a0);
-          dcx gg0[3], gg1[3];
-          for (int q = 0; q < 3; ++q) {
-            gg0[q] = (fourpi * f0) * b0[q];
-            gg1[q] = fourpi * (f0 * b1[q] + f1 * b0[q]);
-          }
-          double *pk = part + ((size_t)k * kHessVB + (v - vb)) * 9;
-          for (int bb = 0; bb < 3; ++bb)
+          const dcx z0 = f0 * a0, z1 = f0 * a1 + f1 * a0;
+          double S[kHessS];
+          S[1] = wmk * (z1 * Om).re;
+#pragma unroll
+          for (int bb = 0; bb < 3; ++bb) S[23 + bb] = wmk * (z0 * dOm[bb]).re;
+          if (full) {
+            const dcx z2 = f0 * a2 + (2.0 * f1) * a1 + f2 * a0;
+            S[0] = wmk * ((z2 - g[Lg.invr] * z1) * Om).re;
+#pragma unroll
+            for (int bb = 0; bb < 3; ++bb) S[2 + bb] = wmk * (z1 * dOm[bb]).re;
+            int e = 5;
+#pragma unroll
+            for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+              for (int bb = aa; bb < 3; ++bb) S[e++] = wmk * (z0 * d2Om[bb * 3 + aa]).re;
+#pragma unroll
             for (int aa = 0; aa < 3; ++aa) {
-              dcx tE = ((G.nh[aa] * G.nh[bb]) * (z2 - G.invr * z1)) * Om + z1 * (G.nh[aa] * dOm[bb] + G.nh[bb] * dOm[aa]) +
-                       z0 * d2Om[bb * 3 + aa];
-              if (aa == bb) tE = tE + G.invr * (z1 * Om);
-              const dcx tD = G.nh[bb] * (gg1[aa] * Om) + gg0[aa] * dOm[bb];
-              pk[bb * 3 + aa] = -wmk * (tE.re + tD.re);
+              const dcx gg0 = f0 * b0[aa], gg1 = f0 * b1[aa] + f1 * b0[aa];
+              S[11 + aa] = wmk * (gg1 * Om).re;
+#pragma unroll
+              for (int bb = 0; bb < 3; ++bb) S[14 + aa * 3 + bb] = wmk * (gg0 * dOm[bb]).re;
             }
+#pragma unroll
+            for (int e2 = 0; e2 < kHessS; ++e2)
+              for (int o = 16; o > 0; o >>= 1) S[e2] += __shfl_xor_sync(0xffffffffu, S[e2], o);
+            if (lane == 0)
+#pragma unroll
+              for (int e2 = 0; e2 < kHessS; ++e2) wsum[v * kHessS + e2] += S[e2];
+          } else {
+#pragma unroll
+            for (int e2 = 0; e2 < 4; ++e2) {
+              const int ix = e2 == 0 ? 1 : 22 + e2;
+              for (int o = 16; o > 0; o >>= 1) S[ix] += __shfl_xor_sync(0xffffffffu, S[ix], o);
+              if (lane == 0) wsum[v * kHessS + ix] += S[ix];
+            }
+          }
         }
-        __syncthreads();
-        // the sum over k, in k order
-        for (int t = tid; t < nvb * 9; t += kHessThreads) {
-          const int v = t / 9, e = t - v * 9;
-          double s = 0.0;
-          for (int k = 0; k < K; ++k) s = s + part[((size_t)k * kHessVB + v) * 9 + e];
-          hv[(vb + v) * 9 + e] = s;
-        }
-        __syncthreads();
       }
-      // dot products of the normalisation: t1 (3), t2 (3), c12 (9), then per v wp, u1 (3), u2 (3)
-      const int n_dots = 15 + 7 * n_vec;
-      for (int d = warp; d < n_dots; d += n_warps) {
-        double r;
-        if (d < 3) r = warp_dot(pvec, 1, h.dp1 + d, 3, ns);
-        else if (d < 6) r = warp_dot(pvec, 1, h.dp2 + (d - 3), 3, ns);
-        else if (d < 15) r = warp_dot(h.dp1 + (d - 6) % 3, 3, h.dp2 + (d - 6) / 3, 3, ns);  // c12[b * 3 + a]
-        else {
-          const int v = (d - 15) / 7, e = (d - 15) % 7;
-          const double *wv = vecs + ((size_t)site * n_vec + v) * ns;
-          if (e == 0) r = warp_dot(wv, 1, pvec, 1, ns);
-          else if (e < 4) r = warp_dot(wv, 1, h.dp1 + (e - 1), 3, ns);
-          else r = warp_dot(wv, 1, h.dp2 + (e - 4), 3, ns);
-        }
-        if (lane == 0) dots[d] = r;
-      }
-      __syncthreads();
-      for (int t = tid; t < 9 * n_vec; t += kHessThreads) {
+      __syncwarp();
+      // the normalisation (:1414-1484): t2 = p . dp_j, c12(b, a) = dp1(:, a) . dp_j(:, b),
+      // u2 = w . dp_j
+      const double invr = g[Lg.invr];
+      const double nh[3] = {g[Lg.nh], g[Lg.nh + 1], g[Lg.nh + 2]};
+      for (int t = lane; t < 9 * n_vec; t += 32) {
         const int v = t / 9, e = t - v * 9, bb = e / 3, aa = e - bb * 3;
-        const double *t1 = dots, *t2 = dots + 3, *c12 = dots + 6, *dv = dots + 15 + 7 * v;
-        const double wp = dv[0], *u1 = dv + 1, *u2 = dv + 4;
-        const double hval = hv[v * 9 + e] * invs - (u1[aa] * t2[bb] + u2[bb] * t1[aa]) * invs3 -
-                            wp * (c12[bb * 3 + aa] + hv[n_vec * 9 + e]) * invs3 + 3.0 * wp * t1[aa] * t2[bb] * invs5;
-        hess[((size_t)k2 * n_vec + v) * 9 + e] = hval;
-        hsum[t] += hval;
+        const double *t1 = sdot, *dv = sdot + 3 + 4 * v;
+        const double wp = dv[0], *u1 = dv + 1;
+        const double *Sp = wsum + n_vec * kHessS, *Sv = wsum + v * kHessS;
+        const double t2b = nh[bb] * Sp[1] + Sp[23 + bb], u2b = nh[bb] * Sv[1] + Sv[23 + bb];
+        const double *Sc = wsum + (n_vec + 1 + aa) * kHessS;
+        const double c12 = nh[bb] * Sc[1] + Sc[23 + bb];
+        const double hvv = hv_block(Sv, nh, invr, aa, bb), hvp = hv_block(Sp, nh, invr, aa, bb);
+        const double hval = hvv * invs - (u1[aa] * t2b + u2b * t1[aa]) * invs3 - wp * (c12 + hvp) * invs3 +
+                            3.0 * wp * t1[aa] * t2b * invs5;
+        hess[((size_t)j * n_vec + v) * 9 + e] = hval;
+        whs[t] += hval;
       }
-      __syncthreads();
+      __syncwarp();
     }
-    // the self pair: minus the sum of the others (:1488-1495); pairs outside
-    // every cutoff keep the zero blocks the launcher cleared
+    __syncthreads();
+    // the self pair: minus the sum of the others (:1488-1495), warps in order;
+    // pairs the Hessian skips keep the zero blocks the launcher cleared
     if (p1 > p0)
-      for (int t = tid; t < 9 * n_vec; t += kHessThreads) hess[((size_t)p0 * n_vec) * 9 + t] = -hsum[t];
+      for (int t = tid; t < 9 * n_vec; t += kHessThreads) {
+        double s = 0.0;
+        for (int w = 0; w < n_warps; ++w) s += sm[sd + (size_t)w * per_warp + kHessS * nva + 3 * N + t];
+        hess[((size_t)p0 * n_vec) * 9 + t] = -s;
+      }
   }
 }
 
 }  // namespace
 
+// Doubles per CTA, a multiple of 32 so that every CTA's region (and the
+// complex tables in it, read with 16-byte loads) starts on a 256-byte boundary.
 size_t hess_scratch_doubles(const DevParams &P, int n_vec) {
-  const size_t nk = (size_t)P.n_max * P.k_max, nv = (size_t)n_vec + 1;
-  return 2 * (3 * nk + nv * nk + 3 * nv * nk) + 6 * (size_t)P.n_soap + 3 * (size_t)P.n_kept + (size_t)P.n_kept + 8;
+  const size_t nk = (size_t)P.n_max * P.k_max;
+  const size_t n = 6 * nk + 2 * (size_t)(n_vec + 4) * nk + 6 * (size_t)(n_vec + 1) * nk + 3 * (size_t)P.n_soap +
+                   4 * (size_t)P.n_kept;
+  return (n + 31) / 32 * 32;
 }
 
+size_t hess_geo_doubles(const DevParams &P) { return (size_t)GeoLayout(P.l_max).size; }
+
 size_t hess_smem_bytes(const DevParams &P, int n_vec) {
-  const size_t N = P.n_max, K = P.k_max, L1 = P.l_max + 1, nv = (size_t)n_vec + 1;
-  return sizeof(double) * (P.n_soap + 4 * N * L1 + K * kHessVB * 9 + 9 * nv + 9 * (size_t)n_vec + 15 + 7 * (size_t)n_vec);
+  const size_t nw = kHessThreads / 32, sd = 3 + 4 * (size_t)n_vec;
+  const size_t pass_a = (size_t)kHessPC * (12 * (size_t)P.k_max + 2 * (size_t)P.n_max);
+  const size_t pass_b = nw * (kHessS * (size_t)(n_vec + 4) + 3 * (size_t)P.n_max + 9 * (size_t)n_vec);
+  return sizeof(double) * (sd + (sd & 1) + (pass_a > pass_b ? pass_a : pass_b));
 }
 
 int hess_grid(const DevParams &P, int n_vec) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k64_hess, kHessThreads, hess_smem_bytes(P, n_vec));
+  const size_t sm = hess_smem_bytes(P, n_vec);
+  if (cudaFuncSetAttribute(k64_hess, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess) return sms;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k64_hess, kHessThreads, sm);
   return sms * (per_sm > 0 ? per_sm : 1);
 }
 
 cudaError_t launch_hessian(const DevParams &P, const DevBatch &B, cudaStream_t s, const Fp64Work &w,
-                           const double *rad_der2, const double *soap, int n_vec, const double *vecs, double *hess,
-                           double *scratch, int grid, int *ticket, int *launches) {
+                           double *rad_der2, double *geo, int *good, const double *soap, int n_vec,
+                           const double *vecs, double *hess, double *scratch, int grid, int *ticket, int *launches) {
   CU_RET(cudaMemsetAsync(hess, 0, sizeof(double) * 9 * (size_t)n_vec * B.n_pairs, s));
   CU_RET(cudaMemsetAsync(ticket, 0, sizeof(int), s));
   if (B.n_pairs > 0) {
     const int blocks = (B.n_pairs + 127) / 128;
     int amax = 0;
     for (int sp = 0; sp < P.n_species; ++sp) amax = amax > P.rad[sp].alpha ? amax : P.rad[sp].alpha;
-    if (amax <= 8) k64_radial_d2<8><<<blocks, 128, 0, s>>>(P, B, (double *)rad_der2);
-    else k64_radial_d2<16><<<blocks, 128, 0, s>>>(P, B, (double *)rad_der2);
-    if (launches) *launches += 1;
+    if (amax <= 8) k64_radial_d2<8><<<blocks, 128, 0, s>>>(P, B, rad_der2);
+    else k64_radial_d2<16><<<blocks, 128, 0, s>>>(P, B, rad_der2);
+    k64_hgeo<<<blocks, 128, 0, s>>>(P, B, geo, good);
+    if (launches) *launches += 2;
   }
   if (B.n_sites > 0) {
     const size_t sm = hess_smem_bytes(P, n_vec);
-    cudaError_t e = cudaFuncSetAttribute(k64_hess, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
+    CU_RET(cudaFuncSetAttribute(k64_hess, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const int g = grid < B.n_sites ? grid : B.n_sites;
-    k64_hess<<<g, kHessThreads, sm, s>>>(P, B, w.rad, w.rad_der, rad_der2, (const double2 *)w.ang,
-                                        (const double2 *)w.cnk, w.norm, soap, n_vec, vecs, hess, scratch,
-                                        hess_scratch_doubles(P, n_vec), ticket);
+    k64_hess<<<g, kHessThreads, sm, s>>>(P, B, w.rad, w.rad_der, rad_der2, geo, good, (const double2 *)w.cnk,
+                                        w.norm, soap, n_vec, vecs, hess, scratch, hess_scratch_doubles(P, n_vec),
+                                        ticket);
     if (launches) *launches += 1;
   }
   return cudaGetLastError();

@@ -199,9 +199,9 @@ struct soapb_context {
   // arena
   DBuf off, bits, err, keep_c, keep_norm, rad, ang;
   DBuf f64_rad, f64_rad_der, f64_ang, f64_cnk, f64_soap_un, f64_norm;
-  // central-atom Hessian: second radial derivatives, per-CTA scratch, the
-  // descriptor it recomputes, its work counter
-  DBuf hs_rad_der2, hs_scratch, hs_soap, hs_ticket;
+  // central-atom Hessian: second radial derivatives, pair geometry records and
+  // flags, per-CTA scratch, the descriptor it recomputes, its work counter
+  DBuf hs_rad_der2, hs_geo, hs_good, hs_scratch, hs_soap, hs_ticket;
   // neighbour-list builder: cell list, counts and the batch it hands out
   DBuf nb_acell, nb_ccount, nb_cstart, nb_cfill, nb_catoms, nb_counts, nb_off, nb_state;
   DBuf nb_rjs, nb_th, nb_ph, nb_mask, nb_natom, nb_nneigh, nb_species, nb_smult;
@@ -230,7 +230,7 @@ struct soapb_context {
   ~soapb_context() {
     timing_release();
     for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &rad, &ang, &f64_rad, &f64_rad_der,
-                    &f64_ang, &f64_cnk, &f64_soap_un, &f64_norm, &hs_rad_der2, &hs_scratch, &hs_soap,
+                    &f64_ang, &f64_cnk, &f64_soap_un, &f64_norm, &hs_rad_der2, &hs_geo, &hs_good, &hs_scratch, &hs_soap,
                     &hs_ticket, &nb_acell, &nb_ccount, &nb_cstart,
                     &nb_cfill, &nb_catoms, &nb_counts, &nb_off, &nb_state, &nb_rjs, &nb_th, &nb_ph,
                     &nb_mask, &nb_natom, &nb_nneigh, &nb_species, &nb_smult})
@@ -972,6 +972,8 @@ int ctx_hessian(soapb_context *c, const soapb_batch *b, const double *d_soap, in
   if ((rc = c->f64_soap_un.ensure(8 * ns * c->n_soap))) return rc;
   if ((rc = c->f64_norm.ensure(8 * ns))) return rc;
   if ((rc = c->hs_rad_der2.ensure(8 * np * c->n_max))) return rc;
+  if ((rc = c->hs_geo.ensure(8 * np * hess_geo_doubles(P)))) return rc;
+  if ((rc = c->hs_good.ensure(4 * np))) return rc;
   if ((rc = c->hs_soap.ensure(8 * ns * c->n_soap))) return rc;
   if ((rc = c->hs_ticket.ensure(16))) return rc;
   const int grid = std::max(1, std::min(hess_grid(P, n_vec), b->n_sites));
@@ -980,8 +982,9 @@ int ctx_hessian(soapb_context *c, const soapb_batch *b, const double *d_soap, in
              c->f64_cnk.as<double>(), c->f64_soap_un.as<double>(), c->f64_norm.as<double>()};
   int nl = 0;
   CU(launch_fp64_descriptor(P, B, c->stream, w, 1, c->hs_soap.as<double>(), nullptr, &nl));
-  CU(launch_hessian(P, B, c->stream, w, c->hs_rad_der2.as<double>(), d_soap ? d_soap : c->hs_soap.as<double>(),
-                    n_vec, d_vecs, d_hess, c->hs_scratch.as<double>(), grid, c->hs_ticket.as<int>(), &nl));
+  CU(launch_hessian(P, B, c->stream, w, c->hs_rad_der2.as<double>(), c->hs_geo.as<double>(), c->hs_good.as<int>(),
+                    d_soap ? d_soap : c->hs_soap.as<double>(), n_vec, d_vecs, d_hess, c->hs_scratch.as<double>(),
+                    grid, c->hs_ticket.as<int>(), &nl));
   c->launches += nl;
   return SOAPB_OK;
 }

@@ -199,11 +199,13 @@ cudaError_t launch_fp64_contract(const DevParams &P, const DevBatch &B, cudaStre
                                  double *pair, int *launches);
 // Central-atom Hessian (soapb_hessian.cu), on the state launch_fp64_descriptor
 // left with do_der: second radial derivatives into rad_der2 (n_pairs, n_max),
-// then hess (n_pairs, n_vec, 3, 3) = 9 n_vec doubles per pair, cleared first.
-// scratch: grid * hess_scratch_doubles doubles; ticket: one int.
+// per-pair geometry records into geo (n_pairs * hess_geo_doubles) and good
+// (n_pairs ints), then hess (n_pairs, n_vec, 3, 3) = 9 n_vec doubles per pair,
+// cleared first.  scratch: grid * hess_scratch_doubles doubles; ticket: one int.
 size_t hess_scratch_doubles(const DevParams &P, int n_vec);
+size_t hess_geo_doubles(const DevParams &P);
 int hess_grid(const DevParams &P, int n_vec);
 cudaError_t launch_hessian(const DevParams &P, const DevBatch &B, cudaStream_t s, const Fp64Work &w,
-                           const double *rad_der2, const double *soap, int n_vec, const double *vecs, double *hess,
-                           double *scratch, int grid, int *ticket, int *launches);
+                           double *rad_der2, double *geo, int *good, const double *soap, int n_vec,
+                           const double *vecs, double *hess, double *scratch, int grid, int *ticket, int *launches);
 }  // namespace soapb
