@@ -47,7 +47,8 @@ enum {
                                     contract (src/soap_turbo.f90:1744-1747)             */
   SOAPB_ERR_COMPRESS_MODE = 4,   /* compress_mode not understood
                                     (src/soap_turbo_compress.f90:305-306)               */
-  SOAPB_ERR_BASIS = 5,           /* basis other than poly3 / poly3gauss                  */
+  SOAPB_ERR_BASIS = 5,           /* basis other than poly3 / poly3gauss / poly3operator,
+                                    or the Hessian asked of poly3operator                */
   SOAPB_ERR_CUDA = 6,            /* CUDA runtime failure                                 */
   SOAPB_ERR_NO_DEVICE = 7,       /* no usable sm_100 device                              */
   SOAPB_ERR_INPUT = 8,           /* non-finite or negative distance, bad CSR, bad mask   */
@@ -56,7 +57,10 @@ enum {
                                     (src/soap_turbo.f90:1206-1227)                       */
 };
 
-enum { SOAPB_BASIS_POLY3 = 0, SOAPB_BASIS_POLY3GAUSS = 1 };
+/* poly3operator (src/soap_turbo_radial.f90:1549-2141): poly3's W with a
+ * piecewise-cubic atom density in place of the Gaussian; alpha_max 1..11; no
+ * second radial derivatives (no central-atom Hessian). */
+enum { SOAPB_BASIS_POLY3 = 0, SOAPB_BASIS_POLY3GAUSS = 1, SOAPB_BASIS_POLY3OPERATOR = 2 };
 enum { SOAPB_SCALING_POLYNOMIAL = 0, SOAPB_SCALING_NONE = 1 };
 /* Arithmetic of the descriptor + VJP path. */
 enum {
@@ -79,7 +83,9 @@ const char *soapb_version(void);
 /* get_soap (src/soap_turbo.f90:139-169).  Same arguments in the same order,
  * as plain pointers plus the extents Fortran would carry in the descriptors:
  * max_species_multiplicity = size(species,1), n_soap = size(soap,1).
- * basis: "poly3" | "poly3gauss"; scaling_mode: "polynomial" | other.
+ * basis: "poly3" | "poly3gauss" | "poly3operator"; scaling_mode: "polynomial" | other
+ * (poly3operator with another scaling mode: amplitude 1, which the reference
+ * leaves unset).
  * soap is overwritten (the reference accumulates into it when compressing,
  * so its callers pass it zeroed; the results then agree).
  * do_derivatives && !contract: soap_cart_der (3, n_soap, n_atom_pairs) is

@@ -97,7 +97,7 @@ def num_threads() -> int:
 # ---------------------------------------------------------------- basis
 def overlap(basis: str, alpha: int, sigma: float = 0.5, rcut: float = 5.0) -> np.ndarray:
     S = np.zeros((alpha, alpha), order="F")
-    if basis == "poly3":
+    if basis in ("poly3", "poly3operator"):  # poly3operator uses poly3's W (src/soap_turbo.f90:380-381)
         lib().or_overlap_poly3(alpha, _p(S, _f64p))
     else:
         lib().or_overlap_poly3gauss(alpha, sigma, rcut, _p(S, _f64p))
@@ -157,6 +157,9 @@ def preflm(lmax):
     return out
 
 
+BASIS_CODE = {"poly3": 0, "poly3gauss": 1, "poly3operator": 2}
+
+
 def radial_eval(hyper, species: int, W_block, r, legacy_seed=True, is_central=False, der2=False):
     """The radial expansion of one species at distances r: (values, r-derivatives)
     and, with der2 (unified seed only), the second r-derivatives as well."""
@@ -167,7 +170,7 @@ def radial_eval(hyper, species: int, W_block, r, legacy_seed=True, is_central=Fa
     d2 = np.zeros((r.shape[0], a)) if der2 else None
     Wb = np.asfortranarray(W_block, dtype=np.float64)
     rc = lib().or_radial_eval(
-        1 if hyper.basis == "poly3gauss" else 0, a, hyper.arr("rcut_soft")[species],
+        BASIS_CODE[hyper.basis], a, hyper.arr("rcut_soft")[species],
         hyper.arr("rcut_hard")[species], hyper.arr("atom_sigma_r")[species],
         hyper.arr("atom_sigma_r_scaling")[species], hyper.arr("amplitude_scaling")[species],
         hyper.arr("nf")[species], _p(Wb, _f64p), 1 if hyper.scaling_mode == "polynomial" else 0,
@@ -175,7 +178,8 @@ def radial_eval(hyper, species: int, W_block, r, legacy_seed=True, is_central=Fa
         int(legacy_seed), r.shape[0], _p(r, _f64p), _p(out, _f64p), _p(der, _f64p),
         _p(d2, _f64p) if der2 else None)
     if rc:
-        raise ValueError("second radial derivatives need the unified filter seed")
+        raise ValueError("second radial derivatives need the unified filter seed (and poly3 or "
+                         "poly3gauss)")
     return (out, der, d2) if der2 else (out, der)
 
 
@@ -325,7 +329,7 @@ def get_soap(hyper, nl, W, S, do_derivatives=True, cart_der=False, legacy_filter
     a.max_mult = arrays["species"].shape[1]
     a.l_max = hyper.l_max
     a.radial_enhancement = hyper.radial_enhancement
-    a.basis = 1 if hyper.basis == "poly3gauss" else 0
+    a.basis = BASIS_CODE[hyper.basis]
     a.scaling_poly = 1 if hyper.scaling_mode == "polynomial" else 0
     a.legacy_filter_seed = int(legacy_filter_seed)
     for name in ("n_neigh", "species", "species_multiplicity", "alpha_max"):

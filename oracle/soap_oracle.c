@@ -47,7 +47,7 @@
 /* ------------------------------------------------------------------------ */
 typedef struct {
   int n_sites, n_species, n_pairs, max_mult, l_max, radial_enhancement;
-  int basis;            /* 0 = poly3, 1 = poly3gauss */
+  int basis;            /* 0 = poly3, 1 = poly3gauss, 2 = poly3operator */
   int scaling_poly;     /* 1 when scaling_mode == "polynomial" */
   int legacy_filter_seed;
   const int *n_neigh, *species, *species_multiplicity;
@@ -594,6 +594,215 @@ static void or_radial_pair(const or_radial_setup *s, double rj_in, int is_centra
 }
 
 /* ------------------------------------------------------------------------ */
+/* poly3operator radial expansion, one pair                                  */
+/* (get_radial_expansion_coefficients_poly3operator,                        */
+/*  src/soap_turbo_radial.f90:1549-2141, and its helpers :2154-2557).       */
+/* The atom density is the piecewise cubic g(x) = 1 - 3x^2 -+ 2x^3 on       */
+/* x = (r - r_j)/w in [-1, 0] (left) and [0, 1] (right), w = 2 sqrt(2 ln 2) */
+/* sigma(r_j); on [r_soft, r_hard] it is multiplied by the filter, the      */
+/* right piece centred at r_soft with width 2 sqrt(2 ln 2)(r_hard - r_soft). */
+/* The overlaps with (1 - r)^(n+2)/N_n (r_hard = 1 after scaling) are taken */
+/* in closed form by repeated integration by parts, as the reference does. */
+/* ------------------------------------------------------------------------ */
+
+/* g_aux / g_aux_array (:2154-2217): value, first derivative, half the second,
+ * a sixth of the third of the piece at r (the Taylor coefficients about r). */
+static void op_gaux(double r, double r0, double w, int right, double *poly) {
+  const double x = (r - r0) / w, iw = 1.0 / w;
+  if (!right) {
+    poly[0] = 1.0 - 3.0 * x * x - 2.0 * x * x * x;
+    poly[1] = -6.0 * (x * x + x) * iw;
+    poly[2] = -3.0 * (2.0 * x + 1.0) * iw * iw;
+    poly[3] = -2.0 * iw * iw * iw;
+  } else {
+    poly[0] = 1.0 - 3.0 * x * x + 2.0 * x * x * x;
+    poly[1] = 6.0 * (x * x - x) * iw;
+    poly[2] = 3.0 * (2.0 * x - 1.0) * iw * iw;
+    poly[3] = 2.0 * iw * iw * iw;
+  }
+}
+
+/* g_aux_der_array (:2227-2267): the same four, differentiated with respect to
+ * r0 where w = w0 + ws r0. */
+static void op_gaux_der(double r, double r0, double w, double ws, int right, double *poly) {
+  const double x = (r - r0) / w, iw = 1.0 / w, iw2 = iw * iw, iw3 = iw2 * iw, iw4 = iw3 * iw;
+  if (!right) {
+    poly[0] = 6.0 * (x + (ws + 1.0) * x * x + ws * x * x * x) * iw;
+    poly[1] = 6.0 * (1.0 + 2.0 * (ws + 1.0) * x + 3.0 * ws * x * x) * iw2;
+    poly[2] = 6.0 * (ws + 1.0 + 3.0 * ws * x) * iw3;
+    poly[3] = 6.0 * ws * iw4;
+  } else {
+    poly[0] = 6.0 * (x + (ws - 1.0) * x * x - ws * x * x * x) * iw;
+    poly[1] = 6.0 * (1.0 + 2.0 * (ws - 1.0) * x - 3.0 * ws * x * x) * iw2;
+    poly[2] = 6.0 * (ws - 1.0 - 3.0 * ws * x) * iw3;
+    poly[3] = -6.0 * ws * iw4;
+  }
+}
+
+/* get_constant_poly_coeff (:2276-2297) with r_hard = 1: A(n, j), j = 1..7 */
+static void op_coeff_A(int alpha, double *A) {
+  for (int n = 1; n <= alpha; n++) {
+    const double Na = sqrt(1.0 / (double)(2 * n + 5));                  /* N_a, :82-96 */
+    A[(n - 1) * 7 + 0] = 1.0 / Na / (double)(n + 3);
+    for (int j = 2; j <= 7; j++) A[(n - 1) * 7 + j - 1] = A[(n - 1) * 7 + j - 2] / (double)(n + 3 + j - 1);
+  }
+}
+
+/* Soft-zone overlap of one piece between limits lo and hi (:1770-1797): the
+ * four integration-by-parts terms at each limit, upper minus lower.
+ * g4(lim) supplies the piece's four coefficients at a limit. */
+static void op_soft_piece(int alpha, const double *A, double lo, double hi, const double *g_lo,
+                          const double *g_hi, double *Ov) {
+  static const double vect[4] = {-1.0, -1.0, -2.0, -6.0};
+  double Ml[4], Mh[4], pl[32], ph[32];
+  pl[0] = ph[0] = 1.0;
+  for (int j = 1; j < alpha + 4; j++) { pl[j] = pl[j - 1] * (1.0 - lo); ph[j] = ph[j - 1] * (1.0 - hi); }
+  for (int j = 0; j < 4; j++) { Ml[j] = pl[j] * g_lo[j] * vect[j]; Mh[j] = ph[j] * g_hi[j] * vect[j]; }
+  for (int n = 1; n <= alpha; n++) {
+    double sh = 0.0, sl = 0.0;
+    for (int j = 0; j < 4; j++) { sh += Mh[j] * A[(n - 1) * 7 + j]; sl += Ml[j] * A[(n - 1) * 7 + j]; }
+    Ov[n - 1] = sh * ph[n + 3] - sl * pl[n + 3];
+  }
+}
+
+/* get_constant_poly_filter_coeff_array (:2307-2344): the monomial coefficients
+ * of (atom piece) x (filter), degree 6.  col: the piece's Taylor coefficients
+ * about r = 0; C: the filter's. */
+static void op_product(const double *col, const double *C, double *B) {
+  for (int m = 0; m < 7; m++) B[m] = 0.0;
+  for (int i = 0; i < 4; i++)
+    for (int q = 0; q < 4; q++) B[i + q] += col[q] * C[i];
+}
+
+/* Buffer-zone overlap of one piece between lo and hi (:1995-2021): seven
+ * integration-by-parts terms, -P^(d-1)(lim) (1 - lim)^(d-1) (M_radial_monomial,
+ * :2481-2500), times A(n, d) (1 - lim)^(n+3). */
+static void op_buffer_piece(int alpha, const double *A, double lo, double hi, const double *B, double *Ov) {
+  double Ml[7], Mh[7], pl[32], ph[32];
+  const int top = alpha + 4 > 7 ? alpha + 4 : 7;
+  pl[0] = ph[0] = 1.0;
+  for (int j = 1; j < top; j++) { pl[j] = pl[j - 1] * (1.0 - lo); ph[j] = ph[j - 1] * (1.0 - hi); }
+  for (int d = 1; d <= 7; d++) {
+    double vl = 0.0, vh = 0.0;
+    for (int q = d; q <= 7; q++) {
+      double f = 1.0;
+      for (int t = q - d + 1; t <= q - 1; t++) f *= (double)t;               /* (q-1)!/(q-d)! */
+      vl += B[q - 1] * f * pow(lo, q - d);
+      vh += B[q - 1] * f * pow(hi, q - d);
+    }
+    Ml[d - 1] = -vl * pl[d - 1];
+    Mh[d - 1] = -vh * ph[d - 1];
+  }
+  for (int n = 1; n <= alpha; n++) {
+    double sh = 0.0, sl = 0.0;
+    for (int d = 0; d < 7; d++) { sh += Mh[d] * A[(n - 1) * 7 + d]; sl += Ml[d] * A[(n - 1) * 7 + d]; }
+    Ov[n - 1] = sh * ph[n + 3] - sl * pl[n + 3];
+  }
+}
+
+/* The amplitude of the poly3operator expansion (:1699-1757): its value and
+ * r-derivative (scaled units), with the central weight and the radial
+ * enhancement.  Not polynomial scaling: the reference leaves it unset; 1 here. */
+static void op_amplitude(double rj, double sig, double sig_c, double amp_scaling, int scaling_poly,
+                         int radial_enhancement, int is_central, double cw, double *amp, double *ampd) {
+  const double pi = acos(-1.0);
+  double a = 1.0, ad = 0.0;
+  if (scaling_poly) {
+    if (amp_scaling == 0.0) {
+      a = 1.0 / sig;
+      ad = -sig_c / (sig * sig);
+    } else if (amp_scaling == 1.0) {
+      a = 1.0 / sig * (1.0 + 2.0 * rj * rj * rj - 3.0 * rj * rj);
+      ad = 6.0 / sig * (rj * rj - rj) - sig_c / sig * a;
+    } else {
+      const double h = 1.0 + 2.0 * rj * rj * rj - 3.0 * rj * rj;
+      a = 1.0 / sig * pow(h, amp_scaling);
+      ad = 6.0 * amp_scaling / sig * (rj * rj - rj) * pow(h, amp_scaling - 1.0) - sig_c / sig * a;
+    }
+  }
+  if (is_central) { a *= cw; ad *= cw; }
+  if (radial_enhancement == 1) {
+    ad = a * (1.0 + sqrt(2.0 / pi) * sig_c) + ad * (rj + sqrt(2.0 / pi) * sig);
+    a = a * (rj + sqrt(2.0 / pi) * sig);
+  } else if (radial_enhancement == 2) {
+    ad = a * (2.0 * rj + 2.0 * sig * sig_c + sqrt(8.0 / pi) * sig + sqrt(8.0 / pi) * rj * sig_c) +
+         ad * (rj * rj + sig * sig + sqrt(8.0 / pi) * sig * rj);
+    a = a * (rj * rj + sig * sig + sqrt(8.0 / pi) * sig * rj);
+  }
+  *amp = a;
+  *ampd = ad;
+}
+
+/* One masked pair: out[alpha] (and der[alpha] when der != NULL), W-transformed
+ * and scaled to the unscaled radius (:2097-2117); global_scaling not applied.
+ * rj_in unscaled.  A pair is in the soft zone when r - w < r_soft and in the
+ * buffer zone when r_soft < r_hard and r + w > r_soft (:1637-1645, 1858-1872);
+ * there is no r_hard cut of its own. */
+static void or_radial_op_pair(int alpha, double rcut_soft_in, double rcut_hard_in, double sigma_in,
+                              double sigma_scaling, double amp_scaling, int scaling_poly, int radial_enhancement,
+                              double central_weight, int is_central, const double *W, int ldw, double rj_in,
+                              double *out, double *der) {
+  const double c_w = 2.0 * sqrt(2.0 * log(2.0));
+  const double rs = rcut_soft_in / rcut_hard_in, sig0 = sigma_in / rcut_hard_in;
+  const double filter_width = c_w * (1.0 - rs);
+  const double w_in = c_w * (sigma_in + sigma_scaling * rj_in);
+  double A[16 * 7], e[16], ed[16], Ov[16], Ov_d[16];
+  op_coeff_A(alpha, A);
+  for (int n = 0; n < alpha; n++) { e[n] = 0.0; ed[n] = 0.0; }
+  const double rj = rj_in / rcut_hard_in, sig = sig0 + sigma_scaling * rj, w = c_w * sig;
+  const double ws = c_w * sigma_scaling;
+  double amp, ampd;
+  op_amplitude(rj, sig, sigma_scaling, amp_scaling, scaling_poly, radial_enhancement, is_central, central_weight,
+               &amp, &ampd);
+  if (rj_in - w_in < rcut_soft_in) {                                     /* soft zone, :1770-1846 */
+    const double l1 = fmax(0.0, rj - w), l2 = fmin(rj, rs), l3 = fmin(rs, rj + w);
+    double g1[4], g2[4], g3[4], h2[4], tmp[16];
+    op_gaux(l1, rj, w, 0, g1); op_gaux(l2, rj, w, 0, g2);
+    op_gaux(l2, rj, w, 1, h2); op_gaux(l3, rj, w, 1, g3);
+    op_soft_piece(alpha, A, l1, l2, g1, g2, Ov);
+    op_soft_piece(alpha, A, l2, l3, h2, g3, tmp);
+    for (int n = 0; n < alpha; n++) { Ov[n] += tmp[n]; e[n] = amp * Ov[n]; }
+    if (der) {
+      op_gaux_der(l1, rj, w, ws, 0, g1); op_gaux_der(l2, rj, w, ws, 0, g2);
+      op_gaux_der(l2, rj, w, ws, 1, h2); op_gaux_der(l3, rj, w, ws, 1, g3);
+      op_soft_piece(alpha, A, l1, l2, g1, g2, Ov_d);
+      op_soft_piece(alpha, A, l2, l3, h2, g3, tmp);
+      for (int n = 0; n < alpha; n++) ed[n] = amp * (Ov_d[n] + tmp[n]) + ampd * Ov[n];
+    }
+  }
+  if (rcut_soft_in < rcut_hard_in && rj_in + w_in > rcut_soft_in) {     /* buffer zone, :1858-2075 */
+    const double l1 = fmax(rs, rj - w), l2 = fmax(rj, rs), l3 = fmin(1.0, rj + w);
+    double C[4], col[4], B[7], tmp[16];
+    op_gaux(0.0, rs, filter_width, 1, C);
+    op_gaux(-rj, 0.0, w, 0, col);
+    op_product(col, C, B);
+    op_buffer_piece(alpha, A, l1, l2, B, Ov);
+    op_gaux(-rj, 0.0, w, 1, col);
+    op_product(col, C, B);
+    op_buffer_piece(alpha, A, l2, l3, B, tmp);
+    for (int n = 0; n < alpha; n++) { Ov[n] += tmp[n]; e[n] += amp * Ov[n]; }
+    if (der) {
+      op_gaux_der(-rj, 0.0, w, ws, 0, col);
+      op_product(col, C, B);
+      op_buffer_piece(alpha, A, l1, l2, B, Ov_d);
+      op_gaux_der(-rj, 0.0, w, ws, 1, col);
+      op_product(col, C, B);
+      op_buffer_piece(alpha, A, l2, l3, B, tmp);
+      for (int n = 0; n < alpha; n++) ed[n] += amp * (Ov_d[n] + tmp[n]) + ampd * Ov[n];
+    }
+  }
+  for (int n = 1; n <= alpha; n++) {                                      /* :2097-2100, 2113-2117 */
+    double v = 0.0, d = 0.0;
+    for (int m = 1; m <= alpha; m++) {
+      v += W[(m - 1) * ldw + (n - 1)] * e[m - 1];
+      d += W[(m - 1) * ldw + (n - 1)] * ed[m - 1];
+    }
+    out[n - 1] = v * sqrt(rcut_hard_in);
+    if (der) der[n - 1] = d / sqrt(rcut_hard_in);
+  }
+}
+
+/* ------------------------------------------------------------------------ */
 /* Per-call state shared by get_soap and soap_contract                       */
 /* ------------------------------------------------------------------------ */
 typedef struct {
@@ -650,6 +859,7 @@ int or_get_soap2(const or_args *a, int do_derivatives, int do_der2, double *soap
   const int n_soap_unc = n_max * (n_max + 1) / 2 * (l_max + 1);      /* :396 */
   const int need_der = do_derivatives;
   if (do_der2 && (!do_derivatives || a->legacy_filter_seed)) return -2;
+  if (do_der2 && a->basis == 2) return -3;  /* no second derivatives for poly3operator, :485-489 */
 
   or_ctx *c = (or_ctx *)calloc(1, sizeof(or_ctx));
   c->n_sites = n_sites; c->n_pairs = n_pairs; c->n_max = n_max; c->k_max = k_max; c->l_max = l_max;
@@ -675,8 +885,9 @@ int or_get_soap2(const or_args *a, int do_derivatives, int do_der2, double *soap
   /* ---- radial, per species (:491-544 -> src/soap_turbo_radial.f90:281-384) */
   for (int sp = 0; sp < a->n_species; sp++) {
     int alpha = a->alpha_max[sp];
-    int with_gauss = a->basis == 1;
+    int with_gauss = a->basis == 1, op = a->basis == 2;
     int do_central = with_gauss ? 0 : (a->central_weight[sp] != 0.0);  /* :238-245; :232-238 */
+    if (op) do_central = 1;                                              /* src/soap_turbo.f90:539 */
     or_radial_setup st;
     or_radial_init(&st, alpha, a->rcut_soft[sp], a->rcut_hard[sp], a->atom_sigma_r[sp],
                    a->atom_sigma_r_scaling[sp], a->amplitude_scaling[sp], a->nf[sp],
@@ -694,10 +905,16 @@ int or_get_soap2(const or_args *a, int do_derivatives, int do_der2, double *soap
         double *der2 = do_der2 ? c->rad_der2 + (size_t)k * n_max + i_beg[sp] : NULL;
         for (int n = 0; n < alpha; n++) { out[n] = 0.0; der[n] = 0.0; if (der2) der2[n] = 0.0; } /* :328-340 */
         if (j == 0 && !do_central) continue;                               /* :342-355 */
-        if (a->rjs[k] >= a->rcut_hard[sp]) continue;
+        if (!op && a->rjs[k] >= a->rcut_hard[sp]) continue;
         if (!a->mask[(size_t)sp * n_pairs + k]) continue;
         double o[32], d[32], d2[32];
-        or_radial_pair(&st, a->rjs[k], j == 0, o, d, der2 ? d2 : NULL);
+        if (op)
+          or_radial_op_pair(alpha, a->rcut_soft[sp], a->rcut_hard[sp], a->atom_sigma_r[sp],
+                            a->atom_sigma_r_scaling[sp], a->amplitude_scaling[sp], a->scaling_poly,
+                            a->radial_enhancement, a->central_weight[sp], j == 0,
+                            a->W + (size_t)i_beg[sp] * n_max + i_beg[sp], n_max, a->rjs[k], o, d);
+        else
+          or_radial_pair(&st, a->rjs[k], j == 0, o, d, der2 ? d2 : NULL);
         for (int n = 0; n < alpha; n++) {
           out[n] = o[n] * gsc;                                             /* :510-511, :532-533 */
           if (need_der) der[n] = d[n] * gsc;
@@ -1462,6 +1679,14 @@ int or_radial_eval(int basis, int alpha, double rcut_soft, double rcut_hard, dou
   or_radial_setup st;
   int with_gauss = basis == 1;
   int do_central = with_gauss ? 0 : (central_weight != 0.0);
+  if (basis == 2) {
+    if (der2) return -1;
+    for (int t = 0; t < n; t++)
+      or_radial_op_pair(alpha, rcut_soft, rcut_hard, sigma, sigma_scaling, amp_scaling, scaling_poly,
+                        radial_enhancement, central_weight, is_central, W, alpha, r[t], out + (size_t)t * alpha,
+                        der + (size_t)t * alpha);
+    return 0;
+  }
   or_radial_init(&st, alpha, rcut_soft, rcut_hard, sigma, sigma_scaling, amp_scaling, nf, W, alpha,
                  scaling_poly, radial_enhancement, 1, do_central, central_weight, with_gauss, legacy_seed);
   if (der2 && or_radial_enable_der2(&st)) return -1;  /* second derivatives need the unified seed */

@@ -24,7 +24,7 @@ ERRORS = {
     7: "SOAPB_ERR_NO_DEVICE", 8: "SOAPB_ERR_INPUT", 9: "SOAPB_ERR_BASIS_MATRIX",
     10: "SOAPB_ERR_HESSIAN_STATE",
 }
-BASIS = {"poly3": 0, "poly3gauss": 1}
+BASIS = {"poly3": 0, "poly3gauss": 1, "poly3operator": 2}
 PREC_MIXED, PREC_FP64 = 0, 1
 G_SITE_FASTEST, G_SOAP_FASTEST = 0, 1
 

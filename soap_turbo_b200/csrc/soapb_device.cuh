@@ -25,11 +25,213 @@ namespace soapb {
 // Recursion table index for alpha index n (n >= -4).
 #define SOAPB_TI(n) ((n) + 4)
 
+// ---------------------------------------------------------------- poly3operator
+// The poly3operator radial expansion of one (pair, species) entry
+// (get_radial_expansion_coefficients_poly3operator, src/soap_turbo_radial.f90:
+// 1549-2141, helpers :2154-2557), in FP64.  The atom density is the piecewise
+// cubic g(x) = 1 - 3x^2 -+ 2x^3 of x = (r - r_j)/w on [-1, 0] and [0, 1],
+// w = 2 sqrt(2 ln 2) sigma(r_j); on [r_soft, r_hard] it is multiplied by the
+// filter, the right piece centred at r_soft with width 2 sqrt(2 ln 2)(r_hard -
+// r_soft).  Its overlaps with (1 - r)^(n+2) sqrt(2n + 5) (r_hard = 1 after
+// scaling) are closed forms by repeated integration by parts: for a piece P
+// of degree d between lo and hi,
+//   I_n = sum_{j=1..d+1} A(n, j) [-(1 - r)^(n+2+j) P^(j-1)(r)]_lo^hi,
+//   A(n, 1) = sqrt(2n + 5)/(n + 3), A(n, j) = A(n, j-1)/(n + 2 + j).
+// The derivative differentiates the density in r_j (with w growing with r_j);
+// the moving limits add nothing (g vanishes at x = -1, 1 and is continuous at 0).
+
+// Taylor coefficients about r of a piece (value, slope, half the curvature, a
+// sixth of the third derivative) and their r0-derivatives (g_aux, g_aux_der_array)
+__device__ __forceinline__ void op_piece(double r, double r0, double w, bool right, double *c) {
+  const double x = (r - r0) / w, iw = 1.0 / w;
+  const double sg = right ? 1.0 : -1.0;
+  c[0] = 1.0 - 3.0 * x * x + sg * 2.0 * x * x * x;
+  c[1] = 6.0 * (sg * x * x - x) * iw;
+  c[2] = 3.0 * (sg * 2.0 * x - 1.0) * iw * iw;
+  c[3] = sg * 2.0 * iw * iw * iw;
+}
+__device__ __forceinline__ void op_piece_d(double r, double r0, double w, double ws, bool right, double *c) {
+  const double x = (r - r0) / w, iw = 1.0 / w, iw2 = iw * iw;
+  const double sg = right ? 1.0 : -1.0;  // right: (ws - 1), left: (ws + 1)
+  c[0] = 6.0 * (x + (ws - sg) * x * x - sg * ws * x * x * x) * iw;
+  c[1] = 6.0 * (1.0 + 2.0 * (ws - sg) * x - 3.0 * sg * ws * x * x) * iw2;
+  c[2] = 6.0 * (ws - sg - 3.0 * sg * ws * x) * iw2 * iw;
+  c[3] = -sg * 6.0 * ws * iw2 * iw2;
+}
+
+// Adds I_n of one piece, given -P^(j-1)(lim)(1 - lim)^(j-1) at both limits
+// (ml, mh, nj terms), scaled by f, to acc[n].
 template <int AMAX>
+__device__ __forceinline__ void op_accumulate(int a, double lo, double hi, const double *ml, const double *mh,
+                                              int nj, double f, double (&acc)[AMAX]) {
+  double pl = (1.0 - lo) * (1.0 - lo), ph = (1.0 - hi) * (1.0 - hi);
+  pl = pl * pl;  // (1 - lim)^(n + 3) at n = 1
+  ph = ph * ph;
+#pragma unroll
+  for (int i = 0; i < AMAX; ++i) {
+    if (i < a) {
+      const int n = i + 1;
+      double An = sqrt((double)(2 * n + 5)) / (double)(n + 3);
+      double sh = 0.0, sl = 0.0;
+      for (int j = 0; j < nj; ++j) {
+        if (j > 0) An = An / (double)(n + 3 + j);
+        sh += mh[j] * An;
+        sl += ml[j] * An;
+      }
+      acc[i] += f * (sh * ph - sl * pl);
+      pl *= (1.0 - lo);
+      ph *= (1.0 - hi);
+    }
+  }
+}
+
+// Soft zone: a cubic piece given by its Taylor coefficients at the two limits
+// (the table's -1, -1, -2, -6 factors turn them into derivatives with the sign).
+__device__ __forceinline__ void op_soft_terms(double lim, const double *c, double *m) {
+  const double q = 1.0 - lim;
+  m[0] = -c[0];
+  m[1] = -c[1] * q;
+  m[2] = -2.0 * c[2] * q * q;
+  m[3] = -6.0 * c[3] * q * q * q;
+}
+
+// Buffer zone: B = (piece) x (filter) as monomials about r = 0, degree 6; m[d] =
+// -B^(d)(lim) (1 - lim)^d for d = 0..6.
+__device__ __forceinline__ void op_buffer_terms(double lim, const double *B, double *m) {
+  const double q = 1.0 - lim;
+  double qd = 1.0;
+  for (int d = 0; d < 7; ++d) {
+    double v = 0.0;
+    for (int p = 6; p >= d; --p) {  // Horner on the d-th derivative
+      double f = 1.0;
+      for (int t = p - d + 1; t <= p; ++t) f *= (double)t;
+      v = v * lim + B[p] * f;
+    }
+    m[d] = -v * qd;
+    qd *= q;
+  }
+}
+
+__device__ __forceinline__ void op_product(const double *col, const double *C, double *B) {
+  for (int m = 0; m < 7; ++m) B[m] = 0.0;
+  for (int i = 0; i < 4; ++i)
+    for (int q = 0; q < 4; ++q) B[i + q] += col[q] * C[i];
+}
+
+template <int AMAX>
+__device__ __forceinline__ void radial_entry_op(const DevParams &P, const RadSp &S, const double *__restrict__ W,
+                                                double r_in, bool is_central, bool do_der, double (&val)[AMAX],
+                                                double (&der)[AMAX]) {
+  const double c_w = 2.3548200450309493820;  // 2 sqrt(2 ln 2)
+  const double sq2pi = 0.79788456080286535588, sq8pi = 1.5957691216057307118;
+  const int a = S.alpha;
+  const double rs = S.rs, c = S.c;
+  const double rj = r_in * S.inv_rcut, sig = S.atom_sigma + c * rj, w = c_w * sig, ws = c_w * c;
+  const double filter_width = c_w * (1.0 - rs);
+  double e[AMAX], ed[AMAX];
+#pragma unroll
+  for (int i = 0; i < AMAX; ++i) {
+    e[i] = 0.0;
+    ed[i] = 0.0;
+  }
+  // amplitude (:1699-1757); not polynomial scaling: 1 (the reference leaves it unset)
+  double amp = 1.0, ampd = 0.0;
+  if (P.scaling_poly) {
+    if (S.amp_scaling == 0.0) {
+      amp = 1.0 / sig;
+      ampd = -c / (sig * sig);
+    } else if (S.amp_scaling == 1.0) {
+      amp = 1.0 / sig * (1.0 + 2.0 * rj * rj * rj - 3.0 * rj * rj);
+      ampd = 6.0 / sig * (rj * rj - rj) - c / sig * amp;
+    } else {
+      const double h = 1.0 + 2.0 * rj * rj * rj - 3.0 * rj * rj;
+      amp = 1.0 / sig * pow(h, S.amp_scaling);
+      ampd = 6.0 * S.amp_scaling / sig * (rj * rj - rj) * pow(h, S.amp_scaling - 1.0) - c / sig * amp;
+    }
+  }
+  if (is_central) {
+    amp *= S.cw;
+    ampd *= S.cw;
+  }
+  if (P.radial_enh == 1) {
+    ampd = amp * (1.0 + sq2pi * c) + ampd * (rj + sq2pi * sig);
+    amp = amp * (rj + sq2pi * sig);
+  } else if (P.radial_enh == 2) {
+    ampd = amp * (2.0 * rj + 2.0 * sig * c + sq8pi * sig + sq8pi * rj * c) +
+           ampd * (rj * rj + sig * sig + sq8pi * sig * rj);
+    amp = amp * (rj * rj + sig * sig + sq8pi * sig * rj);
+  }
+  double m0[7], m1[7], cc[4];
+  if (rj - w < rs) {  // soft zone (:1637-1645, 1770-1846)
+    const double l1 = fmax(0.0, rj - w), l2 = fmin(rj, rs), l3 = fmin(rs, rj + w);
+    op_piece(l1, rj, w, false, cc); op_soft_terms(l1, cc, m0);
+    op_piece(l2, rj, w, false, cc); op_soft_terms(l2, cc, m1);
+    op_accumulate<AMAX>(a, l1, l2, m0, m1, 4, 1.0, e);
+    op_piece(l2, rj, w, true, cc); op_soft_terms(l2, cc, m0);
+    op_piece(l3, rj, w, true, cc); op_soft_terms(l3, cc, m1);
+    op_accumulate<AMAX>(a, l2, l3, m0, m1, 4, 1.0, e);
+    if (do_der) {
+      op_piece_d(l1, rj, w, ws, false, cc); op_soft_terms(l1, cc, m0);
+      op_piece_d(l2, rj, w, ws, false, cc); op_soft_terms(l2, cc, m1);
+      op_accumulate<AMAX>(a, l1, l2, m0, m1, 4, 1.0, ed);
+      op_piece_d(l2, rj, w, ws, true, cc); op_soft_terms(l2, cc, m0);
+      op_piece_d(l3, rj, w, ws, true, cc); op_soft_terms(l3, cc, m1);
+      op_accumulate<AMAX>(a, l2, l3, m0, m1, 4, 1.0, ed);
+    }
+  }
+  if (rs < 1.0 && rj + w > rs) {  // buffer zone (:1858-2075)
+    const double l1 = fmax(rs, rj - w), l2 = fmax(rj, rs), l3 = fmin(1.0, rj + w);
+    double C[4], B[7];
+    op_piece(0.0, rs, filter_width, true, C);
+    for (int pc = 0; pc < (do_der ? 4 : 2); ++pc) {
+      const bool right = pc & 1, dv = pc >= 2;
+      if (dv) op_piece_d(-rj, 0.0, w, ws, right, cc);
+      else op_piece(-rj, 0.0, w, right, cc);
+      op_product(cc, C, B);
+      const double lo = right ? l2 : l1, hi = right ? l3 : l2;
+      op_buffer_terms(lo, B, m0);
+      op_buffer_terms(hi, B, m1);
+      if (dv) op_accumulate<AMAX>(a, lo, hi, m0, m1, 7, 1.0, ed);
+      else op_accumulate<AMAX>(a, lo, hi, m0, m1, 7, 1.0, e);
+    }
+  }
+  // W-transform (:2097-2100) and the change of variable (:2113-2117)
+#pragma unroll
+  for (int i = 0; i < AMAX; ++i) {
+    val[i] = 0.0;
+    der[i] = 0.0;
+  }
+#pragma unroll
+  for (int m = 0; m < AMAX; ++m) {
+    if (m < a) {
+      const double *Wc = W + m * a;
+      const double em = amp * e[m], dm = amp * ed[m] + ampd * e[m];
+#pragma unroll
+      for (int i = 0; i < AMAX; ++i)
+        if (i < a) {
+          val[i] = val[i] + Wc[i] * em;
+          der[i] = der[i] + Wc[i] * dm;
+        }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < AMAX; ++i) {
+    val[i] = val[i] * S.sqrt_rcut;
+    der[i] = der[i] * S.inv_sqrt_rcut;
+  }
+}
+
+// OP: the poly3operator basis (a separate instantiation, so that the poly3 and
+// poly3gauss kernels are compiled without its code).
+template <int AMAX, bool OP = false>
 __device__ __forceinline__ void radial_entry(const DevParams &P, const RadSp &S,
                                              const double *__restrict__ W, double r_in,
                                              bool is_central, bool do_der, double (&val)[AMAX],
                                              double (&der)[AMAX]) {
+  if constexpr (OP) {
+    radial_entry_op<AMAX>(P, S, W, r_in, is_central, do_der, val, der);
+    return;
+  }
   const double sqpi2 = 1.2533141373155002512, isq2 = 0.70710678118654752440;
   const double sq2pi = 0.79788456080286535588, sq8pi = 1.5957691216057307118;
   const int a = S.alpha;

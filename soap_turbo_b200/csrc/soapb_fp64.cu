@@ -14,7 +14,7 @@ namespace soapb {
 constexpr double kFourPi64 = 12.566370614359172954;
 
 // ---- radial, one thread per pair, every species block (:491-544)
-template <int AMAX>
+template <int AMAX, bool OP>
 __global__ void k64_radial(const DevParams P, const DevBatch B, int do_der, double *rad,
                            double *rad_der) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -46,7 +46,7 @@ __global__ void k64_radial(const DevParams P, const DevBatch B, int do_der, doub
     todo &= todo - 1u;
     const RadSp &S = P.rad[s];
     double val[AMAX], der[AMAX];
-    radial_entry<AMAX>(P, S, P.Wblk + (size_t)s * P.wstride, r, is_self, do_der != 0, val, der);
+    radial_entry<AMAX, OP>(P, S, P.Wblk + (size_t)s * P.wstride, r, is_self, do_der != 0, val, der);
     for (int n = 0; n < S.alpha; ++n) {
       ro[S.nbeg + n] = val[n] * S.gscale;
       if (do_der) rdo[S.nbeg + n] = der[n] * S.gscale;
@@ -353,8 +353,14 @@ cudaError_t launch_fp64_descriptor(const DevParams &P, const DevBatch &B, cudaSt
   int nl = 0;
   if (np > 0) {
     const int blocks = (np + 127) / 128;
-    if (max_alpha64(P) <= 8) k64_radial<8><<<blocks, 128, 0, s>>>(P, B, do_der, w.rad, w.rad_der);
-    else k64_radial<16><<<blocks, 128, 0, s>>>(P, B, do_der, w.rad, w.rad_der);
+    const bool op = P.basis == kBasisOperator;
+    if (max_alpha64(P) <= 8) {
+      if (op) k64_radial<8, true><<<blocks, 128, 0, s>>>(P, B, do_der, w.rad, w.rad_der);
+      else k64_radial<8, false><<<blocks, 128, 0, s>>>(P, B, do_der, w.rad, w.rad_der);
+    } else {
+      if (op) k64_radial<16, true><<<blocks, 128, 0, s>>>(P, B, do_der, w.rad, w.rad_der);
+      else k64_radial<16, false><<<blocks, 128, 0, s>>>(P, B, do_der, w.rad, w.rad_der);
+    }
     if (P.l_max <= 8) k64_angular<8><<<blocks, 128, 0, s>>>(P, B, do_der, (double2 *)w.ang);
     else k64_angular<12><<<blocks, 128, 0, s>>>(P, B, do_der, (double2 *)w.ang);
     nl += 2;

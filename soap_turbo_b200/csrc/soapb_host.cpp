@@ -250,12 +250,16 @@ int basis_limit_check(int basis, int alpha) {
     return fail(SOAPB_ERR_ALPHA_TOO_LARGE,
                 "ERROR: Due to numerical instabilities in the basis construction for the "
                 "poly3gauss basis, alpha_max > 11 is refused (recommended: <= 8)");
+  // poly3operator takes poly3's W from the tables for alpha_max = 1..11
+  // (src/soap_turbo_radial.f90:1235-1535, called at src/soap_turbo.f90:380-381)
+  if (basis == SOAPB_BASIS_POLY3OPERATOR && alpha > 11)
+    return fail(SOAPB_ERR_ALPHA_TOO_LARGE, "Bad value of alpha_max (poly3operator: 1..11)");
   if (alpha > SOAPB_MAX_ALPHA) return fail(SOAPB_ERR_ARGUMENT, "alpha_max above %d", SOAPB_MAX_ALPHA);
   return SOAPB_OK;
 }
 
 int species_basis(int basis, int alpha, double sig, double rcut, double *S, double *W) {
-  if (basis == SOAPB_BASIS_POLY3) overlap_poly3(alpha, S);
+  if (basis == SOAPB_BASIS_POLY3 || basis == SOAPB_BASIS_POLY3OPERATOR) overlap_poly3(alpha, S);
   else overlap_poly3gauss(alpha, sig, rcut, S);
   if (inverse_sqrt(alpha, S, W)) return fail(SOAPB_ERR_BASIS_MATRIX, "overlap matrix not positive definite");
   return SOAPB_OK;
@@ -303,11 +307,16 @@ int build_tables(soapb_context *c) {
     R.amp_scaling = c->amp_sc[s];
     R.cw = c->cw[s];
     R.gscale = c->gscale[s];
-    R.rcut_hard = c->rcut_hard[s];
+    // poly3operator selects its pairs by the soft and buffer zones alone, with no
+    // r < rcut_hard test of its own (src/soap_turbo_radial.f90:1637-1645, 1858-1872)
+    R.rcut_hard = c->basis == SOAPB_BASIS_POLY3OPERATOR ? HUGE_VAL : c->rcut_hard[s];
     R.alpha = c->alpha[s];
     R.n_poly = c->basis == SOAPB_BASIS_POLY3GAUSS ? c->alpha[s] - 1 : c->alpha[s];
     R.nbeg = nbeg;
-    R.do_central = c->basis == SOAPB_BASIS_POLY3GAUSS ? 0 : (c->cw[s] != 0.0);
+    // poly3operator always expands the central atom, weighted by central_weight
+    // (src/soap_turbo.f90:534-539)
+    R.do_central = c->basis == SOAPB_BASIS_POLY3GAUSS ? 0
+                   : (c->basis == SOAPB_BASIS_POLY3OPERATOR ? 1 : (c->cw[s] != 0.0));
     nbeg += c->alpha[s];
     amax = std::max(amax, c->alpha[s]);
     P.sig_t[s] = c->sig_t[s];
@@ -668,8 +677,8 @@ int init_context(soapb_context *c, const soapb_hyper *h) {
     return fail(SOAPB_ERR_ARGUMENT, "n_species must be in 1..%d", SOAPB_MAX_SPECIES);
   if (h->l_max < 0 || h->l_max > SOAPB_MAX_LMAX)
     return fail(SOAPB_ERR_ARGUMENT, "l_max must be in 0..%d", SOAPB_MAX_LMAX);
-  if (h->basis != SOAPB_BASIS_POLY3 && h->basis != SOAPB_BASIS_POLY3GAUSS)
-    return fail(SOAPB_ERR_BASIS, "basis must be poly3 or poly3gauss");
+  if (h->basis != SOAPB_BASIS_POLY3 && h->basis != SOAPB_BASIS_POLY3GAUSS && h->basis != SOAPB_BASIS_POLY3OPERATOR)
+    return fail(SOAPB_ERR_BASIS, "basis must be poly3, poly3gauss or poly3operator");
   if (h->radial_enhancement < 0 || h->radial_enhancement > 2)
     return fail(SOAPB_ERR_ARGUMENT, "radial_enhancement must be 0, 1 or 2");
   const double *arrs[] = {h->rcut_hard, h->rcut_soft, h->nf, h->global_scaling, h->atom_sigma_r,
@@ -949,6 +958,10 @@ int ctx_fp64(soapb_context *c, const soapb_batch *b, double *d_soap, double *d_c
 // descriptor the caller holds) may be null: the recomputed one is used.
 int ctx_hessian(soapb_context *c, const soapb_batch *b, const double *d_soap, int n_vec, const double *d_vecs,
                 double *d_hess) {
+  if (c->basis == SOAPB_BASIS_POLY3OPERATOR)
+    return fail(SOAPB_ERR_BASIS,
+                "ERROR: soap_turbo: the central-atom Hessian needs second radial derivatives, which the "
+                "poly3operator basis does not provide. Use poly3 or poly3gauss.");
   if (c->legacy)
     return fail(SOAPB_ERR_ARGUMENT,
                 "ERROR: the second radial derivatives need legacy_filter_seed = .false.; with the legacy "
@@ -1752,7 +1765,12 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
   int b;
   if (!std::strcmp(basis, "poly3")) b = SOAPB_BASIS_POLY3;
   else if (!std::strcmp(basis, "poly3gauss")) b = SOAPB_BASIS_POLY3GAUSS;
-  else return fail(SOAPB_ERR_BASIS, "basis \"%s\" is not supported (poly3, poly3gauss)", basis);
+  else if (!std::strcmp(basis, "poly3operator")) b = SOAPB_BASIS_POLY3OPERATOR;
+  else return fail(SOAPB_ERR_BASIS, "basis \"%s\" is not supported (poly3, poly3gauss, poly3operator)", basis);
+  if (do_hessian && b == SOAPB_BASIS_POLY3OPERATOR)  // src/soap_turbo.f90:485-489
+    return fail(SOAPB_ERR_BASIS,
+                "ERROR: soap_turbo: the central-atom Hessian needs second radial derivatives, which the "
+                "poly3operator basis does not provide. Use poly3 or poly3gauss.");
   if (n_sites < 0 || n_atom_pairs < 0) return fail(SOAPB_ERR_ARGUMENT, "negative sizes");
   if (n_sites > 0 && !n_neigh) return fail(SOAPB_ERR_ARGUMENT, "null n_neigh");
   // CSR check on the host: the kernels trust the offsets

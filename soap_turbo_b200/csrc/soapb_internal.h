@@ -27,9 +27,12 @@ struct RadSp {
   int alpha, n_poly, nbeg, has_filter, do_central, pad;
 };
 
+// DevParams::basis of the poly3operator basis (SOAPB_BASIS_POLY3OPERATOR)
+constexpr int kBasisOperator = 2;
+
 struct DevParams {
   int n_species, l_max, k_max, n_max;
-  int basis;          // 0 poly3, 1 poly3gauss
+  int basis;          // 0 poly3, 1 poly3gauss, 2 poly3operator (kBasisOperator)
   int scaling_poly;   // scaling_mode == "polynomial"
   int radial_enh;     // radial_enhancement
   int legacy_seed;    // legacy_filter_seed

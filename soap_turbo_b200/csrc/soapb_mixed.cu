@@ -223,7 +223,7 @@ int ang_row_floats(const DevParams &P) { return row_len(P.amax_t == 8 ? 8 : 12);
 // The site kernels only read these rows; soap_contract reads the rows of the
 // descriptor call that kept its state, as the reference keeps the radial and
 // angular expansions between get_soap and soap_contract.
-template <int AMAX, int LC>
+template <int AMAX, int LC, bool OP>
 __global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch B, int do_der,
                                               int scan_tiles) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch 
         todo &= todo - 1u;
         const RadSp &RS = *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
         double val[AMAX], der[AMAX];
-        radial_entry<AMAX>(P, RS, sW + s * AMAX * AMAX, r, false, do_der != 0, val, der);
+        radial_entry<AMAX, OP>(P, RS, sW + s * AMAX * AMAX, r, false, do_der != 0, val, der);
         const double g4 = kFourPi * RS.gscale;
         float4 *o = (float4 *)(B.rad + ((size_t)k * P.n_species + s) * 2 * AMAX);
 #pragma unroll
@@ -1102,12 +1102,12 @@ cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int AMAX, int LC>
+template <int AMAX, int LC, bool OP>
 static cudaError_t run_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der) {
   size_t sm = (size_t)P.off_rad + (size_t)P.n_species * SOAPB_RADSP_BYTES +
               (size_t)128 * (row_len(LC) + 1) * sizeof(float);
   if (sm < kScanTile * sizeof(int)) sm = kScanTile * sizeof(int);  // scan tiles reuse it
-  auto kern = k_pair<AMAX, LC>;
+  auto kern = k_pair<AMAX, LC, OP>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int tiles = prep_scan_tiles(B.n_sites);
@@ -1117,8 +1117,12 @@ static cudaError_t run_pair(const DevParams &P, const DevBatch &B, cudaStream_t 
 }
 
 cudaError_t launch_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der) {
-  if (P.amax_t == 8) return run_pair<8, 8>(P, B, s, do_der);
-  return run_pair<16, 12>(P, B, s, do_der);
+  if (P.basis == kBasisOperator) {
+    if (P.amax_t == 8) return run_pair<8, 8, true>(P, B, s, do_der);
+    return run_pair<16, 12, true>(P, B, s, do_der);
+  }
+  if (P.amax_t == 8) return run_pair<8, 8, false>(P, B, s, do_der);
+  return run_pair<16, 12, false>(P, B, s, do_der);
 }
 
 // The radial block is fixed by the definition: the host lays the constants

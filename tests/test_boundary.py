@@ -188,7 +188,7 @@ def _tiny_call(**over):
 def test_argument_checks_before_any_device_work():
     # a bad basis name or inconsistent CSR is refused on the host
     with pytest.raises(_lib.SoapError) as e:
-        D.get_soap(**_tiny_call(basis="poly3operator"))
+        D.get_soap(**_tiny_call(basis="poly3tab"))  # no radial expansion of its own in the reference
     assert e.value.code == 5
     a = _tiny_call()
     a["n_atom_pairs"] = a["n_atom_pairs"] - 1
@@ -229,3 +229,17 @@ def test_central_hessian_state_checks_on_the_host():
         assert e.value.code == 1 and "legacy_filter_seed" in str(e.value)
     finally:
         D.set_soap_hessian_enabled(False)
+
+
+def test_poly3operator_has_no_hessian():
+    """soap_hessian_enabled with the poly3operator basis stops get_soap in the
+    reference (src/soap_turbo.f90:485-489): refused before any device work."""
+    D.set_legacy_filter_seed(False)
+    D.set_soap_hessian_enabled(True)
+    try:
+        with pytest.raises(_lib.SoapError) as e:
+            D.get_soap(**_tiny_call(basis="poly3operator", do_derivatives=True))
+        assert e.value.code == 5 and "poly3operator" in str(e.value)
+    finally:
+        D.set_soap_hessian_enabled(False)
+        D.set_legacy_filter_seed(True)

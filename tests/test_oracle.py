@@ -339,3 +339,72 @@ def test_central_hessian_self_block_and_state():
         plain.central_hessian(vecs)
     with pytest.raises(RuntimeError):  # second radial derivatives need the unified seed
         O.get_soap(hp, nl, W, S, do_derivatives=True, legacy_filter_seed=True, hessian=True)
+
+
+# ---------------------------------------------------------------- poly3operator basis
+def _op_quadrature(alpha, r_in, rcut_soft, rcut_hard, sigma, sigma_scaling):
+    """The overlaps the poly3operator expansion stands for, by adaptive
+    quadrature of the integrand itself (src/soap_turbo_radial.f90:1549-2141, in
+    units of rcut_hard): phi_n(r) = (1 - r)^(n+2) sqrt(2n + 5) against the
+    piecewise-cubic density g of width w = 2 sqrt(2 ln 2) sigma(r_j), times
+    the cubic filter from r_soft (width 2 sqrt(2 ln 2)(1 - r_soft)) on the
+    buffer zone; amplitude 1/sigma (1 + 2r^3 - 3r^2); scaled by sqrt(rcut_hard)."""
+    from scipy.integrate import quad
+    cw = 2.0 * np.sqrt(2.0 * np.log(2.0))
+    rs, rj = rcut_soft / rcut_hard, r_in / rcut_hard
+    sig = sigma / rcut_hard + sigma_scaling * rj
+    w, fw = cw * sig, cw * (1.0 - rs)
+
+    def g(r):
+        x = (r - rj) / w
+        return 1 - 3 * x * x - 2 * x ** 3 if x <= 0 else 1 - 3 * x * x + 2 * x ** 3
+
+    def f(r):
+        y = (r - rs) / fw
+        return 1 - 3 * y * y + 2 * y ** 3
+
+    out = np.zeros(alpha)
+    amp = (1 + 2 * rj ** 3 - 3 * rj ** 2) / sig
+    for n in range(1, alpha + 1):
+        phi = lambda r: (1 - r) ** (n + 2) * np.sqrt(2 * n + 5)
+        tot = 0.0
+        if r_in - cw * (sigma + sigma_scaling * r_in) < rcut_soft:
+            lo, mid, hi = max(0.0, rj - w), min(rj, rs), min(rs, rj + w)
+            tot += quad(lambda r: phi(r) * g(r), lo, mid, epsabs=1e-15, epsrel=1e-13)[0]
+            tot += quad(lambda r: phi(r) * g(r), mid, hi, epsabs=1e-15, epsrel=1e-13)[0]
+        if rcut_soft < rcut_hard and r_in + cw * (sigma + sigma_scaling * r_in) > rcut_soft:
+            lo, mid, hi = max(rs, rj - w), max(rj, rs), min(1.0, rj + w)
+            tot += quad(lambda r: phi(r) * g(r) * f(r), lo, mid, epsabs=1e-15, epsrel=1e-13)[0]
+            tot += quad(lambda r: phi(r) * g(r) * f(r), mid, hi, epsabs=1e-15, epsrel=1e-13)[0]
+        out[n - 1] = amp * tot * np.sqrt(rcut_hard)
+    return out
+
+
+@pytest.mark.parametrize("rcut_soft,sig_scale", [(4.5, 0.0), (4.0, 0.1), (5.0, 0.0)])
+def test_poly3operator_overlaps_match_quadrature(rcut_soft, sig_scale):
+    """The oracle's closed-form integration by parts (the reference's A, I0,
+    g_aux and filter-product tables) against direct quadrature, with W = I so
+    the raw overlaps show; rcut_soft = rcut_hard has no buffer zone."""
+    alpha = 8
+    hp = syn.Hyper(alpha_max=[alpha], basis="poly3operator", rcut_soft=rcut_soft,
+                   atom_sigma_r_scaling=sig_scale)
+    r = np.array([0.3, 1.1, 2.5, 3.7, 4.1, 4.45, 4.6, 4.9])
+    got, _ = O.radial_eval(hp, 0, np.eye(alpha), r)
+    for t, rj in enumerate(r):
+        ref = _op_quadrature(alpha, rj, rcut_soft, 5.0, 0.5, sig_scale)
+        assert np.abs(got[t] - ref).max() <= 1e-10 * max(1.0, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("enh", [0, 1, 2])
+def test_poly3operator_derivative_matches_finite_differences(enh):
+    hp = syn.Hyper(alpha_max=[7], basis="poly3operator", rcut_soft=4.0, atom_sigma_r_scaling=0.08,
+                   radial_enhancement=enh, amplitude_scaling=1.5)
+    W, _ = O.basis_matrices(hp)
+    r = np.linspace(0.4, 4.95, 29)
+    h = 1e-4  # W's norm (~9e4 at alpha 7) amplifies rounding; h balances it against h^2
+    _, d = O.radial_eval(hp, 0, W, r)
+    vp, _ = O.radial_eval(hp, 0, W, r + h)
+    vm, _ = O.radial_eval(hp, 0, W, r - h)
+    assert np.abs(d - (vp - vm) / (2 * h)).max() <= 1e-6 * np.abs(d).max()
+    with pytest.raises(ValueError):  # no second derivatives for this basis (src/soap_turbo.f90:485-489)
+        O.radial_eval(hp, 0, W, r, legacy_seed=False, der2=True)
