@@ -8,6 +8,7 @@ with an upstream gradient G ~ N(0,1).  Inputs are seeded synthetic structures
 of those shapes (no dataset is involved).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --hessian N_VEC [--scale F] [--steps K] [--warmup W]
 
 N > 1 runs one process per GPU (torchrun): every rank processes its own
 structure (sites are independent; no collective on the data path), so the
@@ -15,6 +16,10 @@ scaling is weak and the value is all ranks' sites over the slowest rank's time.
 ``--impl reference`` times the reference algorithm on the host cores instead:
 the FP64 CPU restatement of soap_turbo's get_soap + soap_contract (the
 reference is Fortran and no Fortran compiler exists on these machines).
+``--hessian N_VEC`` times the central-atom Hessian (soapb_central_hessian,
+the reference's get_soap_central_hessian) with N_VEC weight vectors per site
+on the same structure (``--scale`` shrinks it, for profiler captures), beside
+the oracle's restatement on the host cores; it prints its own JSON line.
 """
 import argparse
 import json
@@ -43,6 +48,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--hessian", type=int, default=0, metavar="N_VEC",
+                    help="time the central-atom Hessian with N_VEC weight vectors instead")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="(--hessian) scale the structure's atom count, for profiler captures")
     ap.add_argument("--quick", action="store_true",
                     help="time the two kernels only (no FP64 path, e2e, CPU baseline or peak "
                          "measurement); for profiling runs")
@@ -463,8 +472,65 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def run_hessian(args):
+    """Central-atom Hessian on the benchmark structure: device time per call
+    (CUDA events, inputs resident, L2 flushed between calls), the oracle's
+    restatement on the host cores, and the relative error between them."""
+    import torch
+    from soap_turbo_b200 import synthetic as syn
+    from soap_turbo_b200.context import Context
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    w = syn.config(2, seed=args.seed, scale=args.scale)
+    nl, n_vec = w.nl, args.hessian
+    ctx = Context(w.hyper, legacy_filter_seed=False)
+    b = ctx.batch(nl)
+    vecs_h = np.random.default_rng(args.seed).standard_normal((nl.n_sites, n_vec, ctx.n_soap))
+    vecs = torch.as_tensor(vecs_h).to(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    out = ctx.central_hessian(b, vecs)
+    for _ in range(max(args.warmup, 0)):
+        ctx.central_hessian(b, vecs, out=out)
+    ctx.check_inputs()
+    times = []
+    n0 = ctx.launch_count
+    for _ in range(max(args.steps, 1)):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.central_hessian(b, vecs, out=out)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    launches = (ctx.launch_count - n0) / max(args.steps, 1)
+    ms = statistics.median(times)
+    W, S = ctx.basis()
+    t0 = time.perf_counter()
+    ref = O.get_soap(w.hyper, nl, W, S, do_derivatives=True, legacy_filter_seed=False, hessian=True)
+    href, selftest = ref.central_hessian(vecs_h)
+    t_cpu = time.perf_counter() - t0
+    got = out.cpu().numpy()
+    line = {"metric": "central-atom Hessian (get_soap_central_hessian), sites/s", "unit": "sites/s",
+            "value": nl.n_sites / (ms * 1e-3), "ms_per_call": ms, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "n_vec": n_vec, "gpu_launches_per_call": launches,
+            "config": {"workload": WORKLOAD + (f", atoms scaled by {args.scale}" if args.scale != 1.0 else ""),
+                       "sites": nl.n_sites, "pairs": nl.n_pairs, "l2": "flushed before each call"},
+            "error_vs_fp64_oracle": {"max_rel": float(np.abs(got - href).max() / np.abs(href).max()),
+                                     "oracle_selftest": selftest},
+            "cpu_baseline": {"value": nl.n_sites / t_cpu, "unit": "sites/s", "cores": O.num_threads(),
+                             "kind": "port", "sample": f"one call on the whole structure (get_soap with "
+                                                       f"second derivatives + the Hessian), {t_cpu:.3f} s"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.hessian > 0:
+        run_hessian(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

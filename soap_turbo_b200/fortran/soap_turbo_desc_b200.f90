@@ -1,7 +1,8 @@
 ! soap_turbo_desc_b200 -- Fortran front end of libsoapb200.so.
 !
-! Keeps the argument lists of soap_turbo's get_soap (src/soap_turbo.f90:139-169)
-! and soap_contract (:1723-1730), so a caller switches by changing
+! Keeps the argument lists of soap_turbo's get_soap (src/soap_turbo.f90:139-169),
+! soap_contract (:1723-1730) and get_soap_central_hessian (:1151-1160), so a
+! caller switches by changing
 !   use soap_turbo_desc      ->      use soap_turbo_desc_b200
 ! and linking libsoapb200.so.  The arrays cross the C ABI as base addresses plus
 ! the extents the assumed-shape descriptors carry; LOGICAL masks become bytes;
@@ -24,7 +25,8 @@ module soap_turbo_desc_b200
 
   integer, parameter :: dp = real64
 
-  public :: get_soap, soap_contract, soap_b200_set_legacy_filter_seed, soap_b200_set_precision
+  public :: get_soap, soap_contract, get_soap_central_hessian, soap_b200_set_legacy_filter_seed, &
+            soap_b200_set_precision, soap_b200_set_hessian_enabled
 
   interface
     function soapb_get_soap(n_sites, n_neigh, n_species, species, max_mult, species_multiplicity, &
@@ -63,6 +65,28 @@ module soap_turbo_desc_b200
       real(c_double), value :: sgn
       real(c_double), intent(out) :: pair(*)
       integer(c_int), value :: n_sites, n_soap, n_atom_pairs
+      integer(c_int) :: rc
+    end function
+
+    function soapb_get_soap_central_hessian(n_sites, n_neigh, n_atom_pairs, n_species, mask, rjs, thetas, &
+                                            phis, l_max, rcut_hard, atom_sigma_t, atom_sigma_t_scaling, &
+                                            compress_soap, compress_P_nonzero, compress_P_i, compress_P_j, &
+                                            compress_P_el, soap, n_soap, n_vec, vecs, hess) result(rc) &
+                                            bind(C, name="soapb_get_soap_central_hessian")
+      import :: c_int, c_double, c_int8_t
+      integer(c_int), value :: n_sites, n_atom_pairs, n_species, l_max, compress_soap, compress_P_nonzero
+      integer(c_int), value :: n_soap, n_vec
+      integer(c_int), intent(in) :: n_neigh(*), compress_P_i(*), compress_P_j(*)
+      integer(c_int8_t), intent(in) :: mask(*)
+      real(c_double), intent(in) :: rjs(*), thetas(*), phis(*), rcut_hard(*), atom_sigma_t(*)
+      real(c_double), intent(in) :: atom_sigma_t_scaling(*), compress_P_el(*), soap(*), vecs(*)
+      real(c_double), intent(out) :: hess(*)
+      integer(c_int) :: rc
+    end function
+
+    function soapb_set_soap_hessian_enabled(enabled) result(rc) bind(C, name="soapb_set_soap_hessian_enabled")
+      import :: c_int
+      integer(c_int), value :: enabled
       integer(c_int) :: rc
     end function
 
@@ -166,6 +190,44 @@ contains
                              int(size(soap, 1), c_int), int(size(pair, 2), c_int))
     call check(rc)
   end subroutine soap_contract
+
+  ! get_soap_central_hessian (src/soap_turbo.f90:1151-1160): after get_soap with
+  ! do_derivatives on the same batch, with soap_b200_set_hessian_enabled(.true.)
+  ! called before that get_soap.  hess(1:3, 1:3, 1:n_vec, 1:n_atom_pairs).
+  subroutine get_soap_central_hessian(n_sites, n_neigh, n_atom_pairs, n_species, mask, rjs, thetas, phis, &
+                                      l_max, rcut_hard, atom_sigma_t, atom_sigma_t_scaling, compress_soap, &
+                                      compress_P_nonzero, compress_P_i, compress_P_j, compress_P_el, soap, &
+                                      n_vec, vecs, hess)
+    implicit none
+    integer, intent(in) :: n_sites, n_neigh(:), n_atom_pairs, n_species, l_max, n_vec
+    integer, intent(in) :: compress_P_nonzero, compress_P_i(:), compress_P_j(:)
+    logical, intent(in) :: mask(:,:), compress_soap
+    real(dp), intent(in) :: rjs(:), thetas(:), phis(:), rcut_hard(:)
+    real(dp), intent(in) :: atom_sigma_t(:), atom_sigma_t_scaling(:), compress_P_el(:)
+    real(dp), intent(in) :: soap(:,:), vecs(:,:,:)
+    real(dp), intent(out) :: hess(:,:,:,:)
+
+    integer(c_int8_t), allocatable :: mask8(:,:)
+    integer(c_int) :: rc
+
+    allocate( mask8(size(mask,1), size(mask,2)) )
+    mask8 = merge(1_c_int8_t, 0_c_int8_t, mask)
+    rc = soapb_get_soap_central_hessian(int(n_sites, c_int), n_neigh, int(n_atom_pairs, c_int), &
+                                        int(n_species, c_int), mask8, rjs, thetas, phis, int(l_max, c_int), &
+                                        rcut_hard, atom_sigma_t, atom_sigma_t_scaling, &
+                                        merge(1_c_int, 0_c_int, compress_soap), int(compress_P_nonzero, c_int), &
+                                        compress_P_i, compress_P_j, compress_P_el, soap, &
+                                        int(size(soap, 1), c_int), int(n_vec, c_int), vecs, hess)
+    deallocate( mask8 )
+    call check(rc)
+  end subroutine get_soap_central_hessian
+
+  ! The reference's module flag soap_turbo_desc::soap_hessian_enabled
+  ! (src/soap_turbo.f90:76), default .false.
+  subroutine soap_b200_set_hessian_enabled(enabled)
+    logical, intent(in) :: enabled
+    call check(soapb_set_soap_hessian_enabled(merge(1_c_int, 0_c_int, enabled)))
+  end subroutine
 
   ! The reference's module flag soap_turbo_radial::legacy_filter_seed
   ! (src/soap_turbo_radial.f90:67), default .true.
