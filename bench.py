@@ -9,6 +9,7 @@ of those shapes (no dataset is involved).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
   python bench.py --hessian N_VEC [--scale F] [--steps K] [--warmup W]
+  python bench.py --neighbors [--steps K] [--warmup W]
 
 N > 1 runs one process per GPU (torchrun): every rank processes its own
 structure (sites are independent; no collective on the data path), so the
@@ -20,6 +21,8 @@ reference is Fortran and no Fortran compiler exists on these machines).
 the reference's get_soap_central_hessian) with N_VEC weight vectors per site
 on the same structure (``--scale`` shrinks it, for profiler captures), beside
 the oracle's restatement on the host cores; it prints its own JSON line.
+``--neighbors`` times the device neighbour-list builder (soapb_build_neighbors)
+on the benchmark structure beside the numpy builder the tests check it against.
 """
 import argparse
 import json
@@ -50,6 +53,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--hessian", type=int, default=0, metavar="N_VEC",
                     help="time the central-atom Hessian with N_VEC weight vectors instead")
+    ap.add_argument("--neighbors", action="store_true",
+                    help="time the device neighbour-list builder instead")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="(--hessian) scale the structure's atom count, for profiler captures")
     ap.add_argument("--quick", action="store_true",
@@ -565,8 +570,64 @@ def run_hessian(args):
     print(json.dumps(line), flush=True)
 
 
+def run_neighbors(args):
+    """soapb_build_neighbors on the benchmark structure: positions, cell and
+    species resident on the device, the CSR batch get_soap takes out.  The
+    call waits once for the pair count, so its time is the host's wall clock
+    around it; the device time of its launches is reported beside it."""
+    import torch
+    from soap_turbo_b200 import synthetic as syn
+    from soap_turbo_b200.context import Context
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    w = syn.config(2, seed=args.seed, scale=args.scale)
+    st, nl = w.structures[0], w.nl
+    ctx = Context(w.hyper)
+    pos = torch.as_tensor(np.asarray(st.positions, np.float64)).to(dev)
+    sp = torch.as_tensor((st.species + 1).astype(np.int32).reshape(-1, 1)).to(dev)
+    sites = torch.as_tensor(nl.site_atom.astype(np.int32)).to(dev)
+    lat = np.eye(3) * st.box
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(max(args.warmup, 3)):
+        built = ctx.build_neighbors(pos, lat, sp, sites)
+    torch.cuda.synchronize()
+    wall, dev_ms = [], []
+    n0 = ctx.launch_count
+    for _ in range(max(args.steps, 1)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
+        built = ctx.build_neighbors(pos, lat, sp, sites)
+        e1.record()
+        torch.cuda.synchronize()
+        wall.append((time.perf_counter() - t0) * 1e3)
+        dev_ms.append(e0.elapsed_time(e1))
+    launches = (ctx.launch_count - n0) / max(args.steps, 1)
+    a = built.arrays()
+    same = bool(np.array_equal(a["n_neigh"], nl.n_neigh))
+    t0 = time.perf_counter()
+    syn.neighbour_list(st, 5.0, 3, central_species=1)
+    t_np = time.perf_counter() - t0
+    ms = statistics.median(wall)
+    line = {"metric": "neighbour-list build (soapb_build_neighbors), pairs/s", "unit": "pairs/s",
+            "value": nl.n_pairs / (ms * 1e-3), "ms_per_build": ms,
+            "device_ms_per_build": statistics.median(dev_ms), "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic", "gpu_launches_per_build": launches,
+            "config": {"workload": WORKLOAD, "atoms": int(st.positions.shape[0]), "sites": nl.n_sites,
+                       "pairs": nl.n_pairs, "l2": "flushed before each build"},
+            "counts_match_numpy_builder": same,
+            "cpu_baseline": {"value": nl.n_pairs / t_np, "unit": "pairs/s", "cores": 1, "kind": "port",
+                             "sample": f"the numpy builder the tests compare against, one build, {t_np:.3f} s"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.neighbors:
+        run_neighbors(args)
+        return
     if args.hessian > 0:
         run_hessian(args)
         return

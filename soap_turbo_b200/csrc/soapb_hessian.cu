@@ -632,7 +632,8 @@ __global__ void __launch_bounds__(kHessThreads) k64_hess(const DevParams P, cons
           if (act) {
             const double2 *zv = (const double2 *)h.Zv + (size_t)v * N * K + k;
             const double2 *zg = (const double2 *)h.ZGv + ((size_t)v * N * K + k) * 3;
-            for (int n = 0; n < N; ++n) {
+#pragma unroll 4
+            for (int n = 0; n < N; ++n) {  // unrolled: more of the Z loads in flight
               const double2 zz = zv[(size_t)n * K];
               const dcx zc = cx(zz.x, -zz.y);
               const double r0 = wrad[n], r1 = wrad[N + n];
