@@ -972,6 +972,19 @@ int ctx_hessian(soapb_context *c, const soapb_batch *b, const double *d_soap, in
   if (rc) return rc;
   if (n_vec == 0) return SOAPB_OK;
   if (b->n_sites > 0 && !d_vecs) return fail(SOAPB_ERR_ARGUMENT, "null vecs");
+  {
+    // the per-warp k-sums grow with n_vec; the kernel holds them in shared memory
+    int dev = 0, smem_max = 0;
+    CU(cudaGetDevice(&dev));
+    CU(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t need = hess_smem_bytes(c->P, n_vec);
+    if (need > (size_t)smem_max) {
+      int top = n_vec;
+      while (top > 1 && hess_smem_bytes(c->P, top) > (size_t)smem_max) --top;
+      return fail(SOAPB_ERR_ARGUMENT, "n_vec = %d needs %zu bytes of shared memory per CTA (at most %d): "
+                  "pass at most %d weight vectors per call", n_vec, need, smem_max, top);
+    }
+  }
   if (b->n_atom_pairs > 0 && !d_hess) return fail(SOAPB_ERR_ARGUMENT, "null hess");
   if ((rc = run_prep(c, B))) return rc;
   DevParams P = c->P;

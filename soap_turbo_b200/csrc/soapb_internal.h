@@ -207,6 +207,7 @@ cudaError_t launch_fp64_contract(const DevParams &P, const DevBatch &B, cudaStre
 // cleared first.  scratch: grid * hess_scratch_doubles doubles; ticket: one int.
 size_t hess_scratch_doubles(const DevParams &P, int n_vec);
 size_t hess_geo_doubles(const DevParams &P);
+size_t hess_smem_bytes(const DevParams &P, int n_vec);  // dynamic shared memory of k64_hess
 int hess_grid(const DevParams &P, int n_vec);
 cudaError_t launch_hessian(const DevParams &P, const DevBatch &B, cudaStream_t s, const Fp64Work &w,
                            double *rad_der2, double *geo, int *good, const double *soap, int n_vec,

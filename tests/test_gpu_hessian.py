@@ -100,6 +100,18 @@ def test_legacy_seed_context_is_refused():
     assert e.value.code == 1
 
 
+def test_too_many_weight_vectors_is_an_argument_error():
+    """The kernel keeps per-warp k-sums for every vector in shared memory; past
+    its limit the call says so (SOAPB_ERR_ARGUMENT) instead of failing a launch."""
+    hp, nl = _case("gauss_2sp", n_atoms=12)
+    ctx = Context(hp, legacy_filter_seed=False)
+    b = ctx.batch(nl)
+    vecs = torch.zeros((nl.n_sites, 200, ctx.n_soap), dtype=torch.float64, device="cuda")
+    with pytest.raises(_lib.SoapError) as e:
+        ctx.central_hessian(b, vecs)
+    assert e.value.code == 1 and "weight vectors per call" in str(e.value)
+
+
 def _dropin_args(hp, nl, soap, P):
     return dict(n_sites=nl.n_sites, n_neigh=nl.n_neigh, n_species=hp.n_species,
                 species=nl.species.T, species_multiplicity=nl.species_multiplicity,
