@@ -297,9 +297,9 @@ int soapb_descriptor_fp64(soapb_context *ctx, const soapb_batch *batch, double *
  * (3, 3, n_vec, n_pairs), layouts as there.  FP64; it recomputes the FP64
  * expansion state of the batch, so it needs no earlier call.  d_soap is the
  * normalised descriptor the weights were formed against (NULL: the FP64 one
- * this call computes).  Needs legacy_filter_seed = 0 (SOAPB_ERR_ARGUMENT).  n_vec is
- * bounded by the kernel's shared memory (about 90 for the benchmark definition; larger values
- * return SOAPB_ERR_ARGUMENT with the limit): call again for more vectors. */
+ * this call computes).  Needs legacy_filter_seed = 0 (SOAPB_ERR_ARGUMENT).  More weight
+ * vectors than the kernel's shared memory holds at once (about 90 for the benchmark
+ * definition) are done in chunks, with two strided device copies per chunk. */
 int soapb_central_hessian(soapb_context *ctx, const soapb_batch *batch, const double *d_soap,
                           int32_t n_vec, const double *d_vecs, double *d_hess);
 

@@ -201,7 +201,7 @@ struct soapb_context {
   DBuf f64_rad, f64_rad_der, f64_ang, f64_cnk, f64_soap_un, f64_norm;
   // central-atom Hessian: second radial derivatives, pair geometry records and
   // flags, per-CTA scratch, the descriptor it recomputes, its work counter
-  DBuf hs_rad_der2, hs_geo, hs_good, hs_scratch, hs_soap, hs_ticket;
+  DBuf hs_rad_der2, hs_geo, hs_good, hs_scratch, hs_soap, hs_ticket, hs_vchunk, hs_hchunk;
   // neighbour-list builder: cell list, counts and the batch it hands out
   DBuf nb_acell, nb_ccount, nb_cstart, nb_cfill, nb_catoms, nb_counts, nb_off, nb_state;
   DBuf nb_rjs, nb_th, nb_ph, nb_mask, nb_natom, nb_nneigh, nb_species, nb_smult;
@@ -231,7 +231,7 @@ struct soapb_context {
     timing_release();
     for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &rad, &ang, &f64_rad, &f64_rad_der,
                     &f64_ang, &f64_cnk, &f64_soap_un, &f64_norm, &hs_rad_der2, &hs_geo, &hs_good, &hs_scratch, &hs_soap,
-                    &hs_ticket, &nb_acell, &nb_ccount, &nb_cstart,
+                    &hs_ticket, &hs_vchunk, &hs_hchunk, &nb_acell, &nb_ccount, &nb_cstart,
                     &nb_cfill, &nb_catoms, &nb_counts, &nb_off, &nb_state, &nb_rjs, &nb_th, &nb_ph,
                     &nb_mask, &nb_natom, &nb_nneigh, &nb_species, &nb_smult})
       b->release();
@@ -972,18 +972,17 @@ int ctx_hessian(soapb_context *c, const soapb_batch *b, const double *d_soap, in
   if (rc) return rc;
   if (n_vec == 0) return SOAPB_OK;
   if (b->n_sites > 0 && !d_vecs) return fail(SOAPB_ERR_ARGUMENT, "null vecs");
+  // The kernel keeps per-warp k-sums for every weight vector in shared memory:
+  // more vectors than fit are done in chunks (each vector's block depends on
+  // that vector alone, so the chunking changes no bits).
+  int chunk = n_vec;
   {
-    // the per-warp k-sums grow with n_vec; the kernel holds them in shared memory
     int dev = 0, smem_max = 0;
     CU(cudaGetDevice(&dev));
     CU(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    const size_t need = hess_smem_bytes(c->P, n_vec);
-    if (need > (size_t)smem_max) {
-      int top = n_vec;
-      while (top > 1 && hess_smem_bytes(c->P, top) > (size_t)smem_max) --top;
-      return fail(SOAPB_ERR_ARGUMENT, "n_vec = %d needs %zu bytes of shared memory per CTA (at most %d): "
-                  "pass at most %d weight vectors per call", n_vec, need, smem_max, top);
-    }
+    while (chunk > 1 && hess_smem_bytes(c->P, chunk) > (size_t)smem_max) --chunk;
+    if (hess_smem_bytes(c->P, chunk) > (size_t)smem_max)
+      return fail(SOAPB_ERR_ARGUMENT, "the Hessian kernel needs more shared memory than the device has");
   }
   if (b->n_atom_pairs > 0 && !d_hess) return fail(SOAPB_ERR_ARGUMENT, "null hess");
   if ((rc = run_prep(c, B))) return rc;
@@ -1002,15 +1001,35 @@ int ctx_hessian(soapb_context *c, const soapb_batch *b, const double *d_soap, in
   if ((rc = c->hs_good.ensure(4 * np))) return rc;
   if ((rc = c->hs_soap.ensure(8 * ns * c->n_soap))) return rc;
   if ((rc = c->hs_ticket.ensure(16))) return rc;
-  const int grid = std::max(1, std::min(hess_grid(P, n_vec), b->n_sites));
-  if ((rc = c->hs_scratch.ensure(8 * (size_t)grid * hess_scratch_doubles(P, n_vec)))) return rc;
+  const int grid = std::max(1, std::min(hess_grid(P, chunk), b->n_sites));
+  if ((rc = c->hs_scratch.ensure(8 * (size_t)grid * hess_scratch_doubles(P, chunk)))) return rc;
+  const size_t nsv = (size_t)c->n_soap, npair = (size_t)b->n_atom_pairs, nsite = (size_t)b->n_sites;
+  if (chunk < n_vec) {
+    if ((rc = c->hs_vchunk.ensure(8 * (nsite * chunk * nsv + 1)))) return rc;
+    if ((rc = c->hs_hchunk.ensure(8 * (npair * chunk * 9 + 1)))) return rc;
+  }
   Fp64Work w{c->f64_rad.as<double>(), c->f64_rad_der.as<double>(), c->f64_ang.as<double>(),
              c->f64_cnk.as<double>(), c->f64_soap_un.as<double>(), c->f64_norm.as<double>()};
   int nl = 0;
   CU(launch_fp64_descriptor(P, B, c->stream, w, 1, c->hs_soap.as<double>(), nullptr, &nl));
-  CU(launch_hessian(P, B, c->stream, w, c->hs_rad_der2.as<double>(), c->hs_geo.as<double>(), c->hs_good.as<int>(),
-                    d_soap ? d_soap : c->hs_soap.as<double>(), n_vec, d_vecs, d_hess, c->hs_scratch.as<double>(),
-                    grid, c->hs_ticket.as<int>(), &nl));
+  for (int v0 = 0; v0 < n_vec; v0 += chunk) {
+    const int nc = std::min(chunk, n_vec - v0);
+    const double *vecs = d_vecs;
+    double *hess = d_hess;
+    if (chunk < n_vec) {  // the chunk's vectors gathered, its blocks scattered back
+      vecs = c->hs_vchunk.as<double>();
+      hess = c->hs_hchunk.as<double>();
+      if (nsite > 0)
+        CU(cudaMemcpy2DAsync(c->hs_vchunk.p, 8 * nc * nsv, d_vecs + (size_t)v0 * nsv, 8 * (size_t)n_vec * nsv,
+                             8 * nc * nsv, nsite, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    CU(launch_hessian(P, B, c->stream, w, c->hs_rad_der2.as<double>(), c->hs_geo.as<double>(),
+                      c->hs_good.as<int>(), d_soap ? d_soap : c->hs_soap.as<double>(), nc, vecs, hess,
+                      c->hs_scratch.as<double>(), grid, c->hs_ticket.as<int>(), &nl));
+    if (chunk < n_vec && npair > 0)
+      CU(cudaMemcpy2DAsync(d_hess + (size_t)v0 * 9, 72 * (size_t)n_vec, c->hs_hchunk.p, 72 * (size_t)nc,
+                           72 * (size_t)nc, npair, cudaMemcpyDeviceToDevice, c->stream));
+  }
   c->launches += nl;
   return SOAPB_OK;
 }

@@ -100,16 +100,20 @@ def test_legacy_seed_context_is_refused():
     assert e.value.code == 1
 
 
-def test_too_many_weight_vectors_is_an_argument_error():
-    """The kernel keeps per-warp k-sums for every vector in shared memory; past
-    its limit the call says so (SOAPB_ERR_ARGUMENT) instead of failing a launch."""
+def test_more_weight_vectors_than_one_pass_holds():
+    """Past the kernel's shared-memory limit (about 100 vectors at this
+    definition) the call works in chunks of vectors; every vector's block
+    depends on that vector alone, so the result equals, bit for bit, a call on
+    any subset -- here one straddling a chunk boundary."""
     hp, nl = _case("gauss_2sp", n_atoms=12)
     ctx = Context(hp, legacy_filter_seed=False)
     b = ctx.batch(nl)
-    vecs = torch.zeros((nl.n_sites, 200, ctx.n_soap), dtype=torch.float64, device="cuda")
-    with pytest.raises(_lib.SoapError) as e:
-        ctx.central_hessian(b, vecs)
-    assert e.value.code == 1 and "weight vectors per call" in str(e.value)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    vecs = torch.randn((nl.n_sites, 230, ctx.n_soap), dtype=torch.float64, device="cuda", generator=g)
+    h_all = ctx.central_hessian(b, vecs)
+    for lo, hi in ((0, 5), (95, 110), (220, 230)):
+        h_part = ctx.central_hessian(b, vecs[:, lo:hi].contiguous())
+        assert torch.equal(h_all[:, lo:hi], h_part)
 
 
 def _dropin_args(hp, nl, soap, P):
