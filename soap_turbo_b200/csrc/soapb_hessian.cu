@@ -22,7 +22,7 @@ namespace soapb {
 namespace {
 
 constexpr double kPi = 3.14159265358979323846;
-constexpr int kHessThreads = 256;
+constexpr int kHessThreads = 128;
 constexpr int kHessS = 26;  // k-sums per weight vector in pass B
 constexpr int kHessPC = 8;  // pairs per chunk of pass A
 
@@ -394,6 +394,12 @@ __device__ __forceinline__ double hv_block(const double *S, const double *nh, do
            S[5 + tri] + nh[bb] * S[11 + aa] + S[14 + aa * 3 + bb]);
 }
 
+// Adds x summed over the warp (a fixed shuffle tree) to *dst from lane 0.
+__device__ __forceinline__ void warp_add(double *dst, double x, int lane) {
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  if (lane == 0) *dst += x;
+}
+
 // Per-CTA global scratch of the Hessian kernel (hess_scratch_doubles)
 struct HessScratch {
   double *Gacc;   // (n_max, k_max, 3) complex: G = sum_j d c_nlm / d r_j
@@ -628,64 +634,54 @@ __global__ void __launch_bounds__(kHessThreads) k64_hess(const DevParams P, cons
         const double f0 = fourpi * g[Lg.F + l], f1 = fourpi * g[Lg.F1 + l], f2 = fourpi * g[Lg.F2 + l];
         for (int v = 0; v < nva; ++v) {
           const bool full = v < nvh;
-          dcx a0 = cx(0.0, 0.0), a1 = a0, a2 = a0, b0[3] = {a0, a0, a0}, b1[3] = {a0, a0, a0};
+          double *ws = wsum + v * kHessS;
+          // a-pass: R, R', R'' against Z_v
+          dcx a0 = cx(0.0, 0.0), a1 = a0, a2 = a0;
           if (act) {
             const double2 *zv = (const double2 *)h.Zv + (size_t)v * N * K + k;
-            const double2 *zg = (const double2 *)h.ZGv + ((size_t)v * N * K + k) * 3;
 #pragma unroll 4
-            for (int n = 0; n < N; ++n) {  // unrolled: more of the Z loads in flight
+            for (int n = 0; n < N; ++n) {
               const double2 zz = zv[(size_t)n * K];
               const dcx zc = cx(zz.x, -zz.y);
-              const double r0 = wrad[n], r1 = wrad[N + n];
-              a0 = a0 + r0 * zc;
-              a1 = a1 + r1 * zc;
-              if (full) {
-                a2 = a2 + wrad[2 * N + n] * zc;
-#pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                  const double2 gz = zg[(size_t)n * K * 3 + q];
-                  const dcx gc = cx(gz.x, -gz.y);
-                  b0[q] = b0[q] + r0 * gc;
-                  b1[q] = b1[q] + r1 * gc;
-                }
-              }
+              a0 = a0 + wrad[n] * zc;
+              a1 = a1 + wrad[N + n] * zc;
+              if (full) a2 = a2 + wrad[2 * N + n] * zc;
             }
           }
           const dcx z0 = f0 * a0, z1 = f0 * a1 + f1 * a0;
-          double S[kHessS];
-          S[1] = wmk * (z1 * Om).re;
+          warp_add(ws + 1, wmk * (z1 * Om).re, lane);
 #pragma unroll
-          for (int bb = 0; bb < 3; ++bb) S[23 + bb] = wmk * (z0 * dOm[bb]).re;
-          if (full) {
+          for (int bb = 0; bb < 3; ++bb) warp_add(ws + 23 + bb, wmk * (z0 * dOm[bb]).re, lane);
+          if (!full) continue;
+          {
             const dcx z2 = f0 * a2 + (2.0 * f1) * a1 + f2 * a0;
-            S[0] = wmk * ((z2 - g[Lg.invr] * z1) * Om).re;
+            warp_add(ws + 0, wmk * ((z2 - g[Lg.invr] * z1) * Om).re, lane);
 #pragma unroll
-            for (int bb = 0; bb < 3; ++bb) S[2 + bb] = wmk * (z1 * dOm[bb]).re;
+            for (int bb = 0; bb < 3; ++bb) warp_add(ws + 2 + bb, wmk * (z1 * dOm[bb]).re, lane);
             int e = 5;
 #pragma unroll
             for (int aa = 0; aa < 3; ++aa)
 #pragma unroll
-              for (int bb = aa; bb < 3; ++bb) S[e++] = wmk * (z0 * d2Om[bb * 3 + aa]).re;
+              for (int bb = aa; bb < 3; ++bb) warp_add(ws + e++, wmk * (z0 * d2Om[bb * 3 + aa]).re, lane);
+          }
+          // b-pass: R, R' against ZG_v, one Cartesian component at a time
 #pragma unroll
-            for (int aa = 0; aa < 3; ++aa) {
-              const dcx gg0 = f0 * b0[aa], gg1 = f0 * b1[aa] + f1 * b0[aa];
-              S[11 + aa] = wmk * (gg1 * Om).re;
-#pragma unroll
-              for (int bb = 0; bb < 3; ++bb) S[14 + aa * 3 + bb] = wmk * (gg0 * dOm[bb]).re;
+          for (int q = 0; q < 3; ++q) {
+            dcx b0 = cx(0.0, 0.0), b1 = b0;
+            if (act) {
+              const double2 *zg = (const double2 *)h.ZGv + ((size_t)v * N * K + k) * 3 + q;
+#pragma unroll 4
+              for (int n = 0; n < N; ++n) {
+                const double2 gz = zg[(size_t)n * K * 3];
+                const dcx gc = cx(gz.x, -gz.y);
+                b0 = b0 + wrad[n] * gc;
+                b1 = b1 + wrad[N + n] * gc;
+              }
             }
+            const dcx gg0 = f0 * b0, gg1 = f0 * b1 + f1 * b0;
+            warp_add(ws + 11 + q, wmk * (gg1 * Om).re, lane);
 #pragma unroll
-            for (int e2 = 0; e2 < kHessS; ++e2)
-              for (int o = 16; o > 0; o >>= 1) S[e2] += __shfl_xor_sync(0xffffffffu, S[e2], o);
-            if (lane == 0)
-#pragma unroll
-              for (int e2 = 0; e2 < kHessS; ++e2) wsum[v * kHessS + e2] += S[e2];
-          } else {
-#pragma unroll
-            for (int e2 = 0; e2 < 4; ++e2) {
-              const int ix = e2 == 0 ? 1 : 22 + e2;
-              for (int o = 16; o > 0; o >>= 1) S[ix] += __shfl_xor_sync(0xffffffffu, S[ix], o);
-              if (lane == 0) wsum[v * kHessS + ix] += S[ix];
-            }
+            for (int bb = 0; bb < 3; ++bb) warp_add(ws + 14 + q * 3 + bb, wmk * (gg0 * dOm[bb]).re, lane);
           }
         }
       }
