@@ -57,15 +57,27 @@ def parse():
                     help="time the device neighbour-list builder instead")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="(--hessian) scale the structure's atom count, for profiler captures")
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5],
+                    help="synthetic configuration of our arm (default 2, the headline workload)")
     ap.add_argument("--quick", action="store_true",
                     help="time the two kernels only (no FP64 path, e2e, CPU baseline or peak "
                          "measurement); for profiling runs")
     return ap.parse_args()
 
 
-def workload(rank, seed):
+# the other configurations, for throughput at other sizes (--config; not the headline)
+CONFIG_NAMES = {
+    1: "poly3 alpha=8, l_max=8, 64 atoms in an 8 A cube, d_min=1.2 A (config 1)",
+    3: "512 structures of 16-2048 atoms (log-uniform), rho 0.06-0.14, 3-species poly3gauss as "
+       "config 2 (config 3)",
+    4: "poly3 alpha=8, l_max=8, 32768 atoms, rho=0.11/A^3, d_min=1.2 A (config 4)",
+    5: "3-species poly3gauss as config 2, 262144 atoms (config 5)",
+}
+
+
+def workload(rank, seed, idx=2):
     from soap_turbo_b200 import synthetic as syn
-    return syn.config(2, seed=seed + 7919 * rank)
+    return syn.config(idx, seed=seed + 7919 * rank)
 
 
 def dist_env():
@@ -269,7 +281,8 @@ def run_ours(args):
     from soap_turbo_b200.context import Context
 
     dev = torch.device("cuda", torch.cuda.current_device())
-    w = workload(rank, args.seed)
+    w = workload(rank, args.seed, args.config)
+    wname = WORKLOAD if args.config == 2 else CONFIG_NAMES[args.config]
     nl = w.nl
     ctx = Context(w.hyper)
     b = ctx.batch(nl)
@@ -366,7 +379,9 @@ def run_ours(args):
             print(json.dumps({"metric": METRIC, "value": value, "unit": "envs/s", "n_gpus": ws,
                               "steps": K, "warmup": args.warmup, "ms_per_step": ms_step_max,
                               "kernel_ms": kernel_ms, "autotune": tune,
-                              "quick": True, "gpu_launches": int(launches)}), flush=True)
+                              "quick": True, "gpu_launches": int(launches),
+                              "config": {"workload": wname, "sites_per_gpu": nl.n_sites,
+                                         "pairs_per_gpu": nl.n_pairs}}), flush=True)
         if ws > 1:
             torch.distributed.barrier()
             torch.distributed.destroy_process_group()
@@ -464,7 +479,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_step_max, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded random periodic structures of the configuration's shape)",
-            "config": {"workload": WORKLOAD, "sites_per_gpu": nl.n_sites, "pairs_per_gpu": nl.n_pairs,
+            "config": {"workload": wname, "sites_per_gpu": nl.n_sites, "pairs_per_gpu": nl.n_pairs,
                        "step": "get_soap(do_derivatives, contract) + soap_contract(G), G~N(0,1)",
                        "precision": "FP32 pair/contraction arithmetic; FP64 radial integrals, "
                                     "W transform, i_l and e^{-im phi}; FP64 accumulation of c_nlm "
