@@ -25,6 +25,7 @@ constexpr double kPi = 3.14159265358979323846;
 constexpr int kHessThreads = 128;
 constexpr int kHessS = 26;  // k-sums per weight vector in pass B
 constexpr int kHessPC = 8;  // pairs per chunk of pass A
+constexpr int kHessRed = kHessS + 1;  // row stride of the per-warp transpose buffer
 
 #define CU_RET(x)                         \
   do {                                    \
@@ -394,12 +395,6 @@ __device__ __forceinline__ double hv_block(const double *S, const double *nh, do
            S[5 + tri] + nh[bb] * S[11 + aa] + S[14 + aa * 3 + bb]);
 }
 
-// Adds x summed over the warp (a fixed shuffle tree) to *dst from lane 0.
-__device__ __forceinline__ void warp_add(double *dst, double x, int lane) {
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-  if (lane == 0) *dst += x;
-}
-
 // Per-CTA global scratch of the Hessian kernel (hess_scratch_doubles)
 struct HessScratch {
   double *Gacc;   // (n_max, k_max, 3) complex: G = sum_j d c_nlm / d r_j
@@ -455,9 +450,9 @@ __device__ __forceinline__ double weight(const double *vecs, const double *soap_
 //     derivative hv and the first derivative v . dp_j (what the reference's
 //     self-test rebuilds, here the value used), and from them the
 //     normalisation (:1414-1484).
-// Sums run in a fixed order (pairs to warps by index, a fixed shuffle tree,
-// k rounds in order, warps in index order).
-__global__ void __launch_bounds__(kHessThreads) k64_hess(const DevParams P, const DevBatch B, const double *rad,
+// Sums run in a fixed order (pairs to warps by index, k within a round by lane
+// order through shared memory, k rounds in order, warps in index order).
+__global__ void __launch_bounds__(kHessThreads, 4) k64_hess(const DevParams P, const DevBatch B, const double *rad,
                                                          const double *rad_der, const double *rad_der2,
                                                          const double *geo, const int *good, const double2 *cnk,
                                                          const double *norm, const double *soap, int n_vec,
@@ -474,13 +469,14 @@ __global__ void __launch_bounds__(kHessThreads) k64_hess(const DevParams P, cons
   // by pass B (per warp: the k-sums of its pair (n_vec + 4, kHessS), its radial
   // rows (3 n_max) and its running hsum (n_vec, 9))
   const int sd = 3 + 4 * n_vec + ((3 + 4 * n_vec) & 1);
-  const int per_warp = kHessS * nva + 3 * N + 9 * n_vec;
+  const int per_warp = kHessS * nva + 3 * N + 9 * n_vec + 32 * kHessRed;
   double *sdot = sm;
   double *cab = sm + sd;
   double *crr = cab + (size_t)kHessPC * K * 12;
   double *wsum = sm + sd + (size_t)warp * per_warp;
   double *wrad = wsum + kHessS * nva;
   double *whs = wrad + 3 * N;
+  double *red = whs + 9 * n_vec;  // (32 lanes, kHessRed): the k-sums before their column sums
   const HessScratch h = carve(scratch + scratch_per_cta * blockIdx.x, P, n_vec);
   const double fourpi = 4.0 * kPi;
 
@@ -524,16 +520,36 @@ __global__ void __launch_bounds__(kHessThreads) k64_hess(const DevParams P, cons
         }
       }
       __syncthreads();
-      for (int it = tid; it < N * K; it += kHessThreads) {
-        const int n = it / K, k = it - n * K;
-        double *ga = h.Gacc + (size_t)it * 6;
-        dcx gq[3] = {ldc(ga), ldc(ga + 2), ldc(ga + 4)};
+      // threads over (k, four radial indices): each pair's A, B are loaded once for four n
+      for (int it = tid; it < ((N + 3) >> 2) * K; it += kHessThreads) {
+        const int nb = it / K, k = it - nb * K, n0 = 4 * nb;
+        dcx gq[4][3];
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+#pragma unroll
+          for (int q = 0; q < 3; ++q)
+            gq[t][q] = (n0 + t < N) ? ldc(h.Gacc + ((size_t)(n0 + t) * K + k) * 6 + 2 * q) : cx(0.0, 0.0);
         for (int pp = 0; pp < nc; ++pp) {
-          const double r0 = crr[pp * 2 * N + n], r1 = crr[pp * 2 * N + N + n];
           const double *a = cab + ((size_t)pp * K + k) * 12;
-          for (int q = 0; q < 3; ++q) gq[q] = gq[q] + r1 * ldc(a + 4 * q) + r0 * ldc(a + 4 * q + 2);
+          dcx Aq[3], Bq[3];
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            Aq[q] = ldc(a + 4 * q);
+            Bq[q] = ldc(a + 4 * q + 2);
+          }
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const int n = min(n0 + t, N - 1);  // the tail's extra rows are not stored
+            const double r0 = crr[pp * 2 * N + n], r1 = crr[pp * 2 * N + N + n];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) gq[t][q] = gq[t][q] + r1 * Aq[q] + r0 * Bq[q];
+          }
         }
-        for (int q = 0; q < 3; ++q) stc(ga + 2 * q, gq[q]);
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+          if (n0 + t < N)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) stc(h.Gacc + ((size_t)(n0 + t) * K + k) * 6 + 2 * q, gq[t][q]);
       }
     }
     __syncthreads();
@@ -635,6 +651,7 @@ __global__ void __launch_bounds__(kHessThreads) k64_hess(const DevParams P, cons
         for (int v = 0; v < nva; ++v) {
           const bool full = v < nvh;
           double *ws = wsum + v * kHessS;
+          double *my = red + lane * kHessRed;
           // a-pass: R, R', R'' against Z_v
           dcx a0 = cx(0.0, 0.0), a1 = a0, a2 = a0;
           if (act) {
@@ -649,20 +666,30 @@ __global__ void __launch_bounds__(kHessThreads) k64_hess(const DevParams P, cons
             }
           }
           const dcx z0 = f0 * a0, z1 = f0 * a1 + f1 * a0;
-          warp_add(ws + 1, wmk * (z1 * Om).re, lane);
+          my[1] = wmk * (z1 * Om).re;
 #pragma unroll
-          for (int bb = 0; bb < 3; ++bb) warp_add(ws + 23 + bb, wmk * (z0 * dOm[bb]).re, lane);
-          if (!full) continue;
+          for (int bb = 0; bb < 3; ++bb) my[23 + bb] = wmk * (z0 * dOm[bb]).re;
+          if (!full) {  // the four first-derivative sums: lanes 0..3 add the 32 rows in order
+            __syncwarp();
+            if (lane < 4) {
+              const int e = lane == 0 ? 1 : 22 + lane;
+              double acc = 0.0;
+              for (int r = 0; r < 32; ++r) acc += red[r * kHessRed + e];
+              ws[e] += acc;
+            }
+            __syncwarp();
+            continue;
+          }
           {
             const dcx z2 = f0 * a2 + (2.0 * f1) * a1 + f2 * a0;
-            warp_add(ws + 0, wmk * ((z2 - g[Lg.invr] * z1) * Om).re, lane);
+            my[0] = wmk * ((z2 - g[Lg.invr] * z1) * Om).re;
 #pragma unroll
-            for (int bb = 0; bb < 3; ++bb) warp_add(ws + 2 + bb, wmk * (z1 * dOm[bb]).re, lane);
+            for (int bb = 0; bb < 3; ++bb) my[2 + bb] = wmk * (z1 * dOm[bb]).re;
             int e = 5;
 #pragma unroll
             for (int aa = 0; aa < 3; ++aa)
 #pragma unroll
-              for (int bb = aa; bb < 3; ++bb) warp_add(ws + e++, wmk * (z0 * d2Om[bb * 3 + aa]).re, lane);
+              for (int bb = aa; bb < 3; ++bb) my[e++] = wmk * (z0 * d2Om[bb * 3 + aa]).re;
           }
           // b-pass: R, R' against ZG_v, one Cartesian component at a time
 #pragma unroll
@@ -679,10 +706,18 @@ __global__ void __launch_bounds__(kHessThreads) k64_hess(const DevParams P, cons
               }
             }
             const dcx gg0 = f0 * b0, gg1 = f0 * b1 + f1 * b0;
-            warp_add(ws + 11 + q, wmk * (gg1 * Om).re, lane);
+            my[11 + q] = wmk * (gg1 * Om).re;
 #pragma unroll
-            for (int bb = 0; bb < 3; ++bb) warp_add(ws + 14 + q * 3 + bb, wmk * (gg0 * dOm[bb]).re, lane);
+            for (int bb = 0; bb < 3; ++bb) my[14 + q * 3 + bb] = wmk * (gg0 * dOm[bb]).re;
           }
+          // the 26 sums over the warp's k: lane e adds the 32 rows of column e in order
+          __syncwarp();
+          if (lane < kHessS) {
+            double acc = 0.0;
+            for (int r = 0; r < 32; ++r) acc += red[r * kHessRed + lane];
+            ws[lane] += acc;
+          }
+          __syncwarp();
         }
       }
       __syncwarp();
@@ -734,7 +769,8 @@ size_t hess_geo_doubles(const DevParams &P) { return (size_t)GeoLayout(P.l_max).
 size_t hess_smem_bytes(const DevParams &P, int n_vec) {
   const size_t nw = kHessThreads / 32, sd = 3 + 4 * (size_t)n_vec;
   const size_t pass_a = (size_t)kHessPC * (12 * (size_t)P.k_max + 2 * (size_t)P.n_max);
-  const size_t pass_b = nw * (kHessS * (size_t)(n_vec + 4) + 3 * (size_t)P.n_max + 9 * (size_t)n_vec);
+  const size_t pass_b =
+      nw * (kHessS * (size_t)(n_vec + 4) + 3 * (size_t)P.n_max + 9 * (size_t)n_vec + 32 * (size_t)kHessRed);
   return sizeof(double) * (sd + (sd & 1) + (pass_a > pass_b ? pass_a : pass_b));
 }
 
