@@ -445,13 +445,13 @@ __device__ __forceinline__ double weight(const double *vecs, const double *soap_
 //     sum_j d c / d r_j = G);
 //  Z  every weight vector v spread back through the compression into its
 //     S_v(n, n', l) and applied to c_nlm (Z_v) and to G (ZG_v) (:1336-1376);
-//  B  one warp per pair, lanes over k: Z_v and ZG_v contracted with the pair's
+//  B  one half-warp per pair, lanes over k: Z_v and ZG_v contracted with the pair's
 //     R_n, R'_n, R''_n and Omega, dOmega, d2Omega (:1378-1412) give the second
 //     derivative hv and the first derivative v . dp_j (what the reference's
 //     self-test rebuilds, here the value used), and from them the
 //     normalisation (:1414-1484).
-// Sums run in a fixed order (pairs to warps by index, k within a round by lane
-// order through shared memory, k rounds in order, warps in index order).
+// Sums run in a fixed order (pairs to half-warps by index, k within a round by
+// lane order through shared memory, k rounds in order, half-warps in order).
 __global__ void __launch_bounds__(kHessThreads, 4) k64_hess(const DevParams P, const DevBatch B, const double *rad,
                                                          const double *rad_der, const double *rad_der2,
                                                          const double *geo, const int *good, const double2 *cnk,
@@ -466,17 +466,18 @@ __global__ void __launch_bounds__(kHessThreads, 4) k64_hess(const DevParams P, c
   const GeoLayout Lg(P.l_max);
   // shared: the site's dot products (3 + 4 n_vec), then a region used by pass
   // A (a chunk of kHessPC pairs: their A, B factors (K, 12) and R, R' rows) and
-  // by pass B (per warp: the k-sums of its pair (n_vec + 4, kHessS), its radial
-  // rows (3 n_max) and its running hsum (n_vec, 9))
+  // by pass B (per half-warp: the k-sums of its pair (n_vec + 4, kHessS), its
+  // radial rows (3 n_max), its running hsum (n_vec, 9) and its transpose buffer)
   const int sd = 3 + 4 * n_vec + ((3 + 4 * n_vec) & 1);
-  const int per_warp = kHessS * nva + 3 * N + 9 * n_vec + 32 * kHessRed;
+  const int per_half = kHessS * nva + 3 * N + 9 * n_vec + 16 * kHessRed;  // per half-warp, pass B
   double *sdot = sm;
   double *cab = sm + sd;
   double *crr = cab + (size_t)kHessPC * K * 12;
-  double *wsum = sm + sd + (size_t)warp * per_warp;
+  const int half = lane >> 4, hl = lane & 15, n_halves = 2 * n_warps;
+  double *wsum = sm + sd + (size_t)(2 * warp + half) * per_half;
   double *wrad = wsum + kHessS * nva;
   double *whs = wrad + 3 * N;
-  double *red = whs + 9 * n_vec;  // (32 lanes, kHessRed): the k-sums before their column sums
+  double *red = whs + 9 * n_vec;  // (16 lanes, kHessRed): the k-sums before their column sums
   const HessScratch h = carve(scratch + scratch_per_cta * blockIdx.x, P, n_vec);
   const double fourpi = 4.0 * kPi;
 
@@ -622,36 +623,46 @@ __global__ void __launch_bounds__(kHessThreads, 4) k64_hess(const DevParams P, c
       }
       __syncthreads();
     }
-    // ---- B: one warp per pair, lanes over k (rounds of 32).  Per weight vector
-    // the k-sums below give the block (:1378-1412, reassociated over k):
+    // ---- B: one half-warp per pair, lanes over k (rounds of 16).  Per weight
+    // vector the k-sums below give the block (:1378-1412, reassociated over k):
     //   S1 = sum w Re[(z2 - z1/r) Om]   S2 = sum w Re[z1 Om]    S3_b = sum w Re[z1 dOm_b]
     //   S4_ab = sum w Re[z0 d2Om_ab]    S5_a = sum w Re[gg1_a Om]
     //   S6_ab = sum w Re[gg0_a dOm_b]   S7_b = sum w Re[z0 dOm_b]
     //   hv(b, a) = -(n_a n_b S1 + [a = b] S2 / r + n_a S3_b + n_b S3_a + S4_ab + n_b S5_a + S6_ab)
     //   v . dp_j (b) = n_b S2 + S7_b
-    for (int t = lane; t < 9 * n_vec; t += 32) whs[t] = 0.0;
-    for (int j = p0 + 1 + warp; j < p1; j += n_warps) {
-      if (!good[j]) continue;
-      const double *g = geo + (size_t)j * Lg.size;
-      for (int t = lane; t < 3 * N; t += 32) {
+    // The two halves of a warp read the same Z rows (same k), for two pairs.
+    for (int t = hl; t < 9 * n_vec; t += 16) whs[t] = 0.0;
+    for (int jb = p0 + 1 + 2 * warp; jb < p1; jb += 2 * n_warps) {  // the same trip count for both halves
+      const int j = jb + half;
+      const bool pv = j < p1 && good[j];  // this half has a pair
+      const double *g = geo + (size_t)(pv ? j : 0) * Lg.size;
+      for (int t = hl; t < 3 * N; t += 16) {
         const int w = t / N, n = t - w * N;
-        wrad[t] = (w == 0 ? rad : (w == 1 ? rad_der : rad_der2))[(size_t)j * N + n];
+        wrad[t] = pv ? (w == 0 ? rad : (w == 1 ? rad_der : rad_der2))[(size_t)j * N + n] : 0.0;
       }
-      for (int t = lane; t < kHessS * nva; t += 32) wsum[t] = 0.0;
+      for (int t = hl; t < kHessS * nva; t += 16) wsum[t] = 0.0;
       __syncwarp();
-      for (int k0 = 0; k0 < K; k0 += 32) {
-        const int k = k0 + lane;
-        const bool act = k < K;
+      for (int k0 = 0; k0 < K; k0 += 16) {
+        const int k = k0 + hl;
+        const bool act = pv && k < K;
         const int kc = act ? k : 0;
         const int l = l_of_k(kc), m = kc - l * (l + 1) / 2;
-        dcx Om, dOm[3], d2Om[9];
-        omega_k(g, Lg, kc, l, m, (m & 1) ? -P.preflm64[kc] : P.preflm64[kc], true, Om, dOm, d2Om);
-        const double wmk = act ? ((m > 0) ? 2.0 : 1.0) : 0.0;
-        const double f0 = fourpi * g[Lg.F + l], f1 = fourpi * g[Lg.F1 + l], f2 = fourpi * g[Lg.F2 + l];
+        dcx Om = cx(0.0, 0.0), dOm[3], d2Om[9];
+        for (int e = 0; e < 3; ++e) dOm[e] = Om;
+        for (int e = 0; e < 9; ++e) d2Om[e] = Om;
+        double wmk = 0.0, f0 = 0.0, f1 = 0.0, f2 = 0.0, invr = 0.0;
+        if (act) {
+          omega_k(g, Lg, kc, l, m, (m & 1) ? -P.preflm64[kc] : P.preflm64[kc], true, Om, dOm, d2Om);
+          wmk = (m > 0) ? 2.0 : 1.0;
+          f0 = fourpi * g[Lg.F + l];
+          f1 = fourpi * g[Lg.F1 + l];
+          f2 = fourpi * g[Lg.F2 + l];
+          invr = g[Lg.invr];
+        }
         for (int v = 0; v < nva; ++v) {
           const bool full = v < nvh;
           double *ws = wsum + v * kHessS;
-          double *my = red + lane * kHessRed;
+          double *my = red + hl * kHessRed;
           // a-pass: R, R', R'' against Z_v
           dcx a0 = cx(0.0, 0.0), a1 = a0, a2 = a0;
           if (act) {
@@ -669,12 +680,12 @@ __global__ void __launch_bounds__(kHessThreads, 4) k64_hess(const DevParams P, c
           my[1] = wmk * (z1 * Om).re;
 #pragma unroll
           for (int bb = 0; bb < 3; ++bb) my[23 + bb] = wmk * (z0 * dOm[bb]).re;
-          if (!full) {  // the four first-derivative sums: lanes 0..3 add the 32 rows in order
+          if (!full) {  // the four first-derivative sums: lanes 0..3 of each half add its 16 rows
             __syncwarp();
-            if (lane < 4) {
-              const int e = lane == 0 ? 1 : 22 + lane;
+            if (hl < 4) {
+              const int e = hl == 0 ? 1 : 22 + hl;
               double acc = 0.0;
-              for (int r = 0; r < 32; ++r) acc += red[r * kHessRed + e];
+              for (int r = 0; r < 16; ++r) acc += red[r * kHessRed + e];
               ws[e] += acc;
             }
             __syncwarp();
@@ -682,7 +693,7 @@ __global__ void __launch_bounds__(kHessThreads, 4) k64_hess(const DevParams P, c
           }
           {
             const dcx z2 = f0 * a2 + (2.0 * f1) * a1 + f2 * a0;
-            my[0] = wmk * ((z2 - g[Lg.invr] * z1) * Om).re;
+            my[0] = wmk * ((z2 - invr * z1) * Om).re;
 #pragma unroll
             for (int bb = 0; bb < 3; ++bb) my[2 + bb] = wmk * (z1 * dOm[bb]).re;
             int e = 5;
@@ -710,12 +721,12 @@ __global__ void __launch_bounds__(kHessThreads, 4) k64_hess(const DevParams P, c
 #pragma unroll
             for (int bb = 0; bb < 3; ++bb) my[14 + q * 3 + bb] = wmk * (gg0 * dOm[bb]).re;
           }
-          // the 26 sums over the warp's k: lane e adds the 32 rows of column e in order
+          // the 26 sums over the half's k: lane e adds the 16 rows of column e in order
           __syncwarp();
-          if (lane < kHessS) {
+          for (int e = hl; e < kHessS; e += 16) {
             double acc = 0.0;
-            for (int r = 0; r < 32; ++r) acc += red[r * kHessRed + lane];
-            ws[lane] += acc;
+            for (int r = 0; r < 16; ++r) acc += red[r * kHessRed + e];
+            ws[e] += acc;
           }
           __syncwarp();
         }
@@ -723,31 +734,33 @@ __global__ void __launch_bounds__(kHessThreads, 4) k64_hess(const DevParams P, c
       __syncwarp();
       // the normalisation (:1414-1484): t2 = p . dp_j, c12(b, a) = dp1(:, a) . dp_j(:, b),
       // u2 = w . dp_j
-      const double invr = g[Lg.invr];
-      const double nh[3] = {g[Lg.nh], g[Lg.nh + 1], g[Lg.nh + 2]};
-      for (int t = lane; t < 9 * n_vec; t += 32) {
-        const int v = t / 9, e = t - v * 9, bb = e / 3, aa = e - bb * 3;
-        const double *t1 = sdot, *dv = sdot + 3 + 4 * v;
-        const double wp = dv[0], *u1 = dv + 1;
-        const double *Sp = wsum + n_vec * kHessS, *Sv = wsum + v * kHessS;
-        const double t2b = nh[bb] * Sp[1] + Sp[23 + bb], u2b = nh[bb] * Sv[1] + Sv[23 + bb];
-        const double *Sc = wsum + (n_vec + 1 + aa) * kHessS;
-        const double c12 = nh[bb] * Sc[1] + Sc[23 + bb];
-        const double hvv = hv_block(Sv, nh, invr, aa, bb), hvp = hv_block(Sp, nh, invr, aa, bb);
-        const double hval = hvv * invs - (u1[aa] * t2b + u2b * t1[aa]) * invs3 - wp * (c12 + hvp) * invs3 +
-                            3.0 * wp * t1[aa] * t2b * invs5;
-        hess[((size_t)j * n_vec + v) * 9 + e] = hval;
-        whs[t] += hval;
+      if (pv) {
+        const double invr = g[Lg.invr];
+        const double nh[3] = {g[Lg.nh], g[Lg.nh + 1], g[Lg.nh + 2]};
+        for (int t = hl; t < 9 * n_vec; t += 16) {
+          const int v = t / 9, e = t - v * 9, bb = e / 3, aa = e - bb * 3;
+          const double *t1 = sdot, *dv = sdot + 3 + 4 * v;
+          const double wp = dv[0], *u1 = dv + 1;
+          const double *Sp = wsum + n_vec * kHessS, *Sv = wsum + v * kHessS;
+          const double t2b = nh[bb] * Sp[1] + Sp[23 + bb], u2b = nh[bb] * Sv[1] + Sv[23 + bb];
+          const double *Sc = wsum + (n_vec + 1 + aa) * kHessS;
+          const double c12 = nh[bb] * Sc[1] + Sc[23 + bb];
+          const double hvv = hv_block(Sv, nh, invr, aa, bb), hvp = hv_block(Sp, nh, invr, aa, bb);
+          const double hval = hvv * invs - (u1[aa] * t2b + u2b * t1[aa]) * invs3 - wp * (c12 + hvp) * invs3 +
+                              3.0 * wp * t1[aa] * t2b * invs5;
+          hess[((size_t)j * n_vec + v) * 9 + e] = hval;
+          whs[t] += hval;
+        }
       }
       __syncwarp();
     }
     __syncthreads();
-    // the self pair: minus the sum of the others (:1488-1495), warps in order;
-    // pairs the Hessian skips keep the zero blocks the launcher cleared
+    // the self pair: minus the sum of the others (:1488-1495), half-warps in
+    // order; pairs the Hessian skips keep the zero blocks the launcher cleared
     if (p1 > p0)
       for (int t = tid; t < 9 * n_vec; t += kHessThreads) {
         double s = 0.0;
-        for (int w = 0; w < n_warps; ++w) s += sm[sd + (size_t)w * per_warp + kHessS * nva + 3 * N + t];
+        for (int w = 0; w < n_halves; ++w) s += sm[sd + (size_t)w * per_half + kHessS * nva + 3 * N + t];
         hess[((size_t)p0 * n_vec) * 9 + t] = -s;
       }
   }
@@ -770,7 +783,7 @@ size_t hess_smem_bytes(const DevParams &P, int n_vec) {
   const size_t nw = kHessThreads / 32, sd = 3 + 4 * (size_t)n_vec;
   const size_t pass_a = (size_t)kHessPC * (12 * (size_t)P.k_max + 2 * (size_t)P.n_max);
   const size_t pass_b =
-      nw * (kHessS * (size_t)(n_vec + 4) + 3 * (size_t)P.n_max + 9 * (size_t)n_vec + 32 * (size_t)kHessRed);
+      2 * nw * (kHessS * (size_t)(n_vec + 4) + 3 * (size_t)P.n_max + 9 * (size_t)n_vec + 16 * (size_t)kHessRed);
   return sizeof(double) * (sd + (sd & 1) + (pass_a > pass_b ? pass_a : pass_b));
 }
 
