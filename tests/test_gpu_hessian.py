@@ -90,6 +90,40 @@ def test_many_weight_vectors_and_repeat_calls():
     assert max_rel_err(h1.cpu().numpy(), href) <= FP64_TOL
 
 
+@pytest.mark.parametrize("basis", ["poly3", "poly3gauss"])
+def test_edge_sites(basis):
+    """A site with only itself, a neighbour beyond the cutoff (its block stays
+    zero), neighbours on the poles and at a very short distance, a site whose
+    descriptor is zero (poly3gauss, central weight 0, nothing in range: the
+    norm floor), and ordinary sites beside them."""
+    import dataclasses
+    from test_gpu_edge import make_nl, random_sites
+    rng = np.random.default_rng(11)
+    if basis == "poly3":
+        hp = syn.Hyper(alpha_max=[6], l_max=5, basis="poly3")
+        sites = [(0, []), (0, [(6.0, 1.0, 0.5, 1), (2.0, 0.0, 0.0, 1), (3.0, np.pi, 1.0, 1)]),
+                 (0, [(0.05, 1.2, -2.0, 1), (4.99, 0.7, 0.3, 1)])] + random_sites(rng, 4, 1, 5, 20)
+        nl = make_nl(sites, 1)
+    else:
+        hp = syn.Hyper(alpha_max=[5, 5, 5], l_max=5, basis="poly3gauss", central_weight=[1.0, 0.0, 1.0])
+        sites = [(1, []), (1, [(7.0, 0.3, 0.2, 1)]), (0, [(1.5, 0.0, 1.0, 4), (2.5, np.pi, 0.0, 2)])] + \
+            random_sites(rng, 4, 3, 5, 20)
+        nl = make_nl(sites, 3)
+    ctx = Context(hp, legacy_filter_seed=False)
+    W, S = ctx.basis()
+    ref, vecs, href = _oracle(hp, nl, W, S, 2, seed=3)
+    b = ctx.batch(nl)
+    hess = ctx.central_hessian(b, torch.as_tensor(vecs).cuda(),
+                               soap=torch.as_tensor(np.ascontiguousarray(ref.soap)).cuda()).cpu().numpy()
+    ctx.check_inputs()
+    assert np.isfinite(hess).all()
+    assert max_rel_err(hess, href) <= FP64_TOL
+    off = np.concatenate([[0], np.cumsum(nl.n_neigh)])
+    assert np.abs(hess[off[0]:off[1]]).max() == 0.0  # a site with only itself
+    if basis == "poly3":
+        assert np.abs(hess[off[1] + 1]).max() == 0.0  # the neighbour beyond the cutoff
+
+
 def test_legacy_seed_context_is_refused():
     hp, nl = _case("gauss_2sp", n_atoms=12)
     ctx = Context(hp, legacy_filter_seed=True)
