@@ -667,7 +667,7 @@ __global__ void __launch_bounds__(kHessThreads, 4) k64_hess(const DevParams P, c
           dcx a0 = cx(0.0, 0.0), a1 = a0, a2 = a0;
           if (act) {
             const double2 *zv = (const double2 *)h.Zv + (size_t)v * N * K + k;
-#pragma unroll 4
+#pragma unroll 8
             for (int n = 0; n < N; ++n) {
               const double2 zz = zv[(size_t)n * K];
               const dcx zc = cx(zz.x, -zz.y);
@@ -708,7 +708,7 @@ __global__ void __launch_bounds__(kHessThreads, 4) k64_hess(const DevParams P, c
             dcx b0 = cx(0.0, 0.0), b1 = b0;
             if (act) {
               const double2 *zg = (const double2 *)h.ZGv + ((size_t)v * N * K + k) * 3 + q;
-#pragma unroll 4
+#pragma unroll 8
               for (int n = 0; n < N; ++n) {
                 const double2 gz = zg[(size_t)n * K * 3];
                 const dcx gc = cx(gz.x, -gz.y);
