@@ -30,6 +30,8 @@ CASES = {
                          amplitude_scaling=2.0, atom_sigma_r_scaling=0.1),
     # alpha above 8: the wide radial instantiation
     "gauss_alpha10": dict(alpha_max=[10], l_max=5, basis="poly3gauss", radial_enhancement=1),
+    # a Darby compression mode: its map spreads each output over several (n, n', l)
+    "gauss_3sp_darby": dict(alpha_max=[4, 4, 4], l_max=4, basis="poly3gauss", compress_mode="1_1"),
 }
 TOL = {"gauss_alpha10": 5e-7}
 
@@ -132,6 +134,13 @@ def test_legacy_seed_context_is_refused():
     with pytest.raises(_lib.SoapError) as e:
         ctx.central_hessian(b, vecs)
     assert e.value.code == 1
+    # poly3operator has no second radial derivatives (src/soap_turbo.f90:485-489)
+    op = syn.Hyper(alpha_max=[4, 4], l_max=4, basis="poly3operator")
+    ctx = Context(op, legacy_filter_seed=False)
+    with pytest.raises(_lib.SoapError) as e:
+        ctx.central_hessian(ctx.batch(nl), torch.zeros((nl.n_sites, 1, ctx.n_soap), dtype=torch.float64,
+                                                       device="cuda"))
+    assert e.value.code == 5
 
 
 def test_more_weight_vectors_than_one_pass_holds():
