@@ -1938,12 +1938,19 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
     CU(cudaMemcpyAsync(soap_cart_der, d.cart.p, 8 * (size_t)n_atom_pairs * n_soap * 3,
                        cudaMemcpyDeviceToHost, s));
   if (do_timing) cudaEventRecord(ev[3], s);
-  // the prep error word comes back with the same wait
+  // the prep error word comes back with the same wait; the compute stream
+  // also waits for the last soap rows on copy_out, so one synchronisation
+  // covers both streams (both are synchronised if the join cannot be made)
   if ((rc = dropin_streams(d, 0))) return rc;
+  bool joined = false;
+  if (soap_copied) {
+    cudaEvent_t ej = d.evs[d.chunk.size() - 1];  // unused by the chunks (they take evs[0 .. nch))
+    joined = cudaEventRecord(ej, d.copy_out) == cudaSuccess && cudaStreamWaitEvent(s, ej, 0) == cudaSuccess;
+  }
   *d.err_host = 0;
   if (c->err.p) CU(cudaMemcpyAsync(d.err_host, c->err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   const cudaError_t es = cudaStreamSynchronize(s);
-  const cudaError_t eo = soap_copied ? cudaStreamSynchronize(d.copy_out) : cudaSuccess;
+  const cudaError_t eo = (soap_copied && !joined) ? cudaStreamSynchronize(d.copy_out) : cudaSuccess;
   CU(es);
   CU(eo);
   if ((rc = input_status(*d.err_host, nullptr))) return rc;
@@ -2005,7 +2012,7 @@ int soapb_soap_contract(const double *soap, const double *G, double sgn, double 
   if ((rc = d.G.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
   if ((int)d.chunk.size() < 2 || d.chunk.back() != n_sites) plan_chunks(d, n_sites, false);
   const int nch = (int)d.chunk.size() - 1;
-  if ((rc = dropin_streams(d, 2 * nch))) return rc;
+  if ((rc = dropin_streams(d, 2 * nch + 1))) return rc;
   double *dS = d.soap.as<double>(), *dG = d.G.as<double>(), *dP = d.pair.as<double>();
   CU(cudaEventRecord(d.evs[0], s));  // the copies in must not overwrite what earlier work still reads
   CU(cudaStreamWaitEvent(d.copy_in, d.evs[0], 0));
@@ -2033,7 +2040,16 @@ int soapb_soap_contract(const double *soap, const double *G, double sgn, double 
     return SOAPB_OK;
   };
   rc = ctx_contract(d.ctx, &d.batch, dS, dG, SOAPB_G_SITE_FASTEST, sgn, dP, &ch);
-  // whatever ran, no copy may still be in flight when this returns
+  // whatever ran, no copy may still be in flight when this returns.  The
+  // compute stream has waited for every chunk's copies in; made to wait for the
+  // last pair forces out as well, its synchronisation covers all three streams.
+  if (rc == 0) {
+    cudaEvent_t ej = d.evs[2 * nch];
+    if (cudaEventRecord(ej, d.copy_out) == cudaSuccess && cudaStreamWaitEvent(s, ej, 0) == cudaSuccess) {
+      CU(cudaStreamSynchronize(s));
+      return SOAPB_OK;
+    }
+  }
   const cudaError_t e1 = cudaStreamSynchronize(d.copy_in), e2 = cudaStreamSynchronize(s),
                     e3 = cudaStreamSynchronize(d.copy_out);
   if (rc) return rc;
