@@ -849,11 +849,15 @@ int input_status(unsigned long long w, int64_t *bad_pair) {
 
 // Site chunks for the drop-in layer's overlap of copies with the site kernels:
 // the site kernel runs once per chunk [bounds[i], bounds[i + 1]); before(i) runs
-// before chunk i's launch (to make the stream wait for its inputs) and after(i)
-// after it (to start the copy of its outputs).
+// before chunk i's launches (to make the stream wait for its inputs) and
+// after(i) after them (to start the copy of its outputs).  With site_off (the
+// host's CSR offsets) the descriptor's pair kernel runs per chunk too, on the
+// chunk's pairs [site_off[bounds[i]], site_off[bounds[i + 1]]), so that a
+// chunk's pair inputs may arrive while earlier chunks compute.
 struct SiteChunks {
   int n = 1;
   const int *bounds = nullptr;
+  const long long *site_off = nullptr;
   std::function<int(int)> before, after;
 };
 
@@ -873,8 +877,9 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
   }
   LaunchCfg cfg = site_cfg(c, false);
   // the pair kernel also scans n_neigh into the CSR offsets, packs the mask
-  // and checks the inputs
-  if (b->n_atom_pairs > 0 || b->n_sites > 0) {
+  // and checks the inputs (its first launch scans, when it runs per chunk)
+  const bool pair_chunks = ch && ch->site_off && b->n_sites > 0;
+  if (!pair_chunks && (b->n_atom_pairs > 0 || b->n_sites > 0)) {
     TimedLaunch tl(c, SOAPB_KERNEL_PAIR);
     CU(launch_pair(P, B, c->stream, keep));
     c->launches += 1;
@@ -884,6 +889,13 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
     B.site_lo = ch ? ch->bounds[i] : 0;
     B.site_hi = ch ? ch->bounds[i + 1] : b->n_sites;
     if (ch && ch->before && (rc = ch->before(i))) return rc;
+    if (pair_chunks) {
+      const long long p0 = ch->site_off[B.site_lo], p1 = ch->site_off[B.site_hi];
+      if (p0 < 0 || p0 > p1 || p1 > b->n_atom_pairs) return fail(SOAPB_ERR_ARGUMENT, "bad chunk pair range");
+      TimedLaunch tl(c, SOAPB_KERNEL_PAIR);
+      CU(launch_pair(P, B, c->stream, keep, (int)p0, (int)p1, i == 0));
+      c->launches += 1;
+    }
     {
       TimedLaunch tl(c, SOAPB_KERNEL_DESCRIPTOR);
       CU(launch_descriptor(P, B, cfg, d_soap, keep ? c->keep_c.as<float>() : nullptr,
@@ -1647,16 +1659,26 @@ struct DropIn {
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   std::vector<cudaEvent_t> evs;
   std::vector<int> chunk;                  // site chunk bounds of the last get_soap
+  std::vector<int> cchunk;                 // and of soap_contract
   std::vector<long long> host_off;         // its CSR offsets
   unsigned long long *err_host = nullptr;  // pinned copy of the prep error word
 };
 
-// Site chunks of a drop-in call: about 384 sites each, at most 8 (1 chunk for
-// small batches, and with do_timing, whose per-phase times need the phases apart).
-void plan_chunks(DropIn &d, int n_sites, bool whole) {
-  const int n = whole ? 1 : std::max(1, std::min(8, n_sites / 384));
-  d.chunk.resize(n + 1);
-  for (int i = 0; i <= n; ++i) d.chunk[i] = (int)((long long)n_sites * i / n);
+// Site chunks of the drop-in calls, at most 8.  In get_soap each chunk's pair
+// and site kernels run one after the other on the compute stream, and a small
+// chunk runs them well below the GPU's rate (its grids fill few SMs), so the
+// chunks are about 512 sites.  In soap_contract the copies in set the pace and
+// every chunk's kernels but the last run behind them: its chunks are about 384
+// sites, and the last is half the size of the others, to shorten what remains
+// after the last copy in.
+void plan_chunks(std::vector<int> &bounds, int n_sites, bool contract) {
+  const int n = std::max(1, std::min(8, n_sites / (contract ? 384 : 512)));
+  const bool short_last = contract && n > 1;
+  const long long weight_sum = short_last ? 2LL * n - 1 : n;
+  bounds.resize(n + 1);
+  for (int i = 0; i < n; ++i)
+    bounds[i] = (int)((long long)n_sites * (short_last ? 2LL * i : i) / weight_sum);
+  bounds[n] = n_sites;
 }
 
 int dropin_streams(DropIn &d, int n_events) {
@@ -1706,6 +1728,36 @@ int upload(DBuf &b, const T *src, size_t n, cudaStream_t s) {
   int rc = b.ensure(sizeof(T) * (n + 1));
   if (rc) return rc;
   if (n) CU(cudaMemcpyAsync(b.p, src, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+  return SOAPB_OK;
+}
+
+// get_soap's inputs on the copy-in stream, in the site chunks d.chunk: the
+// per-site arrays first, then each chunk's pair rows of mask, rjs, thetas and
+// phis, after which evs[i] marks chunk i's inputs as present.  The buffers
+// are sized by the caller; the copies wait for the work already queued on the
+// compute stream, which may still read the previous call's inputs.
+int copy_in_chunks(DropIn &d, int n_sites, int n_species, int max_mult, int n_pairs, const int32_t *n_neigh,
+                   const int32_t *species, const int32_t *species_mult, const uint8_t *mask, const double *rjs,
+                   const double *thetas, const double *phis) {
+  const int nch = (int)d.chunk.size() - 1;
+  CU(cudaEventRecord(d.evs[0], d.stream));
+  CU(cudaStreamWaitEvent(d.copy_in, d.evs[0], 0));
+  CU(cudaMemcpyAsync(d.n_neigh.p, n_neigh, 4 * (size_t)n_sites, cudaMemcpyHostToDevice, d.copy_in));
+  CU(cudaMemcpyAsync(d.species.p, species, 4 * (size_t)n_sites * max_mult, cudaMemcpyHostToDevice, d.copy_in));
+  CU(cudaMemcpyAsync(d.species_mult.p, species_mult, 4 * (size_t)n_sites, cudaMemcpyHostToDevice, d.copy_in));
+  for (int i = 0; i < nch; ++i) {
+    const size_t p0 = (size_t)d.host_off[d.chunk[i]], p1 = (size_t)d.host_off[d.chunk[i + 1]];
+    if (p1 > p0) {
+      // mask(n_pairs, n_species) column-major: the chunk's rows of every column
+      CU(cudaMemcpy2DAsync(d.mask.as<uint8_t>() + p0, (size_t)n_pairs, mask + p0, (size_t)n_pairs, p1 - p0,
+                           (size_t)n_species, cudaMemcpyHostToDevice, d.copy_in));
+      CU(cudaMemcpyAsync(d.rjs.as<double>() + p0, rjs + p0, 8 * (p1 - p0), cudaMemcpyHostToDevice, d.copy_in));
+      CU(cudaMemcpyAsync(d.thetas.as<double>() + p0, thetas + p0, 8 * (p1 - p0), cudaMemcpyHostToDevice,
+                         d.copy_in));
+      CU(cudaMemcpyAsync(d.phis.as<double>() + p0, phis + p0, 8 * (p1 - p0), cudaMemcpyHostToDevice, d.copy_in));
+    }
+    CU(cudaEventRecord(d.evs[i], d.copy_in));
+  }
   return SOAPB_OK;
 }
 
@@ -1882,14 +1934,41 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
   if (do_timing)
     for (auto &e : ev) cudaEventCreate(&e);
   if (do_timing) cudaEventRecord(ev[0], s);
-  if ((rc = upload(d.n_neigh, n_neigh, n_sites, s))) return rc;
-  if ((rc = upload(d.species, species, (size_t)n_sites * max_species_multiplicity, s))) return rc;
-  if ((rc = upload(d.species_mult, species_multiplicity, n_sites, s))) return rc;
-  if ((rc = upload(d.mask, mask, (size_t)n_atom_pairs * n_species, s))) return rc;
-  if ((rc = upload(d.rjs, rjs, n_atom_pairs, s))) return rc;
-  if ((rc = upload(d.thetas, thetas, n_atom_pairs, s))) return rc;
-  if ((rc = upload(d.phis, phis, n_atom_pairs, s))) return rc;
-  if ((rc = d.soap.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
+  // The mixed path without do_timing runs in site chunks: chunk i's pair
+  // inputs come in on copy_in (evs[i]), its pair and site kernels run on the
+  // compute stream once they are there, and its soap rows go out on copy_out
+  // (evs[nch + i]) while later chunks compute.  Otherwise everything is copied
+  // in on the compute stream first.
+  const bool chunked = !fp64 && !do_timing && n_sites > 0;
+  int nch = 1;
+  if (chunked) {
+    plan_chunks(d.chunk, n_sites, false);
+    nch = (int)d.chunk.size() - 1;
+    if ((rc = dropin_streams(d, 2 * nch + 1))) return rc;
+    if ((rc = d.n_neigh.ensure(4 * ((size_t)n_sites + 1)))) return rc;
+    if ((rc = d.species.ensure(4 * ((size_t)n_sites * max_species_multiplicity + 1)))) return rc;
+    if ((rc = d.species_mult.ensure(4 * ((size_t)n_sites + 1)))) return rc;
+    if ((rc = d.mask.ensure((size_t)n_atom_pairs * n_species + 1))) return rc;
+    if ((rc = d.rjs.ensure(8 * ((size_t)n_atom_pairs + 1)))) return rc;
+    if ((rc = d.thetas.ensure(8 * ((size_t)n_atom_pairs + 1)))) return rc;
+    if ((rc = d.phis.ensure(8 * ((size_t)n_atom_pairs + 1)))) return rc;
+    if ((rc = d.soap.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
+    const int copied = copy_in_chunks(d, n_sites, n_species, max_species_multiplicity, n_atom_pairs, n_neigh,
+                                      species, species_multiplicity, mask, rjs, thetas, phis);
+    if (copied) {
+      cudaStreamSynchronize(d.copy_in);  // no copy from the caller's arrays outlives the call
+      return copied;
+    }
+  } else {
+    if ((rc = upload(d.n_neigh, n_neigh, n_sites, s))) return rc;
+    if ((rc = upload(d.species, species, (size_t)n_sites * max_species_multiplicity, s))) return rc;
+    if ((rc = upload(d.species_mult, species_multiplicity, n_sites, s))) return rc;
+    if ((rc = upload(d.mask, mask, (size_t)n_atom_pairs * n_species, s))) return rc;
+    if ((rc = upload(d.rjs, rjs, n_atom_pairs, s))) return rc;
+    if ((rc = upload(d.thetas, thetas, n_atom_pairs, s))) return rc;
+    if ((rc = upload(d.phis, phis, n_atom_pairs, s))) return rc;
+    if ((rc = d.soap.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
+  }
   soapb_batch &bt = d.batch;
   bt.n_sites = n_sites;
   bt.n_atom_pairs = n_atom_pairs;
@@ -1907,28 +1986,33 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
   if (fp64) {
     if (keep_cart && (rc = d.cart.ensure(8 * ((size_t)n_atom_pairs * n_soap * 3 + 1)))) return rc;
     rc = soapb_descriptor_fp64(c, &bt, d.soap.as<double>(), keep_cart ? d.cart.as<double>() : nullptr);
-  } else {
-    // each chunk's soap rows go back while the next chunk computes
-    plan_chunks(d, n_sites, do_timing != 0);
-    const int nch = (int)d.chunk.size() - 1;
-    if ((rc = dropin_streams(d, 2 * nch))) return rc;
+  } else if (chunked) {
     SiteChunks ch;
     ch.n = nch;
     ch.bounds = d.chunk.data();
-    if (!do_timing)
-      ch.after = [&](int i) -> int {
-        const size_t lo = (size_t)d.chunk[i], hi = (size_t)d.chunk[i + 1];
-        CU(cudaEventRecord(d.evs[i], s));
-        CU(cudaStreamWaitEvent(d.copy_out, d.evs[i], 0));
-        CU(cudaMemcpyAsync(soap + lo * n_soap, d.soap.as<double>() + lo * n_soap, 8 * (hi - lo) * n_soap,
-                           cudaMemcpyDeviceToHost, d.copy_out));
-        return SOAPB_OK;
-      };
+    ch.site_off = d.host_off.data();
+    ch.before = [&](int i) -> int {
+      CU(cudaStreamWaitEvent(s, d.evs[i], 0));
+      return SOAPB_OK;
+    };
+    ch.after = [&](int i) -> int {
+      const size_t lo = (size_t)d.chunk[i], hi = (size_t)d.chunk[i + 1];
+      CU(cudaEventRecord(d.evs[nch + i], s));
+      CU(cudaStreamWaitEvent(d.copy_out, d.evs[nch + i], 0));
+      CU(cudaMemcpyAsync(soap + lo * n_soap, d.soap.as<double>() + lo * n_soap, 8 * (hi - lo) * n_soap,
+                         cudaMemcpyDeviceToHost, d.copy_out));
+      return SOAPB_OK;
+    };
     rc = ctx_descriptor(c, &bt, d.soap.as<double>(), do_derivatives && contract, &ch);
-    soap_copied = !do_timing;
+    soap_copied = true;
+  } else {
+    rc = ctx_descriptor(c, &bt, d.soap.as<double>(), do_derivatives && contract);
   }
   if (rc) {
-    if (soap_copied) cudaStreamSynchronize(d.copy_out);  // no copy into soap outlives the call
+    if (chunked) {  // no copy from or into the caller's arrays outlives the call
+      cudaStreamSynchronize(d.copy_in);
+      cudaStreamSynchronize(d.copy_out);
+    }
     return rc;
   }
   if (do_timing) cudaEventRecord(ev[2], s);
@@ -1938,20 +2022,23 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
     CU(cudaMemcpyAsync(soap_cart_der, d.cart.p, 8 * (size_t)n_atom_pairs * n_soap * 3,
                        cudaMemcpyDeviceToHost, s));
   if (do_timing) cudaEventRecord(ev[3], s);
-  // the prep error word comes back with the same wait; the compute stream
-  // also waits for the last soap rows on copy_out, so one synchronisation
-  // covers both streams (both are synchronised if the join cannot be made)
+  // the prep error word comes back with the same wait.  The compute stream
+  // has waited for every chunk's copies in; made to wait for the last soap
+  // rows on copy_out as well, its synchronisation covers all three streams
+  // (each is synchronised if the join cannot be made).
   if ((rc = dropin_streams(d, 0))) return rc;
   bool joined = false;
-  if (soap_copied) {
-    cudaEvent_t ej = d.evs[d.chunk.size() - 1];  // unused by the chunks (they take evs[0 .. nch))
+  if (chunked) {
+    cudaEvent_t ej = d.evs[2 * nch];
     joined = cudaEventRecord(ej, d.copy_out) == cudaSuccess && cudaStreamWaitEvent(s, ej, 0) == cudaSuccess;
   }
   *d.err_host = 0;
   if (c->err.p) CU(cudaMemcpyAsync(d.err_host, c->err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   const cudaError_t es = cudaStreamSynchronize(s);
-  const cudaError_t eo = (soap_copied && !joined) ? cudaStreamSynchronize(d.copy_out) : cudaSuccess;
+  const cudaError_t ei = (chunked && !joined) ? cudaStreamSynchronize(d.copy_in) : cudaSuccess;
+  const cudaError_t eo = (chunked && !joined) ? cudaStreamSynchronize(d.copy_out) : cudaSuccess;
   CU(es);
+  CU(ei);
   CU(eo);
   if ((rc = input_status(*d.err_host, nullptr))) return rc;
   if (do_timing) {
@@ -2010,14 +2097,14 @@ int soapb_soap_contract(const double *soap, const double *G, double sgn, double 
   // compute stream once they are there, the chunk's pair forces out on copy_out
   if ((rc = d.soap.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
   if ((rc = d.G.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
-  if ((int)d.chunk.size() < 2 || d.chunk.back() != n_sites) plan_chunks(d, n_sites, false);
-  const int nch = (int)d.chunk.size() - 1;
+  if ((int)d.cchunk.size() < 2 || d.cchunk.back() != n_sites) plan_chunks(d.cchunk, n_sites, true);
+  const int nch = (int)d.cchunk.size() - 1;
   if ((rc = dropin_streams(d, 2 * nch + 1))) return rc;
   double *dS = d.soap.as<double>(), *dG = d.G.as<double>(), *dP = d.pair.as<double>();
   CU(cudaEventRecord(d.evs[0], s));  // the copies in must not overwrite what earlier work still reads
   CU(cudaStreamWaitEvent(d.copy_in, d.evs[0], 0));
   for (int i = 0; i < nch && n_sites > 0; ++i) {
-    const size_t lo = (size_t)d.chunk[i], hi = (size_t)d.chunk[i + 1];
+    const size_t lo = (size_t)d.cchunk[i], hi = (size_t)d.cchunk[i + 1];
     CU(cudaMemcpyAsync(dS + lo * n_soap, soap + lo * n_soap, 8 * (hi - lo) * n_soap, cudaMemcpyHostToDevice,
                        d.copy_in));
     CU(cudaMemcpy2DAsync(dG + lo, 8 * (size_t)n_sites, G + lo, 8 * (size_t)n_sites, 8 * (hi - lo), n_soap,
@@ -2026,13 +2113,13 @@ int soapb_soap_contract(const double *soap, const double *G, double sgn, double 
   }
   SiteChunks ch;
   ch.n = nch;
-  ch.bounds = d.chunk.data();
+  ch.bounds = d.cchunk.data();
   ch.before = [&](int i) -> int {
     CU(cudaStreamWaitEvent(s, d.evs[i], 0));
     return SOAPB_OK;
   };
   ch.after = [&](int i) -> int {
-    const long long p0 = d.host_off[d.chunk[i]], p1 = d.host_off[d.chunk[i + 1]];
+    const long long p0 = d.host_off[d.cchunk[i]], p1 = d.host_off[d.cchunk[i + 1]];
     CU(cudaEventRecord(d.evs[nch + i], s));
     CU(cudaStreamWaitEvent(d.copy_out, d.evs[nch + i], 0));
     if (p1 > p0)

@@ -133,7 +133,10 @@ int prep_err_words(int n_sites);
 // The error code in err[0]: a bad pair's index, a value >= 2^33 for CSR and
 // scan failures, or all ones when the launch found no error.
 unsigned long long prep_error_code(unsigned long long word);
-cudaError_t launch_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der);
+// The pair rows of pairs [pair_lo, pair_hi) (pair_hi < 0: all), with the CSR
+// offset scan of the whole batch when scan is set (one launch per batch must).
+cudaError_t launch_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der, int pair_lo = 0,
+                        int pair_hi = -1, bool scan = true);
 int ang_row_floats(const DevParams &P);
 size_t keep_floats_per_site(const DevParams &P);
 cudaError_t launch_descriptor(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,

@@ -225,7 +225,7 @@ int ang_row_floats(const DevParams &P) { return row_len(P.amax_t == 8 ? 8 : 12);
 // angular expansions between get_soap and soap_contract.
 template <int AMAX, int LC, bool OP>
 __global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch B, int do_der,
-                                              int scan_tiles) {
+                                              int scan_tiles, int pair_lo, int pair_hi) {
   extern __shared__ __align__(16) unsigned char smem[];
   if ((int)blockIdx.x < scan_tiles) {
     prep_scan_tile<128>(B, scan_tiles, (int *)smem);
@@ -239,9 +239,9 @@ __global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch 
   for (int t = threadIdx.x; t < head; t += 128) ((uint4 *)smem)[t] = ((const uint4 *)P.blob)[t];
   float *rows = (float *)(smem + (size_t)head * 16);
   __syncthreads();
-  const int k0 = ((int)blockIdx.x - scan_tiles) * 128;
+  const int k0 = pair_lo + ((int)blockIdx.x - scan_tiles) * 128;
   const int k = k0 + threadIdx.x;
-  if (k < B.n_pairs) {
+  if (k < pair_hi) {
     const unsigned bits = prep_pair(B, k, P.n_species);
     const double r = B.rjs[k];
     if (bits != 0u && r < P.rcut_max) {
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch 
   __syncthreads();
   // coalesced 16-byte stores of the CTA's rows (AW is a multiple of 4 floats)
   constexpr int AW4 = AW / 4;
-  const int n4 = min(128, B.n_pairs - k0) * AW4;
+  const int n4 = min(128, pair_hi - k0) * AW4;
   float4 *dst = (float4 *)(B.ang + (size_t)k0 * AW);
   for (int t = threadIdx.x; t < n4; t += 128) {
     const int i = t / AW4;
@@ -1103,26 +1103,30 @@ cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s) {
 }
 
 template <int AMAX, int LC, bool OP>
-static cudaError_t run_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der) {
+static cudaError_t run_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der, int pair_lo,
+                            int pair_hi, bool scan) {
   size_t sm = (size_t)P.off_rad + (size_t)P.n_species * SOAPB_RADSP_BYTES +
               (size_t)128 * (row_len(LC) + 1) * sizeof(float);
   if (sm < kScanTile * sizeof(int)) sm = kScanTile * sizeof(int);  // scan tiles reuse it
   auto kern = k_pair<AMAX, LC, OP>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  const int tiles = prep_scan_tiles(B.n_sites);
-  const int blocks = tiles + (B.n_pairs + 127) / 128;
-  if (blocks > 0) kern<<<blocks, 128, sm, s>>>(P, B, do_der, tiles);
+  const int tiles = scan ? prep_scan_tiles(B.n_sites) : 0;
+  const int blocks = tiles + (pair_hi - pair_lo + 127) / 128;
+  if (blocks > 0) kern<<<blocks, 128, sm, s>>>(P, B, do_der, tiles, pair_lo, pair_hi);
   return cudaGetLastError();
 }
 
-cudaError_t launch_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der) {
+cudaError_t launch_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der, int pair_lo,
+                        int pair_hi, bool scan) {
+  if (pair_hi < 0) pair_hi = B.n_pairs;
+  if (pair_lo < 0 || pair_lo > pair_hi || pair_hi > B.n_pairs) return cudaErrorInvalidValue;
   if (P.basis == kBasisOperator) {
-    if (P.amax_t == 8) return run_pair<8, 8, true>(P, B, s, do_der);
-    return run_pair<16, 12, true>(P, B, s, do_der);
+    if (P.amax_t == 8) return run_pair<8, 8, true>(P, B, s, do_der, pair_lo, pair_hi, scan);
+    return run_pair<16, 12, true>(P, B, s, do_der, pair_lo, pair_hi, scan);
   }
-  if (P.amax_t == 8) return run_pair<8, 8, false>(P, B, s, do_der);
-  return run_pair<16, 12, false>(P, B, s, do_der);
+  if (P.amax_t == 8) return run_pair<8, 8, false>(P, B, s, do_der, pair_lo, pair_hi, scan);
+  return run_pair<16, 12, false>(P, B, s, do_der, pair_lo, pair_hi, scan);
 }
 
 // The radial block is fixed by the definition: the host lays the constants

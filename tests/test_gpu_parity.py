@@ -155,10 +155,11 @@ def test_dropin_get_soap_and_contract(name):
 
 @pytest.mark.parametrize("pinned", [True, False])
 def test_dropin_site_chunks_match_the_context_layer(pinned):
-    """The drop-in layer runs batches of 768 sites or more in site chunks whose
-    copies overlap the kernels (1703 sites here: four chunks); every site's
-    result is computed the same way, so soap and pair equal the single-launch
-    context calls bit for bit, from pinned or pageable host arrays."""
+    """The drop-in layer runs batches of 1024 sites or more in site chunks whose
+    copies overlap the kernels (1703 sites here: three chunks in get_soap, four
+    in soap_contract, the last of them half size); every site's result is
+    computed the same way, so soap and pair equal the single-launch context
+    calls bit for bit, from pinned or pageable host arrays."""
     import torch
     w = syn.config(2, seed=41)
     nl = w.nl
@@ -189,6 +190,56 @@ def test_dropin_site_chunks_match_the_context_layer(pinned):
             pair = host(np.zeros((3, nl.n_pairs)))
             D.soap_contract(soap, host(G.T), 1.0, pair)
             np.testing.assert_array_equal(pair.T, p_ctx)
+    finally:
+        D.set_basis_matrices(None)
+
+
+def _empty_sites(n, n_species, like):
+    """n sites with no pairs (not even the self pair) in the layout of `like`."""
+    mm = like.species.shape[1]
+    sp = np.zeros((n, mm), np.int32)
+    sp[:, 0] = like.species[0, 0]
+    return syn.NeighbourList(
+        n_sites=n, n_neigh=np.zeros(n, np.int32), rjs=np.zeros(0), thetas=np.zeros(0),
+        phis=np.zeros(0), mask=np.zeros((n_species, 0), np.uint8), species=sp,
+        species_multiplicity=np.ones(n, np.int32), site_atom=np.zeros(n, np.int64),
+        neigh_atom=np.zeros(0, np.int64), disp=np.zeros((0, 3)))
+
+
+def test_dropin_chunks_without_pairs():
+    """Site chunks whose sites have no pairs at all: get_soap's chunk 1 of 3 and
+    soap_contract's chunks 1 and 2 of 5 copy no pair rows and launch the pair
+    kernel on an empty range; the result still equals the context layer's.
+    (An empty site's descriptor is the central-atom term alone, the same for
+    all of them, src/soap_turbo.f90:646-662.)"""
+    import torch
+    hp = syn.Hyper(alpha_max=[8, 8, 8], basis="poly3gauss", compress_mode="trivial")
+    parts = []
+    for seed in (61, 62):
+        st = syn.random_structure(700, density=0.10, d_min=0.9, fractions=(0.4, 0.4, 0.2), seed=seed)
+        parts.append(syn.neighbour_list(st, 5.0, 3, central_species=1))
+    nl = syn.concatenate([parts[0], _empty_sites(1400, 3, parts[0]), parts[1]])
+    n = nl.n_sites
+    lo, hi = parts[0].n_sites, parts[0].n_sites + 1400
+    assert lo <= n // 3 and hi >= 2 * n // 3          # get_soap's middle chunk is empty
+    assert lo <= 2 * n // 9 and hi >= 6 * n // 9      # so are two of soap_contract's
+    w = syn.Workload("gaps", hp, nl, [])
+    ctx = Context(hp)
+    W, S = ctx.basis()
+    b = ctx.batch(nl)
+    s_ctx = ctx.descriptor(b, keep=True)
+    G = np.random.default_rng(9).standard_normal((ctx.n_soap, n))
+    p_ctx = ctx.contract(b, s_ctx, torch.as_tensor(G).cuda()).cpu().numpy()
+    s_ctx = s_ctx.cpu().numpy()
+    np.testing.assert_array_equal(s_ctx[lo:hi], np.broadcast_to(s_ctx[lo], (hi - lo, ctx.n_soap)))
+    D.set_basis_matrices(W, S)
+    try:
+        soap = np.zeros((ctx.n_soap, n), order="F")
+        D.get_soap(**_dropin_args(w, soap), contract=True)
+        np.testing.assert_array_equal(soap.T, s_ctx)
+        pair = np.zeros((3, nl.n_pairs), order="F")
+        D.soap_contract(soap, np.asfortranarray(G.T), 1.0, pair)
+        np.testing.assert_array_equal(pair.T, p_ctx)
     finally:
         D.set_basis_matrices(None)
 
