@@ -223,12 +223,15 @@ int ang_row_floats(const DevParams &P) { return row_len(P.amax_t == 8 ? 8 : 12);
 // The site kernels only read these rows; soap_contract reads the rows of the
 // descriptor call that kept its state, as the reference keeps the radial and
 // angular expansions between get_soap and soap_contract.
+// 128-thread CTAs, 3 per SM (144 registers a thread)
+constexpr int kPairThreads = 128;
 template <int AMAX, int LC, bool OP>
-__global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch B, int do_der,
-                                              int scan_tiles, int pair_lo, int pair_hi) {
+__global__ void __launch_bounds__(kPairThreads)
+    k_pair(const DevParams P, const DevBatch B, int do_der, int scan_tiles, int pair_lo, int pair_hi) {
+  constexpr int NT = kPairThreads;
   extern __shared__ __align__(16) unsigned char smem[];
   if ((int)blockIdx.x < scan_tiles) {
-    prep_scan_tile<128>(B, scan_tiles, (int *)smem);
+    prep_scan_tile<NT>(B, scan_tiles, (int *)smem);
     return;
   }
   constexpr int AW = row_len(LC);
@@ -236,10 +239,10 @@ __global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch 
   // not all map to one bank
   constexpr int AWS = AW + 1;
   const int head = (P.off_rad + P.n_species * SOAPB_RADSP_BYTES) / 16;
-  for (int t = threadIdx.x; t < head; t += 128) ((uint4 *)smem)[t] = ((const uint4 *)P.blob)[t];
+  for (int t = threadIdx.x; t < head; t += NT) ((uint4 *)smem)[t] = ((const uint4 *)P.blob)[t];
   float *rows = (float *)(smem + (size_t)head * 16);
   __syncthreads();
-  const int k0 = pair_lo + ((int)blockIdx.x - scan_tiles) * 128;
+  const int k0 = pair_lo + ((int)blockIdx.x - scan_tiles) * NT;
   const int k = k0 + threadIdx.x;
   if (k < pair_hi) {
     const unsigned bits = prep_pair(B, k, P.n_species);
@@ -294,9 +297,9 @@ __global__ void __launch_bounds__(128) k_pair(const DevParams P, const DevBatch 
   __syncthreads();
   // coalesced 16-byte stores of the CTA's rows (AW is a multiple of 4 floats)
   constexpr int AW4 = AW / 4;
-  const int n4 = min(128, pair_hi - k0) * AW4;
+  const int n4 = min(NT, pair_hi - k0) * AW4;
   float4 *dst = (float4 *)(B.ang + (size_t)k0 * AW);
-  for (int t = threadIdx.x; t < n4; t += 128) {
+  for (int t = threadIdx.x; t < n4; t += NT) {
     const int i = t / AW4;
     const float *src = rows + i * AWS + 4 * (t - i * AW4);
     dst[t] = make_float4(src[0], src[1], src[2], src[3]);
@@ -1106,14 +1109,14 @@ template <int AMAX, int LC, bool OP>
 static cudaError_t run_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der, int pair_lo,
                             int pair_hi, bool scan) {
   size_t sm = (size_t)P.off_rad + (size_t)P.n_species * SOAPB_RADSP_BYTES +
-              (size_t)128 * (row_len(LC) + 1) * sizeof(float);
+              (size_t)kPairThreads * (row_len(LC) + 1) * sizeof(float);
   if (sm < kScanTile * sizeof(int)) sm = kScanTile * sizeof(int);  // scan tiles reuse it
   auto kern = k_pair<AMAX, LC, OP>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int tiles = scan ? prep_scan_tiles(B.n_sites) : 0;
-  const int blocks = tiles + (pair_hi - pair_lo + 127) / 128;
-  if (blocks > 0) kern<<<blocks, 128, sm, s>>>(P, B, do_der, tiles, pair_lo, pair_hi);
+  const int blocks = tiles + (pair_hi - pair_lo + kPairThreads - 1) / kPairThreads;
+  if (blocks > 0) kern<<<blocks, kPairThreads, sm, s>>>(P, B, do_der, tiles, pair_lo, pair_hi);
   return cudaGetLastError();
 }
 

@@ -61,12 +61,9 @@ __device__ __forceinline__ void prep_scan_tile(const DevBatch &B, int scan_tiles
   }
   if (bad) prep_error(B, kErrCsr);
   __syncthreads();
-  int loc[ITEMS], sum = 0;
+  int sum = 0;
 #pragma unroll
-  for (int j = 0; j < ITEMS; ++j) {
-    loc[j] = sum;
-    sum += sv[tid * ITEMS + j];
-  }
+  for (int j = 0; j < ITEMS; ++j) sum += sv[tid * ITEMS + j];
   int x = sum;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -109,11 +106,14 @@ __device__ __forceinline__ void prep_scan_tile(const DevBatch &B, int scan_tiles
     s_excl = (int)excl;
   }
   __syncthreads();
-  const int e0 = s_excl + tpre;
+  // the thread's items again from shared memory, each written as the running
+  // offset before it is added
+  int run = s_excl + tpre;
 #pragma unroll
   for (int j = 0; j < ITEMS; ++j) {
     const int i = base + tid * ITEMS + j;
-    if (i < B.n_sites) B.off[i] = e0 + loc[j];
+    if (i < B.n_sites) B.off[i] = run;
+    run += sv[tid * ITEMS + j];
   }
   if (tile == scan_tiles - 1 && tid == 0) {
     const long long all = (long long)s_excl + total;
