@@ -2051,6 +2051,7 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
     std::printf("  *) Host to device copies: %8.3f ms |\n", t01);
     std::printf("  *) Descriptor kernels:    %8.3f ms |\n", t12);
     std::printf("  *) Device to host copies: %8.3f ms |\n", t23);
+    std::fflush(stdout);
     for (auto &e : ev) cudaEventDestroy(e);
   }
   if (do_hessian) {

@@ -282,6 +282,39 @@ def test_dropin_fp64_precision_contract():
         D.set_basis_matrices(None)
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_dropin_do_timing(precision, capfd):
+    """do_timing (src/soap_turbo.f90:139-169): the call prints its timing table
+    (GPU times of the copies and kernels; the mixed path then runs its kernels
+    unchunked) and returns the same soap as without it; soap_contract works
+    after it."""
+    w = syn.config(2, seed=43)
+    hp, nl = w.hyper, w.nl
+    ctx = Context(hp)
+    W, S = ctx.basis()
+    G = np.asfortranarray(np.random.default_rng(6).standard_normal((nl.n_sites, ctx.n_soap)))
+    D.set_basis_matrices(W, S)
+    D.set_precision(precision)
+    try:
+        out = {}
+        for timing in (False, True):
+            args = _dropin_args(w, np.zeros((ctx.n_soap, nl.n_sites), order="F"))
+            args["do_timing"] = timing
+            D.get_soap(**args, contract=True)
+            pair = np.zeros((3, nl.n_pairs), order="F")
+            D.soap_contract(args["soap"], G, 1.0, pair)
+            out[timing] = (args["soap"], pair)
+        printed = capfd.readouterr().out
+        assert printed.count("SOAP timings") == 1
+        for line in ("Host to device copies:", "Descriptor kernels:", "Device to host copies:"):
+            assert line in printed
+        np.testing.assert_array_equal(out[True][0], out[False][0])
+        np.testing.assert_array_equal(out[True][1], out[False][1])
+    finally:
+        D.set_precision("mixed")
+        D.set_basis_matrices(None)
+
+
 # ---------------------------------------------------------------- gradients
 class SoapFunction(torch.autograd.Function):
     """soap(disp) for a fixed topology; backward is the adjoint contract.
