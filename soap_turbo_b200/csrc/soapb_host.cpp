@@ -2,6 +2,7 @@
 // matrices, the compression and adjoint index tables, device memory, and the
 // two API layers declared in include/soap_b200.h.
 #include <cuda_runtime.h>
+#include <omp.h>
 
 #include <algorithm>
 #include <cmath>
@@ -178,6 +179,70 @@ struct DBuf {
   template <typename T>
   T *as() const { return (T *)p; }
 };
+
+// Grow-only pinned host memory: the staging area through which the drop-in
+// layer moves caller arrays that live in pageable memory.
+struct HBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return SOAPB_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    if (bytes == 0) return SOAPB_OK;
+    cudaError_t e = cudaHostAlloc(&p, bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaHostAlloc");
+    cap = bytes;
+    return SOAPB_OK;
+  }
+  template <typename T>
+  T *as() const { return (T *)p; }
+};
+
+// Whether a caller's host array is page-locked (cudaHostAlloc'd or
+// registered), so that the copy engines can read or write it directly.
+bool is_pinned(const void *ptr) {
+  if (!ptr) return true;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Host copies between a caller's pageable array and the pinned staging area,
+// split over up to 8 OpenMP threads (at most the caller's OMP_NUM_THREADS) in
+// slices of at least 256 KB: one thread's memcpy runs well below what a
+// host-device copy moves.
+int copy_threads(size_t bytes) {
+  const size_t slices = (bytes + (1u << 18) - 1) >> 18;
+  return (int)std::max<size_t>(1, std::min<size_t>({slices, 8, (size_t)omp_get_max_threads()}));
+}
+void par_copy(void *dst, const void *src, size_t bytes) {
+  const int nt = copy_threads(bytes);
+  if (nt <= 1) {
+    if (bytes) std::memcpy(dst, src, bytes);
+    return;
+  }
+#pragma omp parallel for num_threads(nt) schedule(static)
+  for (int t = 0; t < nt; ++t) {
+    const size_t a = bytes * t / nt, b = bytes * (t + 1) / nt;
+    std::memcpy((char *)dst + a, (const char *)src + a, b - a);
+  }
+}
+// rows of `width` bytes, `rows` of them, at the given pitches
+void par_copy2d(void *dst, size_t dpitch, const void *src, size_t spitch, size_t width, size_t rows) {
+  const int nt = std::min<int>(copy_threads(width * rows), (int)std::max<size_t>(rows, 1));
+  if (nt <= 1) {
+    for (size_t r = 0; r < rows; ++r) std::memcpy((char *)dst + r * dpitch, (const char *)src + r * spitch, width);
+    return;
+  }
+#pragma omp parallel for num_threads(nt) schedule(static)
+  for (long long r = 0; r < (long long)rows; ++r)
+    std::memcpy((char *)dst + r * dpitch, (const char *)src + r * spitch, width);
+}
 
 }  // namespace
 
@@ -1661,6 +1726,7 @@ struct DropIn {
   std::vector<int> chunk;                  // site chunk bounds of the last get_soap
   std::vector<int> cchunk;                 // and of soap_contract
   std::vector<long long> host_off;         // its CSR offsets
+  HBuf st_in, st_out;                      // pinned staging of pageable caller arrays
   unsigned long long *err_host = nullptr;  // pinned copy of the prep error word
 };
 
@@ -1731,33 +1797,96 @@ int upload(DBuf &b, const T *src, size_t n, cudaStream_t s) {
   return SOAPB_OK;
 }
 
-// get_soap's inputs on the copy-in stream, in the site chunks d.chunk: the
-// per-site arrays first, then each chunk's pair rows of mask, rjs, thetas and
-// phis, after which evs[i] marks chunk i's inputs as present.  The buffers
-// are sized by the caller; the copies wait for the work already queued on the
-// compute stream, which may still read the previous call's inputs.
-int copy_in_chunks(DropIn &d, int n_sites, int n_species, int max_mult, int n_pairs, const int32_t *n_neigh,
-                   const int32_t *species, const int32_t *species_mult, const uint8_t *mask, const double *rjs,
-                   const double *thetas, const double *phis) {
-  const int nch = (int)d.chunk.size() - 1;
+// Where each of get_soap's inputs is read from: the caller's array when it is
+// page-locked, else a region of the pinned staging area st_in (then filled
+// with host copies, chunk by chunk, just before its asynchronous copy).
+struct GetSoapIn {
+  const int32_t *n_neigh, *species, *species_mult;
+  const uint8_t *mask;
+  const double *rjs, *thetas, *phis;
+  bool pin_nn, pin_sp, pin_sm, pin_mask, pin_pair;  // pin_pair: rjs, thetas and phis
+  uint8_t *st_nn = nullptr, *st_sp = nullptr, *st_sm = nullptr, *st_mask = nullptr, *st_r = nullptr,
+          *st_t = nullptr, *st_f = nullptr;
+};
+
+size_t align16(size_t x) { return (x + 15) / 16 * 16; }
+
+// Lays out st_in for the pageable inputs of one get_soap call.
+int plan_get_soap_staging(DropIn &d, GetSoapIn &in, int n_sites, int max_mult, int n_species, int n_pairs) {
+  const size_t b_nn = in.pin_nn ? 0 : align16(4 * (size_t)n_sites);
+  const size_t b_sp = in.pin_sp ? 0 : align16(4 * (size_t)n_sites * max_mult);
+  const size_t b_sm = in.pin_sm ? 0 : align16(4 * (size_t)n_sites);
+  const size_t b_mask = in.pin_mask ? 0 : align16((size_t)n_pairs * n_species);
+  const size_t b_p = in.pin_pair ? 0 : align16(8 * (size_t)n_pairs);
+  const size_t total = b_nn + b_sp + b_sm + b_mask + 3 * b_p;
+  if (total == 0) return SOAPB_OK;
+  int rc = d.st_in.ensure(total);
+  if (rc) return rc;
+  uint8_t *q = d.st_in.as<uint8_t>();
+  if (b_nn) in.st_nn = q, q += b_nn;
+  if (b_sp) in.st_sp = q, q += b_sp;
+  if (b_sm) in.st_sm = q, q += b_sm;
+  if (b_mask) in.st_mask = q, q += b_mask;
+  if (b_p) {
+    in.st_r = q, q += b_p;
+    in.st_t = q, q += b_p;
+    in.st_f = q;
+  }
+  return SOAPB_OK;
+}
+
+// One host-to-device copy on copy_in from a caller array, through its staging
+// region when it is pageable (the copy of the same byte range into staging
+// comes first, on the host).
+int h2d_in(void *dev, const void *host, uint8_t *stage, size_t bytes, cudaStream_t st) {
+  if (!bytes) return SOAPB_OK;
+  const void *src = host;
+  if (stage) {
+    par_copy(stage, host, bytes);
+    src = stage;
+  }
+  CU(cudaMemcpyAsync(dev, src, bytes, cudaMemcpyHostToDevice, st));
+  return SOAPB_OK;
+}
+
+// get_soap's per-site inputs on the copy-in stream, after the work already
+// queued on the compute stream (which may still read the previous call's).
+int copy_in_sites(DropIn &d, const GetSoapIn &in, int n_sites, int max_mult) {
   CU(cudaEventRecord(d.evs[0], d.stream));
   CU(cudaStreamWaitEvent(d.copy_in, d.evs[0], 0));
-  CU(cudaMemcpyAsync(d.n_neigh.p, n_neigh, 4 * (size_t)n_sites, cudaMemcpyHostToDevice, d.copy_in));
-  CU(cudaMemcpyAsync(d.species.p, species, 4 * (size_t)n_sites * max_mult, cudaMemcpyHostToDevice, d.copy_in));
-  CU(cudaMemcpyAsync(d.species_mult.p, species_mult, 4 * (size_t)n_sites, cudaMemcpyHostToDevice, d.copy_in));
-  for (int i = 0; i < nch; ++i) {
-    const size_t p0 = (size_t)d.host_off[d.chunk[i]], p1 = (size_t)d.host_off[d.chunk[i + 1]];
-    if (p1 > p0) {
-      // mask(n_pairs, n_species) column-major: the chunk's rows of every column
-      CU(cudaMemcpy2DAsync(d.mask.as<uint8_t>() + p0, (size_t)n_pairs, mask + p0, (size_t)n_pairs, p1 - p0,
-                           (size_t)n_species, cudaMemcpyHostToDevice, d.copy_in));
-      CU(cudaMemcpyAsync(d.rjs.as<double>() + p0, rjs + p0, 8 * (p1 - p0), cudaMemcpyHostToDevice, d.copy_in));
-      CU(cudaMemcpyAsync(d.thetas.as<double>() + p0, thetas + p0, 8 * (p1 - p0), cudaMemcpyHostToDevice,
-                         d.copy_in));
-      CU(cudaMemcpyAsync(d.phis.as<double>() + p0, phis + p0, 8 * (p1 - p0), cudaMemcpyHostToDevice, d.copy_in));
+  int rc;
+  if ((rc = h2d_in(d.n_neigh.p, in.n_neigh, in.st_nn, 4 * (size_t)n_sites, d.copy_in))) return rc;
+  if ((rc = h2d_in(d.species.p, in.species, in.st_sp, 4 * (size_t)n_sites * max_mult, d.copy_in))) return rc;
+  if ((rc = h2d_in(d.species_mult.p, in.species_mult, in.st_sm, 4 * (size_t)n_sites, d.copy_in))) return rc;
+  return SOAPB_OK;
+}
+
+// Chunk i's pair rows of mask, rjs, thetas and phis on the copy-in stream;
+// evs[i] then marks the chunk's inputs (and the per-site ones) as present.
+int copy_in_pairs(DropIn &d, const GetSoapIn &in, int i, int n_species, int n_pairs) {
+  const size_t p0 = (size_t)d.host_off[d.chunk[i]], p1 = (size_t)d.host_off[d.chunk[i + 1]];
+  if (p1 > p0) {
+    // mask(n_pairs, n_species) column-major: the chunk's rows of every column
+    const uint8_t *msrc = in.mask + p0;
+    if (in.st_mask) {
+      par_copy2d(in.st_mask + p0, (size_t)n_pairs, in.mask + p0, (size_t)n_pairs, p1 - p0, (size_t)n_species);
+      msrc = in.st_mask + p0;
     }
-    CU(cudaEventRecord(d.evs[i], d.copy_in));
+    CU(cudaMemcpy2DAsync(d.mask.as<uint8_t>() + p0, (size_t)n_pairs, msrc, (size_t)n_pairs, p1 - p0,
+                         (size_t)n_species, cudaMemcpyHostToDevice, d.copy_in));
+    const size_t b0 = 8 * p0, nb = 8 * (p1 - p0);
+    int rc;
+    if ((rc = h2d_in(d.rjs.as<uint8_t>() + b0, (const uint8_t *)in.rjs + b0, in.st_r ? in.st_r + b0 : nullptr, nb,
+                     d.copy_in)))
+      return rc;
+    if ((rc = h2d_in(d.thetas.as<uint8_t>() + b0, (const uint8_t *)in.thetas + b0, in.st_t ? in.st_t + b0 : nullptr,
+                     nb, d.copy_in)))
+      return rc;
+    if ((rc = h2d_in(d.phis.as<uint8_t>() + b0, (const uint8_t *)in.phis + b0, in.st_f ? in.st_f + b0 : nullptr, nb,
+                     d.copy_in)))
+      return rc;
   }
+  CU(cudaEventRecord(d.evs[i], d.copy_in));
   return SOAPB_OK;
 }
 
@@ -1937,14 +2066,23 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
   // The mixed path without do_timing runs in site chunks: chunk i's pair
   // inputs come in on copy_in (evs[i]), its pair and site kernels run on the
   // compute stream once they are there, and its soap rows go out on copy_out
-  // (evs[nch + i]) while later chunks compute.  Otherwise everything is copied
-  // in on the compute stream first.
+  // (evs[nch + i]) while later chunks compute.  Caller arrays in pageable
+  // memory pass through the pinned staging areas: a chunk's inputs are copied
+  // into st_in on the host just before their asynchronous copy (so the host
+  // fills chunk i + 1 while chunk i computes), and the soap rows land in
+  // st_out, from where each chunk is copied out once its copy has arrived
+  // (evs[2 nch + 1 + i]) while later ones are still in flight.  Otherwise
+  // everything is copied in on the compute stream first.
   const bool chunked = !fp64 && !do_timing && n_sites > 0;
   int nch = 1;
+  GetSoapIn in{n_neigh, species, species_multiplicity, mask, rjs, thetas, phis, is_pinned(n_neigh),
+               is_pinned(species), is_pinned(species_multiplicity), is_pinned(mask),
+               is_pinned(rjs) && is_pinned(thetas) && is_pinned(phis)};
+  const bool soap_staged = chunked && !is_pinned(soap);
   if (chunked) {
     plan_chunks(d.chunk, n_sites, false);
     nch = (int)d.chunk.size() - 1;
-    if ((rc = dropin_streams(d, 2 * nch + 1))) return rc;
+    if ((rc = dropin_streams(d, 3 * nch + 1))) return rc;
     if ((rc = d.n_neigh.ensure(4 * ((size_t)n_sites + 1)))) return rc;
     if ((rc = d.species.ensure(4 * ((size_t)n_sites * max_species_multiplicity + 1)))) return rc;
     if ((rc = d.species_mult.ensure(4 * ((size_t)n_sites + 1)))) return rc;
@@ -1953,8 +2091,9 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
     if ((rc = d.thetas.ensure(8 * ((size_t)n_atom_pairs + 1)))) return rc;
     if ((rc = d.phis.ensure(8 * ((size_t)n_atom_pairs + 1)))) return rc;
     if ((rc = d.soap.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
-    const int copied = copy_in_chunks(d, n_sites, n_species, max_species_multiplicity, n_atom_pairs, n_neigh,
-                                      species, species_multiplicity, mask, rjs, thetas, phis);
+    if ((rc = plan_get_soap_staging(d, in, n_sites, max_species_multiplicity, n_species, n_atom_pairs))) return rc;
+    if (soap_staged && (rc = d.st_out.ensure(8 * (size_t)n_sites * n_soap))) return rc;
+    const int copied = copy_in_sites(d, in, n_sites, max_species_multiplicity);
     if (copied) {
       cudaStreamSynchronize(d.copy_in);  // no copy from the caller's arrays outlives the call
       return copied;
@@ -1992,18 +2131,32 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
     ch.bounds = d.chunk.data();
     ch.site_off = d.host_off.data();
     ch.before = [&](int i) -> int {
+      const int r2 = copy_in_pairs(d, in, i, n_species, n_atom_pairs);
+      if (r2) return r2;
       CU(cudaStreamWaitEvent(s, d.evs[i], 0));
       return SOAPB_OK;
     };
+    double *soap_dst = soap_staged ? d.st_out.as<double>() : soap;
     ch.after = [&](int i) -> int {
       const size_t lo = (size_t)d.chunk[i], hi = (size_t)d.chunk[i + 1];
       CU(cudaEventRecord(d.evs[nch + i], s));
       CU(cudaStreamWaitEvent(d.copy_out, d.evs[nch + i], 0));
-      CU(cudaMemcpyAsync(soap + lo * n_soap, d.soap.as<double>() + lo * n_soap, 8 * (hi - lo) * n_soap,
+      CU(cudaMemcpyAsync(soap_dst + lo * n_soap, d.soap.as<double>() + lo * n_soap, 8 * (hi - lo) * n_soap,
                          cudaMemcpyDeviceToHost, d.copy_out));
+      if (soap_staged) CU(cudaEventRecord(d.evs[2 * nch + 1 + i], d.copy_out));
       return SOAPB_OK;
     };
     rc = ctx_descriptor(c, &bt, d.soap.as<double>(), do_derivatives && contract, &ch);
+    // the staged soap rows, chunk by chunk as their copies arrive
+    for (int i = 0; rc == 0 && soap_staged && i < nch; ++i) {
+      const cudaError_t e = cudaEventSynchronize(d.evs[2 * nch + 1 + i]);
+      if (e != cudaSuccess) {
+        rc = cuda_fail(e, "cudaEventSynchronize");
+        break;
+      }
+      const size_t lo = (size_t)d.chunk[i], hi = (size_t)d.chunk[i + 1];
+      par_copy(soap + lo * n_soap, soap_dst + lo * n_soap, 8 * (hi - lo) * n_soap);
+    }
     soap_copied = true;
   } else {
     rc = ctx_descriptor(c, &bt, d.soap.as<double>(), do_derivatives && contract);
@@ -2094,28 +2247,45 @@ int soapb_soap_contract(const double *soap, const double *G, double sgn, double 
     CU(cudaStreamSynchronize(s));
     return SOAPB_OK;
   }
-  // per site chunk: soap rows and G columns in on copy_in, the contract on the
-  // compute stream once they are there, the chunk's pair forces out on copy_out
+  // per site chunk: soap rows and G columns in on copy_in (evs[i]), the
+  // contract on the compute stream once they are there, the chunk's pair
+  // forces out on copy_out.  Pageable caller arrays pass through the pinned
+  // staging areas as in get_soap: a chunk's soap rows and G columns are copied
+  // into st_in on the host just before their asynchronous copy, and the pair
+  // forces land in st_out, copied out chunk by chunk as they arrive
+  // (evs[2 nch + 1 + i]).
   if ((rc = d.soap.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
   if ((rc = d.G.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
   if ((int)d.cchunk.size() < 2 || d.cchunk.back() != n_sites) plan_chunks(d.cchunk, n_sites, true);
   const int nch = (int)d.cchunk.size() - 1;
-  if ((rc = dropin_streams(d, 2 * nch + 1))) return rc;
+  if ((rc = dropin_streams(d, 3 * nch + 1))) return rc;
+  const size_t b_rows = align16(8 * (size_t)n_sites * n_soap);
+  const bool st_soap = !is_pinned(soap), st_G = !is_pinned(G), st_pair = !is_pinned(pair);
+  if ((st_soap || st_G) && (rc = d.st_in.ensure((st_soap ? b_rows : 0) + (st_G ? b_rows : 0)))) return rc;
+  if (st_pair && (rc = d.st_out.ensure(24 * (size_t)n_atom_pairs))) return rc;
+  double *sg_soap = st_soap ? d.st_in.as<double>() : nullptr;
+  double *sg_G = st_G ? (double *)(d.st_in.as<uint8_t>() + (st_soap ? b_rows : 0)) : nullptr;
+  double *pair_dst = st_pair ? d.st_out.as<double>() : pair;
   double *dS = d.soap.as<double>(), *dG = d.G.as<double>(), *dP = d.pair.as<double>();
   CU(cudaEventRecord(d.evs[0], s));  // the copies in must not overwrite what earlier work still reads
   CU(cudaStreamWaitEvent(d.copy_in, d.evs[0], 0));
-  for (int i = 0; i < nch && n_sites > 0; ++i) {
-    const size_t lo = (size_t)d.cchunk[i], hi = (size_t)d.cchunk[i + 1];
-    CU(cudaMemcpyAsync(dS + lo * n_soap, soap + lo * n_soap, 8 * (hi - lo) * n_soap, cudaMemcpyHostToDevice,
-                       d.copy_in));
-    CU(cudaMemcpy2DAsync(dG + lo, 8 * (size_t)n_sites, G + lo, 8 * (size_t)n_sites, 8 * (hi - lo), n_soap,
-                         cudaMemcpyHostToDevice, d.copy_in));
-    CU(cudaEventRecord(d.evs[i], d.copy_in));
-  }
   SiteChunks ch;
   ch.n = nch;
   ch.bounds = d.cchunk.data();
   ch.before = [&](int i) -> int {
+    const size_t lo = (size_t)d.cchunk[i], hi = (size_t)d.cchunk[i + 1];
+    const int r2 = h2d_in(dS + lo * n_soap, soap + lo * n_soap, sg_soap ? (uint8_t *)(sg_soap + lo * n_soap) : nullptr,
+                          8 * (hi - lo) * n_soap, d.copy_in);
+    if (r2) return r2;
+    // G(n_sites, n_soap): the chunk's sites of every column
+    const double *gsrc = G + lo;
+    if (sg_G) {
+      par_copy2d(sg_G + lo, 8 * (size_t)n_sites, G + lo, 8 * (size_t)n_sites, 8 * (hi - lo), (size_t)n_soap);
+      gsrc = sg_G + lo;
+    }
+    CU(cudaMemcpy2DAsync(dG + lo, 8 * (size_t)n_sites, gsrc, 8 * (size_t)n_sites, 8 * (hi - lo), n_soap,
+                         cudaMemcpyHostToDevice, d.copy_in));
+    CU(cudaEventRecord(d.evs[i], d.copy_in));
     CU(cudaStreamWaitEvent(s, d.evs[i], 0));
     return SOAPB_OK;
   };
@@ -2124,10 +2294,22 @@ int soapb_soap_contract(const double *soap, const double *G, double sgn, double 
     CU(cudaEventRecord(d.evs[nch + i], s));
     CU(cudaStreamWaitEvent(d.copy_out, d.evs[nch + i], 0));
     if (p1 > p0)
-      CU(cudaMemcpyAsync(pair + 3 * p0, dP + 3 * p0, 24 * (size_t)(p1 - p0), cudaMemcpyDeviceToHost, d.copy_out));
+      CU(cudaMemcpyAsync(pair_dst + 3 * p0, dP + 3 * p0, 24 * (size_t)(p1 - p0), cudaMemcpyDeviceToHost,
+                         d.copy_out));
+    if (st_pair) CU(cudaEventRecord(d.evs[2 * nch + 1 + i], d.copy_out));
     return SOAPB_OK;
   };
   rc = ctx_contract(d.ctx, &d.batch, dS, dG, SOAPB_G_SITE_FASTEST, sgn, dP, &ch);
+  // the staged pair forces, chunk by chunk as their copies arrive
+  for (int i = 0; rc == 0 && st_pair && n_sites > 0 && i < nch; ++i) {
+    const cudaError_t e = cudaEventSynchronize(d.evs[2 * nch + 1 + i]);
+    if (e != cudaSuccess) {
+      rc = cuda_fail(e, "cudaEventSynchronize");
+      break;
+    }
+    const long long p0 = d.host_off[d.cchunk[i]], p1 = d.host_off[d.cchunk[i + 1]];
+    par_copy(pair + 3 * p0, pair_dst + 3 * p0, 24 * (size_t)(p1 - p0));
+  }
   // whatever ran, no copy may still be in flight when this returns.  The
   // compute stream has waited for every chunk's copies in; made to wait for the
   // last pair forces out as well, its synchronisation covers all three streams.
