@@ -181,7 +181,10 @@ struct DBuf {
 };
 
 // Grow-only pinned host memory: the staging area through which the drop-in
-// layer moves caller arrays that live in pageable memory.
+// layer moves caller arrays that live in pageable memory.  Each of the two
+// areas is held to kStageCap bytes; arrays of larger calls are handed to
+// the CUDA runtime's own pageable copies instead.
+constexpr size_t kStageCap = size_t(256) << 20;
 struct HBuf {
   void *p = nullptr;
   size_t cap = 0;
@@ -1819,7 +1822,7 @@ int plan_get_soap_staging(DropIn &d, GetSoapIn &in, int n_sites, int max_mult, i
   const size_t b_mask = in.pin_mask ? 0 : align16((size_t)n_pairs * n_species);
   const size_t b_p = in.pin_pair ? 0 : align16(8 * (size_t)n_pairs);
   const size_t total = b_nn + b_sp + b_sm + b_mask + 3 * b_p;
-  if (total == 0) return SOAPB_OK;
+  if (total == 0 || total > kStageCap) return SOAPB_OK;  // above the cap: the runtime's copies
   int rc = d.st_in.ensure(total);
   if (rc) return rc;
   uint8_t *q = d.st_in.as<uint8_t>();
@@ -2078,7 +2081,7 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
   GetSoapIn in{n_neigh, species, species_multiplicity, mask, rjs, thetas, phis, is_pinned(n_neigh),
                is_pinned(species), is_pinned(species_multiplicity), is_pinned(mask),
                is_pinned(rjs) && is_pinned(thetas) && is_pinned(phis)};
-  const bool soap_staged = chunked && !is_pinned(soap);
+  const bool soap_staged = chunked && !is_pinned(soap) && 8 * (size_t)n_sites * n_soap <= kStageCap;
   if (chunked) {
     plan_chunks(d.chunk, n_sites, false);
     nch = (int)d.chunk.size() - 1;
@@ -2260,7 +2263,9 @@ int soapb_soap_contract(const double *soap, const double *G, double sgn, double 
   const int nch = (int)d.cchunk.size() - 1;
   if ((rc = dropin_streams(d, 3 * nch + 1))) return rc;
   const size_t b_rows = align16(8 * (size_t)n_sites * n_soap);
-  const bool st_soap = !is_pinned(soap), st_G = !is_pinned(G), st_pair = !is_pinned(pair);
+  const bool big = 2 * b_rows > kStageCap;  // above the cap: the runtime's copies
+  const bool st_soap = !big && !is_pinned(soap), st_G = !big && !is_pinned(G);
+  const bool st_pair = !is_pinned(pair) && 24 * (size_t)n_atom_pairs <= kStageCap;
   if ((st_soap || st_G) && (rc = d.st_in.ensure((st_soap ? b_rows : 0) + (st_G ? b_rows : 0)))) return rc;
   if (st_pair && (rc = d.st_out.ensure(24 * (size_t)n_atom_pairs))) return rc;
   double *sg_soap = st_soap ? d.st_in.as<double>() : nullptr;
