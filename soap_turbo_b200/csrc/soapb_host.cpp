@@ -2363,17 +2363,34 @@ int soapb_get_soap_central_hessian(int32_t n_sites, const int32_t *n_neigh, int3
   cudaStream_t s = d.stream;
   int rc;
   const size_t nsv = (size_t)n_sites * n_soap;
-  if ((rc = upload(d.soap, soap, nsv, s))) return rc;
-  if ((rc = upload(d.vecs, vecs, nsv * n_vec, s))) return rc;
+  const size_t b_soap = align16(8 * nsv), b_vecs = align16(8 * nsv * n_vec);
+  const size_t b_hess = 72 * (size_t)n_vec * n_atom_pairs;
+  // pageable soap and vecs go through the pinned staging area (the host fills
+  // vecs' region while soap's copy runs), pageable hess comes back through it
+  const bool st_soap = !is_pinned(soap) && b_soap + b_vecs <= kStageCap;
+  const bool st_vecs = !is_pinned(vecs) && b_soap + b_vecs <= kStageCap;
+  const bool st_hess = !is_pinned(hess) && b_hess <= kStageCap;
+  if ((st_soap || st_vecs) && (rc = d.st_in.ensure(b_soap + b_vecs))) return rc;
+  if (st_hess && (rc = d.st_out.ensure(b_hess))) return rc;
+  if ((rc = d.soap.ensure(8 * (nsv + 1)))) return rc;
+  if ((rc = d.vecs.ensure(8 * (nsv * n_vec + 1)))) return rc;
   if ((rc = d.hess.ensure(8 * (9 * (size_t)n_vec * n_atom_pairs + 1)))) return rc;
-  if ((rc = ctx_hessian(d.ctx, &d.batch, d.soap.as<double>(), n_vec, d.vecs.as<double>(), d.hess.as<double>())))
+  if ((rc = h2d_in(d.soap.p, soap, st_soap ? d.st_in.as<uint8_t>() : nullptr, 8 * nsv, s))) return rc;
+  if ((rc = h2d_in(d.vecs.p, vecs, st_vecs ? d.st_in.as<uint8_t>() + b_soap : nullptr, 8 * nsv * n_vec, s))) {
+    cudaStreamSynchronize(s);
     return rc;
-  CU(cudaMemcpyAsync(hess, d.hess.p, 72 * (size_t)n_vec * n_atom_pairs, cudaMemcpyDeviceToHost, s));
+  }
+  if ((rc = ctx_hessian(d.ctx, &d.batch, d.soap.as<double>(), n_vec, d.vecs.as<double>(), d.hess.as<double>()))) {
+    cudaStreamSynchronize(s);
+    return rc;
+  }
+  CU(cudaMemcpyAsync(st_hess ? d.st_out.p : (void *)hess, d.hess.p, b_hess, cudaMemcpyDeviceToHost, s));
   if ((rc = dropin_streams(d, 0))) return rc;
   *d.err_host = 0;
   if (d.ctx->err.p)
     CU(cudaMemcpyAsync(d.err_host, d.ctx->err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
+  if (st_hess) par_copy(hess, d.st_out.p, b_hess);
   return input_status(*d.err_host, nullptr);
 }
 
