@@ -244,6 +244,45 @@ def test_dropin_chunks_without_pairs():
         D.set_basis_matrices(None)
 
 
+def test_dropin_batches_of_changing_size():
+    """Consecutive drop-in steps on batches of 1 chunk, 3 chunks and 1 chunk
+    again (chunk plans, events and staging areas re-used or grown between
+    calls), with pageable and page-locked arrays mixed: every step equals the
+    context layer bit for bit."""
+    hp = syn.Hyper(alpha_max=[8, 8, 8], basis="poly3gauss", compress_mode="trivial")
+    ctx = Context(hp)
+    W, S = ctx.basis()
+    D.set_basis_matrices(W, S)
+    try:
+        for n_atoms, seed, pin in ((600, 71, False), (4096, 72, True), (900, 73, False), (4096, 74, False)):
+            st = syn.random_structure(n_atoms, density=0.10, d_min=0.9, fractions=(0.4, 0.4, 0.2), seed=seed)
+            nl = syn.neighbour_list(st, 5.0, 3, central_species=1)
+            w = syn.Workload("step", hp, nl, [st])
+            b = ctx.batch(nl)
+            s_ctx = ctx.descriptor(b, keep=True)
+            G = np.random.default_rng(seed).standard_normal((ctx.n_soap, nl.n_sites))
+            p_ctx = ctx.contract(b, s_ctx, torch.as_tensor(G).cuda()).cpu().numpy()
+            s_ctx = s_ctx.cpu().numpy()
+            keep = []
+
+            def host(a):
+                if not pin:
+                    return np.asfortranarray(a)
+                t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+                keep.append(t)
+                out = t.numpy().reshape(a.shape, order="F")
+                out[...] = a
+                return out
+            soap = host(np.zeros((ctx.n_soap, nl.n_sites)))
+            D.get_soap(**_dropin_args(w, soap), contract=True)
+            np.testing.assert_array_equal(soap.T, s_ctx)
+            pair = np.zeros((3, nl.n_pairs), order="F")
+            D.soap_contract(soap, host(G.T), 1.0, pair)
+            np.testing.assert_array_equal(pair.T, p_ctx)
+    finally:
+        D.set_basis_matrices(None)
+
+
 def test_dropin_soap_cart_der_is_fp64():
     w = WORKLOADS["config1"]()
     r = Run(w, cart=True)
