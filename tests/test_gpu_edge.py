@@ -133,6 +133,30 @@ def test_per_species_cutoffs_and_multi_species_masks():
     check(hp, make_nl(sites, 2))
 
 
+@pytest.mark.parametrize("basis", ["poly3", "poly3gauss"])
+def test_central_atoms_of_two_species(basis):
+    """Sites whose atom carries two species (species(:, i) = (1, 2),
+    species_multiplicity = 2): the self pair has both mask bits, and poly3gauss
+    adds the central-atom term of each species (src/soap_turbo.f90:646-662),
+    with different central weights."""
+    hp = syn.Hyper(alpha_max=[6, 5], basis=basis, central_weight=[1.0, 0.6])
+    rng = np.random.default_rng(9)
+    sites = random_sites(rng, 12, 2)
+    sites = [(cs, [(r, t, p, 3 if i % 5 == 0 else b) for i, (r, t, p, b) in enumerate(ng)])
+             for cs, ng in sites]
+    nl = make_nl(sites, 2)
+    dual = np.arange(nl.n_sites) % 3 == 0
+    species = np.zeros((nl.n_sites, 2), np.int32)
+    species[:, 0] = nl.species[:, 0]
+    species[dual] = (1, 2)
+    mult = np.where(dual, 2, 1).astype(np.int32)
+    mask = nl.mask.copy()
+    first = np.concatenate([[0], np.cumsum(nl.n_neigh)[:-1]])
+    mask[:, first[dual]] = 1                      # the self pair of a two-species atom
+    nl = dataclasses.replace(nl, species=species, species_multiplicity=mult, mask=mask)
+    check(hp, nl)
+
+
 @pytest.mark.parametrize("l_max", [1, 3, 6])
 def test_small_l_max(l_max):
     hp = syn.Hyper(alpha_max=[8, 8, 8], l_max=l_max, basis="poly3gauss", compress_mode="trivial")
