@@ -227,3 +227,27 @@ def test_dropin_central_hessian(precision):
         D.set_precision("mixed")
         D.set_legacy_filter_seed(True)
         D.set_basis_matrices(None)
+
+
+def test_two_species_atoms():
+    """Neighbours and central atoms that carry two species (mask rows with
+    both bits, species_multiplicity 2), as in test_gpu_edge, through the
+    Hessian."""
+    import dataclasses
+    hp, nl = _case("gauss_2sp", seed=5)
+    rng = np.random.default_rng(4)
+    mask = nl.mask.copy()
+    mask[:, rng.random(nl.n_pairs) < 0.2] = 1
+    first = np.concatenate([[0], np.cumsum(nl.n_neigh)[:-1]])
+    dual = np.arange(nl.n_sites) % 3 == 0
+    mask[:, first[dual]] = 1
+    species = np.zeros((nl.n_sites, 2), np.int32)
+    species[:, 0] = nl.species[:, 0]
+    species[dual] = (1, 2)
+    nl = dataclasses.replace(nl, mask=mask, species=species,
+                             species_multiplicity=np.where(dual, 2, 1).astype(np.int32))
+    ctx = Context(hp, legacy_filter_seed=False)
+    W, S = ctx.basis()
+    ref, vecs, href = _oracle(hp, nl, W, S, 2)
+    hess = ctx.central_hessian(ctx.batch(nl), torch.as_tensor(vecs).cuda()).cpu().numpy()
+    assert max_rel_err(hess, href) <= FP64_TOL
