@@ -138,9 +138,12 @@ __device__ __forceinline__ int build_entries(const DevParams &P, const DevBatch 
     const unsigned bits = B.bits[k];
     const int j = k - p_begin;
 #pragma unroll
+    // a pair at or beyond rcut_max has no angular row (the reference zeroes
+    // its angular coefficients, src/soap_turbo_angular.f90:549-574); it only
+    // matters for poly3operator, whose radial part has no rcut_hard cut
     for (int s = 0; s < SOAPB_MAX_SPECIES; ++s) {
       if (s >= P.n_species) break;
-      const bool ok = ((bits >> s) & 1u) && r < P.rad[s].rcut_hard &&
+      const bool ok = ((bits >> s) & 1u) && r < P.rad[s].rcut_hard && r < P.rcut_max &&
                       (vjp ? (j > 0) : (j > 0 || P.rad[s].do_central));
       if (ok) rb |= 1u << s;
     }

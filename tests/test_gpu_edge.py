@@ -133,7 +133,7 @@ def test_per_species_cutoffs_and_multi_species_masks():
     check(hp, make_nl(sites, 2))
 
 
-@pytest.mark.parametrize("basis", ["poly3", "poly3gauss"])
+@pytest.mark.parametrize("basis", ["poly3", "poly3gauss", "poly3operator"])
 def test_central_atoms_of_two_species(basis):
     """Sites whose atom carries two species (species(:, i) = (1, 2),
     species_multiplicity = 2): the self pair has both mask bits, and poly3gauss

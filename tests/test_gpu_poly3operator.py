@@ -96,3 +96,29 @@ def test_dropin_matches_the_context_layer():
         np.testing.assert_array_equal(soap.T, s_ctx)
     finally:
         D.set_basis_matrices(None)
+
+
+@pytest.mark.parametrize("basis", ["poly3operator", "poly3gauss"])
+def test_neighbour_list_with_a_skin(basis):
+    """A neighbour list built beyond the cutoff (5.6 A for rcut_hard 5.0, as an
+    MD code's list with a skin): pairs at or beyond rcut_max have no angular
+    coefficients in the reference (src/soap_turbo_angular.f90:549-574), so they
+    add nothing -- also for poly3operator, whose radial part has no rcut_hard
+    cut of its own."""
+    hp = syn.Hyper(alpha_max=[6, 6], l_max=6, basis=basis)
+    st = syn.random_structure(40, density=0.1, d_min=1.0, fractions=(0.5, 0.5), seed=12)
+    nl = syn.neighbour_list(st, 5.6, 2)
+    assert (nl.rjs >= 5.0).any()
+    ctx = Context(hp)
+    W, S = ctx.basis()
+    ref = O.get_soap(hp, nl, W, S, do_derivatives=True, cart_der=True)
+    b = ctx.batch(nl)
+    soap = ctx.descriptor(b, keep=True)
+    assert site_rel_err(soap.cpu().numpy(), ref.soap) <= SOAP_TOL
+    G = np.random.default_rng(4).standard_normal((ctx.n_soap, nl.n_sites))
+    pair = ctx.contract(b, soap, torch.as_tensor(G).cuda()).cpu().numpy()
+    assert max_rel_err(pair, ref.contract(G, 1.0)) <= VJP_TOL
+    assert not pair[nl.rjs >= 5.0].any()
+    s64, cart = ctx.descriptor_fp64(b, cart=True)
+    assert site_rel_err(s64.cpu().numpy(), ref.soap) <= FP64_TOL
+    assert max_rel_err(cart.cpu().numpy(), ref.soap_cart_der) <= FP64_TOL
