@@ -114,7 +114,7 @@ def test_cutoff_edges_poles_and_small_distances():
     dict(atom_sigma_t_scaling=0.05), dict(global_scaling=2.0), dict(nf=3.0),
     dict(rcut_soft=5.0), dict(scaling_mode="none"), dict(central_weight=0.0),
 ])
-@pytest.mark.parametrize("basis", ["poly3", "poly3gauss"])
+@pytest.mark.parametrize("basis", ["poly3", "poly3gauss", "poly3operator"])
 def test_hyperparameter_variants(variant, basis):
     hp = dataclasses.replace(syn.Hyper(alpha_max=[7, 6], basis=basis), **variant)
     nl = make_nl(random_sites(np.random.default_rng(11), 12, 2), 2)
