@@ -26,3 +26,10 @@ def test_darby_modes_benchmark_basis(mode):
     hp = syn.Hyper(alpha_max=[8, 8, 8], l_max=8, basis="poly3gauss", compress_mode=mode)
     nl = make_nl(random_sites(np.random.default_rng(23), 16, 3, lo=30, hi=80), 3)
     check(hp, nl)
+
+
+@pytest.mark.parametrize("basis", ["poly3", "poly3operator"])
+def test_darby_mode_other_bases(basis):
+    hp = syn.Hyper(alpha_max=[4, 4, 4], l_max=4, basis=basis, compress_mode="1_2")
+    nl = make_nl(random_sites(np.random.default_rng(29), 20, 3), 3)
+    check(hp, nl)

@@ -168,6 +168,8 @@ def test_small_l_max(l_max):
     syn.Hyper(alpha_max=[10], l_max=8, basis="poly3gauss"),
     syn.Hyper(alpha_max=[1], l_max=4, basis="poly3"),
     syn.Hyper(alpha_max=[1, 2], l_max=4, basis="poly3gauss"),
+    syn.Hyper(alpha_max=[5, 4], l_max=10, basis="poly3operator"),
+    syn.Hyper(alpha_max=[2], l_max=3, basis="poly3operator"),
 ])
 def test_generic_kernel_shapes(hp):
     # l_max > 8 or alpha > 8 take the generic kernel instantiation.  alpha = 10
