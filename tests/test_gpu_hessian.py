@@ -251,3 +251,18 @@ def test_two_species_atoms():
     ref, vecs, href = _oracle(hp, nl, W, S, 2)
     hess = ctx.central_hessian(ctx.batch(nl), torch.as_tensor(vecs).cuda()).cpu().numpy()
     assert max_rel_err(hess, href) <= FP64_TOL
+
+
+def test_neighbour_list_with_a_skin():
+    """Pairs beyond rcut_max (a list built to 5.6 A for rcut_hard 5.0) add
+    nothing: their Hessian blocks are zero and the others match the oracle."""
+    hp = syn.Hyper(**CASES["gauss_2sp"])
+    st = syn.random_structure(28, density=0.1, d_min=1.0, fractions=(0.5, 0.5), seed=6)
+    nl = syn.neighbour_list(st, 5.6, hp.n_species)
+    assert (nl.rjs >= 5.0).any()
+    ctx = Context(hp, legacy_filter_seed=False)
+    W, S = ctx.basis()
+    ref, vecs, href = _oracle(hp, nl, W, S, 2)
+    hess = ctx.central_hessian(ctx.batch(nl), torch.as_tensor(vecs).cuda()).cpu().numpy()
+    assert max_rel_err(hess, href) <= FP64_TOL
+    assert not hess[nl.rjs >= 5.0].any()
