@@ -181,6 +181,21 @@ def test_generic_kernel_shapes(hp):
           fp64=not big_alpha)
 
 
+@pytest.mark.parametrize("basis", ["poly3", "poly3gauss"])
+def test_eight_species(basis):
+    """The species limit of the kernels (8: one mask byte per pair) with
+    neighbours of two species at once; a ninth species is refused."""
+    hp = syn.Hyper(alpha_max=[2, 3, 2, 1, 3, 2, 2, 3], l_max=4, basis=basis,
+                   central_weight=[1.0, 0.5, 1.0, 0.8, 1.0, 1.0, 0.3, 1.0])
+    rng = np.random.default_rng(31)
+    sites = random_sites(rng, 16, 8)
+    sites = [(cs, [(r, t, p, b | (1 << ((cs + i) % 8)) if i % 3 == 0 else b)
+                   for i, (r, t, p, b) in enumerate(ng)]) for cs, ng in sites]
+    check(hp, make_nl(sites, 8))
+    with pytest.raises(_lib.SoapError):
+        Context(syn.Hyper(alpha_max=[2] * 9, l_max=4, basis=basis))
+
+
 def test_large_sites_span_chunks_and_rounds():
     rng = np.random.default_rng(9)
     sites = random_sites(rng, 3, 3, lo=140, hi=300, rmax=5.0) + random_sites(rng, 3, 3, lo=65, hi=90)
