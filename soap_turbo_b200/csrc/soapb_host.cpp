@@ -203,8 +203,11 @@ struct HBuf {
   T *as() const { return (T *)p; }
 };
 
-// Whether a caller's host array is page-locked (cudaHostAlloc'd or
-// registered), so that the copy engines can read or write it directly.
+// Whether the copy engines can use a caller's array directly: page-locked
+// host memory (cudaHostAlloc'd or registered), and also device or managed
+// memory, which must not reach the host-side staging copies (the runtime's
+// copy then either handles it or reports the misuse).  Only ordinary pageable
+// host memory is staged.
 bool is_pinned(const void *ptr) {
   if (!ptr) return true;
   cudaPointerAttributes a;
@@ -212,7 +215,7 @@ bool is_pinned(const void *ptr) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeHost;
+  return a.type != cudaMemoryTypeUnregistered;
 }
 
 // Host copies between a caller's pageable array and the pinned staging area,
