@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--quick", action="store_true",
                     help="time the two kernels only (no FP64 path, e2e, CPU baseline or peak "
                          "measurement); for profiling runs")
+    ap.add_argument("--fp64", action="store_true",
+                    help="time the plain FP64 form alone (materialised soap_cart_der, then "
+                         "contracted) on the configuration; for profiling runs")
     return ap.parse_args()
 
 
@@ -78,6 +81,32 @@ CONFIG_NAMES = {
 def workload(rank, seed, idx=2):
     from soap_turbo_b200 import synthetic as syn
     return syn.config(idx, seed=seed + 7919 * rank)
+
+
+def cpu_model():
+    """The host CPU's model name (from /proc/cpuinfo), for the CPU baseline."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def fp32_clock_peak_tflops(torch):
+    """FP32 CUDA-core peak from the clock: SMs x 128 FP32 lanes x 2 (FMA) x
+    the maximum SM clock nvidia-smi reports."""
+    try:
+        out = subprocess.run(["nvidia-smi", "-i", str(torch.cuda.current_device()),
+                              "--query-gpu=clocks.max.sm", "--format=csv,noheader,nounits"],
+                             capture_output=True, text=True, timeout=30).stdout
+        mhz = float(out.strip().splitlines()[0])
+    except (OSError, ValueError, IndexError, subprocess.SubprocessError):
+        return None
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    return sms * 128 * 2 * mhz * 1e6 / 1e12
 
 
 def dist_env():
@@ -137,6 +166,7 @@ def run_reference(args):
         "data": "synthetic", "config": {"workload": WORKLOAD, "sites": w.nl.n_sites,
                                          "pairs": w.nl.n_pairs},
         "cpu_baseline": {"value": rate, "unit": "envs/s", "cores": cores, "kind": "port",
+                         "cpu_model": cpu_model(),
                          "sample": f"{n} full steps of the workload ({w.nl.n_sites} sites), median"},
         "e2e": {"value": rate, "unit": "envs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -374,14 +404,20 @@ def run_ours(args):
     ms_step_max = shard.max_over_ranks(ms_step, device=dev)
     value = ws * nl.n_sites / (ms_step_max * 1e-3)
 
-    if args.quick:
+    if args.quick or args.config != 2:
         if rank == 0:
-            print(json.dumps({"metric": METRIC, "value": value, "unit": "envs/s", "n_gpus": ws,
-                              "steps": K, "warmup": args.warmup, "ms_per_step": ms_step_max,
-                              "kernel_ms": kernel_ms, "autotune": tune,
-                              "quick": True, "gpu_launches": int(launches),
-                              "config": {"workload": wname, "sites_per_gpu": nl.n_sites,
-                                         "pairs_per_gpu": nl.n_pairs}}), flush=True)
+            line = {"metric": METRIC, "value": value, "unit": "envs/s", "n_gpus": ws,
+                    "steps": K, "warmup": args.warmup, "ms_per_step": ms_step_max,
+                    "kernel_ms": kernel_ms, "autotune": tune, "gpu_launches": int(launches),
+                    "dtype": "f32", "clocks": clk.summary(),
+                    "config": {"workload": wname, "sites_per_gpu": nl.n_sites,
+                               "pairs_per_gpu": nl.n_pairs,
+                               "l2": "flushed between timed steps (256 MB write)"}}
+            if args.quick:
+                line["quick"] = True
+            else:
+                line.update(config_accuracy(args, torch, ctx, w, s, p, G_host))
+            print(json.dumps(line), flush=True)
         if ws > 1:
             torch.distributed.barrier()
             torch.distributed.destroy_process_group()
@@ -478,18 +514,25 @@ def run_ours(args):
                    P_j, P_el, h_soap, None, contract=True)
         D.soap_contract(h_soap, h_G, 1.0, h_pair)
 
-    def wall(f, n):
+    def wall(f, n, soap_arr):
+        # The caller zeroes soap before each get_soap, as the reference's callers
+        # do (a compressed soap is added into); that host write is the caller's
+        # and stays outside the timed calls.
         for _ in range(3):
+            soap_arr.fill(0.0)
             f()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
+        total = 0.0
         for _ in range(n):
+            soap_arr.fill(0.0)
+            t0 = time.perf_counter()
             f()
-        return (time.perf_counter() - t0) / n
+            total += time.perf_counter() - t0
+        return total / n
     n_e2e = max(20, min(200, K // 5))
-    t_e2e = shard.max_over_ranks(wall(e2e_step, n_e2e), device=dev)
-    t_e2e_py = shard.max_over_ranks(wall(e2e_step_python, n_e2e), device=dev)
-    t_e2e_pg = shard.max_over_ranks(wall(e2e_step_pageable, n_e2e), device=dev)
+    t_e2e = shard.max_over_ranks(wall(e2e_step, n_e2e, h_soap), device=dev)
+    t_e2e_py = shard.max_over_ranks(wall(e2e_step_python, n_e2e, h_soap), device=dev)
+    t_e2e_pg = shard.max_over_ranks(wall(e2e_step_pageable, n_e2e, pg["soap"]), device=dev)
     h2d = (h_nn.nbytes + h_sp.nbytes + h_sm.nbytes + h_mask.nbytes + h_rjs.nbytes + h_th.nbytes +
            h_ph.nbytes + h_soap.nbytes + h_G.nbytes)
     d2h = h_soap.nbytes + h_pair.nbytes
@@ -501,6 +544,7 @@ def run_ours(args):
     t_dom = kernel_ms[dominant] * 1e-3
     peak32 = gemm_peak_tflops(torch, torch.float32)
     peak64 = gemm_peak_tflops(torch, torch.float64)
+    peak32_clock = fp32_clock_peak_tflops(torch)
     # the pair kernel's arithmetic is FP64 (radial integrals, W transform)
     peak = peak64 if dominant == "pair" else peak32
     achieved = flops[dominant] / t_dom / 1e12
@@ -543,7 +587,9 @@ def run_ours(args):
             "e2e": {"value": ws * nl.n_sites / t_e2e, "unit": "envs/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h),
                     "path": "the drop-in C ABI, soapb_get_soap(contract=1) + soapb_soap_contract, on pinned "
-                            "host arrays, argument lists built once (as the Fortran shim passes them)",
+                            "host arrays, argument lists built once (as the Fortran shim passes them); "
+                            "soap comes in too (a compressed soap is added into, as in the reference), "
+                            "zeroed by the caller before each step outside the timed calls",
                     "python_wrapper_ms_per_step": t_e2e_py * 1e3,
                     "pageable_ms_per_step": t_e2e_pg * 1e3},
             "gpu_launches": int(launches),
@@ -560,6 +606,9 @@ def run_ours(args):
                                         + " 8192^3); MEASURED_PEAKS.json has HBM and bf16 "
                                           "tensor peaks only",
                          "peaks_measured_tflops": {"fp32": peak32, "fp64": peak64},
+                         "fp32_clock_peak_tflops": peak32_clock,
+                         "frac_of_fp32_clock_peak": (achieved / peak32_clock
+                                                     if peak32_clock and dominant != "pair" else None),
                          "step": {"algorithmic_flops": flops["total"],
                                   "achieved_tflops": flops["total"] / (ms_step_max * 1e-3) / 1e12,
                                   "frac_of_fp32": flops["total"] / (ms_step_max * 1e-3) / 1e12 / peak32},
@@ -570,13 +619,95 @@ def run_ours(args):
         }
         if ws == 1:
             result["cpu_baseline"] = {"value": cpu_rate, "unit": "envs/s", "cores": cores,
-                                      "kind": "port",
+                                      "kind": "port", "cpu_model": cpu_model(),
                                       "sample": f"{n_cpu} full steps ({nl.n_sites} sites) of the "
                                                 f"FP64 C restatement, median {t_cpu * 1e3:.1f} ms"}
         print(json.dumps(result), flush=True)
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def config_accuracy(args, torch, ctx, w, soap_t, pair_t, G_host):
+    """Errors of the timed step's outputs against the FP64 oracle on every site
+    and pair of the configuration (the oracle over contiguous site ranges), and
+    the plain FP64 GPU form beside the mixed path: on the whole configuration
+    when its soap_cart_der is at most 20 GB, else (config 5) on a 16384-atom
+    slice of the same configuration, both timed and both against the oracle."""
+    from soap_turbo_b200 import synthetic as syn
+    from soap_turbo_b200.context import Context
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    W, S = ctx.basis()
+    nl = w.nl
+    t0 = time.perf_counter()
+    ref_soap, ref_pair = O.soap_and_vjp_chunked(w.hyper, nl, W, S, G_host)
+    t_oracle = time.perf_counter() - t0
+    soap, pair = soap_t.cpu().numpy(), pair_t.cpu().numpy()
+    rel = np.abs(soap - ref_soap).max(1) / np.abs(ref_soap).max(1)
+    out = {"error_vs_fp64_oracle": {
+        "soap_max_rel": float(rel.max()), "soap_median_rel": float(np.median(rel)),
+        "vjp_max_rel": float(np.abs(pair - ref_pair).max() / np.abs(ref_pair).max()),
+        "coverage": f"all {nl.n_sites} sites and {nl.n_pairs} pairs",
+        "oracle_s": t_oracle, "oracle_threads": O.num_threads()}}
+    dev = soap_t.device
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def timed(f, n=10):
+        for _ in range(2):
+            f()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(n):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            f()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    cart_bytes = 8 * 3 * ctx.n_soap * nl.n_pairs
+    if cart_bytes <= 20e9:
+        sw, sctx, sb, G_s, where = w, ctx, None, G_host, "the whole configuration"
+    else:
+        sw = syn.config(args.config, seed=args.seed, scale=16384 / 262144)
+        sctx = Context(sw.hyper)
+        G_s = np.random.default_rng(args.seed).standard_normal((sctx.n_soap, sw.nl.n_sites))
+        where = f"a 16384-atom slice of the configuration ({sw.nl.n_sites} sites, {sw.nl.n_pairs} pairs)"
+    sb = sctx.batch(sw.nl)
+    Gd = torch.as_tensor(G_s).to(dev)
+    res = {}
+
+    def mixed():
+        s_ = sctx.descriptor(sb, keep=True)
+        res["mixed"] = (s_, sctx.contract(sb, s_, Gd))
+
+    def fp64():
+        s_, c_ = sctx.descriptor_fp64(sb, cart=True)
+        res["fp64"] = (s_, sctx.contract_cart_der(sb, c_, Gd))
+
+    ms_mixed = timed(mixed)
+    ms_fp64 = timed(fp64)
+    if sw is w:
+        rs, rp = ref_soap, ref_pair
+    else:
+        Ws, Ss = sctx.basis()
+        rs, rp = O.soap_and_vjp_chunked(sw.hyper, sw.nl, Ws, Ss, G_s)
+    errs = {}
+    for k, (s_, p_) in res.items():
+        s_, p_ = s_.cpu().numpy(), p_.cpu().numpy()
+        errs[k] = {"soap_max_rel": float((np.abs(s_ - rs).max(1) / np.abs(rs).max(1)).max()),
+                   "vjp_max_rel": float(np.abs(p_ - rp).max() / np.abs(rp).max())}
+    n = sw.nl.n_sites
+    out["fp64_plain"] = {"on": where, "ms_per_step": ms_fp64, "value": n / (ms_fp64 * 1e-3),
+                         "mixed_ms_per_step": ms_mixed, "mixed_value": n / (ms_mixed * 1e-3),
+                         "speedup_of_mixed": ms_fp64 / ms_mixed, "unit": "envs/s",
+                         "error_vs_fp64_oracle": errs,
+                         "how": "device time per step (descriptor + VJP; FP64: soap_cart_der materialised, "
+                                "then contracted), L2 flushed before each step, median of 10"}
+    return out
 
 
 def run_hessian(args):
@@ -686,8 +817,52 @@ def run_neighbors(args):
     print(json.dumps(line), flush=True)
 
 
+def run_fp64(args):
+    """The plain FP64 form alone on the configuration: descriptor with
+    soap_cart_der materialised, then the contraction with G; device time per
+    step (CUDA events, L2 flushed before each step) and per kernel kind."""
+    import torch
+    from soap_turbo_b200.context import Context
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    w = workload(0, args.seed, args.config)
+    nl = w.nl
+    ctx = Context(w.hyper)
+    b = ctx.batch(nl)
+    G = torch.as_tensor(np.random.default_rng(args.seed).standard_normal((ctx.n_soap, nl.n_sites))).to(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(max(args.warmup, 3)):
+        s64, cart = ctx.descriptor_fp64(b, cart=True)
+        ctx.contract_cart_der(b, cart, G)
+    torch.cuda.synchronize()
+    times = []
+    n0 = ctx.launch_count
+    for _ in range(max(args.steps, 1)):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s64, cart = ctx.descriptor_fp64(b, cart=True)
+        ctx.contract_cart_der(b, cart, G)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    launches = (ctx.launch_count - n0) / max(args.steps, 1)
+    ms = statistics.median(times)
+    cart_bytes = 8 * 3 * ctx.n_soap * nl.n_pairs
+    print(json.dumps({"metric": "plain FP64 form, envs/s", "unit": "envs/s",
+                      "value": nl.n_sites / (ms * 1e-3), "ms_per_step": ms, "steps": args.steps,
+                      "warmup": args.warmup, "gpu_launches_per_step": launches,
+                      "soap_cart_der_bytes": cart_bytes,
+                      "hbm_floor_ms": 2 * cart_bytes / (hbm_peak() * 1e9) * 1e3,
+                      "config": {"workload": WORKLOAD if args.config == 2 else CONFIG_NAMES[args.config],
+                                 "sites": nl.n_sites, "pairs": nl.n_pairs}}), flush=True)
+
+
 def main():
     args = parse()
+    if args.fp64:
+        run_fp64(args)
+        return
     if args.neighbors:
         run_neighbors(args)
         return

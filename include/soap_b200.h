@@ -86,8 +86,12 @@ const char *soapb_version(void);
  * basis: "poly3" | "poly3gauss" | "poly3operator"; scaling_mode: "polynomial" | other
  * (poly3operator with another scaling mode: amplitude 1, which the reference
  * leaves unset).
- * soap is overwritten (the reference accumulates into it when compressing,
- * so its callers pass it zeroed; the results then agree).
+ * soap and soap_cart_der are intent(inout) as in the reference: with
+ * compress_soap the descriptor is added into the caller's soap before the norm
+ * is taken (src/soap_turbo.f90:798-802), without it soap is overwritten; the
+ * neighbour columns of soap_cart_der are overwritten and each site's self
+ * column is accumulated into (:888-892).  The reference's callers pass both
+ * zeroed.
  * do_derivatives && !contract: soap_cart_der (3, n_soap, n_atom_pairs) is
  * written, computed in FP64 as the reference does; otherwise it may be NULL.
  * do_derivatives && contract: the state for soapb_soap_contract is kept.
@@ -239,6 +243,21 @@ int soapb_set_threads_per_site(soapb_context *ctx, int32_t threads);
  * CTA size changes the summation grouping within FP32 rounding. */
 int soapb_autotune(soapb_context *ctx, const soapb_batch *batch, int32_t *choice);
 
+/* Radial expansion of the mixed path.  With atom_sigma_r_scaling = 0 (poly3,
+ * poly3gauss), every R_n(r) and dR_n/dr is a fixed function of r per species:
+ * soapb_create fits piecewise polynomials to the FP64 expansion (segments of at
+ * most 0.05 rcut_hard, degree 7, split at the reference's branch points in r,
+ * src/soap_turbo_radial.f90:589-635, 721-769, 875-908) and checks them in FP32
+ * against it; when the largest error relative to each function's largest value
+ * is at most 5e-7 the pair kernel evaluates the tables in FP32 instead of
+ * running the FP64 expansion per pair.  soapb_radial_tables reports whether
+ * the tables are in use and that error (-1: not tabulated: sigma scaling,
+ * poly3operator, or the check failed); soapb_set_radial_tables(ctx, 0) makes
+ * the pair kernel use the FP64 expansion (1: the tables when they passed).  A
+ * change discards the state kept for soapb_contract. */
+int soapb_set_radial_tables(soapb_context *ctx, int32_t enable);
+int soapb_radial_tables(const soapb_context *ctx, int32_t *in_use, double *max_err);
+
 /* Descriptor of one batch: d_soap (n_soap, n_sites), normalised.  With
  * keep_for_contract, the expansion coefficients c_nlm and norms stay in the
  * context for soapb_contract on the same batch. */
@@ -259,8 +278,12 @@ int soapb_descriptor(soapb_context *ctx, const soapb_batch *batch, double *d_soa
  * instead of buffers that grow on demand; the context's constant tables,
  * allocated once by soapb_create, are read as by soapb_descriptor.
  *  - The context's device must be current.  The first call on a device looks
- *    up the array's address (a one-time set-up); make that first call before
- *    any stream capture.
+ *    up the array's address (a one-time set-up, kept for the process).  CUDA
+ *    loads a library's device code lazily by default, so that first call is
+ *    also when the 64 MiB are committed on the device: make it at start-up,
+ *    before reserving a memory pool and before any stream capture.  After a
+ *    cudaDeviceReset the array has a new address, which the kept one does not
+ *    follow: do not call this entry point again in that process.
  *  - A batch needing more scratch than the array holds is rejected with
  *    SOAPB_ERR_ARGUMENT and a message giving both sizes.  The need is about
  *    (2 n_species amax + row) * 4 bytes per atom pair, with amax = 8 and a
@@ -270,8 +293,9 @@ int soapb_descriptor(soapb_context *ctx, const soapb_batch *batch, double *d_soa
  *  - All calls share the array and it keeps the last call's contents; calls
  *    whose work overlaps on the GPU (other streams, host threads or contexts
  *    on the same device) race on it: serialise them.
- *  - Bad inputs are not reported through soapb_check_inputs, which reads the
- *    context's own scratch. */
+ *  - soapb_check_inputs on the context reports the call's input errors (a
+ *    non-finite or negative pair input, a bad CSR), read from the array's
+ *    error word, until another call of this entry point on the device. */
 int soapb_descriptor_noalloc(soapb_context *ctx, const soapb_batch *batch, double *d_soap);
 
 /* Force VJP on the batch of the last soapb_descriptor(keep_for_contract = 1):
@@ -307,9 +331,9 @@ int soapb_central_hessian(soapb_context *ctx, const soapb_batch *batch, const do
 int soapb_contract_cart_der(soapb_context *ctx, const soapb_batch *batch, const double *d_cart,
                             const double *d_G, int32_t g_layout, double sgn, double *d_pair);
 
-/* Status of the device-side input checks of the last calls on this context
- * (waits for the stream): SOAPB_OK or SOAPB_ERR_INPUT, with the first bad
- * pair index in *bad_pair (or -1). */
+/* Status of the device-side input checks of the last call on this context
+ * that checked its inputs (waits for the stream): SOAPB_OK or SOAPB_ERR_INPUT,
+ * with the first bad pair index in *bad_pair (or -1). */
 int soapb_check_inputs(soapb_context *ctx, int64_t *bad_pair);
 
 /* Neighbour list of one periodic structure, built on the device in the
@@ -340,6 +364,16 @@ int soapb_build_neighbors(soapb_context *ctx, int32_t n_atoms, const double *d_p
                           const double *lattice, const int32_t *d_atom_species, int32_t max_mult,
                           const int32_t *d_atom_mult, int32_t n_sites, const int32_t *d_sites,
                           double rcut, soapb_batch *batch, const int32_t **d_neigh_atom);
+
+/* Self-test of the bounded wait in the CSR offset scan (no counterpart in the
+ * reference): one tile of a two-tile scan runs while its predecessor's state is
+ * prepared on the host -- published (publish_predecessor = 1: the wait ends at
+ * once) or never published (0: the wait gives up after max_spins spins).
+ * Returns the status the scan left: SOAPB_OK, or SOAPB_ERR_CUDA for a wait
+ * that gave up; *last_offset (may be NULL) receives the scan's total, 4096
+ * with the predecessor published.  Allocates and frees small device buffers on
+ * the current device and synchronises it. */
+int soapb_selftest_scan_wait(int32_t max_spins, int32_t publish_predecessor, int64_t *last_offset);
 
 /* Number of kernel launches issued by this context since creation. */
 int soapb_launch_count(const soapb_context *ctx, int64_t *count);

@@ -114,6 +114,28 @@ def inverse_sqrt(S: np.ndarray) -> np.ndarray:
     return W
 
 
+def inverse_sqrt_lapack_route(S: np.ndarray) -> np.ndarray:
+    """W = (S^{1/2})^{-1} the way the reference forms it in FP64 LAPACK
+    (src/soap_turbo_radial.f90:1052-1087 poly3, :1177-1212 poly3gauss): dgesvd
+    of S, S^{1/2} = U diag(sqrt(svd)) VT, then dpotrf + dpotri of S^{1/2} and
+    the upper triangle mirrored.  scipy's bundled LAPACK stands in for the
+    (unpinned) LAPACK the reference links."""
+    from scipy.linalg import lapack
+    S = np.asfortranarray(S, dtype=np.float64)
+    u, svd, vt, info = lapack.dgesvd(S, compute_uv=1, full_matrices=1)
+    if info != 0:
+        raise RuntimeError("dgesvd failed")
+    half = np.asfortranarray((u * np.sqrt(svd)) @ vt)
+    c, info = lapack.dpotrf(half, lower=0)
+    if info != 0:
+        raise RuntimeError("dpotrf failed")
+    inv, info = lapack.dpotri(c, lower=0)
+    if info != 0:
+        raise RuntimeError("dpotri failed")
+    up = np.triu(inv)
+    return np.asfortranarray(up + np.triu(inv, 1).T)
+
+
 def basis_matrices(hyper):
     """Block-diagonal (n_max, n_max) W and S, Fortran order."""
     n_max = hyper.n_max
@@ -297,11 +319,15 @@ def compress_arrays(hyper):
 
 
 def get_soap(hyper, nl, W, S, do_derivatives=True, cart_der=False, legacy_filter_seed=True,
-             compress=None, hessian=False) -> Result:
+             compress=None, hessian=False, soap_init=None, cart_init=None) -> Result:
     """Run the oracle get_soap.  ``cart_der`` materialises soap_cart_der
     (contract = .false.); the expansion is always kept for ``contract``;
     ``hessian`` also keeps the second radial derivatives central_hessian needs
-    (the reference's soap_hessian_enabled; unified filter seed only)."""
+    (the reference's soap_hessian_enabled; unified filter seed only).
+    ``soap_init`` (n_sites, n_soap) and ``cart_init`` (n_pairs, n_soap, 3) are
+    the caller's arrays on entry (zero when None): the reference adds the
+    compressed descriptor into soap and the self columns into soap_cart_der
+    (src/soap_turbo.f90:798-802, 888-892)."""
     n_species = hyper.n_species
     if compress is None:
         compress = compress_arrays(hyper)
@@ -356,7 +382,11 @@ def get_soap(hyper, nl, W, S, do_derivatives=True, cart_der=False, legacy_filter
         a.compress = 0
         n_soap = n_unc
     soap = np.zeros((nl.n_sites, n_soap))
+    if soap_init is not None:
+        soap[...] = soap_init
     cart = np.zeros((nl.n_pairs, n_soap, 3)) if (do_derivatives and cart_der) else None
+    if cart is not None and cart_init is not None:
+        cart[...] = cart_init
     ctx = C.c_void_p()
     rc = lib().or_get_soap2(C.byref(a), int(do_derivatives), int(bool(hessian)), _p(soap, _f64p),
                             _p(cart, _f64p) if cart is not None else None, C.byref(ctx))
@@ -365,3 +395,52 @@ def get_soap(hyper, nl, W, S, do_derivatives=True, cart_der=False, legacy_filter
     keep.update(n_sites=nl.n_sites, n_pairs=nl.n_pairs, n_max=n_max,
                 k_max=(hyper.l_max + 1) * (hyper.l_max + 2) // 2, arrays=arrays, args=a)
     return Result(soap, cart, ctx.value, keep)
+
+
+def _slice_sites(nl, lo, hi):
+    """The CSR rows of sites [lo, hi) as a neighbour list of their own."""
+    import copy
+    off = np.concatenate([[0], np.cumsum(nl.n_neigh)])
+    p0, p1 = int(off[lo]), int(off[hi])
+    out = copy.copy(nl)
+    out.n_sites = hi - lo
+    out.n_neigh = nl.n_neigh[lo:hi]
+    out.rjs, out.thetas, out.phis = nl.rjs[p0:p1], nl.thetas[p0:p1], nl.phis[p0:p1]
+    out.mask = nl.mask[:, p0:p1]
+    out.species = nl.species[lo:hi]
+    out.species_multiplicity = nl.species_multiplicity[lo:hi]
+    return out, p0, p1
+
+
+def soap_and_vjp_chunked(hyper, nl, W, S, G, sgn=1.0, max_pairs=400_000, legacy_filter_seed=True,
+                         sites=None):
+    """get_soap + soap_contract over contiguous site ranges of at most
+    ``max_pairs`` pairs each: every site's descriptor and every pair's force
+    depend on its own site's CSR row alone (src/soap_turbo.f90:619-664,
+    1723-1884), so this equals one call on the whole list while bounding the
+    oracle's memory (~3.5 KB of expansions per pair) at full configuration
+    sizes.  G: (n_soap, n_sites), the reference's G(n_sites, n_soap).
+    ``sites`` (optional, sorted) restricts the work to those sites; rows of
+    the others are left NaN.  Returns soap (n_sites, n_soap), pair (n_pairs, 3)."""
+    off = np.concatenate([[0], np.cumsum(nl.n_neigh)]).astype(np.int64)
+    n_soap = G.shape[0]
+    soap = np.full((nl.n_sites, n_soap), np.nan)
+    pair = np.full((nl.n_pairs, 3), np.nan)
+    want = np.ones(nl.n_sites, bool) if sites is None else np.zeros(nl.n_sites, bool)
+    if sites is not None:
+        want[np.asarray(sites)] = True
+    lo = 0
+    while lo < nl.n_sites:
+        if not want[lo]:
+            lo += 1
+            continue
+        hi = lo + 1
+        while hi < nl.n_sites and want[hi] and off[hi + 1] - off[lo] <= max_pairs:
+            hi += 1
+        sub, p0, p1 = _slice_sites(nl, lo, hi)
+        r = get_soap(hyper, sub, W, S, do_derivatives=True, legacy_filter_seed=legacy_filter_seed)
+        soap[lo:hi] = r.soap
+        pair[p0:p1] = r.contract(np.ascontiguousarray(G[:, lo:hi]), sgn)
+        del r
+        lo = hi
+    return soap, pair

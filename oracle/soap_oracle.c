@@ -833,9 +833,13 @@ static void species_blocks(const or_args *a, int *i_beg, int *n_max) {
 }
 
 /* get_soap, src/soap_turbo.f90:139-1037.
- *   soap:          (n_soap, n_sites), overwritten and normalised
- *   soap_cart_der: (3, n_soap, n_pairs) or NULL; overwritten (the reference
- *                  accumulates into the self columns, so its callers zero it)
+ *   soap:          (n_soap, n_sites), normalised.  As in the reference, a
+ *                  compressed soap is accumulated into (:798-802: the
+ *                  caller's values are added before the norm is taken), an
+ *                  uncompressed one is overwritten
+ *   soap_cart_der: (3, n_soap, n_pairs) or NULL; the neighbour columns are
+ *                  overwritten and the self columns accumulated into
+ *                  (:888-892), as in the reference
  *   ctx_out:       when non-NULL, receives the state soap_contract needs
  *                  (the reference's contract = .true.; :1008-1035)
  * Returns n_soap, or a negative code. */
@@ -1079,7 +1083,6 @@ int or_get_soap2(const or_args *a, int do_derivatives, int do_der2, double *soap
           }
       double *si = soap + (size_t)n_soap * i;
       if (a->compress) {
-        for (int s = 0; s < n_soap; s++) si[s] = 0.0;
         for (int t = 0; t < a->P_nonzero; t++)
           si[a->P_i[t] - 1] = si[a->P_i[t] - 1] + a->P_el[t] * this_soap[a->P_j[t] - 1];
       } else {
@@ -1116,8 +1119,6 @@ int or_get_soap2(const or_args *a, int do_derivatives, int do_der2, double *soap
         double inv_p = 1.0 / c->sqrt_dot_p[i];
         double inv_p3 = 1.0 / pow(c->sqrt_dot_p[i], 3);
         double *self = soap_cart_der + (size_t)k3 * n_soap * 3;
-        if (a->n_neigh[i] > 0)
-          for (int t = 0; t < 3 * n_soap; t++) self[t] = 0.0;
         for (int j = 1; j < a->n_neigh[i]; j++) {
           int k2 = c->k_first[i] + j;
           const double *A = c->ang + (size_t)2 * k_max * k2, *Ar = c->ang_r + (size_t)2 * k_max * k2;

@@ -110,6 +110,9 @@ SIGNATURES = {
                                         C.POINTER(Batch), C.POINTER(C.c_void_p)]),
     "soapb_kernel_timing": (C.c_int, [C.c_void_p, C.c_int32]),
     "soapb_kernel_times": (C.c_int, [C.c_void_p, i64p, f64p, i64p]),
+    "soapb_selftest_scan_wait": (C.c_int, [C.c_int32, C.c_int32, i64p]),
+    "soapb_set_radial_tables": (C.c_int, [C.c_void_p, C.c_int32]),
+    "soapb_radial_tables": (C.c_int, [C.c_void_p, i32p, f64p]),
 }
 KERNEL_KINDS = ("prep", "pair", "descriptor", "contract")
 

@@ -162,6 +162,17 @@ class Context:
     def set_threads_per_site(self, threads: int):
         _lib.check(self._lib.soapb_set_threads_per_site(self._h, int(threads)))
 
+    def set_radial_tables(self, enable: bool):
+        """soapb_set_radial_tables: the pair kernel's tabulated FP32 radial
+        expansion (True, when its check passed) or the FP64 expansion (False)."""
+        _lib.check(self._lib.soapb_set_radial_tables(self._h, int(bool(enable))))
+
+    def radial_tables(self):
+        """(in use, largest relative error of the tables; -1 when not tabulated)."""
+        use, err = C.c_int32(0), C.c_double(0.0)
+        _lib.check(self._lib.soapb_radial_tables(self._h, C.byref(use), C.byref(err)))
+        return bool(use.value), float(err.value)
+
     def basis(self):
         W = np.zeros((self.n_max, self.n_max), order="F")
         S = np.zeros((self.n_max, self.n_max), order="F")

@@ -222,9 +222,10 @@ __device__ __forceinline__ void radial_entry_op(const DevParams &P, const RadSp 
 }
 
 // OP: the poly3operator basis (a separate instantiation, so that the poly3 and
-// poly3gauss kernels are compiled without its code).
+// poly3gauss kernels are compiled without its code).  The poly3 / poly3gauss
+// form also runs on the host, which fits the pair kernel's radial tables to it.
 template <int AMAX, bool OP = false>
-__device__ __forceinline__ void radial_entry(const DevParams &P, const RadSp &S,
+__host__ __device__ __forceinline__ void radial_entry(const DevParams &P, const RadSp &S,
                                              const double *__restrict__ W, double r_in,
                                              bool is_central, bool do_der, double (&val)[AMAX],
                                              double (&der)[AMAX]) {
@@ -421,6 +422,63 @@ __device__ __forceinline__ void radial_entry(const DevParams &P, const RadSp &S,
   for (int i = 0; i < AMAX; ++i) {
     val[i] = amp * val[i] * S.sqrt_rcut;
     der[i] = der[i] * S.inv_sqrt_rcut;
+  }
+}
+
+// ---------------------------------------------------------------- radial tables
+// The branch state of a (pair, species) entry at distance r, by the same FP64
+// tests as radial_entry (sigma constant: atom_sigma_r_scaling = 0); -1 where
+// the amplitude is zero (h(r) <= 1e-10), which makes R_n and dR_n/dr zero.
+__host__ __device__ __forceinline__ int radial_branch(const DevParams &P, const RadSp &S, double r_in) {
+  const double rj = r_in * S.inv_rcut;
+  const double sig = S.atom_sigma + S.c * rj;
+  if (P.scaling_poly && S.amp_scaling != 0.0) {
+    const double h = 1.0 + 2.0 * (rj * rj * rj) - 3.0 * rj * rj;
+    if (h <= 1.0e-10) return -1;
+  }
+  const bool keep = S.has_filter != 0 && (S.rs - rj) < 4.0 * sig;
+  const bool gm = P.basis != 1 || rj < 4.0 * (S.atom_sigma + sig);
+  return (keep ? 1 : 0) | (gm ? 0 : 2);
+}
+
+// R_n (out[0..AMAX)) and, with do_der, dR_n/dr (out[AMAX..2 AMAX)) of one entry
+// from its species' table, 4 pi global_scaling included: the segment and its
+// local coordinate t in FP64, the polynomial by Horner in FP32.
+template <int AMAX>
+__device__ __forceinline__ void radial_from_table(const DevParams &P, const RadSp &S, const RadTab &T,
+                                                  double r, bool do_der, float (&out)[2 * AMAX]) {
+  const int st = radial_branch(P, S, r);
+  if (st < 0) {
+#pragma unroll
+    for (int f = 0; f < 2 * AMAX; ++f) out[f] = 0.f;
+    return;
+  }
+  const double u = (r - T.lo[st]) * T.inv_h[st];
+  int seg = (int)floor(u);
+  seg = seg < 0 ? 0 : (seg >= T.nseg[st] ? T.nseg[st] - 1 : seg);
+  const float t = (float)(2.0 * (u - (double)seg) - 1.0);
+  const float4 *c4 = (const float4 *)(P.rtab_coef + (size_t)(T.base[st] + seg) * (kRadTabDeg + 1) * 2 * AMAX);
+  constexpr int F4 = 2 * AMAX / 4;
+  const int nf4 = do_der ? F4 : F4 / 2;
+#pragma unroll
+  for (int j = 0; j < F4; ++j) {
+    if (j < nf4) {
+      float4 a = c4[kRadTabDeg * F4 + j];
+#pragma unroll
+      for (int k = kRadTabDeg - 1; k >= 0; --k) {
+        const float4 b = c4[k * F4 + j];
+        a.x = fmaf(a.x, t, b.x);
+        a.y = fmaf(a.y, t, b.y);
+        a.z = fmaf(a.z, t, b.z);
+        a.w = fmaf(a.w, t, b.w);
+      }
+      out[4 * j] = a.x;
+      out[4 * j + 1] = a.y;
+      out[4 * j + 2] = a.z;
+      out[4 * j + 3] = a.w;
+    } else {
+      out[4 * j] = out[4 * j + 1] = out[4 * j + 2] = out[4 * j + 3] = 0.f;
+    }
   }
 }
 

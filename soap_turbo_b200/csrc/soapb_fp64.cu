@@ -135,9 +135,11 @@ __global__ void k64_cnk(const DevParams P, const DevBatch B, const double *rad, 
   }
 }
 
-// ---- power spectrum + compression + norm, one CTA per site (:750-813)
-__global__ void k64_soap(const DevParams P, const DevBatch B, const double2 *cnk, double *soap_un,
-                         double *norm) {
+// ---- power spectrum + compression + norm, one CTA per site (:750-813).
+// soap_acc (may be null): the caller's soap, added before the norm is taken, as
+// the reference adds the compressed descriptor into soap (:798-802).
+__global__ void k64_soap(const DevParams P, const DevBatch B, const double2 *cnk, const double *soap_acc,
+                         double *soap_un, double *norm) {
   extern __shared__ double sp[];  // n_kept
   __shared__ double red[32];
   const int site = blockIdx.x;
@@ -159,8 +161,9 @@ __global__ void k64_soap(const DevParams P, const DevBatch B, const double2 *cnk
   __syncthreads();
   double part = 0.0;
   double *out = soap_un + (size_t)site * P.n_soap;
+  const double *in = soap_acc ? soap_acc + (size_t)site * P.n_soap : nullptr;
   for (int o = threadIdx.x; o < P.n_soap; o += blockDim.x) {
-    double v = 0.0;
+    double v = in ? in[o] : 0.0;
     for (int t = P.pi_off[o]; t < P.pi_off[o + 1]; ++t) v = v + P.pi_el64[t] * sp[P.pi_q[t]];
     out[o] = v;
     part += v * v;
@@ -177,125 +180,216 @@ __global__ void k64_soap(const DevParams P, const DevBatch B, const double2 *cnk
   }
 }
 
-// ---- spherical derivatives + rotation into soap_cart_der, one CTA per pair
-// (src/soap_turbo.f90:837-895, 1999-2066)
-__global__ void k64_cart(const DevParams P, const DevBatch B, const double *rad,
-                         const double *rad_der, const double2 *ang, const double2 *cnk,
-                         const double *soap_un, const double *norm, double *cart) {
-  extern __shared__ double sm[];
-  const int k = blockIdx.x;
-  int lo = 0, hi = B.n_sites;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (B.off[mid] <= k) lo = mid; else hi = mid;
-  }
-  const int site = lo;
-  if (B.off[site] == k) return;  // self column: built by k64_self
-  const int N = P.n_max, K = P.k_max, L1 = P.l_max + 1, ns = P.n_soap;
-  const size_t plane = (size_t)B.n_pairs * K;
-  double *sPQ = sm;                     // 4 * N * L1
-  double *sd = sPQ + 4 * N * L1;        // n_kept * 3
-  double *sdc = sd + 3 * P.n_kept;      // n_soap * 3
-  __shared__ double red[3][32];
-  const double2 *c = cnk + (size_t)site * N * K;
-  const double2 *A = ang + (size_t)k * K;
-  for (int it = threadIdx.x; it < N * L1; it += blockDim.x) {
-    const int n = it / L1, l = it - n * L1;
-    double ap = 0, aq = 0, aa = 0, ao = 0;
-    for (int m = 0; m <= l; ++m) {
-      const int kk = l * (l + 1) / 2 + m;
-      const double w = (m == 0) ? 1.0 : 2.0;
-      const double2 cc = c[(size_t)n * K + kk];
-      const double2 a0 = A[kk], a1 = A[plane + kk], a2 = A[2 * plane + kk], a3 = A[3 * plane + kk];
-      ap = ap + w * (a0.x * cc.x + a0.y * cc.y);
-      aq = aq + w * (a1.x * cc.x + a1.y * cc.y);
-      aa = aa + w * (a2.x * cc.x + a2.y * cc.y);
-      ao = ao + w * (a3.x * cc.x + a3.y * cc.y);
-    }
-    sPQ[it] = ap;
-    sPQ[N * L1 + it] = aq;
-    sPQ[2 * N * L1 + it] = aa;
-    sPQ[3 * N * L1 + it] = ao;
-  }
-  __syncthreads();
-  const double *R = rad + (size_t)k * N, *Rd = rad_der + (size_t)k * N;
-  for (int q = threadIdx.x; q < P.n_kept; q += blockDim.x) {
-    const int code = P.kept_nnl[q];
-    const int n = code & 0xff, np = (code >> 8) & 0xff, l = code >> 16;
-    const double pre = kFourPi64 * ((n == np) ? 1.0 : sqrt(2.0));
-    const double rn = R[n], rdn = Rd[n], rnp = R[np], rdnp = Rd[np];
-    const double *Pp = sPQ, *Q = sPQ + N * L1, *Qa = sPQ + 2 * N * L1, *Qo = sPQ + 3 * N * L1;
-    sd[3 * q + 0] = pre * (rdn * Pp[np * L1 + l] + rn * Q[np * L1 + l] + rdnp * Pp[n * L1 + l] + rnp * Q[n * L1 + l]);
-    sd[3 * q + 1] = pre * (rn * Qa[np * L1 + l] + rnp * Qa[n * L1 + l]);
-    sd[3 * q + 2] = pre * (rn * Qo[np * L1 + l] + rnp * Qo[n * L1 + l]);
-  }
-  __syncthreads();
-  const double *sv = soap_un + (size_t)site * ns;
-  double dr = 0, da = 0, dp = 0;
-  for (int o = threadIdx.x; o < ns; o += blockDim.x) {
-    double vr = 0, va = 0, vp = 0;
-    for (int t = P.pi_off[o]; t < P.pi_off[o + 1]; ++t) {
-      const double el = P.pi_el64[t];
-      const int q = P.pi_q[t];
-      vr = vr + el * sd[3 * q];
-      va = va + el * sd[3 * q + 1];
-      vp = vp + el * sd[3 * q + 2];
-    }
-    sdc[3 * o] = vr;
-    sdc[3 * o + 1] = va;
-    sdc[3 * o + 2] = vp;
-    dr += sv[o] * vr;
-    da += sv[o] * va;
-    dp += sv[o] * vp;
-  }
+// Fixed-order sum of three values over the CTA (warp shuffles, then warp 0).
+template <int NT>
+__device__ __forceinline__ void cta_sum3(double &a, double &b, double &c, double (*red)[NT / 32]) {
   for (int o = 16; o > 0; o >>= 1) {
-    dr += __shfl_xor_sync(0xffffffffu, dr, o);
-    da += __shfl_xor_sync(0xffffffffu, da, o);
-    dp += __shfl_xor_sync(0xffffffffu, dp, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    red[0][threadIdx.x >> 5] = dr;
-    red[1][threadIdx.x >> 5] = da;
-    red[2][threadIdx.x >> 5] = dp;
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
   }
   __syncthreads();
-  double dot_r = 0, dot_a = 0, dot_o = 0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-    dot_r += red[0][w];
-    dot_a += red[1][w];
-    dot_o += red[2][w];
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = a;
+    red[1][threadIdx.x >> 5] = b;
+    red[2][threadIdx.x >> 5] = c;
   }
-  const double nr = norm[site];
-  const double inv_p = 1.0 / nr, inv_p3 = 1.0 / (nr * nr * nr);
-  double st, ct, sf, cf;
-  sincos(B.thetas[k], &st, &ct);
-  sincos(B.phis[k], &sf, &cf);
-  const double ir = 1.0 / B.rjs[k];
-  const double cx = st * cf, cy = st * sf, cz = ct;
-  const double px = -ct * cf * ir, py = -ct * sf * ir, pz = st * ir;
-  const double ax = -sf * ir, ay = cf * ir;
-  double *out = cart + (size_t)k * ns * 3;
-  for (int o = threadIdx.x; o < ns; o += blockDim.x) {
-    const double s = sv[o];
-    const double vr = sdc[3 * o] * inv_p - s * inv_p3 * dot_r;
-    const double va = sdc[3 * o + 1] * inv_p - s * inv_p3 * dot_a;
-    const double vo = sdc[3 * o + 2] * inv_p - s * inv_p3 * dot_o;
-    out[3 * o + 0] = cx * vr + px * vo + ax * va;
-    out[3 * o + 1] = cy * vr + py * vo + ay * va;
-    out[3 * o + 2] = cz * vr + pz * vo;
+  __syncthreads();
+  a = b = c = 0.0;
+  for (int w = 0; w < NT / 32; ++w) {
+    a += red[0][w];
+    b += red[1][w];
+    c += red[2][w];
   }
 }
 
-// ---- self column = minus the sum of the site's other columns (:888-892)
-__global__ void k64_self(const DevParams P, const DevBatch B, double *cart) {
+// Shared memory of k64_cart_site, in doubles.  STAGED: the site's c_nlm, soap
+// row and self column are in shared memory too (else they are read and summed
+// in global memory, for definitions whose rows do not fit).
+struct CartSmem {
+  int C, A, PQ, sd, sv, dc, self, total;
+};
+__host__ __device__ inline CartSmem cart_smem(const DevParams &P, bool staged) {
+  CartSmem L;
+  const int N = P.n_max, K = P.k_max, L1 = P.l_max + 1;
+  int o = 0;
+  L.A = o;    o += 8 * K;                // the pair's four angular planes
+  L.PQ = o;   o += 4 * N * L1;           // P, Q, Qa, Qo (n, l)
+  L.sd = o;   o += 3 * P.n_kept;         // kept components' spherical derivatives
+  L.dc = o;   o += 3 * P.n_soap;         // compressed derivatives, then the Cartesian column
+  L.C = L.sv = L.self = -1;
+  if (staged) {
+    L.C = o;    o += 2 * N * K;          // the site's c_nlm
+    L.sv = o;   o += P.n_soap;           // the site's unnormalised soap row
+    L.self = o; o += 3 * P.n_soap;       // the self column, summed over the pairs
+  }
+  L.total = o;
+  return L;
+}
+
+// ---- spherical derivatives, normalisation derivative and Cartesian rotation
+// into soap_cart_der (src/soap_turbo.f90:837-895, 1927-2075): one CTA per site,
+// which walks the site's pairs in CSR order with the site's c_nlm and soap row
+// in shared memory, writes each neighbour column with coalesced stores, and
+// sums the self column (minus every other column, :888-892) in shared memory,
+// written once at the end.  self_init (may be null): the caller's self
+// columns on entry, which the reference's subtraction accumulates into.
+template <int NT, bool STAGED>
+__global__ void __launch_bounds__(NT) k64_cart_site(const DevParams P, const DevBatch B, const double *rad,
+                                                    const double *rad_der, const double2 *ang,
+                                                    const double2 *cnk, const double *soap_un,
+                                                    const double *norm, const double *self_init,
+                                                    double *cart) {
+  extern __shared__ double sm[];
+  __shared__ double red[3][NT / 32];
   const int site = blockIdx.x;
   const int p0 = B.off[site], p1 = min(B.off[site + 1], B.n_pairs);
   if (p1 <= p0) return;
-  const int w = 3 * P.n_soap;
-  for (int t = threadIdx.x; t < w; t += blockDim.x) {
-    double acc = 0.0;
-    for (int k = p0 + 1; k < p1; ++k) acc = acc - cart[(size_t)k * w + t];
-    cart[(size_t)p0 * w + t] = acc;
+  const int N = P.n_max, K = P.k_max, L1 = P.l_max + 1, ns = P.n_soap, w3 = 3 * ns;
+  const size_t plane = (size_t)B.n_pairs * K;
+  const CartSmem Ly = cart_smem(P, STAGED);
+  const double2 *c = cnk + (size_t)site * N * K;
+  const double *sv_g = soap_un + (size_t)site * ns;
+  // without staging, the self column is summed in place in global memory (each
+  // element always by the same thread)
+  double *sSelf = STAGED ? sm + Ly.self : cart + (size_t)p0 * w3;
+  const double2 *sC = STAGED ? (const double2 *)(sm + Ly.C) : c;
+  const double *sv = STAGED ? sm + Ly.sv : sv_g;
+  double2 *sA = (double2 *)(sm + Ly.A);
+  double *sPQ = sm + Ly.PQ, *sd = sm + Ly.sd, *sdc = sm + Ly.dc;
+  if (STAGED) {
+    for (int t = threadIdx.x; t < N * K; t += NT) ((double2 *)(sm + Ly.C))[t] = c[t];
+    for (int o = threadIdx.x; o < ns; o += NT) (sm + Ly.sv)[o] = sv_g[o];
+  }
+  const double *si = self_init ? self_init + (size_t)site * w3 : nullptr;
+  for (int t = threadIdx.x; t < w3; t += NT) sSelf[t] = si ? si[t] : 0.0;
+  const double nr = norm[site];
+  const double inv_p = 1.0 / nr, inv_p3 = 1.0 / (nr * nr * nr);
+  const double *Pp = sPQ, *Q = sPQ + N * L1, *Qa = sPQ + 2 * N * L1, *Qo = sPQ + 3 * N * L1;
+
+  for (int k = p0 + 1; k < p1; ++k) {
+    __syncthreads();  // the previous pair's readers of sA, sPQ, sd and sdc are done
+    for (int t = threadIdx.x; t < 4 * K; t += NT) {
+      const int pl = t / K, kk = t - pl * K;
+      sA[t] = ang[pl * plane + (size_t)k * K + kk];
+    }
+    __syncthreads();
+    // P, Q, Qa, Qo(n, l) = sum_m w_m Re(X_lm conj c_nlm) for X = A, dA/dr, dA/dphi, dA/dtheta
+    for (int it = threadIdx.x; it < N * L1; it += NT) {
+      const int n = it / L1, l = it - n * L1;
+      double ap = 0, aq = 0, aa = 0, ao = 0;
+      for (int m = 0; m <= l; ++m) {
+        const int kk = l * (l + 1) / 2 + m;
+        const double w = (m == 0) ? 1.0 : 2.0;
+        const double2 cc = sC[n * K + kk];
+        const double2 a0 = sA[kk], a1 = sA[K + kk], a2 = sA[2 * K + kk], a3 = sA[3 * K + kk];
+        ap = ap + w * (a0.x * cc.x + a0.y * cc.y);
+        aq = aq + w * (a1.x * cc.x + a1.y * cc.y);
+        aa = aa + w * (a2.x * cc.x + a2.y * cc.y);
+        ao = ao + w * (a3.x * cc.x + a3.y * cc.y);
+      }
+      sPQ[it] = ap;
+      sPQ[N * L1 + it] = aq;
+      sPQ[2 * N * L1 + it] = aa;
+      sPQ[3 * N * L1 + it] = ao;
+    }
+    __syncthreads();
+    const double *R = rad + (size_t)k * N, *Rd = rad_der + (size_t)k * N;
+    for (int q = threadIdx.x; q < P.n_kept; q += NT) {
+      const int code = P.kept_nnl[q];
+      const int n = code & 0xff, np = (code >> 8) & 0xff, l = code >> 16;
+      const double pre = kFourPi64 * ((n == np) ? 1.0 : sqrt(2.0));
+      const double rn = R[n], rdn = Rd[n], rnp = R[np], rdnp = Rd[np];
+      sd[3 * q + 0] = pre * (rdn * Pp[np * L1 + l] + rn * Q[np * L1 + l] + rdnp * Pp[n * L1 + l] + rnp * Q[n * L1 + l]);
+      sd[3 * q + 1] = pre * (rn * Qa[np * L1 + l] + rnp * Qa[n * L1 + l]);
+      sd[3 * q + 2] = pre * (rn * Qo[np * L1 + l] + rnp * Qo[n * L1 + l]);
+    }
+    __syncthreads();
+    double dr = 0, da = 0, dp = 0;
+    for (int o = threadIdx.x; o < ns; o += NT) {
+      double vr = 0, va = 0, vp = 0;
+      for (int t = P.pi_off[o]; t < P.pi_off[o + 1]; ++t) {
+        const double el = P.pi_el64[t];
+        const int q = P.pi_q[t];
+        vr = vr + el * sd[3 * q];
+        va = va + el * sd[3 * q + 1];
+        vp = vp + el * sd[3 * q + 2];
+      }
+      sdc[3 * o] = vr;
+      sdc[3 * o + 1] = va;
+      sdc[3 * o + 2] = vp;
+      dr += sv[o] * vr;
+      da += sv[o] * va;
+      dp += sv[o] * vp;
+    }
+    cta_sum3<NT>(dr, da, dp, red);
+    double st, ct, sf, cf;
+    sincos(B.thetas[k], &st, &ct);
+    sincos(B.phis[k], &sf, &cf);
+    const double ir = 1.0 / B.rjs[k];
+    const double cx = st * cf, cy = st * sf, cz = ct;
+    const double px = -ct * cf * ir, py = -ct * sf * ir, pz = st * ir;
+    const double ax = -sf * ir, ay = cf * ir;
+    // each thread turns its own components o into the Cartesian column in place
+    for (int o = threadIdx.x; o < ns; o += NT) {
+      const double s = sv[o];
+      const double vr = sdc[3 * o] * inv_p - s * inv_p3 * dr;
+      const double va = sdc[3 * o + 1] * inv_p - s * inv_p3 * da;
+      const double vo = sdc[3 * o + 2] * inv_p - s * inv_p3 * dp;
+      sdc[3 * o + 0] = cx * vr + px * vo + ax * va;
+      sdc[3 * o + 1] = cy * vr + py * vo + ay * va;
+      sdc[3 * o + 2] = cz * vr + pz * vo;
+    }
+    __syncthreads();
+    double *out = cart + (size_t)k * w3;
+    for (int t = threadIdx.x; t < w3; t += NT) {
+      const double v = sdc[t];
+      out[t] = v;
+      sSelf[t] = sSelf[t] - v;
+    }
+  }
+  if (STAGED) {
+    __syncthreads();
+    double *out = cart + (size_t)p0 * w3;
+    for (int t = threadIdx.x; t < w3; t += NT) out[t] = sSelf[t];
+  }
+}
+
+// ---- pair = sgn * sum_s G(i,s) soap_cart_der(:, s, k): one CTA per site with
+// the site's G row in shared memory, one warp per pair; lane j takes the
+// components o = j, j + 32, ... (a warp's three loads of a step cover 768
+// contiguous bytes of the column).
+template <int NT>
+__global__ void __launch_bounds__(NT) k64_contract_site(const DevParams P, const DevBatch B, const double *cart,
+                                                        const double *G, int g_layout, double sgn,
+                                                        double *pair) {
+  extern __shared__ double sG[];  // n_soap
+  const int site = blockIdx.x;
+  const int p0 = B.off[site], p1 = min(B.off[site + 1], B.n_pairs);
+  const int ns = P.n_soap;
+  for (int o = threadIdx.x; o < ns; o += NT)
+    sG[o] = g_layout == 0 ? G[(size_t)o * B.n_sites + site] : G[(size_t)site * ns + o];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = p0 + warp; k < p1; k += NT / 32) {
+    const double *ck = cart + (size_t)k * 3 * ns;
+    double x = 0.0, y = 0.0, z = 0.0;
+    for (int o = lane; o < ns; o += 32) {
+      const double g = sG[o];
+      x += g * ck[3 * o];
+      y += g * ck[3 * o + 1];
+      z += g * ck[3 * o + 2];
+    }
+    for (int s = 16; s > 0; s >>= 1) {
+      x += __shfl_xor_sync(0xffffffffu, x, s);
+      y += __shfl_xor_sync(0xffffffffu, y, s);
+      z += __shfl_xor_sync(0xffffffffu, z, s);
+    }
+    if (lane == 0) {
+      pair[3 * (size_t)k] = sgn * x;
+      pair[3 * (size_t)k + 1] = sgn * y;
+      pair[3 * (size_t)k + 2] = sgn * z;
+    }
   }
 }
 
@@ -307,48 +401,24 @@ __global__ void k64_normalise(const DevParams P, const DevBatch B, const double 
   soap[t] = soap_un[t] / norm[t / P.n_soap];
 }
 
-// ---- pair = sgn * sum_s G(i,s) soap_cart_der(:, s, k), one warp per pair
-__global__ void k64_contract_cart(const DevParams P, const DevBatch B, const double *cart,
-                                  const double *G, int g_layout, double sgn, double *pair) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= B.n_pairs) return;
-  const int k = warp;
-  int lo = 0, hi = B.n_sites;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (B.off[mid] <= k) lo = mid; else hi = mid;
-  }
-  const int site = lo, ns = P.n_soap;
-  const double *ck = cart + (size_t)k * ns * 3;
-  double x = 0, y = 0, z = 0;
-  for (int o = lane; o < ns; o += 32) {
-    const double g = g_layout == 0 ? G[(size_t)o * B.n_sites + site] : G[(size_t)site * ns + o];
-    x += g * ck[3 * o];
-    y += g * ck[3 * o + 1];
-    z += g * ck[3 * o + 2];
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    x += __shfl_xor_sync(0xffffffffu, x, o);
-    y += __shfl_xor_sync(0xffffffffu, y, o);
-    z += __shfl_xor_sync(0xffffffffu, z, o);
-  }
-  if (lane == 0) {
-    pair[3 * (size_t)k] = sgn * x;
-    pair[3 * (size_t)k + 1] = sgn * y;
-    pair[3 * (size_t)k + 2] = sgn * z;
-  }
-}
-
 static int max_alpha64(const DevParams &P) {
   int a = 0;
   for (int s = 0; s < P.n_species; ++s) a = a > P.rad[s].alpha ? a : P.rad[s].alpha;
   return a;
 }
 
+constexpr int kCartThreads = 256;
+
+// The staged layout when it fits in a CTA's shared memory (227 KB on B200).
+constexpr size_t kCartSmemCap = 227 * 1024;
+size_t fp64_cart_smem(const DevParams &P) {
+  const size_t staged = (size_t)cart_smem(P, true).total * sizeof(double);
+  return staged <= kCartSmemCap ? staged : (size_t)cart_smem(P, false).total * sizeof(double);
+}
+
 cudaError_t launch_fp64_descriptor(const DevParams &P, const DevBatch &B, cudaStream_t s,
                                    const Fp64Work &w, int do_der, double *soap, double *cart,
-                                   int *launches) {
+                                   int *launches, const double *soap_acc, const double *self_init) {
   const int np = B.n_pairs, nsites = B.n_sites;
   int nl = 0;
   if (np > 0) {
@@ -369,18 +439,18 @@ cudaError_t launch_fp64_descriptor(const DevParams &P, const DevBatch &B, cudaSt
     k64_cnk<<<nsites, 256, 0, s>>>(P, B, w.rad, (const double2 *)w.ang, (double2 *)w.cnk);
     const size_t sm = (size_t)P.n_kept * sizeof(double);
     cudaFuncSetAttribute(k64_soap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k64_soap<<<nsites, 256, sm, s>>>(P, B, (const double2 *)w.cnk, w.soap_unnorm, w.norm);
+    k64_soap<<<nsites, 256, sm, s>>>(P, B, (const double2 *)w.cnk, soap_acc, w.soap_unnorm, w.norm);
     nl += 2;
   }
-  if (do_der && cart && np > 0) {
-    const size_t sm = ((size_t)4 * P.n_max * (P.l_max + 1) + 3 * (size_t)P.n_kept + 3 * (size_t)P.n_soap) *
-                      sizeof(double);
-    cudaError_t e = cudaFuncSetAttribute(k64_cart, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (do_der && cart && np > 0 && nsites > 0) {
+    const size_t sm = fp64_cart_smem(P);
+    const bool staged = sm == (size_t)cart_smem(P, true).total * sizeof(double);
+    auto kern = staged ? k64_cart_site<kCartThreads, true> : k64_cart_site<kCartThreads, false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k64_cart<<<np, 128, sm, s>>>(P, B, w.rad, w.rad_der, (const double2 *)w.ang,
-                                 (const double2 *)w.cnk, w.soap_unnorm, w.norm, cart);
-    k64_self<<<nsites, 256, 0, s>>>(P, B, cart);
-    nl += 2;
+    kern<<<nsites, kCartThreads, sm, s>>>(P, B, w.rad, w.rad_der, (const double2 *)w.ang,
+                                          (const double2 *)w.cnk, w.soap_unnorm, w.norm, self_init, cart);
+    nl += 1;
   }
   if (nsites > 0) {
     const size_t n = (size_t)nsites * P.n_soap;
@@ -394,10 +464,12 @@ cudaError_t launch_fp64_descriptor(const DevParams &P, const DevBatch &B, cudaSt
 cudaError_t launch_fp64_contract(const DevParams &P, const DevBatch &B, cudaStream_t s,
                                  const double *cart, const double *G, int g_layout, double sgn,
                                  double *pair, int *launches) {
-  if (B.n_pairs <= 0) return cudaSuccess;
-  const size_t threads = (size_t)B.n_pairs * 32;
-  k64_contract_cart<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(P, B, cart, G, g_layout, sgn,
-                                                                      pair);
+  if (B.n_pairs <= 0 || B.n_sites <= 0) return cudaSuccess;
+  const size_t sm = (size_t)P.n_soap * sizeof(double);
+  auto kern = k64_contract_site<256>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  kern<<<B.n_sites, 256, sm, s>>>(P, B, cart, G, g_layout, sgn, pair);
   if (launches) *launches += 1;
   return cudaGetLastError();
 }

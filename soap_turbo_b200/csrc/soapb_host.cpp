@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/soap_b200.h"
+#include "soapb_device.cuh"
 #include "soapb_internal.h"
 
 using namespace soapb;
@@ -283,6 +284,13 @@ struct soapb_context {
   int tune_td = 0, tune_cd = 0, tune_tc = 0, tune_cc = 0;
   int64_t launches = 0;
   int keep_valid = 0, keep_sites = 0, keep_pairs = 0;
+  // the error word of the last call that checked inputs: the context's own
+  // (err), or the static scratch array's after soapb_descriptor_noalloc
+  unsigned long long *last_err = nullptr;
+  // the pair kernel's radial tables: fitted and within tolerance (rtab_ok),
+  // their largest relative error, and whether the caller allows them
+  int rtab_ok = 0, rtab_enable = 1;
+  double rtab_err = 0.0;
   // device timing of the kernels (soapb_kernel_timing): an event pair around
   // each timed launch, tkind[i] the kernel of pair i, tn pairs recorded so far
   std::vector<cudaEvent_t> tev;
@@ -338,6 +346,136 @@ int species_basis(int basis, int alpha, double sig, double rcut, double *S, doub
 
 int u_index(int n, int np, int l, int N, int L) {  // uncompressed component, 0-based, n <= np
   return (n * N - n * (n - 1) / 2 + (np - n)) * (L + 1) + l;
+}
+
+// ---------------------------------------------------------------- radial tables
+// The pair kernel's FP32 radial expansion for atom_sigma_r_scaling = 0: per
+// species, each branch interval of r (see RadTab) is cut into segments of at
+// most 0.05 rcut_hard, and on each segment every R_n and dR_n/dr (4 pi
+// global_scaling folded in) is interpolated at the kRadTabDeg + 1 Chebyshev
+// nodes from the FP64 expansion itself (radial_entry, run here on the host) and
+// stored as monomials in t in [-1, 1].  The tables are then checked against
+// the FP64 expansion at 16 points inside every segment, evaluated in FP32 as
+// the kernel does; the largest error relative to each function's largest
+// value decides whether the kernel uses them (max_err <= kRadTabTol).
+constexpr double kRadTabTol = 5.0e-7;
+constexpr double kRadTabWidth = 0.05;  // segment width, in units of rcut_hard
+
+template <int AMAX>
+void radial_fp64(const DevParams &P, const RadSp &S, const double *W, double r, double *f) {
+  double val[AMAX], der[AMAX];
+  radial_entry<AMAX, false>(P, S, W, r, false, true, val, der);
+  const double g4 = 4.0 * std::acos(-1.0) * S.gscale;
+  for (int n = 0; n < AMAX; ++n) {
+    f[n] = n < S.alpha ? g4 * val[n] : 0.0;
+    f[AMAX + n] = n < S.alpha ? g4 * der[n] : 0.0;
+  }
+}
+
+template <int AMAX>
+int fit_radial_tables(const soapb_context *c, const DevParams &P, std::vector<float> &coef, RadTab *tabs,
+                      double *max_err) {
+  constexpr int D = kRadTabDeg, NF = 2 * AMAX, SEG = (D + 1) * NF;
+  const double pi = std::acos(-1.0);
+  *max_err = 0.0;
+  coef.clear();
+  if (c->basis != SOAPB_BASIS_POLY3 && c->basis != SOAPB_BASIS_POLY3GAUSS) return 0;
+  for (int s = 0; s < c->n_species; ++s)
+    if (c->sig_r_c[s] != 0.0 || c->alpha[s] > AMAX) return 0;
+  // T_k(x) as monomials: tk[k][j]
+  double tk[D + 1][D + 1] = {};
+  tk[0][0] = 1.0;
+  if (D >= 1) tk[1][1] = 1.0;
+  for (int k = 2; k <= D; ++k)
+    for (int j = 0; j <= k; ++j) tk[k][j] = (j > 0 ? 2.0 * tk[k - 1][j - 1] : 0.0) - tk[k - 2][j];
+  int nseg_total = 0;
+  for (int s = 0; s < c->n_species; ++s) {
+    const RadSp &S = P.rad[s];
+    const int a = c->alpha[s], b = S.nbeg, N = c->n_max;
+    std::vector<double> W((size_t)a * a);
+    for (int j = 0; j < a; ++j)
+      for (int i = 0; i < a; ++i) W[(size_t)j * a + i] = c->W[(size_t)(b + j) * N + (b + i)];
+    const double rc = c->rcut_hard[s];
+    // branch points in r: the filter switch, the Gaussian-moment cut, the amplitude's zero
+    std::vector<double> bp = {0.0};
+    double end = rc;
+    if (P.scaling_poly && S.amp_scaling != 0.0 && radial_branch(P, S, rc * (1.0 - 1e-15)) < 0) {
+      double lo = 0.5 * rc, hi = rc;  // the first r with h(r) <= 1e-10
+      for (int it = 0; it < 200; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        (radial_branch(P, S, mid) < 0 ? hi : lo) = mid;
+      }
+      end = hi;
+    }
+    if (S.has_filter) bp.push_back((S.rs - 4.0 * S.atom_sigma) * rc);
+    if (P.basis == 1) bp.push_back(8.0 * S.atom_sigma * rc);
+    bp.push_back(end);
+    std::sort(bp.begin(), bp.end());
+    RadTab T{};
+    bool seen[4] = {false, false, false, false};
+    std::vector<double> fmax(NF, 0.0), emax(NF, 0.0);
+    for (size_t i = 0; i + 1 < bp.size(); ++i) {
+      const double lo = std::max(bp[i], 0.0), hi = std::min(bp[i + 1], end);
+      if (!(hi > lo)) continue;
+      const int st = radial_branch(P, S, 0.5 * (lo + hi));
+      if (st < 0) continue;
+      if (seen[st]) return 0;  // a branch state in two intervals: not tabulated
+      seen[st] = true;
+      const int ns = std::max(1, (int)std::ceil((hi - lo) / (kRadTabWidth * rc) - 1e-9));
+      const double h = (hi - lo) / ns;
+      T.lo[st] = lo;
+      T.inv_h[st] = 1.0 / h;
+      T.base[st] = nseg_total;
+      T.nseg[st] = ns;
+      for (int g = 0; g < ns; ++g) {
+        const double mid = lo + (g + 0.5) * h, half = 0.5 * h;
+        double fv[D + 1][NF];
+        for (int j = 0; j <= D; ++j) {
+          const double x = std::cos(pi * (j + 0.5) / (D + 1));
+          radial_fp64<AMAX>(P, S, W.data(), mid + half * x, fv[j]);
+        }
+        std::vector<double> mono((size_t)(D + 1) * NF, 0.0);
+        for (int f = 0; f < NF; ++f)
+          for (int k = 0; k <= D; ++k) {
+            double ck = 0.0;
+            for (int j = 0; j <= D; ++j) ck += fv[j][f] * std::cos(pi * k * (j + 0.5) / (D + 1));
+            ck *= (k == 0 ? 1.0 : 2.0) / (D + 1);
+            for (int q = 0; q <= k; ++q) mono[(size_t)q * NF + f] += ck * tk[k][q];
+          }
+        const size_t o = coef.size();
+        coef.resize(o + SEG);
+        for (int q = 0; q < SEG; ++q) coef[o + q] = (float)mono[q];
+        // the check: 16 points inside the segment, FP32 Horner as on the device
+        for (int j = 0; j < 16; ++j) {
+          const double t = -0.995 + 1.99 * j / 15.0;
+          double ref[NF];
+          radial_fp64<AMAX>(P, S, W.data(), mid + half * t, ref);
+          const float tf = (float)t;
+          for (int f = 0; f < NF; ++f) {
+            float acc = coef[o + (size_t)D * NF + f];
+            for (int k = D - 1; k >= 0; --k) acc = std::fma(acc, tf, coef[o + (size_t)k * NF + f]);
+            fmax[f] = std::max(fmax[f], std::fabs(ref[f]));
+            emax[f] = std::max(emax[f], std::fabs((double)acc - ref[f]));
+          }
+        }
+        ++nseg_total;
+      }
+    }
+    for (int f = 0; f < NF; ++f)
+      if (fmax[f] > 0.0) *max_err = std::max(*max_err, emax[f] / fmax[f]);
+    // a state no interval has is never reached; it still names a segment that
+    // exists, so that no read could leave the table
+    if (nseg_total == 0) return 0;
+    for (int st = 0; st < 4; ++st)
+      if (!seen[st]) {
+        T.lo[st] = 0.0;
+        T.inv_h[st] = 0.0;
+        T.base[st] = nseg_total - 1;
+        T.nseg[st] = 1;
+      }
+    tabs[s] = T;
+  }
+  return *max_err <= kRadTabTol ? 1 : 0;
 }
 
 // Builds DevParams and the device tables from the context's definition.
@@ -705,6 +843,11 @@ int build_tables(soapb_context *c) {
     P.cmap_identity = ident ? 1 : 0;
   }
   P.amax_t = amax_t;
+  std::vector<float> rtab;
+  c->rtab_ok = amax_t == 8 ? fit_radial_tables<8>(c, P, rtab, P.rtab_sp, &c->rtab_err)
+                           : fit_radial_tables<16>(c, P, rtab, P.rtab_sp, &c->rtab_err);
+  P.rtab = c->rtab_ok && c->rtab_enable;
+  const size_t iRt = add(rtab.data(), rtab.size() * 4);
   P.blob_bytes = (int)blob.size();
   P.blob_c_bytes = (int)blob_c.size();
   const size_t iBlob = add(blob.data(), blob.size());
@@ -737,6 +880,7 @@ int build_tables(soapb_context *c) {
   P.blob = (const unsigned char *)at(iBlob);
   P.blob_c = (const unsigned char *)at(iBlobC);
   P.hl_packed = (const int *)at(iHp);
+  P.rtab_coef = (const float *)at(iRt);
   P.n_soap = c->n_soap;
   P.n_kept = c->n_kept;
   return SOAPB_OK;
@@ -849,6 +993,7 @@ int ensure_batch(soapb_context *c, const soapb_batch *b, DevBatch &B) {
   B.ticket = (int *)(B.err + prep_err_words(b->n_sites) - 1);
   B.site_lo = 0;
   B.site_hi = b->n_sites;
+  c->last_err = B.err;
   return SOAPB_OK;
 }
 
@@ -932,8 +1077,11 @@ struct SiteChunks {
   std::function<int(int)> before, after;
 };
 
+// accumulate: d_soap holds the caller's soap on entry and the descriptor is
+// added into it before the norm is taken (the reference's compressed get_soap,
+// src/soap_turbo.f90:798-802); else d_soap is overwritten.
 int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int keep,
-                   const SiteChunks *ch = nullptr) {
+                   const SiteChunks *ch = nullptr, bool accumulate = false) {
   DevBatch B{};
   int rc = ensure_batch(c, b, B);
   if (rc) return rc;
@@ -970,7 +1118,7 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
     {
       TimedLaunch tl(c, SOAPB_KERNEL_DESCRIPTOR);
       CU(launch_descriptor(P, B, cfg, d_soap, keep ? c->keep_c.as<float>() : nullptr,
-                           keep ? c->keep_norm.as<double>() : nullptr, keep));
+                           keep ? c->keep_norm.as<double>() : nullptr, (keep ? 1 : 0) | (accumulate ? 2 : 0)));
     }
     c->launches += 1;
     if (ch && ch->after && (rc = ch->after(i))) return rc;
@@ -1011,7 +1159,10 @@ int ctx_contract(soapb_context *c, const soapb_batch *b, const double *d_soap, c
   return SOAPB_OK;
 }
 
-int ctx_fp64(soapb_context *c, const soapb_batch *b, double *d_soap, double *d_cart) {
+// accumulate: as for ctx_descriptor; d_self_init (may be null, with d_cart):
+// the caller's self columns of soap_cart_der, (3, n_soap) per site.
+int ctx_fp64(soapb_context *c, const soapb_batch *b, double *d_soap, double *d_cart, bool accumulate = false,
+             const double *d_self_init = nullptr) {
   DevBatch B{};
   int rc = ensure_batch(c, b, B);
   if (rc) return rc;
@@ -1030,7 +1181,8 @@ int ctx_fp64(soapb_context *c, const soapb_batch *b, double *d_soap, double *d_c
   Fp64Work w{c->f64_rad.as<double>(), c->f64_rad_der.as<double>(), c->f64_ang.as<double>(),
              c->f64_cnk.as<double>(), c->f64_soap_un.as<double>(), c->f64_norm.as<double>()};
   int nl = 0;
-  CU(launch_fp64_descriptor(P, B, c->stream, w, do_der, d_soap, d_cart, &nl));
+  CU(launch_fp64_descriptor(P, B, c->stream, w, do_der, d_soap, d_cart, &nl, accumulate ? d_soap : nullptr,
+                            d_self_init));
   c->launches += nl;
   return SOAPB_OK;
 }
@@ -1210,6 +1362,21 @@ int soapb_set_threads_per_site(soapb_context *c, int32_t threads) {
   return SOAPB_OK;
 }
 
+int soapb_set_radial_tables(soapb_context *c, int32_t enable) {
+  if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
+  c->rtab_enable = enable ? 1 : 0;
+  c->P.rtab = c->rtab_ok && c->rtab_enable;
+  c->keep_valid = 0;  // the kept pair rows came from the other form
+  return SOAPB_OK;
+}
+
+int soapb_radial_tables(const soapb_context *c, int32_t *in_use, double *max_err) {
+  if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
+  if (in_use) *in_use = c->P.rtab;
+  if (max_err) *max_err = c->rtab_ok ? c->rtab_err : -1.0;
+  return SOAPB_OK;
+}
+
 int soapb_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int32_t keep) {
   if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
   return ctx_descriptor(c, b, d_soap, keep);
@@ -1286,16 +1453,22 @@ int soapb_descriptor_noalloc(soapb_context *c, const soapb_batch *b, double *d_s
   B.ang = (float *)(base + o_ang);
   int rc = clear_prep_state(c, B);
   if (rc) return rc;
+  // soapb_check_inputs reports this call's input errors from the array's word
+  c->last_err = B.err;
   DevParams P = c->P;
   P.n_pairs = B.n_pairs;
   P.n_sites = B.n_sites;
   LaunchCfg cfg = site_cfg(c, false);
   if (b->n_atom_pairs > 0 || b->n_sites > 0) {
+    TimedLaunch tl(c, SOAPB_KERNEL_PAIR);
     CU(launch_pair(P, B, c->stream, 0));
     c->launches += 1;
   }
-  if (b->n_sites > 0) CU(launch_descriptor(P, B, cfg, d_soap, nullptr, nullptr, 0));
-  c->launches += (b->n_sites > 0);
+  if (b->n_sites > 0) {
+    TimedLaunch tl(c, SOAPB_KERNEL_DESCRIPTOR);
+    CU(launch_descriptor(P, B, cfg, d_soap, nullptr, nullptr, 0));
+    c->launches += 1;
+  }
   return SOAPB_OK;
 }
 
@@ -1319,9 +1492,9 @@ int soapb_contract_cart_der(soapb_context *c, const soapb_batch *b, const double
 int soapb_check_inputs(soapb_context *c, int64_t *bad_pair) {
   if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
   if (bad_pair) *bad_pair = -1;
-  if (!c->err.p) return SOAPB_OK;
+  if (!c->last_err) return SOAPB_OK;
   unsigned long long w = 0;
-  CU(cudaMemcpyAsync(&w, c->err.p, sizeof w, cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaMemcpyAsync(&w, c->last_err, sizeof w, cudaMemcpyDeviceToHost, c->stream));
   CU(cudaStreamSynchronize(c->stream));
   return input_status(w, bad_pair);
 }
@@ -1448,6 +1621,45 @@ int soapb_build_neighbors(soapb_context *c, int32_t n_atoms, const double *d_pos
   out->phis = o.phis;
   if (d_neigh_atom) *d_neigh_atom = o.neigh_atom;
   return SOAPB_OK;
+}
+
+// Self-test of the scan's bounded look-back wait (the wait of soapb_scan.cuh):
+// a two-tile scan of 2 x 2048 unit counts of which only tile 1 runs, its tile
+// index and its predecessor's state prepared on the host.  With the
+// predecessor published the wait ends at once; without it the wait gives up
+// after max_spins spins and the scan reports it.  Small device buffers are
+// allocated and freed here; the current device is used.
+int soapb_selftest_scan_wait(int32_t max_spins, int32_t publish_predecessor, int64_t *last_offset) {
+  if (max_spins < 0) return fail(SOAPB_ERR_ARGUMENT, "negative max_spins");
+  int rc = check_device();
+  if (rc) return rc;
+  const int n = 2 * kScanTileSites, words = prep_err_words(n);
+  std::vector<int> ones((size_t)n, 1);
+  std::vector<unsigned long long> state((size_t)words, 0ull);
+  state[1] = 1;  // the tile counter: the one block launched takes tile 1
+  if (publish_predecessor) state[2] = (2ull << 32) | (unsigned)kScanTileSites;  // tile 0's inclusive prefix
+  DBuf counts, off, st;
+  auto done = [&](int r) {
+    counts.release();
+    off.release();
+    st.release();
+    return r;
+  };
+  if ((rc = counts.ensure(4 * (size_t)n)) || (rc = off.ensure(4 * ((size_t)n + 1))) ||
+      (rc = st.ensure(8 * (size_t)words)))
+    return done(rc);
+  cudaError_t e = cudaMemcpy(counts.p, ones.data(), 4 * (size_t)n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(st.p, state.data(), 8 * (size_t)words, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = launch_scan(counts.as<int>(), n, off.as<int>(), st.as<unsigned long long>(), 0, 1, max_spins);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  int last = 0;
+  unsigned long long w = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&last, off.as<int>() + n, 4, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(&w, st.p, 8, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return done(cuda_fail(e, "scan self-test"));
+  if (last_offset) *last_offset = last;
+  return done(input_status(w, nullptr));
 }
 
 int soapb_launch_count(const soapb_context *c, int64_t *count) {
@@ -1716,7 +1928,8 @@ struct DropIn {
   std::vector<double> user_W, user_S;  // caller-supplied basis, if any
   bool warned_poly3 = false, warned_gauss = false;
   // device copies of the last batch
-  DBuf n_neigh, species, species_mult, mask, rjs, thetas, phis, soap, G, pair, cart, vecs, hess;
+  DBuf n_neigh, species, species_mult, mask, rjs, thetas, phis, soap, G, pair, cart, cart_self, vecs, hess;
+  std::vector<double> self_host;  // the caller's self columns of soap_cart_der, gathered
   soapb_batch batch{};
   int ct_ready = 0, ct_fp64 = 0, ct_n_sites = 0, ct_n_pairs = 0, ct_n_soap = 0;
   // soap_hessian_enabled and what get_soap_central_hessian checks against
@@ -1813,6 +2026,12 @@ struct GetSoapIn {
   bool pin_nn, pin_sp, pin_sm, pin_mask, pin_pair;  // pin_pair: rjs, thetas and phis
   uint8_t *st_nn = nullptr, *st_sp = nullptr, *st_sm = nullptr, *st_mask = nullptr, *st_r = nullptr,
           *st_t = nullptr, *st_f = nullptr;
+  // the caller's soap, copied in chunk by chunk when the descriptor is added
+  // into it (compressed get_soap), through st_soap when it is staged
+  const double *soap = nullptr;
+  int n_soap = 0;
+  bool acc = false;
+  uint8_t *st_soap = nullptr;
 };
 
 size_t align16(size_t x) { return (x + 15) / 16 * 16; }
@@ -1890,6 +2109,14 @@ int copy_in_pairs(DropIn &d, const GetSoapIn &in, int i, int n_species, int n_pa
       return rc;
     if ((rc = h2d_in(d.phis.as<uint8_t>() + b0, (const uint8_t *)in.phis + b0, in.st_f ? in.st_f + b0 : nullptr, nb,
                      d.copy_in)))
+      return rc;
+  }
+  if (in.acc) {
+    // the chunk's rows of the caller's soap, which the descriptor adds into
+    const size_t b0 = 8 * (size_t)d.chunk[i] * in.n_soap, nb = 8 * (size_t)(d.chunk[i + 1] - d.chunk[i]) * in.n_soap;
+    int rc;
+    if ((rc = h2d_in(d.soap.as<uint8_t>() + b0, (const uint8_t *)in.soap + b0,
+                     in.st_soap ? in.st_soap + b0 : nullptr, nb, d.copy_in)))
       return rc;
   }
   CU(cudaEventRecord(d.evs[i], d.copy_in));
@@ -2085,6 +2312,13 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
                is_pinned(species), is_pinned(species_multiplicity), is_pinned(mask),
                is_pinned(rjs) && is_pinned(thetas) && is_pinned(phis)};
   const bool soap_staged = chunked && !is_pinned(soap) && 8 * (size_t)n_sites * n_soap <= kStageCap;
+  // The reference adds the compressed descriptor into the caller's soap
+  // (src/soap_turbo.f90:798-802; its callers pass it zeroed) and overwrites an
+  // uncompressed one; the caller's values therefore come in when compressing.
+  const bool accumulate = compress_soap != 0 && n_sites > 0;
+  in.soap = soap;
+  in.n_soap = n_soap;
+  in.acc = accumulate;
   if (chunked) {
     plan_chunks(d.chunk, n_sites, false);
     nch = (int)d.chunk.size() - 1;
@@ -2099,6 +2333,9 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
     if ((rc = d.soap.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
     if ((rc = plan_get_soap_staging(d, in, n_sites, max_species_multiplicity, n_species, n_atom_pairs))) return rc;
     if (soap_staged && (rc = d.st_out.ensure(8 * (size_t)n_sites * n_soap))) return rc;
+    // staged soap rows come in through the output staging area: chunk i's rows
+    // are copied out of it only after its kernels, which wait for its copy in
+    if (soap_staged) in.st_soap = d.st_out.as<uint8_t>();
     const int copied = copy_in_sites(d, in, n_sites, max_species_multiplicity);
     if (copied) {
       cudaStreamSynchronize(d.copy_in);  // no copy from the caller's arrays outlives the call
@@ -2113,6 +2350,8 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
     if ((rc = upload(d.thetas, thetas, n_atom_pairs, s))) return rc;
     if ((rc = upload(d.phis, phis, n_atom_pairs, s))) return rc;
     if ((rc = d.soap.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
+    if (accumulate)
+      CU(cudaMemcpyAsync(d.soap.p, soap, 8 * (size_t)n_sites * n_soap, cudaMemcpyHostToDevice, s));
   }
   soapb_batch &bt = d.batch;
   bt.n_sites = n_sites;
@@ -2130,7 +2369,23 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
   bool soap_copied = false;
   if (fp64) {
     if (keep_cart && (rc = d.cart.ensure(8 * ((size_t)n_atom_pairs * n_soap * 3 + 1)))) return rc;
-    rc = soapb_descriptor_fp64(c, &bt, d.soap.as<double>(), keep_cart ? d.cart.as<double>() : nullptr);
+    // The self column of soap_cart_der is accumulated into (:888-892): the
+    // caller's self columns come in, gathered into (3, n_soap) per site.
+    const double *self_init = nullptr;
+    if (want_cart && n_atom_pairs > 0) {
+      const size_t w3 = 3 * (size_t)n_soap;
+      d.self_host.resize(w3 * (size_t)n_sites);
+      double *dst = d.self_host.data();
+      const long long *off = d.host_off.data();
+#pragma omp parallel for schedule(static) num_threads(copy_threads(8 * w3 * (size_t)n_sites))
+      for (int i = 0; i < n_sites; ++i) {
+        if (off[i + 1] > off[i]) std::memcpy(dst + w3 * i, soap_cart_der + w3 * (size_t)off[i], 8 * w3);
+        else std::memset(dst + w3 * i, 0, 8 * w3);
+      }
+      if ((rc = upload(d.cart_self, dst, w3 * (size_t)n_sites, s))) return rc;
+      self_init = d.cart_self.as<double>();
+    }
+    rc = ctx_fp64(c, &bt, d.soap.as<double>(), keep_cart ? d.cart.as<double>() : nullptr, accumulate, self_init);
   } else if (chunked) {
     SiteChunks ch;
     ch.n = nch;
@@ -2152,7 +2407,7 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
       if (soap_staged) CU(cudaEventRecord(d.evs[2 * nch + 1 + i], d.copy_out));
       return SOAPB_OK;
     };
-    rc = ctx_descriptor(c, &bt, d.soap.as<double>(), do_derivatives && contract, &ch);
+    rc = ctx_descriptor(c, &bt, d.soap.as<double>(), do_derivatives && contract, &ch, accumulate);
     // the staged soap rows, chunk by chunk as their copies arrive
     for (int i = 0; rc == 0 && soap_staged && i < nch; ++i) {
       const cudaError_t e = cudaEventSynchronize(d.evs[2 * nch + 1 + i]);
@@ -2165,7 +2420,7 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
     }
     soap_copied = true;
   } else {
-    rc = ctx_descriptor(c, &bt, d.soap.as<double>(), do_derivatives && contract);
+    rc = ctx_descriptor(c, &bt, d.soap.as<double>(), do_derivatives && contract, nullptr, accumulate);
   }
   if (rc) {
     if (chunked) {  // no copy from or into the caller's arrays outlives the call

@@ -30,6 +30,20 @@ struct RadSp {
 // DevParams::basis of the poly3operator basis (SOAPB_BASIS_POLY3OPERATOR)
 constexpr int kBasisOperator = 2;
 
+// The tabulated radial expansion of one species (poly3 / poly3gauss with
+// atom_sigma_r_scaling = 0, when every R_n(r) and dR_n/dr is a fixed function
+// of r): piecewise polynomials in t in [-1, 1] on segments of r.  The
+// reference's expansion branches on r -- the filter kept when r_soft - r < 4
+// sigma (src/soap_turbo_radial.f90:721-769), the origin-Gaussian moment only
+// for r < 4 (sigma_0 + sigma) (:875-908), the amplitude zero where h(r) <=
+// 1e-10 (:589-635) -- so each branch state (keep | !gm << 1) has an interval
+// of its own, chosen per pair by the same FP64 tests.
+constexpr int kRadTabDeg = 7;  // polynomial degree of each segment
+struct RadTab {
+  double lo[4], inv_h[4];  // per branch state: interval start, segments per unit r
+  int base[4], nseg[4];    // first segment in the coefficient table, segment count
+};
+
 struct DevParams {
   int n_species, l_max, k_max, n_max;
   int basis;          // 0 poly3, 1 poly3gauss, 2 poly3operator (kBasisOperator)
@@ -91,6 +105,12 @@ struct DevParams {
   int hl_in_blob;         // the packed Y lists fit in the blob (else read from hl_packed)
   const int *hl_packed;   // global copy of the packed Y lists
   int cmap_identity;      // the compression map sends kept component q to output q, weight 1
+  // tabulated radial expansion (the pair kernel's FP32 form, see RadTab):
+  // coefficients [segment][k = 0..kRadTabDeg][2 amax_t] (R_n then dR_n/dr, with
+  // 4 pi global_scaling folded in), monomials in t ascending
+  int rtab;               // 1: the pair kernel evaluates the tables
+  const float *rtab_coef;
+  RadTab rtab_sp[SOAPB_MAX_SPECIES];
   // power spectrum on the tensor cores: P_l[n, J] for rows n (ps_mt tiles of
   // 16) and the column set J (ps_nt tiles of 8) that covers every kept (n, n')
   int ps_mt, ps_nt;
@@ -127,6 +147,8 @@ struct LaunchCfg {
   int max_ctas;          // persistent grid cap (0 = from the occupancy)
 };
 cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s);
+// sites per tile of the CSR offset scan (soapb_scan.cuh)
+constexpr int kScanTileSites = 2048;
 // 64-bit words of DevBatch::err for a batch of n_sites; the launcher's caller
 // clears them before each prep launch
 int prep_err_words(int n_sites);
@@ -186,8 +208,10 @@ cudaError_t launch_nb_fill(const NbGeom &g, const double *pos, const int *sites,
                            const int *atom_mult, const int4 *atom_cell, const int *cell_start, const int *cell_atoms,
                            const int *off, const NbOut &o, unsigned long long *err, cudaStream_t s);
 // Exclusive scan of n counts into off (n + 1 entries); state: prep_err_words(n)
-// words cleared beforehand.
-cudaError_t launch_scan(const int *counts, int n, int *off, unsigned long long *state, cudaStream_t s);
+// words cleared beforehand.  blocks < 0: one block per tile (the scan); fewer
+// blocks and a smaller max_spins serve the self-test of the bounded wait.
+cudaError_t launch_scan(const int *counts, int n, int *off, unsigned long long *state, cudaStream_t s,
+                        int blocks = -1, int max_spins = 1 << 20);
 
 // Plain FP64 staged path
 struct Fp64Work {
@@ -197,9 +221,15 @@ struct Fp64Work {
   double *soap_unnorm;     // (n_sites, n_soap)
   double *norm;            // n_sites
 };
+// soap_acc (may be null): the caller's soap, accumulated into before the norm
+// (compressed get_soap); self_init (may be null, with cart): the caller's self
+// columns of soap_cart_der, (3, n_soap) per site, which the self column
+// accumulates into.  soap may be the same array as soap_acc.
 cudaError_t launch_fp64_descriptor(const DevParams &P, const DevBatch &B, cudaStream_t s,
                                    const Fp64Work &w, int do_der, double *soap, double *cart,
-                                   int *launches);
+                                   int *launches, const double *soap_acc = nullptr,
+                                   const double *self_init = nullptr);
+size_t fp64_cart_smem(const DevParams &P);  // dynamic shared memory of the soap_cart_der kernel
 cudaError_t launch_fp64_contract(const DevParams &P, const DevBatch &B, cudaStream_t s,
                                  const double *cart, const double *G, int g_layout, double sgn,
                                  double *pair, int *launches);

@@ -226,9 +226,11 @@ int ang_row_floats(const DevParams &P) { return row_len(P.amax_t == 8 ? 8 : 12);
 // The site kernels only read these rows; soap_contract reads the rows of the
 // descriptor call that kept its state, as the reference keeps the radial and
 // angular expansions between get_soap and soap_contract.
-// 128-thread CTAs, 3 per SM (144 registers a thread)
+// TAB: R_n and dR_n/dr come from the context's piecewise-polynomial tables
+// (FP32 evaluation of the FP64 expansion fitted per species; see RadTab)
+// instead of the FP64 expansion itself.
 constexpr int kPairThreads = 128;
-template <int AMAX, int LC, bool OP>
+template <int AMAX, int LC, bool OP, bool TAB>
 __global__ void __launch_bounds__(kPairThreads)
     k_pair(const DevParams P, const DevBatch B, int do_der, int scan_tiles, int pair_lo, int pair_hi) {
   constexpr int NT = kPairThreads;
@@ -281,10 +283,23 @@ __global__ void __launch_bounds__(kPairThreads)
         const int s = __ffs(todo) - 1;
         todo &= todo - 1u;
         const RadSp &RS = *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
+        float4 *o = (float4 *)(B.rad + ((size_t)k * P.n_species + s) * 2 * AMAX);
+        if constexpr (TAB) {
+          float v[2 * AMAX];
+          radial_from_table<AMAX>(P, RS, P.rtab_sp[s], r, do_der != 0, v);
+#pragma unroll
+          for (int n4 = 0; n4 < AMAX / 4; ++n4)
+            o[n4] = make_float4(v[4 * n4], v[4 * n4 + 1], v[4 * n4 + 2], v[4 * n4 + 3]);
+          if (do_der)
+#pragma unroll
+            for (int n4 = 0; n4 < AMAX / 4; ++n4)
+              o[AMAX / 4 + n4] = make_float4(v[AMAX + 4 * n4], v[AMAX + 4 * n4 + 1], v[AMAX + 4 * n4 + 2],
+                                             v[AMAX + 4 * n4 + 3]);
+          continue;
+        }
         double val[AMAX], der[AMAX];
         radial_entry<AMAX, OP>(P, RS, sW + s * AMAX * AMAX, r, false, do_der != 0, val, der);
         const double g4 = kFourPi * RS.gscale;
-        float4 *o = (float4 *)(B.rad + ((size_t)k * P.n_species + s) * 2 * AMAX);
 #pragma unroll
         for (int n4 = 0; n4 < AMAX / 4; ++n4)
           o[n4] = make_float4((float)(g4 * val[4 * n4]), (float)(g4 * val[4 * n4 + 1]),
@@ -564,6 +579,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
                                                       double *__restrict__ soap_out,
                                                       float *__restrict__ keep_c,
                                                       double *__restrict__ keep_norm, int keep) {
+  // keep: bit 0 keeps c_nlm and the norm for the contract, bit 1 accumulates
+  // into soap_out
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int CH = stage_entries_per_round(NT, 0);
   constexpr int NH = AMAX / 2;  // radial indices per c_nlm item
@@ -736,13 +753,27 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
         nrm2 += (double)v * (double)v;
       }
     }
+    double *out = soap_out + (size_t)site * P.n_soap;
+    // accumulate: the caller's soap row is added before the norm is taken, as
+    // the reference adds the compressed descriptor into soap (:798-802).  Each
+    // thread reads and writes the same components of the row.
+    const bool acc = (keep & 2) != 0;
+    if (acc) {
+      nrm2 = 0.0;
+      for (int o = tid; o < P.n_soap; o += NT) {
+        const double v = (double)sS[o] + out[o];
+        nrm2 += v * v;
+      }
+    }
     nrm2 = block_sum<NT>(nrm2, sRed);  // (:805-809)
     double norm = sqrt(nrm2);
     if (norm < 1.0e-5) norm = 1.0;
     const double inv = 1.0 / norm;
-    double *out = soap_out + (size_t)site * P.n_soap;
-    for (int o = tid; o < P.n_soap; o += NT) out[o] = (double)sS[o] * inv;
-    if (keep) {
+    if (acc)
+      for (int o = tid; o < P.n_soap; o += NT) out[o] = ((double)sS[o] + out[o]) * inv;
+    else
+      for (int o = tid; o < P.n_soap; o += NT) out[o] = (double)sS[o] * inv;
+    if (keep & 1) {
       float *kc = keep_c + (size_t)site * keep_stride(P);
       const int n4 = (2 * n_max * KS) / 4;
       for (int t = tid; t < n4; t += NT) ((float4 *)kc)[t] = ((const float4 *)sC)[t];
@@ -1108,13 +1139,13 @@ cudaError_t launch_prep(const DevParams &P, const DevBatch &B, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int AMAX, int LC, bool OP>
+template <int AMAX, int LC, bool OP, bool TAB = false>
 static cudaError_t run_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der, int pair_lo,
                             int pair_hi, bool scan) {
   size_t sm = (size_t)P.off_rad + (size_t)P.n_species * SOAPB_RADSP_BYTES +
               (size_t)kPairThreads * (row_len(LC) + 1) * sizeof(float);
   if (sm < kScanTile * sizeof(int)) sm = kScanTile * sizeof(int);  // scan tiles reuse it
-  auto kern = k_pair<AMAX, LC, OP>;
+  auto kern = k_pair<AMAX, LC, OP, TAB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int tiles = scan ? prep_scan_tiles(B.n_sites) : 0;
@@ -1130,6 +1161,10 @@ cudaError_t launch_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, i
   if (P.basis == kBasisOperator) {
     if (P.amax_t == 8) return run_pair<8, 8, true>(P, B, s, do_der, pair_lo, pair_hi, scan);
     return run_pair<16, 12, true>(P, B, s, do_der, pair_lo, pair_hi, scan);
+  }
+  if (P.rtab) {
+    if (P.amax_t == 8) return run_pair<8, 8, false, true>(P, B, s, do_der, pair_lo, pair_hi, scan);
+    return run_pair<16, 12, false, true>(P, B, s, do_der, pair_lo, pair_hi, scan);
   }
   if (P.amax_t == 8) return run_pair<8, 8, false>(P, B, s, do_der, pair_lo, pair_hi, scan);
   return run_pair<16, 12, false>(P, B, s, do_der, pair_lo, pair_hi, scan);

@@ -255,9 +255,9 @@ __global__ void __launch_bounds__(32 * kNbFillWarps) k_nb_fill(NbGeom g, const d
   for (int m = lane; m < g.max_mult; m += 32) o.species[(size_t)w * g.max_mult + m] = atom_species[(size_t)a * g.max_mult + m];
 }
 
-__global__ void __launch_bounds__(256) k_nb_scan(DevBatch B, int tiles) {
+__global__ void __launch_bounds__(256) k_nb_scan(DevBatch B, int tiles, int max_spins) {
   __shared__ int sv[kScanTile];
-  prep_scan_tile<256>(B, tiles, sv);
+  prep_scan_tile<256>(B, tiles, sv, max_spins);
 }
 
 }  // namespace
@@ -292,7 +292,8 @@ cudaError_t launch_nb_fill(const NbGeom &g, const double *pos, const int *sites,
   return cudaGetLastError();
 }
 
-cudaError_t launch_scan(const int *counts, int n, int *off, unsigned long long *state, cudaStream_t s) {
+cudaError_t launch_scan(const int *counts, int n, int *off, unsigned long long *state, cudaStream_t s,
+                        int blocks, int max_spins) {
   DevBatch B{};
   B.n_sites = n;
   B.n_pairs = -1;
@@ -300,7 +301,8 @@ cudaError_t launch_scan(const int *counts, int n, int *off, unsigned long long *
   B.off = off;
   B.err = state;
   const int tiles = prep_scan_tiles(n);
-  if (tiles > 0) k_nb_scan<<<tiles, 256, 0, s>>>(B, tiles);
+  if (blocks < 0 || blocks > tiles) blocks = tiles;
+  if (blocks > 0) k_nb_scan<<<blocks, 256, 0, s>>>(B, tiles, max_spins);
   return cudaGetLastError();
 }
 

@@ -23,7 +23,9 @@ namespace soapb {
 // last tile writes off[n_sites] and checks it against n_pairs (skipped when
 // n_pairs < 0: the neighbour-list builder scans counts whose total it learns
 // from the scan).
-constexpr int kScanTile = 2048;
+constexpr int kScanTile = kScanTileSites;
+// Spins of the look-back wait before it gives up (each sleeps ~64 ns).
+constexpr int kScanSpins = 1 << 20;
 
 __host__ __device__ inline int prep_scan_tiles(int n_sites) { return (n_sites + kScanTile - 1) / kScanTile; }
 
@@ -31,9 +33,11 @@ __device__ __forceinline__ void prep_error(const DevBatch &B, unsigned long long
   atomicMax(B.err, kErrTop - code);
 }
 
-// One scan tile per calling block (NTH threads); sv: kScanTile ints of shared memory.
+// One scan tile per calling block (NTH threads); sv: kScanTile ints of shared
+// memory; max_spins bounds the wait for a predecessor.
 template <int NTH>
-__device__ __forceinline__ void prep_scan_tile(const DevBatch &B, int scan_tiles, int *sv) {
+__device__ __forceinline__ void prep_scan_tile(const DevBatch &B, int scan_tiles, int *sv,
+                                               int max_spins = kScanSpins) {
   constexpr int ITEMS = kScanTile / NTH;
   __shared__ int wtot[NTH / 32];
   __shared__ int s_tile, s_excl;
@@ -94,7 +98,7 @@ __device__ __forceinline__ void prep_scan_tile(const DevBatch &B, int scan_tiles
           excl += (unsigned)w;
           if (f == 2u) break;
           --j;
-        } else if (++spins > (1 << 20)) {
+        } else if (++spins > max_spins) {
           prep_error(B, kErrScan);
           break;
         } else {

@@ -54,9 +54,12 @@ def get_soap(n_sites, n_neigh, n_species, species, species_multiplicity, n_atom_
 
     Shapes as in Fortran: species (max_mult, n_sites), mask (n_atom_pairs,
     n_species), soap (n_soap, n_sites) and soap_cart_der (3, n_soap,
-    n_atom_pairs), all Fortran-ordered float64 / int32 / bool arrays.  soap is
-    overwritten with the normalised descriptor; soap_cart_der is written when
-    do_derivatives and not contract (pass None otherwise)."""
+    n_atom_pairs), all Fortran-ordered float64 / int32 / bool arrays.  soap
+    receives the normalised descriptor; soap_cart_der is written when
+    do_derivatives and not contract (pass None otherwise).  As in the
+    reference, a compressed soap is added into (the caller's values count in
+    the norm) and the self columns of soap_cart_der are accumulated into, so
+    callers pass both zeroed (src/soap_turbo.f90:798-802, 888-892)."""
     lib = _lib.load()
     if not (isinstance(soap, np.ndarray) and soap.dtype == _f64 and soap.flags.f_contiguous):
         raise TypeError("soap must be a Fortran-ordered float64 array (written in place)")

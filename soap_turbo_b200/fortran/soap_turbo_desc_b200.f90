@@ -11,8 +11,10 @@
 ! bad input.
 !
 ! Behavioural notes for callers of the reference:
-!  * soap is overwritten.  The reference accumulates into it when compressing,
-!    so its callers pass it zeroed; with a zeroed soap the results agree.
+!  * soap and soap_cart_der are intent(inout) with the reference's meaning: a
+!    compressed soap is added into (src/soap_turbo.f90:798-802), the self
+!    columns of soap_cart_der are accumulated into (:888-892); callers pass
+!    both zeroed, as for the reference.
 !  * soap_cart_der is written only when do_derivatives and not contract, and
 !    then in FP64 like the reference.  With contract, call soap_contract.
 module soap_turbo_desc_b200

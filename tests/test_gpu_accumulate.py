@@ -1,0 +1,104 @@
+"""The drop-in get_soap keeps the reference's intent(inout) meaning of soap and
+soap_cart_der: a compressed soap is added into before the norm is taken
+(src/soap_turbo.f90:798-802), an uncompressed one is overwritten, and each
+site's self column of soap_cart_der is accumulated into (:888-892).  Checked
+against the oracle given the same arrays on entry; the contract that follows
+reads the norms of the accumulated rows, as the reference's does."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from conftest import FP64_TOL, SOAP_TOL, VJP_TOL, max_rel_err, site_rel_err
+from soap_turbo_b200 import descriptor as D
+from soap_turbo_b200 import synthetic as syn
+from soap_turbo_b200.context import Context
+from test_gpu_parity import _dropin_args
+
+pytestmark = pytest.mark.gpu
+
+
+def _host(a, pinned, keep):
+    if not pinned:
+        return np.asfortranarray(a)
+    t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+    out = t.numpy().reshape(a.shape, order="F")
+    out[...] = a
+    keep.append(t)
+    return out
+
+
+@pytest.mark.parametrize("case", ["chunked_pinned", "chunked_pageable", "single_launch", "timed"])
+def test_compressed_soap_is_added_into(case):
+    # 1703 sites: the drop-in runs three site chunks, each copying its soap rows
+    # in beside its pair inputs; a quarter-size batch runs as one launch, and
+    # do_timing takes the unchunked path
+    w = syn.config(2, seed=41, scale=0.25 if case == "single_launch" else 1.0)
+    nl = w.nl
+    ctx = Context(w.hyper)
+    W, S = ctx.basis()
+    rng = np.random.default_rng(3)
+    soap0 = 0.05 * rng.standard_normal((ctx.n_soap, nl.n_sites))  # Fortran soap(n_soap, n_sites)
+    ref = O.get_soap(w.hyper, nl, W, S, do_derivatives=True, soap_init=soap0.T)
+    ref_zero = O.get_soap(w.hyper, nl, W, S, do_derivatives=True)
+    assert site_rel_err(ref.soap, ref_zero.soap) > 1e-3  # the caller's values matter
+    G = rng.standard_normal((ctx.n_soap, nl.n_sites))
+    keep = []
+    pinned = case == "chunked_pinned"
+    D.set_basis_matrices(W, S)
+    try:
+        for _ in range(2):  # the second call must not see the first call's rows
+            soap = _host(soap0, pinned, keep)
+            args = _dropin_args(w, soap)
+            args["do_timing"] = case == "timed"
+            D.get_soap(**args, contract=True)
+            assert site_rel_err(soap.T, ref.soap) <= SOAP_TOL
+            pair = _host(np.zeros((3, nl.n_pairs)), pinned, keep)
+            D.soap_contract(soap, _host(G.T, pinned, keep), 1.0, pair)
+            assert max_rel_err(pair.T, ref.contract(G, 1.0)) <= VJP_TOL
+    finally:
+        D.set_basis_matrices(None)
+
+
+def test_uncompressed_soap_is_overwritten():
+    w = syn.config(1, seed=7)
+    nl = w.nl
+    ctx = Context(w.hyper)
+    W, S = ctx.basis()
+    ref = O.get_soap(w.hyper, nl, W, S, do_derivatives=True)
+    D.set_basis_matrices(W, S)
+    try:
+        soap = np.asfortranarray(np.random.default_rng(4).standard_normal((ctx.n_soap, nl.n_sites)))
+        D.get_soap(**_dropin_args(w, soap), contract=True)
+        assert site_rel_err(soap.T, ref.soap) <= SOAP_TOL
+    finally:
+        D.set_basis_matrices(None)
+
+
+def test_soap_cart_der_self_columns_are_accumulated_into():
+    # do_derivatives without contract: the FP64 path writes soap_cart_der; its
+    # neighbour columns are overwritten, its self columns accumulate
+    w = syn.config(2, seed=11, scale=0.25)
+    nl = w.nl
+    ctx = Context(w.hyper)
+    W, S = ctx.basis()
+    rng = np.random.default_rng(5)
+    soap0 = 0.05 * rng.standard_normal((ctx.n_soap, nl.n_sites))
+    cart0 = rng.standard_normal((3, ctx.n_soap, nl.n_pairs))
+    ref = O.get_soap(w.hyper, nl, W, S, do_derivatives=True, cart_der=True, soap_init=soap0.T,
+                     cart_init=np.transpose(cart0, (2, 1, 0)))
+    D.set_basis_matrices(W, S)
+    try:
+        soap = np.asfortranarray(soap0)
+        cart = np.asfortranarray(cart0)
+        D.get_soap(**_dropin_args(w, soap, cart=cart), contract=False)
+        assert site_rel_err(soap.T, ref.soap) <= SOAP_TOL
+        got = np.transpose(cart, (2, 1, 0))
+        assert max_rel_err(got, ref.soap_cart_der) <= FP64_TOL
+        # the self columns really carry the caller's values
+        first = np.concatenate([[0], np.cumsum(nl.n_neigh)[:-1]])
+        ref_zero = O.get_soap(w.hyper, nl, W, S, do_derivatives=True, cart_der=True, soap_init=soap0.T)
+        d = got[first] - ref_zero.soap_cart_der[first]
+        np.testing.assert_allclose(d, np.transpose(cart0, (2, 1, 0))[first], rtol=1e-9, atol=1e-9)
+    finally:
+        D.set_basis_matrices(None)

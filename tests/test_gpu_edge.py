@@ -228,3 +228,19 @@ def test_bad_inputs_are_reported():
     with pytest.raises(_lib.SoapError) as e:
         ctx.check_inputs()
     assert e.value.code == 8
+
+
+def test_scan_wait_gives_up_and_reports():
+    """The CSR offset scan's look-back wait is bounded: a tile whose predecessor
+    never publishes gives up after its spin limit and the scan reports it
+    (SOAPB_ERR_CUDA, "gave up waiting"); with the predecessor published (tile
+    states prepared on the host) the same launch ends normally with the right
+    total.  Nothing hangs or faults either way."""
+    import ctypes as C
+    lib = _lib.load()
+    last = C.c_int64(-1)
+    assert lib.soapb_selftest_scan_wait(1000, 1, C.byref(last)) == 0
+    assert last.value == 4096
+    rc = lib.soapb_selftest_scan_wait(1000, 0, C.byref(last))
+    assert rc == 6 and b"gave up waiting" in lib.soapb_last_error()
+    assert last.value == 2048  # the tile's own sum, no predecessor's prefix

@@ -59,3 +59,43 @@ def test_noalloc_rejects_batches_beyond_its_array(setup):
     ctx2_out = ctx.descriptor_noalloc(setup[2])
     ref = ctx.descriptor(setup[2], keep=False)
     assert site_rel_err(ctx2_out.cpu().numpy(), ref.cpu().numpy()) < SOAP_TOL
+
+
+def test_noalloc_allocates_no_device_memory(setup):
+    """After the first call on the device (which loads the static array), the
+    free device memory does not move across further calls: neither the library
+    nor the CUDA runtime allocates for them."""
+    import torch
+    ctx, b_big, b_small = setup
+    out_big = torch.empty(b_big.n_sites, ctx.n_soap, dtype=torch.float64, device="cuda")
+    out_small = torch.empty(b_small.n_sites, ctx.n_soap, dtype=torch.float64, device="cuda")
+    ctx.descriptor_noalloc(b_big, out=out_big)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        ctx.descriptor_noalloc(b_small, out=out_small)
+        ctx.descriptor_noalloc(b_big, out=out_big)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
+def test_noalloc_reports_bad_inputs(setup):
+    """A non-finite pair input of an allocation-free call is reported by
+    soapb_check_inputs (from the static array's error word), with its index;
+    the next clean call clears it."""
+    from soap_turbo_b200 import _lib
+    ctx, _, b_small = setup
+    ctx.descriptor_noalloc(b_small)
+    ctx.check_inputs()
+    saved = b_small.rjs[7].item()
+    b_small.rjs[7] = float("nan")
+    try:
+        ctx.descriptor_noalloc(b_small)
+        with pytest.raises(_lib.SoapError) as e:
+            ctx.check_inputs()
+        assert e.value.code == 8 and "pair 7" in str(e.value)
+    finally:
+        b_small.rjs[7] = saved
+    ctx.descriptor_noalloc(b_small)
+    ctx.check_inputs()
