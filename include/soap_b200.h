@@ -232,12 +232,14 @@ int soapb_set_stream(soapb_context *ctx, void *stream);
 /* Work tuning: threads per site CTA (64, 128 or 256) for both site kernels;
  * 0 returns to the autotuner's choice, or 128 before any autotuning. */
 int soapb_set_threads_per_site(soapb_context *ctx, int32_t threads);
-/* Autotuner: times the descriptor and the contract on this batch for every
- * CTA size (64, 128, 256 threads per site) and persistent grid cap (the
- * occupancy limit, 2 and 1 CTAs per SM), and keeps the fastest per kernel in
- * the context.  choice (4, may be NULL) receives {descriptor threads,
- * descriptor grid cap, contract threads, contract grid cap}, 0 meaning the
- * occupancy limit.  A set-up call: it allocates and frees work buffers,
+/* Autotuner: times the descriptor and the contract on this batch in each form
+ * -- the tensor-core kernels (when allowed, see soapb_set_tensor_cores) and the
+ * CUDA-core kernels at every CTA size (64, 128, 256 threads per site) -- and
+ * each persistent grid cap (the occupancy limit, 2 and 1 CTAs per SM), and
+ * keeps the fastest per kernel in the context.  choice (4, may be NULL)
+ * receives {descriptor threads, descriptor grid cap, contract threads,
+ * contract grid cap}: threads 0 means the tensor-core kernel, a grid cap of 0
+ * the occupancy limit.  A set-up call: it allocates and frees work buffers,
  * synchronises the context's stream and discards the state kept for
  * soapb_contract.  Results are bit-reproducible for a fixed choice; another
  * CTA size changes the summation grouping within FP32 rounding. */
@@ -257,6 +259,12 @@ int soapb_autotune(soapb_context *ctx, const soapb_batch *batch, int32_t *choice
  * change discards the state kept for soapb_contract. */
 int soapb_set_radial_tables(soapb_context *ctx, int32_t enable);
 int soapb_radial_tables(const soapb_context *ctx, int32_t *in_use, double *max_err);
+
+/* Tensor cores (tcgen05, 3xTF32 with FP32 accumulation in tensor memory) for
+ * the site kernels' contractions where the definition has them (every
+ * alpha_max <= 8 and l_max <= 8): 1 (the default) or 0 (the CUDA-core forms).
+ * Results agree within FP32 rounding; each form is bitwise reproducible. */
+int soapb_set_tensor_cores(soapb_context *ctx, int32_t enable);
 
 /* Descriptor of one batch: d_soap (n_soap, n_sites), normalised.  With
  * keep_for_contract, the expansion coefficients c_nlm and norms stay in the

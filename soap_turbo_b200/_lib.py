@@ -113,6 +113,7 @@ SIGNATURES = {
     "soapb_selftest_scan_wait": (C.c_int, [C.c_int32, C.c_int32, i64p]),
     "soapb_set_radial_tables": (C.c_int, [C.c_void_p, C.c_int32]),
     "soapb_radial_tables": (C.c_int, [C.c_void_p, i32p, f64p]),
+    "soapb_set_tensor_cores": (C.c_int, [C.c_void_p, C.c_int32]),
 }
 KERNEL_KINDS = ("prep", "pair", "descriptor", "contract")
 

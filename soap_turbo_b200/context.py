@@ -167,6 +167,11 @@ class Context:
         expansion (True, when its check passed) or the FP64 expansion (False)."""
         _lib.check(self._lib.soapb_set_radial_tables(self._h, int(bool(enable))))
 
+    def set_tensor_cores(self, enable: bool):
+        """soapb_set_tensor_cores: the site kernels' contractions on the tensor
+        cores (True, the default) or on the CUDA cores (False)."""
+        _lib.check(self._lib.soapb_set_tensor_cores(self._h, int(bool(enable))))
+
     def radial_tables(self):
         """(in use, largest relative error of the tables; -1 when not tabulated)."""
         use, err = C.c_int32(0), C.c_double(0.0)
@@ -251,12 +256,14 @@ class Context:
         return out
 
     def autotune(self, b: DeviceBatch) -> dict:
-        """soapb_autotune: time every CTA size and grid cap of both site
-        kernels on this batch and keep the fastest; returns the choice."""
+        """soapb_autotune: time both site kernels on this batch in each form
+        (tensor cores, CUDA cores at every CTA size) and grid cap, and keep the
+        fastest; returns the choice (threads 0: the tensor-core kernel)."""
         ch = (C.c_int32 * 4)()
         _lib.check(self._lib.soapb_autotune(self._h, b.c, ch))
         return {"descriptor_threads": ch[0], "descriptor_max_ctas": ch[1],
-                "contract_threads": ch[2], "contract_max_ctas": ch[3]}
+                "contract_threads": ch[2], "contract_max_ctas": ch[3],
+                "descriptor_tensor_cores": ch[0] == 0, "contract_tensor_cores": ch[2] == 0}
 
     def descriptor_noalloc(self, b: DeviceBatch, out=None):
         """soapb_descriptor_noalloc: the descriptor with its scratch in the

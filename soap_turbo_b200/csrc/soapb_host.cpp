@@ -291,6 +291,9 @@ struct soapb_context {
   // their largest relative error, and whether the caller allows them
   int rtab_ok = 0, rtab_enable = 1;
   double rtab_err = 0.0;
+  // the site kernels' contractions on the tensor cores (where instantiated):
+  // allowed by the caller, and the autotuner's choice per kernel
+  int tc_enable = 0, tune_tcd = 1, tune_tcc = 1;
   // device timing of the kernels (soapb_kernel_timing): an event pair around
   // each timed launch, tkind[i] the kernel of pair i, tn pairs recorded so far
   std::vector<cudaEvent_t> tev;
@@ -847,6 +850,8 @@ int build_tables(soapb_context *c) {
   c->rtab_ok = amax_t == 8 ? fit_radial_tables<8>(c, P, rtab, P.rtab_sp, &c->rtab_err)
                            : fit_radial_tables<16>(c, P, rtab, P.rtab_sp, &c->rtab_err);
   P.rtab = c->rtab_ok && c->rtab_enable;
+  P.tc_contract = c->tc_enable && c->tune_tcc;
+  P.tc_descriptor = c->tc_enable && c->tune_tcd;
   const size_t iRt = add(rtab.data(), rtab.size() * 4);
   P.blob_bytes = (int)blob.size();
   P.blob_c_bytes = (int)blob_c.size();
@@ -1058,6 +1063,7 @@ int input_status(unsigned long long w, int64_t *bad_pair) {
   const unsigned long long v = prep_error_code(w);
   if (v == ~0ull) return SOAPB_OK;
   if (v == (1ull << 33)) return fail(SOAPB_ERR_INPUT, "n_neigh is negative or does not sum to n_atom_pairs");
+  if (v == kErrTc) return fail(SOAPB_ERR_CUDA, "a site kernel gave up waiting for its tensor-core MMAs");
   if (v > (1ull << 33)) return fail(SOAPB_ERR_CUDA, "the CSR offset scan gave up waiting for a preceding tile");
   if (bad_pair) *bad_pair = (int64_t)v;
   return fail(SOAPB_ERR_INPUT, "non-finite or negative pair input at pair %llu", v);
@@ -1367,6 +1373,14 @@ int soapb_set_radial_tables(soapb_context *c, int32_t enable) {
   c->rtab_enable = enable ? 1 : 0;
   c->P.rtab = c->rtab_ok && c->rtab_enable;
   c->keep_valid = 0;  // the kept pair rows came from the other form
+  return SOAPB_OK;
+}
+
+int soapb_set_tensor_cores(soapb_context *c, int32_t enable) {
+  if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
+  c->tc_enable = enable ? 1 : 0;
+  c->P.tc_contract = c->tc_enable && c->tune_tcc;
+  c->P.tc_descriptor = c->tc_enable && c->tune_tcd;
   return SOAPB_OK;
 }
 
@@ -1727,15 +1741,20 @@ int soapb_autotune(soapb_context *c, const soapb_batch *b, int32_t *choice) {
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
-  const int tcand[3] = {64, 128, 256};
+  // candidates: the tensor-core kernels (one CTA size) when the caller allows
+  // them, then the CUDA-core kernels at each CTA size; each with three grid caps
+  const int tcand[4] = {0, 64, 128, 256};  // 0: the tensor-core kernel
   const int ccand[3] = {0, 2 * sms, sms};
+  const int saved_tcd = c->tune_tcd, saved_tcc = c->tune_tcc;
   float best_d = 1e30f, best_c = 1e30f;
   int td = 128, cd = 0, tc = 128, cc = 0;
   rc = SOAPB_OK;
-  for (int it = 0; it < 3 && !rc; ++it)
+  for (int it = c->tc_enable ? 0 : 1; it < 4 && !rc; ++it)
     for (int ic = 0; ic < 3 && !rc; ++ic) {
-      c->threads = tcand[it];
+      c->threads = tcand[it] ? tcand[it] : 128;
       c->max_ctas = ccand[ic];
+      c->tune_tcd = c->tune_tcc = tcand[it] == 0;
+      c->P.tc_descriptor = c->P.tc_contract = tcand[it] == 0;
       float md = 1e30f, mc = 1e30f;
       for (int rep = 0; rep < 4 && !rc; ++rep) {
         float t1 = 0.f, t2 = 0.f;
@@ -1766,10 +1785,20 @@ int soapb_autotune(soapb_context *c, const soapb_batch *b, int32_t *choice) {
   c->threads = saved_threads;
   c->max_ctas = saved_ctas;
   c->keep_valid = 0;  // the timed calls replaced the kept state
-  if (rc) return rc;
-  c->tune_td = td;
+  if (rc) {
+    c->tune_tcd = saved_tcd;
+    c->tune_tcc = saved_tcc;
+    c->P.tc_descriptor = c->tc_enable && c->tune_tcd;
+    c->P.tc_contract = c->tc_enable && c->tune_tcc;
+    return rc;
+  }
+  c->tune_tcd = td == 0;
+  c->tune_tcc = tc == 0;
+  c->P.tc_descriptor = c->tc_enable && c->tune_tcd;
+  c->P.tc_contract = c->tc_enable && c->tune_tcc;
+  c->tune_td = td ? td : 128;
   c->tune_cd = cd;
-  c->tune_tc = tc;
+  c->tune_tc = tc ? tc : 128;
   c->tune_cc = cc;
   if (choice) {
     choice[0] = td;

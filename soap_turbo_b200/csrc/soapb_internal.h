@@ -109,6 +109,8 @@ struct DevParams {
   // coefficients [segment][k = 0..kRadTabDeg][2 amax_t] (R_n then dR_n/dr, with
   // 4 pi global_scaling folded in), monomials in t ascending
   int rtab;               // 1: the pair kernel evaluates the tables
+  int tc_contract;        // 1: the contract's per-entry contraction runs on the tensor cores
+  int tc_descriptor;      // 1: the descriptor's c_nlm runs on the tensor cores
   const float *rtab_coef;
   RadTab rtab_sp[SOAPB_MAX_SPECIES];
   // power spectrum on the tensor cores: P_l[n, J] for rows n (ps_mt tiles of
@@ -171,12 +173,14 @@ size_t descriptor_smem(const DevParams &P, int threads);
 // `device` must be current.
 cudaError_t noalloc_scratch(int device, unsigned char **addr, size_t *bytes);
 size_t contract_smem(const DevParams &P, int threads);
+size_t contract_tc_smem(const DevParams &P);  // dynamic shared memory of the tensor-core contract
 
 // Error codes reported through an error word (kErrTop - code under atomicMax,
 // so the smallest code wins; 0 = none): a pair or site index below 2^32, else
 constexpr unsigned long long kErrCsr = 1ull << 33;        // n_neigh negative or sum != n_pairs
 constexpr unsigned long long kErrScan = (1ull << 33) + 1;  // the scan's look-back wait gave up
 constexpr unsigned long long kErrWrap = (1ull << 33) + 2;  // an atom far outside the cell
+constexpr unsigned long long kErrTc = (1ull << 33) + 3;    // a wait for tensor-core MMAs gave up
 constexpr unsigned long long kErrTop = 1ull << 34;
 
 // Neighbour-list builder (soapb_neigh.cu)

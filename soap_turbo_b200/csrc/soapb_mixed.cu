@@ -26,6 +26,7 @@
 
 #include "soapb_device.cuh"
 #include "soapb_scan.cuh"
+#include "soapb_tc.cuh"
 
 namespace soapb {
 
@@ -573,6 +574,89 @@ __device__ __forceinline__ void ps_tensor(const DevParams &P, const float *sC, f
   }
 }
 
+// ---- C. of a site, from its c_nlm in sC (FP32, (re/im, n, KS)): the power
+// spectrum of the kept components (src/soap_turbo.f90:750-795), the
+// compression, the norm and the normalised FP64 output (:798-809, 904-909),
+// and with keep the c_nlm and norm the contract reads.  keep: bit 0 keeps, bit
+// 1 accumulates into soap_out.  sPl: the tensor-core tile buffer (ps_mt > 0).
+template <int NT>
+__device__ __forceinline__ void site_output(const DevParams &P, unsigned char *smem, const float *sC, float *sP,
+                                            float *sS, float *sPl, const int *kept, double *sRed, int site,
+                                            double *__restrict__ soap_out, float *__restrict__ keep_c,
+                                            double *__restrict__ keep_norm, int keep) {
+  const int tid = threadIdx.x;
+  const int KS = P.k_max | 1;
+  const int n_max = P.n_max;
+    // ---- C. power spectrum of the kept components (src/soap_turbo.f90:750-795)
+    float *pout = P.cmap_identity ? sS : sP;
+    double nrm2 = 0.0;
+    if (P.ps_mt > 0) {
+      // on the tensor cores, then gathered into the kept components with the
+      // sqrt 2 of n != n'
+      ps_tensor<NT>(P, sC, sPl, (const int *)SBLOB(off_psj));
+      __syncthreads();
+      const int *kpos = (const int *)SBLOB(off_kpos);
+      for (int q = tid; q < P.n_kept; q += NT) {
+        const int code = kpos[q];
+        const float v = (code < 0 ? 1.41421356237309504880f : 1.f) * sPl[code & 0x7fffffff];
+        pout[q] = v;
+        nrm2 += (double)v * (double)v;
+      }
+    } else
+    for (int q = tid; q < P.n_kept; q += NT) {
+      const int code = kept[q];
+      const int n = code & 0xff, np = (code >> 8) & 0xff, l = code >> 16;
+      const int kb = l * (l + 1) / 2;
+      const float *cn_r = sC + (size_t)n * KS + kb, *cn_i = sC + (size_t)(n_max + n) * KS + kb;
+      const float *cp_r = sC + (size_t)np * KS + kb, *cp_i = sC + (size_t)(n_max + np) * KS + kb;
+      const float acc0 = cn_r[0] * cp_r[0] + cn_i[0] * cp_i[0];
+      float acc = 0.f;
+      for (int m = 1; m <= l; ++m) acc += cn_r[m] * cp_r[m] + cn_i[m] * cp_i[m];
+      const float base = (n == np) ? 1.f : 1.41421356237309504880f;
+      const float v = base * (acc0 + 2.f * acc);
+      pout[q] = v;
+      nrm2 += (double)v * (double)v;
+    }
+    if (!P.cmap_identity) {
+      // compression through the map (:798-802)
+      __syncthreads();
+      nrm2 = 0.0;
+      for (int o = tid; o < P.n_soap; o += NT) {
+        float v = 0.f;
+        for (int t = P.pi_off[o]; t < P.pi_off[o + 1]; ++t) v += P.pi_el[t] * sP[P.pi_q[t]];
+        sS[o] = v;
+        nrm2 += (double)v * (double)v;
+      }
+    }
+    double *out = soap_out + (size_t)site * P.n_soap;
+    // accumulate: the caller's soap row is added before the norm is taken, as
+    // the reference adds the compressed descriptor into soap (:798-802).  Each
+    // thread reads and writes the same components of the row.
+    const bool acc = (keep & 2) != 0;
+    if (acc) {
+      nrm2 = 0.0;
+      for (int o = tid; o < P.n_soap; o += NT) {
+        const double v = (double)sS[o] + out[o];
+        nrm2 += v * v;
+      }
+    }
+    nrm2 = block_sum<NT>(nrm2, sRed);  // (:805-809)
+    double norm = sqrt(nrm2);
+    if (norm < 1.0e-5) norm = 1.0;
+    const double inv = 1.0 / norm;
+    if (acc)
+      for (int o = tid; o < P.n_soap; o += NT) out[o] = ((double)sS[o] + out[o]) * inv;
+    else
+      for (int o = tid; o < P.n_soap; o += NT) out[o] = (double)sS[o] * inv;
+    if (keep & 1) {
+      float *kc = keep_c + (size_t)site * keep_stride(P);
+      const int n4 = (2 * n_max * KS) / 4;
+      for (int t = tid; t < n4; t += NT) ((float4 *)kc)[t] = ((const float4 *)sC)[t];
+      for (int t = 4 * n4 + tid; t < 2 * n_max * KS; t += NT) kc[t] = sC[t];
+      if (tid == 0) keep_norm[site] = norm;
+    }
+}
+
 // ------------------------------------------------------------ descriptor
 template <int NT, int AMAX, int LC>
 __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, const DevBatch B,
@@ -711,77 +795,254 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
     for (int t = tid; t < 2 * n_max * KS; t += NT) sC[t] = (float)sC64[t];
     __syncthreads();
 
-    // ---- C. power spectrum of the kept components (src/soap_turbo.f90:750-795)
-    float *pout = P.cmap_identity ? sS : sP;
-    double nrm2 = 0.0;
-    if (P.ps_mt > 0) {
-      // on the tensor cores, then gathered into the kept components with the
-      // sqrt 2 of n != n'
-      float *sPl = (float *)(smem + Ly.Pl);
-      ps_tensor<NT>(P, sC, sPl, (const int *)SBLOB(off_psj));
-      __syncthreads();
-      const int *kpos = (const int *)SBLOB(off_kpos);
-      for (int q = tid; q < P.n_kept; q += NT) {
-        const int code = kpos[q];
-        const float v = (code < 0 ? 1.41421356237309504880f : 1.f) * sPl[code & 0x7fffffff];
-        pout[q] = v;
-        nrm2 += (double)v * (double)v;
-      }
-    } else
-    for (int q = tid; q < P.n_kept; q += NT) {
-      const int code = kept[q];
-      const int n = code & 0xff, np = (code >> 8) & 0xff, l = code >> 16;
-      const int kb = l * (l + 1) / 2;
-      const float *cn_r = sC + (size_t)n * KS + kb, *cn_i = sC + (size_t)(n_max + n) * KS + kb;
-      const float *cp_r = sC + (size_t)np * KS + kb, *cp_i = sC + (size_t)(n_max + np) * KS + kb;
-      const float acc0 = cn_r[0] * cp_r[0] + cn_i[0] * cp_i[0];
-      float acc = 0.f;
-      for (int m = 1; m <= l; ++m) acc += cn_r[m] * cp_r[m] + cn_i[m] * cp_i[m];
-      const float base = (n == np) ? 1.f : 1.41421356237309504880f;
-      const float v = base * (acc0 + 2.f * acc);
-      pout[q] = v;
-      nrm2 += (double)v * (double)v;
-    }
-    if (!P.cmap_identity) {
-      // compression through the map (:798-802)
-      __syncthreads();
-      nrm2 = 0.0;
-      for (int o = tid; o < P.n_soap; o += NT) {
-        float v = 0.f;
-        for (int t = P.pi_off[o]; t < P.pi_off[o + 1]; ++t) v += P.pi_el[t] * sP[P.pi_q[t]];
-        sS[o] = v;
-        nrm2 += (double)v * (double)v;
-      }
-    }
-    double *out = soap_out + (size_t)site * P.n_soap;
-    // accumulate: the caller's soap row is added before the norm is taken, as
-    // the reference adds the compressed descriptor into soap (:798-802).  Each
-    // thread reads and writes the same components of the row.
-    const bool acc = (keep & 2) != 0;
-    if (acc) {
-      nrm2 = 0.0;
-      for (int o = tid; o < P.n_soap; o += NT) {
-        const double v = (double)sS[o] + out[o];
-        nrm2 += v * v;
-      }
-    }
-    nrm2 = block_sum<NT>(nrm2, sRed);  // (:805-809)
-    double norm = sqrt(nrm2);
-    if (norm < 1.0e-5) norm = 1.0;
-    const double inv = 1.0 / norm;
-    if (acc)
-      for (int o = tid; o < P.n_soap; o += NT) out[o] = ((double)sS[o] + out[o]) * inv;
-    else
-      for (int o = tid; o < P.n_soap; o += NT) out[o] = (double)sS[o] * inv;
-    if (keep & 1) {
-      float *kc = keep_c + (size_t)site * keep_stride(P);
-      const int n4 = (2 * n_max * KS) / 4;
-      for (int t = tid; t < n4; t += NT) ((float4 *)kc)[t] = ((const float4 *)sC)[t];
-      for (int t = 4 * n4 + tid; t < 2 * n_max * KS; t += NT) kc[t] = sC[t];
-      if (tid == 0) keep_norm[site] = norm;
-    }
+    site_output<NT>(P, smem, sC, sP, sS, (float *)(smem + Ly.Pl), kept, sRed, site, soap_out, keep_c, keep_norm,
+                    keep);
     ahead_publish(sSite, nx, nx0, nx1);
   }
+}
+
+// ------------------------------------------------------------ descriptor on tensor cores
+// get_soap's c_nlm (src/soap_turbo.f90:619-664) as a tcgen05 product per site:
+// D[2 k + re/im][n] = sum_e A_e(k, re/im) R_e(n), with A_e(k) = u_k e^{-i m phi}
+// of entry e (u_k = (preflm_k P_k)(amp i_l), the same FP32 products as the
+// CUDA-core kernel) and R_e its species' 4 pi R_n (zero in the other species'
+// columns).  M = 128 rows (2 k_max <= 128), N = 32 columns (n_max <= 32), K =
+// the entries, 16 at a time (two K-steps of 3xTF32 MMAs); each group's FP32
+// partial sums are read from TMEM by the thread that owns the row and added to
+// its FP64 accumulators (fixed order, no atomics) -- the accuracy of the
+// CUDA-core kernel's FP32 groups flushed into FP64.  Then the poly3gauss
+// central term, and k_descriptor's power spectrum, norm and output.
+constexpr int kTdGroup = 16;   // entries per group (two K-steps)
+constexpr int kTdCols = 32;    // D columns (n)
+constexpr int kTdTmemCols = 32;
+
+struct TdLayout {
+  size_t red, ent, wcnt, misc, mbar, tmem, Ahi, Alo, Bhi, Blo, X, R, A, C, P, S, Pl, total;
+};
+__host__ __device__ inline TdLayout make_td_layout(const DevParams &P, int NT, int AMAX, int LC) {
+  TdLayout L{};
+  const size_t KS = (size_t)(P.k_max | 1), nsp = (size_t)P.n_species;
+  size_t o = site_blob_bytes(P, 0);
+  L.red = o;  o += 40 * sizeof(double);
+  L.ent = o;  o += (size_t)NT * nsp * sizeof(int);
+  L.wcnt = o; o += (size_t)SOAPB_MAX_SPECIES * (NT / 32) * sizeof(int);
+  L.misc = o; o += 64 * sizeof(int);
+  L.mbar = align_up(o, 8); o = L.mbar + 8;
+  L.tmem = o; o += 8;
+  o = align_up(o, 1024);
+  L.Ahi = o; o += 128 * kTdGroup * 4;
+  L.Alo = o; o += 128 * kTdGroup * 4;
+  L.Bhi = o; o += kTdCols * kTdGroup * 4;
+  L.Blo = o; o += kTdCols * kTdGroup * 4;
+  o = align_up(o, 16);
+  L.X = o;
+  size_t x = o;
+  L.R = x; x += kTdGroup * AMAX * sizeof(float);
+  L.A = x; x += kTdGroup * (size_t)stage_stride(LC, 0) * sizeof(float);
+  const size_t end_stage = x;
+  x = o;
+  L.C = x; x += 2 * (size_t)P.n_max * KS * sizeof(float);
+  L.P = x; x += (size_t)P.n_kept * sizeof(float);
+  L.S = x; x += (size_t)P.n_soap * sizeof(float);
+  if (P.ps_mt > 0) {
+    x = align_up(x, 16);
+    L.Pl = x; x += (size_t)(P.l_max + 1) * 16 * P.ps_mt * 8 * P.ps_nt * sizeof(float);
+  }
+  L.total = align_up(end_stage > x ? end_stage : x, 16);
+  return L;
+}
+
+template <int NT, int AMAX, int LC>
+__global__ void __launch_bounds__(NT) k_descriptor_tc(const DevParams P, const DevBatch B,
+                                                      double *__restrict__ soap_out, float *__restrict__ keep_c,
+                                                      double *__restrict__ keep_norm, int keep) {
+  static_assert(NT == 128, "one thread per TMEM lane");
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int AS = stage_stride(LC, 0);
+  const TdLayout Ly = make_td_layout(P, NT, AMAX, LC);
+  const int *klm = (const int *)SBLOB(off_klm);
+  const int *kept = (const int *)SBLOB(off_kept);
+  const double *central = (const double *)SBLOB(off_central);
+  double *sRed = (double *)(smem + Ly.red);
+  float *sR = (float *)(smem + Ly.R);
+  float *sA = (float *)(smem + Ly.A);
+  float *sC = (float *)(smem + Ly.C);
+  float *sP = (float *)(smem + Ly.P);
+  float *sS = (float *)(smem + Ly.S);
+  unsigned char *sAhi = smem + Ly.Ahi, *sAlo = smem + Ly.Alo, *sBhi = smem + Ly.Bhi, *sBlo = smem + Ly.Blo;
+  uint64_t *mbar = (uint64_t *)(smem + Ly.mbar);
+  uint32_t *tmem_slot = (uint32_t *)(smem + Ly.tmem);
+  int *sEnt = (int *)(smem + Ly.ent);
+  int *sW_cnt = (int *)(smem + Ly.wcnt);
+  int *sMisc = (int *)(smem + Ly.misc);
+  int *sBase = sMisc, *sCnt = sMisc + SOAPB_MAX_SPECIES, *sNent = sMisc + 2 * SOAPB_MAX_SPECIES;
+  int *sSite = sMisc + 3 * SOAPB_MAX_SPECIES;
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int KS = P.k_max | 1;
+  const int n_max = P.n_max, nsp = P.n_species, k_max = P.k_max;
+  const uint32_t idesc = tc::idesc_tf32(128, kTdCols);
+  // this thread's row of D: (k, re/im)
+  const int my_k = tid >> 1, my_ri = tid & 1;
+  const int my_l = my_k < k_max ? (klm[my_k] & 0xff) : 0, my_m = my_k < k_max ? (klm[my_k] >> 8) : 0;
+  // the species and local index of each D column n
+  copy_site_blob<NT>(P, smem, 0);
+  if (warp == 0) tc::tmem_alloc(tmem_slot, kTdTmemCols);
+  if (tid == 0) tc::mbar_init(mbar);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tmem_slot;
+  uint32_t phase = 0;
+  bool failed = false;
+  int col_s = -1, col_n = 0;  // (tid < 32) the species and local index of column tid
+  if (tid < kTdCols)
+    for (int s = 0; s < nsp; ++s) {
+      const RadSp &RS = rad_of(smem, P, s);
+      if (tid >= RS.nbeg && tid < RS.nbeg + RS.alpha) {
+        col_s = s;
+        col_n = tid - RS.nbeg;
+      }
+    }
+
+  first_site(B, B.ticket, sSite);
+  for (;;) {
+    const int site = sSite[0];
+    if (site >= B.site_hi || failed) break;
+    const int p_begin = sSite[1];
+    const int p_end = min(sSite[2], B.n_pairs);
+    int nx = 0, nx0 = 0, nx1 = 0;
+    if (tid == 0) nx = take_ticket(B, B.ticket);
+    double acc[kTdCols];
+#pragma unroll
+    for (int n = 0; n < kTdCols; ++n) acc[n] = 0.0;
+
+    for (int chunk = p_begin; chunk < p_end && !failed; chunk += NT) {
+      int slot[SOAPB_MAX_SPECIES];
+      unsigned my_bits;
+      double my_r;
+      const int n_ent = build_entries<NT>(P, B, p_begin, chunk, p_end, false, sEnt, sW_cnt, sBase, sCnt, sNent,
+                                          slot, my_bits, my_r);
+      for (int ebase = 0; ebase < n_ent; ebase += kTdGroup) {
+        const int n_g = min(kTdGroup, n_ent - ebase);
+        // ---- the group's rows (angular and radial) into shared memory
+        stage_entries<NT, AMAX, LC, false>(P, B, sEnt, chunk, ebase, n_g, sA, sR, nullptr);
+        __syncthreads();
+        // the central pair's entries carry central_weight (:638-646)
+        if (chunk == p_begin) {
+          for (int el = tid; el < n_g; el += NT) {
+            const int code = sEnt[ebase + el];
+            const double cw = rad_of(smem, P, code >> 24).cw;
+            if ((code & 0xffffff) == 0 && cw != 1.0)
+#pragma unroll
+              for (int n = 0; n < AMAX; ++n) sR[(size_t)el * AMAX + n] *= (float)cw;
+          }
+          __syncthreads();
+        }
+        // ---- A operand: row (k, re/im) of this thread, 16 entries
+        {
+          float v[kTdGroup];
+#pragma unroll
+          for (int e = 0; e < kTdGroup; ++e) {
+            v[e] = 0.f;
+            if (e < n_g && my_k < k_max) {
+              const float *Ae = sA + (size_t)e * AS;
+              // u_k = (preflm_k P_k)(amp i_l) (src/soap_turbo_angular.f90:590-594)
+              const float u = Ae[row_p(LC) + my_k] * Ae[row_il(LC) + my_l];
+              v[e] = u * Ae[(my_ri ? row_ei(LC) : row_er(LC)) + my_m];
+            }
+          }
+#pragma unroll
+          for (int e4 = 0; e4 < kTdGroup / 4; ++e4) {
+            uint4 h, lo;
+            tc::split(v[4 * e4], h.x, lo.x);
+            tc::split(v[4 * e4 + 1], h.y, lo.y);
+            tc::split(v[4 * e4 + 2], h.z, lo.z);
+            tc::split(v[4 * e4 + 3], h.w, lo.w);
+            const uint32_t off = tc::kmajor_off(tid, 4 * e4, kTdGroup);
+            *(uint4 *)(sAhi + off) = h;
+            *(uint4 *)(sAlo + off) = lo;
+          }
+        }
+        // ---- B operand: row n, the entries' R_n of their species (else 0)
+        if (tid < kTdCols) {
+          float v[kTdGroup];
+#pragma unroll
+          for (int e = 0; e < kTdGroup; ++e) {
+            v[e] = 0.f;
+            if (e < n_g && col_s >= 0 && (sEnt[ebase + e] >> 24) == col_s) v[e] = sR[(size_t)e * AMAX + col_n];
+          }
+#pragma unroll
+          for (int e4 = 0; e4 < kTdGroup / 4; ++e4) {
+            uint4 h, lo;
+            tc::split(v[4 * e4], h.x, lo.x);
+            tc::split(v[4 * e4 + 1], h.y, lo.y);
+            tc::split(v[4 * e4 + 2], h.z, lo.z);
+            tc::split(v[4 * e4 + 3], h.w, lo.w);
+            const uint32_t off = tc::kmajor_off(tid, 4 * e4, kTdGroup);
+            *(uint4 *)(sBhi + off) = h;
+            *(uint4 *)(sBlo + off) = lo;
+          }
+        }
+        tc::fence_proxy_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        if (tid == 0) {
+          const uint32_t ahi = tc::smem_addr(sAhi), alo = tc::smem_addr(sAlo);
+          const uint32_t bhi = tc::smem_addr(sBhi), blo = tc::smem_addr(sBlo);
+          for (int k0 = 0; k0 < kTdGroup; k0 += 8)
+            tc::mma3_step(tmem, ahi, alo, kTdGroup, bhi, blo, kTdGroup, k0, idesc, k0 > 0);
+          tc::commit(mbar);
+        }
+        const int ok = tc::mbar_wait(mbar, phase, tc::kMaxTries);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+          if (tid == 0) prep_error(B, kErrTc);
+          tc::mbar_wait(mbar, phase ^ 1u, tc::kMaxTries);
+          failed = true;
+          break;
+        }
+        tc::fence_after_sync();
+        // ---- the group's FP32 partial sums into the FP64 accumulators
+#pragma unroll
+        for (int j = 0; j < kTdCols / 16; ++j) {
+          float v[16];
+          tc::ld16(tc::taddr(tmem, 32 * warp, 16 * j), v);
+#pragma unroll
+          for (int q = 0; q < 16; ++q) acc[16 * j + q] += (double)v[q];
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+      }
+    }
+    if (failed) break;
+    ahead_bounds(B, nx, nx0, nx1);
+    // ---- poly3gauss central-atom term (src/soap_turbo.f90:646-662), row (k = 0, re)
+    if (P.basis == 1 && tid == 0) {
+      const int mult = B.species_mult[site];
+      for (int mm = 0; mm < mult; ++mm) {
+        const int s = B.species[(size_t)site * B.max_mult + mm] - 1;
+        if (s < 0 || s >= nsp) continue;
+        const RadSp &RS = rad_of(smem, P, s);
+#pragma unroll
+        for (int n = 0; n < kTdCols; ++n)
+          if (n >= RS.nbeg && n < RS.nbeg + RS.alpha) acc[n] += central[n];
+      }
+    }
+    // ---- c_nlm to FP32 in sC (re/im, n, KS); the padding column k_max stays 0
+    if (my_k < KS)
+#pragma unroll
+      for (int n = 0; n < kTdCols; ++n)
+        if (n < n_max) sC[(size_t)(my_ri * n_max + n) * KS + my_k] = my_k < k_max ? (float)acc[n] : 0.f;
+    __syncthreads();
+    site_output<NT>(P, smem, sC, sP, sS, (float *)(smem + Ly.Pl), kept, sRed, site, soap_out, keep_c, keep_norm,
+                    keep);
+    ahead_publish(sSite, nx, nx0, nx1);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, kTdTmemCols);
 }
 
 // ------------------------------------------------------------ contract
@@ -1085,6 +1346,403 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_contract(const DevParams P, co
   }
 }
 
+// ------------------------------------------------------------ contract on tensor cores
+// soap_contract (src/soap_turbo.f90:1723-1884) with the per-entry contraction
+// on the tensor cores.  Per site, as k_contract: Gp, Gu and H(k, n) on the CUDA
+// cores.  H becomes the B operand of a tcgen05 MMA, [96 columns c = 2k + re/im
+// (k < 48, beyond k_max zero) x KB = n_species * AMAX] (K-major, split into
+// TF32 head and tail).  The site's entries go in rounds of 64: the A operand
+// is [128 x KB], row e < 64 the entry's dR_n/dr and row 64 + e its R_n, each
+// in its species' AMAX columns (zero elsewhere), so that one 3xTF32 product
+// D = A B^T (9 MMAs of 128 x 96 x 8) gives every entry's
+//   U(k) = sum_n dR_n/dr H(k, n)  (rows < 64),   V(k) = sum_n R_n H(k, n)  (rows >= 64)
+// in TMEM (the reference's four dot products per n, src/soap_turbo.f90:
+// 1842-1866, reassociated over n).  Thread t < 64 then takes U of entry t and
+// forms u Re(e conj U); thread 64 + t takes V of entry t and forms the rest of
+// the radial, azimuthal and polar sums, each over k in a fixed order, from the
+// entry's angular row (read from global memory, where the descriptor's pair
+// kernel left it).  The per-pair rotation and the self pair are k_contract's.
+constexpr int kTcEntries = 64;   // entries per round
+constexpr int kTcCols = 96;      // U / V columns: 2 k + re/im for k < 48
+constexpr int kTcTmemCols = 128; // TMEM columns a CTA holds
+
+__host__ __device__ inline int tc_kb(const DevParams &P, int AMAX) { return (P.n_species * AMAX + 7) / 8 * 8; }
+
+struct TcLayout {
+  size_t red, ent, wcnt, misc, H, Rot, F, Fu, Bhi, Blo, X, Ahi, Alo, C, Gu, Gp, mbar, tmem, total;
+};
+__host__ __device__ inline TcLayout make_tc_layout(const DevParams &P, int NT, int AMAX) {
+  TcLayout L{};
+  const size_t KS = (size_t)(P.k_max | 1), nsp = (size_t)P.n_species, KB = (size_t)tc_kb(P, AMAX);
+  size_t o = site_blob_bytes(P, 1);
+  L.red = o;  o += 40 * sizeof(double);
+  L.ent = o;  o += (size_t)NT * nsp * sizeof(int);
+  L.wcnt = o; o += (size_t)SOAPB_MAX_SPECIES * (NT / 32) * sizeof(int);
+  L.misc = o; o += 64 * sizeof(int);
+  L.mbar = align_up(o, 8); o = L.mbar + 8;
+  L.tmem = o; o += 8;
+  o = align_up(o, 16);
+  L.H = o;   o += 2 * KS * (size_t)h_stride(P.n_species, AMAX) * sizeof(float);
+  L.Rot = o; o += (size_t)NT * 4 * sizeof(float);
+  L.F = o;   o += (size_t)NT * nsp * 3 * sizeof(float);
+  L.Fu = o;  o += (size_t)NT * nsp * sizeof(float);
+  o = align_up(o, 1024);
+  L.Bhi = o; o += (size_t)kTcCols * KB * 4;
+  L.Blo = o; o += (size_t)kTcCols * KB * 4;
+  o = align_up(o, 1024);
+  L.X = o;
+  // per round: the A tiles; per site (before H is built): c_nlm, Gu, Gp
+  size_t x = o;
+  L.Ahi = x; x += 128 * KB * 4;
+  L.Alo = x; x += 128 * KB * 4;
+  const size_t end_round = x;
+  x = o;
+  L.C = x;  x += 2 * (size_t)P.n_max * KS * sizeof(float);
+  L.Gu = x; x += (size_t)P.n_kept * sizeof(float);
+  L.Gp = x; x += (size_t)P.n_soap * sizeof(float);
+  L.total = align_up(end_round > x ? end_round : x, 16);
+  return L;
+}
+
+__host__ __device__ constexpr int tc_l_of(int kk) {
+  int l = 0;
+  while ((l + 1) * (l + 2) / 2 <= kk) ++l;
+  return l;
+}
+__host__ __device__ constexpr int tc_m_of(int kk) { return kk - tc_l_of(kk) * (tc_l_of(kk) + 1) / 2; }
+
+template <int NT, int AMAX, int LC>
+__global__ void __launch_bounds__(NT) k_contract_tc(const DevParams P, const DevBatch B,
+                                                    const double *__restrict__ soap_in,
+                                                    const double *__restrict__ G, int g_layout, double sgn,
+                                                    const float *__restrict__ keep_c,
+                                                    const double *__restrict__ keep_norm,
+                                                    double *__restrict__ pair_out) {
+  static_assert(NT == 128, "one thread per TMEM lane");
+  constexpr int KC = (LC + 1) * (LC + 2) / 2;
+  static_assert(KC <= 2 * kTcCols / 4 && 2 * KC <= kTcCols, "U/V columns");
+  constexpr int GPT = 8;
+  constexpr int AW = row_len(LC);
+  constexpr int O_IL = row_il(LC), O_ILD = row_ild(LC), O_ER = row_er(LC), O_EI = row_ei(LC),
+                O_SF = row_sf(LC), O_X = row_x(LC), O_SQ = row_sq(LC), O_P = row_p(LC);
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const TcLayout Ly = make_tc_layout(P, NT, AMAX);
+  const float4 *kcoef = (const float4 *)SBLOBC(off_kcoef);
+  const int *nmap = (const int *)SBLOBC(off_nmap);
+  const int *hitem = (const int *)SBLOBC(off_hitem);
+  const int *hloff = (const int *)SBLOBC(off_hloff);
+  const int *hl = P.hl_in_blob ? (const int *)SBLOBC(off_hl) : P.hl_packed;
+  double *sRed = (double *)(smem + Ly.red);
+  float *sH = (float *)(smem + Ly.H);
+  float *sRot = (float *)(smem + Ly.Rot);
+  float *sF = (float *)(smem + Ly.F);
+  float *sFu = (float *)(smem + Ly.Fu);
+  float *sC = (float *)(smem + Ly.C);
+  float *sGu = (float *)(smem + Ly.Gu);
+  float *sGp = (float *)(smem + Ly.Gp);
+  unsigned char *sAhi = smem + Ly.Ahi, *sAlo = smem + Ly.Alo, *sBhi = smem + Ly.Bhi, *sBlo = smem + Ly.Blo;
+  uint64_t *mbar = (uint64_t *)(smem + Ly.mbar);
+  uint32_t *tmem_slot = (uint32_t *)(smem + Ly.tmem);
+  int *sEnt = (int *)(smem + Ly.ent);
+  int *sW_cnt = (int *)(smem + Ly.wcnt);
+  int *sMisc = (int *)(smem + Ly.misc);
+  int *sBase = sMisc, *sCnt = sMisc + SOAPB_MAX_SPECIES, *sNent = sMisc + 2 * SOAPB_MAX_SPECIES;
+  int *sSite = sMisc + 3 * SOAPB_MAX_SPECIES;
+  int *sFail = sMisc + 3 * SOAPB_MAX_SPECIES + 4;
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int KS = P.k_max | 1;
+  const int HS = h_stride(P.n_species, AMAX);
+  const size_t HPL = (size_t)KS * HS;
+  const int n_max = P.n_max, k_max = P.k_max, n_soap = P.n_soap, nsp = P.n_species;
+  const int n_sites = B.n_sites;
+  const int KB = tc_kb(P, AMAX);
+  const uint32_t idesc = tc::idesc_tf32(128, kTcCols);
+  float *sGu_eff = P.cmap_identity ? sGp : sGu;
+
+  copy_site_blob<NT>(P, smem, 1);
+  for (int t = tid; t < 2 * (int)HPL; t += NT) sH[t] = 0.f;  // entries no item writes stay 0
+  if (warp == 0) tc::tmem_alloc(tmem_slot, kTcTmemCols);
+  if (tid == 0) {
+    tc::mbar_init(mbar);
+    *sFail = 0;
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tmem_slot;
+  uint32_t phase = 0;
+  bool failed = false;
+
+  first_site(B, B.ticket + 1, sSite);
+  for (;;) {
+    const int site = sSite[0];
+    if (site >= B.site_hi || failed) break;
+    const int p_begin = sSite[1];
+    const int p_end = min(sSite[2], B.n_pairs);
+    int nx = 0, nx0 = 0, nx1 = 0;
+    if (tid == 0) nx = take_ticket(B, B.ticket + 1);
+    // ---- per-site loads, Gp, Gu and H, as k_contract (:1783-1835)
+    const double knorm = keep_norm[site];
+    const double *q = soap_in + (size_t)site * n_soap;
+    double gv[GPT], qv[GPT];
+#pragma unroll
+    for (int j = 0; j < GPT; ++j) {
+      const int o = tid + j * NT;
+      gv[j] = qv[j] = 0.0;
+      if (o < n_soap) {
+        gv[j] = g_layout == 0 ? G[(size_t)o * n_sites + site] : G[(size_t)site * n_soap + o];
+        qv[j] = q[o];
+      }
+    }
+    {
+      const float *kc = keep_c + (size_t)site * keep_stride(P);
+      const int n4 = (2 * n_max * KS) / 4;
+      for (int t = tid; t < n4; t += NT) cp_async16(sC + 4 * t, kc + 4 * t);
+      for (int t = 4 * n4 + tid; t < 2 * n_max * KS; t += NT) sC[t] = kc[t];
+      cp_async_wait_all();
+    }
+    double qg = 0.0;
+#pragma unroll
+    for (int j = 0; j < GPT; ++j) qg += qv[j] * gv[j];
+    for (int o = tid + GPT * NT; o < n_soap; o += NT) {
+      const double g = g_layout == 0 ? G[(size_t)o * n_sites + site] : G[(size_t)site * n_soap + o];
+      sGp[o] = (float)g;
+      qg += q[o] * g;
+    }
+    qg = block_sum<NT>(qg, sRed);
+    const double inv = 1.0 / knorm;
+#pragma unroll
+    for (int j = 0; j < GPT; ++j) {
+      const int o = tid + j * NT;
+      if (o < n_soap) sGp[o] = (float)((gv[j] - qv[j] * qg) * inv);
+    }
+    for (int o = tid + GPT * NT; o < n_soap; o += NT) sGp[o] = (float)(((double)sGp[o] - q[o] * qg) * inv);
+    __syncthreads();
+    if (!P.cmap_identity) {
+      for (int t = tid; t < P.n_kept; t += NT) {
+        float v = 0.f;
+        for (int e = P.pj_off[t]; e < P.pj_off[t + 1]; ++e) v += P.pj_el[e] * sGp[P.pj_o[e]];
+        sGu[t] = v;
+      }
+      __syncthreads();
+    }
+    for (int it = tid; it < P.n_hitem; it += NT) {
+      const int code = hitem[it];
+      const int n = code & 0xff, l = (code >> 8) & 0xff, m0 = code >> 16;
+      const int kb = l * (l + 1) / 2 + m0, mn = min(kHM, l + 1 - m0);
+      float hr[kHM], hi[kHM];
+#pragma unroll
+      for (int j = 0; j < kHM; ++j) hr[j] = hi[j] = 0.f;
+      const int li = l * n_max + n;
+      for (int t = hloff[li]; t < hloff[li + 1]; ++t) {
+        const int e = hl[t];
+        const int np = e & 0xff, qq = (e >> 8) & 0xffff;
+        const float y = ((e >> 31) ? 2.f : 1.41421356237309504880f) * sGu_eff[qq];
+        const float *cr = sC + (size_t)np * KS + kb;
+        const float *ci = cr + (size_t)n_max * KS;
+#pragma unroll
+        for (int j = 0; j < kHM; ++j) {
+          if (j < mn) {
+            hr[j] = fmaf(y, cr[j], hr[j]);
+            hi[j] = fmaf(y, ci[j], hi[j]);
+          }
+        }
+      }
+      const int nm = nmap[n];
+      const int col = (nm & 0xff) * AMAX + (nm >> 8);
+#pragma unroll
+      for (int j = 0; j < kHM; ++j) {
+        if (j < mn) {
+          const float w = (m0 + j == 0) ? 1.f : 2.f;
+          sH[(size_t)(kb + j) * HS + col] = w * hr[j];
+          sH[HPL + (size_t)(kb + j) * HS + col] = w * hi[j];
+        }
+      }
+    }
+    __syncthreads();
+    // ---- the B operand: H as [96 x KB], column c = 2 k + (re, im)
+    for (int t = tid; t < kTcCols * KB; t += NT) {
+      const int c = t / KB, kk = t - c * KB, k = c >> 1;
+      const float v = (k < k_max && kk < nsp * AMAX) ? sH[(c & 1) * HPL + (size_t)k * HS + kk] : 0.f;
+      uint32_t h, lo;
+      tc::split(v, h, lo);
+      const uint32_t off = tc::kmajor_off(c, kk, KB);
+      *(uint32_t *)(sBhi + off) = h;
+      *(uint32_t *)(sBlo + off) = lo;
+    }
+    ahead_bounds(B, nx, nx0, nx1);
+    double self_x = 0.0, self_y = 0.0, self_z = 0.0;
+
+    for (int chunk = p_begin; chunk < p_end; chunk += NT) {
+      int slot[SOAPB_MAX_SPECIES];
+      unsigned my_bits;
+      double my_r;
+      // (its barriers also order the B tiles' stores before the first round)
+      const int n_ent = build_entries<NT>(P, B, p_begin, chunk, p_end, true, sEnt, sW_cnt, sBase, sCnt, sNent,
+                                          slot, my_bits, my_r);
+      for (int ebase = 0; ebase < n_ent && !failed; ebase += kTcEntries) {
+        const int n_round = min(kTcEntries, n_ent - ebase);
+        // ---- A operand: rows e < 64 dR/dr, rows 64 + e R, in the species' columns
+        for (int t = tid; t < 128 * KB; t += NT) {
+          const int r = t / KB, kk = t - r * KB, e = r & (kTcEntries - 1);
+          float v = 0.f;
+          if (e < n_round) {
+            const int code = sEnt[ebase + e];
+            const int s = code >> 24;
+            const int n = kk - s * AMAX;
+            if (n >= 0 && n < AMAX) {
+              const int k = chunk + (code & 0xffffff);
+              v = B.rad[((size_t)k * nsp + s) * 2 * AMAX + (r < kTcEntries ? AMAX : 0) + n];
+            }
+          }
+          uint32_t h, lo;
+          tc::split(v, h, lo);
+          const uint32_t off = tc::kmajor_off(r, kk, KB);
+          *(uint32_t *)(sAhi + off) = h;
+          *(uint32_t *)(sAlo + off) = lo;
+        }
+        tc::fence_proxy_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        if (tid == 0) {
+          const uint32_t ahi = tc::smem_addr(sAhi), alo = tc::smem_addr(sAlo);
+          const uint32_t bhi = tc::smem_addr(sBhi), blo = tc::smem_addr(sBlo);
+          for (int k0 = 0; k0 < KB; k0 += 8) tc::mma3_step(tmem, ahi, alo, KB, bhi, blo, KB, k0, idesc, k0 > 0);
+          tc::commit(mbar);
+        }
+        const int ok = tc::mbar_wait(mbar, phase, tc::kMaxTries);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+          // give up: report, and make sure the MMAs are no longer running
+          // before the TMEM is freed
+          if (tid == 0) {
+            prep_error(B, kErrTc);
+            *sFail = 1;
+          }
+          tc::mbar_wait(mbar, phase ^ 1u, tc::kMaxTries);
+          failed = true;
+          break;
+        }
+        tc::fence_after_sync();
+        // ---- epilogue: thread tid reads TMEM lane tid
+        const bool vrole = tid >= kTcEntries;
+        const int e = tid & (kTcEntries - 1);
+        const bool act = e < n_round;
+        const int code = act ? sEnt[ebase + e] : 0;
+        const float *Ae = B.ang + (size_t)(chunk + (code & 0xffffff)) * AW;
+        float il[LC + 1], ild[LC + 1], er[LC + 1], ei[LC + 1], sfac = 0.f;
+#pragma unroll
+        for (int l = 0; l <= LC; ++l) {
+          il[l] = act ? __ldg(Ae + O_IL + l) : 0.f;
+          er[l] = act ? __ldg(Ae + O_ER + l) : 0.f;
+          ei[l] = act ? __ldg(Ae + O_EI + l) : 0.f;
+          ild[l] = (act && vrole) ? __ldg(Ae + O_ILD + l) : 0.f;
+        }
+        if (act && vrole) sfac = __ldg(Ae + O_SF);
+        float f_rad = 0.f, f_azi = 0.f, f_pol = 0.f;
+        const float *Pe = Ae + O_P;
+#pragma unroll
+        for (int j = 0; j < (2 * KC + 15) / 16; ++j) {
+          float v[16];
+          tc::ld16(tc::taddr(tmem, 32 * warp, 16 * j), v);
+#pragma unroll
+          for (int qq = 0; qq < 8; ++qq) {
+            const int kk = 8 * j + qq;
+            if (kk >= KC) break;
+            const int l = tc_l_of(kk), m = tc_m_of(kk);
+            if (!act || l > P.l_max) continue;
+            const float xr = v[2 * qq], xi = v[2 * qq + 1];
+            const float Pk = __ldg(Pe + kk);
+            const float u = Pk * il[l];
+            if (!vrole) {
+              f_rad = fmaf(u, er[m] * xr + ei[m] * xi, f_rad);
+            } else {
+              const float4 cf = kcoef[kk];
+              // the derivative forms' P_l^m indices (src/soap_turbo_angular.f90:194-246)
+              const int ixx = (m == 0) ? (l > 0 ? l * (l + 1) / 2 + 1 : kk) : kk - 1;
+              const int ixy = (m == 0) ? (l > 0 ? l * (l + 1) / 2 + 1 : kk) : (m != l ? kk + 1 : kk);
+              const int ixz = (m == 0) ? kk : (l + 1) * (l + 2) / 2 + m - 1;
+              const int ixw = (m == 0) ? kk : (l + 1) * (l + 2) / 2 + m + 1;
+              const float dms = cf.x * __ldg(Pe + ixx) + cf.y * __ldg(Pe + ixy);
+              const float dvs = cf.z * __ldg(Pe + ixz) + cf.w * __ldg(Pe + ixw);
+              const float ur = Pk * ild[l] - sfac * u;
+              const float ua = dvs * il[l];
+              const float up = dms * il[l];
+              const float reV = er[m] * xr + ei[m] * xi;
+              const float imV = ei[m] * xr - er[m] * xi;
+              f_rad = fmaf(ur, reV, f_rad);
+              f_azi = fmaf(-ua, imV, f_azi);
+              f_pol = fmaf(up, reV, f_pol);
+            }
+          }
+        }
+        if (act) {
+          if (vrole) {
+            float *Fe = sF + (size_t)(ebase + e) * 3;
+            Fe[0] = f_rad;
+            Fe[1] = f_azi;
+            Fe[2] = f_pol;
+            // the rotation to Cartesian uses the same angles (:1867-1871)
+            float *rot = sRot + 4 * (code & 0xffffff);
+            rot[0] = __ldg(Ae + O_X);
+            rot[1] = __ldg(Ae + O_SQ);
+            rot[2] = er[1];
+            rot[3] = -ei[1];
+          } else {
+            sFu[ebase + e] = f_rad;
+          }
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+      }
+      if (failed) break;
+      // ---- per pair: sum its entries, rotate to Cartesian (:1864-1875)
+      const int k = chunk + tid;
+      if (k < p_end && k > p_begin) {
+        double px = 0.0, py = 0.0, pz = 0.0;
+        if (my_bits != 0u) {
+          double fr = 0.0, fa = 0.0, fp = 0.0;
+#pragma unroll
+          for (int s = 0; s < SOAPB_MAX_SPECIES; ++s) {
+            if (s < nsp && slot[s] >= 0) {
+              fr += (double)(sF[3 * slot[s] + 0] + sFu[slot[s]]);
+              fa += sF[3 * slot[s] + 1];
+              fp += sF[3 * slot[s] + 2];
+            }
+          }
+          const float *rot = sRot + 4 * tid;
+          const double ct = rot[0], st = rot[1], cf = rot[2], sf = rot[3];
+          const double ir = 1.0 / my_r;
+          px = sgn * (st * cf * fr - ct * cf * ir * fp - sf * ir * fa);
+          py = sgn * (st * sf * fr - ct * sf * ir * fp + cf * ir * fa);
+          pz = sgn * (ct * fr + st * ir * fp);
+        }
+        double *po = pair_out + (size_t)3 * k;
+        po[0] = px;
+        po[1] = py;
+        po[2] = pz;
+        self_x -= px;
+        self_y -= py;
+        self_z -= pz;
+      }
+    }
+    if (failed) break;
+    block_sum3<NT>(self_x, self_y, self_z, sRed);
+    if (tid == 0 && p_end > p_begin) {
+      double *po = pair_out + (size_t)3 * p_begin;
+      po[0] = self_x;
+      po[1] = self_y;
+      po[2] = self_z;
+    }
+    ahead_publish(sSite, nx, nx0, nx1);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, kTcTmemCols);
+}
+
 // ------------------------------------------------------------ launchers
 template <typename K>
 static int persistent_grid(K kernel, int threads, size_t smem, int n_sites, int max_ctas) {
@@ -1097,9 +1755,34 @@ static int persistent_grid(K kernel, int threads, size_t smem, int n_sites, int 
   return g < n_sites ? g : n_sites;
 }
 
+// The tensor-core descriptor: definitions with alpha <= 8, l_max <= 8 and n_max
+// <= 32 (the D tile's 32 columns).
+bool descriptor_tc_fits(const DevParams &P) { return P.tc_descriptor && P.amax_t == 8 && P.n_max <= kTdCols; }
+size_t descriptor_tc_smem(const DevParams &P) { return make_td_layout(P, 128, 8, 8).total; }
+
+static cudaError_t run_descriptor_tc(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg, double *soap,
+                                     float *keep_c, double *keep_norm, int keep) {
+  const size_t sm = descriptor_tc_smem(P);
+  auto kern = k_descriptor_tc<128, 8, 8>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  if (B.site_hi > B.site_lo) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int cap = sms * (512 / kTdTmemCols);
+    const int grid = persistent_grid(kern, 128, sm, B.site_hi - B.site_lo,
+                                     cfg.max_ctas > 0 ? (cfg.max_ctas < cap ? cfg.max_ctas : cap) : cap);
+    kern<<<grid, 128, sm, cfg.stream>>>(P, B, soap, keep_c, keep_norm, keep);
+  }
+  return cudaGetLastError();
+}
+
 template <int NT, int AMAX, int LC>
 static cudaError_t run_descriptor(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
                                   double *soap, float *keep_c, double *keep_norm, int keep) {
+  if (AMAX == 8 && LC == 8 && descriptor_tc_fits(P))
+    return run_descriptor_tc(P, B, cfg, soap, keep_c, keep_norm, keep);
   const size_t sm = make_layout(P, NT, AMAX, LC, 0).total;
   auto kern = k_descriptor<NT, AMAX, LC>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -1111,10 +1794,36 @@ static cudaError_t run_descriptor(const DevParams &P, const DevBatch &B, const L
   return cudaGetLastError();
 }
 
+// The tensor-core contract for the alpha <= 8, l_max <= 8 instantiation: a
+// persistent grid of at most 4 CTAs per SM, so that the CTAs resident on an SM
+// never ask for more than its 512 TMEM columns.
+size_t contract_tc_smem(const DevParams &P) { return make_tc_layout(P, 128, 8).total; }
+
+static cudaError_t run_contract_tc(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
+                                   const double *soap, const double *G, int g_layout, double sgn,
+                                   const float *keep_c, const double *keep_norm, double *pair) {
+  const size_t sm = contract_tc_smem(P);
+  auto kern = k_contract_tc<128, 8, 8>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  if (B.site_hi > B.site_lo) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int cap = sms * (512 / kTcTmemCols);
+    const int grid = persistent_grid(kern, 128, sm, B.site_hi - B.site_lo,
+                                     cfg.max_ctas > 0 ? (cfg.max_ctas < cap ? cfg.max_ctas : cap) : cap);
+    kern<<<grid, 128, sm, cfg.stream>>>(P, B, soap, G, g_layout, sgn, keep_c, keep_norm, pair);
+  }
+  return cudaGetLastError();
+}
+
 template <int NT, int AMAX, int LC>
 static cudaError_t run_contract(const DevParams &P, const DevBatch &B, const LaunchCfg &cfg,
                                 const double *soap, const double *G, int g_layout, double sgn,
                                 const float *keep_c, const double *keep_norm, double *pair) {
+  if (AMAX == 8 && LC == 8 && P.tc_contract)
+    return run_contract_tc(P, B, cfg, soap, G, g_layout, sgn, keep_c, keep_norm, pair);
   const size_t sm = make_layout(P, NT, AMAX, LC, 1).total;
   auto kern = k_contract<NT, AMAX, LC>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

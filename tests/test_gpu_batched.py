@@ -33,10 +33,12 @@ def batched():
     return Batched(syn.config(3, seed=29, scale=1 / 32))
 
 
-@pytest.mark.parametrize("threads", [64, 128, 256])
-def test_every_cta_size_matches_the_oracle(batched, threads):
+@pytest.mark.parametrize("tensor_cores,threads", [(True, 128), (False, 64), (False, 128), (False, 256)])
+def test_every_cta_size_matches_the_oracle(batched, tensor_cores, threads):
+    # the tensor-core kernels have one CTA size; the CUDA-core ones three
     c = batched.ctx
     c.set_threads_per_site(threads)
+    c.set_tensor_cores(tensor_cores)
     try:
         soap = c.descriptor(batched.b)
         pair = c.contract(batched.b, soap, batched.Gt)
@@ -48,13 +50,15 @@ def test_every_cta_size_matches_the_oracle(batched, threads):
         assert torch.equal(soap, soap2) and torch.equal(pair, pair2)
     finally:
         c.set_threads_per_site(0)
+        c.set_tensor_cores(True)
 
 
 def test_autotuner_choice_is_valid_and_used(batched):
     c = batched.ctx
     choice = c.autotune(batched.b)
-    assert choice["descriptor_threads"] in (64, 128, 256)
-    assert choice["contract_threads"] in (64, 128, 256)
+    # 0: the tensor-core kernel
+    assert choice["descriptor_threads"] in (0, 64, 128, 256)
+    assert choice["contract_threads"] in (0, 64, 128, 256)
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     for k in ("descriptor_max_ctas", "contract_max_ctas"):
         assert choice[k] in (0, sms, 2 * sms)
