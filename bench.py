@@ -56,12 +56,16 @@ def parse():
     ap.add_argument("--neighbors", action="store_true",
                     help="time the device neighbour-list builder instead")
     ap.add_argument("--scale", type=float, default=1.0,
-                    help="(--hessian) scale the structure's atom count, for profiler captures")
+                    help="(--hessian, --quick, --fp64) scale the structure's atom count, for profiler "
+                         "captures")
     ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5],
                     help="synthetic configuration of our arm (default 2, the headline workload)")
     ap.add_argument("--quick", action="store_true",
                     help="time the two kernels only (no FP64 path, e2e, CPU baseline or peak "
                          "measurement); for profiling runs")
+    ap.add_argument("--tensor-cores", default="default", choices=["default", "on", "off"],
+                    help="the site kernels' contractions on the tensor cores (on), on the CUDA cores "
+                         "(off), or the library's default")
     ap.add_argument("--fp64", action="store_true",
                     help="time the plain FP64 form alone (materialised soap_cart_der, then "
                          "contracted) on the configuration; for profiling runs")
@@ -78,9 +82,9 @@ CONFIG_NAMES = {
 }
 
 
-def workload(rank, seed, idx=2):
+def workload(rank, seed, idx=2, scale=1.0):
     from soap_turbo_b200 import synthetic as syn
-    return syn.config(idx, seed=seed + 7919 * rank)
+    return syn.config(idx, seed=seed + 7919 * rank, scale=scale)
 
 
 def cpu_model():
@@ -311,10 +315,15 @@ def run_ours(args):
     from soap_turbo_b200.context import Context
 
     dev = torch.device("cuda", torch.cuda.current_device())
-    w = workload(rank, args.seed, args.config)
+    # a reduced structure only for profiler captures (--quick); timed lines use the full size
+    w = workload(rank, args.seed, args.config, args.scale if args.quick else 1.0)
     wname = WORKLOAD if args.config == 2 else CONFIG_NAMES[args.config]
+    if args.quick and args.scale != 1.0:
+        wname += f", atoms scaled by {args.scale}"
     nl = w.nl
     ctx = Context(w.hyper)
+    if args.tensor_cores != "default":
+        ctx.set_tensor_cores(args.tensor_cores == "on")
     b = ctx.batch(nl)
     rng = np.random.default_rng(args.seed + rank)
     G_host = rng.standard_normal((ctx.n_soap, nl.n_sites))  # Fortran G(n_sites, n_soap)
@@ -825,7 +834,7 @@ def run_fp64(args):
     from soap_turbo_b200.context import Context
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
-    w = workload(0, args.seed, args.config)
+    w = workload(0, args.seed, args.config, args.scale)
     nl = w.nl
     ctx = Context(w.hyper)
     b = ctx.batch(nl)

@@ -882,20 +882,19 @@ __global__ void __launch_bounds__(NT) k_descriptor_tc(const DevParams P, const D
   const int KS = P.k_max | 1;
   const int n_max = P.n_max, nsp = P.n_species, k_max = P.k_max;
   const uint32_t idesc = tc::idesc_tf32(128, kTdCols);
-  // this thread's row of D: (k, re/im)
-  const int my_k = tid >> 1, my_ri = tid & 1;
-  const int my_l = my_k < k_max ? (klm[my_k] & 0xff) : 0, my_m = my_k < k_max ? (klm[my_k] >> 8) : 0;
-  // the species and local index of each D column n
   copy_site_blob<NT>(P, smem, 0);
   if (warp == 0) tc::tmem_alloc(tmem_slot, kTdTmemCols);
   if (tid == 0) tc::mbar_init(mbar);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
+  // this thread's row of D: (k, re/im)
+  const int my_k = tid >> 1, my_ri = tid & 1;
+  const int my_l = my_k < k_max ? (klm[my_k] & 0xff) : 0, my_m = my_k < k_max ? (klm[my_k] >> 8) : 0;
   const uint32_t tmem = *tmem_slot;
   uint32_t phase = 0;
   bool failed = false;
-  int col_s = -1, col_n = 0;  // (tid < 32) the species and local index of column tid
+  int col_s = -1, col_n = 0;  // (tid < 32) the species and local index of D column tid
   if (tid < kTdCols)
     for (int s = 0; s < nsp; ++s) {
       const RadSp &RS = rad_of(smem, P, s);
