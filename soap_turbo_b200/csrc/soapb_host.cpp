@@ -837,6 +837,43 @@ int build_tables(soapb_context *c) {
       if ((size_t)(L + 1) * MR * JP * sizeof(float) > 65536) P.ps_mt = P.ps_nt = 0;
       P.off_psj = put(J.data(), J.size() * 4);
       P.off_kpos = put(kpos.data(), kpos.size() * 4);
+      // the tcgen05 form's l groups: as many consecutive l per group as fit in
+      // 128 rows (l, n), 128 B rows (l, J) and K <= 32 columns (each l's block
+      // 2(l+1) wide, rounded up to 4)
+      const int nJ = (int)std::count_if(J.begin(), J.end(), [](int v) { return v >= 0; });
+      P.ps_nj = nJ;
+      P.ps_ng = 0;
+      std::vector<int> psrow;
+      constexpr int kPsTcK = 32;
+      bool ok = P.ps_mt > 0 && nJ > 0;
+      for (int l = 0; ok && l <= L;) {
+        const int g = P.ps_ng, l0 = l;
+        int k = 0, cnt = 0;
+        while (l <= L) {
+          const int w = (2 * (l + 1) + 3) / 4 * 4;
+          if ((k + w + 7) / 8 * 8 > kPsTcK || (cnt + 1) * N > 128 || (cnt + 1) * nJ > 128) break;
+          P.ps_ko[l] = k;
+          k += w;
+          ++cnt;
+          ++l;
+        }
+        if (cnt == 0) {
+          ok = false;
+          break;
+        }
+        P.ps_gk[g] = (k + 7) / 8 * 8;
+        P.ps_gnb[g] = std::max(16, (cnt * nJ + 15) / 16 * 16);
+        P.ps_grows[g] = cnt * N;
+        P.ps_grow[g] = (int)psrow.size();
+        for (int li = l0; li < l0 + cnt; ++li)  // the J rows first, so that B is the tile's head
+          for (int jc = 0; jc < nJ; ++jc) psrow.push_back(J[jc] | (li << 8) | (((li - l0) * nJ) << 16));
+        for (int li = l0; li < l0 + cnt; ++li)
+          for (int n = 0; n < N; ++n)
+            if (jpos[n] < 0) psrow.push_back(n | (li << 8) | (((li - l0) * nJ) << 16));
+        ++P.ps_ng;
+      }
+      if (!ok) P.ps_ng = 0;
+      P.off_psrow = put(psrow.data(), psrow.size() * 4);
     }
     // one-to-one compression: output q is kept component q with weight 1
     bool ident = (ns == nk) && (nz == nk);

@@ -116,6 +116,16 @@ struct DevParams {
   // power spectrum on the tensor cores: P_l[n, J] for rows n (ps_mt tiles of
   // 16) and the column set J (ps_nt tiles of 8) that covers every kept (n, n')
   int ps_mt, ps_nt;
+  // ... with tcgen05 (k_descriptor_tc): the l values in ps_ng groups; group g
+  // stacks rows (l, n) for its l, the J rows first, into one M = 128 tile of
+  // K = ps_gk[g] columns (l's block at ps_ko[l], 2(l+1) wide); B is the tile's
+  // first ps_gnb[g] rows.  Row r of group g is described by the blob's
+  // off_psrow table at ps_grow[g] + r: n | l << 8 | (D column of its P_l[n, J_0]) << 16.
+  int ps_ng;              // 0: the mma.sync form
+  int ps_nj;              // |J|
+  int ps_gk[SOAPB_MAX_LMAX + 1], ps_gnb[SOAPB_MAX_LMAX + 1], ps_grows[SOAPB_MAX_LMAX + 1];
+  int ps_grow[SOAPB_MAX_LMAX + 1], ps_ko[SOAPB_MAX_LMAX + 1];
+  int off_psrow;          // (blob) the row tables of all groups
   int off_psj;            // (blob) 8 ps_nt int: the radial index of each column (-1 = padding)
   int off_kpos;           // (blob) n_kept int: tile position (l, row, column) | (n != n') << 31
 };

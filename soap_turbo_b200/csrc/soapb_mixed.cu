@@ -579,11 +579,12 @@ __device__ __forceinline__ void ps_tensor(const DevParams &P, const float *sC, f
 // compression, the norm and the normalised FP64 output (:798-809, 904-909),
 // and with keep the c_nlm and norm the contract reads.  keep: bit 0 keeps, bit
 // 1 accumulates into soap_out.  sPl: the tensor-core tile buffer (ps_mt > 0).
+// ps_ready: sPl already holds the power-spectrum tiles (the tcgen05 form).
 template <int NT>
 __device__ __forceinline__ void site_output(const DevParams &P, unsigned char *smem, const float *sC, float *sP,
                                             float *sS, float *sPl, const int *kept, double *sRed, int site,
                                             double *__restrict__ soap_out, float *__restrict__ keep_c,
-                                            double *__restrict__ keep_norm, int keep) {
+                                            double *__restrict__ keep_norm, int keep, bool ps_ready = false) {
   const int tid = threadIdx.x;
   const int KS = P.k_max | 1;
   const int n_max = P.n_max;
@@ -593,8 +594,10 @@ __device__ __forceinline__ void site_output(const DevParams &P, unsigned char *s
     if (P.ps_mt > 0) {
       // on the tensor cores, then gathered into the kept components with the
       // sqrt 2 of n != n'
-      ps_tensor<NT>(P, sC, sPl, (const int *)SBLOB(off_psj));
-      __syncthreads();
+      if (!ps_ready) {
+        ps_tensor<NT>(P, sC, sPl, (const int *)SBLOB(off_psj));
+        __syncthreads();
+      }
       const int *kpos = (const int *)SBLOB(off_kpos);
       for (int q = tid; q < P.n_kept; q += NT) {
         const int code = kpos[q];
@@ -814,11 +817,12 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
 // central term, and k_descriptor's power spectrum, norm and output.
 constexpr int kTdGroup = 16;   // entries per group (two K-steps)
 constexpr int kTdCols = 32;    // D columns (n)
-constexpr int kTdTmemCols = 32;
+constexpr int kTdTmemCols = 128;  // c_nlm's 32 columns, then the power spectrum's up to 128
 
 struct TdLayout {
-  size_t red, ent, wcnt, misc, mbar, tmem, Ahi, Alo, Bhi, Blo, X, R, A, C, P, S, Pl, total;
+  size_t red, ent, wcnt, misc, mbar, tmem, Ahi, Alo, Bhi, Blo, Phi, Plo, X, R, A, C, P, S, Pl, total;
 };
+constexpr int kPsTcK = 32;  // K columns of a power-spectrum tile (the host's groups agree)
 __host__ __device__ inline TdLayout make_td_layout(const DevParams &P, int NT, int AMAX, int LC) {
   TdLayout L{};
   const size_t KS = (size_t)(P.k_max | 1), nsp = (size_t)P.n_species;
@@ -830,10 +834,18 @@ __host__ __device__ inline TdLayout make_td_layout(const DevParams &P, int NT, i
   L.mbar = align_up(o, 8); o = L.mbar + 8;
   L.tmem = o; o += 8;
   o = align_up(o, 1024);
+  // the c_nlm tiles, and afterwards the power-spectrum tiles, in one region
+  const size_t tcb = o;
   L.Ahi = o; o += 128 * kTdGroup * 4;
   L.Alo = o; o += 128 * kTdGroup * 4;
   L.Bhi = o; o += kTdCols * kTdGroup * 4;
   L.Blo = o; o += kTdCols * kTdGroup * 4;
+  if (P.ps_ng > 0) {
+    L.Phi = tcb;
+    L.Plo = tcb + 128 * kPsTcK * 4;
+    const size_t pe = tcb + 2 * 128 * kPsTcK * 4;
+    o = o > pe ? o : pe;
+  }
   o = align_up(o, 16);
   L.X = o;
   size_t x = o;
@@ -1035,8 +1047,84 @@ __global__ void __launch_bounds__(NT) k_descriptor_tc(const DevParams P, const D
       for (int n = 0; n < kTdCols; ++n)
         if (n < n_max) sC[(size_t)(my_ri * n_max + n) * KS + my_k] = my_k < k_max ? (float)acc[n] : 0.f;
     __syncthreads();
+    // ---- power spectrum on the tensor cores (src/soap_turbo.f90:750-795): per
+    // group of l, A = rows (l, n) with X_l[n] = (Re c_nl0, r2 Re c_nl1 .., Im
+    // c_nl0, r2 Im c_nl1 ..) in l's block of K (zero elsewhere), the J rows
+    // first; B = A's first rows, so D[(l, n)][(l, j)] = P_l[n, J_j] (the other
+    // blocks of D are zero and unread).  Written to sPl as ps_tensor writes it.
+    const bool ps_tc = P.ps_ng > 0;
+    if (ps_tc) {
+      float *sPl = (float *)(smem + Ly.Pl);
+      const int *psrow = (const int *)SBLOB(off_psrow);
+      unsigned char *sPhi = smem + Ly.Phi, *sPlo = smem + Ly.Plo;
+      const int MR = 16 * P.ps_mt, JP = 8 * P.ps_nt, nJ = P.ps_nj;
+      for (int g = 0; g < P.ps_ng && !failed; ++g) {
+        const int K = P.ps_gk[g], NB = P.ps_gnb[g];
+        int l = -1, n = 0, cb = 0;
+        if (tid < P.ps_grows[g]) {
+          const int code = psrow[P.ps_grow[g] + tid];
+          n = code & 0xff;
+          l = (code >> 8) & 0xff;
+          cb = code >> 16;
+        }
+        const int ko = l >= 0 ? P.ps_ko[l] : 0, kb = l * (l + 1) / 2;
+        for (int k4 = 0; k4 < K; k4 += 4) {
+          float v[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int c = k4 + q - ko;
+            v[q] = 0.f;
+            if (l >= 0 && c >= 0 && c < 2 * (l + 1)) {
+              const int im = c > l, m = im ? c - l - 1 : c;
+              const float x = sC[(size_t)(im ? n_max + n : n) * KS + kb + m];
+              v[q] = m ? 1.41421356237309504880f * x : x;
+            }
+          }
+          uint4 h, lo;
+          tc::split(v[0], h.x, lo.x);
+          tc::split(v[1], h.y, lo.y);
+          tc::split(v[2], h.z, lo.z);
+          tc::split(v[3], h.w, lo.w);
+          const uint32_t off = tc::kmajor_off(tid, k4, K);
+          *(uint4 *)(sPhi + off) = h;
+          *(uint4 *)(sPlo + off) = lo;
+        }
+        tc::fence_proxy_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        if (tid == 0) {
+          const uint32_t phi = tc::smem_addr(sPhi), plo = tc::smem_addr(sPlo);
+          const uint32_t id = tc::idesc_tf32(128, NB);
+          for (int k0 = 0; k0 < K; k0 += 8) tc::mma3_step(tmem, phi, plo, K, phi, plo, K, k0, id, k0 > 0);
+          tc::commit(mbar);
+        }
+        const int ok = tc::mbar_wait(mbar, phase, tc::kMaxTries);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+          if (tid == 0) prep_error(B, kErrTc);
+          tc::mbar_wait(mbar, phase ^ 1u, tc::kMaxTries);
+          failed = true;
+          break;
+        }
+        tc::fence_after_sync();
+        for (int j = 0; j < NB / 16; ++j) {
+          float v[16];
+          tc::ld16(tc::taddr(tmem, 32 * warp, 16 * j), v);
+          if (l >= 0)
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+              const int jc = 16 * j + q - cb;
+              if (jc >= 0 && jc < nJ) sPl[(size_t)(l * MR + n) * JP + jc] = v[q];
+            }
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+      }
+      if (failed) break;
+    }
     site_output<NT>(P, smem, sC, sP, sS, (float *)(smem + Ly.Pl), kept, sRed, site, soap_out, keep_c, keep_norm,
-                    keep);
+                    keep, ps_tc);
     ahead_publish(sSite, nx, nx0, nx1);
   }
   tc::fence_before_sync();
