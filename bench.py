@@ -336,8 +336,12 @@ def run_ours(args):
         p = ctx.contract(b, s, G)
         return s, p
 
-    # the project's autotuner picks CTA size and persistent grid cap per site kernel
+    # the project's autotuner picks the form (tensor or CUDA cores), CTA size and
+    # persistent grid cap per site kernel; --tensor-cores on forces the tensor cores
     tune = ctx.autotune(b)
+    if args.tensor_cores == "on":
+        ctx.set_tensor_cores(True)
+        tune["forced"] = "tensor cores"
     for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize()

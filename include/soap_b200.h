@@ -263,7 +263,9 @@ int soapb_radial_tables(const soapb_context *ctx, int32_t *in_use, double *max_e
 /* Tensor cores (tcgen05, 3xTF32 with FP32 accumulation in tensor memory) for
  * the site kernels' contractions where the definition has them (every
  * alpha_max <= 8 and l_max <= 8): 1 (the default) or 0 (the CUDA-core forms).
- * Results agree within FP32 rounding; each form is bitwise reproducible. */
+ * Results agree within FP32 rounding; each form is bitwise reproducible.  The
+ * call replaces the form soapb_autotune chose; a later soapb_autotune chooses
+ * again (among the tensor-core and CUDA-core kernels when enable is 1). */
 int soapb_set_tensor_cores(soapb_context *ctx, int32_t enable);
 
 /* Descriptor of one batch: d_soap (n_soap, n_sites), normalised.  With

@@ -1416,6 +1416,8 @@ int soapb_set_radial_tables(soapb_context *c, int32_t enable) {
 int soapb_set_tensor_cores(soapb_context *c, int32_t enable) {
   if (!c) return fail(SOAPB_ERR_ARGUMENT, "null context");
   c->tc_enable = enable ? 1 : 0;
+  // an explicit choice replaces the autotuner's choice of form
+  c->tune_tcd = c->tune_tcc = 1;
   c->P.tc_contract = c->tc_enable && c->tune_tcc;
   c->P.tc_descriptor = c->tc_enable && c->tune_tcd;
   return SOAPB_OK;

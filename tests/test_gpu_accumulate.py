@@ -38,10 +38,13 @@ def test_compressed_soap_is_added_into(case):
     ctx = Context(w.hyper)
     W, S = ctx.basis()
     rng = np.random.default_rng(3)
-    soap0 = 0.05 * rng.standard_normal((ctx.n_soap, nl.n_sites))  # Fortran soap(n_soap, n_sites)
-    ref = O.get_soap(w.hyper, nl, W, S, do_derivatives=True, soap_init=soap0.T)
     ref_zero = O.get_soap(w.hyper, nl, W, S, do_derivatives=True)
-    assert site_rel_err(ref.soap, ref_zero.soap) > 1e-3  # the caller's values matter
+    # entry values of the unnormalised descriptor's size (its norm per site), so
+    # that they change the result visibly; Fortran soap(n_soap, n_sites)
+    soap0 = (0.3 * ref_zero.norm() / np.sqrt(ctx.n_soap) *
+             rng.standard_normal((ctx.n_soap, nl.n_sites)))
+    ref = O.get_soap(w.hyper, nl, W, S, do_derivatives=True, soap_init=soap0.T)
+    assert site_rel_err(ref.soap, ref_zero.soap) > 1e-2  # the caller's values matter
     G = rng.standard_normal((ctx.n_soap, nl.n_sites))
     keep = []
     pinned = case == "chunked_pinned"
@@ -83,7 +86,8 @@ def test_soap_cart_der_self_columns_are_accumulated_into():
     ctx = Context(w.hyper)
     W, S = ctx.basis()
     rng = np.random.default_rng(5)
-    soap0 = 0.05 * rng.standard_normal((ctx.n_soap, nl.n_sites))
+    nrm = O.get_soap(w.hyper, nl, W, S, do_derivatives=True).norm()
+    soap0 = 0.3 * nrm / np.sqrt(ctx.n_soap) * rng.standard_normal((ctx.n_soap, nl.n_sites))
     cart0 = rng.standard_normal((3, ctx.n_soap, nl.n_pairs))
     ref = O.get_soap(w.hyper, nl, W, S, do_derivatives=True, cart_der=True, soap_init=soap0.T,
                      cart_init=np.transpose(cart0, (2, 1, 0)))
