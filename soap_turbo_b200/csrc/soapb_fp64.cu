@@ -355,6 +355,160 @@ __global__ void __launch_bounds__(NT) k64_cart_site(const DevParams P, const Dev
   }
 }
 
+// ---- the same, for n_soap <= OPT * NT (OPT = 3): each thread keeps the compressed
+// spherical derivatives of its components o = tid, tid + NT, .. in registers,
+// formed directly from P, Q, Qa, Qo and the pair's radial values (no kept- or
+// output-sized arrays in shared memory), so that three CTAs fit an SM; the
+// pair's angles are turned into the rotation once per CTA.  Shared memory: the
+// site's c_nlm, soap row and self column, the pair's angular planes, radial
+// values and P, Q, Qa, Qo.
+struct Cart2Smem {
+  int C, sv, self, A, R, PQ, rot, total;
+};
+__host__ __device__ inline Cart2Smem cart2_smem(const DevParams &P) {
+  Cart2Smem L;
+  const int N = P.n_max, K = P.k_max, L1 = P.l_max + 1;
+  int o = 0;
+  L.C = o;    o += 2 * N * K;
+  L.sv = o;   o += P.n_soap;
+  L.self = o; o += 3 * P.n_soap;
+  L.A = o;    o += 8 * K;
+  L.R = o;    o += 2 * N;
+  L.PQ = o;   o += 4 * N * L1;
+  L.rot = o;  o += 8;
+  L.total = o;
+  return L;
+}
+
+template <int NT, int OPT>
+__global__ void __launch_bounds__(NT, 3) k64_cart_site2(const DevParams P, const DevBatch B, const double *rad,
+                                                     const double *rad_der, const double2 *ang,
+                                                     const double2 *cnk, const double *soap_un,
+                                                     const double *norm, const double *self_init,
+                                                     double *cart) {
+  extern __shared__ double sm[];
+  __shared__ double red[3][NT / 32];
+  const int site = blockIdx.x;
+  const int p0 = B.off[site], p1 = min(B.off[site + 1], B.n_pairs);
+  if (p1 <= p0) return;
+  const int N = P.n_max, K = P.k_max, L1 = P.l_max + 1, ns = P.n_soap, w3 = 3 * ns;
+  const size_t plane = (size_t)B.n_pairs * K;
+  const Cart2Smem Ly = cart2_smem(P);
+  double2 *sC = (double2 *)(sm + Ly.C);
+  double2 *sA = (double2 *)(sm + Ly.A);
+  double *sv = sm + Ly.sv, *sSelf = sm + Ly.self, *sR = sm + Ly.R, *sPQ = sm + Ly.PQ, *sRot = sm + Ly.rot;
+  const double2 *c = cnk + (size_t)site * N * K;
+  for (int t = threadIdx.x; t < N * K; t += NT) sC[t] = c[t];
+  for (int o = threadIdx.x; o < ns; o += NT) sv[o] = soap_un[(size_t)site * ns + o];
+  const double *si = self_init ? self_init + (size_t)site * w3 : nullptr;
+  for (int t = threadIdx.x; t < w3; t += NT) sSelf[t] = si ? si[t] : 0.0;
+  const double nr = norm[site];
+  const double inv_p = 1.0 / nr, inv_p3 = 1.0 / (nr * nr * nr);
+  const double *Pp = sPQ, *Q = sPQ + N * L1, *Qa = sPQ + 2 * N * L1, *Qo = sPQ + 3 * N * L1;
+  // this thread's kept components (the compression map is one-to-one here or
+  // read through its CSR below)
+  int code[OPT];
+#pragma unroll
+  for (int j = 0; j < OPT; ++j) {
+    const int o = threadIdx.x + j * NT;
+    code[j] = (o < ns && P.cmap_identity) ? P.kept_nnl[o] : 0;
+  }
+
+  for (int k = p0 + 1; k < p1; ++k) {
+    __syncthreads();  // the previous pair's readers of sA, sR, sPQ and sRot are done
+    for (int t = threadIdx.x; t < 4 * K; t += NT) {
+      const int pl = t / K, kk = t - pl * K;
+      sA[t] = ang[pl * plane + (size_t)k * K + kk];
+    }
+    for (int t = threadIdx.x; t < 2 * N; t += NT) sR[t] = t < N ? rad[(size_t)k * N + t] : rad_der[(size_t)k * N + t - N];
+    if (threadIdx.x == NT - 1) {
+      double st, ct, sf, cf;
+      sincos(B.thetas[k], &st, &ct);
+      sincos(B.phis[k], &sf, &cf);
+      const double ir = 1.0 / B.rjs[k];
+      sRot[0] = st * cf; sRot[1] = st * sf; sRot[2] = ct;           // cx cy cz
+      sRot[3] = -ct * cf * ir; sRot[4] = -ct * sf * ir; sRot[5] = st * ir;  // px py pz
+      sRot[6] = -sf * ir; sRot[7] = cf * ir;                        // ax ay
+    }
+    __syncthreads();
+    // P, Q, Qa, Qo(n, l) = sum_m w_m Re(X_lm conj c_nlm) for X = A, dA/dr, dA/dphi, dA/dtheta
+    for (int it = threadIdx.x; it < N * L1; it += NT) {
+      const int n = it / L1, l = it - n * L1;
+      double ap = 0, aq = 0, aa = 0, ao = 0;
+      for (int m = 0; m <= l; ++m) {
+        const int kk = l * (l + 1) / 2 + m;
+        const double w = (m == 0) ? 1.0 : 2.0;
+        const double2 cc = sC[n * K + kk];
+        const double2 a0 = sA[kk], a1 = sA[K + kk], a2 = sA[2 * K + kk], a3 = sA[3 * K + kk];
+        ap = ap + w * (a0.x * cc.x + a0.y * cc.y);
+        aq = aq + w * (a1.x * cc.x + a1.y * cc.y);
+        aa = aa + w * (a2.x * cc.x + a2.y * cc.y);
+        ao = ao + w * (a3.x * cc.x + a3.y * cc.y);
+      }
+      sPQ[it] = ap;
+      sPQ[N * L1 + it] = aq;
+      sPQ[2 * N * L1 + it] = aa;
+      sPQ[3 * N * L1 + it] = ao;
+    }
+    __syncthreads();
+    // the compressed spherical derivatives of this thread's components (:1999-2066)
+    double vr[OPT], va[OPT], vp[OPT];
+    double dr = 0, da = 0, dp = 0;
+#pragma unroll
+    for (int j = 0; j < OPT; ++j) {
+      const int o = threadIdx.x + j * NT;
+      vr[j] = va[j] = vp[j] = 0.0;
+      if (o >= ns) continue;
+      if (P.cmap_identity) {
+        const int n = code[j] & 0xff, np = (code[j] >> 8) & 0xff, l = code[j] >> 16;
+        const double pre = kFourPi64 * ((n == np) ? 1.0 : sqrt(2.0));
+        const double rn = sR[n], rdn = sR[N + n], rnp = sR[np], rdnp = sR[N + np];
+        vr[j] = pre * (rdn * Pp[np * L1 + l] + rn * Q[np * L1 + l] + rdnp * Pp[n * L1 + l] + rnp * Q[n * L1 + l]);
+        va[j] = pre * (rn * Qa[np * L1 + l] + rnp * Qa[n * L1 + l]);
+        vp[j] = pre * (rn * Qo[np * L1 + l] + rnp * Qo[n * L1 + l]);
+      } else {
+        for (int t = P.pi_off[o]; t < P.pi_off[o + 1]; ++t) {
+          const double el = P.pi_el64[t];
+          const int cq = P.kept_nnl[P.pi_q[t]];
+          const int n = cq & 0xff, np = (cq >> 8) & 0xff, l = cq >> 16;
+          const double pre = kFourPi64 * ((n == np) ? 1.0 : sqrt(2.0));
+          const double rn = sR[n], rdn = sR[N + n], rnp = sR[np], rdnp = sR[N + np];
+          vr[j] = vr[j] + el * (pre * (rdn * Pp[np * L1 + l] + rn * Q[np * L1 + l] + rdnp * Pp[n * L1 + l] +
+                                       rnp * Q[n * L1 + l]));
+          va[j] = va[j] + el * (pre * (rn * Qa[np * L1 + l] + rnp * Qa[n * L1 + l]));
+          vp[j] = vp[j] + el * (pre * (rn * Qo[np * L1 + l] + rnp * Qo[n * L1 + l]));
+        }
+      }
+      dr += sv[o] * vr[j];
+      da += sv[o] * va[j];
+      dp += sv[o] * vp[j];
+    }
+    cta_sum3<NT>(dr, da, dp, red);
+    const double cx = sRot[0], cy = sRot[1], cz = sRot[2], px = sRot[3], py = sRot[4], pz = sRot[5];
+    const double ax = sRot[6], ay = sRot[7];
+    double *out = cart + (size_t)k * w3;
+#pragma unroll
+    for (int j = 0; j < OPT; ++j) {
+      const int o = threadIdx.x + j * NT;
+      if (o >= ns) continue;
+      const double s = sv[o];
+      const double r_ = vr[j] * inv_p - s * inv_p3 * dr;
+      const double a_ = va[j] * inv_p - s * inv_p3 * da;
+      const double o_ = vp[j] * inv_p - s * inv_p3 * dp;
+      const double x = cx * r_ + px * o_ + ax * a_, y = cy * r_ + py * o_ + ay * a_, z = cz * r_ + pz * o_;
+      out[3 * o] = x;
+      out[3 * o + 1] = y;
+      out[3 * o + 2] = z;
+      sSelf[3 * o] -= x;
+      sSelf[3 * o + 1] -= y;
+      sSelf[3 * o + 2] -= z;
+    }
+  }
+  __syncthreads();
+  double *out = cart + (size_t)p0 * w3;
+  for (int t = threadIdx.x; t < w3; t += NT) out[t] = sSelf[t];
+}
+
 // ---- pair = sgn * sum_s G(i,s) soap_cart_der(:, s, k): one CTA per site with
 // the site's G row in shared memory, one warp per pair; lane j takes the
 // components o = j, j + 32, ... (a warp's three loads of a step cover 768
@@ -443,13 +597,22 @@ cudaError_t launch_fp64_descriptor(const DevParams &P, const DevBatch &B, cudaSt
     nl += 2;
   }
   if (do_der && cart && np > 0 && nsites > 0) {
-    const size_t sm = fp64_cart_smem(P);
-    const bool staged = sm == (size_t)cart_smem(P, true).total * sizeof(double);
-    auto kern = staged ? k64_cart_site<kCartThreads, true> : k64_cart_site<kCartThreads, false>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    kern<<<nsites, kCartThreads, sm, s>>>(P, B, w.rad, w.rad_der, (const double2 *)w.ang,
-                                          (const double2 *)w.cnk, w.soap_unnorm, w.norm, self_init, cart);
+    const size_t sm2 = (size_t)cart2_smem(P).total * sizeof(double);
+    if (P.n_soap <= 3 * kCartThreads && sm2 <= kCartSmemCap) {
+      auto kern = k64_cart_site2<kCartThreads, 3>;
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+      if (e != cudaSuccess) return e;
+      kern<<<nsites, kCartThreads, sm2, s>>>(P, B, w.rad, w.rad_der, (const double2 *)w.ang,
+                                             (const double2 *)w.cnk, w.soap_unnorm, w.norm, self_init, cart);
+    } else {
+      const size_t sm = fp64_cart_smem(P);
+      const bool staged = sm == (size_t)cart_smem(P, true).total * sizeof(double);
+      auto kern = staged ? k64_cart_site<kCartThreads, true> : k64_cart_site<kCartThreads, false>;
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+      kern<<<nsites, kCartThreads, sm, s>>>(P, B, w.rad, w.rad_der, (const double2 *)w.ang,
+                                            (const double2 *)w.cnk, w.soap_unnorm, w.norm, self_init, cart);
+    }
     nl += 1;
   }
   if (nsites > 0) {
