@@ -108,9 +108,63 @@ __global__ void k64_angular(const DevParams P, const DevBatch B, int do_der, dou
   }
 }
 
-// ---- c_nlm, one CTA per site, threads over (n, k) (src/soap_turbo.f90:626-664)
-__global__ void k64_cnk(const DevParams P, const DevBatch B, const double *rad, const double2 *ang,
-                        double2 *cnk) {
+// ---- c_nlm, one CTA per site, threads over (n, k) (src/soap_turbo.f90:626-664).
+// The site's pairs go in chunks of kCnkChunk whose radial values and angular
+// plane are staged in shared memory with coalesced loads; each thread then sums
+// its (n, k) items over the chunk's pairs in CSR order.
+constexpr int kCnkChunk = 32;
+__global__ void __launch_bounds__(256) k64_cnk(const DevParams P, const DevBatch B, const double *rad,
+                                               const double2 *ang, double2 *cnk) {
+  extern __shared__ double csm[];
+  const int site = blockIdx.x;
+  const int K = P.k_max, N = P.n_max;
+  const int p0 = B.off[site], p1 = min(B.off[site + 1], B.n_pairs);
+  double *sR = csm;                          // kCnkChunk x N
+  double2 *sA = (double2 *)(csm + kCnkChunk * N);  // kCnkChunk x K
+  constexpr int IT = 8;                      // items per thread (N K <= 8 * 256)
+  double cr[IT], ci[IT];
+#pragma unroll
+  for (int j = 0; j < IT; ++j) cr[j] = ci[j] = 0.0;
+  for (int c0 = p0; c0 < p1; c0 += kCnkChunk) {
+    const int np_ = min(kCnkChunk, p1 - c0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < np_ * N; t += blockDim.x) sR[t] = rad[(size_t)c0 * N + t];
+    for (int t = threadIdx.x; t < np_ * K; t += blockDim.x) sA[t] = ang[(size_t)c0 * K + t];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < IT; ++j) {
+      const int it = threadIdx.x + j * blockDim.x;
+      if (it >= N * K) break;
+      const int n = it / K, kk = it - n * K;
+      for (int q = 0; q < np_; ++q) {
+        const double fr = kFourPi64 * sR[q * N + n];
+        const double2 a = sA[q * K + kk];
+        cr[j] = cr[j] + fr * a.x;
+        ci[j] = ci[j] + fr * a.y;
+      }
+    }
+  }
+  double2 *c = cnk + (size_t)site * N * K;
+#pragma unroll
+  for (int j = 0; j < IT; ++j) {
+    const int it = threadIdx.x + j * blockDim.x;
+    if (it >= N * K) break;
+    const int n = it / K, kk = it - n * K;
+    double r = cr[j];
+    if (P.basis == 1 && kk == 0) {
+      for (int mm = 0; mm < B.species_mult[site]; ++mm) {
+        const int s = B.species[(size_t)site * B.max_mult + mm] - 1;
+        if (s >= 0 && s < P.n_species && n >= P.rad[s].nbeg && n < P.rad[s].nbeg + P.rad[s].alpha)
+          r += P.central[n];
+      }
+    }
+    c[it] = make_double2(r, ci[j]);
+  }
+}
+
+// The CSR-order item loop of the form above for definitions with N K > 8 x 256.
+__global__ void k64_cnk_wide(const DevParams P, const DevBatch B, const double *rad, const double2 *ang,
+                             double2 *cnk) {
   const int site = blockIdx.x;
   const int K = P.k_max, N = P.n_max;
   const int p0 = B.off[site], p1 = min(B.off[site + 1], B.n_pairs);
@@ -590,7 +644,13 @@ cudaError_t launch_fp64_descriptor(const DevParams &P, const DevBatch &B, cudaSt
     nl += 2;
   }
   if (nsites > 0) {
-    k64_cnk<<<nsites, 256, 0, s>>>(P, B, w.rad, (const double2 *)w.ang, (double2 *)w.cnk);
+    if (P.n_max * P.k_max <= 8 * 256) {
+      const size_t smc = (size_t)kCnkChunk * (P.n_max + 2 * P.k_max) * sizeof(double);
+      cudaFuncSetAttribute(k64_cnk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc);
+      k64_cnk<<<nsites, 256, smc, s>>>(P, B, w.rad, (const double2 *)w.ang, (double2 *)w.cnk);
+    } else {
+      k64_cnk_wide<<<nsites, 256, 0, s>>>(P, B, w.rad, (const double2 *)w.ang, (double2 *)w.cnk);
+    }
     const size_t sm = (size_t)P.n_kept * sizeof(double);
     cudaFuncSetAttribute(k64_soap, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k64_soap<<<nsites, 256, sm, s>>>(P, B, (const double2 *)w.cnk, soap_acc, w.soap_unnorm, w.norm);
