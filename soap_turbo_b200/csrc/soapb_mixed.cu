@@ -1648,15 +1648,23 @@ __global__ void __launch_bounds__(NT) k_contract_tc(const DevParams P, const Dev
       }
     }
     __syncthreads();
-    // ---- the B operand: H as [96 x KB], column c = 2 k + (re, im)
-    for (int t = tid; t < kTcCols * KB; t += NT) {
-      const int c = t / KB, kk = t - c * KB, k = c >> 1;
-      const float v = (k < k_max && kk < nsp * AMAX) ? sH[(c & 1) * HPL + (size_t)k * HS + kk] : 0.f;
-      uint32_t h, lo;
-      tc::split(v, h, lo);
-      const uint32_t off = tc::kmajor_off(c, kk, KB);
-      *(uint32_t *)(sBhi + off) = h;
-      *(uint32_t *)(sBlo + off) = lo;
+    // ---- the B operand: H as [96 x KB], column c = 2 k + (re, im); one row per
+    // thread, 16 bytes at a time (H rows are 16-byte aligned: HS is a multiple of 4)
+    if (tid < kTcCols) {
+      const int c = tid, k = c >> 1;
+      const float *hrow = sH + (c & 1) * HPL + (size_t)k * HS;
+      for (int kk4 = 0; kk4 < KB; kk4 += 4) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (k < k_max && kk4 < nsp * AMAX) v = *(const float4 *)(hrow + kk4);
+        uint4 h, lo;
+        tc::split(v.x, h.x, lo.x);
+        tc::split(v.y, h.y, lo.y);
+        tc::split(v.z, h.z, lo.z);
+        tc::split(v.w, h.w, lo.w);
+        const uint32_t off = tc::kmajor_off(c, kk4, KB);
+        *(uint4 *)(sBhi + off) = h;
+        *(uint4 *)(sBlo + off) = lo;
+      }
     }
     ahead_bounds(B, nx, nx0, nx1);
     double self_x = 0.0, self_y = 0.0, self_z = 0.0;
@@ -1670,24 +1678,39 @@ __global__ void __launch_bounds__(NT) k_contract_tc(const DevParams P, const Dev
                                           slot, my_bits, my_r);
       for (int ebase = 0; ebase < n_ent && !failed; ebase += kTcEntries) {
         const int n_round = min(kTcEntries, n_ent - ebase);
-        // ---- A operand: rows e < 64 dR/dr, rows 64 + e R, in the species' columns
-        for (int t = tid; t < 128 * KB; t += NT) {
-          const int r = t / KB, kk = t - r * KB, e = r & (kTcEntries - 1);
-          float v = 0.f;
+        // ---- A operand: rows e < 64 dR/dr, rows 64 + e R, in the species' columns;
+        // row tid per thread: its entry's AMAX values, zero in the other columns
+        {
+          const int e = tid & (kTcEntries - 1);
+          int sp = -1;
+          float4 rv[AMAX / 4];
+#pragma unroll
+          for (int j = 0; j < AMAX / 4; ++j) rv[j] = make_float4(0.f, 0.f, 0.f, 0.f);
           if (e < n_round) {
             const int code = sEnt[ebase + e];
-            const int s = code >> 24;
-            const int n = kk - s * AMAX;
-            if (n >= 0 && n < AMAX) {
-              const int k = chunk + (code & 0xffffff);
-              v = B.rad[((size_t)k * nsp + s) * 2 * AMAX + (r < kTcEntries ? AMAX : 0) + n];
-            }
+            sp = code >> 24;
+            const float4 *src = (const float4 *)(B.rad + ((size_t)(chunk + (code & 0xffffff)) * nsp + sp) * 2 * AMAX +
+                                                 (tid < kTcEntries ? AMAX : 0));
+#pragma unroll
+            for (int j = 0; j < AMAX / 4; ++j) rv[j] = src[j];
           }
-          uint32_t h, lo;
-          tc::split(v, h, lo);
-          const uint32_t off = tc::kmajor_off(r, kk, KB);
-          *(uint32_t *)(sAhi + off) = h;
-          *(uint32_t *)(sAlo + off) = lo;
+          for (int kk4 = 0; kk4 < KB; kk4 += 4) {
+            const int blk = kk4 / AMAX, j = (kk4 - blk * AMAX) >> 2;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (blk == sp) {
+#pragma unroll
+              for (int q = 0; q < AMAX / 4; ++q)
+                if (q == j) v = rv[q];
+            }
+            uint4 h, lo;
+            tc::split(v.x, h.x, lo.x);
+            tc::split(v.y, h.y, lo.y);
+            tc::split(v.z, h.z, lo.z);
+            tc::split(v.w, h.w, lo.w);
+            const uint32_t off = tc::kmajor_off(tid, kk4, KB);
+            *(uint4 *)(sAhi + off) = h;
+            *(uint4 *)(sAlo + off) = lo;
+          }
         }
         tc::fence_proxy_async();
         tc::fence_before_sync();
