@@ -216,6 +216,11 @@ __host__ __device__ constexpr int row_p(int LC) { return 4 * (LC + 1) + 4; }
 __host__ __device__ constexpr int row_len(int LC) { return (row_p(LC) + (LC + 2) * (LC + 3) / 2 + 3) / 4 * 4; }
 
 int ang_row_floats(const DevParams &P) { return row_len(P.amax_t == 8 ? 8 : 12); }
+// the pair kernel's staging stride in floats (odd): the whole row, or with TAB
+// the larger of its two halves
+__host__ __device__ constexpr int pair_stage_stride(int LC, bool TAB) {
+  return TAB ? (row_p(LC) > row_len(LC) - row_p(LC) ? row_p(LC) : row_len(LC) - row_p(LC)) + 1 : row_len(LC) + 1;
+}
 
 // ------------------------------------------------------------ pair kernel
 // One thread per pair, all FP64 work of the path:
@@ -242,20 +247,23 @@ __global__ void __launch_bounds__(kPairThreads)
   }
   constexpr int AW = row_len(LC);
   // odd stride in shared memory: each thread fills its own row, so lanes must
-  // not all map to one bank
-  constexpr int AWS = AW + 1;
+  // not all map to one bank.  TAB stages the row in two halves (the scalars,
+  // then the P_l^m values) through half the buffer, for more CTAs per SM.
+  constexpr int AWS = pair_stage_stride(LC, TAB);
   const int head = (P.off_rad + P.n_species * SOAPB_RADSP_BYTES) / 16;
   for (int t = threadIdx.x; t < head; t += NT) ((uint4 *)smem)[t] = ((const uint4 *)P.blob)[t];
   float *rows = (float *)(smem + (size_t)head * 16);
   __syncthreads();
   const int k0 = pair_lo + ((int)blockIdx.x - scan_tiles) * NT;
   const int k = k0 + threadIdx.x;
+  bool active = false;
+  double x = 0.0, sq = 0.0;
+  float *row = rows + threadIdx.x * AWS;
   if (k < pair_hi) {
     const unsigned bits = prep_pair(B, k, P.n_species);
     const double r = B.rjs[k];
     if (bits != 0u && r < P.rcut_max) {
-      float *row = rows + threadIdx.x * AWS;
-      double x, sq;
+      active = true;
       const int isp = __ffs(bits) - 1;
       if (do_der)
         angular_stage<LC, true>(P, isp, r, B.thetas[k], B.phis[k], row, row_il(LC), row_ild(LC),
@@ -265,10 +273,12 @@ __global__ void __launch_bounds__(kPairThreads)
                                  row_er(LC), row_ei(LC), row_amp(LC), row_sf(LC), x, sq);
       row[row_x(LC)] = (float)x;
       row[row_sq(LC)] = (float)sq;
-      float *Pr = row + row_p(LC);
-      const float *kpx = (const float *)(smem + P.off_kpx);
-      plm_rows<LC + 1>(P.l_max + (do_der ? 1 : 0), (float)x, (float)sq,
-                       [&](int kk, float v) { Pr[kk] = v * kpx[kk]; });
+      if constexpr (!TAB) {
+        float *Pr = row + row_p(LC);
+        const float *kpx = (const float *)(smem + P.off_kpx);
+        plm_rows<LC + 1>(P.l_max + (do_der ? 1 : 0), (float)x, (float)sq,
+                         [&](int kk, float v) { Pr[kk] = v * kpx[kk]; });
+      }
       // the radial expansion of each species in range, as for a neighbour: the
       // central pair's expansion (:342-355) differs only by the factor
       // central_weight (:638-646), which the descriptor applies to that entry
@@ -314,9 +324,34 @@ __global__ void __launch_bounds__(kPairThreads)
     }
   }
   __syncthreads();
+  const int nrow = min(NT, pair_hi - k0);
+  if constexpr (TAB) {
+    // coalesced 16-byte stores of the rows' first parts, then the P_l^m values
+    // through the same buffer
+    constexpr int P1 = row_p(LC) / 4, P2 = (AW - row_p(LC)) / 4;
+    for (int t = threadIdx.x; t < nrow * P1; t += NT) {
+      const int i = t / P1, j = t - i * P1;
+      const float *src = rows + i * AWS + 4 * j;
+      *(float4 *)(B.ang + (size_t)(k0 + i) * AW + 4 * j) = make_float4(src[0], src[1], src[2], src[3]);
+    }
+    __syncthreads();
+    if (active) {
+      const float *kpx = (const float *)(smem + P.off_kpx);
+      plm_rows<LC + 1>(P.l_max + (do_der ? 1 : 0), (float)x, (float)sq,
+                       [&](int kk, float v) { row[kk] = v * kpx[kk]; });
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nrow * P2; t += NT) {
+      const int i = t / P2, j = t - i * P2;
+      const float *src = rows + i * AWS + 4 * j;
+      *(float4 *)(B.ang + (size_t)(k0 + i) * AW + row_p(LC) + 4 * j) =
+          make_float4(src[0], src[1], src[2], src[3]);
+    }
+    return;
+  }
   // coalesced 16-byte stores of the CTA's rows (AW is a multiple of 4 floats)
   constexpr int AW4 = AW / 4;
-  const int n4 = min(NT, pair_hi - k0) * AW4;
+  const int n4 = nrow * AW4;
   float4 *dst = (float4 *)(B.ang + (size_t)k0 * AW);
   for (int t = threadIdx.x; t < n4; t += NT) {
     const int i = t / AW4;
@@ -1962,7 +1997,7 @@ template <int AMAX, int LC, bool OP, bool TAB = false>
 static cudaError_t run_pair(const DevParams &P, const DevBatch &B, cudaStream_t s, int do_der, int pair_lo,
                             int pair_hi, bool scan) {
   size_t sm = (size_t)P.off_rad + (size_t)P.n_species * SOAPB_RADSP_BYTES +
-              (size_t)kPairThreads * (row_len(LC) + 1) * sizeof(float);
+              (size_t)kPairThreads * pair_stage_stride(LC, TAB) * sizeof(float);
   if (sm < kScanTile * sizeof(int)) sm = kScanTile * sizeof(int);  // scan tiles reuse it
   auto kern = k_pair<AMAX, LC, OP, TAB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
