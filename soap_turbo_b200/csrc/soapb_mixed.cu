@@ -1491,7 +1491,7 @@ constexpr int kTcTmemCols = 128; // TMEM columns a CTA holds
 __host__ __device__ inline int tc_kb(const DevParams &P, int AMAX) { return (P.n_species * AMAX + 7) / 8 * 8; }
 
 struct TcLayout {
-  size_t red, ent, wcnt, misc, H, Rot, F, Fu, Bhi, Blo, X, Ahi, Alo, C, Gu, Gp, mbar, tmem, total;
+  size_t red, ent, wcnt, misc, H, Rot, F, Fu, Bhi, Blo, X, Ahi, Alo, AT, C, Gu, Gp, mbar, tmem, total;
 };
 __host__ __device__ inline TcLayout make_tc_layout(const DevParams &P, int NT, int AMAX) {
   TcLayout L{};
@@ -1517,6 +1517,7 @@ __host__ __device__ inline TcLayout make_tc_layout(const DevParams &P, int NT, i
   size_t x = o;
   L.Ahi = x; x += 128 * KB * 4;
   L.Alo = x; x += 128 * KB * 4;
+  L.AT = x;  x += (size_t)row_len(AMAX == 8 ? 8 : 12) * kTcEntries * 4;  // the round's angular rows, transposed
   const size_t end_round = x;
   x = o;
   L.C = x;  x += 2 * (size_t)P.n_max * KS * sizeof(float);
@@ -1563,6 +1564,7 @@ __global__ void __launch_bounds__(NT) k_contract_tc(const DevParams P, const Dev
   float *sGu = (float *)(smem + Ly.Gu);
   float *sGp = (float *)(smem + Ly.Gp);
   unsigned char *sAhi = smem + Ly.Ahi, *sAlo = smem + Ly.Alo, *sBhi = smem + Ly.Bhi, *sBlo = smem + Ly.Blo;
+  float *sAT = (float *)(smem + Ly.AT);
   uint64_t *mbar = (uint64_t *)(smem + Ly.mbar);
   uint32_t *tmem_slot = (uint32_t *)(smem + Ly.tmem);
   int *sEnt = (int *)(smem + Ly.ent);
@@ -1747,6 +1749,18 @@ __global__ void __launch_bounds__(NT) k_contract_tc(const DevParams P, const Dev
             *(uint4 *)(sAlo + off) = lo;
           }
         }
+        // the round's angular rows, transposed to [field][entry] for the epilogue
+        // (thread-per-entry reads then fall in distinct banks); pieces of 16 bytes
+        for (int t = tid; t < (AW / 4) * kTcEntries; t += NT) {
+          const int j4 = t / kTcEntries, e = t - j4 * kTcEntries;
+          if (e < n_round) {
+            const float4 v = __ldg((const float4 *)(B.ang + (size_t)(chunk + (sEnt[ebase + e] & 0xffffff)) * AW) + j4);
+            sAT[(4 * j4) * kTcEntries + e] = v.x;
+            sAT[(4 * j4 + 1) * kTcEntries + e] = v.y;
+            sAT[(4 * j4 + 2) * kTcEntries + e] = v.z;
+            sAT[(4 * j4 + 3) * kTcEntries + e] = v.w;
+          }
+        }
         tc::fence_proxy_async();
         tc::fence_before_sync();
         __syncthreads();
@@ -1776,18 +1790,19 @@ __global__ void __launch_bounds__(NT) k_contract_tc(const DevParams P, const Dev
         const int e = tid & (kTcEntries - 1);
         const bool act = e < n_round;
         const int code = act ? sEnt[ebase + e] : 0;
-        const float *Ae = B.ang + (size_t)(chunk + (code & 0xffffff)) * AW;
+        // field f of this entry's row: Ae[f * kTcEntries]
+        const float *Ae = sAT + e;
         float il[LC + 1], ild[LC + 1], er[LC + 1], ei[LC + 1], sfac = 0.f;
 #pragma unroll
         for (int l = 0; l <= LC; ++l) {
-          il[l] = act ? __ldg(Ae + O_IL + l) : 0.f;
-          er[l] = act ? __ldg(Ae + O_ER + l) : 0.f;
-          ei[l] = act ? __ldg(Ae + O_EI + l) : 0.f;
-          ild[l] = (act && vrole) ? __ldg(Ae + O_ILD + l) : 0.f;
+          il[l] = act ? Ae[(O_IL + l) * kTcEntries] : 0.f;
+          er[l] = act ? Ae[(O_ER + l) * kTcEntries] : 0.f;
+          ei[l] = act ? Ae[(O_EI + l) * kTcEntries] : 0.f;
+          ild[l] = (act && vrole) ? Ae[(O_ILD + l) * kTcEntries] : 0.f;
         }
-        if (act && vrole) sfac = __ldg(Ae + O_SF);
+        if (act && vrole) sfac = Ae[O_SF * kTcEntries];
         float f_rad = 0.f, f_azi = 0.f, f_pol = 0.f;
-        const float *Pe = Ae + O_P;
+        const float *Pe = Ae + O_P * kTcEntries;
 #pragma unroll
         for (int j = 0; j < (2 * KC + 15) / 16; ++j) {
           float v[16];
@@ -1799,7 +1814,7 @@ __global__ void __launch_bounds__(NT) k_contract_tc(const DevParams P, const Dev
             const int l = tc_l_of(kk), m = tc_m_of(kk);
             if (!act || l > P.l_max) continue;
             const float xr = v[2 * qq], xi = v[2 * qq + 1];
-            const float Pk = __ldg(Pe + kk);
+            const float Pk = Pe[kk * kTcEntries];
             const float u = Pk * il[l];
             if (!vrole) {
               f_rad = fmaf(u, er[m] * xr + ei[m] * xi, f_rad);
@@ -1810,8 +1825,8 @@ __global__ void __launch_bounds__(NT) k_contract_tc(const DevParams P, const Dev
               const int ixy = (m == 0) ? (l > 0 ? l * (l + 1) / 2 + 1 : kk) : (m != l ? kk + 1 : kk);
               const int ixz = (m == 0) ? kk : (l + 1) * (l + 2) / 2 + m - 1;
               const int ixw = (m == 0) ? kk : (l + 1) * (l + 2) / 2 + m + 1;
-              const float dms = cf.x * __ldg(Pe + ixx) + cf.y * __ldg(Pe + ixy);
-              const float dvs = cf.z * __ldg(Pe + ixz) + cf.w * __ldg(Pe + ixw);
+              const float dms = cf.x * Pe[ixx * kTcEntries] + cf.y * Pe[ixy * kTcEntries];
+              const float dvs = cf.z * Pe[ixz * kTcEntries] + cf.w * Pe[ixw * kTcEntries];
               const float ur = Pk * ild[l] - sfac * u;
               const float ua = dvs * il[l];
               const float up = dms * il[l];
@@ -1831,8 +1846,8 @@ __global__ void __launch_bounds__(NT) k_contract_tc(const DevParams P, const Dev
             Fe[2] = f_pol;
             // the rotation to Cartesian uses the same angles (:1867-1871)
             float *rot = sRot + 4 * (code & 0xffffff);
-            rot[0] = __ldg(Ae + O_X);
-            rot[1] = __ldg(Ae + O_SQ);
+            rot[0] = Ae[O_X * kTcEntries];
+            rot[1] = Ae[O_SQ * kTcEntries];
             rot[2] = er[1];
             rot[3] = -ei[1];
           } else {
@@ -1895,6 +1910,24 @@ static int persistent_grid(K kernel, int threads, size_t smem, int n_sites, int 
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  // the count from the kernel's registers and shared memory as well: the
+  // occupancy query has been seen to answer 1 for CTAs of 66-74 KB that fit
+  // three times.  Too many CTAs is harmless here -- a persistent CTA that
+  // starts late finds the remaining sites, none waits on another.
+  cudaFuncAttributes fa{};
+  int sm_per_sm = 0, regs_per_sm = 0;
+  if (cudaFuncGetAttributes(&fa, kernel) == cudaSuccess &&
+      cudaDeviceGetAttribute(&sm_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
+      cudaDeviceGetAttribute(&regs_per_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) == cudaSuccess) {
+    const int by_smem = (int)((size_t)sm_per_sm / (smem + fa.sharedSizeBytes + 1024));
+    const int by_regs = fa.numRegs > 0 ? regs_per_sm / (fa.numRegs * threads) : by_smem;
+    const int by_threads = 2048 / threads;
+    const int est = by_smem < by_regs ? (by_smem < by_threads ? by_smem : by_threads)
+                                      : (by_regs < by_threads ? by_regs : by_threads);
+    if (est > per_sm) per_sm = est;
+  } else {
+    cudaGetLastError();
+  }
   int g = sms * (per_sm > 0 ? per_sm : 1);
   if (max_ctas > 0 && g > max_ctas) g = max_ctas;
   return g < n_sites ? g : n_sites;
