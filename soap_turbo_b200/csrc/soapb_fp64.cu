@@ -108,6 +108,98 @@ __global__ void k64_angular(const DevParams P, const DevBatch B, int do_der, dou
   }
 }
 
+// ---- the same with the associated Legendre rows streamed: P_l^m of rows l - 1,
+// l and l + 1 only (the recursion of get_plm_array, src/soap_turbo_angular.f90:
+// 108-160), every loop unrolled so that they stay in registers, and each (l, m)
+// written as soon as rows l and l + 1 exist (the derivative forms need
+// P_{l+1}^{m+-1}, :181-248).  Same arithmetic as k64_angular.
+template <int LC>
+__global__ void __launch_bounds__(128) k64_angular2(const DevParams P, const DevBatch B, int do_der, double2 *ang) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= B.n_pairs) return;
+  const int K = P.k_max, L = P.l_max;
+  const size_t plane = (size_t)B.n_pairs * K;
+  double2 *A = ang + (size_t)k * K;
+  const double r = B.rjs[k];
+  const unsigned bits = B.bits[k];
+  if (!(r < P.rcut_max) || bits == 0u) {
+    for (int kk = 0; kk < K; ++kk) {
+      A[kk] = make_double2(0.0, 0.0);
+      if (do_der) {
+        A[plane + kk] = make_double2(0.0, 0.0);
+        A[2 * plane + kk] = make_double2(0.0, 0.0);
+        A[3 * plane + kk] = make_double2(0.0, 0.0);
+      }
+    }
+    return;
+  }
+  AngScalars<LC> S;
+  angular_scalars<LC>(P, __ffs(bits) - 1, r, B.thetas[k], B.phis[k], do_der != 0, S);
+  const double x = S.x, sq = S.sq, x2 = x * x;
+  // rows: pm (l - 1), pc (l), pn (l + 1); m <= l + 1 <= LC + 1
+  double pm[LC + 2], pc[LC + 2], pn[LC + 2];
+#pragma unroll
+  for (int m = 0; m < LC + 2; ++m) pm[m] = pc[m] = pn[m] = 0.0;
+  pc[0] = 1.0;        // l = 0
+  pn[0] = x;          // l = 1
+  pn[1] = -sq;
+#pragma unroll
+  for (int l = 0; l <= LC; ++l) {
+    if (l > L) break;
+#pragma unroll
+    for (int m = 0; m <= l; ++m) {
+      const int kk = l * (l + 1) / 2 + m;
+      const double e_re = S.il[l] * S.er[m], e_im = S.il[l] * S.ei[m];
+      const double u = S.amp * P.preflm64[kk];
+      const double v = u * pc[m];
+      A[kk] = make_double2(v * e_re, v * e_im);
+      if (do_der) {
+        const double er_re = S.ild[l] * S.er[m], er_im = S.ild[l] * S.ei[m];
+        A[plane + kk] = make_double2(v * er_re - S.sig_fac * v * e_re, v * er_im - S.sig_fac * v * e_im);
+        double dms, dvs;
+        if (m == 0) {
+          dms = (l == 0) ? 0.0 : -0.5 * pc[1];
+          dvs = 0.0;
+        } else {
+          dms = 0.5 * (double)(l + m) * (double)(l - m + 1) * pc[m - 1];
+          dvs = 0.5 * (double)(l - m + 1) * (double)(l - m + 2) * pn[m - 1] + 0.5 * pn[m + 1];
+        }
+        if (m != l) dms = dms + -0.5 * pc[m + 1];
+        const double w = u * dvs;
+        A[2 * plane + kk] = make_double2(-(w * e_im), w * e_re);
+        const double w2 = u * dms;
+        A[3 * plane + kk] = make_double2(w2 * e_re, w2 * e_im);
+      }
+    }
+    // advance: row l + 2 from rows l + 1 (pn) and l (pc)
+    const int l2 = l + 2;
+    double nn[LC + 2];
+#pragma unroll
+    for (int m = 0; m < LC + 2; ++m) nn[m] = 0.0;
+    if (l2 == 2) {
+      nn[0] = 1.5 * x2 - 0.5;
+      nn[1] = -3.0 * x * sq;
+      nn[2] = 3.0 - 3.0 * x2;
+    } else if (l2 <= LC + 1) {
+#pragma unroll
+      for (int m = 0; m <= l2 - 2 && m < LC + 2; ++m) {
+        const double aa = (double)(2 * l2 - 1) / (double)(l2 - m);
+        const double bb = (double)(l2 - 1 + m) / (double)(l2 - m);
+        nn[m] = aa * x * pn[m] - bb * pc[m];
+      }
+      if (l2 - 1 < LC + 2) nn[l2 - 1] = x * (double)(2 * l2 - 1) * pn[l2 - 1];
+      if (l2 < LC + 2) nn[l2] = -(double)(2 * l2 - 1) * sq * pn[l2 - 1];
+    }
+#pragma unroll
+    for (int m = 0; m < LC + 2; ++m) {
+      pm[m] = pc[m];
+      pc[m] = pn[m];
+      pn[m] = nn[m];
+    }
+  }
+  (void)pm;
+}
+
 // ---- c_nlm, one CTA per site, threads over (n, k) (src/soap_turbo.f90:626-664).
 // The site's pairs go in chunks of kCnkChunk whose radial values and angular
 // plane are staged in shared memory with coalesced loads; each thread then sums
@@ -639,7 +731,7 @@ cudaError_t launch_fp64_descriptor(const DevParams &P, const DevBatch &B, cudaSt
       if (op) k64_radial<16, true><<<blocks, 128, 0, s>>>(P, B, do_der, w.rad, w.rad_der);
       else k64_radial<16, false><<<blocks, 128, 0, s>>>(P, B, do_der, w.rad, w.rad_der);
     }
-    if (P.l_max <= 8) k64_angular<8><<<blocks, 128, 0, s>>>(P, B, do_der, (double2 *)w.ang);
+    if (P.l_max <= 8) k64_angular2<8><<<blocks, 128, 0, s>>>(P, B, do_der, (double2 *)w.ang);
     else k64_angular<12><<<blocks, 128, 0, s>>>(P, B, do_der, (double2 *)w.ang);
     nl += 2;
   }
