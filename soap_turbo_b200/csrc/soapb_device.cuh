@@ -444,20 +444,32 @@ __host__ __device__ __forceinline__ int radial_branch(const DevParams &P, const 
 // R_n (out[0..AMAX)) and, with do_der, dR_n/dr (out[AMAX..2 AMAX)) of one entry
 // from its species' table, 4 pi global_scaling included: the segment and its
 // local coordinate t in FP64, the polynomial by Horner in FP32.
+// The entry's segment: the offset of its coefficients in rtab_coef (floats;
+// -1 where R_n and dR_n/dr are zero) and its local coordinate t in [-1, 1].
+template <int AMAX>
+__device__ __forceinline__ int radial_table_locate(const DevParams &P, const RadSp &S, const RadTab &T, double r,
+                                                   float &t) {
+  const int st = radial_branch(P, S, r);
+  t = 0.f;
+  if (st < 0) return -1;
+  const double u = (r - T.lo[st]) * T.inv_h[st];
+  int seg = (int)floor(u);
+  seg = seg < 0 ? 0 : (seg >= T.nseg[st] ? T.nseg[st] - 1 : seg);
+  t = (float)(2.0 * (u - (double)seg) - 1.0);
+  return (T.base[st] + seg) * (kRadTabDeg + 1) * 2 * AMAX;
+}
+
 template <int AMAX>
 __device__ __forceinline__ void radial_from_table(const DevParams &P, const RadSp &S, const RadTab &T,
                                                   double r, bool do_der, float (&out)[2 * AMAX]) {
-  const int st = radial_branch(P, S, r);
-  if (st < 0) {
+  float t;
+  const int cb = radial_table_locate<AMAX>(P, S, T, r, t);
+  if (cb < 0) {
 #pragma unroll
     for (int f = 0; f < 2 * AMAX; ++f) out[f] = 0.f;
     return;
   }
-  const double u = (r - T.lo[st]) * T.inv_h[st];
-  int seg = (int)floor(u);
-  seg = seg < 0 ? 0 : (seg >= T.nseg[st] ? T.nseg[st] - 1 : seg);
-  const float t = (float)(2.0 * (u - (double)seg) - 1.0);
-  const float4 *c4 = (const float4 *)(P.rtab_coef + (size_t)(T.base[st] + seg) * (kRadTabDeg + 1) * 2 * AMAX);
+  const float4 *c4 = (const float4 *)(P.rtab_coef + cb);
   constexpr int F4 = 2 * AMAX / 4;
   const int nf4 = do_der ? F4 : F4 / 2;
 #pragma unroll

@@ -114,7 +114,7 @@ __global__ void k64_angular(const DevParams P, const DevBatch B, int do_der, dou
 // written as soon as rows l and l + 1 exist (the derivative forms need
 // P_{l+1}^{m+-1}, :181-248).  Same arithmetic as k64_angular.
 template <int LC>
-__global__ void __launch_bounds__(128) k64_angular2(const DevParams P, const DevBatch B, int do_der, double2 *ang) {
+__global__ void __launch_bounds__(128, 4) k64_angular2(const DevParams P, const DevBatch B, int do_der, double2 *ang) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= B.n_pairs) return;
   const int K = P.k_max, L = P.l_max;
@@ -365,6 +365,7 @@ __host__ __device__ inline CartSmem cart_smem(const DevParams &P, bool staged) {
   L.dc = o;   o += 3 * P.n_soap;         // compressed derivatives, then the Cartesian column
   L.C = L.sv = L.self = -1;
   if (staged) {
+    o = (o + 1) & ~1;                    // c_nlm is read as double2: an even offset
     L.C = o;    o += 2 * N * K;          // the site's c_nlm
     L.sv = o;   o += P.n_soap;           // the site's unnormalised soap row
     L.self = o; o += 3 * P.n_soap;       // the self column, summed over the pairs
@@ -655,6 +656,239 @@ __global__ void __launch_bounds__(NT, 3) k64_cart_site2(const DevParams P, const
   for (int t = threadIdx.x; t < w3; t += NT) out[t] = sSelf[t];
 }
 
+// ---- soap_cart_der for n_max <= 32, l_max <= 8, n_soap <= 3 x 256: the CTA
+// takes its site's pairs kC3Pairs at a time.
+//  * P, Q, Qa, Qo: two warps per pair, lane n summing sum_m w_m Re(X_lm conj
+//    c_nlm) over every (l, m) for two of the four planes X in registers (the
+//    angular values broadcast from shared memory, c_nlm rows padded to 49 so
+//    that the lanes' rows fall in distinct banks, the (n, l) rows stored with
+//    an odd stride of 9 so that the lanes' stores do too);
+//  * the compressed spherical derivatives, the normalisation derivative and the
+//    rotation CTA-wide: thread t owns components o = t, t + 256, t + 512 (their
+//    (n, n', l) offsets decoded once per site), sums the self column in its
+//    registers in pair order, forms the batch's dot products with p (reduced
+//    together, in a fixed order), then forms the derivatives again to write the
+//    columns (cheaper than holding them: the registers would halve the CTAs
+//    per SM).
+constexpr int kC3Pairs = 4;
+constexpr int kC3Kp = 49;  // padded c_nlm row (double2), k_max <= 45
+constexpr int kC3L1 = 9;   // P, Q rows of l_max + 1 <= 9 entries
+struct Cart3Smem {
+  int C, A, PQ, R, sv, rot, red, total;
+};
+__host__ __device__ inline Cart3Smem cart3_smem(const DevParams &P) {
+  Cart3Smem L;
+  const int N = P.n_max, K = P.k_max;
+  // the double2 arrays first, at even offsets (16-byte aligned), then the doubles
+  int o = 0;
+  L.C = o;   o += 2 * N * kC3Kp;
+  L.A = o;   o += kC3Pairs * 8 * K;
+  L.PQ = o;  o += kC3Pairs * 4 * N * kC3L1;
+  L.R = o;   o += kC3Pairs * 2 * N;
+  L.sv = o;  o += P.n_soap;
+  L.rot = o; o += kC3Pairs * 8;
+  L.red = o; o += 8 * 3 * kC3Pairs;
+  L.total = o;
+  return L;
+}
+
+template <int LC>
+__global__ void __launch_bounds__(256, 2) k64_cart_site3(const DevParams P, const DevBatch B, const double *rad,
+                                                         const double *rad_der, const double2 *ang,
+                                                         const double2 *cnk, const double *soap_un,
+                                                         const double *norm, const double *self_init,
+                                                         double *cart) {
+  static_assert(LC + 1 == kC3L1, "P, Q row length");
+  static_assert(kC3Pairs * 2 == 256 / 32, "two warps per pair");
+  constexpr int NT = 256, OPT = 3, L1 = LC + 1;
+  extern __shared__ double sm[];
+  const int site = blockIdx.x;
+  const int p0 = B.off[site], p1 = min(B.off[site + 1], B.n_pairs);
+  if (p1 <= p0) return;
+  const int N = P.n_max, K = P.k_max, ns = P.n_soap, w3 = 3 * ns, L = P.l_max;
+  const size_t plane = (size_t)B.n_pairs * K;
+  const Cart3Smem Ly = cart3_smem(P);
+  double2 *sC = (double2 *)(sm + Ly.C);
+  double2 *sA = (double2 *)(sm + Ly.A);
+  double *sPQ = sm + Ly.PQ, *sR = sm + Ly.R, *sv = sm + Ly.sv, *sRot = sm + Ly.rot, *sRed = sm + Ly.red;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double2 *c = cnk + (size_t)site * N * K;
+  for (int t = tid; t < N * K; t += NT) {
+    const int n = t / K, kk = t - n * K;
+    sC[n * kC3Kp + kk] = c[t];
+  }
+  for (int o = tid; o < ns; o += NT) sv[o] = soap_un[(size_t)site * ns + o];
+  const double nr = norm[site];
+  const double inv_p = 1.0 / nr, inv_p3 = 1.0 / (nr * nr * nr);
+  // this thread's components: offsets of (n, l) and (n', l) in a pair's P, Q
+  // rows, and the multiplicity prefactor (identity compression map)
+  int ia[OPT], ib[OPT];
+  double pre[OPT], self_[OPT][3];
+  const double *si = self_init ? self_init + (size_t)site * w3 : nullptr;
+#pragma unroll
+  for (int j = 0; j < OPT; ++j) {
+    const int o = tid + j * NT;
+    const int code = (o < ns && P.cmap_identity) ? P.kept_nnl[o] : 0;
+    const int n = code & 0xff, np = (code >> 8) & 0xff, l = code >> 16;
+    ia[j] = n * L1 + l;
+    ib[j] = np * L1 + l;
+    pre[j] = kFourPi64 * ((n == np) ? 1.0 : sqrt(2.0));
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) self_[j][cc] = (o < ns && si) ? si[3 * o + cc] : 0.0;
+  }
+  const int NL = N * L1;
+  // the derivatives of component (n, n', l) of pair q; a_, b_ = n L1 + l, n' L1 + l
+  auto deriv1 = [&](int q, int a_, int b_, double pf, double &vr, double &va, double &vp) {
+    const double *Pp = sPQ + (size_t)(q * 4) * NL, *Q = Pp + NL, *Qa = Q + NL, *Qo = Qa + NL;
+    const double *R = sR + q * 2 * N;
+    const int n = a_ / L1, np = b_ / L1;
+    const double rn = R[n], rdn = R[N + n], rnp = R[np], rdnp = R[N + np];
+    vr = pf * (rdn * Pp[b_] + rn * Q[b_] + rdnp * Pp[a_] + rnp * Q[a_]);
+    va = pf * (rn * Qa[b_] + rnp * Qa[a_]);
+    vp = pf * (rn * Qo[b_] + rnp * Qo[a_]);
+  };
+  auto deriv = [&](int q, int j, double &vr, double &va, double &vp) {
+    if (P.cmap_identity) {
+      deriv1(q, ia[j], ib[j], pre[j], vr, va, vp);
+      return;
+    }
+    const int o = tid + j * NT;
+    vr = va = vp = 0.0;
+    for (int t = P.pi_off[o]; t < P.pi_off[o + 1]; ++t) {
+      const double el = P.pi_el64[t];
+      const int cq = P.kept_nnl[P.pi_q[t]];
+      const int n = cq & 0xff, np = (cq >> 8) & 0xff, l = cq >> 16;
+      double r_, a_, p_;
+      deriv1(q, n * L1 + l, np * L1 + l, kFourPi64 * ((n == np) ? 1.0 : sqrt(2.0)), r_, a_, p_);
+      vr = vr + el * r_;
+      va = va + el * a_;
+      vp = vp + el * p_;
+    }
+  };
+
+  for (int kb = p0 + 1; kb < p1; kb += kC3Pairs) {
+    const int nb = min(kC3Pairs, p1 - kb);
+    __syncthreads();  // the previous batch's readers are done
+    for (int t = tid; t < nb * 4 * K; t += NT) {
+      const int q = t / (4 * K), r = t - q * 4 * K, pl = r / K, kk = r - pl * K;
+      sA[(q * 4 + pl) * K + kk] = ang[pl * plane + (size_t)(kb + q) * K + kk];
+    }
+    for (int t = tid; t < nb * 2 * N; t += NT) {
+      const int q = t / (2 * N), r = t - q * 2 * N;
+      sR[q * 2 * N + r] = r < N ? rad[(size_t)(kb + q) * N + r] : rad_der[(size_t)(kb + q) * N + r - N];
+    }
+    if (tid < nb) {
+      const int k = kb + tid;
+      double st, ct, sf, cf;
+      sincos(B.thetas[k], &st, &ct);
+      sincos(B.phis[k], &sf, &cf);
+      const double ir = 1.0 / B.rjs[k];
+      double *rt = sRot + 8 * tid;
+      rt[0] = st * cf; rt[1] = st * sf; rt[2] = ct;
+      rt[3] = -ct * cf * ir; rt[4] = -ct * sf * ir; rt[5] = st * ir;
+      rt[6] = -sf * ir; rt[7] = cf * ir;
+    }
+    __syncthreads();
+    // ---- P, Q, Qa, Qo: warp 2q + h, lane n: planes 2h, 2h + 1 of pair q
+    {
+      const int q = warp >> 1, h = warp & 1, n = lane;
+      if (q < nb && n < N) {
+        const double2 *A0 = sA + (q * 4 + 2 * h) * K, *A1 = A0 + K;
+        const double2 *cn = sC + n * kC3Kp;
+        double *o0 = sPQ + (size_t)(q * 4 + 2 * h) * NL + n * L1, *o1 = o0 + NL;
+#pragma unroll
+        for (int l = 0; l <= LC; ++l) {
+          double s0 = 0.0, s1 = 0.0;
+          if (l <= L) {
+#pragma unroll
+            for (int m = 0; m <= l; ++m) {
+              const int kk = l * (l + 1) / 2 + m;
+              const double w = (m == 0) ? 1.0 : 2.0;
+              const double2 cc = cn[kk], a0 = A0[kk], a1 = A1[kk];
+              s0 = s0 + w * (a0.x * cc.x + a0.y * cc.y);
+              s1 = s1 + w * (a1.x * cc.x + a1.y * cc.y);
+            }
+          }
+          o0[l] = s0;
+          o1[l] = s1;
+        }
+      }
+    }
+    __syncthreads();
+    // ---- the compressed spherical derivatives (:1999-2066): pass 1, each
+    // pair's dots with p, reduced in a fixed order (warp shuffles, then the
+    // eight warps in order)
+#pragma unroll 1
+    for (int q = 0; q < nb; ++q) {
+      double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+#pragma unroll
+      for (int j = 0; j < OPT; ++j) {
+        const int o = tid + j * NT;
+        if (o >= ns) continue;
+        double vr, va, vp;
+        deriv(q, j, vr, va, vp);
+        d0 += sv[o] * vr;
+        d1 += sv[o] * va;
+        d2 += sv[o] * vp;
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        d0 += __shfl_xor_sync(0xffffffffu, d0, off);
+        d1 += __shfl_xor_sync(0xffffffffu, d1, off);
+        d2 += __shfl_xor_sync(0xffffffffu, d2, off);
+      }
+      if (lane == 0) {
+        sRed[(q * 3 + 0) * 8 + warp] = d0;
+        sRed[(q * 3 + 1) * 8 + warp] = d1;
+        sRed[(q * 3 + 2) * 8 + warp] = d2;
+      }
+    }
+    __syncthreads();
+    // ---- pass 2: the Cartesian columns, and the self column in registers
+#pragma unroll 1
+    for (int q = 0; q < nb; ++q) {
+      double dr = 0.0, da = 0.0, dp = 0.0;
+#pragma unroll
+      for (int w = 0; w < NT / 32; ++w) {
+        dr += sRed[(q * 3 + 0) * 8 + w];
+        da += sRed[(q * 3 + 1) * 8 + w];
+        dp += sRed[(q * 3 + 2) * 8 + w];
+      }
+      const double *rt = sRot + 8 * q;
+      const double cx = rt[0], cy = rt[1], cz = rt[2], px = rt[3], py = rt[4], pz = rt[5], ax = rt[6], ay = rt[7];
+      double *out = cart + (size_t)(kb + q) * w3;
+#pragma unroll
+      for (int j = 0; j < OPT; ++j) {
+        const int o = tid + j * NT;
+        if (o >= ns) continue;
+        double vr, va, vp;
+        deriv(q, j, vr, va, vp);
+        const double s = sv[o];
+        const double r_ = vr * inv_p - s * inv_p3 * dr;
+        const double a_ = va * inv_p - s * inv_p3 * da;
+        const double o_ = vp * inv_p - s * inv_p3 * dp;
+        const double x = cx * r_ + px * o_ + ax * a_, y = cy * r_ + py * o_ + ay * a_, z = cz * r_ + pz * o_;
+        out[3 * o] = x;
+        out[3 * o + 1] = y;
+        out[3 * o + 2] = z;
+        self_[j][0] -= x;
+        self_[j][1] -= y;
+        self_[j][2] -= z;
+      }
+    }
+  }
+  double *out = cart + (size_t)p0 * w3;
+#pragma unroll
+  for (int j = 0; j < OPT; ++j) {
+    const int o = tid + j * NT;
+    if (o < ns) {
+      out[3 * o] = self_[j][0];
+      out[3 * o + 1] = self_[j][1];
+      out[3 * o + 2] = self_[j][2];
+    }
+  }
+}
+
 // ---- pair = sgn * sum_s G(i,s) soap_cart_der(:, s, k): one CTA per site with
 // the site's G row in shared memory, one warp per pair; lane j takes the
 // components o = j, j + 32, ... (a warp's three loads of a step cover 768
@@ -750,7 +984,14 @@ cudaError_t launch_fp64_descriptor(const DevParams &P, const DevBatch &B, cudaSt
   }
   if (do_der && cart && np > 0 && nsites > 0) {
     const size_t sm2 = (size_t)cart2_smem(P).total * sizeof(double);
-    if (P.n_soap <= 3 * kCartThreads && sm2 <= kCartSmemCap) {
+    const size_t sm3 = (size_t)cart3_smem(P).total * sizeof(double);
+    if (P.n_max <= 32 && P.l_max <= 8 && P.n_soap <= 3 * 256 && sm3 <= kCartSmemCap) {
+      auto kern = k64_cart_site3<8>;
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3);
+      if (e != cudaSuccess) return e;
+      kern<<<nsites, 256, sm3, s>>>(P, B, w.rad, w.rad_der, (const double2 *)w.ang, (const double2 *)w.cnk,
+                                    w.soap_unnorm, w.norm, self_init, cart);
+    } else if (P.n_soap <= 3 * kCartThreads && sm2 <= kCartSmemCap) {
       auto kern = k64_cart_site2<kCartThreads, 3>;
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
       if (e != cudaSuccess) return e;

@@ -258,6 +258,8 @@ __global__ void __launch_bounds__(kPairThreads)
   const int k = k0 + threadIdx.x;
   bool active = false;
   double x = 0.0, sq = 0.0;
+  unsigned tab_todo = 0u;  // TAB: the species whose tables this pair is evaluated against
+  double tab_r = 0.0;
   float *row = rows + threadIdx.x * AWS;
   if (k < pair_hi) {
     const unsigned bits = prep_pair(B, k, P.n_species);
@@ -288,6 +290,11 @@ __global__ void __launch_bounds__(kPairThreads)
         const RadSp &RS = *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
         if (((bits >> s) & 1u) && r < RS.rcut_hard) todo |= 1u << s;
       }
+      if constexpr (TAB) {
+        tab_todo = todo;
+        tab_r = r;
+        todo = 0u;
+      }
       // species are data, not control flow: lanes of different species share
       // one expansion call
       while (todo) {
@@ -295,19 +302,6 @@ __global__ void __launch_bounds__(kPairThreads)
         todo &= todo - 1u;
         const RadSp &RS = *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
         float4 *o = (float4 *)(B.rad + ((size_t)k * P.n_species + s) * 2 * AMAX);
-        if constexpr (TAB) {
-          float v[2 * AMAX];
-          radial_from_table<AMAX>(P, RS, P.rtab_sp[s], r, do_der != 0, v);
-#pragma unroll
-          for (int n4 = 0; n4 < AMAX / 4; ++n4)
-            o[n4] = make_float4(v[4 * n4], v[4 * n4 + 1], v[4 * n4 + 2], v[4 * n4 + 3]);
-          if (do_der)
-#pragma unroll
-            for (int n4 = 0; n4 < AMAX / 4; ++n4)
-              o[AMAX / 4 + n4] = make_float4(v[AMAX + 4 * n4], v[AMAX + 4 * n4 + 1], v[AMAX + 4 * n4 + 2],
-                                             v[AMAX + 4 * n4 + 3]);
-          continue;
-        }
         double val[AMAX], der[AMAX];
         radial_entry<AMAX, OP>(P, RS, sW + s * AMAX * AMAX, r, false, do_der != 0, val, der);
         const double g4 = kFourPi * RS.gscale;
@@ -320,6 +314,49 @@ __global__ void __launch_bounds__(kPairThreads)
           for (int n4 = 0; n4 < AMAX / 4; ++n4)
             o[AMAX / 4 + n4] = make_float4((float)(g4 * der[4 * n4]), (float)(g4 * der[4 * n4 + 1]),
                                            (float)(g4 * der[4 * n4 + 2]), (float)(g4 * der[4 * n4 + 3]));
+      }
+    }
+  }
+  if constexpr (TAB) {
+    // R_n and dR_n/dr from the tables, a warp's entries of one species at a
+    // time: 2 AMAX lanes per entry, lane f evaluating function f, so that the
+    // segment's coefficients (stored [degree][function]) are read and the
+    // entry's radial row is written as contiguous 64-byte runs
+    constexpr int G = 2 * AMAX, EPW = 32 / G;
+    static_assert(32 % G == 0, "lanes per entry");
+    const int lane = threadIdx.x & 31, f = lane % G, sub = lane / G;
+    const int nf = do_der ? G : AMAX;
+    for (int s = 0; s < P.n_species; ++s) {
+      const bool mine = (tab_todo >> s) & 1u;
+      unsigned m = __ballot_sync(0xffffffffu, mine);
+      if (!m) continue;
+      float t = 0.f;
+      int cb = -1;
+      if (mine) {
+        const RadSp &RS = *(const RadSp *)(smem + P.off_rad + (size_t)s * SOAPB_RADSP_BYTES);
+        cb = radial_table_locate<AMAX>(P, RS, P.rtab_sp[s], tab_r, t);
+      }
+      while (m) {
+        unsigned mm = m;
+#pragma unroll
+        for (int i = 0; i < EPW - 1; ++i)
+          if (i < sub) mm &= mm - 1u;
+#pragma unroll
+        for (int i = 0; i < EPW; ++i) m &= m - 1u;
+        const int src = mm ? __ffs(mm) - 1 : 0;
+        const int cbe = __shfl_sync(0xffffffffu, cb, src);
+        const float te = __shfl_sync(0xffffffffu, t, src);
+        if (mm && f < nf) {
+          float a = 0.f;
+          if (cbe >= 0) {
+            const float *c = P.rtab_coef + cbe + f;
+            a = c[kRadTabDeg * G];
+#pragma unroll
+            for (int d = kRadTabDeg - 1; d >= 0; --d) a = fmaf(a, te, c[d * G]);
+          }
+          const int ke = k0 + (threadIdx.x & ~31) + src;
+          B.rad[((size_t)ke * P.n_species + s) * G + f] = a;
+        }
       }
     }
   }
@@ -904,7 +941,7 @@ __global__ void __launch_bounds__(NT) k_descriptor_tc(const DevParams P, const D
                                                       double *__restrict__ soap_out, float *__restrict__ keep_c,
                                                       double *__restrict__ keep_norm, int keep) {
   static_assert(NT == 128, "one thread per TMEM lane");
-  extern __shared__ __align__(1024) unsigned char smem[];
+  extern __shared__ __align__(16) unsigned char smem[];  // no-swizzle operand tiles need 16-byte alignment
   const int AS = stage_stride(LC, 0);
   const TdLayout Ly = make_td_layout(P, NT, AMAX, LC);
   const int *klm = (const int *)SBLOB(off_klm);
@@ -1548,7 +1585,7 @@ __global__ void __launch_bounds__(NT) k_contract_tc(const DevParams P, const Dev
   constexpr int AW = row_len(LC);
   constexpr int O_IL = row_il(LC), O_ILD = row_ild(LC), O_ER = row_er(LC), O_EI = row_ei(LC),
                 O_SF = row_sf(LC), O_X = row_x(LC), O_SQ = row_sq(LC), O_P = row_p(LC);
-  extern __shared__ __align__(1024) unsigned char smem[];
+  extern __shared__ __align__(16) unsigned char smem[];  // no-swizzle operand tiles need 16-byte alignment
   const TcLayout Ly = make_tc_layout(P, NT, AMAX);
   const float4 *kcoef = (const float4 *)SBLOBC(off_kcoef);
   const int *nmap = (const int *)SBLOBC(off_nmap);
