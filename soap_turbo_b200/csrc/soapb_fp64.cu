@@ -112,34 +112,31 @@ __global__ void k64_angular(const DevParams P, const DevBatch B, int do_der, dou
 // l and l + 1 only (the recursion of get_plm_array, src/soap_turbo_angular.f90:
 // 108-160), every loop unrolled so that they stay in registers, and each (l, m)
 // written as soon as rows l and l + 1 exist (the derivative forms need
-// P_{l+1}^{m+-1}, :181-248).  Same arithmetic as k64_angular.
+// P_{l+1}^{m+-1}, :181-248).  With derivatives the CTA is four warps over the
+// same 32 pairs, warp w writing plane w (the expansion, its radial, azimuthal
+// and polar derivative), so that a pair's four planes are formed at once;
+// without, one warp writes the expansion.  Same arithmetic as k64_angular.
 template <int LC>
 __global__ void __launch_bounds__(128, 4) k64_angular2(const DevParams P, const DevBatch B, int do_der, double2 *ang) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pl = do_der ? (int)(threadIdx.x >> 5) : 0;  // warp-uniform
+  const int k = blockIdx.x * 32 + (threadIdx.x & 31);
   if (k >= B.n_pairs) return;
   const int K = P.k_max, L = P.l_max;
   const size_t plane = (size_t)B.n_pairs * K;
-  double2 *A = ang + (size_t)k * K;
+  double2 *A = ang + pl * plane + (size_t)k * K;
   const double r = B.rjs[k];
   const unsigned bits = B.bits[k];
   if (!(r < P.rcut_max) || bits == 0u) {
-    for (int kk = 0; kk < K; ++kk) {
-      A[kk] = make_double2(0.0, 0.0);
-      if (do_der) {
-        A[plane + kk] = make_double2(0.0, 0.0);
-        A[2 * plane + kk] = make_double2(0.0, 0.0);
-        A[3 * plane + kk] = make_double2(0.0, 0.0);
-      }
-    }
+    for (int kk = 0; kk < K; ++kk) A[kk] = make_double2(0.0, 0.0);
     return;
   }
   AngScalars<LC> S;
-  angular_scalars<LC>(P, __ffs(bits) - 1, r, B.thetas[k], B.phis[k], do_der != 0, S);
+  angular_scalars<LC>(P, __ffs(bits) - 1, r, B.thetas[k], B.phis[k], pl == 1, S);
   const double x = S.x, sq = S.sq, x2 = x * x;
-  // rows: pm (l - 1), pc (l), pn (l + 1); m <= l + 1 <= LC + 1
-  double pm[LC + 2], pc[LC + 2], pn[LC + 2];
+  // rows: pc (l), pn (l + 1); m <= l + 1 <= LC + 1
+  double pc[LC + 2], pn[LC + 2];
 #pragma unroll
-  for (int m = 0; m < LC + 2; ++m) pm[m] = pc[m] = pn[m] = 0.0;
+  for (int m = 0; m < LC + 2; ++m) pc[m] = pn[m] = 0.0;
   pc[0] = 1.0;        // l = 0
   pn[0] = x;          // l = 1
   pn[1] = -sq;
@@ -152,23 +149,23 @@ __global__ void __launch_bounds__(128, 4) k64_angular2(const DevParams P, const 
       const double e_re = S.il[l] * S.er[m], e_im = S.il[l] * S.ei[m];
       const double u = S.amp * P.preflm64[kk];
       const double v = u * pc[m];
-      A[kk] = make_double2(v * e_re, v * e_im);
-      if (do_der) {
+      if (pl == 0) {
+        A[kk] = make_double2(v * e_re, v * e_im);
+      } else if (pl == 1) {
         const double er_re = S.ild[l] * S.er[m], er_im = S.ild[l] * S.ei[m];
-        A[plane + kk] = make_double2(v * er_re - S.sig_fac * v * e_re, v * er_im - S.sig_fac * v * e_im);
-        double dms, dvs;
-        if (m == 0) {
-          dms = (l == 0) ? 0.0 : -0.5 * pc[1];
-          dvs = 0.0;
-        } else {
-          dms = 0.5 * (double)(l + m) * (double)(l - m + 1) * pc[m - 1];
-          dvs = 0.5 * (double)(l - m + 1) * (double)(l - m + 2) * pn[m - 1] + 0.5 * pn[m + 1];
-        }
-        if (m != l) dms = dms + -0.5 * pc[m + 1];
+        A[kk] = make_double2(v * er_re - S.sig_fac * v * e_re, v * er_im - S.sig_fac * v * e_im);
+      } else if (pl == 2) {
+        const double dvs =
+            (m == 0) ? 0.0 : 0.5 * (double)(l - m + 1) * (double)(l - m + 2) * pn[m - 1] + 0.5 * pn[m + 1];
         const double w = u * dvs;
-        A[2 * plane + kk] = make_double2(-(w * e_im), w * e_re);
+        A[kk] = make_double2(-(w * e_im), w * e_re);
+      } else {
+        double dms;
+        if (m == 0) dms = (l == 0) ? 0.0 : -0.5 * pc[1];
+        else dms = 0.5 * (double)(l + m) * (double)(l - m + 1) * pc[m - 1];
+        if (m != l) dms = dms + -0.5 * pc[m + 1];
         const double w2 = u * dms;
-        A[3 * plane + kk] = make_double2(w2 * e_re, w2 * e_im);
+        A[kk] = make_double2(w2 * e_re, w2 * e_im);
       }
     }
     // advance: row l + 2 from rows l + 1 (pn) and l (pc)
@@ -192,12 +189,10 @@ __global__ void __launch_bounds__(128, 4) k64_angular2(const DevParams P, const 
     }
 #pragma unroll
     for (int m = 0; m < LC + 2; ++m) {
-      pm[m] = pc[m];
       pc[m] = pn[m];
       pn[m] = nn[m];
     }
   }
-  (void)pm;
 }
 
 // ---- c_nlm, one CTA per site, threads over (n, k) (src/soap_turbo.f90:626-664).
@@ -658,6 +653,9 @@ __global__ void __launch_bounds__(NT, 3) k64_cart_site2(const DevParams P, const
 
 // ---- soap_cart_der for n_max <= 32, l_max <= 8, n_soap <= 3 x 256: the CTA
 // takes its site's pairs kC3Pairs at a time.
+//  * the next batch's angular planes and radial values are copied
+//    asynchronously into a second buffer, and its rotations formed, while a
+//    batch computes;
 //  * P, Q, Qa, Qo: two warps per pair, lane n summing sum_m w_m Re(X_lm conj
 //    c_nlm) over every (l, m) for two of the four planes X in registers (the
 //    angular values broadcast from shared memory, c_nlm rows padded to 49 so
@@ -670,6 +668,17 @@ __global__ void __launch_bounds__(NT, 3) k64_cart_site2(const DevParams P, const
 //    together, in a fixed order), then forms the derivatives again to write the
 //    columns (cheaper than holding them: the registers would halve the CTAs
 //    per SM).
+__device__ __forceinline__ void cp_async_16(void *dst_smem, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_8(void *dst_smem, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 constexpr int kC3Pairs = 4;
 constexpr int kC3Kp = 49;  // padded c_nlm row (double2), k_max <= 45
 constexpr int kC3L1 = 9;   // P, Q rows of l_max + 1 <= 9 entries
@@ -682,11 +691,11 @@ __host__ __device__ inline Cart3Smem cart3_smem(const DevParams &P) {
   // the double2 arrays first, at even offsets (16-byte aligned), then the doubles
   int o = 0;
   L.C = o;   o += 2 * N * kC3Kp;
-  L.A = o;   o += kC3Pairs * 8 * K;
+  L.A = o;   o += 2 * kC3Pairs * 8 * K;  // two buffers: this batch, the next
   L.PQ = o;  o += kC3Pairs * 4 * N * kC3L1;
-  L.R = o;   o += kC3Pairs * 2 * N;
+  L.R = o;   o += 2 * kC3Pairs * 2 * N;  // two buffers
   L.sv = o;  o += P.n_soap;
-  L.rot = o; o += kC3Pairs * 8;
+  L.rot = o; o += 2 * kC3Pairs * 8;      // two buffers
   L.red = o; o += 8 * 3 * kC3Pairs;
   L.total = o;
   return L;
@@ -737,10 +746,11 @@ __global__ void __launch_bounds__(256, 2) k64_cart_site3(const DevParams P, cons
     for (int cc = 0; cc < 3; ++cc) self_[j][cc] = (o < ns && si) ? si[3 * o + cc] : 0.0;
   }
   const int NL = N * L1;
+  const double *cR = sR;  // the current batch's radial values (set per batch)
   // the derivatives of component (n, n', l) of pair q; a_, b_ = n L1 + l, n' L1 + l
   auto deriv1 = [&](int q, int a_, int b_, double pf, double &vr, double &va, double &vp) {
     const double *Pp = sPQ + (size_t)(q * 4) * NL, *Q = Pp + NL, *Qa = Q + NL, *Qo = Qa + NL;
-    const double *R = sR + q * 2 * N;
+    const double *R = cR + q * 2 * N;
     const int n = a_ / L1, np = b_ / L1;
     const double rn = R[n], rdn = R[N + n], rnp = R[np], rdnp = R[N + np];
     vr = pf * (rdn * Pp[b_] + rn * Q[b_] + rdnp * Pp[a_] + rnp * Q[a_]);
@@ -766,34 +776,63 @@ __global__ void __launch_bounds__(256, 2) k64_cart_site3(const DevParams P, cons
     }
   };
 
-  for (int kb = p0 + 1; kb < p1; kb += kC3Pairs) {
-    const int nb = min(kC3Pairs, p1 - kb);
-    __syncthreads();  // the previous batch's readers are done
-    for (int t = tid; t < nb * 4 * K; t += NT) {
+  const int szA = kC3Pairs * 4 * K, szR = kC3Pairs * 2 * N;
+  // a batch's angular planes and radial values, copied asynchronously into
+  // buffer b while the previous batch computes, and its rotations (FP64
+  // sincos), formed by the CTA's last kC3Pairs threads during that batch
+  auto stage = [&](int b, int kb_) {
+    const int nb_ = min(kC3Pairs, p1 - kb_);
+    double2 *dA = sA + b * szA;
+    double *dR = sR + b * szR;
+    for (int t = tid; t < nb_ * 4 * K; t += NT) {
       const int q = t / (4 * K), r = t - q * 4 * K, pl = r / K, kk = r - pl * K;
-      sA[(q * 4 + pl) * K + kk] = ang[pl * plane + (size_t)(kb + q) * K + kk];
+      cp_async_16(dA + (q * 4 + pl) * K + kk, ang + pl * plane + (size_t)(kb_ + q) * K + kk);
     }
-    for (int t = tid; t < nb * 2 * N; t += NT) {
+    for (int t = tid; t < nb_ * 2 * N; t += NT) {
       const int q = t / (2 * N), r = t - q * 2 * N;
-      sR[q * 2 * N + r] = r < N ? rad[(size_t)(kb + q) * N + r] : rad_der[(size_t)(kb + q) * N + r - N];
+      cp_async_8(dR + t, r < N ? rad + (size_t)(kb_ + q) * N + r : rad_der + (size_t)(kb_ + q) * N + r - N);
     }
-    if (tid < nb) {
-      const int k = kb + tid;
+    cp_async_commit();
+  };
+  auto rotation = [&](int b, int kb_) {
+    const int j = tid - (NT - kC3Pairs);
+    if (j >= 0 && j < min(kC3Pairs, p1 - kb_)) {
+      const int k = kb_ + j;
       double st, ct, sf, cf;
       sincos(B.thetas[k], &st, &ct);
       sincos(B.phis[k], &sf, &cf);
       const double ir = 1.0 / B.rjs[k];
-      double *rt = sRot + 8 * tid;
+      double *rt = sRot + b * kC3Pairs * 8 + 8 * j;
       rt[0] = st * cf; rt[1] = st * sf; rt[2] = ct;
       rt[3] = -ct * cf * ir; rt[4] = -ct * sf * ir; rt[5] = st * ir;
       rt[6] = -sf * ir; rt[7] = cf * ir;
     }
+  };
+  if (p0 + 1 < p1) {
+    stage(0, p0 + 1);
+    rotation(0, p0 + 1);
+  }
+
+  int buf = 0;
+  for (int kb = p0 + 1; kb < p1; kb += kC3Pairs, buf ^= 1) {
+    const int nb = min(kC3Pairs, p1 - kb);
+    __syncthreads();  // the previous batch's readers are done, buffer buf ^ 1 is free
+    const bool more = kb + kC3Pairs < p1;
+    if (more) {
+      stage(buf ^ 1, kb + kC3Pairs);
+      cp_async_wait_1();
+    } else {
+      cp_async_wait_0();
+    }
     __syncthreads();
+    const double2 *cA = sA + buf * szA;
+    cR = sR + buf * szR;
+    const double *cRot = sRot + buf * kC3Pairs * 8;
     // ---- P, Q, Qa, Qo: warp 2q + h, lane n: planes 2h, 2h + 1 of pair q
     {
       const int q = warp >> 1, h = warp & 1, n = lane;
       if (q < nb && n < N) {
-        const double2 *A0 = sA + (q * 4 + 2 * h) * K, *A1 = A0 + K;
+        const double2 *A0 = cA + (q * 4 + 2 * h) * K, *A1 = A0 + K;
         const double2 *cn = sC + n * kC3Kp;
         double *o0 = sPQ + (size_t)(q * 4 + 2 * h) * NL + n * L1, *o1 = o0 + NL;
 #pragma unroll
@@ -843,6 +882,7 @@ __global__ void __launch_bounds__(256, 2) k64_cart_site3(const DevParams P, cons
         sRed[(q * 3 + 2) * 8 + warp] = d2;
       }
     }
+    if (more) rotation(buf ^ 1, kb + kC3Pairs);
     __syncthreads();
     // ---- pass 2: the Cartesian columns, and the self column in registers
 #pragma unroll 1
@@ -854,7 +894,7 @@ __global__ void __launch_bounds__(256, 2) k64_cart_site3(const DevParams P, cons
         da += sRed[(q * 3 + 1) * 8 + w];
         dp += sRed[(q * 3 + 2) * 8 + w];
       }
-      const double *rt = sRot + 8 * q;
+      const double *rt = cRot + 8 * q;
       const double cx = rt[0], cy = rt[1], cz = rt[2], px = rt[3], py = rt[4], pz = rt[5], ax = rt[6], ay = rt[7];
       double *out = cart + (size_t)(kb + q) * w3;
 #pragma unroll
@@ -965,7 +1005,7 @@ cudaError_t launch_fp64_descriptor(const DevParams &P, const DevBatch &B, cudaSt
       if (op) k64_radial<16, true><<<blocks, 128, 0, s>>>(P, B, do_der, w.rad, w.rad_der);
       else k64_radial<16, false><<<blocks, 128, 0, s>>>(P, B, do_der, w.rad, w.rad_der);
     }
-    if (P.l_max <= 8) k64_angular2<8><<<blocks, 128, 0, s>>>(P, B, do_der, (double2 *)w.ang);
+    if (P.l_max <= 8) k64_angular2<8><<<(np + 31) / 32, do_der ? 128 : 32, 0, s>>>(P, B, do_der, (double2 *)w.ang);
     else k64_angular<12><<<blocks, 128, 0, s>>>(P, B, do_der, (double2 *)w.ang);
     nl += 2;
   }
