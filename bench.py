@@ -274,6 +274,12 @@ def hbm_peak():
     return 6650.0
 
 
+def hbm_peak_source():
+    if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")):
+        return "measured (MEASURED_PEAKS.json)"
+    return "fallback: 6.65 TB/s, an earlier copy measurement on this pool's B200s (no MEASURED_PEAKS.json)"
+
+
 def gemm_peak_tflops(torch, dtype):
     """CUDA-core peak measured here: cuBLAS SGEMM with TF32 disabled (FP32)
     or DGEMM (FP64), 8192^3, best of 4."""
@@ -546,8 +552,9 @@ def run_ours(args):
     t_e2e = shard.max_over_ranks(wall(e2e_step, n_e2e, h_soap), device=dev)
     t_e2e_py = shard.max_over_ranks(wall(e2e_step_python, n_e2e, h_soap), device=dev)
     t_e2e_pg = shard.max_over_ranks(wall(e2e_step_pageable, n_e2e, pg["soap"]), device=dev)
+    # soap goes in twice: get_soap adds into it, soap_contract reads it beside G
     h2d = (h_nn.nbytes + h_sp.nbytes + h_sm.nbytes + h_mask.nbytes + h_rjs.nbytes + h_th.nbytes +
-           h_ph.nbytes + h_soap.nbytes + h_G.nbytes)
+           h_ph.nbytes + 2 * h_soap.nbytes + h_G.nbytes)
     d2h = h_soap.nbytes + h_pair.nbytes
 
     # ---- roofline of the dominant kernel: the one with the largest device time
@@ -583,9 +590,11 @@ def run_ours(args):
             "data": "synthetic (seeded random periodic structures of the configuration's shape)",
             "config": {"workload": wname, "sites_per_gpu": nl.n_sites, "pairs_per_gpu": nl.n_pairs,
                        "step": "get_soap(do_derivatives, contract) + soap_contract(G), G~N(0,1)",
-                       "precision": "FP32 pair/contraction arithmetic; FP64 radial integrals, "
-                                    "W transform, i_l and e^{-im phi}; FP64 accumulation of c_nlm "
-                                    "over groups of 4 pairs",
+                       "precision": "FP32 pair/contraction arithmetic; R_n and dR_n/dr from "
+                                    "piecewise polynomials fitted to the FP64 expansion and "
+                                    "evaluated in FP32 (checked to 5e-7 at context creation); "
+                                    "FP64 i_l and e^{-im phi}; FP64 accumulation of c_nlm over "
+                                    "groups of 4 pairs",
                        "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"site shards, {ws} GPU(s), no data-path collective"},
             "kernel_ms": kernel_ms,
@@ -627,7 +636,7 @@ def run_ours(args):
                                   "frac_of_fp32": flops["total"] / (ms_step_max * 1e-3) / 1e12 / peak32},
                          "hbm": {"algorithmic_bytes_per_launch": algorithmic_bytes(w).get(dominant),
                                  "algorithmic_GBps": (algorithmic_bytes(w).get(dominant) or 0.0) / t_dom / 1e9,
-                                 "peak_GBps": hbm_peak(), "peak_source": "measured (MEASURED_PEAKS.json)"}},
+                                 "peak_GBps": hbm_peak(), "peak_source": hbm_peak_source()}},
             "clocks": clk.summary(),
         }
         if ws == 1:
@@ -867,6 +876,7 @@ def run_fp64(args):
                       "warmup": args.warmup, "gpu_launches_per_step": launches,
                       "soap_cart_der_bytes": cart_bytes,
                       "hbm_floor_ms": 2 * cart_bytes / (hbm_peak() * 1e9) * 1e3,
+                      "hbm_peak_source": hbm_peak_source(),
                       "config": {"workload": WORKLOAD if args.config == 2 else CONFIG_NAMES[args.config],
                                  "sites": nl.n_sites, "pairs": nl.n_pairs}}), flush=True)
 

@@ -634,15 +634,20 @@ template <int LC, bool DER>
 __device__ __forceinline__ void angular_stage(const DevParams &P, int i_sp, double rj, double theta,
                                               double phi, float *out, int o_il, int o_ild, int o_er,
                                               int o_ei, int o_amp, int o_sf, double &x, double &sq) {
+  // The pair kernel rounds everything below to FP32, so the quotients of the
+  // reference's expressions are taken as products with one reciprocal each of
+  // sigma, x^2 and r (an FP64 division is a long dependent sequence; these are
+  // the kernel's critical path), which moves the FP64 values by an ulp or so.
   const int L = P.l_max;
   const double sig = P.sig_t[i_sp] + P.sig_t_c[i_sp] * rj;               // :579-580
-  const double amp = P.rcut2 / (sig * sig);
+  const double isig = 1.0 / sig;
+  const double amp = P.rcut2 * (isig * isig);
   out[o_amp] = (float)amp;
   x = cos(theta);
   sq = sqrt(1.0 - x * x);
   // i_l(x^2) exp(-x^2) (src/soap_turbo_angular.f90:361-422) and its radial
   // derivative (:436-463), streamed over l
-  const double xx = rj / sig;
+  const double xx = rj * isig;
   const double xcut = 1.0e-7;
   const double x2 = xx * xx, x4 = x2 * x2;
   const double inv_x2 = (x2 > 0.0) ? 1.0 / x2 : 0.0;
@@ -650,14 +655,14 @@ __device__ __forceinline__ void angular_stage(const DevParams &P, int i_sp, doub
   double flm2, flm1;
   if (xx > 0.0) {
     const double e2 = exp(-2.0 * x2);
-    flm2 = fabs((1.0 - e2) / 2.0 / x2);
-    flm1 = fabs((x2 - 1.0 + e2 * (x2 + 1.0)) / 2.0 / x4);
+    flm2 = fabs((1.0 - e2) * 0.5 * inv_x2);
+    flm1 = fabs((x2 - 1.0 + e2 * (x2 + 1.0)) * 0.5 * (inv_x2 * inv_x2));
   } else {
     flm2 = 1.0;
     flm1 = 0.0;
   }
   const double sc = P.sig_t_c[i_sp];
-  const double c1 = 2.0 * rj / (sig * sig), c2 = 1.0 - sc * rj / sig;
+  const double c1 = 2.0 * rj * (isig * isig), c2 = 1.0 - sc * rj * isig;
   const bool dz = !(rj >= 1.0e-5);
   const double irj = dz ? 0.0 : 1.0 / rj;  // one division for every l below
   double fact = 1.0, il_prev = 0.0, il0 = 0.0;
@@ -692,9 +697,11 @@ __device__ __forceinline__ void angular_stage(const DevParams &P, int i_sp, doub
     }
     il_prev = il;
   }
-  if (DER) out[o_sf] = (float)(2.0 * sc / sig);                         // :589
+  if (DER) out[o_sf] = (float)(2.0 * sc * isig);                         // :589
   // e^{-i m phi}, Chebyshev recursion of get_eimphi_conjg (:284-298)
-  double cosm2 = cos(phi), sinm2 = -sin(phi);
+  double sphi, cphi;
+  sincos(phi, &sphi, &cphi);
+  double cosm2 = cphi, sinm2 = -sphi;
   const double cosphi2 = 2.0 * cosm2;
   double cosm1 = 1.0, sinm1 = 0.0;
   out[o_er] = 1.f;
