@@ -284,6 +284,8 @@ struct soapb_context {
   int tune_td = 0, tune_cd = 0, tune_tc = 0, tune_cc = 0;
   int64_t launches = 0;
   int keep_valid = 0, keep_sites = 0, keep_pairs = 0;
+  DBuf order;           // the last whole-batch descriptor call's site order
+  int order_sites = -1; // its batch's site count (-1: none)
   // the error word of the last call that checked inputs: the context's own
   // (err), or the static scratch array's after soapb_descriptor_noalloc
   unsigned long long *last_err = nullptr;
@@ -311,7 +313,7 @@ struct soapb_context {
 
   ~soapb_context() {
     timing_release();
-    for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &rad, &ang, &f64_rad, &f64_rad_der,
+    for (DBuf *b : {&tables, &off, &bits, &err, &keep_c, &keep_norm, &order, &rad, &ang, &f64_rad, &f64_rad_der,
                     &f64_ang, &f64_cnk, &f64_soap_un, &f64_norm, &hs_rad_der2, &hs_geo, &hs_good, &hs_scratch, &hs_soap,
                     &hs_ticket, &hs_vchunk, &hs_hchunk, &nb_acell, &nb_ccount, &nb_cstart,
                     &nb_cfill, &nb_catoms, &nb_counts, &nb_off, &nb_state, &nb_rjs, &nb_th, &nb_ph,
@@ -1141,6 +1143,13 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
   // the pair kernel also scans n_neigh into the CSR offsets, packs the mask
   // and checks the inputs (its first launch scans, when it runs per chunk)
   const bool pair_chunks = ch && ch->site_off && b->n_sites > 0;
+  // a batch one scan tile covers, run whole: the scan orders its sites
+  // heaviest first for the site kernels (and the contract that follows)
+  c->order_sites = -1;
+  if (!ch && b->n_sites > 0 && b->n_sites <= kScanTileSites) {
+    if ((rc = c->order.ensure(sizeof(int) * (size_t)b->n_sites))) return rc;
+    B.order = c->order.as<int>();
+  }
   if (!pair_chunks && (b->n_atom_pairs > 0 || b->n_sites > 0)) {
     TimedLaunch tl(c, SOAPB_KERNEL_PAIR);
     CU(launch_pair(P, B, c->stream, keep));
@@ -1169,6 +1178,7 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
   c->keep_valid = keep;
   c->keep_sites = b->n_sites;
   c->keep_pairs = b->n_atom_pairs;
+  if (B.order) c->order_sites = b->n_sites;
   return SOAPB_OK;
 }
 
@@ -1186,6 +1196,8 @@ int ctx_contract(soapb_context *c, const soapb_batch *b, const double *d_soap, c
   P.n_pairs = B.n_pairs;
   P.n_sites = B.n_sites;
   LaunchCfg cfg = site_cfg(c, true);
+  // the descriptor call's site order (a permutation of the batch's sites)
+  if (!ch && c->order_sites == b->n_sites && b->n_sites > 0) B.order = c->order.as<int>();
   const int nch = (ch && b->n_sites > 0) ? ch->n : 1;
   for (int i = 0; i < nch && b->n_sites > 0; ++i) {
     B.site_lo = ch ? ch->bounds[i] : 0;

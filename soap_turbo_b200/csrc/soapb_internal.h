@@ -149,6 +149,9 @@ struct DevBatch {
   int *ticket;           // work counters of the persistent site kernels, in the last word
                          // of err (the kernels put them back to 0 when they finish)
   int site_lo, site_hi;  // the sites a site-kernel launch processes (all: 0, n_sites)
+  int *order = nullptr;  // n_sites: the order in which the persistent site kernels take the
+                         // sites, heaviest rows first (written by the pair kernel's scan when
+                         // one scan tile covers the batch), or null: index order
 };
 
 // Kernel launchers (soapb_mixed.cu, soapb_fp64.cu)

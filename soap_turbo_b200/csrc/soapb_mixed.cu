@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(kPairThreads)
   constexpr int NT = kPairThreads;
   extern __shared__ __align__(16) unsigned char smem[];
   if ((int)blockIdx.x < scan_tiles) {
-    prep_scan_tile<NT>(B, scan_tiles, (int *)smem);
+    prep_scan_tile<NT>(B, scan_tiles, (int *)smem, kScanSpins, (int *)smem + kScanTile);
     return;
   }
   constexpr int AW = row_len(LC);
@@ -505,7 +505,7 @@ __device__ __forceinline__ int take_ticket(const DevBatch &B, int *ticket) {
   const int n = B.site_hi - B.site_lo;
   const int t = atomicAdd(ticket, 1);
   if (t == n + (int)gridDim.x - 1) atomicExch(ticket, 0);
-  return B.site_lo + min(t, n);
+  return (B.order != nullptr && t < n) ? B.order[t] : B.site_lo + min(t, n);
 }
 __device__ __forceinline__ void first_site(const DevBatch &B, int *ticket, int *cur) {
   if (threadIdx.x == 0) {
@@ -2068,7 +2068,8 @@ static cudaError_t run_pair(const DevParams &P, const DevBatch &B, cudaStream_t 
                             int pair_hi, bool scan) {
   size_t sm = (size_t)P.off_rad + (size_t)P.n_species * SOAPB_RADSP_BYTES +
               (size_t)kPairThreads * pair_stage_stride(LC, TAB) * sizeof(float);
-  if (sm < kScanTile * sizeof(int)) sm = kScanTile * sizeof(int);  // scan tiles reuse it
+  // scan tiles reuse it: the tile's counts, then the site order's buckets
+  if (sm < (kScanTile + kScanOrderBuckets) * sizeof(int)) sm = (kScanTile + kScanOrderBuckets) * sizeof(int);
   auto kern = k_pair<AMAX, LC, OP, TAB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
