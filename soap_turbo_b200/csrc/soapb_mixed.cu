@@ -236,13 +236,25 @@ __host__ __device__ constexpr int pair_stage_stride(int LC, bool TAB) {
 // (FP32 evaluation of the FP64 expansion fitted per species; see RadTab)
 // instead of the FP64 expansion itself.
 constexpr int kPairThreads = 128;
+// CTAs of the pair kernel before its pair CTAs: the scan tiles, and one that
+// orders the sites when the batch is one tile and has an order to fill
+__host__ __device__ inline int pair_cta_offset(const DevBatch &B, int scan_tiles) {
+  return scan_tiles + ((B.order != nullptr && scan_tiles == 1) ? 1 : 0);
+}
 template <int AMAX, int LC, bool OP, bool TAB>
 __global__ void __launch_bounds__(kPairThreads)
     k_pair(const DevParams P, const DevBatch B, int do_der, int scan_tiles, int pair_lo, int pair_hi) {
   constexpr int NT = kPairThreads;
   extern __shared__ __align__(16) unsigned char smem[];
+  // the first CTAs scan n_neigh; with a site order to build, one more orders
+  // the sites (pair_cta_offset gives the host the same count)
+  const int lead = pair_cta_offset(B, scan_tiles);
   if ((int)blockIdx.x < scan_tiles) {
-    prep_scan_tile<NT>(B, scan_tiles, (int *)smem, kScanSpins, (int *)smem + kScanTile);
+    prep_scan_tile<NT>(B, scan_tiles, (int *)smem);
+    return;
+  }
+  if ((int)blockIdx.x < lead) {
+    order_sites<NT>(B, (int *)smem, (int *)smem + kScanTile);
     return;
   }
   constexpr int AW = row_len(LC);
@@ -254,7 +266,7 @@ __global__ void __launch_bounds__(kPairThreads)
   for (int t = threadIdx.x; t < head; t += NT) ((uint4 *)smem)[t] = ((const uint4 *)P.blob)[t];
   float *rows = (float *)(smem + (size_t)head * 16);
   __syncthreads();
-  const int k0 = pair_lo + ((int)blockIdx.x - scan_tiles) * NT;
+  const int k0 = pair_lo + ((int)blockIdx.x - lead) * NT;
   const int k = k0 + threadIdx.x;
   bool active = false;
   double x = 0.0, sq = 0.0;
@@ -2074,7 +2086,7 @@ static cudaError_t run_pair(const DevParams &P, const DevBatch &B, cudaStream_t 
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
   const int tiles = scan ? prep_scan_tiles(B.n_sites) : 0;
-  const int blocks = tiles + (pair_hi - pair_lo + kPairThreads - 1) / kPairThreads;
+  const int blocks = pair_cta_offset(B, tiles) + (pair_hi - pair_lo + kPairThreads - 1) / kPairThreads;
   if (blocks > 0) kern<<<blocks, kPairThreads, sm, s>>>(P, B, do_der, tiles, pair_lo, pair_hi);
   return cudaGetLastError();
 }

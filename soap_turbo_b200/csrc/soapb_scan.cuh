@@ -35,12 +35,9 @@ __device__ __forceinline__ void prep_error(const DevBatch &B, unsigned long long
 
 // One scan tile per calling block (NTH threads); sv: kScanTile ints of shared
 // memory; max_spins bounds the wait for a predecessor.
-// hist: kScanOrderBuckets ints of shared memory for the site order (below),
-// or null when the caller has none to spare.
-constexpr int kScanOrderBuckets = 256;
 template <int NTH>
 __device__ __forceinline__ void prep_scan_tile(const DevBatch &B, int scan_tiles, int *sv,
-                                               int max_spins = kScanSpins, int *hist = nullptr) {
+                                               int max_spins = kScanSpins) {
   constexpr int ITEMS = kScanTile / NTH;
   __shared__ int wtot[NTH / 32];
   __shared__ int s_tile, s_excl;
@@ -127,62 +124,73 @@ __device__ __forceinline__ void prep_scan_tile(const DevBatch &B, int scan_tiles
     B.off[B.n_sites] = (int)all;
     if (B.n_pairs >= 0 && all != (long long)B.n_pairs) prep_error(B, kErrCsr);
   }
-  // One tile holds every row length: order the sites heaviest first for the
-  // persistent site kernels (a counting sort on min(n_neigh, 255); the order
-  // within a count is whatever the atomics give, which changes only which CTA
-  // computes a site, not its result), so that their last sites are the
-  // lightest.
-  if (B.order != nullptr && hist != nullptr && scan_tiles == 1) {
-    constexpr int NB = kScanOrderBuckets, BPT = NB / NTH > 0 ? NB / NTH : 1;
-    for (int i = tid; i < NB; i += NTH) hist[i] = 0;
-    __syncthreads();
-    // the lanes of a warp with equal keys add once (rows of similar length are
-    // common, and same-address atomics in one warp would run one by one)
+}
+
+// The sites of a batch one scan tile covers, heaviest row first, into
+// B.order for the persistent site kernels (a counting sort on min(n_neigh, 255);
+// the order within a count is whatever the atomics give, which changes only
+// which CTA computes a site, not its result), so that their last sites are the
+// lightest.  One CTA of NTH threads, beside the scan CTA; sv: kScanTile ints
+// and hist: kScanOrderBuckets ints of shared memory.
+constexpr int kScanOrderBuckets = 256;
+template <int NTH>
+__device__ __forceinline__ void order_sites(const DevBatch &B, int *sv, int *hist) {
+  constexpr int ITEMS = kScanTile / NTH, NB = kScanOrderBuckets, BPT = NB / NTH > 0 ? NB / NTH : 1;
+  __shared__ int wtot[NTH / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < NB; i += NTH) hist[i] = 0;
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-      const int i = j * NTH + tid;
-      const int key = i < B.n_sites ? NB - 1 - min(sv[i], NB - 1) : -1;
-      const unsigned peers = __match_any_sync(0xffffffffu, key);
-      if (key >= 0 && lane == __ffs(peers) - 1) atomicAdd(&hist[key], __popc(peers));
+  for (int j = 0; j < ITEMS; ++j) {
+    const int i = j * NTH + tid;
+    sv[i] = i < B.n_sites ? max(B.n_neigh[i], 0) : 0;
+  }
+  __syncthreads();
+  // the lanes of a warp with equal keys add once (rows of similar length are
+  // common, and same-address atomics in one warp would run one by one)
+#pragma unroll
+  for (int j = 0; j < ITEMS; ++j) {
+    const int i = j * NTH + tid;
+    const int key = i < B.n_sites ? NB - 1 - min(sv[i], NB - 1) : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (key >= 0 && lane == __ffs(peers) - 1) atomicAdd(&hist[key], __popc(peers));
+  }
+  __syncthreads();
+  // exclusive scan of the counts: BPT consecutive buckets per thread
+  int loc = 0;
+  if (tid * BPT < NB)
+#pragma unroll
+    for (int b = 0; b < BPT; ++b) loc += hist[tid * BPT + b];
+  int xs = loc;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, xs, o);
+    if (lane >= o) xs += y;
+  }
+  if (lane == 31) wtot[warp] = xs;
+  __syncthreads();
+  int pre = xs - loc;
+#pragma unroll
+  for (int w = 0; w < NTH / 32; ++w)
+    if (w < warp) pre += wtot[w];
+  __syncthreads();
+  if (tid * BPT < NB)
+#pragma unroll
+    for (int b = 0; b < BPT; ++b) {
+      const int c = hist[tid * BPT + b];
+      hist[tid * BPT + b] = pre;
+      pre += c;
     }
-    __syncthreads();
-    // exclusive scan of the counts: BPT consecutive buckets per thread
-    int loc = 0;
-    if (tid * BPT < NB)
+  __syncthreads();
 #pragma unroll
-      for (int b = 0; b < BPT; ++b) loc += hist[tid * BPT + b];
-    int xs = loc;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, xs, o);
-      if (lane >= o) xs += y;
-    }
-    if (lane == 31) wtot[warp] = xs;
-    __syncthreads();
-    int pre = xs - loc;
-#pragma unroll
-    for (int w = 0; w < NTH / 32; ++w)
-      if (w < warp) pre += wtot[w];
-    __syncthreads();
-    if (tid * BPT < NB)
-#pragma unroll
-      for (int b = 0; b < BPT; ++b) {
-        const int c = hist[tid * BPT + b];
-        hist[tid * BPT + b] = pre;
-        pre += c;
-      }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-      const int i = j * NTH + tid;
-      const int key = i < B.n_sites ? NB - 1 - min(sv[i], NB - 1) : -1;
-      const unsigned peers = __match_any_sync(0xffffffffu, key);
-      const int leader = __ffs(peers) - 1;
-      int base = 0;
-      if (key >= 0 && lane == leader) base = atomicAdd(&hist[key], __popc(peers));
-      base = __shfl_sync(0xffffffffu, base, leader);
-      if (key >= 0) B.order[base + __popc(peers & ((1u << lane) - 1u))] = i;
-    }
+  for (int j = 0; j < ITEMS; ++j) {
+    const int i = j * NTH + tid;
+    const int key = i < B.n_sites ? NB - 1 - min(sv[i], NB - 1) : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (key >= 0 && lane == leader) base = atomicAdd(&hist[key], __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (key >= 0) B.order[base + __popc(peers & ((1u << lane) - 1u))] = i;
   }
 }
 
