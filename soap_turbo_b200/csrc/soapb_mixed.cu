@@ -13,7 +13,8 @@
 //      u_k = amp * preflm_k * P_k * ilexp_l in shared memory.
 //   B. c_nlm: one thread per (species, k) sums its species' entries in CSR
 //      order -- a fixed-order segmented reduction, no atomics.
-//   C. power spectrum of the kept components, compression, norm, normalise.
+//   C. power spectrum of the kept components (a dot product per component),
+//      compression, norm, normalise.
 // contract (soap_contract, src/soap_turbo.f90:1723-1884):
 //   G -> Gp -> Gu -> H(n,k) in shared memory, then one thread per entry
 //   recomputes R_n, dR_n/dr and the four angular factors in registers and
@@ -419,7 +420,7 @@ struct Layout {
   size_t C64, H, Rot, F;
   size_t X;
   size_t R, Rd, A;       // staging inside X
-  size_t C, P, S, Pl;    // per-site arrays inside X
+  size_t C, P, S;        // per-site arrays inside X
   size_t total;
 };
 
@@ -477,10 +478,6 @@ __host__ __device__ inline Layout make_layout(const DevParams &P, int NT, int AM
   L.C = x; x += nC * sizeof(float);
   L.P = x; x += (size_t)P.n_kept * sizeof(float);
   L.S = x; x += (size_t)P.n_soap * sizeof(float);
-  if (mode == 0 && P.ps_mt > 0) {
-    x = align_up(x, 16);
-    L.Pl = x; x += (size_t)(P.l_max + 1) * 16 * P.ps_mt * 8 * P.ps_nt * sizeof(float);
-  }
   const size_t end_site = x;
   o = end_stage > end_site ? end_stage : end_site;
   L.total = align_up(o, 16);
@@ -662,20 +659,24 @@ __device__ __forceinline__ void ps_tensor(const DevParams &P, const float *sC, f
 // spectrum of the kept components (src/soap_turbo.f90:750-795), the
 // compression, the norm and the normalised FP64 output (:798-809, 904-909),
 // and with keep the c_nlm and norm the contract reads.  keep: bit 0 keeps, bit
-// 1 accumulates into soap_out.  sPl: the tensor-core tile buffer (ps_mt > 0).
-// ps_ready: sPl already holds the power-spectrum tiles (the tcgen05 form).
+// 1 accumulates into soap_out.  tiles: the power spectrum from tensor-core
+// tiles in sPl (the tcgen05 kernel: formed there when ps_ready, else here with
+// mma.sync 3xTF32 tiles); else one dot product per kept component on the CUDA
+// cores (k_descriptor: measured faster than the mma.sync tiles, whose buffer
+// also held it to four CTAs per SM).
 template <int NT>
 __device__ __forceinline__ void site_output(const DevParams &P, unsigned char *smem, const float *sC, float *sP,
                                             float *sS, float *sPl, const int *kept, double *sRed, int site,
                                             double *__restrict__ soap_out, float *__restrict__ keep_c,
-                                            double *__restrict__ keep_norm, int keep, bool ps_ready = false) {
+                                            double *__restrict__ keep_norm, int keep, bool tiles,
+                                            bool ps_ready = false) {
   const int tid = threadIdx.x;
   const int KS = P.k_max | 1;
   const int n_max = P.n_max;
     // ---- C. power spectrum of the kept components (src/soap_turbo.f90:750-795)
     float *pout = P.cmap_identity ? sS : sP;
     double nrm2 = 0.0;
-    if (P.ps_mt > 0) {
+    if (tiles) {
       // on the tensor cores, then gathered into the kept components with the
       // sqrt 2 of n != n'
       if (!ps_ready) {
@@ -746,7 +747,7 @@ __device__ __forceinline__ void site_output(const DevParams &P, unsigned char *s
 
 // ------------------------------------------------------------ descriptor
 template <int NT, int AMAX, int LC>
-__global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, const DevBatch B,
+__global__ void __launch_bounds__(NT, 640 / NT) k_descriptor(const DevParams P, const DevBatch B,
                                                       double *__restrict__ soap_out,
                                                       float *__restrict__ keep_c,
                                                       double *__restrict__ keep_norm, int keep) {
@@ -882,8 +883,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_descriptor(const DevParams P, 
     for (int t = tid; t < 2 * n_max * KS; t += NT) sC[t] = (float)sC64[t];
     __syncthreads();
 
-    site_output<NT>(P, smem, sC, sP, sS, (float *)(smem + Ly.Pl), kept, sRed, site, soap_out, keep_c, keep_norm,
-                    keep);
+    site_output<NT>(P, smem, sC, sP, sS, nullptr, kept, sRed, site, soap_out, keep_c, keep_norm, keep, false);
     ahead_publish(sSite, nx, nx0, nx1);
   }
 }
@@ -1208,7 +1208,7 @@ __global__ void __launch_bounds__(NT) k_descriptor_tc(const DevParams P, const D
       if (failed) break;
     }
     site_output<NT>(P, smem, sC, sP, sS, (float *)(smem + Ly.Pl), kept, sRed, site, soap_out, keep_c, keep_norm,
-                    keep, ps_tc);
+                    keep, P.ps_mt > 0, ps_tc);
     ahead_publish(sSite, nx, nx0, nx1);
   }
   tc::fence_before_sync();
