@@ -662,8 +662,7 @@ __device__ __forceinline__ void ps_tensor(const DevParams &P, const float *sC, f
 // 1 accumulates into soap_out.  tiles: the power spectrum from tensor-core
 // tiles in sPl (the tcgen05 kernel: formed there when ps_ready, else here with
 // mma.sync 3xTF32 tiles); else one dot product per kept component on the CUDA
-// cores (k_descriptor: measured faster than the mma.sync tiles, whose buffer
-// also held it to four CTAs per SM).
+// cores (k_descriptor: measured faster than the mma.sync tiles).
 template <int NT>
 __device__ __forceinline__ void site_output(const DevParams &P, unsigned char *smem, const float *sC, float *sP,
                                             float *sS, float *sPl, const int *kept, double *sRed, int site,
