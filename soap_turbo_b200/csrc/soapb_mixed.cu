@@ -24,6 +24,8 @@
 // Everything is deterministic: no atomics touch results, and every reduction
 // runs in an order fixed by the launch shape.
 #include <cstdio>
+#include <mutex>
+#include <vector>
 
 #include "soapb_device.cuh"
 #include "soapb_scan.cuh"
@@ -1952,10 +1954,79 @@ __global__ void __launch_bounds__(NT) k_contract_tc(const DevParams P, const Dev
 }
 
 // ------------------------------------------------------------ launchers
+// What a launch needs from the runtime besides the launch itself -- the
+// kernel's dynamic shared memory limit raised, its resident CTAs per SM for a
+// persistent grid -- asked once per (kernel, device, CTA size, shared memory)
+// and remembered: the drop-in layer launches the same kernels once per site
+// chunk, and these queries would otherwise cost it host time on every call.
+struct LaunchMemo {
+  const void *fn;
+  int dev, threads;
+  size_t smem;
+  int sms, per_sm;
+};
+struct SmemLimit {
+  const void *fn;
+  int dev;
+  size_t smem;
+};
+static std::mutex g_launch_mu;
+static std::vector<LaunchMemo> g_launch_memo;
+static std::vector<SmemLimit> g_smem_limit;
+
+// Raises fn's dynamic shared memory limit on the current device to at least
+// smem (never lowers it, so that launches of other sizes stay valid).
+template <typename K>
+static cudaError_t ensure_smem_limit(K kernel, size_t smem) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const void *fn = (const void *)kernel;
+  std::lock_guard<std::mutex> g(g_launch_mu);
+  for (auto &x : g_smem_limit)
+    if (x.fn == fn && x.dev == dev) {
+      if (x.smem >= smem) return cudaSuccess;
+      e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess) x.smem = smem;
+      return e;
+    }
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) g_smem_limit.push_back({fn, dev, smem});
+  return e;
+}
+
+template <typename K>
+static int persistent_grid_query(K kernel, int threads, size_t smem, int dev, int &sms);
+
 template <typename K>
 static int persistent_grid(K kernel, int threads, size_t smem, int n_sites, int max_ctas) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
+  const void *fn = (const void *)kernel;
+  bool found = false;
+  {
+    std::lock_guard<std::mutex> g(g_launch_mu);
+    for (const auto &x : g_launch_memo)
+      if (x.fn == fn && x.dev == dev && x.threads == threads && x.smem == smem) {
+        sms = x.sms;
+        per_sm = x.per_sm;
+        found = true;
+        break;
+      }
+  }
+  if (!found) {
+    per_sm = persistent_grid_query(kernel, threads, smem, dev, sms);
+    std::lock_guard<std::mutex> g(g_launch_mu);
+    g_launch_memo.push_back({fn, dev, threads, smem, sms, per_sm});
+  }
+  int g = sms * (per_sm > 0 ? per_sm : 1);
+  if (max_ctas > 0 && g > max_ctas) g = max_ctas;
+  return g < n_sites ? g : n_sites;
+}
+
+template <typename K>
+static int persistent_grid_query(K kernel, int threads, size_t smem, int dev, int &sms) {
+  int per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
   // the count from the kernel's registers and shared memory as well: the
@@ -1976,9 +2047,7 @@ static int persistent_grid(K kernel, int threads, size_t smem, int n_sites, int 
   } else {
     cudaGetLastError();
   }
-  int g = sms * (per_sm > 0 ? per_sm : 1);
-  if (max_ctas > 0 && g > max_ctas) g = max_ctas;
-  return g < n_sites ? g : n_sites;
+  return per_sm;
 }
 
 // The tensor-core descriptor: definitions with alpha <= 8, l_max <= 8 and n_max
@@ -1990,7 +2059,7 @@ static cudaError_t run_descriptor_tc(const DevParams &P, const DevBatch &B, cons
                                      float *keep_c, double *keep_norm, int keep) {
   const size_t sm = descriptor_tc_smem(P);
   auto kern = k_descriptor_tc<128, 8, 8>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = ensure_smem_limit(kern, sm);
   if (e != cudaSuccess) return e;
   if (B.site_hi > B.site_lo) {
     int dev = 0, sms = 0;
@@ -2011,7 +2080,7 @@ static cudaError_t run_descriptor(const DevParams &P, const DevBatch &B, const L
     return run_descriptor_tc(P, B, cfg, soap, keep_c, keep_norm, keep);
   const size_t sm = make_layout(P, NT, AMAX, LC, 0).total;
   auto kern = k_descriptor<NT, AMAX, LC>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = ensure_smem_limit(kern, sm);
   if (e != cudaSuccess) return e;
   if (B.site_hi > B.site_lo) {
     const int grid = persistent_grid(kern, NT, sm, B.site_hi - B.site_lo, cfg.max_ctas);
@@ -2030,7 +2099,7 @@ static cudaError_t run_contract_tc(const DevParams &P, const DevBatch &B, const 
                                    const float *keep_c, const double *keep_norm, double *pair) {
   const size_t sm = contract_tc_smem(P);
   auto kern = k_contract_tc<128, 8, 8>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = ensure_smem_limit(kern, sm);
   if (e != cudaSuccess) return e;
   if (B.site_hi > B.site_lo) {
     int dev = 0, sms = 0;
@@ -2052,7 +2121,7 @@ static cudaError_t run_contract(const DevParams &P, const DevBatch &B, const Lau
     return run_contract_tc(P, B, cfg, soap, G, g_layout, sgn, keep_c, keep_norm, pair);
   const size_t sm = make_layout(P, NT, AMAX, LC, 1).total;
   auto kern = k_contract<NT, AMAX, LC>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = ensure_smem_limit(kern, sm);
   if (e != cudaSuccess) return e;
   if (B.site_hi > B.site_lo) {
     const int grid = persistent_grid(kern, NT, sm, B.site_hi - B.site_lo, cfg.max_ctas);
@@ -2082,7 +2151,7 @@ static cudaError_t run_pair(const DevParams &P, const DevBatch &B, cudaStream_t 
   // scan tiles reuse it: the tile's counts, then the site order's buckets
   if (sm < (kScanTile + kScanOrderBuckets) * sizeof(int)) sm = (kScanTile + kScanOrderBuckets) * sizeof(int);
   auto kern = k_pair<AMAX, LC, OP, TAB>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaError_t e = ensure_smem_limit(kern, sm);
   if (e != cudaSuccess) return e;
   const int tiles = scan ? prep_scan_tiles(B.n_sites) : 0;
   const int blocks = pair_cta_offset(B, tiles) + (pair_hi - pair_lo + kPairThreads - 1) / kPairThreads;
