@@ -239,6 +239,26 @@ void par_copy(void *dst, const void *src, size_t bytes) {
     std::memcpy((char *)dst + a, (const char *)src + a, b - a);
   }
 }
+// Whether `bytes` bytes of host memory are all zero bits (8-byte aligned,
+// length a multiple of 8), read by up to 8 threads.
+bool host_all_zero(const void *p, size_t bytes) {
+  const uint64_t *w = (const uint64_t *)p;
+  const size_t n = bytes / 8;
+  const int nt = copy_threads(bytes);
+  int nonzero = 0;
+#pragma omp parallel for num_threads(nt) schedule(static) reduction(| : nonzero)
+  for (int t = 0; t < nt; ++t) {
+    const size_t a = n * t / nt, b = n * (t + 1) / nt;
+    uint64_t acc = 0;
+    for (size_t i = a; i < b; i += 512) {  // blocks of 4 KB, so that a non-zero block ends the scan early
+      const size_t e = std::min(b, i + 512);
+      for (size_t j = i; j < e; ++j) acc |= w[j];
+      if (acc) break;
+    }
+    nonzero |= acc != 0;
+  }
+  return !nonzero;
+}
 // rows of `width` bytes, `rows` of them, at the given pitches
 void par_copy2d(void *dst, size_t dpitch, const void *src, size_t spitch, size_t width, size_t rows) {
   const int nt = std::min<int>(copy_threads(width * rows), (int)std::max<size_t>(rows, 1));
@@ -2192,12 +2212,19 @@ int copy_in_pairs(DropIn &d, const GetSoapIn &in, int i, int n_species, int n_pa
       return rc;
   }
   if (in.acc) {
-    // the chunk's rows of the caller's soap, which the descriptor adds into
+    // the chunk's rows of the caller's soap, which the descriptor adds into;
+    // rows that are all zero (the usual call: the reference's callers pass
+    // soap zeroed) are cleared on the device instead of copied, which saves
+    // their share of the host link
     const size_t b0 = 8 * (size_t)d.chunk[i] * in.n_soap, nb = 8 * (size_t)(d.chunk[i + 1] - d.chunk[i]) * in.n_soap;
-    int rc;
-    if ((rc = h2d_in(d.soap.as<uint8_t>() + b0, (const uint8_t *)in.soap + b0,
-                     in.st_soap ? in.st_soap + b0 : nullptr, nb, d.copy_in)))
-      return rc;
+    if (host_all_zero((const uint8_t *)in.soap + b0, nb)) {
+      CU(cudaMemsetAsync(d.soap.as<uint8_t>() + b0, 0, nb, d.copy_in));
+    } else {
+      int rc;
+      if ((rc = h2d_in(d.soap.as<uint8_t>() + b0, (const uint8_t *)in.soap + b0,
+                       in.st_soap ? in.st_soap + b0 : nullptr, nb, d.copy_in)))
+        return rc;
+    }
   }
   CU(cudaEventRecord(d.evs[i], d.copy_in));
   return SOAPB_OK;
@@ -2430,8 +2457,11 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
     if ((rc = upload(d.thetas, thetas, n_atom_pairs, s))) return rc;
     if ((rc = upload(d.phis, phis, n_atom_pairs, s))) return rc;
     if ((rc = d.soap.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
-    if (accumulate)
-      CU(cudaMemcpyAsync(d.soap.p, soap, 8 * (size_t)n_sites * n_soap, cudaMemcpyHostToDevice, s));
+    if (accumulate) {
+      const size_t nb = 8 * (size_t)n_sites * n_soap;
+      if (host_all_zero(soap, nb)) CU(cudaMemsetAsync(d.soap.p, 0, nb, s));
+      else CU(cudaMemcpyAsync(d.soap.p, soap, nb, cudaMemcpyHostToDevice, s));
+    }
   }
   soapb_batch &bt = d.batch;
   bt.n_sites = n_sites;
