@@ -209,6 +209,18 @@ struct HBuf {
 // memory, which must not reach the host-side staging copies (the runtime's
 // copy then either handles it or reports the misuse).  Only ordinary pageable
 // host memory is staged.
+// The device address of host memory the GPU can write directly (page-locked
+// and mapped), or null.
+void *mapped_host(const void *ptr) {
+  if (!ptr) return nullptr;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
 bool is_pinned(const void *ptr) {
   if (!ptr) return true;
   cudaPointerAttributes a;
@@ -1140,6 +1152,9 @@ struct SiteChunks {
   const int *bounds = nullptr;
   const long long *site_off = nullptr;
   std::function<int(int)> before, after;
+  // when set: whether chunk i adds into d_soap (asked after before(i)),
+  // instead of the call's accumulate
+  std::function<bool(int)> acc_of;
 };
 
 // accumulate: d_soap holds the caller's soap on entry and the descriptor is
@@ -1189,8 +1204,9 @@ int ctx_descriptor(soapb_context *c, const soapb_batch *b, double *d_soap, int k
     }
     {
       TimedLaunch tl(c, SOAPB_KERNEL_DESCRIPTOR);
+      const bool acc = (ch && ch->acc_of) ? ch->acc_of(i) : accumulate;
       CU(launch_descriptor(P, B, cfg, d_soap, keep ? c->keep_c.as<float>() : nullptr,
-                           keep ? c->keep_norm.as<double>() : nullptr, (keep ? 1 : 0) | (accumulate ? 2 : 0)));
+                           keep ? c->keep_norm.as<double>() : nullptr, (keep ? 1 : 0) | (acc ? 2 : 0)));
     }
     c->launches += 1;
     if (ch && ch->after && (rc = ch->after(i))) return rc;
@@ -2049,15 +2065,17 @@ struct DropIn {
   unsigned long long *err_host = nullptr;  // pinned copy of the prep error word
 };
 
-// Site chunks of the drop-in calls, at most 8.  In get_soap each chunk's pair
-// and site kernels run one after the other on the compute stream, and a small
-// chunk runs them well below the GPU's rate (its grids fill few SMs), so the
-// chunks are about 512 sites.  In soap_contract the copies in set the pace and
+// Site chunks of the drop-in calls, at most 8, of at least min_sites sites.
+// In get_soap each chunk's pair and site kernels run one after the other on
+// the compute stream, and a small chunk runs them well below the GPU's rate
+// (its grids fill few SMs), so the chunks are about 512 sites, or 850 when the
+// site kernel writes the soap rows into the caller's page-locked array (its
+// pace is then the host link's).  In soap_contract the copies in set the pace and
 // every chunk's kernels but the last run behind them: its chunks are about 384
 // sites, and the last is half the size of the others, to shorten what remains
 // after the last copy in.
-void plan_chunks(std::vector<int> &bounds, int n_sites, bool contract) {
-  const int n = std::max(1, std::min(8, n_sites / (contract ? 384 : 512)));
+void plan_chunks(std::vector<int> &bounds, int n_sites, bool contract, int min_sites) {
+  const int n = std::max(1, std::min(8, n_sites / min_sites));
   const bool short_last = contract && n > 1;
   const long long weight_sum = short_last ? 2LL * n - 1 : n;
   bounds.resize(n + 1);
@@ -2418,16 +2436,23 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
   GetSoapIn in{n_neigh, species, species_multiplicity, mask, rjs, thetas, phis, is_pinned(n_neigh),
                is_pinned(species), is_pinned(species_multiplicity), is_pinned(mask),
                is_pinned(rjs) && is_pinned(thetas) && is_pinned(phis)};
-  const bool soap_staged = chunked && !is_pinned(soap) && 8 * (size_t)n_sites * n_soap <= kStageCap;
+  // soap in page-locked memory the GPU can address: the site kernel writes
+  // its rows there directly, so they cross the host link while later sites
+  // compute, instead of in copies after each chunk's kernels
+  double *soap_dev = chunked ? (double *)mapped_host(soap) : nullptr;
+  const bool soap_staged = chunked && !soap_dev && !is_pinned(soap) && 8 * (size_t)n_sites * n_soap <= kStageCap;
   // The reference adds the compressed descriptor into the caller's soap
   // (src/soap_turbo.f90:798-802; its callers pass it zeroed) and overwrites an
   // uncompressed one; the caller's values therefore come in when compressing.
   const bool accumulate = compress_soap != 0 && n_sites > 0;
   in.soap = soap;
   in.n_soap = n_soap;
-  in.acc = accumulate;
+  in.acc = accumulate && !soap_dev;
   if (chunked) {
-    plan_chunks(d.chunk, n_sites, false);
+    // written in place, soap rows take the host link at the rate the site
+    // kernel produces them: fewer, larger chunks (each chunk's kernels start
+    // and end on a partly idle GPU)
+    plan_chunks(d.chunk, n_sites, false, soap_dev ? 850 : 512);
     nch = (int)d.chunk.size() - 1;
     if ((rc = dropin_streams(d, 3 * nch + 1))) return rc;
     if ((rc = d.n_neigh.ensure(4 * ((size_t)n_sites + 1)))) return rc;
@@ -2508,7 +2533,17 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
       return SOAPB_OK;
     };
     double *soap_dst = soap_staged ? d.st_out.as<double>() : soap;
+    // with soap_dev, a chunk whose caller rows are all zero (the usual call)
+    // is written without reading them; any other is added into in place.  The
+    // host scans a chunk's rows after its pair kernel is queued, while the
+    // GPU copies its inputs and runs that kernel.
+    if (soap_dev)
+      ch.acc_of = [&](int i) {
+        const size_t b0 = 8 * (size_t)d.chunk[i] * n_soap, nb = 8 * (size_t)(d.chunk[i + 1] - d.chunk[i]) * n_soap;
+        return accumulate && !host_all_zero((const uint8_t *)soap + b0, nb);
+      };
     ch.after = [&](int i) -> int {
+      if (soap_dev) return SOAPB_OK;
       const size_t lo = (size_t)d.chunk[i], hi = (size_t)d.chunk[i + 1];
       CU(cudaEventRecord(d.evs[nch + i], s));
       CU(cudaStreamWaitEvent(d.copy_out, d.evs[nch + i], 0));
@@ -2517,7 +2552,8 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
       if (soap_staged) CU(cudaEventRecord(d.evs[2 * nch + 1 + i], d.copy_out));
       return SOAPB_OK;
     };
-    rc = ctx_descriptor(c, &bt, d.soap.as<double>(), do_derivatives && contract, &ch, accumulate);
+    rc = ctx_descriptor(c, &bt, soap_dev ? soap_dev : d.soap.as<double>(), do_derivatives && contract, &ch,
+                        accumulate);
     // the staged soap rows, chunk by chunk as their copies arrive
     for (int i = 0; rc == 0 && soap_staged && i < nch; ++i) {
       const cudaError_t e = cudaEventSynchronize(d.evs[2 * nch + 1 + i]);
@@ -2627,19 +2663,22 @@ int soapb_soap_contract(const double *soap, const double *G, double sgn, double 
   // (evs[2 nch + 1 + i]).
   if ((rc = d.soap.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
   if ((rc = d.G.ensure(8 * ((size_t)n_sites * n_soap + 1)))) return rc;
-  if ((int)d.cchunk.size() < 2 || d.cchunk.back() != n_sites) plan_chunks(d.cchunk, n_sites, true);
+  if ((int)d.cchunk.size() < 2 || d.cchunk.back() != n_sites) plan_chunks(d.cchunk, n_sites, true, 384);
   const int nch = (int)d.cchunk.size() - 1;
   if ((rc = dropin_streams(d, 3 * nch + 1))) return rc;
   const size_t b_rows = align16(8 * (size_t)n_sites * n_soap);
   const bool big = 2 * b_rows > kStageCap;  // above the cap: the runtime's copies
   const bool st_soap = !big && !is_pinned(soap), st_G = !big && !is_pinned(G);
-  const bool st_pair = !is_pinned(pair) && 24 * (size_t)n_atom_pairs <= kStageCap;
+  // pair in page-locked memory the GPU can address: the contract writes the
+  // forces there directly, so no copy out follows the last chunk
+  double *pair_mapped = (double *)mapped_host(pair);
+  const bool st_pair = !pair_mapped && !is_pinned(pair) && 24 * (size_t)n_atom_pairs <= kStageCap;
   if ((st_soap || st_G) && (rc = d.st_in.ensure((st_soap ? b_rows : 0) + (st_G ? b_rows : 0)))) return rc;
   if (st_pair && (rc = d.st_out.ensure(24 * (size_t)n_atom_pairs))) return rc;
   double *sg_soap = st_soap ? d.st_in.as<double>() : nullptr;
   double *sg_G = st_G ? (double *)(d.st_in.as<uint8_t>() + (st_soap ? b_rows : 0)) : nullptr;
   double *pair_dst = st_pair ? d.st_out.as<double>() : pair;
-  double *dS = d.soap.as<double>(), *dG = d.G.as<double>(), *dP = d.pair.as<double>();
+  double *dS = d.soap.as<double>(), *dG = d.G.as<double>(), *dP = pair_mapped ? pair_mapped : d.pair.as<double>();
   CU(cudaEventRecord(d.evs[0], s));  // the copies in must not overwrite what earlier work still reads
   CU(cudaStreamWaitEvent(d.copy_in, d.evs[0], 0));
   SiteChunks ch;
@@ -2663,6 +2702,7 @@ int soapb_soap_contract(const double *soap, const double *G, double sgn, double 
     return SOAPB_OK;
   };
   ch.after = [&](int i) -> int {
+    if (pair_mapped) return SOAPB_OK;
     const long long p0 = d.host_off[d.cchunk[i]], p1 = d.host_off[d.cchunk[i + 1]];
     CU(cudaEventRecord(d.evs[nch + i], s));
     CU(cudaStreamWaitEvent(d.copy_out, d.evs[nch + i], 0));
