@@ -613,9 +613,11 @@ def run_ours(args):
                     "path": "the drop-in C ABI, soapb_get_soap(contract=1) + soapb_soap_contract, on pinned "
                             "host arrays, argument lists built once (as the Fortran shim passes them); "
                             "get_soap adds into the caller's compressed soap, as in the reference: the "
-                            "caller zeroes it before each step outside the timed calls, and all-zero rows "
-                            "are cleared on the device instead of copied in (a host scan of the rows "
-                            "inside the timed call); soap_contract copies soap in beside G",
+                            "caller zeroes it before each step outside the timed calls, and a host scan "
+                            "inside the timed call finds its rows all zero, so they are not read back; "
+                            "the site kernels write the soap rows and the pair forces into the pinned "
+                            "arrays themselves (the d2h bytes cross the host link as the kernels' "
+                            "stores, no copy follows); soap_contract copies soap in beside G",
                     "python_wrapper_ms_per_step": t_e2e_py * 1e3,
                     "pageable_ms_per_step": t_e2e_pg * 1e3},
             "gpu_launches": int(launches),
