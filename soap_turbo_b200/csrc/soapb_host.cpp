@@ -2068,9 +2068,9 @@ struct DropIn {
 // Site chunks of the drop-in calls, at most 8, of at least min_sites sites.
 // In get_soap each chunk's pair and site kernels run one after the other on
 // the compute stream, and a small chunk runs them well below the GPU's rate
-// (its grids fill few SMs), so the chunks are about 512 sites, or 850 when the
-// site kernel writes the soap rows into the caller's page-locked array (its
-// pace is then the host link's).  In soap_contract the copies in set the pace and
+// (its grids fill few SMs), so the chunks are about 512 sites, or at least
+// 4096 when the site kernel writes the soap rows into the caller's page-locked
+// array (its pace is then the host link's).  In soap_contract the copies in set the pace and
 // every chunk's kernels but the last run behind them: its chunks are about 384
 // sites, and the last is half the size of the others, to shorten what remains
 // after the last copy in.
@@ -2450,9 +2450,10 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species, c
   in.acc = accumulate && !soap_dev;
   if (chunked) {
     // written in place, soap rows take the host link at the rate the site
-    // kernel produces them: fewer, larger chunks (each chunk's kernels start
-    // and end on a partly idle GPU)
-    plan_chunks(d.chunk, n_sites, false, soap_dev ? 850 : 512);
+    // kernel produces them, and a chunk's kernels start and end with the link
+    // idle: chunks of at least 4096 sites (the chunking then only overlaps
+    // the inputs of large batches with their kernels)
+    plan_chunks(d.chunk, n_sites, false, soap_dev ? 4096 : 512);
     nch = (int)d.chunk.size() - 1;
     if ((rc = dropin_streams(d, 3 * nch + 1))) return rc;
     if ((rc = d.n_neigh.ensure(4 * ((size_t)n_sites + 1)))) return rc;

@@ -30,9 +30,10 @@ def _host(a, pinned, keep):
 
 @pytest.mark.parametrize("case", ["chunked_pinned", "chunked_pageable", "single_launch", "timed"])
 def test_compressed_soap_is_added_into(case):
-    # 1703 sites: the drop-in runs three site chunks, each copying its soap rows
-    # in beside its pair inputs; a quarter-size batch runs as one launch, and
-    # do_timing takes the unchunked path
+    # 1703 sites: from pageable arrays the drop-in runs three site chunks, each
+    # copying its soap rows in beside its pair inputs; a page-locked soap is
+    # added into in place by the site kernel (one chunk); a quarter-size batch
+    # runs as one launch, and do_timing takes the unchunked path
     w = syn.config(2, seed=41, scale=0.25 if case == "single_launch" else 1.0)
     nl = w.nl
     ctx = Context(w.hyper)
@@ -106,3 +107,45 @@ def test_soap_cart_der_self_columns_are_accumulated_into():
         np.testing.assert_allclose(d, np.transpose(cart0, (2, 1, 0))[first], rtol=1e-9, atol=1e-9)
     finally:
         D.set_basis_matrices(None)
+
+
+def test_pinned_soap_written_in_place_matches_the_staged_path():
+    """A page-locked soap is written by the site kernel in place, in chunks of
+    at least 4096 sites: a chunk whose entry rows are all zero is not read, any
+    other is added into in place (read over the host link).  Two chunks here,
+    the first entered all zero and the second partly not; soap, and the pair
+    forces the contract writes into a page-locked pair array, equal bit for bit
+    those of the same calls on pageable copies (staged through the library's
+    buffers in 512-site chunks whose rows are copied in and out)."""
+    w = syn.config(5, seed=43, scale=0.08)
+    nl = w.nl
+    assert nl.n_sites >= 2 * 4096
+    ctx = Context(w.hyper)
+    W, S = ctx.basis()
+    rng = np.random.default_rng(6)
+    nrm = O.get_soap(w.hyper, nl, W, S, do_derivatives=False).norm()
+    soap0 = np.zeros((ctx.n_soap, nl.n_sites))
+    lo = 3 * nl.n_sites // 4  # inside the second chunk
+    soap0[:, lo:] = 0.3 * nrm[lo:] / np.sqrt(ctx.n_soap) * rng.standard_normal((ctx.n_soap, nl.n_sites - lo))
+    G = rng.standard_normal((ctx.n_soap, nl.n_sites))
+    out = {}
+    keep = []
+    D.set_basis_matrices(W, S)
+    try:
+        for pinned in (True, False):
+            soap = _host(soap0, pinned, keep)
+            D.get_soap(**_dropin_args(w, soap), contract=True)
+            pair = _host(np.zeros((3, nl.n_pairs)), pinned, keep)
+            D.soap_contract(soap, _host(G.T, pinned, keep), 1.0, pair)
+            out[pinned] = (np.array(soap), np.array(pair))
+    finally:
+        D.set_basis_matrices(None)
+    assert np.all(np.isfinite(out[True][0])) and np.abs(out[True][1]).max() > 0
+    np.testing.assert_array_equal(out[True][0], out[False][0])
+    np.testing.assert_array_equal(out[True][1], out[False][1])
+    # the entry rows mattered where they were not zero
+    ref = Context(w.hyper)
+    b = ref.batch(nl)
+    plain = ref.descriptor(b, keep=False).cpu().numpy().T
+    assert np.abs(out[True][0][:, :lo] - plain[:, :lo]).max() < 1e-12
+    assert site_rel_err(out[True][0][:, lo:].T, plain[:, lo:].T) > 1e-4

@@ -156,8 +156,9 @@ def test_dropin_get_soap_and_contract(name):
 @pytest.mark.parametrize("pinned", [True, False])
 def test_dropin_site_chunks_match_the_context_layer(pinned):
     """The drop-in layer runs batches of 1024 sites or more in site chunks whose
-    copies overlap the kernels (1703 sites here: three chunks in get_soap, four
-    in soap_contract, the last of them half size); every site's result is
+    copies overlap the kernels (1703 sites here: three chunks in get_soap from
+    pageable arrays, one when the kernel writes a page-locked soap in place;
+    four in soap_contract, the last of them half size); every site's result is
     computed the same way, so soap and pair equal the single-launch context
     calls bit for bit, from pinned or pageable host arrays."""
     import torch
