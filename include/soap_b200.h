@@ -95,7 +95,11 @@ const char *soapb_version(void);
  * do_derivatives && !contract: soap_cart_der (3, n_soap, n_atom_pairs) is
  * written, computed in FP64 as the reference does; otherwise it may be NULL.
  * do_derivatives && contract: the state for soapb_soap_contract is kept.
- * do_timing prints per-phase GPU times, as the reference's do_timing does. */
+ * do_timing prints per-phase GPU times, as the reference's do_timing does.
+ * Host arrays may be pageable (staged through the library's page-locked
+ * buffers) or page-locked; a page-locked soap that the GPU can address (mapped,
+ * as every page-locked allocation is on a 64-bit host with unified addressing)
+ * is written by the site kernel in place while the call runs. */
 int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species,
                    const int32_t *species, int32_t max_species_multiplicity,
                    const int32_t *species_multiplicity, int32_t n_atom_pairs,
@@ -116,7 +120,8 @@ int soapb_get_soap(int32_t n_sites, const int32_t *n_neigh, int32_t n_species,
  * sgn * sum_s G(i,s) * d soap(s,i) / d r_k, for the batch of the last
  * soapb_get_soap called with do_derivatives and contract.  G is
  * G(n_sites, n_soap) (site fastest), soap the normalised descriptor that call
- * returned.  The extents must match that call. */
+ * returned.  The extents must match that call.  A page-locked pair that the
+ * GPU can address is written by the contract kernel in place. */
 int soapb_soap_contract(const double *soap, const double *G, double sgn, double *pair,
                         int32_t n_sites, int32_t n_soap, int32_t n_atom_pairs);
 
